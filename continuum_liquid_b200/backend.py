@@ -1,0 +1,179 @@
+"""ctypes binding of libclb200.so (include/clb200.h).
+
+``Backend`` replaces the reference's OpenCL context, queue and kernel dictionaries
+(Solver/Kernel/helper.py:22-69, solver.py:29-82): it loads the CUDA library, selects the device and
+exposes every C entry point as a method taking torch tensors. A non-zero status from the library
+becomes ``RuntimeError(clb_last_error())``, the exception type the reference raises for device and
+runtime failures (helper.py:55,64; output.py:94-96).
+
+There is no CPU path: if the library is missing or no B200 is visible, constructing a Backend
+raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+from typing import Any
+
+import torch
+
+from . import build as _build
+
+LIBRARY_PATH = _build.LIBRARY
+MG_MAX_LEVELS = 16
+SCAN_TILE = 4096  # elements per scan tile (SCAN_THREADS * SCAN_ITEMS in csrc/binning.cuh)
+
+P, I, L, F, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+
+# name -> argument types (every entry point returns int status unless listed in _RESTYPES)
+SIGNATURES: dict[str, list[Any]] = {
+    "clb_init": [I],
+    "clb_last_error": [],
+    "clb_device_error": [P],
+    "clb_abi_version": [],
+    "clb_count_particles_per_cell": [P, P, P, P, L, F, I, I, I, P],
+    "clb_scan_scratch_bytes": [L],
+    "clb_exclusive_prefix_sum": [P, P, P, L, P, L, P],
+    "clb_sort_particles": [P, P, P, P, P, P, P, P, P, P, L, P],
+    "clb_particle_to_grid_gather": [P, P, P, P, P, P, P, P, F, F, I, I, I, P],
+    "clb_particle_to_grid": [P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, L, L, F, F, I, I, I, P],
+    "clb_grid_to_particle": [P, P, P, P, P, P, P, P, L, F, I, I, I, F, P],
+    "clb_advect_particles": [P, P, L, F, P],
+    "clb_particle_domain_bc": [P, P, L, F, F, F, F, P],
+    "clb_particle_obstacle_bc": [P, P, P, P, L, F, I, I, I, P],
+    "clb_particle_update": [P, P, P, P, P, P, P, P, P, P, L, F, I, I, I, F, F, F, F, F, F, P],
+    "clb_update_velocity": [P, P, P, P, P, P, P, F, F, F, F, F, F, F, F, F, F, I, I, I, P],
+    "clb_grid_domain_bc": [P, P, P, I, I, I, P],
+    "clb_grid_obstacle_bc": [P, P, P, P, P, I, I, I, P],
+    "clb_pressure_rhs": [P, P, P, P, P, F, F, I, I, I, P],
+    "clb_pressure_correction": [P, P, P, P, F, F, I, I, I, P],
+    "clb_neumann_domain_bc": [P, I, I, I, P],
+    "clb_build_finest_operator": [P, P, P, P, P, I, I, I, P],
+    "clb_rbgs_step": [P, P, P, P, P, P, P, F, I, I, I, I, P],
+    "clb_restrict_residual": [P] * 14 + [F, I, I, I, I, I, I, P],
+    "clb_prolongate": [P, P, P, I, I, I, I, I, I, P],
+    "clb_coarse_smooth": [P, P, P, P, P, P, P, F, I, I, I, I, P],
+    "clb_mg_rhs_operator": [P, P, P, P, P, P, F, F, I, I, I, P],
+    "clb_mg_build_coarse": [P, P],
+    "clb_mg_w_cycle": [P, P, P, I, I, I, P],
+    "clb_mg_residual_partials": [L],
+    "clb_mg_residual_norms": [P, I, P, P, F, I, I, I, P, P, P, P],
+    "clb_mg_ir_init": [P, P, P, I, I, I, P],
+    "clb_mg_ir_update": [P, P, L, P],
+    "clb_mg_ir_store": [P, P, L, P],
+    "clb_voxelise_mesh": [P, P, I, I, I, I, F, F, F, F, I, P],
+    "clb_voxelise_direction": [P],
+}
+_RESTYPES = {"clb_last_error": ctypes.c_char_p, "clb_scan_scratch_bytes": ctypes.c_int64}
+
+
+class MGHierarchy(ctypes.Structure):
+    """Mirror of clb_mg_hierarchy (include/clb200.h)."""
+
+    _fields_ = [
+        ("levels", ctypes.c_int32),
+        ("shape", (ctypes.c_int32 * 3) * MG_MAX_LEVELS),
+        ("delta", ctypes.c_float),
+        ("reserved", ctypes.c_int32),
+        ("op0", ctypes.c_void_p),
+        ("p", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("b", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("mask", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("op", ctypes.c_void_p * MG_MAX_LEVELS),
+    ]
+
+
+def load_library(path: Path | str = LIBRARY_PATH) -> ctypes.CDLL:
+    """Load libclb200.so and declare every entry point's signature (no device work)."""
+    path = Path(path)
+    if not path.exists():
+        raise RuntimeError(
+            f"{path.name} is not built; run `python -m continuum_liquid_b200.build` (needs nvcc) before use"
+        )
+    lib = ctypes.CDLL(str(path))
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = _RESTYPES.get(name, ctypes.c_int)
+    return lib
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    """Device address of a contiguous tensor (None -> NULL)."""
+    if t is None:
+        return None
+    if not t.is_contiguous():
+        raise ValueError("tensors passed to the CUDA backend must be contiguous")
+    return t.data_ptr()
+
+
+class Backend:
+    """Loaded CUDA library bound to one device; methods enqueue on the given (or current) stream."""
+
+    _lock = threading.Lock()
+    _lib: ctypes.CDLL | None = None
+
+    def __init__(self, device: int | torch.device = 0):
+        if not torch.cuda.is_available():
+            raise RuntimeError("No CUDA device found: the Continuum Liquid B200 backend needs a B200 GPU")
+        self.device = torch.device("cuda", device if isinstance(device, int) else device.index or 0)
+        with Backend._lock:
+            if Backend._lib is None:
+                Backend._lib = load_library()
+        self.lib = Backend._lib
+        torch.cuda.set_device(self.device)
+        self._check(self.lib.clb_init(self.device.index), "clb_init")
+        direction = (ctypes.c_float * 3)()
+        self._check(self.lib.clb_voxelise_direction(direction), "clb_voxelise_direction")
+        self.voxelise_direction = tuple(float(x) for x in direction)
+
+    # -- plumbing -----------------------------------------------------------------------------
+    def _check(self, status: int, name: str) -> None:
+        if status != 0:
+            message = (self.lib.clb_last_error() or b"").decode(errors="replace")
+            raise RuntimeError(f"{name} failed: {message}")
+
+    def stream_handle(self, stream: torch.cuda.Stream | None = None) -> int:
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        return s.cuda_stream
+
+    def call(self, name: str, *args: Any, stream: torch.cuda.Stream | None = None) -> None:
+        """Invoke entry point `name`; tensors are passed as device pointers, the stream last."""
+        converted = [ptr(a) if isinstance(a, torch.Tensor) or a is None else a for a in args]
+        self._check(getattr(self.lib, name)(*converted, self.stream_handle(stream)), name)
+
+    def device_error(self) -> int:
+        code = ctypes.c_uint32(0)
+        self._check(self.lib.clb_device_error(ctypes.byref(code)), "clb_device_error")
+        return int(code.value)
+
+    def scan_scratch_bytes(self, count: int) -> int:
+        return int(self.lib.clb_scan_scratch_bytes(count))
+
+    @staticmethod
+    def scan_scratch_bytes_static(count: int) -> int:
+        """Same value as clb_scan_scratch_bytes without loading the library: a 16-byte ticket
+        header plus one 8-byte look-back status word per 4096-element tile."""
+        tiles = (int(count) + SCAN_TILE - 1) // SCAN_TILE
+        return 16 + 8 * max(tiles, 1)
+
+    def residual_partials(self, cells: int) -> int:
+        return int(self.lib.clb_mg_residual_partials(cells))
+
+    def call_hierarchy(self, name: str, hierarchy: MGHierarchy, *args: Any, stream=None) -> None:
+        converted = [ptr(a) if isinstance(a, torch.Tensor) or a is None else a for a in args]
+        status = getattr(self.lib, name)(ctypes.byref(hierarchy), *converted, self.stream_handle(stream))
+        self._check(status, name)
+
+
+_default: Backend | None = None
+
+
+def default_backend() -> Backend:
+    """Process-wide backend on cuda:0 (the reference serves compute_devices[0], helper.py:62-69)."""
+    global _default
+    if _default is None:
+        _default = Backend(0)
+    return _default

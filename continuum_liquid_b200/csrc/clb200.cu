@@ -1,0 +1,582 @@
+// libclb200.so: C ABI entry points (include/clb200.h). Unity build: the kernels live in the headers
+// included below; this file validates arguments, picks launch shapes and enqueues the kernels.
+#include "../../include/clb200.h"
+#include "binning.cuh"
+#include "particles.cuh"
+#include "grid.cuh"
+#include "multigrid.cuh"
+#include "voxelise.cuh"
+
+using namespace clb;
+
+#define CLB_STREAM(s) (reinterpret_cast<cudaStream_t>(s))
+#define CLB_GRID_ARGS_OK(nx, ny, nz)                                                                   \
+    CLB_REQUIRE((nx) >= 3 && (ny) >= 3 && (nz) >= 3, "grid %dx%dx%d: every dimension must be >= 3", (nx), (ny), \
+                (nz));                                                                                 \
+    CLB_REQUIRE((i64)(nx) * (ny) * (nz) < (1ll << 31), "grid %dx%dx%d has more than 2^31 cells", (nx), (ny), (nz))
+
+static const int kAbiVersion = 1;
+
+extern "C" {
+
+int clb_abi_version(void) { return kAbiVersion; }
+
+const char* clb_last_error(void) { return t_last_error; }
+
+int clb_init(int device) {
+    int count = 0;
+    if (check_call(cudaGetDeviceCount(&count), "cudaGetDeviceCount")) return 1;
+    CLB_REQUIRE(device >= 0 && device < count, "device %d not present (%d CUDA devices)", device, count);
+    if (check_call(cudaSetDevice(device), "cudaSetDevice")) return 1;
+    cudaDeviceProp prop;
+    if (check_call(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties")) return 1;
+    CLB_REQUIRE(prop.major == 10 && prop.minor == 0,
+                "device %d is sm_%d%d; this library is built for sm_100a (B200) only", device, prop.major, prop.minor);
+    g_sm_count = prop.multiProcessorCount;
+    const int smem_max = (int)coarse_smem_bytes(COARSE_SMEM_CELLS);
+    if (check_call(cudaFuncSetAttribute(k_coarse_solve<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        smem_max),
+                   "coarse solve attribute"))
+        return 1;
+    if (check_call(cudaFuncSetAttribute(k_coarse_solve<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        smem_max),
+                   "coarse solve attribute"))
+        return 1;
+    return 0;
+}
+
+int clb_device_error(uint32_t* code) {
+    CLB_REQUIRE(code != nullptr, "clb_device_error: null output");
+    unsigned int v = 0, zero = 0;
+    if (check_call(cudaMemcpyFromSymbol(&v, g_device_error, sizeof(v)), "read device error")) return 1;
+    if (check_call(cudaMemcpyToSymbol(g_device_error, &zero, sizeof(zero)), "clear device error")) return 1;
+    *code = v;
+    return 0;
+}
+
+// ---- particles --------------------------------------------------------------------------------
+
+int clb_count_particles_per_cell(const float* particles, int32_t* bin_counts, int32_t* keys, int32_t* ranks,
+                                 int64_t n, float inv_dx, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0 && n < (1ll << 31), "count_particles_per_cell: n=%lld out of range", (long long)n);
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && bin_counts, "count_particles_per_cell: null pointer");
+    k_bin_count<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, n, inv_dx, nx, ny, nz, bin_counts, keys,
+                                                                   ranks);
+    CLB_LAUNCH_CHECK("k_bin_count");
+    return 0;
+}
+
+int64_t clb_scan_scratch_bytes(int64_t count) { return scan_scratch_bytes(count); }
+
+int clb_exclusive_prefix_sum(const int32_t* values, int32_t* output, int32_t* total, int64_t count, void* scratch,
+                             int64_t scratch_bytes, void* stream) {
+    CLB_REQUIRE(count >= 0, "exclusive_prefix_sum: negative count");
+    CLB_REQUIRE(count == 0 || (values && output), "exclusive_prefix_sum: null pointer");
+    return launch_scan(values, output, count, scratch, scratch_bytes, total, CLB_STREAM(stream));
+}
+
+int clb_sort_particles(const float* particles, const float* velocity, float* particles_sorted, float* velocity_sorted,
+                       const int32_t* bin_offsets, const int32_t* bin_counts, const int32_t* keys,
+                       const int32_t* ranks, int32_t* perm, int32_t* slot_keys, int64_t n, void* stream) {
+    CLB_REQUIRE(n >= 0 && n < (1ll << 31), "sort_particles: n=%lld out of range", (long long)n);
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && velocity && particles_sorted && velocity_sorted && bin_offsets && bin_counts && keys &&
+                    ranks && perm && slot_keys,
+                "sort_particles: null pointer");
+    cudaStream_t s = CLB_STREAM(stream);
+    k_scatter_perm<<<blocks_for(n, PT), PT, 0, s>>>(keys, ranks, bin_offsets, n, perm, slot_keys);
+    CLB_LAUNCH_CHECK("k_scatter_perm");
+    k_stable_gather<<<blocks_for(n, PT), PT, 0, s>>>(perm, slot_keys, bin_offsets, bin_counts, particles, velocity, n,
+                                                      particles_sorted, velocity_sorted);
+    CLB_LAUNCH_CHECK("k_stable_gather");
+    return 0;
+}
+
+int clb_particle_to_grid_gather(const float* particles, const float* velocity, const int32_t* bin_offsets,
+                                const int32_t* bin_counts, float* u, float* v, float* w, float* fluid_fraction,
+                                float inv_dx, float inv_particles_per_cell, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(bin_offsets && bin_counts && u && v && w && fluid_fraction, "particle_to_grid_gather: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_p2g_gather<<<blocks_for(C * P2G_LANES, P2G_THREADS), P2G_THREADS, 0, CLB_STREAM(stream)>>>(
+        particles, velocity, bin_offsets, bin_counts, u, v, w, fluid_fraction, inv_dx, inv_particles_per_cell, nx, ny,
+        nz);
+    CLB_LAUNCH_CHECK("k_p2g_gather");
+    return 0;
+}
+
+int clb_particle_to_grid(const float* particles, const float* velocity, float* particles_work, float* velocity_work,
+                         float* u, float* v, float* w, float* fluid_fraction, int32_t* bin_counts,
+                         int32_t* bin_offsets, int32_t* keys, int32_t* ranks, int32_t* perm, int32_t* slot_keys,
+                         void* scan_scratch, int64_t scan_scratch_bytes_, int64_t n, float inv_dx,
+                         float inv_ppc, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(inv_dx > 0.0f && inv_ppc > 0.0f, "particle_to_grid: inv_dx and inv_particles_per_cell must be > 0");
+    CLB_REQUIRE(n >= 0 && n < (1ll << 31), "particle_to_grid: n=%lld out of range", (long long)n);
+    cudaStream_t s = CLB_STREAM(stream);
+    const i64 C = (i64)nx * ny * nz;
+    if (check_call(cudaMemsetAsync(bin_counts, 0, sizeof(int32_t) * C, s), "zero bin_counts")) return 1;
+    if (clb_count_particles_per_cell(particles, bin_counts, keys, ranks, n, inv_dx, nx, ny, nz, stream)) return 1;
+    if (clb_exclusive_prefix_sum(bin_counts, bin_offsets, nullptr, C, scan_scratch, scan_scratch_bytes_, stream))
+        return 1;
+    if (clb_sort_particles(particles, velocity, particles_work, velocity_work, bin_offsets, bin_counts, keys, ranks,
+                           perm, slot_keys, n, stream))
+        return 1;
+    return clb_particle_to_grid_gather(particles_work, velocity_work, bin_offsets, bin_counts, u, v, w, fluid_fraction,
+                                       inv_dx, inv_ppc, nx, ny, nz, stream);
+}
+
+int clb_grid_to_particle(float* velocity, const float* particles, const float* u, const float* v, const float* w,
+                         const float* u_old, const float* v_old, const float* w_old, int64_t n, float inv_dx, int nx,
+                         int ny, int nz, float flip_ratio, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0, "grid_to_particle: negative n");
+    if (n == 0) return 0;
+    CLB_REQUIRE(velocity && particles && u && v && w && u_old && v_old && w_old, "grid_to_particle: null pointer");
+    k_grid_to_particle<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(velocity, particles, u, v, w, u_old, v_old,
+                                                                          w_old, n, inv_dx, nx, ny, nz, flip_ratio);
+    CLB_LAUNCH_CHECK("k_grid_to_particle");
+    return 0;
+}
+
+int clb_advect_particles(float* particles, const float* velocity, int64_t n, float dt, void* stream) {
+    CLB_REQUIRE(n >= 0, "advect_particles: negative n");
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && velocity, "advect_particles: null pointer");
+    k_advect<<<blocks_for(3 * n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, velocity, 3 * n, dt);
+    CLB_LAUNCH_CHECK("k_advect");
+    return 0;
+}
+
+int clb_particle_domain_bc(float* particles, float* velocity, int64_t n, float lower, float upper_x, float upper_y,
+                           float upper_z, void* stream) {
+    CLB_REQUIRE(n >= 0, "particle_domain_bc: negative n");
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && velocity, "particle_domain_bc: null pointer");
+    k_particle_domain_bc<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, velocity, n, lower, upper_x,
+                                                                            upper_y, upper_z);
+    CLB_LAUNCH_CHECK("k_particle_domain_bc");
+    return 0;
+}
+
+int clb_particle_obstacle_bc(float* particles, const float* previous, float* velocity, const uint8_t* obstacle,
+                             int64_t n, float inv_dx, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0, "particle_obstacle_bc: negative n");
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && previous && velocity && obstacle, "particle_obstacle_bc: null pointer");
+    k_particle_obstacle_bc<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, previous, velocity, obstacle, n,
+                                                                              inv_dx, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_particle_obstacle_bc");
+    return 0;
+}
+
+int clb_particle_update(float* particles, float* velocity, float* previous_out, const float* u, const float* v,
+                        const float* w, const float* u_old, const float* v_old, const float* w_old,
+                        const uint8_t* obstacle, int64_t n, float inv_dx, int nx, int ny, int nz, float flip_ratio,
+                        float dt, float lower, float upper_x, float upper_y, float upper_z, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0, "particle_update: negative n");
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && velocity && u && v && w && u_old && v_old && w_old, "particle_update: null pointer");
+    k_particle_update<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(
+        particles, velocity, previous_out, u, v, w, u_old, v_old, w_old, obstacle, n, inv_dx, nx, ny, nz, flip_ratio,
+        dt, lower, upper_x, upper_y, upper_z);
+    CLB_LAUNCH_CHECK("k_particle_update");
+    return 0;
+}
+
+// ---- grid -------------------------------------------------------------------------------------
+
+int clb_update_velocity(const float* u, const float* v, const float* w, float* result_u, float* result_v,
+                        float* result_w, const float* fluid_fraction, float gravity_x, float gravity_y,
+                        float gravity_z, float force_x, float force_y, float force_z, float rho, float nu,
+                        float inv_dx2, float dt, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(u && v && w && result_u && result_v && result_w && fluid_fraction, "update_velocity: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_update_velocity<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, result_u, result_v, result_w,
+                                                                         fluid_fraction, gravity_x, gravity_y,
+                                                                         gravity_z, force_x, force_y, force_z, rho, nu,
+                                                                         inv_dx2, dt, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_update_velocity");
+    return 0;
+}
+
+int clb_grid_domain_bc(float* u, float* v, float* w, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(u && v && w, "grid_domain_bc: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_grid_domain_bc<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_grid_domain_bc");
+    return 0;
+}
+
+int clb_grid_obstacle_bc(float* u, float* v, float* w, float* fluid_fraction, const uint8_t* obstacle, int nx, int ny,
+                         int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(u && v && w && fluid_fraction && obstacle, "grid_obstacle_bc: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    cudaStream_t s = CLB_STREAM(stream);
+    k_grid_obstacle_bc<<<blocks_for(C, GT), GT, 0, s>>>(u, v, w, fluid_fraction, obstacle, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_grid_obstacle_bc");
+    k_extrapolate_obstacle_velocity<<<blocks_for(C, GT), GT, 0, s>>>(u, v, w, obstacle, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_extrapolate_obstacle_velocity");
+    return 0;
+}
+
+int clb_pressure_rhs(const float* u, const float* v, const float* w, const float* fluid_fraction, float* rhs,
+                     float rho_over_dt, float inv_dx, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(u && v && w && fluid_fraction && rhs, "pressure_rhs: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_pressure_rhs<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, fluid_fraction, rhs, rho_over_dt, inv_dx,
+                                                                      nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_pressure_rhs");
+    return 0;
+}
+
+int clb_pressure_correction(float* u, float* v, float* w, const float* pressure, float dt_over_rho, float inv_dx,
+                            int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(u && v && w && pressure, "pressure_correction: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_pressure_correction<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, pressure, dt_over_rho, inv_dx, nx,
+                                                                             ny, nz);
+    CLB_LAUNCH_CHECK("k_pressure_correction");
+    return 0;
+}
+
+int clb_neumann_domain_bc(float* pressure, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(pressure, "neumann_domain_bc: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_neumann_domain_bc<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(pressure, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_neumann_domain_bc");
+    return 0;
+}
+
+// ---- multigrid, reference layout ----------------------------------------------------------------
+
+int clb_build_finest_operator(const float* mask, float* diagonal, float* weight_x, float* weight_y, float* weight_z,
+                              int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(mask && diagonal && weight_x && weight_y && weight_z, "build_finest_operator: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_ref_build_finest_operator<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(mask, diagonal, weight_x, weight_y,
+                                                                                     weight_z, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_ref_build_finest_operator");
+    return 0;
+}
+
+int clb_rbgs_step(float* p, const float* b, const float* mask, const float* diagonal, const float* weight_x,
+                  const float* weight_y, const float* weight_z, float delta, int parity, int nx, int ny, int nz,
+                  void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(parity == 0 || parity == 1, "rbgs_step: parity must be 0 or 1");
+    CLB_REQUIRE(p && b && mask && diagonal && weight_x && weight_y && weight_z, "rbgs_step: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_ref_rbgs_step<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(p, b, mask, diagonal, weight_x, weight_y,
+                                                                         weight_z, delta, parity, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_ref_rbgs_step");
+    return 0;
+}
+
+int clb_restrict_residual(const float* fine_p, const float* fine_b, const float* fine_mask, const float* fine_diagonal,
+                          const float* fine_weight_x, const float* fine_weight_y, const float* fine_weight_z,
+                          float* coarse_p, float* coarse_b, float* coarse_mask, float* coarse_diagonal,
+                          float* coarse_weight_x, float* coarse_weight_y, float* coarse_weight_z, float delta,
+                          int fine_nx, int fine_ny, int fine_nz, int coarse_nx, int coarse_ny, int coarse_nz,
+                          void* stream) {
+    CLB_GRID_ARGS_OK(fine_nx, fine_ny, fine_nz);
+    CLB_GRID_ARGS_OK(coarse_nx, coarse_ny, coarse_nz);
+    CLB_REQUIRE(fine_p && fine_b && fine_mask && fine_diagonal && fine_weight_x && fine_weight_y && fine_weight_z &&
+                    coarse_p && coarse_b && coarse_mask && coarse_diagonal && coarse_weight_x && coarse_weight_y &&
+                    coarse_weight_z,
+                "restrict_residual: null pointer");
+    const i64 C = (i64)coarse_nx * coarse_ny * coarse_nz;
+    k_ref_restrict_residual<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(
+        fine_p, fine_b, fine_mask, fine_diagonal, fine_weight_x, fine_weight_y, fine_weight_z, coarse_p, coarse_b,
+        coarse_mask, coarse_diagonal, coarse_weight_x, coarse_weight_y, coarse_weight_z, delta, fine_nx, fine_ny,
+        fine_nz, coarse_nx, coarse_ny, coarse_nz);
+    CLB_LAUNCH_CHECK("k_ref_restrict_residual");
+    return 0;
+}
+
+int clb_prolongate(const float* coarse_error, float* fine_p, const float* fine_mask, int coarse_nx, int coarse_ny,
+                   int coarse_nz, int fine_nx, int fine_ny, int fine_nz, void* stream) {
+    CLB_GRID_ARGS_OK(fine_nx, fine_ny, fine_nz);
+    CLB_GRID_ARGS_OK(coarse_nx, coarse_ny, coarse_nz);
+    CLB_REQUIRE(coarse_error && fine_p && fine_mask, "prolongate: null pointer");
+    const i64 C = (i64)fine_nx * fine_ny * fine_nz;
+    k_ref_prolongate<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(coarse_error, fine_p, fine_mask, coarse_nx,
+                                                                          coarse_ny, coarse_nz, fine_nx, fine_ny,
+                                                                          fine_nz);
+    CLB_LAUNCH_CHECK("k_ref_prolongate");
+    return 0;
+}
+
+// The reference-layout coarse smooth runs one block of 1024 threads directly on the float arrays:
+// rbgs_step's update formula in a loop with block barriers, like multigrid.cl:232-264.
+__global__ void __launch_bounds__(COARSE_THREADS) k_ref_coarse_smooth(float* p, const float* b, const float* mask,
+                                                                       const float* diag, const float* wx,
+                                                                       const float* wy, const float* wz, float delta,
+                                                                       int iterations, int nx, int ny, int nz) {
+    const int C = nx * ny * nz;
+    const float d2 = delta * delta;
+    const i64 sx = (i64)ny * nz, sy = nz;
+    for (int it = 0; it < iterations; ++it)
+        for (int parity = 0; parity < 2; ++parity) {
+            for (int c = threadIdx.x; c < C; c += COARSE_THREADS) {
+                int i, j, k;
+                gcoord(c, ny, nz, i, j, k);
+                if (!interior(i, j, k, nx, ny, nz) || mask[c] <= 0.0f || ((i + j + k) & 1) != parity) continue;
+                const float d = diag[c];
+                if (d > 0.0f) p[c] = (ref_wsum(p, wx, wy, wz, c, sx, sy) - d2 * b[c]) / d;
+            }
+            __syncthreads();
+        }
+}
+
+int clb_coarse_smooth(float* p, const float* b, const float* mask, const float* diagonal, const float* weight_x,
+                      const float* weight_y, const float* weight_z, float delta, int iterations, int nx, int ny,
+                      int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(iterations >= 0, "coarse_smooth: negative iterations");
+    CLB_REQUIRE(p && b && mask && diagonal && weight_x && weight_y && weight_z, "coarse_smooth: null pointer");
+    k_ref_coarse_smooth<<<1, COARSE_THREADS, 0, CLB_STREAM(stream)>>>(p, b, mask, diagonal, weight_x, weight_y,
+                                                                       weight_z, delta, iterations, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_ref_coarse_smooth");
+    return 0;
+}
+
+// ---- multigrid, packed layout ---------------------------------------------------------------------
+
+int clb_mg_rhs_operator(const float* u, const float* v, const float* w, const float* fluid_fraction, float* rhs,
+                        uint8_t* op0, float rho_over_dt, float inv_dx, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(u && v && w && fluid_fraction && rhs && op0, "mg_rhs_operator: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_rhs_op0<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(u, v, w, fluid_fraction, rhs, op0, rho_over_dt,
+                                                                   inv_dx, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_rhs_op0");
+    return 0;
+}
+
+static int check_hierarchy(const clb_mg_hierarchy* h) {
+    CLB_REQUIRE(h != nullptr, "multigrid: null hierarchy");
+    CLB_REQUIRE(h->levels >= 1 && h->levels <= CLB_MG_MAX_LEVELS, "multigrid: %d levels (1..%d allowed)", h->levels,
+                CLB_MG_MAX_LEVELS);
+    CLB_REQUIRE(h->op0 != nullptr, "multigrid: null level-0 operator");
+    for (int l = 0; l < h->levels; ++l) {
+        CLB_GRID_ARGS_OK(h->shape[l][0], h->shape[l][1], h->shape[l][2]);
+        if (l > 0)
+            CLB_REQUIRE(h->p[l] && h->b[l] && h->mask[l] && h->op[l], "multigrid: level %d has a null array", l);
+    }
+    return 0;
+}
+
+int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream) {
+    if (check_hierarchy(h)) return 1;
+    cudaStream_t s = CLB_STREAM(stream);
+    for (int l = 1; l < h->levels; ++l) {
+        const int* f = h->shape[l - 1];
+        const int* c = h->shape[l];
+        const i64 C = (i64)c[0] * c[1] * c[2];
+        if (l == 1)
+            k_coarse_operator<true><<<blocks_for(C, MGT), MGT, 0, s>>>(
+                h->op0, nullptr, nullptr, (float4*)h->op[l], h->mask[l], f[0], f[1], f[2], c[0], c[1], c[2]);
+        else
+            k_coarse_operator<false><<<blocks_for(C, MGT), MGT, 0, s>>>(nullptr, (const float4*)h->op[l - 1],
+                                                                         h->mask[l - 1], (float4*)h->op[l], h->mask[l],
+                                                                         f[0], f[1], f[2], c[0], c[1], c[2]);
+        CLB_LAUNCH_CHECK("k_coarse_operator");
+    }
+    return 0;
+}
+
+namespace {
+
+struct LevelView {
+    float* p;
+    const float* b;
+    const uint8_t* op0;
+    const float4* opc;
+    const uint8_t* mask;
+    int nx, ny, nz;
+    bool l0;
+};
+
+LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rhs) {
+    LevelView v;
+    v.l0 = (l == 0);
+    v.p = v.l0 ? x : h->p[l];
+    v.b = v.l0 ? rhs : h->b[l];
+    v.op0 = h->op0;
+    v.opc = v.l0 ? nullptr : (const float4*)h->op[l];
+    v.mask = v.l0 ? nullptr : h->mask[l];
+    v.nx = h->shape[l][0];
+    v.ny = h->shape[l][1];
+    v.nz = h->shape[l][2];
+    return v;
+}
+
+int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
+    const i64 C = (i64)v.nx * v.ny * v.nz;
+    for (int it = 0; it < iterations; ++it)
+        for (int parity = 0; parity < 2; ++parity) {
+            if (v.l0)
+                k_rbgs<true><<<blocks_for(C, MGT), MGT, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta, parity, v.nx,
+                                                                 v.ny, v.nz);
+            else
+                k_rbgs<false><<<blocks_for(C, MGT), MGT, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta, parity, v.nx,
+                                                                  v.ny, v.nz);
+            CLB_LAUNCH_CHECK("k_rbgs");
+        }
+    return 0;
+}
+
+int coarse_solve(const LevelView& v, float delta, int iterations, cudaStream_t s) {
+    const int C = v.nx * v.ny * v.nz;
+    if (C <= COARSE_SMEM_CELLS) {
+        const size_t bytes = coarse_smem_bytes(C);
+        if (v.l0)
+            k_coarse_solve<true, true><<<1, COARSE_THREADS, bytes, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta,
+                                                                         iterations, v.nx, v.ny, v.nz);
+        else
+            k_coarse_solve<true, false><<<1, COARSE_THREADS, bytes, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta,
+                                                                          iterations, v.nx, v.ny, v.nz);
+    } else {
+        if (v.l0)
+            k_coarse_solve<false, true><<<1, COARSE_THREADS, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta,
+                                                                      iterations, v.nx, v.ny, v.nz);
+        else
+            k_coarse_solve<false, false><<<1, COARSE_THREADS, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta,
+                                                                       iterations, v.nx, v.ny, v.nz);
+    }
+    CLB_LAUNCH_CHECK("k_coarse_solve");
+    return 0;
+}
+
+// multigrid.py:53-187 w_cycle
+int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int pre, int post, int coarse_iters,
+            cudaStream_t s) {
+    const LevelView v = level_view(h, level, x, rhs);
+    if (level == h->levels - 1) return coarse_solve(v, h->delta, pre + coarse_iters, s);
+    if (smooth(v, h->delta, pre, s)) return 1;
+    const LevelView c = level_view(h, level + 1, x, rhs);
+    const i64 Cc = (i64)c.nx * c.ny * c.nz;
+    if (v.l0)
+        k_restrict<true><<<blocks_for(Cc, MGT), MGT, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, c.p,
+                                                              const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
+                                                              c.nx, c.ny, c.nz);
+    else
+        k_restrict<false><<<blocks_for(Cc, MGT), MGT, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, c.p,
+                                                               const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
+                                                               c.nx, c.ny, c.nz);
+    CLB_LAUNCH_CHECK("k_restrict");
+    if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+    if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+    const i64 Cf = (i64)v.nx * v.ny * v.nz;
+    if (v.l0)
+        k_prolong<true><<<blocks_for(Cf, MGT), MGT, 0, s>>>(c.p, v.p, v.op0, nullptr, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                                             v.nz);
+    else
+        k_prolong<false><<<blocks_for(Cf, MGT), MGT, 0, s>>>(c.p, v.p, nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                                              v.nz);
+    CLB_LAUNCH_CHECK("k_prolong");
+    return smooth(v, h->delta, post, s);
+}
+
+}  // namespace
+
+int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pre_smooth, int post_smooth,
+                   int coarse_iterations, void* stream) {
+    if (check_hierarchy(h)) return 1;
+    CLB_REQUIRE(x && rhs, "mg_w_cycle: null level-0 array");
+    CLB_REQUIRE(pre_smooth >= 0 && post_smooth >= 0 && coarse_iterations >= 0, "mg_w_cycle: negative sweep count");
+    return w_cycle(h, 0, x, rhs, pre_smooth, post_smooth, coarse_iterations, CLB_STREAM(stream));
+}
+
+int clb_mg_residual_partials(int64_t cells) {
+    const i64 need = (cells + RN_THREADS - 1) / RN_THREADS;
+    const i64 cap = 148 * 8;
+    return (int)(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
+int clb_mg_residual_norms(const void* p, int p_is_double, const float* b, const uint8_t* op0, float delta, int nx,
+                          int ny, int nz, float* r_out, void* partials, double* out, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(p && b && op0 && partials && out, "mg_residual_norms: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    const int blocks = clb_mg_residual_partials(C);
+    const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
+    cudaStream_t s = CLB_STREAM(stream);
+    if (p_is_double)
+        k_residual_norms<double><<<blocks, RN_THREADS, 0, s>>>((const double*)p, b, op0, inv_delta2, nx, ny, nz, r_out,
+                                                               (double2*)partials);
+    else
+        k_residual_norms<float><<<blocks, RN_THREADS, 0, s>>>((const float*)p, b, op0, inv_delta2, nx, ny, nz, r_out,
+                                                              (double2*)partials);
+    CLB_LAUNCH_CHECK("k_residual_norms");
+    k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
+    CLB_LAUNCH_CHECK("k_reduce_partials");
+    return 0;
+}
+
+int clb_mg_ir_init(const float* p32, const uint8_t* op0, double* p64, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(p32 && op0 && p64, "mg_ir_init: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    k_ir_init<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(p32, op0, p64, nx, ny, nz);
+    CLB_LAUNCH_CHECK("k_ir_init");
+    return 0;
+}
+
+int clb_mg_ir_update(double* p64, const float* e, int64_t cells, void* stream) {
+    CLB_REQUIRE(p64 && e && cells >= 0, "mg_ir_update: bad arguments");
+    if (cells == 0) return 0;
+    k_ir_update<<<blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream)>>>(p64, e, cells);
+    CLB_LAUNCH_CHECK("k_ir_update");
+    return 0;
+}
+
+int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream) {
+    CLB_REQUIRE(p64 && p32 && cells >= 0, "mg_ir_store: bad arguments");
+    if (cells == 0) return 0;
+    k_ir_store<<<blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream)>>>(p64, p32, cells);
+    CLB_LAUNCH_CHECK("k_ir_store");
+    return 0;
+}
+
+// ---- voxelisation ---------------------------------------------------------------------------------
+
+int clb_voxelise_direction(float* out3) {
+    CLB_REQUIRE(out3 != nullptr, "voxelise_direction: null output");
+    voxelise_direction(out3);
+    return 0;
+}
+
+int clb_voxelise_mesh(const float* triangles, uint8_t* mask, int triangle_count, int nx, int ny, int nz, float delta,
+                      float ox, float oy, float oz, int cull, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(triangle_count >= 0, "voxelise_mesh: negative triangle count");
+    CLB_REQUIRE(mask != nullptr, "voxelise_mesh: null mask");
+    if (triangle_count == 0) return 0;
+    CLB_REQUIRE(triangles != nullptr, "voxelise_mesh: null triangles");
+    float d[3];
+    voxelise_direction(d);
+    const dim3 grid((nz + VOX_BK - 1) / VOX_BK, (ny + VOX_BJ - 1) / VOX_BJ, (nx + VOX_BI - 1) / VOX_BI);
+    if (cull)
+        k_voxelise<true><<<grid, VOX_THREADS, 0, CLB_STREAM(stream)>>>(triangles, mask, triangle_count, nx, ny, nz,
+                                                                       delta, ox, oy, oz, d[0], d[1], d[2]);
+    else
+        k_voxelise<false><<<grid, VOX_THREADS, 0, CLB_STREAM(stream)>>>(triangles, mask, triangle_count, nx, ny, nz,
+                                                                        delta, ox, oy, oz, d[0], d[1], d[2]);
+    CLB_LAUNCH_CHECK("k_voxelise");
+    return 0;
+}
+
+}  // extern "C"

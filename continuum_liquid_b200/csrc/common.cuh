@@ -1,0 +1,82 @@
+// Shared definitions for the Continuum Liquid B200 kernels.
+//
+// The whole library is compiled with -fmad=false, so every floating-point + - * / in these kernels is
+// a separately rounded IEEE operation (division and sqrt are correctly rounded: -prec-div/-prec-sqrt
+// stay at their defaults). Together with the reference's evaluation orders, restated per kernel, this
+// makes the bin keys, sort, P2G, G2P, boundary conditions and red-black Gauss-Seidel sweeps
+// reproduce the CPU restatement bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdarg.h>
+#include <stdio.h>
+
+namespace clb {
+
+typedef int64_t i64;
+
+// helper.cl:4-6 grid_index (k fastest); 64-bit so that 1024^3 grids do not overflow.
+__host__ __device__ __forceinline__ i64 gidx(int i, int j, int k, int ny, int nz) {
+    return ((i64)i * ny + j) * nz + k;
+}
+
+// helper.cl:8-15 grid_coordinates
+__device__ __forceinline__ void gcoord(i64 index, int ny, int nz, int& i, int& j, int& k) {
+    const i64 yz = (i64)ny * nz;
+    i = (int)(index / yz);
+    const i64 rem = index - (i64)i * yz;
+    j = (int)(rem / nz);
+    k = (int)(rem - (i64)j * nz);
+}
+
+// helper.cl:21-23 is_interior_cell
+__host__ __device__ __forceinline__ bool interior(int i, int j, int k, int nx, int ny, int nz) {
+    return i > 0 && j > 0 && k > 0 && i < nx - 1 && j < ny - 1 && k < nz - 1;
+}
+
+__host__ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Error word written by kernels whose bounded waits ran out (read and cleared by clb_device_error).
+// Codes: 1 = scan look-back gave up, 2 = bounded wait elsewhere gave up, 3 = index out of range.
+__device__ unsigned int g_device_error = 0;
+
+__device__ __forceinline__ void raise_device_error(unsigned int code) { atomicCAS(&g_device_error, 0u, code); }
+
+// Thread-local last error text (clb_last_error).
+static thread_local char t_last_error[512] = {0};
+
+static inline int set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_last_error, sizeof(t_last_error), fmt, ap);
+    va_end(ap);
+    return 1;
+}
+
+static inline int check_launch(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error("%s: %s", what, cudaGetErrorString(e));
+    return 0;
+}
+
+static inline int check_call(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) return set_error("%s: %s", what, cudaGetErrorString(e));
+    return 0;
+}
+
+static inline unsigned int blocks_for(i64 n, int threads) { return (unsigned int)((n + threads - 1) / threads); }
+
+// Number of SMs on the current device (cached per process; the library serves one GPU).
+static int g_sm_count = 0;
+
+}  // namespace clb
+
+#define CLB_REQUIRE(cond, ...)                  \
+    do {                                        \
+        if (!(cond)) return clb::set_error(__VA_ARGS__); \
+    } while (0)
+
+#define CLB_LAUNCH_CHECK(what)                    \
+    do {                                          \
+        if (clb::check_launch(what)) return 1;    \
+    } while (0)

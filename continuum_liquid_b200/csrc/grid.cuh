@@ -1,0 +1,184 @@
+// Cell-wide kernels: forces/viscosity, MAC boundary conditions, pressure right-hand side and
+// projection (Solver/Kernel/OpenCL/velocity_update.cl, boundary_conditions.cl, pressure_solve.cl).
+#pragma once
+#include "common.cuh"
+
+namespace clb {
+
+constexpr int GT = 256;  // threads per block for cell-wide kernels
+
+// helper.cl:54-66 laplacian
+__device__ __forceinline__ float laplacian(const float* __restrict__ f, i64 c, i64 sx, i64 sy, float inv_dx2) {
+    const float center = __ldg(f + c);
+    const float s = __ldg(f + c + sx) + __ldg(f + c - sx) + __ldg(f + c + sy) + __ldg(f + c - sy) + __ldg(f + c + 1) +
+                    __ldg(f + c - 1);
+    return (s - 6.0f * center) * inv_dx2;
+}
+
+// velocity_update.cl:3-43 update_velocity
+__global__ void __launch_bounds__(GT) k_update_velocity(const float* __restrict__ u, const float* __restrict__ v,
+                                                         const float* __restrict__ w, float* __restrict__ ru,
+                                                         float* __restrict__ rv, float* __restrict__ rw,
+                                                         const float* __restrict__ ff, float gx, float gy, float gz,
+                                                         float fx, float fy, float fz, float rho, float nu,
+                                                         float inv_dx2, float dt, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    float r0 = __ldg(u + c), r1 = __ldg(v + c), r2 = __ldg(w + c);
+    if (__ldg(ff + c) > 0.0f) {
+        r0 += dt * (gx + fx / rho);
+        r1 += dt * (gy + fy / rho);
+        r2 += dt * (gz + fz / rho);
+    }
+    if (interior(i, j, k, nx, ny, nz)) {
+        const i64 sx = (i64)ny * nz, sy = nz;
+        r0 += nu * dt * laplacian(u, c, sx, sy, inv_dx2);
+        r1 += nu * dt * laplacian(v, c, sx, sy, inv_dx2);
+        r2 += nu * dt * laplacian(w, c, sx, sy, inv_dx2);
+    }
+    ru[c] = r0;
+    rv[c] = r1;
+    rw[c] = r2;
+}
+
+// boundary_conditions.cl:33-67 grid_domain_bc. A ghost copies a component from its clamped
+// interior cell only where the ghost's own wall flag for that component is clear, and the interior
+// source shares that flag, so the source component is never written by the same launch.
+__global__ void __launch_bounds__(GT) k_grid_domain_bc(float* u, float* v, float* w, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    const bool ghost = !interior(i, j, k, nx, ny, nz);
+    const bool wu = i == 0 || i >= nx - 2, wv = j == 0 || j >= ny - 2, ww = k == 0 || k >= nz - 2;
+    if (!ghost && !wu && !wv && !ww) return;
+    if (ghost) {
+        const i64 s = gidx(clampi(i, 1, nx - 2), clampi(j, 1, ny - 2), clampi(k, 1, nz - 2), ny, nz);
+        u[c] = wu ? 0.0f : u[s];
+        v[c] = wv ? 0.0f : v[s];
+        w[c] = ww ? 0.0f : w[s];
+        return;
+    }
+    if (wu) u[c] = 0.0f;
+    if (wv) v[c] = 0.0f;
+    if (ww) w[c] = 0.0f;
+}
+
+// boundary_conditions.cl:99-119 grid_obstacle_bc
+__global__ void __launch_bounds__(GT) k_grid_obstacle_bc(float* __restrict__ u, float* __restrict__ v,
+                                                          float* __restrict__ w, float* __restrict__ ff,
+                                                          const uint8_t* __restrict__ obs, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    const bool self = __ldg(obs + c) != 0;
+    if (self) ff[c] = 0.0f;
+    const bool xs = self || (i + 1 < nx && __ldg(obs + c + (i64)ny * nz));
+    const bool ys = self || (j + 1 < ny && __ldg(obs + c + nz));
+    const bool zs = self || (k + 1 < nz && __ldg(obs + c + 1));
+    if (xs) u[c] = 0.0f;
+    if (ys) v[c] = 0.0f;
+    if (zs) w[c] = 0.0f;
+}
+
+// boundary_conditions.cl:121-173 extrapolate_obstacle_velocity (reads non-obstacle cells only and
+// writes obstacle cells only, so one launch has no read/write overlap).
+__global__ void __launch_bounds__(GT) k_extrapolate_obstacle_velocity(float* u, float* v, float* w,
+                                                                       const uint8_t* __restrict__ obs, int nx, int ny,
+                                                                       int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C || !__ldg(obs + c)) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
+    int n = 0, ax = 0, ay = 0, az = 0;
+    const i64 sx = (i64)ny * nz, sy = nz;
+#define CLB_ACC(q, axis)          \
+    if (!__ldg(obs + (q))) {      \
+        t0 += u[q];               \
+        t1 += v[q];               \
+        t2 += w[q];               \
+        n += 1;                   \
+        axis = 1;                 \
+    }
+    if (i > 0) CLB_ACC(c - sx, ax);
+    if (i + 1 < nx) CLB_ACC(c + sx, ax);
+    if (j > 0) CLB_ACC(c - sy, ay);
+    if (j + 1 < ny) CLB_ACC(c + sy, ay);
+    if (k > 0) CLB_ACC(c - 1, az);
+    if (k + 1 < nz) CLB_ACC(c + 1, az);
+#undef CLB_ACC
+    if (n == 0) return;
+    const float fn = (float)n;
+    t0 = t0 / fn;
+    t1 = t1 / fn;
+    t2 = t2 / fn;
+    u[c] = ax ? 0.0f : t0;
+    v[c] = ay ? 0.0f : t1;
+    w[c] = az ? 0.0f : t2;
+}
+
+// pressure_solve.cl:3-24 pressure_rhs (helper.cl:39-52 divergence)
+__device__ __forceinline__ float rhs_at(const float* __restrict__ u, const float* __restrict__ v,
+                                        const float* __restrict__ w, i64 c, i64 sx, i64 sy, float rho_over_dt,
+                                        float inv_dx) {
+    const float du = __ldg(u + c) - __ldg(u + c - sx);
+    const float dv = __ldg(v + c) - __ldg(v + c - sy);
+    const float dw = __ldg(w + c) - __ldg(w + c - 1);
+    return rho_over_dt * ((du + dv + dw) * inv_dx);
+}
+
+__global__ void __launch_bounds__(GT) k_pressure_rhs(const float* __restrict__ u, const float* __restrict__ v,
+                                                      const float* __restrict__ w, const float* __restrict__ ff,
+                                                      float* __restrict__ rhs, float rho_over_dt, float inv_dx, int nx,
+                                                      int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    if (!interior(i, j, k, nx, ny, nz) || __ldg(ff + c) <= 0.0f) {
+        rhs[c] = 0.0f;
+        return;
+    }
+    rhs[c] = rhs_at(u, v, w, c, (i64)ny * nz, nz, rho_over_dt, inv_dx);
+}
+
+// pressure_solve.cl:26-47 pressure_correction (helper.cl:25-37 gradient)
+__global__ void __launch_bounds__(GT) k_pressure_correction(float* __restrict__ u, float* __restrict__ v,
+                                                             float* __restrict__ w, const float* __restrict__ p,
+                                                             float dt_over_rho, float inv_dx, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    if (!interior(i, j, k, nx, ny, nz)) return;
+    const float center = __ldg(p + c);
+    const float gx = (__ldg(p + c + (i64)ny * nz) - center) * inv_dx;
+    const float gy = (__ldg(p + c + nz) - center) * inv_dx;
+    const float gz = (__ldg(p + c + 1) - center) * inv_dx;
+    u[c] -= dt_over_rho * gx;
+    v[c] -= dt_over_rho * gy;
+    w[c] -= dt_over_rho * gz;
+}
+
+// boundary_conditions.cl:18-31 neumann_domain_bc (ghosts read interior cells only)
+__global__ void __launch_bounds__(GT) k_neumann_domain_bc(float* p, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    if (interior(i, j, k, nx, ny, nz)) return;
+    p[c] = p[gidx(clampi(i, 1, nx - 2), clampi(j, 1, ny - 2), clampi(k, 1, nz - 2), ny, nz)];
+}
+
+}  // namespace clb

@@ -1,0 +1,542 @@
+// Multigrid pressure Poisson solve (Solver/Kernel/OpenCL/multigrid.cl, Solver/Kernel/multigrid.py,
+// Solver/Kernel/pressure_solve.py).
+//
+// Two storage layouts are served:
+//  * the reference layout (separate float32 mask/diag/wx/wy/wz arrays per level), one kernel per
+//    reference kernel, used by the stage API for per-kernel parity;
+//  * the product layout: level 0 keeps its operator in one byte per cell (diag 0..6 in bits 0-2,
+//    wx/wy/wz in bits 3-5, fluid flag in bit 6 -- on the finest level diag is a small integer and
+//    the weights are 0/1, multigrid.cl:63-88), coarse levels keep (diag, wx, wy, wz) as one float4
+//    plus a one-byte mask. The Galerkin coarse operators depend only on the masks, so they are built
+//    once per solve instead of on every restriction (multigrid.cl:127-179 recomputes them on every
+//    visit; the values are the same).
+// The arithmetic of every update keeps the reference's evaluation order, so both layouts give the
+// same values as the CPU restatement.
+#pragma once
+#include "common.cuh"
+
+namespace clb {
+
+constexpr int MGT = 256;
+constexpr int MG_MAX_LEVELS = 16;
+
+// multigrid.cl:3-5 domain_diagonal
+__device__ __forceinline__ float domain_diagonal(int i, int j, int k, int nx, int ny, int nz) {
+    return 6.0f - (float)(i == 1) - (float)(i == nx - 2) - (float)(j == 1) - (float)(j == ny - 2) - (float)(k == 1) -
+           (float)(k == nz - 2);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Reference layout kernels
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float ref_wsum(const float* p, const float* wx, const float* wy, const float* wz, i64 c,
+                                          i64 sx, i64 sy) {
+    return wx[c] * p[c + sx] + wx[c - sx] * p[c - sx] + wy[c] * p[c + sy] + wy[c - sy] * p[c - sy] + wz[c] * p[c + 1] +
+           wz[c - 1] * p[c - 1];
+}
+
+// multigrid.cl:63-88 build_finest_operator
+__global__ void __launch_bounds__(MGT) k_ref_build_finest_operator(const float* __restrict__ mask, float* diag,
+                                                                    float* wx, float* wy, float* wz, int nx, int ny,
+                                                                    int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    diag[c] = 0.0f;
+    wx[c] = 0.0f;
+    wy[c] = 0.0f;
+    wz[c] = 0.0f;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    if (!interior(i, j, k, nx, ny, nz) || mask[c] <= 0.0f) return;
+    diag[c] = domain_diagonal(i, j, k, nx, ny, nz);
+    if (i < nx - 2) wx[c] = mask[c + (i64)ny * nz] > 0.0f ? 1.0f : 0.0f;
+    if (j < ny - 2) wy[c] = mask[c + nz] > 0.0f ? 1.0f : 0.0f;
+    if (k < nz - 2) wz[c] = mask[c + 1] > 0.0f ? 1.0f : 0.0f;
+}
+
+// multigrid.cl:203-230 rbgs_step (one colour; zeroes p wherever mask <= 0)
+__global__ void __launch_bounds__(MGT) k_ref_rbgs_step(float* p, const float* __restrict__ b,
+                                                        const float* __restrict__ mask, const float* __restrict__ diag,
+                                                        const float* __restrict__ wx, const float* __restrict__ wy,
+                                                        const float* __restrict__ wz, float delta, int parity, int nx,
+                                                        int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    const float m = mask[c];
+    if (!interior(i, j, k, nx, ny, nz) || m <= 0.0f || ((i + j + k) & 1) != parity) {
+        if (m <= 0.0f) p[c] = 0.0f;
+        return;
+    }
+    const float d = diag[c];
+    if (d > 0.0f) p[c] = (ref_wsum(p, wx, wy, wz, c, (i64)ny * nz, nz) - delta * delta * b[c]) / d;
+}
+
+// multigrid.cl:25-61 residual on the reference layout
+__device__ __forceinline__ float ref_residual(const float* p, const float* b, const float* mask, const float* diag,
+                                              const float* wx, const float* wy, const float* wz, float inv_delta2,
+                                              int i, int j, int k, int nx, int ny, int nz) {
+    const i64 c = gidx(i, j, k, ny, nz);
+    float ap = 0.0f;
+    if (interior(i, j, k, nx, ny, nz) && !(mask[c] <= 0.0f))
+        ap = (ref_wsum(p, wx, wy, wz, c, (i64)ny * nz, nz) - diag[c] * p[c]) * inv_delta2;
+    return b[c] - ap;
+}
+
+// multigrid.cl:90-180 restrict_residual
+__global__ void __launch_bounds__(MGT) k_ref_restrict_residual(
+    const float* __restrict__ fp, const float* __restrict__ fb, const float* __restrict__ fm,
+    const float* __restrict__ fd, const float* __restrict__ fwx, const float* __restrict__ fwy,
+    const float* __restrict__ fwz, float* cp, float* cb, float* cm, float* cd, float* cwx, float* cwy, float* cwz,
+    float delta, int fnx, int fny, int fnz, int cnx, int cny, int cnz) {
+    const i64 C = (i64)cnx * cny * cnz;
+    const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (ci >= C) return;
+    cp[ci] = 0.0f;
+    cb[ci] = 0.0f;
+    cm[ci] = 0.0f;
+    cd[ci] = 0.0f;
+    cwx[ci] = 0.0f;
+    cwy[ci] = 0.0f;
+    cwz[ci] = 0.0f;
+    int I, J, K;
+    gcoord(ci, cny, cnz, I, J, K);
+    if (!interior(I, J, K, cnx, cny, cnz)) return;
+    const int si = 1 + 2 * (I - 1), sj = 1 + 2 * (J - 1), sk = 1 + 2 * (K - 1);
+    const float inv_delta2 = 1.0f / (delta * delta);
+    float rhs = 0.0f, dsum = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    int active = 0;
+    for (int di = 0; di < 2; ++di)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int dk = 0; dk < 2; ++dk) {
+                const int i = si + di, j = sj + dj, k = sk + dk;
+                if (!interior(i, j, k, fnx, fny, fnz)) continue;
+                const i64 f = gidx(i, j, k, fny, fnz);
+                if (fm[f] <= 0.0f) continue;
+                ++active;
+                rhs += ref_residual(fp, fb, fm, fd, fwx, fwy, fwz, inv_delta2, i, j, k, fnx, fny, fnz);
+                dsum += fd[f];
+                const float wx = fwx[f], wy = fwy[f], wz = fwz[f];
+                if (wx > 0.0f) {
+                    if (di == 0) dsum -= 2.0f * wx;
+                    else cx += wx;
+                }
+                if (wy > 0.0f) {
+                    if (dj == 0) dsum -= 2.0f * wy;
+                    else cy += wy;
+                }
+                if (wz > 0.0f) {
+                    if (dk == 0) dsum -= 2.0f * wz;
+                    else cz += wz;
+                }
+            }
+    if (active > 0) {
+        cb[ci] = rhs;
+        cm[ci] = 1.0f;
+        cd[ci] = dsum;
+        cwx[ci] = cx;
+        cwy[ci] = cy;
+        cwz[ci] = cz;
+    }
+}
+
+// multigrid.cl:182-201 prolongate
+__global__ void __launch_bounds__(MGT) k_ref_prolongate(const float* __restrict__ ce, float* fp,
+                                                         const float* __restrict__ fm, int cnx, int cny, int cnz,
+                                                         int fnx, int fny, int fnz) {
+    const i64 C = (i64)fnx * fny * fnz;
+    const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (f >= C) return;
+    int i, j, k;
+    gcoord(f, fny, fnz, i, j, k);
+    if (!interior(i, j, k, fnx, fny, fnz) || fm[f] <= 0.0f) return;
+    const int I = min((i - 1) / 2 + 1, cnx - 2), J = min((j - 1) / 2 + 1, cny - 2), K = min((k - 1) / 2 + 1, cnz - 2);
+    fp[f] += ce[gidx(I, J, K, cny, cnz)];
+}
+
+// ------------------------------------------------------------------------------------------------
+// Product layout
+// ------------------------------------------------------------------------------------------------
+struct Op0 {  // finest level: packed byte per cell
+    const uint8_t* __restrict__ op;
+    __device__ __forceinline__ uint32_t at(i64 c) const { return __ldg(op + c); }
+    __device__ __forceinline__ bool fluid(i64 c) const { return (at(c) & 64u) != 0u; }
+};
+struct OpC {  // coarse levels: float4 (diag, wx, wy, wz) + mask byte
+    const float4* __restrict__ op;
+    const uint8_t* __restrict__ mask;
+    __device__ __forceinline__ bool fluid(i64 c) const { return __ldg(mask + c) != 0; }
+};
+
+__device__ __forceinline__ float bitf(uint32_t v, int bit) { return (float)((v >> bit) & 1u); }
+
+// Weighted neighbour sum (multigrid.cl:7-23) for each layout, same term order.
+template <typename T>
+__device__ __forceinline__ T wsum0(const uint8_t* __restrict__ op, const T* p, i64 c, i64 sx, i64 sy, uint32_t self) {
+    const uint32_t ox = __ldg(op + c - sx), oy = __ldg(op + c - sy), oz = __ldg(op + c - 1);
+    return (T)bitf(self, 3) * p[c + sx] + (T)bitf(ox, 3) * p[c - sx] + (T)bitf(self, 4) * p[c + sy] +
+           (T)bitf(oy, 4) * p[c - sy] + (T)bitf(self, 5) * p[c + 1] + (T)bitf(oz, 5) * p[c - 1];
+}
+__device__ __forceinline__ float wsumC(const float4* __restrict__ op, const float* p, i64 c, i64 sx, i64 sy,
+                                       float4 self) {
+    return self.y * p[c + sx] + __ldg(op + c - sx).y * p[c - sx] + self.z * p[c + sy] + __ldg(op + c - sy).z * p[c - sy] +
+           self.w * p[c + 1] + __ldg(op + c - 1).w * p[c - 1];
+}
+
+// Fused pressure_rhs (pressure_solve.cl:3-24) + build_finest_operator (multigrid.cl:63-88) into the
+// packed layout. mask is the fluid fraction, as in pressure_solve.py:299-308.
+__global__ void __launch_bounds__(MGT) k_rhs_op0(const float* __restrict__ u, const float* __restrict__ v,
+                                                  const float* __restrict__ w, const float* __restrict__ ff,
+                                                  float* __restrict__ rhs, uint8_t* __restrict__ op0,
+                                                  float rho_over_dt, float inv_dx, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    const i64 sx = (i64)ny * nz, sy = nz;
+    if (!interior(i, j, k, nx, ny, nz) || __ldg(ff + c) <= 0.0f) {
+        rhs[c] = 0.0f;
+        op0[c] = 0;
+        return;
+    }
+    const float du = __ldg(u + c) - __ldg(u + c - sx);
+    const float dv = __ldg(v + c) - __ldg(v + c - sy);
+    const float dw = __ldg(w + c) - __ldg(w + c - 1);
+    rhs[c] = rho_over_dt * ((du + dv + dw) * inv_dx);
+    uint32_t d = 6u - (i == 1) - (i == nx - 2) - (j == 1) - (j == ny - 2) - (k == 1) - (k == nz - 2);
+    uint32_t bits = d | 64u;
+    if (i < nx - 2 && __ldg(ff + c + sx) > 0.0f) bits |= 8u;
+    if (j < ny - 2 && __ldg(ff + c + sy) > 0.0f) bits |= 16u;
+    if (k < nz - 2 && __ldg(ff + c + 1) > 0.0f) bits |= 32u;
+    op0[c] = (uint8_t)bits;
+}
+
+// Operator part of restrict_residual (multigrid.cl:127-179) for one coarse level, from either layout.
+template <bool FINE0>
+__global__ void __launch_bounds__(MGT) k_coarse_operator(const uint8_t* __restrict__ fop0,
+                                                          const float4* __restrict__ fopc,
+                                                          const uint8_t* __restrict__ fmask, float4* __restrict__ cop,
+                                                          uint8_t* __restrict__ cmask, int fnx, int fny, int fnz,
+                                                          int cnx, int cny, int cnz) {
+    const i64 C = (i64)cnx * cny * cnz;
+    const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (ci >= C) return;
+    int I, J, K;
+    gcoord(ci, cny, cnz, I, J, K);
+    float dsum = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    int active = 0;
+    if (interior(I, J, K, cnx, cny, cnz)) {
+        const int si = 1 + 2 * (I - 1), sj = 1 + 2 * (J - 1), sk = 1 + 2 * (K - 1);
+        for (int di = 0; di < 2; ++di)
+            for (int dj = 0; dj < 2; ++dj)
+                for (int dk = 0; dk < 2; ++dk) {
+                    const int i = si + di, j = sj + dj, k = sk + dk;
+                    if (!interior(i, j, k, fnx, fny, fnz)) continue;
+                    const i64 f = gidx(i, j, k, fny, fnz);
+                    float d, wx, wy, wz;
+                    if (FINE0) {
+                        const uint32_t o = __ldg(fop0 + f);
+                        if (!(o & 64u)) continue;
+                        d = (float)(o & 7u);
+                        wx = bitf(o, 3);
+                        wy = bitf(o, 4);
+                        wz = bitf(o, 5);
+                    } else {
+                        if (!__ldg(fmask + f)) continue;
+                        const float4 o = __ldg(fopc + f);
+                        d = o.x;
+                        wx = o.y;
+                        wy = o.z;
+                        wz = o.w;
+                    }
+                    ++active;
+                    dsum += d;
+                    if (wx > 0.0f) {
+                        if (di == 0) dsum -= 2.0f * wx;
+                        else cx += wx;
+                    }
+                    if (wy > 0.0f) {
+                        if (dj == 0) dsum -= 2.0f * wy;
+                        else cy += wy;
+                    }
+                    if (wz > 0.0f) {
+                        if (dk == 0) dsum -= 2.0f * wz;
+                        else cz += wz;
+                    }
+                }
+    }
+    if (active > 0) {
+        cop[ci] = make_float4(dsum, cx, cy, cz);
+        cmask[ci] = 1;
+    } else {
+        cop[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        cmask[ci] = 0;
+    }
+}
+
+// One red-black Gauss-Seidel colour (multigrid.cl:203-230) on either layout.
+template <bool L0>
+__global__ void __launch_bounds__(MGT) k_rbgs(float* p, const float* __restrict__ b, const uint8_t* __restrict__ op0,
+                                               const float4* __restrict__ opc, const uint8_t* __restrict__ mask,
+                                               float delta, int parity, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    const i64 sx = (i64)ny * nz, sy = nz;
+    const float d2 = delta * delta;
+    if (L0) {
+        const uint32_t o = __ldg(op0 + c);
+        const bool fluid = (o & 64u) != 0u;
+        if (!interior(i, j, k, nx, ny, nz) || !fluid || ((i + j + k) & 1) != parity) {
+            if (!fluid) p[c] = 0.0f;
+            return;
+        }
+        const float d = (float)(o & 7u);
+        if (d > 0.0f) p[c] = (wsum0<float>(op0, p, c, sx, sy, o) - d2 * __ldg(b + c)) / d;
+    } else {
+        const bool fluid = __ldg(mask + c) != 0;
+        if (!interior(i, j, k, nx, ny, nz) || !fluid || ((i + j + k) & 1) != parity) {
+            if (!fluid) p[c] = 0.0f;
+            return;
+        }
+        const float4 o = __ldg(opc + c);
+        if (o.x > 0.0f) p[c] = (wsumC(opc, p, c, sx, sy, o) - d2 * __ldg(b + c)) / o.x;
+    }
+}
+
+// Residual (multigrid.cl:45-61) at one fine cell for either layout; 0 contribution when not fluid.
+template <bool L0>
+__device__ __forceinline__ float residual_at(const float* p, const float* __restrict__ b,
+                                             const uint8_t* __restrict__ op0, const float4* __restrict__ opc,
+                                             const uint8_t* __restrict__ mask, float inv_delta2, i64 f, i64 sx,
+                                             i64 sy) {
+    float ap;
+    if (L0) {
+        const uint32_t o = __ldg(op0 + f);
+        ap = (wsum0<float>(op0, p, f, sx, sy, o) - (float)(o & 7u) * p[f]) * inv_delta2;
+    } else {
+        const float4 o = __ldg(opc + f);
+        ap = (wsumC(opc, p, f, sx, sy, o) - o.x * p[f]) * inv_delta2;
+    }
+    return __ldg(b + f) - ap;
+}
+
+// Right-hand-side part of restrict_residual (multigrid.cl:90-180): coarse b = sum of the eight fine
+// residuals in (di, dj, dk) order, coarse p = 0.
+template <bool L0>
+__global__ void __launch_bounds__(MGT) k_restrict(const float* __restrict__ fp, const float* __restrict__ fb,
+                                                   const uint8_t* __restrict__ fop0, const float4* __restrict__ fopc,
+                                                   const uint8_t* __restrict__ fmask, float* __restrict__ cp,
+                                                   float* __restrict__ cb, float delta, int fnx, int fny, int fnz,
+                                                   int cnx, int cny, int cnz) {
+    const i64 C = (i64)cnx * cny * cnz;
+    const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (ci >= C) return;
+    cp[ci] = 0.0f;
+    int I, J, K;
+    gcoord(ci, cny, cnz, I, J, K);
+    float rhs = 0.0f;
+    if (interior(I, J, K, cnx, cny, cnz)) {
+        const int si = 1 + 2 * (I - 1), sj = 1 + 2 * (J - 1), sk = 1 + 2 * (K - 1);
+        const float inv_delta2 = 1.0f / (delta * delta);
+        const i64 sx = (i64)fny * fnz, sy = fnz;
+        for (int di = 0; di < 2; ++di)
+            for (int dj = 0; dj < 2; ++dj)
+                for (int dk = 0; dk < 2; ++dk) {
+                    const int i = si + di, j = sj + dj, k = sk + dk;
+                    if (!interior(i, j, k, fnx, fny, fnz)) continue;
+                    const i64 f = gidx(i, j, k, fny, fnz);
+                    const bool fl = L0 ? ((__ldg(fop0 + f) & 64u) != 0u) : (__ldg(fmask + f) != 0);
+                    if (!fl) continue;
+                    rhs += residual_at<L0>(fp, fb, fop0, fopc, fmask, inv_delta2, f, sx, sy);
+                }
+    }
+    cb[ci] = rhs;
+}
+
+// prolongate (multigrid.cl:182-201) for either layout
+template <bool L0>
+__global__ void __launch_bounds__(MGT) k_prolong(const float* __restrict__ ce, float* __restrict__ fp,
+                                                  const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
+                                                  int cnx, int cny, int cnz, int fnx, int fny, int fnz) {
+    const i64 C = (i64)fnx * fny * fnz;
+    const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (f >= C) return;
+    int i, j, k;
+    gcoord(f, fny, fnz, i, j, k);
+    const bool fl = L0 ? ((__ldg(fop0 + f) & 64u) != 0u) : (__ldg(fmask + f) != 0);
+    if (!interior(i, j, k, fnx, fny, fnz) || !fl) return;
+    const int I = min((i - 1) / 2 + 1, cnx - 2), J = min((j - 1) / 2 + 1, cny - 2), K = min((k - 1) / 2 + 1, cnz - 2);
+    fp[f] += __ldg(ce + gidx(I, J, K, cny, cnz));
+}
+
+// coarse_smooth (multigrid.cl:232-264): one block runs all colour sweeps of the coarsest level,
+// with the level's p, b and operator held in shared memory when they fit. Cells that are not
+// interior fluid cells are never written (as in the reference).
+constexpr int COARSE_THREADS = 1024;
+constexpr int COARSE_SMEM_CELLS = 8192;  // 25 bytes per cell -> 200 KB
+
+template <bool SMEM, bool L0>
+__global__ void __launch_bounds__(COARSE_THREADS) k_coarse_solve(float* p, const float* __restrict__ b,
+                                                                  const uint8_t* __restrict__ op0,
+                                                                  const float4* __restrict__ opc,
+                                                                  const uint8_t* __restrict__ mask, float delta,
+                                                                  int iterations, int nx, int ny, int nz) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int C = nx * ny * nz;
+    const float d2 = delta * delta;
+    const i64 sx = (i64)ny * nz, sy = nz;
+    float* sp = reinterpret_cast<float*>(smem);
+    float* sb = sp + C;
+    float4* so = reinterpret_cast<float4*>(sb + C + ((4 - (2 * C) % 4) % 4));
+    if (SMEM) {
+        for (int c = threadIdx.x; c < C; c += COARSE_THREADS) {
+            sp[c] = p[c];
+            sb[c] = b[c];
+            float4 o;
+            if (L0) {
+                const uint32_t v = op0[c];
+                o = make_float4((v & 64u) ? (float)(v & 7u) : -1.0f, bitf(v, 3), bitf(v, 4), bitf(v, 5));
+            } else {
+                o = opc[c];
+                if (!mask[c]) o.x = -1.0f;  // marks "not fluid"; diag itself is never negative
+            }
+            so[c] = o;
+        }
+        __syncthreads();
+    }
+    for (int it = 0; it < iterations; ++it)
+        for (int parity = 0; parity < 2; ++parity) {
+            for (int c = threadIdx.x; c < C; c += COARSE_THREADS) {
+                int i, j, k;
+                gcoord(c, ny, nz, i, j, k);
+                if (!interior(i, j, k, nx, ny, nz) || ((i + j + k) & 1) != parity) continue;
+                if (SMEM) {
+                    const float4 o = so[c];
+                    if (o.x < 0.0f) continue;
+                    const float ws = o.y * sp[c + sx] + so[c - sx].y * sp[c - sx] + o.z * sp[c + sy] +
+                                     so[c - sy].z * sp[c - sy] + o.w * sp[c + 1] + so[c - 1].w * sp[c - 1];
+                    if (o.x > 0.0f) sp[c] = (ws - d2 * sb[c]) / o.x;
+                } else if (L0) {
+                    const uint32_t o = op0[c];
+                    if (!(o & 64u)) continue;
+                    const float d = (float)(o & 7u);
+                    if (d > 0.0f) p[c] = (wsum0<float>(op0, p, c, sx, sy, o) - d2 * b[c]) / d;
+                } else {
+                    if (!mask[c]) continue;
+                    const float4 o = opc[c];
+                    if (o.x > 0.0f) p[c] = (wsumC(opc, p, c, sx, sy, o) - d2 * b[c]) / o.x;
+                }
+            }
+            __syncthreads();
+        }
+    if (SMEM)
+        for (int c = threadIdx.x; c < C; c += COARSE_THREADS) p[c] = sp[c];
+}
+
+static inline size_t coarse_smem_bytes(int C) {
+    return (size_t)C * 8 + (size_t)(((4 - (2 * C) % 4) % 4) * 4) + (size_t)C * 16;
+}
+
+// ------------------------------------------------------------------------------------------------
+// FP64 residual norms and iterative refinement on the finest level (packed layout).
+// ------------------------------------------------------------------------------------------------
+constexpr int RN_THREADS = 256;
+
+// Per block: sums of r^2 and b^2 over interior fluid cells, r = b - A p evaluated in FP64 from a
+// float or double p (A is multigrid.cl:25-43 apply_operator). When r_out is given the residual is
+// also stored, rounded to float, at every cell (0 outside interior fluid cells): it becomes the
+// right-hand side of the next correction solve.
+template <typename PT>
+__global__ void __launch_bounds__(RN_THREADS) k_residual_norms(const PT* __restrict__ p, const float* __restrict__ b,
+                                                                const uint8_t* __restrict__ op0, double inv_delta2,
+                                                                int nx, int ny, int nz, float* __restrict__ r_out,
+                                                                double2* __restrict__ partials) {
+    __shared__ double2 s_red[RN_THREADS / 32];
+    const i64 C = (i64)nx * ny * nz;
+    const i64 sx = (i64)ny * nz, sy = nz;
+    double rr = 0.0, bb = 0.0;
+    for (i64 c = (i64)blockIdx.x * RN_THREADS + threadIdx.x; c < C; c += (i64)gridDim.x * RN_THREADS) {
+        int i, j, k;
+        gcoord(c, ny, nz, i, j, k);
+        const uint32_t o = __ldg(op0 + c);
+        float rf = 0.0f;
+        if (interior(i, j, k, nx, ny, nz) && (o & 64u)) {
+            const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
+            const double ws = (double)bitf(o, 3) * (double)p[c + sx] + (double)bitf(ox, 3) * (double)p[c - sx] +
+                              (double)bitf(o, 4) * (double)p[c + sy] + (double)bitf(oy, 4) * (double)p[c - sy] +
+                              (double)bitf(o, 5) * (double)p[c + 1] + (double)bitf(oz, 5) * (double)p[c - 1];
+            const double bv = (double)__ldg(b + c);
+            const double r = bv - (ws - (double)(o & 7u) * (double)p[c]) * inv_delta2;
+            rr += r * r;
+            bb += bv * bv;
+            rf = (float)r;
+        }
+        if (r_out) r_out[c] = rf;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rr += __shfl_xor_sync(0xffffffffu, rr, o);
+        bb += __shfl_xor_sync(0xffffffffu, bb, o);
+    }
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = make_double2(rr, bb);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 t = s_red[0];
+        for (int q = 1; q < RN_THREADS / 32; ++q) {
+            t.x += s_red[q].x;
+            t.y += s_red[q].y;
+        }
+        partials[blockIdx.x] = t;
+    }
+}
+
+// Fixed-order reduction of the block partials (deterministic for a given grid size).
+__global__ void k_reduce_partials(const double2* __restrict__ partials, int count, double2* __restrict__ out) {
+    __shared__ double2 s[256];
+    double2 t = make_double2(0.0, 0.0);
+    for (int q = threadIdx.x; q < count; q += 256) {
+        t.x += partials[q].x;
+        t.y += partials[q].y;
+    }
+    s[threadIdx.x] = t;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s[threadIdx.x].x += s[threadIdx.x + o].x;
+            s[threadIdx.x].y += s[threadIdx.x + o].y;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+// p64 = warm-start pressure at interior fluid cells, 0 elsewhere (cells that left the liquid since
+// the previous step must not keep a stale pressure).
+__global__ void __launch_bounds__(MGT) k_ir_init(const float* __restrict__ p, const uint8_t* __restrict__ op0,
+                                                  double* __restrict__ p64, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    p64[c] = (interior(i, j, k, nx, ny, nz) && (__ldg(op0 + c) & 64u)) ? (double)__ldg(p + c) : 0.0;
+}
+
+__global__ void __launch_bounds__(MGT) k_ir_update(double* __restrict__ p64, const float* __restrict__ e, i64 C) {
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c < C) p64[c] += (double)__ldg(e + c);
+}
+
+__global__ void __launch_bounds__(MGT) k_ir_store(const double* __restrict__ p64, float* __restrict__ p, i64 C) {
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c < C) p[c] = (float)__ldg(p64 + c);
+}
+
+}  // namespace clb

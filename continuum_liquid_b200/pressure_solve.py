@@ -1,0 +1,157 @@
+"""Pressure solve and projection (mirrors Solver/Kernel/pressure_solve.py).
+
+``pressure_solve`` keeps the reference's signature and algorithm (pressure_rhs,
+build_finest_operator, ``num_vcycles`` W-cycles, Neumann ghost copy) on the reference layout.
+
+``PressureSolver`` is the product path behind the same stage: the packed multigrid hierarchy plus
+
+* parity mode (``tol=None``): exactly ``num_vcycles`` W-cycles on the pressure, as the reference;
+* tolerance mode (``tol=1e-6``): mixed-precision iterative refinement. The pressure is accumulated
+  in FP64; each refinement computes the FP64 residual r = b - A p (and its norm), solves A e = r
+  with one FP32 W-cycle from e = 0 and adds e to p, until ||r||_2 / ||b||_2 <= tol over the
+  interior fluid cells. A W-cycle is an affine map, so this is the same iteration as running
+  W-cycles on p, with the rounding of the FP32 residual (which cannot reach 1e-6 by itself)
+  removed.
+"""
+
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import boundary_conditions, multigrid
+from .backend import Backend
+
+FIELD_DTYPE = np.float32
+
+
+def pressure_solve(kernels: Backend, multigrid_kernels, boundary_kernels, queue, velocity, fluid_fraction, pressure,
+                   rhs, p_levels, b_levels, mask_levels, operator_level0, operator_levels, multigrid_level_shapes, dx,
+                   dt, rho, num_vcycles, grid_shape):
+    """pressure_solve.py:10-85 on the reference layout (one kernel per reference kernel)."""
+    nx, ny, nz = grid_shape
+    u, v, w = velocity
+    kernels.call("clb_pressure_rhs", u, v, w, fluid_fraction, rhs, float(FIELD_DTYPE(rho / dt)),
+                 float(FIELD_DTYPE(1.0 / dx)), nx, ny, nz, stream=queue)
+    kernels.call("clb_build_finest_operator", fluid_fraction, *operator_level0, nx, ny, nz, stream=queue)
+    for _ in range(num_vcycles):
+        multigrid.w_cycle(kernels, queue, 0, p_levels, b_levels, mask_levels, operator_levels, pressure, rhs,
+                          fluid_fraction, operator_level0, dx, multigrid_level_shapes, grid_shape,
+                          multigrid.PRE_SMOOTH, multigrid.POST_SMOOTH, multigrid.COARSE_SMOOTH_ITERATIONS)
+    boundary_conditions.neumann_domain_bc(kernels, queue, pressure, grid_shape)
+    return pressure
+
+
+def pressure_correction(kernels: Backend, queue, velocity, pressure, dx, dt, rho, grid_shape):
+    """pressure_solve.py:88-114."""
+    nx, ny, nz = grid_shape
+    u, v, w = velocity
+    kernels.call("clb_pressure_correction", u, v, w, pressure, float(FIELD_DTYPE(dt / rho)),
+                 float(FIELD_DTYPE(1.0 / dx)), nx, ny, nz, stream=queue)
+    return velocity
+
+
+@dataclass
+class SolveStats:
+    """Per-solve record (added to the reference's stats messages): W-cycles run, final relative
+    residual (FP64, None in parity mode unless measured) and wall time of the solve in ms."""
+
+    cycles: int = 0
+    rel_residual: float | None = None
+    initial_rel_residual: float | None = None
+    ms: float = 0.0
+    history: list = field(default_factory=list)
+
+
+class PressureSolver:
+    """Packed-layout pressure solve for one grid (allocates its workspace once)."""
+
+    def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100):
+        self.kernels = kernels
+        self.grid_shape = tuple(int(s) for s in grid_shape)
+        self.dx = float(dx)
+        self.max_cycles = int(max_cycles)
+        self.hierarchy = multigrid.MultigridHierarchy(kernels, self.grid_shape, dx, min_size)
+        device = kernels.device
+        self.cells = int(np.prod(self.grid_shape))
+        self.rhs = torch.zeros(self.grid_shape, dtype=torch.float32, device=device)
+        self.residual = torch.zeros(self.grid_shape, dtype=torch.float32, device=device)
+        self.correction = torch.zeros(self.grid_shape, dtype=torch.float32, device=device)
+        self.p64 = torch.zeros(self.grid_shape, dtype=torch.float64, device=device)
+        self.norms_host = torch.zeros(2, dtype=torch.float64, pin_memory=True)
+        self._refine_graph: torch.cuda.CUDAGraph | None = None
+
+    # -- pieces ---------------------------------------------------------------------------------
+    def prepare(self, velocity, fluid_fraction, dt, rho, queue=None) -> None:
+        """Right-hand side, packed finest operator and the Galerkin coarse operators."""
+        self.hierarchy.rhs_operator(velocity, fluid_fraction, self.rhs, dt, rho, queue=queue)
+        self.hierarchy.build_coarse(queue=queue)
+
+    def _relative(self, norms: torch.Tensor) -> float:
+        self.norms_host.copy_(norms, non_blocking=True)
+        torch.cuda.current_stream(self.kernels.device).synchronize()
+        rr, bb = float(self.norms_host[0]), float(self.norms_host[1])
+        return 0.0 if bb == 0.0 else math.sqrt(rr / bb)
+
+    def relative_residual(self, pressure, queue=None) -> float:
+        """FP64 ||b - A p|| / ||b|| of a float32 or float64 pressure against the prepared system."""
+        return self._relative(self.hierarchy.residual_norms(pressure, self.rhs, queue=queue))
+
+    def refine_once(self, queue=None) -> None:
+        """One refinement: e = W-cycle(0, r); p64 += e; r = b - A p64 (FP64) and its norms."""
+        h = self.hierarchy
+        self.correction.zero_()
+        h.w_cycle(self.correction, self.residual, queue=queue)
+        self.kernels.call("clb_mg_ir_update", self.p64, self.correction, self.cells, stream=queue)
+        h.residual_norms(self.p64, self.rhs, r_out=self.residual, queue=queue)
+
+    def _refine(self, use_graph: bool) -> None:
+        if not use_graph:
+            self.refine_once()
+            return
+        if self._refine_graph is None:
+            side = torch.cuda.Stream(self.kernels.device)
+            side.wait_stream(torch.cuda.current_stream(self.kernels.device))
+            with torch.cuda.stream(side):
+                self.refine_once()  # warm-up outside capture
+            torch.cuda.current_stream(self.kernels.device).wait_stream(side)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                self.refine_once()
+            self._refine_graph = graph
+        self._refine_graph.replay()
+
+    # -- solves ---------------------------------------------------------------------------------
+    def solve(self, velocity, fluid_fraction, pressure, dt, rho, num_vcycles: int = 1, tol: float | None = None,
+              use_graph: bool = True, measure: bool = False) -> SolveStats:
+        """Solve for ``pressure`` in place (warm-started from its current contents) and apply the
+        Neumann ghost copy. ``tol=None`` runs ``num_vcycles`` W-cycles (reference semantics)."""
+        stats = SolveStats()
+        t0 = time.perf_counter()
+        self.prepare(velocity, fluid_fraction, dt, rho)
+        h = self.hierarchy
+        if tol is None:
+            for _ in range(int(num_vcycles)):
+                h.w_cycle(pressure, self.rhs)
+            stats.cycles = int(num_vcycles)
+            if measure:
+                stats.rel_residual = self.relative_residual(pressure)
+        else:
+            self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64, *self.grid_shape)
+            rel = self._relative(h.residual_norms(self.p64, self.rhs, r_out=self.residual))
+            stats.initial_rel_residual = rel
+            stats.history.append(rel)
+            while rel > tol and stats.cycles < self.max_cycles:
+                self._refine(use_graph)
+                stats.cycles += 1
+                rel = self._relative(h.norms)
+                stats.history.append(rel)
+            stats.rel_residual = rel
+            self.kernels.call("clb_mg_ir_store", self.p64, pressure, self.cells)
+        boundary_conditions.neumann_domain_bc(self.kernels, None, pressure, self.grid_shape)
+        stats.ms = (time.perf_counter() - t0) * 1e3
+        return stats

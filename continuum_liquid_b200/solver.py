@@ -1,0 +1,266 @@
+"""FLIP timestep driver (mirrors Solver/Kernel/solver.py).
+
+``FlipSolver`` owns one scene's device buffers and advances it with the reference's stage order
+(solver.py:308-510):
+
+ 1. particle_to_grid: count, scan, stable sort, gather -> u, v, w, fluid_fraction
+ 2. grid_obstacle_bc (+ extrapolation) and grid_domain_bc
+ 3. update_velocity into the work buffers, then swap (u_work keeps the post-BC P2G field)
+ 4. grid_domain_bc and grid_obstacle_bc
+ 5. pressure solve (rhs, operator, W-cycles, Neumann ghost copy)
+ 6. pressure_correction, grid_domain_bc, grid_obstacle_bc
+ 7. grid_to_particle, previous-position copy, advection, particle domain and obstacle BCs
+
+Steps 7's five passes run as one fused kernel; step 5 runs on the packed multigrid hierarchy.
+With no collider the obstacle passes are skipped (they are exact no-ops on an empty mask).
+
+``solver(config)`` is the reference's top-level entry (solver.py:22-531): config parsing,
+voxelised static masks, host seeding, the time loop with cancellation, the particle cache and the
+stats messages.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import boundary_conditions, output, particles as particle_methods, source_particles, velocity_update
+from . import voxelise_mesh
+from .backend import Backend, default_backend
+from .pressure_solve import PressureSolver, SolveStats, pressure_correction
+
+FIELD_DTYPE = np.float32
+
+
+@dataclass
+class StepOptions:
+    """Per-step numerical options. The defaults are the reference's semantics (pure FLIP, a fixed
+    number of W-cycles); ``tol`` switches the pressure solve to mixed-precision iterative
+    refinement to that relative residual."""
+
+    flip_ratio: float = 1.0
+    num_vcycles: int = 1
+    tol: float | None = None
+    gravity: tuple[float, float, float] = (0.0, 0.0, -9.81)
+    force: tuple[float, float, float] = (0.0, 0.0, 0.0)
+    rho: float = 1000.0
+    nu: float = 1.0e-6
+    use_graph: bool = True
+
+
+class FlipSolver:
+    """Device state and timestep of one FLIP scene on one GPU."""
+
+    def __init__(self, kernels: Backend, grid_shape, dx: float, positions, velocities, obstacle=None,
+                 dt: float = 1.0 / 240.0, options: StepOptions | None = None, particles_per_cell: int = 8,
+                 min_size: int = 8, capacity: int | None = None):
+        self.kernels = kernels
+        self.device = kernels.device
+        self.grid_shape = tuple(int(s) for s in grid_shape)
+        self.dx = float(dx)
+        self.dt = float(dt)
+        self.options = options or StepOptions()
+        self.particles_per_cell = particles_per_cell
+        positions = torch.as_tensor(np.ascontiguousarray(positions, dtype=np.float32)).reshape(-1, 3)
+        velocities = torch.as_tensor(np.ascontiguousarray(velocities, dtype=np.float32)).reshape(-1, 3)
+        self.n = int(positions.shape[0])
+        cap = max(1, int(capacity or self.n))
+        dev = self.device
+        self.particles = torch.zeros((cap, 3), dtype=torch.float32, device=dev)
+        self.particle_velocity = torch.zeros((cap, 3), dtype=torch.float32, device=dev)
+        self.particles[: self.n].copy_(positions)
+        self.particle_velocity[: self.n].copy_(velocities)
+        (self.particle_work, self.particle_velocity_work, self.bin_counts, self.scan_outputs,
+         self.scan_sums) = particle_methods.create_particle_sort_buffers(kernels, self.grid_shape, cap)
+        grid = lambda: torch.zeros(self.grid_shape, dtype=torch.float32, device=dev)  # noqa: E731
+        self.u, self.v, self.w = grid(), grid(), grid()
+        self.u_work, self.v_work, self.w_work = grid(), grid(), grid()
+        self.fluid_fraction = grid()
+        self.pressure = grid()
+        self.obstacle = None
+        if obstacle is not None:
+            ob = torch.as_tensor(np.ascontiguousarray(obstacle, dtype=np.uint8)) if isinstance(obstacle, np.ndarray) \
+                else obstacle
+            if bool(ob.any()):
+                self.obstacle = ob.to(dev).contiguous()
+        self.pressure_solver = PressureSolver(kernels, self.grid_shape, self.dx, min_size=min_size)
+        self.last_solve: SolveStats | None = None
+        self.steps_done = 0
+
+    # -- the step --------------------------------------------------------------------------------
+    def pre_solve(self, queue=None) -> None:
+        """Stages 1-4: P2G, grid BCs, forces, BCs (everything before the pressure solve)."""
+        k, o, gs = self.kernels, self.options, self.grid_shape
+        (self.particles, self.particle_velocity, self.particle_work, self.particle_velocity_work,
+         _, self.fluid_fraction) = particle_methods.particle_to_grid(
+            k, queue, self.particles, self.particle_velocity, self.particle_work, self.particle_velocity_work,
+            (self.u, self.v, self.w), self.bin_counts, self.scan_outputs, self.scan_sums, self.fluid_fraction, self.n,
+            gs, self.dx, self.particles_per_cell)
+        vel = (self.u, self.v, self.w)
+        if self.obstacle is not None:
+            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)
+        boundary_conditions.grid_domain_bc(k, queue, vel, gs)
+        velocity_update.update_velocity(k, queue, vel, (self.u_work, self.v_work, self.w_work), self.fluid_fraction,
+                                        o.gravity, *o.force, o.rho, o.nu, self.dx, self.dt, gs)
+        self.u, self.u_work = self.u_work, self.u
+        self.v, self.v_work = self.v_work, self.v
+        self.w, self.w_work = self.w_work, self.w
+        vel = (self.u, self.v, self.w)
+        boundary_conditions.grid_domain_bc(k, queue, vel, gs)
+        if self.obstacle is not None:
+            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)
+
+    def solve(self, tol: float | None = None, num_vcycles: int | None = None) -> SolveStats:
+        """Stage 5: the pressure solve, warm-started from the previous step's pressure."""
+        o = self.options
+        stats = self.pressure_solver.solve((self.u, self.v, self.w), self.fluid_fraction, self.pressure, self.dt,
+                                           o.rho, num_vcycles=o.num_vcycles if num_vcycles is None else num_vcycles,
+                                           tol=o.tol if tol is None else tol, use_graph=o.use_graph)
+        self.last_solve = stats
+        return stats
+
+    def post_solve(self, queue=None) -> None:
+        """Stages 6-7: projection, BCs and the fused particle update."""
+        k, o, gs = self.kernels, self.options, self.grid_shape
+        vel = (self.u, self.v, self.w)
+        pressure_correction(k, queue, vel, self.pressure, self.dx, self.dt, o.rho, gs)
+        boundary_conditions.grid_domain_bc(k, queue, vel, gs)
+        if self.obstacle is not None:
+            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)
+        particle_methods.particle_update(k, queue, self.particles, self.particle_velocity, vel,
+                                         (self.u_work, self.v_work, self.w_work), self.obstacle, self.n, gs, self.dx,
+                                         self.dt, o.flip_ratio)
+
+    def step(self) -> SolveStats:
+        if self.n == 0:
+            self.steps_done += 1
+            return SolveStats()
+        self.pre_solve()
+        stats = self.solve()
+        self.post_solve()
+        self.steps_done += 1
+        return stats
+
+    # -- host views -------------------------------------------------------------------------------
+    def positions(self) -> np.ndarray:
+        return self.particles[: self.n].cpu().numpy()
+
+    def velocities(self) -> np.ndarray:
+        return self.particle_velocity[: self.n].cpu().numpy()
+
+
+def scene_solver(kernels: Backend, scene, options: StepOptions | None = None) -> FlipSolver:
+    """Build a FlipSolver for a ``scenes.Scene``: voxelise its colliders on the device, seed its
+    particles on the host around the solid cells, upload."""
+    obstacle = torch.zeros(scene.grid_shape, dtype=torch.uint8, device=kernels.device)
+    for tris in scene.obstacles:
+        voxelise_mesh.voxelise_triangles(kernels, None, tris, obstacle, scene.grid_shape, scene.dx, scene.origin)
+    from .scenes import seed_particles
+
+    positions, velocities = seed_particles(scene, obstacle.cpu().numpy())
+    opts = options or StepOptions(flip_ratio=scene.flip_ratio, gravity=scene.gravity, rho=scene.rho, nu=scene.nu)
+    return FlipSolver(kernels, scene.grid_shape, scene.dx, positions, velocities, obstacle=obstacle, dt=scene.dt,
+                      options=opts, particles_per_cell=scene.particles_per_cell, min_size=scene.min_size)
+
+
+# ------------------------------------------------------------------------------------------------
+# solver(config): the reference's entry point (solver.py:22-531)
+# ------------------------------------------------------------------------------------------------
+def solver(config: dict, timings=None) -> None:
+    from .general.main import emit_message
+
+    simulation = config.get("simulation") or {}
+    settings = simulation.get("settings") or {}
+    kernels = default_backend()
+    domain = simulation.get("domain") or {}
+    domain_size = domain.get("size") or {}
+    physics = simulation.get("physics") or {}
+    water = physics.get("water") or {}
+    output_dir = Path(simulation["output_path"]).expanduser().resolve()
+    cancel_event = (config.get("meta") or {}).get("cancel_event")
+
+    start_frame = int(settings.get("start_frame", 1))
+    end_frame = int(settings.get("end_frame", 250))
+    fps = int(settings.get("fps", 24))
+    substeps = max(0, int(settings.get("substeps", 1)))
+    steps_per_frame = substeps + 1
+    total_frames = max(0, end_frame - start_frame)
+    total_solver_steps = total_frames * steps_per_frame
+    dt = 1.0 / (fps * steps_per_frame)
+
+    delta = float(domain["resolution"])
+    grid_shape = (int(float(domain_size["x"]) / delta), int(float(domain_size["y"]) / delta),
+                  int(float(domain_size["z"]) / delta))
+    rho_water = float(water["density"])
+    nu_water = float(water["viscosity"])
+    options = StepOptions(
+        flip_ratio=float(settings.get("flip_ratio", 1.0)),
+        num_vcycles=max(1, int(settings.get("iterations", 1))),
+        tol=settings.get("tolerance"),
+        gravity=tuple(settings.get("gravity", (0.0, 0.0, -9.81))),
+        rho=rho_water,
+        nu=nu_water,
+    )
+
+    sources_dev, obstacle_mask = voxelise_mesh.build_static_masks(kernels, None, kernels, simulation, grid_shape,
+                                                                  delta)
+    sources, obstacle_host = source_particles.download_static_masks(None, sources_dev, obstacle_mask, grid_shape)
+    rng = np.random.default_rng(0)
+    particles_host = np.empty((0, 3), dtype=FIELD_DTYPE)
+    velocity_host = np.empty((0, 3), dtype=FIELD_DTYPE)
+    particles_host, velocity_host = source_particles.apply_sources(particles_host, velocity_host, sources,
+                                                                   obstacle_host, delta, rng, initial=True)
+    sim = FlipSolver(kernels, grid_shape, delta, particles_host, velocity_host, obstacle=obstacle_mask, dt=dt,
+                     options=options, particles_per_cell=8)
+
+    output_dir.mkdir(parents=True, exist_ok=True)
+    cache = output.create_cache(output_dir, fps=fps, start_frame=start_frame, end_frame=end_frame)
+    writer = output.create_output(cache)
+    try:
+        output.submit_host(writer, particles_host, frame=start_frame)
+        emit_message({"type": "stats", "frame": 0, "total_frames": total_frames, "particle_count": sim.n})
+        dynamic = any(source.get("type") in {"INFLOW", "OUTFLOW"} for source in sources)
+        for solver_step in range(total_solver_steps):
+            if cancel_event is not None and cancel_event.is_set():
+                print("Bake cancellation requested. Stopping the simulation cleanly...")
+                break
+            output_frame = (solver_step + 1) // steps_per_frame
+            substep_index = solver_step % steps_per_frame
+            if dynamic:
+                particles_host, velocity_host = source_particles.apply_sources(
+                    sim.positions(), sim.velocities(), sources, obstacle_host, delta, rng)
+                sim = _resized(sim, particles_host, velocity_host)
+            t0 = time.perf_counter()
+            stats = sim.step()
+            if substep_index == steps_per_frame - 1:
+                output.submit_output(writer, particles=sim.particles, particle_count=sim.n,
+                                     frame=start_frame + output_frame)
+                emit_message({"type": "stats", "frame": output_frame, "total_frames": total_frames,
+                              "particle_count": sim.n, "solve": {"cycles": stats.cycles,
+                                                                 "rel_residual": stats.rel_residual,
+                                                                 "ms": (time.perf_counter() - t0) * 1e3}})
+    finally:
+        output.close_output(writer)
+
+
+def _resized(sim: FlipSolver, positions: np.ndarray, velocities: np.ndarray) -> FlipSolver:
+    """Re-upload host-edited particles (dynamic sources), growing capacity by 1.5x like
+    solver.py:290-303."""
+    n = len(positions)
+    cap = sim.particles.shape[0]
+    if n > cap:
+        new_cap = max(n, (cap * 3) // 2)
+        fresh = FlipSolver(sim.kernels, sim.grid_shape, sim.dx, positions, velocities, obstacle=sim.obstacle,
+                           dt=sim.dt, options=sim.options, particles_per_cell=sim.particles_per_cell,
+                           capacity=new_cap)
+        fresh.pressure.copy_(sim.pressure)
+        return fresh
+    sim.n = n
+    if n:
+        sim.particles[:n].copy_(torch.from_numpy(np.ascontiguousarray(positions, dtype=np.float32)))
+        sim.particle_velocity[:n].copy_(torch.from_numpy(np.ascontiguousarray(velocities, dtype=np.float32)))
+    return sim

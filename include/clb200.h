@@ -1,0 +1,225 @@
+/*
+ * clb200.h -- C ABI of the Continuum Liquid B200 backend (libclb200.so).
+ *
+ * Each entry point replaces one OpenCL kernel dispatch (or one host stage function) of the
+ * reference add-on's solver, Solver/Kernel/ of Continuum Liquid; the comment above each
+ * declaration names the reference interface it replaces (file:line).
+ *
+ * Conventions
+ *  - Every pointer is a device pointer to contiguous memory allocated by the caller; the library
+ *    never allocates. Grids are float32 [nx][ny][nz] with k fastest (helper.cl:4-6), particles
+ *    are float32 (N,3) records (particles.cl:56), counts and offsets int32, masks uint8.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream). Every call only enqueues work.
+ *  - Every function returns 0 on success and non-zero on failure; clb_last_error() then returns
+ *    the message (thread-local). Launch-configuration and argument errors are reported this way;
+ *    errors of asynchronous work surface at the caller's next synchronisation.
+ *  - Device-side bounded waits that run out do not hang: they record a code that
+ *    clb_device_error() returns (and clears).
+ */
+#ifndef CLB200_H
+#define CLB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- library ------------------------------------------------------------------------------ */
+
+/* Selects the device and prepares kernel attributes. Replaces helper.py:51-69
+ * select_opencl_device + cl.Context/CommandQueue creation (solver.py:29-37). */
+int clb_init(int device);
+/* Message of the last failed call on this thread ("" if none). */
+const char* clb_last_error(void);
+/* Reads and clears the device error word (0 = none, 1 = scan look-back wait gave up). Synchronous. */
+int clb_device_error(uint32_t* code);
+/* ABI version of this header (bumped on any signature change). */
+int clb_abi_version(void);
+
+/* ---- particles: binning, scan, sort, P2G (Solver/Kernel/particles.py, OpenCL/particles.cl) -- */
+
+/* particles.cl:44-59 count_particles_per_cell. Accumulates into bin_counts (the caller zero-fills
+ * it, as particles.py:146 does). keys/ranks (nullable, int32[n]) receive each particle's bin and a
+ * unique slot within it for clb_sort_particles. */
+int clb_count_particles_per_cell(const float* particles, int32_t* bin_counts, int32_t* keys, int32_t* ranks,
+                                 int64_t n, float inv_dx, int nx, int ny, int nz, void* stream);
+
+/* Scratch bytes clb_exclusive_prefix_sum needs for `count` elements. */
+int64_t clb_scan_scratch_bytes(int64_t count);
+
+/* particles.py:39-70 exclusive_prefix_sum (particles.cl:61-108 scan_blocks_exclusive +
+ * add_scanned_block_offsets), as one single-pass decoupled look-back scan. total (nullable)
+ * receives the sum of all values. scratch: clb_scan_scratch_bytes(count) bytes, 16-byte aligned. */
+int clb_exclusive_prefix_sum(const int32_t* values, int32_t* output, int32_t* total, int64_t count, void* scratch,
+                             int64_t scratch_bytes, void* stream);
+
+/* particles.cl:110-133 sort_particles (+ the buffer swap of particles.py:119-140 is the caller's).
+ * Stable counting-sort scatter: within a bin, particles keep their input order. perm and slot_keys
+ * are int32[n] scratch. */
+int clb_sort_particles(const float* particles, const float* velocity, float* particles_sorted, float* velocity_sorted,
+                       const int32_t* bin_offsets, const int32_t* bin_counts, const int32_t* keys,
+                       const int32_t* ranks, int32_t* perm, int32_t* slot_keys, int64_t n, void* stream);
+
+/* particles.cl:135-227 particle_to_grid_gather. */
+int clb_particle_to_grid_gather(const float* particles, const float* velocity, const int32_t* bin_offsets,
+                                const int32_t* bin_counts, float* u, float* v, float* w, float* fluid_fraction,
+                                float inv_dx, float inv_particles_per_cell, int nx, int ny, int nz, void* stream);
+
+/* particles.py:73-171 particle_to_grid: zero-fill, count, scan, stable sort into
+ * particles_work/velocity_work, gather. inv_dx and inv_particles_per_cell are the float32 values
+ * the reference passes (FIELD_DTYPE(1.0 / dx), FIELD_DTYPE(1.0 / particles_per_cell)). Workspace: keys, ranks, perm, slot_keys int32[n];
+ * scan_scratch of clb_scan_scratch_bytes(nx*ny*nz) bytes. The caller swaps the particle buffers
+ * afterwards, as the reference does. */
+int clb_particle_to_grid(const float* particles, const float* velocity, float* particles_work, float* velocity_work,
+                         float* u, float* v, float* w, float* fluid_fraction, int32_t* bin_counts,
+                         int32_t* bin_offsets, int32_t* keys, int32_t* ranks, int32_t* perm, int32_t* slot_keys,
+                         void* scan_scratch, int64_t scan_scratch_bytes, int64_t n, float inv_dx,
+                         float inv_particles_per_cell, int nx, int ny, int nz, void* stream);
+
+/* particles.cl:229-262 grid_to_particle (particles.py:174-206), plus a FLIP/PIC blend:
+ * flip_ratio = 1 is the reference's pure FLIP update. */
+int clb_grid_to_particle(float* velocity, const float* particles, const float* u, const float* v, const float* w,
+                         const float* u_old, const float* v_old, const float* w_old, int64_t n, float inv_dx, int nx,
+                         int ny, int nz, float flip_ratio, void* stream);
+
+/* particles.cl:264-276 advect_particles (particles.py:209-225). */
+int clb_advect_particles(float* particles, const float* velocity, int64_t n, float dt, void* stream);
+
+/* boundary_conditions.cl:69-97 particle_domain_bc (boundary_conditions.py:82-103). */
+int clb_particle_domain_bc(float* particles, float* velocity, int64_t n, float lower, float upper_x, float upper_y,
+                           float upper_z, void* stream);
+
+/* boundary_conditions.cl:175-264 particle_obstacle_bc (boundary_conditions.py:106-132). */
+int clb_particle_obstacle_bc(float* particles, const float* previous, float* velocity, const uint8_t* obstacle,
+                             int64_t n, float inv_dx, int nx, int ny, int nz, void* stream);
+
+/* solver.py:453-510 in one launch: grid_to_particle, the previous-position copy, advection,
+ * particle_domain_bc and (obstacle != NULL) particle_obstacle_bc. previous_out is nullable. */
+int clb_particle_update(float* particles, float* velocity, float* previous_out, const float* u, const float* v,
+                        const float* w, const float* u_old, const float* v_old, const float* w_old,
+                        const uint8_t* obstacle, int64_t n, float inv_dx, int nx, int ny, int nz, float flip_ratio,
+                        float dt, float lower, float upper_x, float upper_y, float upper_z, void* stream);
+
+/* ---- grid forces and boundary conditions --------------------------------------------------- */
+
+/* velocity_update.cl:3-43 update_velocity (velocity_update.py:8-52). */
+int clb_update_velocity(const float* u, const float* v, const float* w, float* result_u, float* result_v,
+                        float* result_w, const float* fluid_fraction, float gravity_x, float gravity_y,
+                        float gravity_z, float force_x, float force_y, float force_z, float rho, float nu,
+                        float inv_dx2, float dt, int nx, int ny, int nz, void* stream);
+
+/* boundary_conditions.cl:33-67 grid_domain_bc (boundary_conditions.py:36-50). */
+int clb_grid_domain_bc(float* u, float* v, float* w, int nx, int ny, int nz, void* stream);
+
+/* boundary_conditions.py:53-79 grid_obstacle_bc: boundary_conditions.cl:99-119 grid_obstacle_bc then
+ * boundary_conditions.cl:121-173 extrapolate_obstacle_velocity, as two launches. */
+int clb_grid_obstacle_bc(float* u, float* v, float* w, float* fluid_fraction, const uint8_t* obstacle, int nx, int ny,
+                         int nz, void* stream);
+
+/* pressure_solve.cl:3-24 pressure_rhs (pressure_solve.py:35-49). */
+int clb_pressure_rhs(const float* u, const float* v, const float* w, const float* fluid_fraction, float* rhs,
+                     float rho_over_dt, float inv_dx, int nx, int ny, int nz, void* stream);
+
+/* pressure_solve.cl:26-47 pressure_correction (pressure_solve.py:88-114). */
+int clb_pressure_correction(float* u, float* v, float* w, const float* pressure, float dt_over_rho, float inv_dx,
+                            int nx, int ny, int nz, void* stream);
+
+/* boundary_conditions.cl:18-31 neumann_domain_bc (boundary_conditions.py:22-33). */
+int clb_neumann_domain_bc(float* pressure, int nx, int ny, int nz, void* stream);
+
+/* ---- multigrid, reference layout (float32 mask/diagonal/weight arrays per level) -------------- */
+
+/* multigrid.cl:63-88 build_finest_operator (pressure_solve.py:50-59). */
+int clb_build_finest_operator(const float* mask, float* diagonal, float* weight_x, float* weight_y, float* weight_z,
+                              int nx, int ny, int nz, void* stream);
+
+/* multigrid.cl:203-230 rbgs_step (one colour; multigrid.py:190-220 calls it twice per iteration). */
+int clb_rbgs_step(float* p, const float* b, const float* mask, const float* diagonal, const float* weight_x,
+                  const float* weight_y, const float* weight_z, float delta, int parity, int nx, int ny, int nz,
+                  void* stream);
+
+/* multigrid.cl:90-180 restrict_residual (multigrid.py:106-125). */
+int clb_restrict_residual(const float* fine_p, const float* fine_b, const float* fine_mask, const float* fine_diagonal,
+                          const float* fine_weight_x, const float* fine_weight_y, const float* fine_weight_z,
+                          float* coarse_p, float* coarse_b, float* coarse_mask, float* coarse_diagonal,
+                          float* coarse_weight_x, float* coarse_weight_y, float* coarse_weight_z, float delta,
+                          int fine_nx, int fine_ny, int fine_nz, int coarse_nx, int coarse_ny, int coarse_nz,
+                          void* stream);
+
+/* multigrid.cl:182-201 prolongate (multigrid.py:172-185). */
+int clb_prolongate(const float* coarse_error, float* fine_p, const float* fine_mask, int coarse_nx, int coarse_ny,
+                   int coarse_nz, int fine_nx, int fine_ny, int fine_nz, void* stream);
+
+/* multigrid.cl:232-264 coarse_smooth (multigrid.py:223-249): one block, all sweeps. */
+int clb_coarse_smooth(float* p, const float* b, const float* mask, const float* diagonal, const float* weight_x,
+                      const float* weight_y, const float* weight_z, float delta, int iterations, int nx, int ny,
+                      int nz, void* stream);
+
+/* ---- multigrid, packed layout (product path) ------------------------------------------------ */
+
+#define CLB_MG_MAX_LEVELS 16
+
+/* A level pyramid as created by multigrid.py:18-50 create_multigrid_levels. Level 0 is the
+ * simulation grid; its operator is one byte per cell (bits 0-2 diagonal, 3-5 wx/wy/wz, 6 fluid).
+ * Coarse levels l >= 1 hold p, b (float32), a mask byte and a float4 (diagonal, wx, wy, wz). */
+typedef struct clb_mg_hierarchy {
+    int32_t levels;                      /* including level 0 */
+    int32_t shape[CLB_MG_MAX_LEVELS][3]; /* nx, ny, nz per level (ghost layer included) */
+    float delta;                         /* grid spacing used by every level (multigrid.py:65) */
+    int32_t reserved;
+    uint8_t* op0;                        /* level 0 packed operator */
+    float* p[CLB_MG_MAX_LEVELS];         /* [0] unused: level-0 x is passed per call */
+    float* b[CLB_MG_MAX_LEVELS];         /* [0] unused: level-0 rhs is passed per call */
+    uint8_t* mask[CLB_MG_MAX_LEVELS];    /* [0] unused */
+    void* op[CLB_MG_MAX_LEVELS];         /* [0] unused; float4 per cell */
+} clb_mg_hierarchy;
+
+/* pressure_solve.cl:3-24 pressure_rhs fused with multigrid.cl:63-88 build_finest_operator, writing
+ * the packed level-0 operator. */
+int clb_mg_rhs_operator(const float* u, const float* v, const float* w, const float* fluid_fraction, float* rhs,
+                        uint8_t* op0, float rho_over_dt, float inv_dx, int nx, int ny, int nz, void* stream);
+
+/* Operator part of multigrid.cl:90-180 restrict_residual for every coarse level, once per solve. */
+int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream);
+
+/* multigrid.py:53-187 w_cycle on level-0 unknown x and right-hand side rhs (pre/post/coarse sweeps
+ * as pressure_solve.py:61-83: 2, 4, 64). */
+int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pre_smooth, int post_smooth,
+                   int coarse_iterations, void* stream);
+
+/* Block-partial count used by clb_mg_residual_norms for a grid of `cells` cells. */
+int clb_mg_residual_partials(int64_t cells);
+
+/* FP64 relative-residual pieces over interior fluid cells of level 0: out[0] = sum (b - A p)^2,
+ * out[1] = sum b^2 (A = multigrid.cl:25-43 apply_operator). p is float32 (p_is_double = 0) or
+ * float64. r_out (nullable) receives the residual rounded to float32 (0 off the fluid). partials:
+ * clb_mg_residual_partials(cells) double2 scratch. */
+int clb_mg_residual_norms(const void* p, int p_is_double, const float* b, const uint8_t* op0, float delta, int nx,
+                          int ny, int nz, float* r_out, void* partials, double* out, void* stream);
+
+/* Iterative-refinement steps (FP64 accumulation of the pressure):
+ *  init:   p64 = p32 at interior fluid cells, 0 elsewhere
+ *  update: p64 += e
+ *  store:  p32 = (float) p64 */
+int clb_mg_ir_init(const float* p32, const uint8_t* op0, double* p64, int nx, int ny, int nz, void* stream);
+int clb_mg_ir_update(double* p64, const float* e, int64_t cells, void* stream);
+int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream);
+
+/* ---- collider voxelisation (Solver/Kernel/voxelise_mesh.py, OpenCL/voxelise_mesh.cl) ------- */
+
+/* voxelise_mesh.cl:24-48 voxelise_mesh: ORs 1 into mask for interior cells whose centre ray has an
+ * odd hit count (voxelise_mesh.py:111-135 launches it once per mesh on the same mask). triangles:
+ * float32 (T,3,3) world space; origin (ox,oy,oz) as voxelise_mesh.py:140. cull = 0 runs the
+ * brute-force test over every triangle; 1 skips triangles that lie behind all rays of a block. */
+int clb_voxelise_mesh(const float* triangles, uint8_t* mask, int triangle_count, int nx, int ny, int nz, float delta,
+                      float ox, float oy, float oz, int cull, void* stream);
+
+/* The ray direction of voxelise_mesh.cl:24 as three floats (host helper). */
+int clb_voxelise_direction(float* out3);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLB200_H */

@@ -1,0 +1,57 @@
+"""The C ABI library loads and exports every symbol include/clb200.h declares (no device work)."""
+
+import ctypes
+import re
+from pathlib import Path
+
+from continuum_liquid_b200 import backend, build
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "clb200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(clb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    build.build_library()
+    lib = ctypes.CDLL(str(build.LIBRARY))
+    names = declared_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing
+
+
+def test_python_signature_table_covers_the_header():
+    assert sorted(backend.SIGNATURES) == declared_functions()
+
+
+def test_load_library_sets_signatures_and_pure_helpers():
+    lib = backend.load_library()
+    assert lib.clb_abi_version() == 1
+    for count in (0, 1, 4096, 4097, 16777216):
+        assert lib.clb_scan_scratch_bytes(count) == backend.Backend.scan_scratch_bytes_static(count)
+    assert lib.clb_mg_residual_partials(1000) == 4
+    d = (ctypes.c_float * 3)()
+    assert lib.clb_voxelise_direction(d) == 0
+    assert abs(d[0] ** 2 + d[1] ** 2 + d[2] ** 2 - 1.0) < 1e-6
+
+
+def test_hierarchy_struct_layout():
+    # int32 levels (0), int32[16][3] (4..196), float delta (196), int32 reserved (200), then
+    # 8-byte-aligned pointers: op0 at 208 and the four pointer tables after it
+    assert backend.MGHierarchy.delta.offset == 196
+    assert backend.MGHierarchy.op0.offset == 208
+    assert backend.MGHierarchy.p.offset == 216
+    assert ctypes.sizeof(backend.MGHierarchy) == 216 + 4 * 16 * 8
+
+
+def test_backend_without_gpu_fails_loudly(monkeypatch):
+    import pytest
+    import torch
+
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        backend.Backend(0)

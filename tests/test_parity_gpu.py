@@ -1,0 +1,412 @@
+"""GPU parity: every CUDA entry point against the oracle on the same seeded inputs.
+
+Equality here is IEEE value equality (numpy.array_equal: -0 == +0). Everything except the
+documented tolerance cases must match exactly; the whole library is compiled without FMA
+contraction and keeps the reference's evaluation orders.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from continuum_liquid_b200 import boundary_conditions, multigrid, particles, pressure_solve, scenes, solver
+from continuum_liquid_b200 import velocity_update, voxelise_mesh
+
+pytestmark = pytest.mark.gpu
+
+F32 = np.float32
+
+
+def dev(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def scene_particles(n, seed=0, jitter_vel=True, shape=None):
+    s = scenes.dam_break(n, seed)
+    if shape is not None:
+        s.grid_shape = shape
+    pos, vel = scenes.seed_particles(s)
+    if jitter_vel:
+        vel = np.random.default_rng(seed + 1).standard_normal(pos.shape).astype(F32)
+    return s, pos, vel
+
+
+@pytest.fixture(params=[(16, 16, 16), (33, 33, 33), (40, 24, 31)], ids=lambda s: "x".join(map(str, s)))
+def case(request):
+    shape = request.param
+    n = shape[0]
+    s, pos, vel = scene_particles(n, seed=n, shape=shape)
+    s.grid_shape = shape
+    s.dx = 1.0 / n
+    pos = pos[np.all(pos < np.asarray(shape, F32) * F32(s.dx), axis=1)]
+    vel = vel[: len(pos)]
+    return shape, F32(s.dx), pos, vel
+
+
+# ---- binning, scan, sort, P2G ---------------------------------------------------------------------
+def test_count_keys_ranks(backend, oracle, case):
+    shape, dx, pos, _ = case
+    C, n = int(np.prod(shape)), len(pos)
+    counts = torch.zeros(C, dtype=torch.int32, device="cuda")
+    keys = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ranks = torch.zeros(n, dtype=torch.int32, device="cuda")
+    particles.count_particles_per_cell(backend, None, dev(pos), counts, n, shape, dx, keys, ranks)
+    assert np.array_equal(host(counts), oracle.count_particles(pos, dx, shape))
+    k = host(keys)
+    assert np.array_equal(k, oracle.bin_keys(pos, dx, shape))
+    r = host(ranks)
+    order = np.lexsort((r, k))
+    # ranks within each bin are exactly 0..count-1
+    kk, rr = k[order], r[order]
+    starts = np.r_[0, np.flatnonzero(np.diff(kk)) + 1]
+    expect = np.arange(n) - np.repeat(starts, np.diff(np.r_[starts, n]))
+    assert np.array_equal(rr, expect)
+
+
+@pytest.mark.parametrize("size", [0, 1, 5, 4095, 4096, 4097, 100003, 16777216 + 77])
+def test_scan(backend, size):
+    rng = np.random.default_rng(size)
+    values = rng.integers(0, 9, size).astype(np.int32)
+    out = torch.zeros(max(size, 1), dtype=torch.int32, device="cuda")[:size]
+    total = torch.zeros(1, dtype=torch.int32, device="cuda")
+    scratch = torch.zeros(backend.scan_scratch_bytes(size), dtype=torch.uint8, device="cuda")
+    backend.call("clb_exclusive_prefix_sum", dev(values) if size else out, out, total, size, scratch,
+                 scratch.numel())
+    expect = (np.cumsum(values) - values).astype(np.int64)
+    assert np.array_equal(host(out).astype(np.int64), expect)
+    assert int(host(total)[0]) == int(values.sum())
+    assert backend.device_error() == 0
+
+
+def test_scan_rejects_small_scratch(backend):
+    values = torch.ones(10000, dtype=torch.int32, device="cuda")
+    scratch = torch.zeros(8, dtype=torch.uint8, device="cuda")
+    with pytest.raises(RuntimeError, match="scratch"):
+        backend.call("clb_exclusive_prefix_sum", values, values, None, 10000, scratch, 8)
+
+
+def test_particle_to_grid_stage_bit_exact(backend, oracle, case):
+    shape, dx, pos, vel = case
+    n = len(pos)
+    work, vwork, counts, outs, sums = particles.create_particle_sort_buffers(backend, shape, n)
+    grid = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(4)]
+    P, V = dev(pos), dev(vel)
+    res = particles.particle_to_grid(backend, None, P, V, work, vwork, tuple(grid[:3]), counts, outs, sums, grid[3],
+                                     n, shape, float(dx), 8)
+    pos_s, vel_s, u, v, w, ff, ocounts, ooffsets = oracle.particle_to_grid(pos, vel, dx, shape)
+    assert res[0] is work and res[2] is P  # buffers swapped like particles.py:188-192
+    assert np.array_equal(host(counts), ocounts)
+    assert np.array_equal(host(outs[0]), ooffsets)
+    assert np.array_equal(host(res[0]), pos_s)
+    assert np.array_equal(host(res[1]), vel_s)
+    for g, o in zip(grid, (u, v, w, ff)):
+        assert np.array_equal(host(g), o)
+
+
+def test_dense_bins_and_outside_particles(backend, oracle):
+    """Many particles in one bin (slow path of the stable sort) and particles outside the grid
+    (clamped bins), as the reference allows."""
+    shape, dx = (12, 12, 12), F32(1.0 / 12)
+    rng = np.random.default_rng(5)
+    dense = (np.array([5.6, 5.6, 5.6]) + rng.random((300, 3)) * 0.3) * dx
+    outside = np.array([[-0.2, 0.5, 0.5], [0.5, 1.7, 0.5], [0.5, 0.5, -3.0]])
+    pos = np.concatenate([dense, rng.random((200, 3)), outside]).astype(F32)
+    vel = rng.standard_normal(pos.shape).astype(F32)
+    n = len(pos)
+    work, vwork, counts, outs, sums = particles.create_particle_sort_buffers(backend, shape, n)
+    grid = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(4)]
+    res = particles.particle_to_grid(backend, None, dev(pos), dev(vel), work, vwork, tuple(grid[:3]), counts, outs,
+                                     sums, grid[3], n, shape, float(dx), 8)
+    pos_s, vel_s, u, v, w, ff, _, _ = oracle.particle_to_grid(pos, vel, dx, shape)
+    assert np.array_equal(host(res[0]), pos_s) and np.array_equal(host(res[1]), vel_s)
+    for g, o in zip(grid, (u, v, w, ff)):
+        assert np.array_equal(host(g), o)
+
+
+def test_empty_particle_set(backend):
+    shape = (8, 8, 8)
+    work, vwork, counts, outs, sums = particles.create_particle_sort_buffers(backend, shape, 0)
+    grid = [torch.ones(shape, dtype=torch.float32, device="cuda") for _ in range(4)]
+    e = torch.zeros((1, 3), dtype=torch.float32, device="cuda")
+    particles.particle_to_grid(backend, None, e, e.clone(), work, vwork, tuple(grid[:3]), counts, outs, sums,
+                               grid[3], 0, shape, 0.125, 8)
+    assert not any(host(g).any() for g in grid)
+
+
+# ---- G2P and the fused particle update -----------------------------------------------------------
+@pytest.mark.parametrize("flip_ratio", [1.0, 0.95])
+def test_grid_to_particle(backend, oracle, case, flip_ratio):
+    shape, dx, pos, vel = case
+    rng = np.random.default_rng(7)
+    cur = [rng.standard_normal(shape).astype(F32) for _ in range(3)]
+    old = [rng.standard_normal(shape).astype(F32) for _ in range(3)]
+    V = dev(vel)
+    particles.grid_to_particle(backend, None, V, dev(pos), tuple(dev(a) for a in cur), tuple(dev(a) for a in old),
+                               len(pos), shape, float(dx), flip_ratio)
+    assert np.array_equal(host(V), oracle.grid_to_particle(vel, pos, cur, old, dx, shape, flip_ratio))
+
+
+@pytest.mark.parametrize("with_obstacle", [False, True])
+def test_fused_particle_update(backend, oracle, case, with_obstacle):
+    shape, dx, pos, vel = case
+    rng = np.random.default_rng(8)
+    cur = [rng.standard_normal(shape).astype(F32) for _ in range(3)]
+    old = [rng.standard_normal(shape).astype(F32) for _ in range(3)]
+    dt = 1.0 / 60.0
+    obstacle = (rng.random(shape) < 0.2).astype(np.uint8) if with_obstacle else np.zeros(shape, np.uint8)
+    P, V, prev = dev(pos), dev(vel), torch.zeros(pos.shape, dtype=torch.float32, device="cuda")
+    particles.particle_update(backend, None, P, V, tuple(dev(a) for a in cur), tuple(dev(a) for a in old),
+                              dev(obstacle) if with_obstacle else None, len(pos), shape, float(dx), dt, 0.95,
+                              previous_particles=prev)
+    v2 = oracle.grid_to_particle(vel, pos, cur, old, dx, shape, 0.95)
+    p2 = oracle.advect(pos, v2, dt)
+    p2, v2 = oracle.particle_domain_bc(p2, v2, dx, shape)
+    p2, v2 = oracle.particle_obstacle_bc(p2, pos, v2, obstacle, dx, shape)
+    assert np.array_equal(host(prev), pos)
+    assert np.array_equal(host(P), p2)
+    assert np.array_equal(host(V), v2)
+
+
+def test_separate_particle_kernels(backend, oracle, case):
+    shape, dx, pos, vel = case
+    rng = np.random.default_rng(9)
+    obstacle = (rng.random(shape) < 0.2).astype(np.uint8)
+    prev = (pos - rng.random(pos.shape).astype(F32) * F32(dx)).astype(F32)
+    P, V = dev(pos), dev(vel)
+    particles.advect_particles(backend, None, P, V, len(pos), 0.01)
+    boundary_conditions.particle_domain_bc(backend, None, P, V, len(pos), shape, float(dx))
+    boundary_conditions.particle_obstacle_bc(backend, None, P, dev(prev), V, dev(obstacle), len(pos), shape,
+                                             float(dx))
+    p2 = oracle.advect(pos, vel, 0.01)
+    p2, v2 = oracle.particle_domain_bc(p2, vel, dx, shape)
+    p2, v2 = oracle.particle_obstacle_bc(p2, prev, v2, obstacle, dx, shape)
+    assert np.array_equal(host(P), p2) and np.array_equal(host(V), v2)
+
+
+# ---- grid kernels ---------------------------------------------------------------------------------
+def test_grid_kernels(backend, oracle, case):
+    shape, dx, _, _ = case
+    rng = np.random.default_rng(11)
+    u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
+    ff = (rng.random(shape) * (rng.random(shape) < 0.6)).astype(F32)
+    ff[[0, -1]] = 0
+    ff[:, [0, -1]] = 0
+    ff[:, :, [0, -1]] = 0
+    obstacle = (rng.random(shape) < 0.1).astype(np.uint8)
+    p = rng.standard_normal(shape).astype(F32)
+    dt, rho, nu = 1.0 / 240.0, 1000.0, 1e-3
+    # update_velocity
+    out = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(3)]
+    velocity_update.update_velocity(backend, None, (dev(u), dev(v), dev(w)), tuple(out), dev(ff), (0.0, -9.81, 0.0),
+                                    0.0, 0.0, 0.0, rho, nu, float(dx), dt, shape)
+    exp = oracle.update_velocity(u, v, w, ff, (0.0, -9.81, 0.0), (0.0, 0.0, 0.0), rho, nu, dx, dt, shape)
+    for a, b in zip(out, exp):
+        assert np.array_equal(host(a), b)
+    # grid_domain_bc
+    U, Vv, W = dev(u), dev(v), dev(w)
+    boundary_conditions.grid_domain_bc(backend, None, (U, Vv, W), shape)
+    for a, b in zip((U, Vv, W), oracle.grid_domain_bc(u, v, w, shape)):
+        assert np.array_equal(host(a), b)
+    # grid_obstacle_bc (+ extrapolation)
+    U, Vv, W, FF = dev(u), dev(v), dev(w), dev(ff)
+    boundary_conditions.grid_obstacle_bc(backend, None, (U, Vv, W), FF, dev(obstacle), shape)
+    for a, b in zip((U, Vv, W, FF), oracle.grid_obstacle_bc(u, v, w, ff, obstacle, shape)):
+        assert np.array_equal(host(a), b)
+    # pressure_rhs / pressure_correction / neumann
+    rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    backend.call("clb_pressure_rhs", dev(u), dev(v), dev(w), dev(ff), rhs, float(F32(rho / dt)), float(F32(1 / dx)),
+                 *shape)
+    assert np.array_equal(host(rhs), oracle.pressure_rhs(u, v, w, ff, dx, dt, rho, shape))
+    U, Vv, W = dev(u), dev(v), dev(w)
+    pressure_solve.pressure_correction(backend, None, (U, Vv, W), dev(p), float(dx), dt, rho, shape)
+    for a, b in zip((U, Vv, W), oracle.pressure_correction(u, v, w, p, dx, dt, rho, shape)):
+        assert np.array_equal(host(a), b)
+    Pp = dev(p)
+    boundary_conditions.neumann_domain_bc(backend, None, Pp, shape)
+    assert np.array_equal(host(Pp), oracle.neumann_domain_bc(p, shape))
+
+
+# ---- multigrid ------------------------------------------------------------------------------------
+def random_system(shape, seed):
+    rng = np.random.default_rng(seed)
+    ff = np.zeros(shape, F32)
+    ff[1:-1, 1 : shape[1] // 2 + 2, 1:-1] = 0.5
+    ff[rng.random(shape) < 0.1] = 0
+    ff[[0, -1]] = 0
+    ff[:, [0, -1]] = 0
+    ff[:, :, [0, -1]] = 0
+    b = (rng.standard_normal(shape) * 1e4 * (ff > 0)).astype(F32)
+    p0 = rng.standard_normal(shape).astype(F32)
+    return ff, b, p0
+
+
+def test_reference_layout_kernels(backend, oracle, case):
+    shape, dx, _, _ = case
+    ff, b, p0 = random_system(shape, 12)
+    ops = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(4)]
+    backend.call("clb_build_finest_operator", dev(ff), *ops, *shape)
+    oops = oracle.build_finest_operator(ff, shape)
+    for a, o in zip(ops, oops):
+        assert np.array_equal(host(a), o)
+    P = dev(p0)
+    for parity in (0, 1, 0):
+        backend.call("clb_rbgs_step", P, dev(b), dev(ff), *ops, float(dx), parity, *shape)
+    q = p0.copy()
+    for parity in (0, 1, 0):
+        oracle.lib().orc_rbgs_step_f32(q, b, ff, *oops, dx, parity, *shape)
+    assert np.array_equal(host(P), q)
+    cshape = tuple(oracle.coarse_grid_size(s) for s in shape)
+    carr = [torch.zeros(cshape, dtype=torch.float32, device="cuda") for _ in range(7)]
+    backend.call("clb_restrict_residual", P, dev(b), dev(ff), *ops, *carr, float(dx), *shape, *cshape)
+    oc = [np.zeros(cshape, F32) for _ in range(7)]
+    oracle.lib().orc_restrict_residual_f32(q, b, ff, *oops, *oc, dx, *shape, *cshape)
+    for a, o in zip(carr, oc):
+        assert np.array_equal(host(a), o)
+    ce = np.random.default_rng(13).standard_normal(cshape).astype(F32)
+    backend.call("clb_prolongate", dev(ce), P, dev(ff), *cshape, *shape)
+    oracle.lib().orc_prolongate_f32(ce, q, ff, *cshape, *shape)
+    assert np.array_equal(host(P), q)
+    # coarse smooth on the coarse level produced by restriction
+    cp = carr[0]
+    backend.call("clb_coarse_smooth", cp, *carr[1:], float(dx), 66, *cshape)
+    ocp = oc[0].copy()
+    oracle.lib().orc_coarse_smooth_f32(ocp, *oc[1:], dx, 66, *cshape)
+    assert np.array_equal(host(cp), ocp)
+
+
+def test_reference_layout_w_cycle(backend, oracle):
+    shape, dx = (34, 34, 34), F32(1.0 / 34)
+    ff, b, p0 = random_system(shape, 14)
+    lv = multigrid.create_multigrid_levels(backend, shape)
+    ops = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(4)]
+    backend.call("clb_build_finest_operator", dev(ff), *ops, *shape)
+    P = dev(p0)
+    for _ in range(2):
+        multigrid.w_cycle(backend, None, 0, lv[0], lv[1], lv[2], lv[3], P, dev(b), dev(ff), tuple(ops), float(dx),
+                          lv[4], shape, 2, 4, 64)
+    levels = oracle.Levels(shape)
+    q = p0.copy()
+    oops = oracle.build_finest_operator(ff, shape)
+    for _ in range(2):
+        levels.w_cycle(q, b, ff, oops, dx)
+    assert np.array_equal(host(P), q)
+
+
+@pytest.mark.parametrize("shape", [(34, 34, 34), (66, 66, 66), (48, 40, 56)])
+def test_packed_w_cycle_equals_reference(backend, oracle, shape):
+    dx = F32(1.0 / shape[0])
+    rng = np.random.default_rng(15)
+    u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
+    ff, _, p0 = random_system(shape, 16)
+    dt, rho = 1.0 / 240.0, 1000.0
+    h = multigrid.MultigridHierarchy(backend, shape, float(dx))
+    rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    h.rhs_operator((dev(u), dev(v), dev(w)), dev(ff), rhs, dt, rho)
+    orhs = oracle.pressure_rhs(u, v, w, ff, dx, dt, rho, shape)
+    oops = oracle.build_finest_operator(ff, shape)
+    assert np.array_equal(host(rhs), orhs)
+    unpacked = multigrid.unpack_op0(host(h.op0))
+    inner = np.zeros(shape, bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    assert np.array_equal(unpacked[0], ((ff > 0) & inner).astype(F32))
+    for a, o in zip(unpacked[1:], oops):
+        assert np.array_equal(a, o)
+    h.build_coarse()
+    P = dev(p0)
+    for _ in range(2):
+        h.w_cycle(P, rhs)
+    levels = oracle.Levels(shape)
+    q = p0.copy()
+    for _ in range(2):
+        levels.w_cycle(q, orhs, ff, oops, dx)
+    assert np.array_equal(host(P), q)
+    # coarse operators equal the oracle's (its levels hold the last restriction's operator)
+    for lvl in range(1, h.levels):
+        arr = h.level_arrays(lvl)
+        assert np.array_equal(arr["op"][..., 0], levels.ops[lvl][0])
+        assert np.array_equal(arr["op"][..., 1], levels.ops[lvl][1])
+        assert np.array_equal(arr["mask"].astype(F32), levels.m[lvl])
+    # FP64 residual norms
+    norms = host(h.residual_norms(P, rhs))
+    rr, bb = oracle.residual_norms(q, orhs, ff, oops, dx)
+    assert norms[0] == pytest.approx(rr, rel=1e-12) and norms[1] == pytest.approx(bb, rel=1e-12)
+
+
+def test_iterative_refinement_reaches_tolerance(backend, oracle):
+    shape, dx = (34, 34, 34), F32(1.0 / 34)
+    rng = np.random.default_rng(17)
+    u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
+    ff, _, _ = random_system(shape, 18)
+    dt, rho = 1.0 / 240.0, 1000.0
+    ps = pressure_solve.PressureSolver(backend, shape, float(dx))
+    P = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    stats = ps.solve((dev(u), dev(v), dev(w)), dev(ff), P, dt, rho, tol=1e-6)
+    assert stats.rel_residual <= 1e-6
+    assert stats.cycles >= 3
+    orhs = oracle.pressure_rhs(u, v, w, ff, dx, dt, rho, shape)
+    p64, hist = oracle.fp64_pressure_solve(orhs, ff, shape, dx, tol=1e-13)
+    got = host(P)
+    interior = ff > 0
+    err = np.abs(got[interior] - p64[interior]).max() / np.abs(p64[interior]).max()
+    assert err < 1e-5
+    # air cells inside the domain hold zero pressure; ghosts carry the Neumann copy
+    inner = np.zeros(shape, bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    assert not got[inner & (ff <= 0)].any()
+    assert np.array_equal(got, oracle.neumann_domain_bc(got, shape))
+
+
+# ---- voxelisation ---------------------------------------------------------------------------------
+@pytest.mark.parametrize("n,sub", [(32, 2), (48, 3), (40, 4)])
+def test_voxelise_bit_exact(backend, oracle, n, sub):
+    shape, delta = (n, n, n), 1.0 / n
+    origin = (-0.5, -0.5, 0.0)
+    rng = np.random.default_rng(n)
+    tris = scenes.icosphere(sub, 0.21, (rng.uniform(-0.1, 0.1), rng.uniform(-0.1, 0.1), 0.5))
+    expect = oracle.voxelise(tris, shape, delta, origin)
+    for cull in (False, True):
+        mask = torch.zeros(shape, dtype=torch.uint8, device="cuda")
+        voxelise_mesh.voxelise_triangles(backend, None, tris, mask, shape, delta, origin, cull=cull)
+        assert np.array_equal(host(mask), expect), f"cull={cull}"
+    assert expect.sum() > 0
+
+
+def test_voxelise_direction_matches_oracle(backend, oracle):
+    assert np.array_equal(np.asarray(backend.voxelise_direction, F32), oracle.voxelise_direction())
+
+
+# ---- whole steps -----------------------------------------------------------------------------------
+@pytest.mark.parametrize("with_obstacle", [False, True])
+def test_full_steps_match_oracle(backend, oracle, with_obstacle):
+    n = 32
+    s = scenes.collider_pool(n, subdivisions=2) if with_obstacle else scenes.dam_break(n)
+    obstacle = np.zeros(s.grid_shape, np.uint8)
+    for tris in s.obstacles:
+        obstacle = oracle.voxelise(tris, s.grid_shape, s.dx, s.origin, obstacle)
+    pos, vel = scenes.seed_particles(s, obstacle)
+    opts = solver.StepOptions(flip_ratio=1.0, num_vcycles=1, gravity=s.gravity, use_graph=False)
+    sim = solver.FlipSolver(backend, s.grid_shape, s.dx, pos, vel, obstacle=obstacle, dt=s.dt, options=opts)
+    ref = oracle.OracleSim(s.grid_shape, s.dx, pos, vel, obstacle=obstacle, dt=s.dt, flip_ratio=1.0,
+                           gravity=s.gravity)
+    for step in range(4):
+        sim.step()
+        ref.step()
+        assert np.array_equal(host(sim.pressure), ref.pressure), f"pressure, step {step}"
+        assert np.array_equal(sim.positions(), ref.pos), f"positions, step {step}"
+        assert np.array_equal(sim.velocities(), ref.vel), f"velocities, step {step}"
+
+
+def test_bad_arguments_raise(backend):
+    t = torch.zeros(8, dtype=torch.float32, device="cuda")
+    with pytest.raises(RuntimeError, match="grid"):
+        backend.call("clb_grid_domain_bc", t, t, t, 2, 2, 2)
+    with pytest.raises(RuntimeError, match="parity"):
+        backend.call("clb_rbgs_step", t, t, t, t, t, t, t, 1.0, 3, 4, 4, 4)
