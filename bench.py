@@ -1,0 +1,362 @@
+"""Benchmark: FLIP steps/s on the 256^3 block scene (~23M particles) and Poisson ms to 1e-6.
+
+One "step" is one full FLIP timestep of the hot path (binning + counting sort + P2G, grid forces and
+boundary conditions, pressure solve to a 1e-6 relative residual by FP64-refined W-cycles, projection,
+fused G2P/advection/particle BCs). Synthetic scene: seeded, see continuum_liquid_b200/scenes.py.
+
+  python bench.py [--gpus N --steps K --warmup W]         this backend (value, e2e, roofline, cpu_baseline)
+  python bench.py --impl reference [...]                  the reference algorithm on the host cores (the
+                                                          CPU restatement; the OpenCL original cannot run here)
+
+Under torchrun with N > 1 every rank advances an independent replica of the scene (the solver is
+single-GPU; scenes do not exchange data), the timed region is bracketed by barriers and the time is
+the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "steps/s at 256^3; Poisson ms to 1e-6 rel. residual, learned vs plain W-cycle"
+UNIT = "steps/s"
+TOL = 1e-6
+
+# DRAM bytes per launch of the dominant kernel from one ncu capture (see profiles/); None if not captured.
+NCU_TRAFFIC_BYTES = {}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=256, help="grid size n of the n^3 block scene")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-cycles", type=int, default=None, help="W-cycles per CPU step (default: measured)")
+    return ap.parse_args()
+
+
+def workload_config(size, n_particles, args):
+    return {
+        "workload": f"flip_step_block_{size}^3",
+        "grid": [size, size, size],
+        "particles": int(n_particles),
+        "liquid_block": [[0, 0, 0], [0.5, 0.7, 0.5]],
+        "dt": 1.0 / 240.0,
+        "flip_ratio": 0.95,
+        "pressure_tolerance": TOL,
+        "pressure_solver": "W-cycle (pre 2, post 4, coarse 2+64) in FP64 iterative refinement",
+        "multigrid_levels": None,
+        "l2": "inputs larger than L2 (particle state 24 B x N, grid fields 4 B x n^3 each)",
+        "parallelism": "replicas" if args.gpus > 1 else "single",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi sampler running during the timed region (clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        sm_max = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None, "sm_max_mhz": sm_max, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peak_hbm():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------------------
+def run_cpu_steps(scene, positions, velocities, steps, cycles, threads_note=True):
+    """The reference algorithm on the host cores (oracle restatement, OpenMP): `steps` full steps
+    with `cycles` W-cycles each; returns seconds per step and the cycle count used."""
+    from oracle import oracle
+
+    sim = oracle.OracleSim(scene.grid_shape, scene.dx, positions, velocities, dt=scene.dt, flip_ratio=0.95,
+                           gravity=scene.gravity, num_vcycles=cycles)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        sim.step()
+        times.append(time.perf_counter() - t0)
+    return float(np.mean(times)), oracle.lib().orc_num_threads()
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from continuum_liquid_b200 import scenes
+
+    scene = scenes.block(args.size)
+    positions, velocities = scenes.seed_particles(scene)
+    cycles = args.cpu_cycles or 6
+    steps = max(1, min(args.steps, 2))
+    warm = 1 if args.warmup > 0 else 0
+    if warm:
+        run_cpu_steps(scene, positions, velocities, 1, cycles)
+    sec, threads = run_cpu_steps(scene, positions, velocities, steps, cycles)
+    value = 1.0 / sec
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": warm,
+        "ms_per_step": sec * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": workload_config(args.size, len(positions), args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{steps} full step(s) of the {args.size}^3 block scene ({len(positions)} particles) "
+                                   f"with {cycles} FP32 W-cycles per step (the reference method: fixed cycle count; "
+                                   f"the OpenCL original cannot run on this host)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+def our_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    from continuum_liquid_b200 import scenes, solver
+    from continuum_liquid_b200.backend import Backend
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    kernels = Backend(local)
+    dev = kernels.device
+    scene = scenes.block(args.size)
+    obstacle = torch.zeros(scene.grid_shape, dtype=torch.uint8, device=dev)
+    positions, velocities = scenes.seed_particles(scene)
+    opts = solver.StepOptions(flip_ratio=0.95, tol=TOL, gravity=scene.gravity, rho=scene.rho, nu=scene.nu)
+    sim = solver.FlipSolver(kernels, scene.grid_shape, scene.dx, positions, velocities, obstacle=obstacle, dt=scene.dt,
+                            options=opts)
+    n = sim.n
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        sim.step()
+    torch.cuda.synchronize()
+
+    # --- device-resident timed region -------------------------------------------------------
+    stats = []
+    solve_ms = []
+    launches0 = kernels.launch_count()
+    replays0 = sim.pressure_solver.graph_replays
+    with ClockSampler(dev.index) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed")
+        start.record()
+        for _ in range(args.steps):
+            stats.append(sim.step())
+        end.record()
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        barrier()
+    clock_summary = clocks.summary()
+    elapsed_ms = max_over_ranks(start.elapsed_time(end))
+    direct_launches = kernels.launch_count() - launches0
+    replays = sim.pressure_solver.graph_replays - replays0
+    gpu_launches = direct_launches + replays * sim.pressure_solver.graph_launches
+    cycles = [s.cycles for s in stats]
+    solve_ms = [s.ms for s in stats]
+    value = world * args.steps / (elapsed_ms / 1e3)
+
+    # --- plain vs learned Poisson time to 1e-6 (learned part: reported when available) -------
+    poisson = {"plain_ms_mean": float(np.mean(solve_ms)), "plain_cycles_mean": float(np.mean(cycles)),
+               "final_rel_residual_max": float(max(s.rel_residual or 0.0 for s in stats)),
+               "initial_rel_residual_mean": float(np.mean([s.initial_rel_residual or 0.0 for s in stats])),
+               "history_last_step": [float(x) for x in stats[-1].history]}
+
+    # --- end to end through the stage API with host buffers ------------------------------------
+    e2e = None
+    if not args.no_e2e:
+        host_pos = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        host_vel = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        host_pos.copy_(sim.particles[:n])
+        host_vel.copy_(sim.particle_velocity[:n])
+        torch.cuda.synchronize()
+        barrier()
+        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2e_steps = max(1, args.steps // 2)
+        s2.record()
+        for _ in range(e2e_steps):
+            sim.particles[:n].copy_(host_pos, non_blocking=True)
+            sim.particle_velocity[:n].copy_(host_vel, non_blocking=True)
+            sim.step()
+            host_pos.copy_(sim.particles[:n], non_blocking=True)
+            host_vel.copy_(sim.particle_velocity[:n], non_blocking=True)
+        e2.record()
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = max_over_ranks(s2.elapsed_time(e2))
+        e2e = {"value": world * e2e_steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+               "d2h_bytes_per_step": 24 * n, "steps": e2e_steps,
+               "path": "FlipSolver.step with the particle state copied from pinned host buffers before and back "
+                       "after every step (the reference's per-step host round trip of solver.py:252-306)"}
+
+    # --- roofline: level-0 red-black Gauss-Seidel sweep, timed alone on the stream ------------
+    ps = sim.pressure_solver
+    h = ps.hierarchy
+    iters = 20
+    torch.cuda.synchronize()
+    ps.correction.zero_()
+    h.smooth(0, 2, ps.correction, ps.residual)
+    s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s3.record()
+    h.smooth(0, iters, ps.correction, ps.residual)
+    e3.record()
+    torch.cuda.synchronize()
+    fused = h.alt[0] is not None
+    launches_timed = iters if fused else 2 * iters
+    per_launch_s = s3.elapsed_time(e3) / 1e3 / launches_timed
+    cells = int(np.prod(scene.grid_shape))
+    # p read + write 8 B, b 4 B, packed operator 1 B per cell per red-black iteration
+    algorithmic = 13.0 * cells if fused else 13.0 * cells / 2.0
+    achieved = algorithmic / per_launch_s / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    kernel = "k_rbgs_iter<true>" if fused else "k_rbgs<true>"
+    traffic = NCU_TRAFFIC_BYTES.get(kernel)
+    roofline = {"kernel": f"{kernel} (level-0 red-black Gauss-Seidel, {'one iteration' if fused else 'one colour'} "
+                          "per launch)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                "traffic": traffic, "algorithmic_bytes_per_launch": algorithmic, "launch_us": per_launch_s * 1e6}
+
+    # --- CPU baseline (rank 0, N = 1): the reference algorithm on the host cores ---------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        k = args.cpu_cycles or max(1, int(round(float(np.mean(cycles)))))
+        sec, threads = run_cpu_steps(scene, positions, velocities, 1, k)
+        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"1 full step of the same scene ({n} particles) by the CPU restatement of the reference "
+                         f"kernels with {k} FP32 W-cycles (the GPU's mean cycle count)"}
+
+    if rank == 0:
+        config = workload_config(args.size, n, args)
+        config["multigrid_levels"] = [list(s) for s in h.shapes]
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": config,
+            "particles_per_s": value * n,
+            "poisson": poisson,
+            "e2e": e2e,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clock_summary,
+            "gpu_launches": int(gpu_launches),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -33,6 +33,7 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_last_error": [],
     "clb_device_error": [P],
     "clb_abi_version": [],
+    "clb_launch_count": [],
     "clb_count_particles_per_cell": [P, P, P, P, L, F, I, I, I, P],
     "clb_scan_scratch_bytes": [L],
     "clb_exclusive_prefix_sum": [P, P, P, L, P, L, P],
@@ -58,15 +59,22 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_rhs_operator": [P, P, P, P, P, P, F, F, I, I, I, P],
     "clb_mg_build_coarse": [P, P],
     "clb_mg_w_cycle": [P, P, P, I, I, I, P],
+    "clb_mg_smooth": [P, I, P, P, I, P],
+    "clb_mg_set_option": [I, I],
     "clb_mg_residual_partials": [L],
     "clb_mg_residual_norms": [P, I, P, P, F, I, I, I, P, P, P, P],
     "clb_mg_ir_init": [P, P, P, I, I, I, P],
+    "clb_mg_ir_step": [P, P, P, P, P, F, I, I, I, P, P, P, P],
     "clb_mg_ir_update": [P, P, L, P],
     "clb_mg_ir_store": [P, P, L, P],
     "clb_voxelise_mesh": [P, P, I, I, I, I, F, F, F, F, I, P],
     "clb_voxelise_direction": [P],
 }
-_RESTYPES = {"clb_last_error": ctypes.c_char_p, "clb_scan_scratch_bytes": ctypes.c_int64}
+_RESTYPES = {
+    "clb_last_error": ctypes.c_char_p,
+    "clb_scan_scratch_bytes": ctypes.c_int64,
+    "clb_launch_count": ctypes.c_int64,
+}
 
 
 class MGHierarchy(ctypes.Structure):
@@ -82,6 +90,7 @@ class MGHierarchy(ctypes.Structure):
         ("b", ctypes.c_void_p * MG_MAX_LEVELS),
         ("mask", ctypes.c_void_p * MG_MAX_LEVELS),
         ("op", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("alt", ctypes.c_void_p * MG_MAX_LEVELS),
     ]
 
 
@@ -158,6 +167,10 @@ class Backend:
         header plus one 8-byte look-back status word per 4096-element tile."""
         tiles = (int(count) + SCAN_TILE - 1) // SCAN_TILE
         return 16 + 8 * max(tiles, 1)
+
+    def launch_count(self) -> int:
+        """Kernels launched directly by the library so far (graph replays excluded)."""
+        return int(self.lib.clb_launch_count())
 
     def residual_partials(self, cells: int) -> int:
         return int(self.lib.clb_mg_residual_partials(cells))

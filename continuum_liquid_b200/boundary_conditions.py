@@ -40,10 +40,10 @@ def particle_domain_bc(kernels: Backend, queue, particles, particle_velocity, pa
         particles,
         particle_velocity,
         int(particle_count_total),
-        float(FIELD_DTYPE(1.001 * dx)),
-        float(FIELD_DTYPE((grid_shape[0] - 1.001) * dx)),
-        float(FIELD_DTYPE((grid_shape[1] - 1.001) * dx)),
-        float(FIELD_DTYPE((grid_shape[2] - 1.001) * dx)),
+        float(FIELD_DTYPE(1.001 * float(dx))),
+        float(FIELD_DTYPE((grid_shape[0] - 1.001) * float(dx))),
+        float(FIELD_DTYPE((grid_shape[1] - 1.001) * float(dx))),
+        float(FIELD_DTYPE((grid_shape[2] - 1.001) * float(dx))),
         stream=queue,
     )
     return particles, particle_velocity
@@ -54,5 +54,5 @@ def particle_obstacle_bc(kernels: Backend, queue, particles, previous_particles,
     """boundary_conditions.py:106-132 (boundary_conditions.cl:175-264)."""
     nx, ny, nz = grid_shape
     kernels.call("clb_particle_obstacle_bc", particles, previous_particles, particle_velocity, obstacle,
-                 int(particle_count_total), float(FIELD_DTYPE(1.0 / dx)), nx, ny, nz, stream=queue)
+                 int(particle_count_total), float(FIELD_DTYPE(1.0 / float(dx))), nx, ny, nz, stream=queue)
     return particles, particle_velocity

@@ -5,6 +5,8 @@
 #include "particles.cuh"
 #include "grid.cuh"
 #include "multigrid.cuh"
+#include "mg_bottom.cuh"
+#include "mg_sweep.cuh"
 #include "voxelise.cuh"
 
 using namespace clb;
@@ -15,11 +17,15 @@ using namespace clb;
                 (nz));                                                                                 \
     CLB_REQUIRE((i64)(nx) * (ny) * (nz) < (1ll << 31), "grid %dx%dx%d has more than 2^31 cells", (nx), (ny), (nz))
 
-static const int kAbiVersion = 1;
+static const int kAbiVersion = 2;
+static const size_t kBottomSmemLimit = 220 * 1024;
+static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 
 extern "C" {
 
 int clb_abi_version(void) { return kAbiVersion; }
+
+int64_t clb_launch_count(void) { return (int64_t)g_launches.load(std::memory_order_relaxed); }
 
 const char* clb_last_error(void) { return t_last_error; }
 
@@ -42,6 +48,14 @@ int clb_init(int device) {
                                         smem_max),
                    "coarse solve attribute"))
         return 1;
+    const int bottom_max = (int)kBottomSmemLimit;
+    cudaError_t e = cudaSuccess;
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    if (check_call(e, "bottom visit attribute")) return 1;
     return 0;
 }
 
@@ -401,6 +415,7 @@ namespace {
 
 struct LevelView {
     float* p;
+    float* alt;
     const float* b;
     const uint8_t* op0;
     const float4* opc;
@@ -412,6 +427,7 @@ struct LevelView {
 LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rhs) {
     LevelView v;
     v.l0 = (l == 0);
+    v.alt = h->alt[l];
     v.p = v.l0 ? x : h->p[l];
     v.b = v.l0 ? rhs : h->b[l];
     v.op0 = h->op0;
@@ -425,6 +441,36 @@ LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rh
 
 int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
     const i64 C = (i64)v.nx * v.ny * v.nz;
+    if (v.alt != nullptr && iterations > 0) {
+        // fused iterations, alternating between the level's buffer and its second buffer
+        const dim3 big((v.nz + 31) / 32, (v.ny + 7) / 8, (v.nx + 7) / 8);
+        const dim3 small((v.nz + 31) / 32, (v.ny + 3) / 4, (v.nx + 3) / 4);
+        const bool use_big = (i64)big.x * big.y * big.z >= 4 * (i64)(g_sm_count > 0 ? g_sm_count : 148);
+        float* cur = v.p;
+        float* other = v.alt;
+        for (int it = 0; it < iterations; ++it) {
+            if (v.l0 && use_big)
+                k_rbgs_iter<true, 8, 8, 32><<<big, SW_THREADS, 0, s>>>(cur, other, v.b, v.op0, nullptr, nullptr,
+                                                                       delta, v.nx, v.ny, v.nz);
+            else if (v.l0)
+                k_rbgs_iter<true, 4, 4, 32><<<small, SW_THREADS, 0, s>>>(cur, other, v.b, v.op0, nullptr, nullptr,
+                                                                         delta, v.nx, v.ny, v.nz);
+            else if (use_big)
+                k_rbgs_iter<false, 8, 8, 32><<<big, SW_THREADS, 0, s>>>(cur, other, v.b, nullptr, v.opc, v.mask,
+                                                                        delta, v.nx, v.ny, v.nz);
+            else
+                k_rbgs_iter<false, 4, 4, 32><<<small, SW_THREADS, 0, s>>>(cur, other, v.b, nullptr, v.opc, v.mask,
+                                                                          delta, v.nx, v.ny, v.nz);
+            CLB_LAUNCH_CHECK("k_rbgs_iter");
+            float* t = cur;
+            cur = other;
+            other = t;
+        }
+        if (cur != v.p && check_call(cudaMemcpyAsync(v.p, cur, sizeof(float) * C, cudaMemcpyDeviceToDevice, s),
+                                     "smooth copy-back"))
+            return 1;
+        return 0;
+    }
     for (int it = 0; it < iterations; ++it)
         for (int parity = 0; parity < 2; ++parity) {
             if (v.l0)
@@ -460,11 +506,43 @@ int coarse_solve(const LevelView& v, float delta, int iterations, cudaStream_t s
     return 0;
 }
 
+// One launch for a whole visit of the second-coarsest level when both bottom levels fit in shared
+// memory (mg_bottom.cuh); returns 1 if it launched, 0 if the caller must recurse, -1 on error.
+int bottom_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int coarse_iters, cudaStream_t s) {
+    if (!g_use_bottom || level < 1 || level != h->levels - 2) return 0;
+    const int* a = h->shape[level];
+    const int* b = h->shape[level + 1];
+    const int ca = a[0] * a[1] * a[2], cb = b[0] * b[1] * b[2];
+    const int ma = (a[0] - 2) * (a[1] - 2) * (a[2] - 2), mb = (b[0] - 2) * (b[1] - 2) * (b[2] - 2);
+    const size_t bytes = bottom_smem_bytes(ca, cb);
+    const int mbc = mb / 2;  // cells of each colour (the B extent along k must be even)
+    if (bytes > kBottomSmemLimit || ((b[2] - 2) & 1) || mbc > BOTTOM_MAX_B * BOTTOM_BTHREADS ||
+        ma > BOTTOM_MAX_A * BOTTOM_THREADS)
+        return 0;
+    const int ka = (ma + BOTTOM_THREADS - 1) / BOTTOM_THREADS;
+    const int kb = (mbc + BOTTOM_BTHREADS - 1) / BOTTOM_BTHREADS;
+#define CLB_BOTTOM(KA, KB)                                                                                      \
+    k_bottom_visit<KA, KB><<<1, BOTTOM_THREADS, bytes, s>>>(                                                      \
+        h->p[level], h->b[level], (const float4*)h->op[level], h->mask[level], a[0], a[1], a[2], h->p[level + 1], \
+        h->b[level + 1], (const float4*)h->op[level + 1], h->mask[level + 1], b[0], b[1], b[2], h->delta, pre,  \
+        post, coarse_iters)
+    if (ka <= 1 && kb <= 1) CLB_BOTTOM(1, 1);
+    else if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1);
+    else if (ka <= 4 && kb <= 1) CLB_BOTTOM(4, 1);
+    else if (ka <= 4 && kb <= 2) CLB_BOTTOM(4, 2);
+    else CLB_BOTTOM(8, 4);
+#undef CLB_BOTTOM
+    if (check_launch("k_bottom_visit")) return -1;
+    return 1;
+}
+
 // multigrid.py:53-187 w_cycle
 int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int pre, int post, int coarse_iters,
             cudaStream_t s) {
     const LevelView v = level_view(h, level, x, rhs);
     if (level == h->levels - 1) return coarse_solve(v, h->delta, pre + coarse_iters, s);
+    const int bottom = bottom_visit(h, level, pre, post, coarse_iters, s);
+    if (bottom != 0) return bottom < 0 ? 1 : 0;
     if (smooth(v, h->delta, pre, s)) return 1;
     const LevelView c = level_view(h, level + 1, x, rhs);
     const i64 Cc = (i64)c.nx * c.ny * c.nz;
@@ -500,6 +578,20 @@ int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pr
     return w_cycle(h, 0, x, rhs, pre_smooth, post_smooth, coarse_iterations, CLB_STREAM(stream));
 }
 
+int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int iterations, void* stream) {
+    if (check_hierarchy(h)) return 1;
+    CLB_REQUIRE(level >= 0 && level < h->levels, "mg_smooth: level %d outside 0..%d", level, h->levels - 1);
+    CLB_REQUIRE(iterations >= 0, "mg_smooth: negative iterations");
+    CLB_REQUIRE(level > 0 || (x && rhs), "mg_smooth: null level-0 array");
+    return smooth(level_view(h, level, x, rhs), h->delta, iterations, CLB_STREAM(stream));
+}
+
+int clb_mg_set_option(int option, int value) {
+    CLB_REQUIRE(option == 0, "mg_set_option: unknown option %d", option);
+    g_use_bottom = value != 0;
+    return 0;
+}
+
 int clb_mg_residual_partials(int64_t cells) {
     const i64 need = (cells + RN_THREADS - 1) / RN_THREADS;
     const i64 cap = 148 * 8;
@@ -521,6 +613,23 @@ int clb_mg_residual_norms(const void* p, int p_is_double, const float* b, const 
         k_residual_norms<float><<<blocks, RN_THREADS, 0, s>>>((const float*)p, b, op0, inv_delta2, nx, ny, nz, r_out,
                                                               (double2*)partials);
     CLB_LAUNCH_CHECK("k_residual_norms");
+    k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
+    CLB_LAUNCH_CHECK("k_reduce_partials");
+    return 0;
+}
+
+int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const float* b, const uint8_t* op0,
+                   float delta, int nx, int ny, int nz, float* r_out, void* partials, double* out, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(p64_in && e && p64_out && b && op0 && r_out && partials && out, "mg_ir_step: null pointer");
+    CLB_REQUIRE(p64_in != p64_out, "mg_ir_step: p64_out must not alias p64_in");
+    const i64 C = (i64)nx * ny * nz;
+    const int blocks = clb_mg_residual_partials(C);
+    const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
+    cudaStream_t s = CLB_STREAM(stream);
+    k_ir_step<<<blocks, RN_THREADS, 0, s>>>(p64_in, e, p64_out, b, op0, inv_delta2, nx, ny, nz, r_out,
+                                           (double2*)partials);
+    CLB_LAUNCH_CHECK("k_ir_step");
     k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
     return 0;

@@ -8,6 +8,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <atomic>
 #include <stdarg.h>
 #include <stdio.h>
 
@@ -20,13 +21,17 @@ __host__ __device__ __forceinline__ i64 gidx(int i, int j, int k, int ny, int nz
     return ((i64)i * ny + j) * nz + k;
 }
 
-// helper.cl:8-15 grid_coordinates
+// helper.cl:8-15 grid_coordinates. Every grid has fewer than 2^31 cells (checked at each entry
+// point), so the decode uses 32-bit unsigned division.
 __device__ __forceinline__ void gcoord(i64 index, int ny, int nz, int& i, int& j, int& k) {
-    const i64 yz = (i64)ny * nz;
-    i = (int)(index / yz);
-    const i64 rem = index - (i64)i * yz;
-    j = (int)(rem / nz);
-    k = (int)(rem - (i64)j * nz);
+    const uint32_t yz = (uint32_t)ny * (uint32_t)nz;
+    const uint32_t c = (uint32_t)index;
+    const uint32_t ii = c / yz;
+    const uint32_t rem = c - ii * yz;
+    const uint32_t jj = rem / (uint32_t)nz;
+    i = (int)ii;
+    j = (int)jj;
+    k = (int)(rem - jj * (uint32_t)nz);
 }
 
 // helper.cl:21-23 is_interior_cell
@@ -53,7 +58,11 @@ static inline int set_error(const char* fmt, ...) {
     return 1;
 }
 
+// Kernels launched by this library since load (host side; graph replays are not counted).
+static std::atomic<long long> g_launches{0};
+
 static inline int check_launch(const char* what) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error("%s: %s", what, cudaGetErrorString(e));
     return 0;

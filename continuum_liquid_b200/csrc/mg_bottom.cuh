@@ -1,0 +1,223 @@
+// Bottom of the W-cycle in one launch.
+//
+// With L levels the second-coarsest level A = L-2 is visited 2^(L-2) times per W-cycle, and each
+// visit runs (multigrid.py:53-187) pre-smoothing of A, restriction to the coarsest level B, two
+// coarse solves of B (multigrid.py:127-170, 2 + 64 red-black iterations each), prolongation and
+// post-smoothing of A: about 280 dependent red-black phases on a few thousand cells. As separate
+// launches these are bound by launch latency; here one block of 1024 threads runs the whole visit
+// with both levels in shared memory and block barriers between phases.
+//
+// Each thread owns a fixed set of A cells and B cells (interior cells in index order, strided by the
+// block size); the cell index, diagonal and delta^2 * b of each owned cell stay in registers across
+// all sweeps (the neighbour weights are read from shared memory). The update formula and every summation order
+// are those of multigrid.cl (rbgs_step, restrict_residual, prolongate), so the result is identical
+// to the launch-per-kernel W-cycle.
+#pragma once
+#include "multigrid.cuh"
+
+namespace clb {
+
+constexpr int BOTTOM_THREADS = 1024;
+constexpr int BOTTOM_MAX_A = 8;  // A cells per thread
+constexpr int BOTTOM_MAX_B = 4;  // B cells of each colour per B thread
+
+static inline size_t bottom_smem_bytes(int ca, int cb) {
+    // A: p, b, op(float4); B: p, op(float4); each region padded to 16 bytes
+    auto pad = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    return pad((size_t)ca * 4) * 2 + (size_t)ca * 16 + pad((size_t)cb * 4) + (size_t)cb * 16;
+}
+
+// Constants of one owned cell: smem index, diagonal (< 0: not fluid, never updated), delta^2 * b
+// and colour (2 for threads without a cell).
+struct OwnedCell {
+    int c;
+    float d;
+    float d2b;
+    int colour;
+};
+
+__device__ __forceinline__ void owned_cell(int q, int nx, int ny, int nz, const float4* so, bool valid, OwnedCell& o) {
+    const int my = ny - 2, mz = nz - 2;
+    o.d = -1.0f;
+    o.c = 0;
+    o.colour = 2;
+    if (!valid) return;
+    const int i = 1 + q / (my * mz), rem = q % (my * mz), j = 1 + rem / mz, k = 1 + rem % mz;
+    (void)nx;
+    const int sx = ny * nz, sy = nz;
+    const int c = (i * ny + j) * nz + k;
+    o.c = c;
+    o.colour = (i + j + k) & 1;
+    (void)sx;
+    (void)sy;
+    o.d = so[c].x;  // -1 when not fluid
+}
+
+// One red-black update of an owned cell (multigrid.cl:225-229), p and weights in shared memory.
+__device__ __forceinline__ void relax(const OwnedCell& o, float* sp, const float4* so, int sx, int sy) {
+    const int c = o.c;
+    const float4 self = so[c];
+    const float ws = self.y * sp[c + sx] + so[c - sx].y * sp[c - sx] + self.z * sp[c + sy] + so[c - sy].z * sp[c - sy] +
+                     self.w * sp[c + 1] + so[c - 1].w * sp[c - 1];
+    sp[c] = (ws - o.d2b) / o.d;
+}
+
+// The coarsest level B runs on BOTTOM_BTHREADS threads (8 warps) that synchronise with a named
+// barrier: each owns the r-th red and the r-th black interior cell (r = thread, thread + 256, ...), so
+// every thread updates one cell per colour phase. This needs an even interior extent along k (each
+// row then holds the same number of cells of either colour).
+constexpr int BOTTOM_BTHREADS = 256;
+
+__device__ __forceinline__ void bar_b() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+// interior cell of colour `colour` with ordinal r (rows of mz/2 cells of each colour, index order)
+__device__ __forceinline__ int colour_cell(int r, int colour, int ny, int nz) {
+    const int half = (nz - 2) / 2, my = ny - 2;
+    const int row = r / half, m = r - row * half;
+    const int i = 1 + row / my, j = 1 + row % my;
+    const int k = 1 + 2 * m + ((i + j + 1 + colour) & 1);
+    return (i * ny + j) * nz + k;
+}
+
+template <int KA, int KB>
+__global__ void __launch_bounds__(BOTTOM_THREADS, 1)
+    k_bottom_visit(float* __restrict__ pa, const float* __restrict__ ba, const float4* __restrict__ opa,
+                   const uint8_t* __restrict__ ma, int anx, int any, int anz, float* __restrict__ pb,
+                   float* __restrict__ bb, const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx,
+                   int bny, int bnz, float delta, int pre, int post, int coarse_iters) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int CA = anx * any * anz, CB = bnx * bny * bnz;
+    auto pad = [](int x) { return (x + 3) & ~3; };  // in floats
+    float* spa = reinterpret_cast<float*>(smem);
+    float* sba = spa + pad(CA);
+    float4* soa = reinterpret_cast<float4*>(sba + pad(CA));
+    float* spb = reinterpret_cast<float*>(soa + CA);
+    float4* sob = reinterpret_cast<float4*>(spb + pad(CB));
+    const float d2 = delta * delta;
+    const float inv_delta2 = 1.0f / (delta * delta);
+
+    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
+        spa[c] = pa[c];
+        sba[c] = ba[c];
+        float4 o = opa[c];
+        if (!ma[c]) o.x = -1.0f;
+        soa[c] = o;
+    }
+    for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
+        float4 o = opb[c];
+        if (!mb[c]) o.x = -1.0f;
+        sob[c] = o;
+        spb[c] = 0.0f;  // restriction zeroes the coarse pressure (multigrid.cl:114)
+    }
+    __syncthreads();
+
+    const int asx = any * anz, asy = anz, bsx = bny * bnz, bsy = bnz;
+    const int MA = (anx - 2) * (any - 2) * (anz - 2);
+    const int MBC = (bnx - 2) * (bny - 2) * (bnz - 2) / 2;  // cells of each colour on B
+    OwnedCell A[KA];
+#pragma unroll
+    for (int m = 0; m < KA; ++m) {
+        const int q = threadIdx.x + m * BOTTOM_THREADS;
+        owned_cell(q, anx, any, anz, soa, q < MA, A[m]);
+        A[m].d2b = q < MA ? d2 * sba[A[m].c] : 0.0f;
+    }
+    const bool btile = threadIdx.x < BOTTOM_BTHREADS;
+    OwnedCell B[2][KB];  // [colour][m]
+#pragma unroll
+    for (int colour = 0; colour < 2; ++colour)
+#pragma unroll
+        for (int m = 0; m < KB; ++m) {
+            const int r = threadIdx.x + m * BOTTOM_BTHREADS;
+            OwnedCell& o = B[colour][m];
+            o.colour = colour;
+            o.d2b = 0.0f;
+            o.c = 0;
+            o.d = -1.0f;
+            if (btile && r < MBC) {
+                o.c = colour_cell(r, colour, bny, bnz);
+                o.d = sob[o.c].x;
+            }
+        }
+
+    auto smooth_a = [&](int iterations) {
+        for (int it = 0; it < iterations; ++it)
+            for (int parity = 0; parity < 2; ++parity) {
+#pragma unroll
+                for (int m = 0; m < KA; ++m)
+                    if (A[m].colour == parity && A[m].d > 0.0f) relax(A[m], spa, soa, asx, asy);
+                __syncthreads();
+            }
+    };
+
+    smooth_a(pre);
+    // restriction of the residual (multigrid.cl:90-180, right-hand-side part) into B's owners
+    float bvals[2][KB];
+#pragma unroll
+    for (int colour = 0; colour < 2; ++colour)
+#pragma unroll
+        for (int m = 0; m < KB; ++m) {
+            const int r = threadIdx.x + m * BOTTOM_BTHREADS;
+            float rhs = 0.0f;
+            if (btile && r < MBC) {
+                const int c = B[colour][m].c;
+                const int I = c / bsx, J = (c / bsy) % bny, K = c % bnz;
+                const int si = 1 + 2 * (I - 1), sj = 1 + 2 * (J - 1), sk = 1 + 2 * (K - 1);
+                for (int di = 0; di < 2; ++di)
+                    for (int dj = 0; dj < 2; ++dj)
+                        for (int dk = 0; dk < 2; ++dk) {
+                            const int i = si + di, j = sj + dj, k = sk + dk;
+                            if (!interior(i, j, k, anx, any, anz)) continue;
+                            const int f = (i * any + j) * anz + k;
+                            const float4 o = soa[f];
+                            if (o.x < 0.0f) continue;
+                            const float ws = o.y * spa[f + asx] + soa[f - asx].y * spa[f - asx] + o.z * spa[f + asy] +
+                                             soa[f - asy].z * spa[f - asy] + o.w * spa[f + 1] +
+                                             soa[f - 1].w * spa[f - 1];
+                            rhs += sba[f] - (ws - o.x * spa[f]) * inv_delta2;
+                        }
+            }
+            bvals[colour][m] = rhs;
+            B[colour][m].d2b = d2 * rhs;
+        }
+    if (btile) {
+        // two coarse solves of the W (multigrid.py:127-170), pre + coarse_iters iterations each
+        const int iterations = 2 * (pre + coarse_iters);
+        for (int it = 0; it < iterations; ++it)
+#pragma unroll
+            for (int colour = 0; colour < 2; ++colour) {
+#pragma unroll
+                for (int m = 0; m < KB; ++m)
+                    if (B[colour][m].d > 0.0f) relax(B[colour][m], spb, sob, bsx, bsy);
+                bar_b();
+            }
+    }
+    __syncthreads();
+    // prolongation (multigrid.cl:182-201)
+#pragma unroll
+    for (int m = 0; m < KA; ++m) {
+        if (A[m].d < 0.0f) continue;  // interior fluid cells only
+        const int c = A[m].c;
+        const int i = c / asx, j = (c / asy) % any, k = c % anz;
+        const int I = min((i - 1) / 2 + 1, bnx - 2), J = min((j - 1) / 2 + 1, bny - 2),
+                  K = min((k - 1) / 2 + 1, bnz - 2);
+        spa[c] += spb[(I * bny + J) * bnz + K];
+    }
+    __syncthreads();
+    smooth_a(post);
+
+    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) pa[c] = spa[c];
+    for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
+        pb[c] = spb[c];
+        const int I = c / bsx, J = (c / bsy) % bny, K = c % bnz;
+        if (!interior(I, J, K, bnx, bny, bnz)) bb[c] = 0.0f;  // multigrid.cl:115
+    }
+#pragma unroll
+    for (int colour = 0; colour < 2; ++colour)
+#pragma unroll
+        for (int m = 0; m < KB; ++m) {
+            const int r = threadIdx.x + m * BOTTOM_BTHREADS;
+            if (btile && r < MBC) bb[B[colour][m].c] = bvals[colour][m];
+        }
+}
+
+}  // namespace clb

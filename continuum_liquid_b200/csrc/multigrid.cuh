@@ -497,6 +497,56 @@ __global__ void __launch_bounds__(RN_THREADS) k_residual_norms(const PT* __restr
     }
 }
 
+// Refinement step fused with the next residual: p_out = p_in + e at every cell and, at interior
+// fluid cells, r = b - A p_out in FP64 (neighbour values formed as p_in + e on the fly, so p_out
+// must not alias p_in), r rounded to float into r_out, with the block partials of r^2 and b^2.
+__global__ void __launch_bounds__(RN_THREADS) k_ir_step(const double* __restrict__ p_in, const float* __restrict__ e,
+                                                         double* __restrict__ p_out, const float* __restrict__ b,
+                                                         const uint8_t* __restrict__ op0, double inv_delta2, int nx,
+                                                         int ny, int nz, float* __restrict__ r_out,
+                                                         double2* __restrict__ partials) {
+    __shared__ double2 s_red[RN_THREADS / 32];
+    const i64 C = (i64)nx * ny * nz;
+    const i64 sx = (i64)ny * nz, sy = nz;
+    double rr = 0.0, bb = 0.0;
+    for (i64 c = (i64)blockIdx.x * RN_THREADS + threadIdx.x; c < C; c += (i64)gridDim.x * RN_THREADS) {
+        int i, j, k;
+        gcoord(c, ny, nz, i, j, k);
+        const double pc = __ldg(p_in + c) + (double)__ldg(e + c);
+        p_out[c] = pc;
+        const uint32_t o = __ldg(op0 + c);
+        float rf = 0.0f;
+        if (interior(i, j, k, nx, ny, nz) && (o & 64u)) {
+            auto pv = [&](i64 q) { return __ldg(p_in + q) + (double)__ldg(e + q); };
+            const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
+            const double ws = (double)bitf(o, 3) * pv(c + sx) + (double)bitf(ox, 3) * pv(c - sx) +
+                              (double)bitf(o, 4) * pv(c + sy) + (double)bitf(oy, 4) * pv(c - sy) +
+                              (double)bitf(o, 5) * pv(c + 1) + (double)bitf(oz, 5) * pv(c - 1);
+            const double bv = (double)__ldg(b + c);
+            const double r = bv - (ws - (double)(o & 7u) * pc) * inv_delta2;
+            rr += r * r;
+            bb += bv * bv;
+            rf = (float)r;
+        }
+        r_out[c] = rf;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rr += __shfl_xor_sync(0xffffffffu, rr, o);
+        bb += __shfl_xor_sync(0xffffffffu, bb, o);
+    }
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = make_double2(rr, bb);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 t = s_red[0];
+        for (int q = 1; q < RN_THREADS / 32; ++q) {
+            t.x += s_red[q].x;
+            t.y += s_red[q].y;
+        }
+        partials[blockIdx.x] = t;
+    }
+}
+
 // Fixed-order reduction of the block partials (deterministic for a given grid size).
 __global__ void k_reduce_partials(const double2* __restrict__ partials, int count, double2* __restrict__ out) {
     __shared__ double2 s[256];

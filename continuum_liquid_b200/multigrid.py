@@ -122,7 +122,7 @@ class MultigridHierarchy:
     float32 [..., 4] tensor). ``shapes[l]`` includes the ghost layer, as in the reference.
     """
 
-    def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8):
+    def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, fused_min_cells: int = 20**3):
         self.kernels = kernels
         self.grid_shape = tuple(int(s) for s in grid_shape)
         self.dx = float(dx)
@@ -153,6 +153,14 @@ class MultigridHierarchy:
             self.struct.b[l] = self.b[l].data_ptr()
             self.struct.mask[l] = self.mask[l].data_ptr()
             self.struct.op[l] = self.op[l].data_ptr()
+        # second buffers for the fused red-black iteration on every level of at least fused_min_cells
+        # cells (smaller levels are served by the single-block bottom visit or two-launch sweeps)
+        self.alt: list[torch.Tensor | None] = []
+        for l, shape in enumerate(self.shapes):
+            big = int(np.prod(shape)) >= fused_min_cells
+            self.alt.append(torch.zeros(shape, dtype=torch.float32, device=device) if big else None)
+            if big:
+                self.struct.alt[l] = self.alt[l].data_ptr()
         cells = int(np.prod(self.grid_shape))
         self.partials = torch.zeros((kernels.residual_partials(cells), 2), dtype=torch.float64, device=device)
         self.norms = torch.zeros(2, dtype=torch.float64, device=device)
@@ -165,7 +173,7 @@ class MultigridHierarchy:
         """pressure_rhs + build_finest_operator (pressure_solve.py:35-59) into rhs and op0."""
         u, v, w = velocity
         self.kernels.call("clb_mg_rhs_operator", u, v, w, fluid_fraction, rhs, self.op0,
-                          float(FIELD_DTYPE(rho / dt)), float(FIELD_DTYPE(1.0 / self.dx)), *self.grid_shape,
+                          float(FIELD_DTYPE(float(rho) / float(dt))), float(FIELD_DTYPE(1.0 / self.dx)), *self.grid_shape,
                           stream=queue)
 
     def build_coarse(self, queue=None) -> None:
@@ -177,6 +185,10 @@ class MultigridHierarchy:
         """One W-cycle on level-0 unknown ``x`` and right-hand side ``rhs``."""
         self.kernels.call_hierarchy("clb_mg_w_cycle", self.struct, x, rhs, int(pre_smooth), int(post_smooth),
                                     int(coarse_iterations), stream=queue)
+
+    def smooth(self, level: int, iterations: int, x=None, rhs=None, queue=None) -> None:
+        """``iterations`` red-black Gauss-Seidel iterations on one level."""
+        self.kernels.call_hierarchy("clb_mg_smooth", self.struct, int(level), x, rhs, int(iterations), stream=queue)
 
     def residual_norms(self, p, rhs, r_out=None, queue=None) -> torch.Tensor:
         """Device tensor [sum r^2, sum b^2] (FP64) over interior fluid cells of level 0."""

@@ -68,7 +68,7 @@ def count_particles_per_cell(kernels: Backend, queue, particles, bin_counts, par
     """particles.cl:44-59 (accumulates into bin_counts; zero-fill first as particles.py:146 does)."""
     nx, ny, nz = grid_shape
     kernels.call("clb_count_particles_per_cell", particles, bin_counts, keys, ranks, int(particle_count_total),
-                 float(FIELD_DTYPE(1.0 / dx)), nx, ny, nz, stream=queue)
+                 float(FIELD_DTYPE(1.0 / float(dx))), nx, ny, nz, stream=queue)
     return bin_counts
 
 
@@ -94,7 +94,7 @@ def particle_to_grid_gather(kernels: Backend, queue, particles, particle_velocit
     nx, ny, nz = grid_shape
     u, v, w = velocity
     kernels.call("clb_particle_to_grid_gather", particles, particle_velocity, bin_offsets, bin_counts, u, v, w,
-                 fluid_fraction, float(FIELD_DTYPE(1.0 / dx)), float(FIELD_DTYPE(1.0 / particles_per_cell)), nx, ny,
+                 fluid_fraction, float(FIELD_DTYPE(1.0 / float(dx))), float(FIELD_DTYPE(1.0 / particles_per_cell)), nx, ny,
                  nz, stream=queue)
 
 
@@ -142,7 +142,7 @@ def particle_to_grid(
         scratch.scan,
         int(scratch.scan.numel()),
         int(particle_count_total),
-        float(FIELD_DTYPE(1.0 / dx)),
+        float(FIELD_DTYPE(1.0 / float(dx))),
         float(FIELD_DTYPE(1.0 / particles_per_cell)),
         nx,
         ny,
@@ -161,7 +161,7 @@ def grid_to_particle(kernels: Backend, queue, particle_velocity, particles, velo
     u, v, w = velocity
     ou, ov, ow = old_velocity
     kernels.call("clb_grid_to_particle", particle_velocity, particles, u, v, w, ou, ov, ow, int(particle_count_total),
-                 float(FIELD_DTYPE(1.0 / dx)), nx, ny, nz, float(FIELD_DTYPE(flip_ratio)), stream=queue)
+                 float(FIELD_DTYPE(1.0 / float(dx))), nx, ny, nz, float(FIELD_DTYPE(flip_ratio)), stream=queue)
     return particle_velocity
 
 
@@ -195,16 +195,16 @@ def particle_update(kernels: Backend, queue, particles, particle_velocity, veloc
         ow,
         obstacle,
         int(particle_count_total),
-        float(FIELD_DTYPE(1.0 / dx)),
+        float(FIELD_DTYPE(1.0 / float(dx))),
         nx,
         ny,
         nz,
         float(FIELD_DTYPE(flip_ratio)),
         float(FIELD_DTYPE(dt)),
-        float(FIELD_DTYPE(1.001 * dx)),
-        float(FIELD_DTYPE((grid_shape[0] - 1.001) * dx)),
-        float(FIELD_DTYPE((grid_shape[1] - 1.001) * dx)),
-        float(FIELD_DTYPE((grid_shape[2] - 1.001) * dx)),
+        float(FIELD_DTYPE(1.001 * float(dx))),
+        float(FIELD_DTYPE((grid_shape[0] - 1.001) * float(dx))),
+        float(FIELD_DTYPE((grid_shape[1] - 1.001) * float(dx))),
+        float(FIELD_DTYPE((grid_shape[2] - 1.001) * float(dx))),
         stream=queue,
     )
     return particles, particle_velocity

@@ -35,8 +35,8 @@ def pressure_solve(kernels: Backend, multigrid_kernels, boundary_kernels, queue,
     """pressure_solve.py:10-85 on the reference layout (one kernel per reference kernel)."""
     nx, ny, nz = grid_shape
     u, v, w = velocity
-    kernels.call("clb_pressure_rhs", u, v, w, fluid_fraction, rhs, float(FIELD_DTYPE(rho / dt)),
-                 float(FIELD_DTYPE(1.0 / dx)), nx, ny, nz, stream=queue)
+    kernels.call("clb_pressure_rhs", u, v, w, fluid_fraction, rhs, float(FIELD_DTYPE(float(rho) / float(dt))),
+                 float(FIELD_DTYPE(1.0 / float(dx))), nx, ny, nz, stream=queue)
     kernels.call("clb_build_finest_operator", fluid_fraction, *operator_level0, nx, ny, nz, stream=queue)
     for _ in range(num_vcycles):
         multigrid.w_cycle(kernels, queue, 0, p_levels, b_levels, mask_levels, operator_levels, pressure, rhs,
@@ -50,8 +50,8 @@ def pressure_correction(kernels: Backend, queue, velocity, pressure, dx, dt, rho
     """pressure_solve.py:88-114."""
     nx, ny, nz = grid_shape
     u, v, w = velocity
-    kernels.call("clb_pressure_correction", u, v, w, pressure, float(FIELD_DTYPE(dt / rho)),
-                 float(FIELD_DTYPE(1.0 / dx)), nx, ny, nz, stream=queue)
+    kernels.call("clb_pressure_correction", u, v, w, pressure, float(FIELD_DTYPE(float(dt) / float(rho))),
+                 float(FIELD_DTYPE(1.0 / float(dx))), nx, ny, nz, stream=queue)
     return velocity
 
 
@@ -68,7 +68,14 @@ class SolveStats:
 
 
 class PressureSolver:
-    """Packed-layout pressure solve for one grid (allocates its workspace once)."""
+    """Packed-layout pressure solve for one grid (allocates its workspace once).
+
+    In tolerance mode one refinement is: e = 0; one W-cycle on A e = r; p64 <- p64 + e fused with
+    the FP64 residual r = b - A p64 and its norms (clb_mg_ir_step). The FP64 pressure alternates
+    between two buffers, so two CUDA graphs (one per direction) capture the refinement. The host
+    reads the residual norm only when the refinement count predicted from the observed contraction
+    rate has run, so most refinements are replayed back to back without a host round trip.
+    """
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100):
         self.kernels = kernels
@@ -81,9 +88,12 @@ class PressureSolver:
         self.rhs = torch.zeros(self.grid_shape, dtype=torch.float32, device=device)
         self.residual = torch.zeros(self.grid_shape, dtype=torch.float32, device=device)
         self.correction = torch.zeros(self.grid_shape, dtype=torch.float32, device=device)
-        self.p64 = torch.zeros(self.grid_shape, dtype=torch.float64, device=device)
+        self.p64 = [torch.zeros(self.grid_shape, dtype=torch.float64, device=device) for _ in range(2)]
+        self.cur = 0  # index of the FP64 buffer holding the current pressure
         self.norms_host = torch.zeros(2, dtype=torch.float64, pin_memory=True)
-        self._refine_graph: torch.cuda.CUDAGraph | None = None
+        self._graphs: list[torch.cuda.CUDAGraph | None] = [None, None]
+        self.graph_replays = 0  # refinement-graph replays so far
+        self.graph_launches = 0  # kernels inside one refinement graph
 
     # -- pieces ---------------------------------------------------------------------------------
     def prepare(self, velocity, fluid_fraction, dt, rho, queue=None) -> None:
@@ -101,29 +111,37 @@ class PressureSolver:
         """FP64 ||b - A p|| / ||b|| of a float32 or float64 pressure against the prepared system."""
         return self._relative(self.hierarchy.residual_norms(pressure, self.rhs, queue=queue))
 
-    def refine_once(self, queue=None) -> None:
-        """One refinement: e = W-cycle(0, r); p64 += e; r = b - A p64 (FP64) and its norms."""
+    def refine_once(self, src: int, queue=None) -> None:
+        """One refinement from FP64 buffer ``src`` into the other one."""
         h = self.hierarchy
         self.correction.zero_()
         h.w_cycle(self.correction, self.residual, queue=queue)
-        self.kernels.call("clb_mg_ir_update", self.p64, self.correction, self.cells, stream=queue)
-        h.residual_norms(self.p64, self.rhs, r_out=self.residual, queue=queue)
+        self.kernels.call("clb_mg_ir_step", self.p64[src], self.correction, self.p64[1 - src], self.rhs, h.op0,
+                          float(FIELD_DTYPE(self.dx)), *self.grid_shape, self.residual, h.partials, h.norms,
+                          stream=queue)
 
     def _refine(self, use_graph: bool) -> None:
+        src = self.cur
         if not use_graph:
-            self.refine_once()
-            return
-        if self._refine_graph is None:
-            side = torch.cuda.Stream(self.kernels.device)
-            side.wait_stream(torch.cuda.current_stream(self.kernels.device))
-            with torch.cuda.stream(side):
-                self.refine_once()  # warm-up outside capture
-            torch.cuda.current_stream(self.kernels.device).wait_stream(side)
-            graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph):
-                self.refine_once()
-            self._refine_graph = graph
-        self._refine_graph.replay()
+            self.refine_once(src)
+        else:
+            if self._graphs[src] is None:
+                stream = torch.cuda.current_stream(self.kernels.device)
+                side = torch.cuda.Stream(self.kernels.device)
+                side.wait_stream(stream)
+                with torch.cuda.stream(side):
+                    self.refine_once(src)  # warm-up outside capture (the result is recomputed below)
+                stream.wait_stream(side)
+                graph = torch.cuda.CUDAGraph()
+                before = self.kernels.launch_count()
+                with torch.cuda.graph(graph):
+                    self.refine_once(src)
+                # +1: the correction zero-fill is a torch kernel captured with ours
+                self.graph_launches = self.kernels.launch_count() - before + 1
+                self._graphs[src] = graph
+            self._graphs[src].replay()
+            self.graph_replays += 1
+        self.cur = 1 - src
 
     # -- solves ---------------------------------------------------------------------------------
     def solve(self, velocity, fluid_fraction, pressure, dt, rho, num_vcycles: int = 1, tol: float | None = None,
@@ -141,17 +159,27 @@ class PressureSolver:
             if measure:
                 stats.rel_residual = self.relative_residual(pressure)
         else:
-            self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64, *self.grid_shape)
-            rel = self._relative(h.residual_norms(self.p64, self.rhs, r_out=self.residual))
+            self.cur = 0
+            self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64[0], *self.grid_shape)
+            rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
             stats.initial_rel_residual = rel
             stats.history.append(rel)
+            rate = None
             while rel > tol and stats.cycles < self.max_cycles:
-                self._refine(use_graph)
-                stats.cycles += 1
+                # refinements to run before the next host check: one less than predicted, at least 1
+                batch = 1
+                if rate is not None and 0.0 < rate < 1.0:
+                    batch = max(1, int(math.ceil(math.log(tol / rel) / math.log(rate))) - 1)
+                batch = min(batch, self.max_cycles - stats.cycles, 8)
+                for _ in range(batch):
+                    self._refine(use_graph)
+                previous = rel
+                stats.cycles += batch
                 rel = self._relative(h.norms)
                 stats.history.append(rel)
+                rate = (rel / previous) ** (1.0 / batch) if previous > 0 and stats.cycles > 1 else None
             stats.rel_residual = rel
-            self.kernels.call("clb_mg_ir_store", self.p64, pressure, self.cells)
+            self.kernels.call("clb_mg_ir_store", self.p64[self.cur], pressure, self.cells)
         boundary_conditions.neumann_domain_bc(self.kernels, None, pressure, self.grid_shape)
         stats.ms = (time.perf_counter() - t0) * 1e3
         return stats

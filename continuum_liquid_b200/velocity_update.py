@@ -32,7 +32,7 @@ def update_velocity(kernels: Backend, queue, velocity, result, fluid_fraction, g
         float(FIELD_DTYPE(fz)),
         float(FIELD_DTYPE(rho)),
         float(FIELD_DTYPE(nu)),
-        float(FIELD_DTYPE(1.0 / (dx * dx))),
+        float(FIELD_DTYPE(1.0 / (float(dx) * float(dx)))),
         float(FIELD_DTYPE(dt)),
         nx,
         ny,

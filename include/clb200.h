@@ -36,6 +36,9 @@ const char* clb_last_error(void);
 int clb_device_error(uint32_t* code);
 /* ABI version of this header (bumped on any signature change). */
 int clb_abi_version(void);
+/* Number of kernels this library has launched directly since it was loaded (replays of captured
+ * CUDA graphs are not included). Host-side counter for launch accounting. */
+int64_t clb_launch_count(void);
 
 /* ---- particles: binning, scan, sort, P2G (Solver/Kernel/particles.py, OpenCL/particles.cl) -- */
 
@@ -173,6 +176,9 @@ typedef struct clb_mg_hierarchy {
     float* b[CLB_MG_MAX_LEVELS];         /* [0] unused: level-0 rhs is passed per call */
     uint8_t* mask[CLB_MG_MAX_LEVELS];    /* [0] unused */
     void* op[CLB_MG_MAX_LEVELS];         /* [0] unused; float4 per cell */
+    float* alt[CLB_MG_MAX_LEVELS];       /* optional second buffer per level (level 0 included): when
+                                            set, each red-black iteration is one fused launch that
+                                            writes the other buffer; NULL: two launches in place */
 } clb_mg_hierarchy;
 
 /* pressure_solve.cl:3-24 pressure_rhs fused with multigrid.cl:63-88 build_finest_operator, writing
@@ -187,6 +193,16 @@ int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream);
  * as pressure_solve.py:61-83: 2, 4, 64). */
 int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pre_smooth, int post_smooth,
                    int coarse_iterations, void* stream);
+
+/* multigrid.py:190-220 smooth: `iterations` red-black Gauss-Seidel iterations on one level (level 0
+ * uses x and rhs; coarse levels their own p and b). */
+int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int iterations, void* stream);
+
+/* Process-wide multigrid options (host-side switches, no device work):
+ *  option 0: 1 (default) runs each visit of the second-coarsest level, including both coarse solves,
+ *            as one single-block launch from shared memory; 0 launches one kernel per sweep as the
+ *            reference does. Both give identical results. */
+int clb_mg_set_option(int option, int value);
 
 /* Block-partial count used by clb_mg_residual_norms for a grid of `cells` cells. */
 int clb_mg_residual_partials(int64_t cells);
@@ -203,6 +219,10 @@ int clb_mg_residual_norms(const void* p, int p_is_double, const float* b, const 
  *  update: p64 += e
  *  store:  p32 = (float) p64 */
 int clb_mg_ir_init(const float* p32, const uint8_t* op0, double* p64, int nx, int ny, int nz, void* stream);
+/* One refinement update fused with the next residual: p64_out = p64_in + e, r_out = b - A p64_out
+ * (FP64, rounded to float), out = [sum r^2, sum b^2]; p64_out must not alias p64_in. */
+int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const float* b, const uint8_t* op0,
+                   float delta, int nx, int ny, int nz, float* r_out, void* partials, double* out, void* stream);
 int clb_mg_ir_update(double* p64, const float* e, int64_t cells, void* stream);
 int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream);
 

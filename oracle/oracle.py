@@ -95,13 +95,13 @@ def c(a, dtype=np.float32):
 # ---- particles ---------------------------------------------------------------------------------
 def bin_keys(pos, dx, shape):
     keys = np.zeros(len(pos), np.int32)
-    lib().orc_bin_keys(c(pos), keys, len(pos), F32(1.0 / dx), *shape)
+    lib().orc_bin_keys(c(pos), keys, len(pos), F32(1.0 / float(dx)), *shape)
     return keys
 
 
 def count_particles(pos, dx, shape):
     counts = np.zeros(int(np.prod(shape)), np.int32)
-    lib().orc_count_particles_per_cell(c(pos), counts, len(pos), F32(1.0 / dx), *shape)
+    lib().orc_count_particles_per_cell(c(pos), counts, len(pos), F32(1.0 / float(dx)), *shape)
     return counts
 
 
@@ -116,7 +116,7 @@ def exclusive_scan(values, L=256):
 def sort_particles(pos, vel, offsets, dx, shape):
     pos_s, vel_s = np.zeros_like(c(pos)), np.zeros_like(c(vel))
     cursors = np.zeros(int(np.prod(shape)), np.int32)
-    lib().orc_sort_particles(c(pos), c(vel), pos_s, vel_s, c(offsets, np.int32), cursors, len(pos), F32(1.0 / dx),
+    lib().orc_sort_particles(c(pos), c(vel), pos_s, vel_s, c(offsets, np.int32), cursors, len(pos), F32(1.0 / float(dx)),
                              *shape)
     return pos_s, vel_s, cursors
 
@@ -125,7 +125,7 @@ def p2g_gather(pos_sorted, vel_sorted, offsets, counts, dx, shape, ppc=8, lanes=
     C = int(np.prod(shape))
     u, v, w, ff = (np.zeros(C, np.float32) for _ in range(4))
     lib().orc_particle_to_grid_gather(c(pos_sorted), c(vel_sorted), c(offsets, np.int32), c(counts, np.int32), u, v, w,
-                                      ff, F32(1.0 / dx), F32(1.0 / ppc), *shape, lanes)
+                                      ff, F32(1.0 / float(dx)), F32(1.0 / ppc), *shape, lanes)
     return tuple(a.reshape(shape) for a in (u, v, w, ff))
 
 
@@ -140,7 +140,7 @@ def particle_to_grid(pos, vel, dx, shape, ppc=8):
 
 def grid_to_particle(vel, pos, cur, old, dx, shape, flip_ratio=1.0):
     vel = c(vel).copy()
-    lib().orc_grid_to_particle(vel, c(pos), *(c(a) for a in cur), *(c(a) for a in old), len(pos), F32(1.0 / dx),
+    lib().orc_grid_to_particle(vel, c(pos), *(c(a) for a in cur), *(c(a) for a in old), len(pos), F32(1.0 / float(dx)),
                                *shape, F32(flip_ratio))
     return vel
 
@@ -153,14 +153,14 @@ def advect(pos, vel, dt):
 
 def particle_domain_bc(pos, vel, dx, shape):
     pos, vel = c(pos).copy(), c(vel).copy()
-    lib().orc_particle_domain_bc(pos, vel, len(pos), F32(1.001 * dx), F32((shape[0] - 1.001) * dx),
-                                 F32((shape[1] - 1.001) * dx), F32((shape[2] - 1.001) * dx))
+    lib().orc_particle_domain_bc(pos, vel, len(pos), F32(1.001 * float(dx)), F32((shape[0] - 1.001) * float(dx)),
+                                 F32((shape[1] - 1.001) * float(dx)), F32((shape[2] - 1.001) * float(dx)))
     return pos, vel
 
 
 def particle_obstacle_bc(pos, prev, vel, obstacle, dx, shape):
     pos, vel = c(pos).copy(), c(vel).copy()
-    lib().orc_particle_obstacle_bc(pos, c(prev), vel, c(obstacle, np.uint8), len(pos), F32(1.0 / dx), *shape)
+    lib().orc_particle_obstacle_bc(pos, c(prev), vel, c(obstacle, np.uint8), len(pos), F32(1.0 / float(dx)), *shape)
     return pos, vel
 
 
@@ -183,7 +183,7 @@ def voxelise(triangles, shape, delta, origin, mask=None):
 def update_velocity(u, v, w, ff, gravity, force, rho, nu, dx, dt, shape):
     out = [np.zeros(shape, np.float32) for _ in range(3)]
     lib().orc_update_velocity(c(u), c(v), c(w), *out, c(ff), F32(gravity[0]), F32(gravity[1]), F32(gravity[2]),
-                              F32(force[0]), F32(force[1]), F32(force[2]), F32(rho), F32(nu), F32(1.0 / (dx * dx)),
+                              F32(force[0]), F32(force[1]), F32(force[2]), F32(rho), F32(nu), F32(1.0 / (float(dx) * float(dx))),
                               F32(dt), *shape)
     return out
 
@@ -205,13 +205,13 @@ def grid_obstacle_bc(u, v, w, ff, obstacle, shape):
 
 def pressure_rhs(u, v, w, ff, dx, dt, rho, shape):
     rhs = np.zeros(shape, np.float32)
-    lib().orc_pressure_rhs(c(u), c(v), c(w), c(ff), rhs, F32(rho / dt), F32(1.0 / dx), *shape)
+    lib().orc_pressure_rhs(c(u), c(v), c(w), c(ff), rhs, F32(float(rho) / float(dt)), F32(1.0 / float(dx)), *shape)
     return rhs
 
 
 def pressure_correction(u, v, w, p, dx, dt, rho, shape):
     u, v, w = c(u).copy(), c(v).copy(), c(w).copy()
-    lib().orc_pressure_correction(u, v, w, c(p), F32(dt / rho), F32(1.0 / dx), *shape)
+    lib().orc_pressure_correction(u, v, w, c(p), F32(float(dt) / float(rho)), F32(1.0 / float(dx)), *shape)
     return u, v, w
 
 
@@ -303,7 +303,7 @@ def pressure_solve(u, v, w, ff, pressure, dx, dt, rho, num_vcycles, shape, level
     op0 = build_finest_operator(ff, shape)
     p = c(pressure).copy()
     for _ in range(num_vcycles):
-        levels.w_cycle(p, rhs, c(ff), op0, dx)
+        levels.w_cycle(p, rhs, c(ff), op0, F32(float(dx)))
     return neumann_domain_bc(p, shape), rhs, op0
 
 

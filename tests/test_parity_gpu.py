@@ -222,7 +222,7 @@ def test_grid_kernels(backend, oracle, case):
         assert np.array_equal(host(a), b)
     # pressure_rhs / pressure_correction / neumann
     rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
-    backend.call("clb_pressure_rhs", dev(u), dev(v), dev(w), dev(ff), rhs, float(F32(rho / dt)), float(F32(1 / dx)),
+    backend.call("clb_pressure_rhs", dev(u), dev(v), dev(w), dev(ff), rhs, float(F32(rho / dt)), float(F32(1.0 / float(dx))),
                  *shape)
     assert np.array_equal(host(rhs), oracle.pressure_rhs(u, v, w, ff, dx, dt, rho, shape))
     U, Vv, W = dev(u), dev(v), dev(w)
@@ -336,7 +336,8 @@ def test_packed_w_cycle_equals_reference(backend, oracle, shape):
         assert np.array_equal(arr["mask"].astype(F32), levels.m[lvl])
     # FP64 residual norms
     norms = host(h.residual_norms(P, rhs))
-    rr, bb = oracle.residual_norms(q, orhs, ff, oops, dx)
+    f64 = lambda a: np.asarray(a, np.float64)  # noqa: E731 - the GPU evaluates the residual in FP64
+    rr, bb = oracle.residual_norms(f64(q), f64(orhs), f64(ff), [f64(a) for a in oops], float(dx))
     assert norms[0] == pytest.approx(rr, rel=1e-12) and norms[1] == pytest.approx(bb, rel=1e-12)
 
 
@@ -410,3 +411,48 @@ def test_bad_arguments_raise(backend):
         backend.call("clb_grid_domain_bc", t, t, t, 2, 2, 2)
     with pytest.raises(RuntimeError, match="parity"):
         backend.call("clb_rbgs_step", t, t, t, t, t, t, t, 1.0, 3, 4, 4, 4)
+
+
+@pytest.mark.parametrize("bottom", [1, 0])
+@pytest.mark.parametrize("shape", [(66, 66, 66), (34, 40, 30)])
+def test_w_cycle_paths_agree(backend, oracle, shape, bottom):
+    """The single-block bottom visit and the fused red-black iterations give the reference values."""
+    dx = F32(1.0 / shape[0])
+    ff, b, p0 = random_system(shape, 21)
+    backend.lib.clb_mg_set_option(0, bottom)
+    try:
+        h = multigrid.MultigridHierarchy(backend, shape, float(dx))
+        h.op0.copy_(torch.zeros_like(h.op0))
+        u, v, w = (np.random.default_rng(22 + a).standard_normal(shape).astype(F32) for a in range(3))
+        rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+        h.rhs_operator((dev(u), dev(v), dev(w)), dev(ff), rhs, 1.0 / 240.0, 1000.0)
+        h.build_coarse()
+        P = dev(p0)
+        h.w_cycle(P, rhs)
+        levels = oracle.Levels(shape)
+        q = p0.copy()
+        orhs = oracle.pressure_rhs(u, v, w, ff, dx, 1.0 / 240.0, 1000.0, shape)
+        levels.w_cycle(q, orhs, ff, oracle.build_finest_operator(ff, shape), dx)
+        assert np.array_equal(host(P), q)
+    finally:
+        backend.lib.clb_mg_set_option(0, 1)
+
+
+@pytest.mark.parametrize("iterations", [1, 3])
+def test_fused_smoothing_odd_iterations(backend, oracle, iterations):
+    shape, dx = (40, 36, 44), F32(1.0 / 40)
+    ff, b, p0 = random_system(shape, 23)
+    h = multigrid.MultigridHierarchy(backend, shape, float(dx))
+    u, v, w = (np.random.default_rng(24 + a).standard_normal(shape).astype(F32) for a in range(3))
+    rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    h.rhs_operator((dev(u), dev(v), dev(w)), dev(ff), rhs, 1.0 / 240.0, 1000.0)
+    assert h.alt[0] is not None
+    P = dev(p0)
+    h.smooth(0, iterations, P, rhs)
+    orhs = oracle.pressure_rhs(u, v, w, ff, dx, 1.0 / 240.0, 1000.0, shape)
+    oops = oracle.build_finest_operator(ff, shape)
+    q = p0.copy()
+    for _ in range(iterations):
+        for parity in (0, 1):
+            oracle.lib().orc_rbgs_step_f32(q, orhs, ff, *oops, dx, parity, *shape)
+    assert np.array_equal(host(P), q)
