@@ -37,6 +37,7 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_count_particles_per_cell": [P, P, P, P, L, F, I, I, I, P],
     "clb_scan_scratch_bytes": [L],
     "clb_exclusive_prefix_sum": [P, P, P, L, P, L, P],
+    "clb_exclusive_prefix_sum_static": [P, P, P, L, P],
     "clb_sort_particles": [P, P, P, P, P, P, P, P, P, P, L, P],
     "clb_particle_to_grid_gather": [P, P, P, P, P, P, P, P, F, F, I, I, I, P],
     "clb_particle_to_grid": [P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, L, L, F, F, I, I, I, P],

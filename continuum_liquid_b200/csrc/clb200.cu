@@ -9,6 +9,8 @@
 #include "mg_sweep.cuh"
 #include "voxelise.cuh"
 
+#include <mutex>
+
 using namespace clb;
 
 #define CLB_STREAM(s) (reinterpret_cast<cudaStream_t>(s))
@@ -89,6 +91,49 @@ int clb_exclusive_prefix_sum(const int32_t* values, int32_t* output, int32_t* to
     CLB_REQUIRE(count >= 0, "exclusive_prefix_sum: negative count");
     CLB_REQUIRE(count == 0 || (values && output), "exclusive_prefix_sum: null pointer");
     return launch_scan(values, output, count, scratch, scratch_bytes, total, CLB_STREAM(stream));
+}
+
+// ---- exclusive scan with library-owned scratch --------------------------------------------------
+// Some callers cannot allocate device memory: a host application that has handed the whole device
+// memory budget to its own pool, or code that must not add the device-wide synchronisation that
+// cudaMalloc/cudaFree imply in the middle of asynchronous work. For them this variant keeps the
+// scan's look-back state (a 16-byte ticket header and one 8-byte status word per 4096-element tile)
+// in a fixed array compiled into the library, sized for CLB_SCAN_STATIC_MAX_COUNT elements:
+// 16 + 8 * 16384 bytes, held on every GPU that loads the library until the process exits.
+//
+// In host code the array's name only stands for it; its device address is obtained once per device
+// with cudaGetSymbolAddress, on the first call made while that device is current.
+static constexpr i64 kScanStaticTiles = (CLB_SCAN_STATIC_MAX_COUNT + SCAN_TILE - 1) / SCAN_TILE;
+static __device__ __align__(256) unsigned char g_scan_static_scratch[16 + 8 * kScanStaticTiles];
+static std::mutex g_scan_static_mutex;
+static void* g_scan_static_address[256] = {};  // per device ordinal
+
+int clb_exclusive_prefix_sum_static(const int32_t* values, int32_t* output, int32_t* total, int64_t count,
+                                    void* stream) {
+    CLB_REQUIRE(count >= 0, "exclusive_prefix_sum_static: negative count");
+    CLB_REQUIRE(count <= CLB_SCAN_STATIC_MAX_COUNT,
+                "exclusive_prefix_sum_static: %lld elements exceed the fixed scratch limit of %lld elements; "
+                "use clb_exclusive_prefix_sum with caller-provided scratch",
+                (long long)count, (long long)CLB_SCAN_STATIC_MAX_COUNT);
+    CLB_REQUIRE(count == 0 || (values && output), "exclusive_prefix_sum_static: null pointer");
+    int device = 0;
+    if (check_call(cudaGetDevice(&device), "exclusive_prefix_sum_static: cudaGetDevice")) return 1;
+    CLB_REQUIRE(device >= 0 && device < 256, "exclusive_prefix_sum_static: device ordinal %d out of range", device);
+    void* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scan_static_mutex);
+        if (g_scan_static_address[device] == nullptr) {
+            void* address = nullptr;
+            if (check_call(cudaGetSymbolAddress(&address, g_scan_static_scratch),
+                           "exclusive_prefix_sum_static: cudaGetSymbolAddress"))
+                return 1;
+            g_scan_static_address[device] = address;
+        }
+        scratch = g_scan_static_address[device];
+    }
+    // launch_scan clears the ticket and the status words this count uses before the scan runs
+    return launch_scan(values, output, count, scratch, (i64)sizeof(g_scan_static_scratch), total,
+                       CLB_STREAM(stream));
 }
 
 int clb_sort_particles(const float* particles, const float* velocity, float* particles_sorted, float* velocity_sorted,

@@ -57,6 +57,20 @@ int64_t clb_scan_scratch_bytes(int64_t count);
 int clb_exclusive_prefix_sum(const int32_t* values, int32_t* output, int32_t* total, int64_t count, void* scratch,
                              int64_t scratch_bytes, void* stream);
 
+/* No counterpart in the reference. The same scan as clb_exclusive_prefix_sum for callers that
+ * cannot allocate device memory -- a host application that has given its whole device memory budget
+ * to its own pool, or code that must not add the device-wide synchronisation of cudaMalloc/cudaFree
+ * to work already in flight. The look-back scratch is a fixed array inside this library
+ * (16 + 8 * 16384 bytes, held on every GPU that loads the library until the process exits), so at
+ * most CLB_SCAN_STATIC_MAX_COUNT elements are accepted; larger counts fail with an error. The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture. Every call clears the part of the array
+ * it uses and all calls share it: calls whose work overlaps on the GPU (different streams, or
+ * different host threads on one device) race and must be serialised by the caller. */
+#define CLB_SCAN_STATIC_MAX_COUNT 67108864LL
+int clb_exclusive_prefix_sum_static(const int32_t* values, int32_t* output, int32_t* total, int64_t count,
+                                    void* stream);
+
 /* particles.cl:110-133 sort_particles (+ the buffer swap of particles.py:119-140 is the caller's).
  * Stable counting-sort scatter: within a bin, particles keep their input order. perm and slot_keys
  * are int32[n] scratch. */
