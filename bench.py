@@ -247,7 +247,7 @@ def our_arm(args):
     replays = sim.pressure_solver.graph_replays - replays0
     gpu_launches = direct_launches + replays * sim.pressure_solver.graph_launches
     cycles = [s.cycles for s in stats]
-    solve_ms = [s.ms for s in stats]
+    solve_ms = [s.device_ms() for s in stats]
     value = world * args.steps / (elapsed_ms / 1e3)
 
     # --- plain vs learned Poisson time to 1e-6 (learned part: reported when available) -------
@@ -295,7 +295,8 @@ def our_arm(args):
     h.smooth(0, iters, ps.correction, ps.residual)
     e3.record()
     torch.cuda.synchronize()
-    fused = h.alt[0] is not None
+    kind0 = h.sweeps()[0] or 1
+    fused = kind0 in (2, 3)
     launches_timed = iters if fused else 2 * iters
     per_launch_s = s3.elapsed_time(e3) / 1e3 / launches_timed
     cells = int(np.prod(scene.grid_shape))
@@ -303,7 +304,8 @@ def our_arm(args):
     algorithmic = 13.0 * cells if fused else 13.0 * cells / 2.0
     achieved = algorithmic / per_launch_s / 1e9
     peak, peak_kind = measured_peak_hbm()
-    kernel = "k_rbgs_iter<true>" if fused else "k_rbgs<true>"
+    kernel = {1: "k_rbgs_colour<true,4>", 2: "k_rbgs_iter<true,8,8,32>", 3: "k_rbgs_iter<true,4,4,32>",
+              4: "k_rbgs<true>"}[kind0]
     traffic = NCU_TRAFFIC_BYTES.get(kernel)
     roofline = {"kernel": f"{kernel} (level-0 red-black Gauss-Seidel, {'one iteration' if fused else 'one colour'} "
                           "per launch)", "bound": "hbm",
@@ -323,6 +325,8 @@ def our_arm(args):
     if rank == 0:
         config = workload_config(args.size, n, args)
         config["multigrid_levels"] = [list(s) for s in h.shapes]
+        config["sweep_kinds"] = h.sweeps()
+        config["sweep_tuning_ms_per_iteration"] = h.tuning
         line = {
             "metric": METRIC,
             "value": value,

@@ -92,6 +92,7 @@ class MGHierarchy(ctypes.Structure):
         ("mask", ctypes.c_void_p * MG_MAX_LEVELS),
         ("op", ctypes.c_void_p * MG_MAX_LEVELS),
         ("alt", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("sweep", ctypes.c_int32 * MG_MAX_LEVELS),
     ]
 
 

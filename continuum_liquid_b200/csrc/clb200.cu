@@ -19,7 +19,7 @@ using namespace clb;
                 (nz));                                                                                 \
     CLB_REQUIRE((i64)(nx) * (ny) * (nz) < (1ll << 31), "grid %dx%dx%d has more than 2^31 cells", (nx), (ny), (nz))
 
-static const int kAbiVersion = 2;
+static const int kAbiVersion = 3;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 
@@ -52,11 +52,11 @@ int clb_init(int device) {
         return 1;
     const int bottom_max = (int)kBottomSmemLimit;
     cudaError_t e = cudaSuccess;
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     if (check_call(e, "bottom visit attribute")) return 1;
     return 0;
 }
@@ -461,6 +461,7 @@ namespace {
 struct LevelView {
     float* p;
     float* alt;
+    int sweep;
     const float* b;
     const uint8_t* op0;
     const float4* opc;
@@ -473,6 +474,7 @@ LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rh
     LevelView v;
     v.l0 = (l == 0);
     v.alt = h->alt[l];
+    v.sweep = h->sweep[l];
     v.p = v.l0 ? x : h->p[l];
     v.b = v.l0 ? rhs : h->b[l];
     v.op0 = h->op0;
@@ -486,11 +488,35 @@ LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rh
 
 int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
     const i64 C = (i64)v.nx * v.ny * v.nz;
-    if (v.alt != nullptr && iterations > 0) {
+    const int kind = v.sweep == 0 ? 1 : v.sweep;
+    if (kind == 1) {
+        const bool vec4 = (v.nz % 4) == 0 && (((uintptr_t)v.p) & 15) == 0;
+        const int vec = vec4 ? 4 : 1;
+        const dim3 block(32, 4);
+        const dim3 grid((v.nz + 32 * vec - 1) / (32 * vec), (v.ny + 3) / 4, v.nx);
+        for (int it = 0; it < iterations; ++it)
+            for (int parity = 0; parity < 2; ++parity) {
+                if (v.l0 && vec4)
+                    k_rbgs_colour<true, 4><<<grid, block, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta, parity,
+                                                                  v.nx, v.ny, v.nz);
+                else if (v.l0)
+                    k_rbgs_colour<true, 1><<<grid, block, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta, parity,
+                                                                  v.nx, v.ny, v.nz);
+                else if (vec4)
+                    k_rbgs_colour<false, 4><<<grid, block, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta, parity,
+                                                                   v.nx, v.ny, v.nz);
+                else
+                    k_rbgs_colour<false, 1><<<grid, block, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta, parity,
+                                                                   v.nx, v.ny, v.nz);
+                CLB_LAUNCH_CHECK("k_rbgs_colour");
+            }
+        return 0;
+    }
+    if ((kind == 2 || kind == 3) && v.alt != nullptr && iterations > 0) {
         // fused iterations, alternating between the level's buffer and its second buffer
         const dim3 big((v.nz + 31) / 32, (v.ny + 7) / 8, (v.nx + 7) / 8);
         const dim3 small((v.nz + 31) / 32, (v.ny + 3) / 4, (v.nx + 3) / 4);
-        const bool use_big = (i64)big.x * big.y * big.z >= 4 * (i64)(g_sm_count > 0 ? g_sm_count : 148);
+        const bool use_big = kind == 2;
         float* cur = v.p;
         float* other = v.alt;
         for (int it = 0; it < iterations; ++it) {
@@ -571,11 +597,11 @@ int bottom_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int co
         h->p[level], h->b[level], (const float4*)h->op[level], h->mask[level], a[0], a[1], a[2], h->p[level + 1], \
         h->b[level + 1], (const float4*)h->op[level + 1], h->mask[level + 1], b[0], b[1], b[2], h->delta, pre,  \
         post, coarse_iters)
-    if (ka <= 1 && kb <= 1) CLB_BOTTOM(1, 1);
-    else if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1);
+    if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1);
     else if (ka <= 4 && kb <= 1) CLB_BOTTOM(4, 1);
-    else if (ka <= 4 && kb <= 2) CLB_BOTTOM(4, 2);
-    else CLB_BOTTOM(8, 4);
+    else if (ka <= 8 && kb <= 1) CLB_BOTTOM(8, 1);
+    else if (ka <= 8 && kb <= 2) CLB_BOTTOM(8, 2);
+    else CLB_BOTTOM(16, 4);
 #undef CLB_BOTTOM
     if (check_launch("k_bottom_visit")) return -1;
     return 1;

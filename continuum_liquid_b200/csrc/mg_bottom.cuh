@@ -4,7 +4,7 @@
 // visit runs (multigrid.py:53-187) pre-smoothing of A, restriction to the coarsest level B, two
 // coarse solves of B (multigrid.py:127-170, 2 + 64 red-black iterations each), prolongation and
 // post-smoothing of A: about 280 dependent red-black phases on a few thousand cells. As separate
-// launches these are bound by launch latency; here one block of 1024 threads runs the whole visit
+// launches these are bound by launch latency; here one block of 512 threads runs the whole visit
 // with both levels in shared memory and block barriers between phases.
 //
 // Each thread owns a fixed set of A cells and B cells (interior cells in index order, strided by the
@@ -17,8 +17,8 @@
 
 namespace clb {
 
-constexpr int BOTTOM_THREADS = 1024;
-constexpr int BOTTOM_MAX_A = 8;  // A cells per thread
+constexpr int BOTTOM_THREADS = 512;
+constexpr int BOTTOM_MAX_A = 16;  // A cells per thread
 constexpr int BOTTOM_MAX_B = 4;  // B cells of each colour per B thread
 
 static inline size_t bottom_smem_bytes(int ca, int cb) {
@@ -51,6 +51,20 @@ __device__ __forceinline__ void owned_cell(int q, int nx, int ny, int nz, const 
     (void)sx;
     (void)sy;
     o.d = so[c].x;  // -1 when not fluid
+}
+
+// Owned coarsest-level cell with its neighbour weights in registers (constant for the whole visit).
+struct OwnedCellW {
+    int c;
+    float d, d2b;
+    float wxp, wxm, wyp, wym, wzp, wzm;
+};
+
+__device__ __forceinline__ void relax_w(const OwnedCellW& o, float* sp, int sx, int sy) {
+    const int c = o.c;
+    const float ws = o.wxp * sp[c + sx] + o.wxm * sp[c - sx] + o.wyp * sp[c + sy] + o.wym * sp[c - sy] +
+                     o.wzp * sp[c + 1] + o.wzm * sp[c - 1];
+    sp[c] = (ws - o.d2b) / o.d;
 }
 
 // One red-black update of an owned cell (multigrid.cl:225-229), p and weights in shared memory.
@@ -122,20 +136,28 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
         A[m].d2b = q < MA ? d2 * sba[A[m].c] : 0.0f;
     }
     const bool btile = threadIdx.x < BOTTOM_BTHREADS;
-    OwnedCell B[2][KB];  // [colour][m]
+    OwnedCellW B[2][KB];  // [colour][m]
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KB; ++m) {
             const int r = threadIdx.x + m * BOTTOM_BTHREADS;
-            OwnedCell& o = B[colour][m];
-            o.colour = colour;
+            OwnedCellW& o = B[colour][m];
             o.d2b = 0.0f;
             o.c = 0;
             o.d = -1.0f;
+            o.wxp = o.wxm = o.wyp = o.wym = o.wzp = o.wzm = 0.0f;
             if (btile && r < MBC) {
-                o.c = colour_cell(r, colour, bny, bnz);
-                o.d = sob[o.c].x;
+                const int c = colour_cell(r, colour, bny, bnz);
+                const float4 self = sob[c];
+                o.c = c;
+                o.d = self.x;
+                o.wxp = self.y;
+                o.wyp = self.z;
+                o.wzp = self.w;
+                o.wxm = sob[c - bsx].y;
+                o.wym = sob[c - bsy].z;
+                o.wzm = sob[c - 1].w;
             }
         }
 
@@ -187,7 +209,7 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
             for (int colour = 0; colour < 2; ++colour) {
 #pragma unroll
                 for (int m = 0; m < KB; ++m)
-                    if (B[colour][m].d > 0.0f) relax(B[colour][m], spb, sob, bsx, bsy);
+                    if (B[colour][m].d > 0.0f) relax_w(B[colour][m], spb, bsx, bsy);
                 bar_b();
             }
     }

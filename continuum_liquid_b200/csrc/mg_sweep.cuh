@@ -136,3 +136,94 @@ __global__ void __launch_bounds__(SW_THREADS) k_rbgs_iter(const float* __restric
 }
 
 }  // namespace clb
+
+namespace clb {
+
+// One red-black colour (multigrid.cl:203-230) with a 3-D launch and no index division: thread
+// (x, y, z) of the grid owns VEC consecutive cells along k of row (i = z, j = y). With VEC = 4 the
+// row is read with 16-byte loads (needs nz % 4 == 0); every cell of the vector is written back
+// (unchanged cells of the other colour keep their value, cells that are not fluid are set to 0, as
+// rbgs_step does). Each update keeps the reference's term order.
+template <bool L0, int VEC>
+__global__ void __launch_bounds__(128) k_rbgs_colour(float* p, const float* __restrict__ b,
+                                                      const uint8_t* __restrict__ op0,
+                                                      const float4* __restrict__ opc,
+                                                      const uint8_t* __restrict__ mask, float delta, int parity,
+                                                      int nx, int ny, int nz) {
+    const int k0 = (blockIdx.x * blockDim.x + threadIdx.x) * VEC;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k0 >= nz || j >= ny) return;
+    const int sx = ny * nz, sy = nz;
+    const int c0 = i * sx + j * sy + k0;
+    const bool row_inner = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
+    const float d2 = delta * delta;
+    float pc[VEC], out[VEC];
+    uint32_t fl[VEC];
+    if (VEC == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p + c0);
+        pc[0] = v.x;
+        pc[1] = v.y;
+        pc[2] = v.z;
+        pc[3] = v.w;
+    } else {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) pc[q] = (k0 + q < nz) ? p[c0 + q] : 0.0f;
+    }
+    uint32_t ob[VEC];
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+        const bool in = k0 + q < nz;
+        if (L0) {
+            ob[q] = in ? (uint32_t)__ldg(op0 + c0 + q) : 0u;
+            fl[q] = (ob[q] >> 6) & 1u;
+        } else {
+            ob[q] = 0u;
+            fl[q] = in ? (uint32_t)(__ldg(mask + c0 + q) != 0) : 0u;
+        }
+        out[q] = fl[q] ? pc[q] : 0.0f;
+    }
+    if (row_inner) {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const int k = k0 + q;
+            if (!fl[q] || k < 1 || k > nz - 2 || ((i + j + k) & 1) != parity) continue;
+            const int c = c0 + q;
+            float d, wxp, wxm, wyp, wym, wzp, wzm;
+            if (L0) {
+                const uint32_t o = ob[q];
+                d = (float)(o & 7u);
+                wxp = bitf(o, 3);
+                wyp = bitf(o, 4);
+                wzp = bitf(o, 5);
+                wxm = bitf(__ldg(op0 + c - sx), 3);
+                wym = bitf(__ldg(op0 + c - sy), 4);
+                wzm = bitf(q > 0 ? ob[q - 1] : (uint32_t)__ldg(op0 + c - 1), 5);
+            } else {
+                const float4 o = __ldg(opc + c);
+                d = o.x;
+                wxp = o.y;
+                wyp = o.z;
+                wzp = o.w;
+                wxm = __ldg(opc + c - sx).y;
+                wym = __ldg(opc + c - sy).z;
+                wzm = __ldg(opc + c - 1).w;
+            }
+            if (!(d > 0.0f)) continue;
+            const float kp = (q + 1 < VEC) ? pc[q + 1] : p[c + 1];
+            const float km = (q > 0) ? pc[q - 1] : p[c - 1];
+            const float ws = wxp * p[c + sx] + wxm * p[c - sx] + wyp * p[c + sy] + wym * p[c - sy] + wzp * kp +
+                             wzm * km;
+            out[q] = (ws - d2 * __ldg(b + c)) / d;
+        }
+    }
+    if (VEC == 4) {
+        *reinterpret_cast<float4*>(p + c0) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q)
+            if (k0 + q < nz) p[c0 + q] = out[q];
+    }
+}
+
+}  // namespace clb

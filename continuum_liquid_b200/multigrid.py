@@ -161,6 +161,7 @@ class MultigridHierarchy:
             self.alt.append(torch.zeros(shape, dtype=torch.float32, device=device) if big else None)
             if big:
                 self.struct.alt[l] = self.alt[l].data_ptr()
+        self.tuning: dict | None = None  # per-level sweep timings from the autotuner (ms per iteration)
         cells = int(np.prod(self.grid_shape))
         self.partials = torch.zeros((kernels.residual_partials(cells), 2), dtype=torch.float64, device=device)
         self.norms = torch.zeros(2, dtype=torch.float64, device=device)
@@ -185,6 +186,13 @@ class MultigridHierarchy:
         """One W-cycle on level-0 unknown ``x`` and right-hand side ``rhs``."""
         self.kernels.call_hierarchy("clb_mg_w_cycle", self.struct, x, rhs, int(pre_smooth), int(post_smooth),
                                     int(coarse_iterations), stream=queue)
+
+    def set_sweep(self, level: int, kind: int) -> None:
+        """Red-black sweep implementation of one level (see clb_mg_hierarchy.sweep)."""
+        self.struct.sweep[level] = int(kind)
+
+    def sweeps(self) -> list[int]:
+        return [int(self.struct.sweep[l]) for l in range(self.levels)]
 
     def smooth(self, level: int, iterations: int, x=None, rhs=None, queue=None) -> None:
         """``iterations`` red-black Gauss-Seidel iterations on one level."""

@@ -65,6 +65,14 @@ class SolveStats:
     initial_rel_residual: float | None = None
     ms: float = 0.0
     history: list = field(default_factory=list)
+    events: tuple | None = None  # CUDA events bracketing the solve on its stream
+
+    def device_ms(self) -> float:
+        """Device time of the solve from its CUDA events (synchronises on the end event)."""
+        if self.events is None:
+            return self.ms
+        self.events[1].synchronize()
+        return self.events[0].elapsed_time(self.events[1])
 
 
 class PressureSolver:
@@ -77,7 +85,8 @@ class PressureSolver:
     rate has run, so most refinements are replayed back to back without a host round trip.
     """
 
-    def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100):
+    def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100,
+                 autotune: bool = True):
         self.kernels = kernels
         self.grid_shape = tuple(int(s) for s in grid_shape)
         self.dx = float(dx)
@@ -92,6 +101,8 @@ class PressureSolver:
         self.cur = 0  # index of the FP64 buffer holding the current pressure
         self.norms_host = torch.zeros(2, dtype=torch.float64, pin_memory=True)
         self._graphs: list[torch.cuda.CUDAGraph | None] = [None, None]
+        self.autotune = autotune
+        self.tuned = False
         self.graph_replays = 0  # refinement-graph replays so far
         self.graph_launches = 0  # kernels inside one refinement graph
 
@@ -150,8 +161,16 @@ class PressureSolver:
         Neumann ghost copy. ``tol=None`` runs ``num_vcycles`` W-cycles (reference semantics)."""
         stats = SolveStats()
         t0 = time.perf_counter()
+        stats.events = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        stats.events[0].record()
         self.prepare(velocity, fluid_fraction, dt, rho)
         h = self.hierarchy
+        if self.autotune and not self.tuned:
+            # sweep kinds are chosen on the first real operator, before any graph captures them
+            from .autotune import tune_hierarchy
+
+            tune_hierarchy(h, self.correction, self.residual)
+            self.tuned = True
         if tol is None:
             for _ in range(int(num_vcycles)):
                 h.w_cycle(pressure, self.rhs)
@@ -181,5 +200,6 @@ class PressureSolver:
             stats.rel_residual = rel
             self.kernels.call("clb_mg_ir_store", self.p64[self.cur], pressure, self.cells)
         boundary_conditions.neumann_domain_bc(self.kernels, None, pressure, self.grid_shape)
+        stats.events[1].record()
         stats.ms = (time.perf_counter() - t0) * 1e3
         return stats

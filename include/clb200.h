@@ -190,9 +190,15 @@ typedef struct clb_mg_hierarchy {
     float* b[CLB_MG_MAX_LEVELS];         /* [0] unused: level-0 rhs is passed per call */
     uint8_t* mask[CLB_MG_MAX_LEVELS];    /* [0] unused */
     void* op[CLB_MG_MAX_LEVELS];         /* [0] unused; float4 per cell */
-    float* alt[CLB_MG_MAX_LEVELS];       /* optional second buffer per level (level 0 included): when
-                                            set, each red-black iteration is one fused launch that
-                                            writes the other buffer; NULL: two launches in place */
+    float* alt[CLB_MG_MAX_LEVELS];       /* optional second buffer per level (level 0 included), used
+                                            by the fused sweep kinds */
+    int32_t sweep[CLB_MG_MAX_LEVELS];    /* red-black sweep implementation per level:
+                                            0 = default (two colour launches),
+                                            1 = two colour launches, 16-byte row vectors when nz % 4 == 0,
+                                            2 = one fused launch per iteration, 8x8x32 tiles (needs alt),
+                                            3 = one fused launch per iteration, 4x4x32 tiles (needs alt),
+                                            4 = two colour launches, one thread per cell.
+                                            All kinds give identical values. */
 } clb_mg_hierarchy;
 
 /* pressure_solve.cl:3-24 pressure_rhs fused with multigrid.cl:63-88 build_finest_operator, writing

@@ -456,3 +456,29 @@ def test_fused_smoothing_odd_iterations(backend, oracle, iterations):
         for parity in (0, 1):
             oracle.lib().orc_rbgs_step_f32(q, orhs, ff, *oops, dx, parity, *shape)
     assert np.array_equal(host(P), q)
+
+
+@pytest.mark.parametrize("kind", [1, 2, 3, 4])
+@pytest.mark.parametrize("shape", [(40, 36, 44), (33, 33, 33)])
+def test_every_sweep_kind_matches_oracle(backend, oracle, shape, kind):
+    dx = F32(1.0 / shape[0])
+    ff, b, p0 = random_system(shape, 25)
+    h = multigrid.MultigridHierarchy(backend, shape, float(dx), fused_min_cells=1)
+    for level in range(h.levels):
+        h.set_sweep(level, kind)
+    u, v, w = (np.random.default_rng(26 + a).standard_normal(shape).astype(F32) for a in range(3))
+    rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    h.rhs_operator((dev(u), dev(v), dev(w)), dev(ff), rhs, 1.0 / 240.0, 1000.0)
+    h.build_coarse()
+    orhs = oracle.pressure_rhs(u, v, w, ff, dx, 1.0 / 240.0, 1000.0, shape)
+    oops = oracle.build_finest_operator(ff, shape)
+    P = dev(p0)
+    h.smooth(0, 3, P, rhs)
+    q = p0.copy()
+    for _ in range(3):
+        for parity in (0, 1):
+            oracle.lib().orc_rbgs_step_f32(q, orhs, ff, *oops, dx, parity, *shape)
+    assert np.array_equal(host(P), q)
+    h.w_cycle(P, rhs)
+    oracle.Levels(shape).w_cycle(q, orhs, ff, oops, dx)
+    assert np.array_equal(host(P), q)
