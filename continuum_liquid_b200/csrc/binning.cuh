@@ -275,12 +275,12 @@ __global__ void __launch_bounds__(PT) k_stable_gather(const int* __restrict__ pe
 // 4, 2, 1. Using the reference's summation order makes the result bit-identical to the CPU
 // restatement for the same sorted particle order.
 //
-// Terms whose tent weight is exactly zero are skipped: a particle in bin b has
-// s = p/dx in [b + 0.5, b + 1.5) on each axis (for clamped bins, farther away), so for the u face of
-// cell c (at c + (1, 0.5, 0.5)) the y and z weights vanish when the bin is one above the cell
-// (o_y = +1 or o_z = +1), and likewise for v and w; the inside count needs o <= 0 on all axes.
-// Bins with two or more +1 offsets contribute nothing. Adding an exactly-zero term does not change a
-// sum (up to the sign of a zero sum), so the result keeps the reference's values.
+// Bins whose every term is exactly zero are skipped: a particle in bin b has s = p/dx in
+// [b + 0.5, b + 1.5) on each axis (for clamped bins, farther away), so for the u face of cell c (at
+// c + (1, 0.5, 0.5)) the y and z weights vanish when the bin is one above the cell (o_y = +1 or
+// o_z = +1), likewise for v and w, and the inside count needs o <= 0 on all axes: a bin with two or
+// more +1 offsets contributes nothing. Adding an exactly-zero term does not change a sum (up to the
+// sign of a zero sum), so the result keeps the reference's values.
 // ------------------------------------------------------------------------------------------------
 constexpr int P2G_LANES = 8;
 constexpr int P2G_THREADS = 256;
@@ -313,54 +313,27 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_gather(const float* __restr
             if (by < 0 || by >= ny - 1) continue;
             const int bz = ck + oz;
             if (bz < 0 || bz >= nz - 1) continue;
-            const int plus = (ox > 0) + (oy > 0) + (oz > 0);
-            if (plus >= 2) continue;  // every weight of this bin is zero
+            if ((ox > 0) + (oy > 0) + (oz > 0) >= 2) continue;  // every weight of this bin is zero
             const i64 bin = gidx(bx, by, bz, ny, nz);
             const int begin = __ldg(offsets + bin);
             const int end = begin + __ldg(counts + bin);
-            if (plus == 0) {  // all three faces and the inside count
-                for (int q = begin; q < end; ++q) {
-                    const float* P = pos + 3 * (i64)q;
-                    const float* V = vel + 3 * (i64)q;
-                    const float s0 = __ldg(P) * inv_dx, s1 = __ldg(P + 1) * inv_dx, s2 = __ldg(P + 2) * inv_dx;
-                    const int pc0 = clampi((int)s0, 1, nx - 2);
-                    const int pc1 = clampi((int)s1, 1, ny - 2);
-                    const int pc2 = clampi((int)s2, 1, nz - 2);
-                    inside += (pc0 == ci && pc1 == cj && pc2 == ck) ? 1 : 0;
-                    const float wu = tent(s0, ux) * tent(s1, uy) * tent(s2, uz);
-                    const float wv = tent(s0, vx) * tent(s1, vy) * tent(s2, vz);
-                    const float ww = tent(s0, wx) * tent(s1, wy) * tent(s2, wz);
-                    vs0 += wu * __ldg(V);
-                    vs1 += wv * __ldg(V + 1);
-                    vs2 += ww * __ldg(V + 2);
-                    ws0 += wu;
-                    ws1 += wv;
-                    ws2 += ww;
-                }
-            } else if (ox > 0) {  // only the u face (o_y, o_z <= 0)
-                for (int q = begin; q < end; ++q) {
-                    const float* P = pos + 3 * (i64)q;
-                    const float wu =
-                        tent(__ldg(P) * inv_dx, ux) * tent(__ldg(P + 1) * inv_dx, uy) * tent(__ldg(P + 2) * inv_dx, uz);
-                    vs0 += wu * __ldg(vel + 3 * (i64)q);
-                    ws0 += wu;
-                }
-            } else if (oy > 0) {  // only the v face
-                for (int q = begin; q < end; ++q) {
-                    const float* P = pos + 3 * (i64)q;
-                    const float wv =
-                        tent(__ldg(P) * inv_dx, vx) * tent(__ldg(P + 1) * inv_dx, vy) * tent(__ldg(P + 2) * inv_dx, vz);
-                    vs1 += wv * __ldg(vel + 3 * (i64)q + 1);
-                    ws1 += wv;
-                }
-            } else {  // only the w face
-                for (int q = begin; q < end; ++q) {
-                    const float* P = pos + 3 * (i64)q;
-                    const float ww =
-                        tent(__ldg(P) * inv_dx, wx) * tent(__ldg(P + 1) * inv_dx, wy) * tent(__ldg(P + 2) * inv_dx, wz);
-                    vs2 += ww * __ldg(vel + 3 * (i64)q + 2);
-                    ws2 += ww;
-                }
+            for (int q = begin; q < end; ++q) {
+                const float* P = pos + 3 * (i64)q;
+                const float* V = vel + 3 * (i64)q;
+                const float s0 = __ldg(P) * inv_dx, s1 = __ldg(P + 1) * inv_dx, s2 = __ldg(P + 2) * inv_dx;
+                const int pc0 = clampi((int)s0, 1, nx - 2);
+                const int pc1 = clampi((int)s1, 1, ny - 2);
+                const int pc2 = clampi((int)s2, 1, nz - 2);
+                inside += (pc0 == ci && pc1 == cj && pc2 == ck) ? 1 : 0;
+                const float wu = tent(s0, ux) * tent(s1, uy) * tent(s2, uz);
+                const float wv = tent(s0, vx) * tent(s1, vy) * tent(s2, vz);
+                const float ww = tent(s0, wx) * tent(s1, wy) * tent(s2, wz);
+                vs0 += wu * __ldg(V);
+                vs1 += wv * __ldg(V + 1);
+                vs2 += ww * __ldg(V + 2);
+                ws0 += wu;
+                ws1 += wv;
+                ws2 += ww;
             }
         }
     }

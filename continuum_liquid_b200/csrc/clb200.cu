@@ -678,12 +678,13 @@ int clb_mg_residual_norms(const void* p, int p_is_double, const float* b, const 
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
     if (p_is_double)
-        k_residual_norms<double><<<blocks, RN_THREADS, 0, s>>>((const double*)p, b, op0, inv_delta2, nx, ny, nz, r_out,
-                                                               (double2*)partials);
+        k_residual_rows<double, false><<<blocks, RN_THREADS, 0, s>>>((const double*)p, nullptr, nullptr, b, op0,
+                                                                     inv_delta2, nx, ny, nz, r_out,
+                                                                     (double2*)partials);
     else
-        k_residual_norms<float><<<blocks, RN_THREADS, 0, s>>>((const float*)p, b, op0, inv_delta2, nx, ny, nz, r_out,
-                                                              (double2*)partials);
-    CLB_LAUNCH_CHECK("k_residual_norms");
+        k_residual_rows<float, false><<<blocks, RN_THREADS, 0, s>>>((const float*)p, nullptr, nullptr, b, op0,
+                                                                    inv_delta2, nx, ny, nz, r_out, (double2*)partials);
+    CLB_LAUNCH_CHECK("k_residual_rows");
     k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
     return 0;
@@ -698,9 +699,9 @@ int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const 
     const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    k_ir_step<<<blocks, RN_THREADS, 0, s>>>(p64_in, e, p64_out, b, op0, inv_delta2, nx, ny, nz, r_out,
-                                           (double2*)partials);
-    CLB_LAUNCH_CHECK("k_ir_step");
+    k_residual_rows<double, true><<<blocks, RN_THREADS, 0, s>>>(p64_in, e, p64_out, b, op0, inv_delta2, nx, ny, nz,
+                                                                r_out, (double2*)partials);
+    CLB_LAUNCH_CHECK("k_residual_rows");
     k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
     return 0;

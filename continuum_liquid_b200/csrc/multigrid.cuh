@@ -449,93 +449,61 @@ static inline size_t coarse_smem_bytes(int C) {
 // ------------------------------------------------------------------------------------------------
 constexpr int RN_THREADS = 256;
 
-// Per block: sums of r^2 and b^2 over interior fluid cells, r = b - A p evaluated in FP64 from a
-// float or double p (A is multigrid.cl:25-43 apply_operator). When r_out is given the residual is
-// also stored, rounded to float, at every cell (0 outside interior fluid cells): it becomes the
-// right-hand side of the next correction solve.
-template <typename PT>
-__global__ void __launch_bounds__(RN_THREADS) k_residual_norms(const PT* __restrict__ p, const float* __restrict__ b,
-                                                                const uint8_t* __restrict__ op0, double inv_delta2,
-                                                                int nx, int ny, int nz, float* __restrict__ r_out,
-                                                                double2* __restrict__ partials) {
+// FP64 residual over the finest level, one (i, j) row per warp (lanes stride along k, so there is no
+// per-cell index division). Per block: sums of r^2 and b^2 over interior fluid cells, with
+// r = b - A p evaluated in FP64 (A is multigrid.cl:25-43 apply_operator).
+//  STEP = false: p is the float or double pressure p_in.
+//  STEP = true:  the refinement update fused in: p = p_in + e is formed on the fly for the cell and
+//                its neighbours and written to p_out (which must not alias p_in).
+// When r_out is given the residual is stored rounded to float at every cell (0 outside interior
+// fluid cells): it is the right-hand side of the next correction solve.
+template <typename PT, bool STEP>
+__global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restrict__ p_in,
+                                                               const float* __restrict__ e,
+                                                               double* __restrict__ p_out,
+                                                               const float* __restrict__ b,
+                                                               const uint8_t* __restrict__ op0, double inv_delta2,
+                                                               int nx, int ny, int nz, float* __restrict__ r_out,
+                                                               double2* __restrict__ partials) {
     __shared__ double2 s_red[RN_THREADS / 32];
-    const i64 C = (i64)nx * ny * nz;
-    const i64 sx = (i64)ny * nz, sy = nz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sx = ny * nz, sy = nz;
     double rr = 0.0, bb = 0.0;
-    for (i64 c = (i64)blockIdx.x * RN_THREADS + threadIdx.x; c < C; c += (i64)gridDim.x * RN_THREADS) {
-        int i, j, k;
-        gcoord(c, ny, nz, i, j, k);
-        const uint32_t o = __ldg(op0 + c);
-        float rf = 0.0f;
-        if (interior(i, j, k, nx, ny, nz) && (o & 64u)) {
-            const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
-            const double ws = (double)bitf(o, 3) * (double)p[c + sx] + (double)bitf(ox, 3) * (double)p[c - sx] +
-                              (double)bitf(o, 4) * (double)p[c + sy] + (double)bitf(oy, 4) * (double)p[c - sy] +
-                              (double)bitf(o, 5) * (double)p[c + 1] + (double)bitf(oz, 5) * (double)p[c - 1];
-            const double bv = (double)__ldg(b + c);
-            const double r = bv - (ws - (double)(o & 7u) * (double)p[c]) * inv_delta2;
-            rr += r * r;
-            bb += bv * bv;
-            rf = (float)r;
+    auto pv = [&](int q) -> double {
+        if (STEP) return (double)__ldg(p_in + q) + (double)__ldg(e + q);
+        return (double)__ldg(p_in + q);
+    };
+    const int rows = nx * ny;
+    for (int r = blockIdx.x * (RN_THREADS / 32) + warp; r < rows; r += gridDim.x * (RN_THREADS / 32)) {
+        const int i = r / ny, j = r - i * ny;
+        const bool row_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
+        const int base = r * nz;
+        for (int k = lane; k < nz; k += 32) {
+            const int c = base + k;
+            const double pc = pv(c);
+            if (STEP) p_out[c] = pc;
+            const uint32_t o = __ldg(op0 + c);
+            float rf = 0.0f;
+            if (row_in && k >= 1 && k <= nz - 2 && (o & 64u)) {
+                const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
+                const double ws = (double)bitf(o, 3) * pv(c + sx) + (double)bitf(ox, 3) * pv(c - sx) +
+                                  (double)bitf(o, 4) * pv(c + sy) + (double)bitf(oy, 4) * pv(c - sy) +
+                                  (double)bitf(o, 5) * pv(c + 1) + (double)bitf(oz, 5) * pv(c - 1);
+                const double bv = (double)__ldg(b + c);
+                const double res = bv - (ws - (double)(o & 7u) * pc) * inv_delta2;
+                rr += res * res;
+                bb += bv * bv;
+                rf = (float)res;
+            }
+            if (r_out) r_out[c] = rf;
         }
-        if (r_out) r_out[c] = rf;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         rr += __shfl_xor_sync(0xffffffffu, rr, o);
         bb += __shfl_xor_sync(0xffffffffu, bb, o);
     }
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = make_double2(rr, bb);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double2 t = s_red[0];
-        for (int q = 1; q < RN_THREADS / 32; ++q) {
-            t.x += s_red[q].x;
-            t.y += s_red[q].y;
-        }
-        partials[blockIdx.x] = t;
-    }
-}
-
-// Refinement step fused with the next residual: p_out = p_in + e at every cell and, at interior
-// fluid cells, r = b - A p_out in FP64 (neighbour values formed as p_in + e on the fly, so p_out
-// must not alias p_in), r rounded to float into r_out, with the block partials of r^2 and b^2.
-__global__ void __launch_bounds__(RN_THREADS) k_ir_step(const double* __restrict__ p_in, const float* __restrict__ e,
-                                                         double* __restrict__ p_out, const float* __restrict__ b,
-                                                         const uint8_t* __restrict__ op0, double inv_delta2, int nx,
-                                                         int ny, int nz, float* __restrict__ r_out,
-                                                         double2* __restrict__ partials) {
-    __shared__ double2 s_red[RN_THREADS / 32];
-    const i64 C = (i64)nx * ny * nz;
-    const i64 sx = (i64)ny * nz, sy = nz;
-    double rr = 0.0, bb = 0.0;
-    for (i64 c = (i64)blockIdx.x * RN_THREADS + threadIdx.x; c < C; c += (i64)gridDim.x * RN_THREADS) {
-        int i, j, k;
-        gcoord(c, ny, nz, i, j, k);
-        const double pc = __ldg(p_in + c) + (double)__ldg(e + c);
-        p_out[c] = pc;
-        const uint32_t o = __ldg(op0 + c);
-        float rf = 0.0f;
-        if (interior(i, j, k, nx, ny, nz) && (o & 64u)) {
-            auto pv = [&](i64 q) { return __ldg(p_in + q) + (double)__ldg(e + q); };
-            const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
-            const double ws = (double)bitf(o, 3) * pv(c + sx) + (double)bitf(ox, 3) * pv(c - sx) +
-                              (double)bitf(o, 4) * pv(c + sy) + (double)bitf(oy, 4) * pv(c - sy) +
-                              (double)bitf(o, 5) * pv(c + 1) + (double)bitf(oz, 5) * pv(c - 1);
-            const double bv = (double)__ldg(b + c);
-            const double r = bv - (ws - (double)(o & 7u) * pc) * inv_delta2;
-            rr += r * r;
-            bb += bv * bv;
-            rf = (float)r;
-        }
-        r_out[c] = rf;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        rr += __shfl_xor_sync(0xffffffffu, rr, o);
-        bb += __shfl_xor_sync(0xffffffffu, bb, o);
-    }
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = make_double2(rr, bb);
+    if (lane == 0) s_red[warp] = make_double2(rr, bb);
     __syncthreads();
     if (threadIdx.x == 0) {
         double2 t = s_red[0];
