@@ -68,6 +68,7 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_ir_step": [P, P, P, P, P, F, I, I, I, P, P, P, P],
     "clb_mg_ir_update": [P, P, L, P],
     "clb_mg_ir_store": [P, P, L, P],
+    "clb_tc_test_gemm": [P, P, P, I, I, I, I, P],
     "clb_voxelise_mesh": [P, P, I, I, I, I, F, F, F, F, I, P],
     "clb_voxelise_direction": [P],
 }

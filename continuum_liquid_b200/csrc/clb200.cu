@@ -8,6 +8,7 @@
 #include "mg_bottom.cuh"
 #include "mg_sweep.cuh"
 #include "voxelise.cuh"
+#include "tc_gemm.cuh"
 
 #include <mutex>
 
@@ -729,6 +730,41 @@ int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream) 
     if (cells == 0) return 0;
     k_ir_store<<<blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream)>>>(p64, p32, cells);
     CLB_LAUNCH_CHECK("k_ir_store");
+    return 0;
+}
+
+// ---- tensor-core GEMM check ----------------------------------------------------------------------
+
+int clb_tc_test_gemm(const void* a, const void* b, float* c, int M, int N, int K, int mn_major, void* stream) {
+    CLB_REQUIRE(a && b && c, "tc_test_gemm: null pointer");
+    CLB_REQUIRE(M > 0 && K > 0 && K % 8 == 0 && M % 8 == 0, "tc_test_gemm: M, K must be positive multiples of 8");
+    CLB_REQUIRE(N == 16 || N == 32 || N == 64 || N == 128, "tc_test_gemm: N must be 16, 32, 64 or 128");
+    const dim3 grid((M + tc::TC_M - 1) / tc::TC_M);
+    cudaStream_t s = CLB_STREAM(stream);
+    const __nv_bfloat16* A = (const __nv_bfloat16*)a;
+    const __nv_bfloat16* B = (const __nv_bfloat16*)b;
+#define CLB_TCG(AMN, BMN, NN)                                                                               \
+    do {                                                                                                    \
+        const size_t bytes = tc::tile_smem_bytes<NN>();                                                     \
+        if (check_call(cudaFuncSetAttribute(tc::k_tc_test_gemm<AMN, BMN, NN>,                               \
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),       \
+                       "tc_test_gemm attribute"))                                                           \
+            return 1;                                                                                       \
+        tc::k_tc_test_gemm<AMN, BMN, NN><<<grid, tc::TC_THREADS, bytes, s>>>(A, B, c, M, K);                \
+    } while (0)
+    if (mn_major) {
+        if (N == 16) CLB_TCG(true, true, 16);
+        else if (N == 32) CLB_TCG(true, true, 32);
+        else if (N == 64) CLB_TCG(true, true, 64);
+        else CLB_TCG(true, true, 128);
+    } else {
+        if (N == 16) CLB_TCG(false, false, 16);
+        else if (N == 32) CLB_TCG(false, false, 32);
+        else if (N == 64) CLB_TCG(false, false, 64);
+        else CLB_TCG(false, false, 128);
+    }
+#undef CLB_TCG
+    CLB_LAUNCH_CHECK("k_tc_test_gemm");
     return 0;
 }
 

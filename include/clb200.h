@@ -246,6 +246,14 @@ int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const 
 int clb_mg_ir_update(double* p64, const float* e, int64_t cells, void* stream);
 int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream);
 
+/* ---- tensor cores -------------------------------------------------------------------------- */
+
+/* No counterpart in the reference (the learned warm start is new). Check of the tcgen05 GEMM core
+ * used by the 3-D convolutions: c[M][N] (float32) = a * b^T in BF16 with FP32 accumulation.
+ * mn_major = 0: a is [M][K] and b is [N][K] (K contiguous); 1: a is [K][M] and b is [K][N].
+ * M and K multiples of 8, N one of 16, 32, 64, 128. */
+int clb_tc_test_gemm(const void* a, const void* b, float* c, int M, int N, int K, int mn_major, void* stream);
+
 /* ---- collider voxelisation (Solver/Kernel/voxelise_mesh.py, OpenCL/voxelise_mesh.cl) ------- */
 
 /* voxelise_mesh.cl:24-48 voxelise_mesh: ORs 1 into mask for interior cells whose centre ray has an
