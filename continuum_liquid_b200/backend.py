@@ -69,6 +69,18 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_ir_update": [P, P, L, P],
     "clb_mg_ir_store": [P, P, L, P],
     "clb_tc_test_gemm": [P, P, P, I, I, I, I, P],
+    "clb_conv3d_arrange_weights": [P, P, P, I, I, I, I, P],
+    "clb_conv3d_forward": [P, P, P, P, I, I, I, I, I, I, I, I, P],
+    "clb_conv3d_dgrad": [P, P, P, P, I, I, I, I, I, I, I, P],
+    "clb_conv3d_wgrad": [P, P, P, I, I, I, I, I, I, I, P],
+    "clb_unet_avgpool2": [P, P, I, I, I, I, I, P],
+    "clb_unet_avgpool2_backward": [P, P, P, I, I, I, I, I, P],
+    "clb_unet_upsample_concat": [P, P, P, I, I, I, I, I, I, P],
+    "clb_unet_upsample_concat_backward": [P, P, P, I, I, I, I, I, I, P],
+    "clb_unet_head_forward": [P, P, P, P, I, I, P],
+    "clb_unet_head_backward": [P, P, P, P, P, P, I, I, P],
+    "clb_unet_bias_grad": [P, P, I, I, P],
+    "clb_adam_step": [P, P, P, P, L, F, F, F, F, I, P],
     "clb_voxelise_mesh": [P, P, I, I, I, I, F, F, F, F, I, P],
     "clb_voxelise_direction": [P],
 }

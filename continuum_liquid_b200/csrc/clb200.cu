@@ -9,6 +9,7 @@
 #include "mg_sweep.cuh"
 #include "voxelise.cuh"
 #include "tc_gemm.cuh"
+#include "conv3d.cuh"
 
 #include <mutex>
 
@@ -23,6 +24,32 @@ using namespace clb;
 static const int kAbiVersion = 3;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
+
+template <int N, bool DG>
+static cudaError_t conv_rows_attr() {
+    return cudaFuncSetAttribute(conv::k_conv_rows<N, DG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tc::tile_smem_bytes<N>());
+}
+template <int N>
+static cudaError_t conv_wgrad_attr() {
+    return cudaFuncSetAttribute(conv::k_conv_wgrad<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tc::tile_smem_bytes<N>());
+}
+static int conv_set_attributes() {
+    cudaError_t e = cudaSuccess;
+    e = e != cudaSuccess ? e : conv_rows_attr<16, false>();
+    e = e != cudaSuccess ? e : conv_rows_attr<32, false>();
+    e = e != cudaSuccess ? e : conv_rows_attr<64, false>();
+    e = e != cudaSuccess ? e : conv_rows_attr<16, true>();
+    e = e != cudaSuccess ? e : conv_rows_attr<32, true>();
+    e = e != cudaSuccess ? e : conv_rows_attr<48, true>();
+    e = e != cudaSuccess ? e : conv_rows_attr<64, true>();
+    e = e != cudaSuccess ? e : conv_rows_attr<96, true>();
+    e = e != cudaSuccess ? e : conv_wgrad_attr<16>();
+    e = e != cudaSuccess ? e : conv_wgrad_attr<32>();
+    e = e != cudaSuccess ? e : conv_wgrad_attr<64>();
+    return check_call(e, "convolution attributes");
+}
 
 extern "C" {
 
@@ -59,6 +86,7 @@ int clb_init(int device) {
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     if (check_call(e, "bottom visit attribute")) return 1;
+    if (conv_set_attributes()) return 1;
     return 0;
 }
 
@@ -765,6 +793,182 @@ int clb_tc_test_gemm(const void* a, const void* b, float* c, int M, int N, int K
     }
 #undef CLB_TCG
     CLB_LAUNCH_CHECK("k_tc_test_gemm");
+    return 0;
+}
+
+// ---- 3-D convolutions and the U-Net's elementwise operations ------------------------------------
+
+#define CLB_VOL_OK(B, D, H, W)                                                                   \
+    CLB_REQUIRE((B) > 0 && (D) > 0 && (H) > 0 && (W) > 0 && (i64)(B) * (D) * (H) * (W) < (1ll << 31), \
+                "volume %dx%dx%dx%d out of range", (B), (D), (H), (W))
+
+static unsigned ew_blocks(i64 n) {
+    const i64 b = (n + conv::EW - 1) / conv::EW;
+    return (unsigned)(b < 148 * 32 ? (b > 0 ? b : 1) : 148 * 32);
+}
+
+int clb_conv3d_forward(const void* x, const void* wf, const float* bias, void* y, int B, int D, int H, int W, int cin,
+                       int cout, int kpad, int relu, void* stream) {
+    CLB_VOL_OK(B, D, H, W);
+    CLB_REQUIRE(x && wf && y, "conv3d_forward: null pointer");
+    CLB_REQUIRE(cin > 0 && cin % 8 == 0, "conv3d_forward: cin=%d must be a positive multiple of 8", cin);
+    CLB_REQUIRE(kpad % 64 == 0 && kpad >= 27 * cin, "conv3d_forward: kpad=%d must be a multiple of 64 >= 27*cin", kpad);
+    const conv::Vol g{B, D, H, W};
+    const unsigned blocks = (unsigned)(((i64)B * D * H * W + tc::TC_M - 1) / tc::TC_M);
+    cudaStream_t s = CLB_STREAM(stream);
+    const auto* X = (const __nv_bfloat16*)x;
+    const auto* Wf = (const __nv_bfloat16*)wf;
+    auto* Y = (__nv_bfloat16*)y;
+    if (cout == 16)
+        conv::k_conv_rows<16, false><<<blocks, tc::TC_THREADS, tc::tile_smem_bytes<16>(), s>>>(X, Wf, bias, nullptr, Y, g,
+                                                                                              cin, kpad, relu);
+    else if (cout == 32)
+        conv::k_conv_rows<32, false><<<blocks, tc::TC_THREADS, tc::tile_smem_bytes<32>(), s>>>(X, Wf, bias, nullptr, Y, g,
+                                                                                              cin, kpad, relu);
+    else if (cout == 64)
+        conv::k_conv_rows<64, false><<<blocks, tc::TC_THREADS, tc::tile_smem_bytes<64>(), s>>>(X, Wf, bias, nullptr, Y, g,
+                                                                                              cin, kpad, relu);
+    else
+        return set_error("conv3d_forward: cout=%d not supported (16, 32, 64)", cout);
+    CLB_LAUNCH_CHECK("k_conv_rows<forward>");
+    return 0;
+}
+
+int clb_conv3d_dgrad(const void* dy, const void* wd, const void* mask_x, void* dx, int B, int D, int H, int W, int cout,
+                     int cin, int kpad, void* stream) {
+    CLB_VOL_OK(B, D, H, W);
+    CLB_REQUIRE(dy && wd && dx, "conv3d_dgrad: null pointer");
+    CLB_REQUIRE(cout > 0 && cout % 8 == 0, "conv3d_dgrad: cout=%d must be a positive multiple of 8", cout);
+    CLB_REQUIRE(kpad % 64 == 0 && kpad >= 27 * cout, "conv3d_dgrad: kpad=%d must be a multiple of 64 >= 27*cout", kpad);
+    const conv::Vol g{B, D, H, W};
+    const unsigned blocks = (unsigned)(((i64)B * D * H * W + tc::TC_M - 1) / tc::TC_M);
+    cudaStream_t s = CLB_STREAM(stream);
+    const auto* DY = (const __nv_bfloat16*)dy;
+    const auto* Wd = (const __nv_bfloat16*)wd;
+    const auto* MX = (const __nv_bfloat16*)mask_x;
+    auto* DX = (__nv_bfloat16*)dx;
+#define CLB_DG(NN)                                                                                             \
+    conv::k_conv_rows<NN, true><<<blocks, tc::TC_THREADS, tc::tile_smem_bytes<NN>(), s>>>(DY, Wd, nullptr, MX, DX, g, \
+                                                                                         cout, kpad, 0)
+    if (cin == 16) CLB_DG(16);
+    else if (cin == 32) CLB_DG(32);
+    else if (cin == 48) CLB_DG(48);
+    else if (cin == 64) CLB_DG(64);
+    else if (cin == 96) CLB_DG(96);
+    else return set_error("conv3d_dgrad: cin=%d not supported (16, 32, 48, 64, 96)", cin);
+#undef CLB_DG
+    CLB_LAUNCH_CHECK("k_conv_rows<dgrad>");
+    return 0;
+}
+
+int clb_conv3d_wgrad(const void* x, const void* dy, float* dw, int B, int D, int H, int W, int cin, int cout,
+                     int chunks_per_block, void* stream) {
+    CLB_VOL_OK(B, D, H, W);
+    CLB_REQUIRE(x && dy && dw, "conv3d_wgrad: null pointer");
+    CLB_REQUIRE(cin > 0 && cin % 8 == 0, "conv3d_wgrad: cin=%d must be a positive multiple of 8", cin);
+    CLB_REQUIRE(chunks_per_block > 0, "conv3d_wgrad: chunks_per_block must be positive");
+    const conv::Vol g{B, D, H, W};
+    const i64 chunks = ((i64)B * D * H * W + tc::TC_KC - 1) / tc::TC_KC;
+    const dim3 grid((unsigned)((27 * cin + tc::TC_M - 1) / tc::TC_M),
+                    (unsigned)((chunks + chunks_per_block - 1) / chunks_per_block));
+    cudaStream_t s = CLB_STREAM(stream);
+    const auto* X = (const __nv_bfloat16*)x;
+    const auto* DY = (const __nv_bfloat16*)dy;
+    if (cout == 16)
+        conv::k_conv_wgrad<16><<<grid, tc::TC_THREADS, tc::tile_smem_bytes<16>(), s>>>(X, DY, dw, g, cin, chunks_per_block);
+    else if (cout == 32)
+        conv::k_conv_wgrad<32><<<grid, tc::TC_THREADS, tc::tile_smem_bytes<32>(), s>>>(X, DY, dw, g, cin, chunks_per_block);
+    else if (cout == 64)
+        conv::k_conv_wgrad<64><<<grid, tc::TC_THREADS, tc::tile_smem_bytes<64>(), s>>>(X, DY, dw, g, cin, chunks_per_block);
+    else
+        return set_error("conv3d_wgrad: cout=%d not supported (16, 32, 64)", cout);
+    CLB_LAUNCH_CHECK("k_conv_wgrad");
+    return 0;
+}
+
+int clb_conv3d_arrange_weights(const float* w, void* wf, void* wd, int cin, int cout, int kpad, int kpad2,
+                               void* stream) {
+    CLB_REQUIRE(w && wf, "conv3d_arrange_weights: null pointer");
+    CLB_REQUIRE(kpad >= 27 * cin && (!wd || kpad2 >= 27 * cout), "conv3d_arrange_weights: K padding too small");
+    const i64 total = (i64)cout * kpad + (wd ? (i64)cin * kpad2 : 0);
+    conv::k_arrange_weights<<<ew_blocks(total), conv::EW, 0, CLB_STREAM(stream)>>>(
+        w, (__nv_bfloat16*)wf, (__nv_bfloat16*)wd, cin, cout, kpad, kpad2);
+    CLB_LAUNCH_CHECK("k_arrange_weights");
+    return 0;
+}
+
+int clb_unet_avgpool2(const void* x, void* y, int B, int D, int H, int W, int C, void* stream) {
+    CLB_VOL_OK(B, D, H, W);
+    CLB_REQUIRE(D % 2 == 0 && H % 2 == 0 && W % 2 == 0, "unet_avgpool2: extents must be even");
+    const conv::Vol g{B, D, H, W};
+    conv::k_avgpool2<<<ew_blocks((i64)B * D * H * W * C / 8), conv::EW, 0, CLB_STREAM(stream)>>>(
+        (const __nv_bfloat16*)x, (__nv_bfloat16*)y, g, C);
+    CLB_LAUNCH_CHECK("k_avgpool2");
+    return 0;
+}
+
+int clb_unet_avgpool2_backward(const void* dy, const void* x, void* dx, int B, int D, int H, int W, int C,
+                               void* stream) {
+    CLB_VOL_OK(B, D, H, W);
+    const conv::Vol g{B, D, H, W};
+    conv::k_avgpool2_backward<<<ew_blocks((i64)B * D * H * W * C), conv::EW, 0, CLB_STREAM(stream)>>>(
+        (const __nv_bfloat16*)dy, (const __nv_bfloat16*)x, (__nv_bfloat16*)dx, g, C);
+    CLB_LAUNCH_CHECK("k_avgpool2_backward");
+    return 0;
+}
+
+int clb_unet_upsample_concat(const void* coarse, const void* skip, void* out, int B, int D, int H, int W, int c1,
+                             int c2, void* stream) {
+    CLB_VOL_OK(B, D, H, W);
+    const conv::Vol g{B, D, H, W};
+    conv::k_upsample_concat<<<ew_blocks((i64)B * D * H * W * (c1 + c2)), conv::EW, 0, CLB_STREAM(stream)>>>(
+        (const __nv_bfloat16*)coarse, (const __nv_bfloat16*)skip, (__nv_bfloat16*)out, g, c1, c2);
+    CLB_LAUNCH_CHECK("k_upsample_concat");
+    return 0;
+}
+
+int clb_unet_upsample_concat_backward(const void* dout, void* dcoarse, void* dskip, int B, int D, int H, int W,
+                                      int c1, int c2, void* stream) {
+    CLB_VOL_OK(B, D, H, W);
+    const conv::Vol g{B, D, H, W};
+    conv::k_upsample_concat_backward<<<ew_blocks((i64)B * D * H * W * (c1 + c2)), conv::EW, 0, CLB_STREAM(stream)>>>(
+        (const __nv_bfloat16*)dout, (__nv_bfloat16*)dcoarse, (__nv_bfloat16*)dskip, g, c1, c2);
+    CLB_LAUNCH_CHECK("k_upsample_concat_backward");
+    return 0;
+}
+
+int clb_unet_head_forward(const void* h, const float* w, const float* b, float* out, int voxels, int C,
+                          void* stream) {
+    CLB_REQUIRE(C > 0 && C <= 16, "unet_head_forward: C=%d must be in 1..16", C);
+    conv::k_head_forward<<<ew_blocks(voxels), conv::EW, 0, CLB_STREAM(stream)>>>((const __nv_bfloat16*)h, w, b, out,
+                                                                                 voxels, C);
+    CLB_LAUNCH_CHECK("k_head_forward");
+    return 0;
+}
+
+int clb_unet_head_backward(const void* h, const float* w, const float* dout, void* dh, float* dw, float* db,
+                           int voxels, int C, void* stream) {
+    CLB_REQUIRE(C > 0 && C <= 16, "unet_head_backward: C=%d must be in 1..16", C);
+    conv::k_head_backward<<<ew_blocks(voxels), conv::EW, 0, CLB_STREAM(stream)>>>(
+        (const __nv_bfloat16*)h, w, dout, (__nv_bfloat16*)dh, dw, db, voxels, C);
+    CLB_LAUNCH_CHECK("k_head_backward");
+    return 0;
+}
+
+int clb_unet_bias_grad(const void* dy, float* db, int voxels, int C, void* stream) {
+    CLB_REQUIRE(C > 0 && C <= 256, "unet_bias_grad: C=%d must be in 1..256", C);
+    conv::k_bias_grad<<<ew_blocks((i64)voxels * C / 16), conv::EW, 0, CLB_STREAM(stream)>>>((const __nv_bfloat16*)dy, db,
+                                                                                            voxels, C);
+    CLB_LAUNCH_CHECK("k_bias_grad");
+    return 0;
+}
+
+int clb_adam_step(float* p, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2, float eps,
+                  int step, void* stream) {
+    CLB_REQUIRE(p && g && m && v && n >= 0 && step >= 1, "adam_step: bad arguments");
+    const float bc1 = 1.0f - powf(beta1, (float)step), bc2 = 1.0f - powf(beta2, (float)step);
+    conv::k_adam<<<ew_blocks(n), conv::EW, 0, CLB_STREAM(stream)>>>(p, g, m, v, n, lr, beta1, beta2, eps, bc1, bc2);
+    CLB_LAUNCH_CHECK("k_adam");
     return 0;
 }
 

@@ -1,0 +1,392 @@
+// 3x3x3 convolutions (padding 1, stride 1) of the learned pressure warm start as implicit GEMMs on
+// the tcgen05 core (tc_gemm.cuh). Activations are channels-last BF16 volumes [B][D][H][W][C] with C a
+// multiple of 8; the 27 taps are ordered (dz, dy, dx) with dx fastest, offsets -1..1.
+//
+//   forward   y[v][co] = act(b[co] + sum_{tap,ci} x[v + o(tap)][ci] * W[tap][ci][co])
+//             GEMM: M = voxels (tiles of 128), N = Cout, K = 27 * Cin (K-major gathers of x, weights
+//             pre-arranged as wf[co][tap * Cin + ci]); bias and ReLU fused in the epilogue.
+//   data grad dx[v][ci] = mask(ci) * sum_{tap,co} dy[v - o(tap)][co] * W[tap][ci][co]
+//             GEMM: M = voxels, N = Cin, K = 27 * Cout (wd[ci][tap * Cout + co]); the ReLU backward
+//             of the layer that produced x (mask = x > 0) is fused in the epilogue.
+//   weight grad dW[tap * Cin + ci][co] += sum_v x[v + o(tap)][ci] * dy[v][co]
+//             GEMM: M = 27 * Cin (tiles of 128), N = Cout, K = voxels split over blocks; both
+//             operands MN-major (16-byte rows of 8 consecutive channels); FP32 atomics in the
+//             epilogue accumulate the blocks' partial sums.
+#pragma once
+#include "tc_gemm.cuh"
+
+namespace clb {
+namespace conv {
+
+using tc::TC_KC;
+using tc::TC_M;
+using tc::TC_THREADS;
+
+struct Vol {
+    int B, D, H, W;
+    __device__ __forceinline__ int voxels() const { return B * D * H * W; }
+};
+
+// neighbour of voxel (b, z, y, x) at tap t, or -1 outside the volume
+__device__ __forceinline__ int tap_neighbour(const Vol& g, int b, int z, int y, int x, int tap, int sign) {
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    const int zz = z + sign * dz, yy = y + sign * dy, xx = x + sign * dx;
+    if (zz < 0 || zz >= g.D || yy < 0 || yy >= g.H || xx < 0 || xx >= g.W) return -1;
+    return ((b * g.D + zz) * g.H + yy) * g.W + xx;
+}
+
+__device__ __forceinline__ void decode(const Vol& g, int v, int& b, int& z, int& y, int& x) {
+    x = v % g.W;
+    int r = v / g.W;
+    y = r % g.H;
+    r /= g.H;
+    z = r % g.D;
+    b = r / g.D;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// ---- forward and data gradient: A = gathered activations (K-major), B = arranged weights ----------
+template <int N, bool DGRAD>
+struct ConvRows {
+    static constexpr bool A_MN = false, B_MN = false;
+    const __nv_bfloat16* src;  // forward: x [V][Cs]; data grad: dy [V][Cs]
+    const __nv_bfloat16* wmat;  // [N][Kpad] bf16
+    const float* bias;          // forward only (nullable)
+    const __nv_bfloat16* mask_src;  // data grad: x [V][N] for the ReLU mask (nullable)
+    __nv_bfloat16* out;         // [V][N]
+    Vol g;
+    int Cs, K, Kpad, chunks, m0, relu;
+    int vb, vz, vy, vx;  // this thread's row voxel (row = threadIdx.x)
+    bool valid;
+    __device__ void setup() {
+        const int v = m0 + threadIdx.x;
+        valid = v < g.voxels();
+        if (valid) decode(g, v, vb, vz, vy, vx);
+    }
+    __device__ void gather_a(uint8_t* st, int chunk) const {
+        const int row = threadIdx.x;
+#pragma unroll
+        for (int kv = 0; kv < TC_KC / 8; ++kv) {
+            const int k = chunk * TC_KC + kv * 8;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (valid && k < K) {
+                const int tap = k / Cs, c = k - tap * Cs;
+                const int nb = tap_neighbour(g, vb, vz, vy, vx, tap, DGRAD ? -1 : 1);
+                if (nb >= 0) val = __ldg(reinterpret_cast<const uint4*>(src + (i64)nb * Cs + c));
+            }
+            *reinterpret_cast<uint4*>(st + tc::kmajor_off(row, kv)) = val;
+        }
+    }
+    __device__ void gather_b(uint8_t* st, int chunk) const {
+        for (int t = threadIdx.x; t < N * (TC_KC / 8); t += TC_THREADS) {
+            const int row = t / (TC_KC / 8), kv = t % (TC_KC / 8);
+            const uint4 val = __ldg(reinterpret_cast<const uint4*>(wmat + (i64)row * Kpad + chunk * TC_KC + kv * 8));
+            *reinterpret_cast<uint4*>(st + tc::kmajor_off(row, kv)) = val;
+        }
+    }
+    __device__ void epilogue(int row, const float* acc, int col0) const {
+        const int v = m0 + row;
+        if (v >= g.voxels()) return;
+        float r[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            float a = acc[q];
+            if (!DGRAD) {
+                if (bias) a += __ldg(bias + col0 + q);
+                if (relu) a = fmaxf(a, 0.0f);
+            }
+            r[q] = a;
+        }
+        if (DGRAD && mask_src) {
+            const uint4* m4 = reinterpret_cast<const uint4*>(mask_src + (i64)v * N + col0);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint4 mv = __ldg(m4 + h);
+                const __nv_bfloat16* mb = reinterpret_cast<const __nv_bfloat16*>(&mv);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (!(__bfloat162float(mb[q]) > 0.0f)) r[8 * h + q] = 0.0f;
+            }
+        }
+        uint4* o4 = reinterpret_cast<uint4*>(out + (i64)v * N + col0);
+        o4[0] = make_uint4(pack_bf16x2(r[0], r[1]), pack_bf16x2(r[2], r[3]), pack_bf16x2(r[4], r[5]),
+                           pack_bf16x2(r[6], r[7]));
+        o4[1] = make_uint4(pack_bf16x2(r[8], r[9]), pack_bf16x2(r[10], r[11]), pack_bf16x2(r[12], r[13]),
+                           pack_bf16x2(r[14], r[15]));
+    }
+};
+
+template <int N, bool DGRAD>
+__global__ void __launch_bounds__(TC_THREADS) k_conv_rows(const __nv_bfloat16* src, const __nv_bfloat16* wmat,
+                                                           const float* bias, const __nv_bfloat16* mask_src,
+                                                           __nv_bfloat16* out, Vol g, int Cs, int Kpad, int relu) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    ConvRows<N, DGRAD> op;
+    op.src = src;
+    op.wmat = wmat;
+    op.bias = bias;
+    op.mask_src = mask_src;
+    op.out = out;
+    op.g = g;
+    op.Cs = Cs;
+    op.K = 27 * Cs;
+    op.Kpad = Kpad;
+    op.chunks = Kpad / TC_KC;
+    op.m0 = blockIdx.x * TC_M;
+    op.relu = relu;
+    op.setup();
+    tc::tile_gemm<ConvRows<N, DGRAD>, N>(op, smem);
+}
+
+// ---- weight gradient: A = x at tap offsets (MN-major over (tap, ci)), B = dy (MN-major over co) ---
+template <int N>
+struct ConvWgrad {
+    static constexpr bool A_MN = true, B_MN = true;
+    const __nv_bfloat16* x;   // [V][Cin]
+    const __nv_bfloat16* dy;  // [V][N]
+    float* dw;                // [27 * Cin][N], accumulated
+    Vol g;
+    int Cin, Mrows, m0, chunk0, chunks;
+    __device__ void gather_a(uint8_t* st, int chunk) const {
+        const int kk = threadIdx.x & (TC_KC - 1);
+        const int v = (chunk0 + chunk) * TC_KC + kk;
+        int b = 0, z = 0, y = 0, xx = 0;
+        const bool valid = v < g.voxels();
+        if (valid) decode(g, v, b, z, y, xx);
+        for (int mv = threadIdx.x / TC_KC; mv < TC_M / 8; mv += TC_THREADS / TC_KC) {
+            const int m = m0 + mv * 8;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (valid && m < Mrows) {
+                const int tap = m / Cin, c = m - tap * Cin;
+                const int nb = tap_neighbour(g, b, z, y, xx, tap, 1);
+                if (nb >= 0) val = __ldg(reinterpret_cast<const uint4*>(x + (i64)nb * Cin + c));
+            }
+            *reinterpret_cast<uint4*>(st + tc::mnmajor_off(mv, kk)) = val;
+        }
+    }
+    __device__ void gather_b(uint8_t* st, int chunk) const {
+        const int kk = threadIdx.x & (TC_KC - 1);
+        const int v = (chunk0 + chunk) * TC_KC + kk;
+        const bool valid = v < g.voxels();
+        for (int nv = threadIdx.x / TC_KC; nv < N / 8; nv += TC_THREADS / TC_KC) {
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (valid) val = __ldg(reinterpret_cast<const uint4*>(dy + (i64)v * N + nv * 8));
+            *reinterpret_cast<uint4*>(st + tc::mnmajor_off(nv, kk)) = val;
+        }
+    }
+    __device__ void epilogue(int row, const float* acc, int col0) const {
+        const int m = m0 + row;
+        if (m >= Mrows) return;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) atomicAdd(dw + (i64)m * N + col0 + q, acc[q]);
+    }
+};
+
+template <int N>
+__global__ void __launch_bounds__(TC_THREADS) k_conv_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dy,
+                                                            float* dw, Vol g, int Cin, int chunks_per_block) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    ConvWgrad<N> op;
+    op.x = x;
+    op.dy = dy;
+    op.dw = dw;
+    op.g = g;
+    op.Cin = Cin;
+    op.Mrows = 27 * Cin;
+    op.m0 = blockIdx.x * TC_M;
+    const int total_chunks = (g.B * g.D * g.H * g.W + TC_KC - 1) / TC_KC;
+    op.chunk0 = blockIdx.y * chunks_per_block;
+    op.chunks = max(0, min(chunks_per_block, total_chunks - op.chunk0));
+    tc::tile_gemm<ConvWgrad<N>, N>(op, smem);
+}
+
+// ---- elementwise pieces of the network ------------------------------------------------------------
+constexpr int EW = 256;
+
+// master weights [27 * Cin][Cout] (fp32) -> forward matrix wf[Cout][Kpad] and data-grad matrix
+// wd[Cin][Kpad2] (bf16, zero-padded along K to multiples of 64)
+__global__ void k_arrange_weights(const float* __restrict__ w, __nv_bfloat16* __restrict__ wf,
+                                  __nv_bfloat16* __restrict__ wd, int Cin, int Cout, int Kpad, int Kpad2) {
+    const int total = Cout * Kpad + (wd ? Cin * Kpad2 : 0);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        if (t < Cout * Kpad) {
+            const int co = t / Kpad, k = t % Kpad;
+            wf[t] = __float2bfloat16_rn(k < 27 * Cin ? w[(i64)k * Cout + co] : 0.0f);
+        } else {
+            const int u = t - Cout * Kpad;
+            const int ci = u / Kpad2, k = u % Kpad2;
+            float val = 0.0f;
+            if (k < 27 * Cout) {
+                const int tap = k / Cout, co = k % Cout;
+                val = w[((i64)tap * Cin + ci) * Cout + co];
+            }
+            wd[u] = __float2bfloat16_rn(val);
+        }
+    }
+}
+
+// 2x2x2 average pooling of a channels-last volume (D, H, W even)
+__global__ void k_avgpool2(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ y, Vol fine, int C) {
+    const i64 total = (i64)fine.B * (fine.D / 2) * (fine.H / 2) * (fine.W / 2) * C;
+    for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
+        const int c = (int)(t % C);
+        i64 v = t / C;
+        const int X = (int)(v % (fine.W / 2));
+        v /= fine.W / 2;
+        const int Y = (int)(v % (fine.H / 2));
+        v /= fine.H / 2;
+        const int Z = (int)(v % (fine.D / 2));
+        const int b = (int)(v / (fine.D / 2));
+        float s = 0.0f;
+        for (int d = 0; d < 8; ++d) {
+            const int z = 2 * Z + (d >> 2), y2 = 2 * Y + ((d >> 1) & 1), x2 = 2 * X + (d & 1);
+            s += __bfloat162float(x[(((i64)(b * fine.D + z) * fine.H + y2) * fine.W + x2) * C + c]);
+        }
+        y[t] = __float2bfloat16_rn(0.125f * s);
+    }
+}
+
+// nearest 2x upsampling of `coarse` (C1 channels) written into channels [0, C1) of `out`, and a copy
+// of `skip` (C2 channels) into channels [C1, C1 + C2): the decoder's concatenated input
+__global__ void k_upsample_concat(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip,
+                                  __nv_bfloat16* __restrict__ out, Vol fine, int C1, int C2) {
+    const int C = C1 + C2;
+    const i64 total = (i64)fine.B * fine.D * fine.H * fine.W * C;
+    for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
+        const int c = (int)(t % C);
+        const i64 v = t / C;
+        if (c < C1) {
+            const int x = (int)(v % fine.W);
+            i64 r = v / fine.W;
+            const int y = (int)(r % fine.H);
+            r /= fine.H;
+            const int z = (int)(r % fine.D);
+            const int b = (int)(r / fine.D);
+            const i64 cv = (((i64)b * (fine.D / 2) + z / 2) * (fine.H / 2) + y / 2) * (fine.W / 2) + x / 2;
+            out[t] = coarse[cv * C1 + c];
+        } else {
+            out[t] = skip[v * C2 + (c - C1)];
+        }
+    }
+}
+
+// backward of k_upsample_concat: d coarse = sum over the 8 children (into FP32 then BF16), d skip +=
+// the copied channels (added to an existing gradient, as the skip tensor also feeds the encoder)
+__global__ void k_upsample_concat_backward(const __nv_bfloat16* __restrict__ dout, __nv_bfloat16* __restrict__ dcoarse,
+                                           __nv_bfloat16* __restrict__ dskip, Vol fine, int C1, int C2) {
+    const int C = C1 + C2;
+    const i64 coarse_total = (i64)fine.B * (fine.D / 2) * (fine.H / 2) * (fine.W / 2) * C1;
+    const i64 skip_total = (i64)fine.B * fine.D * fine.H * fine.W * C2;
+    for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < coarse_total + skip_total;
+         t += (i64)gridDim.x * blockDim.x) {
+        if (t < coarse_total) {
+            const int c = (int)(t % C1);
+            i64 v = t / C1;
+            const int X = (int)(v % (fine.W / 2));
+            v /= fine.W / 2;
+            const int Y = (int)(v % (fine.H / 2));
+            v /= fine.H / 2;
+            const int Z = (int)(v % (fine.D / 2));
+            const int b = (int)(v / (fine.D / 2));
+            float s = 0.0f;
+            for (int d = 0; d < 8; ++d) {
+                const int z = 2 * Z + (d >> 2), y = 2 * Y + ((d >> 1) & 1), x = 2 * X + (d & 1);
+                s += __bfloat162float(dout[(((i64)(b * fine.D + z) * fine.H + y) * fine.W + x) * C + c]);
+            }
+            dcoarse[t] = __float2bfloat16_rn(s);
+        } else {
+            const i64 u = t - coarse_total;
+            const int c = (int)(u % C2);
+            const i64 v = u / C2;
+            dskip[u] = __float2bfloat16_rn(__bfloat162float(dskip[u]) + __bfloat162float(dout[v * C + C1 + c]));
+        }
+    }
+}
+
+// backward of 2x2x2 average pooling: each fine voxel gets 1/8 of its parent's gradient, added to an
+// existing gradient and masked by the ReLU of the pooled activation's producer (x > 0)
+__global__ void k_avgpool2_backward(const __nv_bfloat16* __restrict__ dy, const __nv_bfloat16* __restrict__ x,
+                                    __nv_bfloat16* __restrict__ dx, Vol fine, int C) {
+    const i64 total = (i64)fine.B * fine.D * fine.H * fine.W * C;
+    for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
+        const int c = (int)(t % C);
+        const i64 v = t / C;
+        const int xx = (int)(v % fine.W);
+        i64 r = v / fine.W;
+        const int y = (int)(r % fine.H);
+        r /= fine.H;
+        const int z = (int)(r % fine.D);
+        const int b = (int)(r / fine.D);
+        const i64 cv = (((i64)b * (fine.D / 2) + z / 2) * (fine.H / 2) + y / 2) * (fine.W / 2) + xx / 2;
+        float g = __bfloat162float(dx[t]) + 0.125f * __bfloat162float(dy[cv * C + c]);
+        if (!(__bfloat162float(x[t]) > 0.0f)) g = 0.0f;
+        dx[t] = __float2bfloat16_rn(g);
+    }
+}
+
+// 1x1x1 output head: out[v] = sum_c h[v][c] * w[c] + b (C = 16), and its backward
+__global__ void k_head_forward(const __nv_bfloat16* __restrict__ h, const float* __restrict__ w, const float* bias,
+                               float* __restrict__ out, int V, int C) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        float s = bias[0];
+        for (int c = 0; c < C; ++c) s += __bfloat162float(h[(i64)v * C + c]) * w[c];
+        out[v] = s;
+    }
+}
+
+// dh[v][c] = dout[v] * w[c] masked by (h > 0); dw[c] += sum_v dout[v] h[v][c]; db += sum dout
+__global__ void k_head_backward(const __nv_bfloat16* __restrict__ h, const float* __restrict__ w,
+                                const float* __restrict__ dout, __nv_bfloat16* __restrict__ dh, float* dw, float* db,
+                                int V, int C) {
+    __shared__ float s_dw[64 + 1];
+    for (int c = threadIdx.x; c <= C; c += blockDim.x) s_dw[c] = 0.0f;
+    __syncthreads();
+    float ldw[16] = {0};
+    float ldb = 0.0f;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        const float g = dout[v];
+        ldb += g;
+        for (int c = 0; c < C; ++c) {
+            const float hv = __bfloat162float(h[(i64)v * C + c]);
+            ldw[c & 15] += g * hv;
+            dh[(i64)v * C + c] = __float2bfloat16_rn(hv > 0.0f ? g * w[c] : 0.0f);
+        }
+    }
+    for (int c = 0; c < C; ++c) atomicAdd(&s_dw[c], ldw[c & 15]);
+    atomicAdd(&s_dw[C], ldb);
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(dw + c, s_dw[c]);
+    if (threadIdx.x == 0) atomicAdd(db, s_dw[C]);
+}
+
+// bias gradient of a conv: db[co] += sum_v dy[v][co]
+__global__ void k_bias_grad(const __nv_bfloat16* __restrict__ dy, float* db, int V, int C) {
+    __shared__ float s[256];
+    for (int c = threadIdx.x; c < C; c += blockDim.x) s[c] = 0.0f;
+    __syncthreads();
+    for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < (i64)V * C; t += (i64)gridDim.x * blockDim.x)
+        atomicAdd(&s[t % C], __bfloat162float(dy[t]));
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(db + c, s[c]);
+}
+
+// Adam step (Kingma & Ba) on FP32 master parameters
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, i64 n, float lr, float beta1, float beta2, float eps, float bc1,
+                       float bc2) {
+    for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (i64)gridDim.x * blockDim.x) {
+        const float gt = g[t];
+        const float mt = beta1 * m[t] + (1.0f - beta1) * gt;
+        const float vt = beta2 * v[t] + (1.0f - beta2) * gt * gt;
+        m[t] = mt;
+        v[t] = vt;
+        p[t] -= lr * (mt / bc1) / (sqrtf(vt / bc2) + eps);
+    }
+}
+
+}  // namespace conv
+}  // namespace clb

@@ -254,6 +254,42 @@ int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream);
  * M and K multiples of 8, N one of 16, 32, 64, 128. */
 int clb_tc_test_gemm(const void* a, const void* b, float* c, int M, int N, int K, int mn_major, void* stream);
 
+/* Learned warm start (no counterpart in the reference): 3x3x3 convolutions, padding 1, on
+ * channels-last BF16 volumes [B][D][H][W][C] as implicit GEMMs on tcgen05 with FP32 accumulation.
+ * Taps are ordered (dz, dy, dx), dx fastest. Master weights are FP32 [27 * cin][cout].
+ *  arrange_weights: wf[cout][kpad] (forward) and, when wd != NULL, wd[cin][kpad2] (data grad), BF16,
+ *                   kpad >= 27*cin and kpad2 >= 27*cout multiples of 64, zero-padded.
+ *  forward:  y = act(bias + conv(x)), cin % 8 == 0, cout in {16, 32, 64}, relu = 0/1.
+ *  dgrad:    dx = conv^T(dy) * (mask_x > 0) (mask_x nullable), cout % 8 == 0, cin in {16,32,48,64,96}.
+ *  wgrad:    dw[27*cin][cout] += sum over voxels (FP32 atomics; zero dw first), cout in {16, 32, 64};
+ *            each block reduces chunks_per_block chunks of 64 voxels. */
+int clb_conv3d_arrange_weights(const float* w, void* wf, void* wd, int cin, int cout, int kpad, int kpad2,
+                               void* stream);
+int clb_conv3d_forward(const void* x, const void* wf, const float* bias, void* y, int B, int D, int H, int W, int cin,
+                       int cout, int kpad, int relu, void* stream);
+int clb_conv3d_dgrad(const void* dy, const void* wd, const void* mask_x, void* dx, int B, int D, int H, int W, int cout,
+                     int cin, int kpad, void* stream);
+int clb_conv3d_wgrad(const void* x, const void* dy, float* dw, int B, int D, int H, int W, int cin, int cout,
+                     int chunks_per_block, void* stream);
+/* U-Net elementwise pieces (BF16 channels-last): 2x2x2 average pooling (extents of the fine volume
+ * given) and its backward (adds into dx, then masks by x > 0); nearest 2x upsampling of `coarse`
+ * concatenated with `skip` along channels, and its backward (dcoarse written, dskip added into);
+ * the 1x1x1 output head (FP32 weights, C <= 16) and its backward (dh masked by h > 0, dw and db
+ * accumulated); the bias gradient of a convolution (accumulated); an Adam step on FP32 parameters. */
+int clb_unet_avgpool2(const void* x, void* y, int B, int D, int H, int W, int C, void* stream);
+int clb_unet_avgpool2_backward(const void* dy, const void* x, void* dx, int B, int D, int H, int W, int C,
+                               void* stream);
+int clb_unet_upsample_concat(const void* coarse, const void* skip, void* out, int B, int D, int H, int W, int c1,
+                             int c2, void* stream);
+int clb_unet_upsample_concat_backward(const void* dout, void* dcoarse, void* dskip, int B, int D, int H, int W,
+                                      int c1, int c2, void* stream);
+int clb_unet_head_forward(const void* h, const float* w, const float* b, float* out, int voxels, int C, void* stream);
+int clb_unet_head_backward(const void* h, const float* w, const float* dout, void* dh, float* dw, float* db,
+                           int voxels, int C, void* stream);
+int clb_unet_bias_grad(const void* dy, float* db, int voxels, int C, void* stream);
+int clb_adam_step(float* p, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2, float eps,
+                  int step, void* stream);
+
 /* ---- collider voxelisation (Solver/Kernel/voxelise_mesh.py, OpenCL/voxelise_mesh.cl) ------- */
 
 /* voxelise_mesh.cl:24-48 voxelise_mesh: ORs 1 into mask for interior cells whose centre ray has an
