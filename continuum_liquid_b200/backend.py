@@ -81,6 +81,10 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_unet_head_backward": [P, P, P, P, P, P, I, I, P],
     "clb_unet_bias_grad": [P, P, I, I, P],
     "clb_adam_step": [P, P, P, P, L, F, F, F, F, I, P],
+    "clb_unet_pack_input": [P, P, P, P, F, F, I, I, I, I, I, I, P, I, I, I, I, P],
+    "clb_unet_pack_target": [P, P, P, F, I, I, I, I, I, I, P, P, I, I, I, I, P],
+    "clb_unet_unpack_output": [P, P, P, F, P, I, I, I, I, I, I, P],
+    "clb_unet_mse": [P, P, P, P, P, L, F, P],
     "clb_voxelise_mesh": [P, P, I, I, I, I, F, F, F, F, I, P],
     "clb_voxelise_direction": [P],
 }

@@ -972,6 +972,46 @@ int clb_adam_step(float* p, const float* g, float* m, float* v, int64_t n, float
     return 0;
 }
 
+int clb_unet_pack_input(const float* b, const uint8_t* op0, const uint8_t* solid, const float* p, float scale_b,
+                        float inv_s, int nx, int ny, int nz, int oi, int oj, int ok, void* x0, int slot, int D, int H,
+                        int W, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(b && op0 && p && x0 && slot >= 0, "unet_pack_input: bad arguments");
+    conv::k_pack_input<<<ew_blocks((i64)D * H * W), conv::EW, 0, CLB_STREAM(stream)>>>(
+        b, op0, solid, p, scale_b, inv_s, nx, ny, nz, oi, oj, ok, (__nv_bfloat16*)x0, slot, D, H, W);
+    CLB_LAUNCH_CHECK("k_pack_input");
+    return 0;
+}
+
+int clb_unet_pack_target(const float* p, const float* p_prev, const uint8_t* op0, float inv_s, int nx, int ny,
+                         int nz, int oi, int oj, int ok, float* t, float* m, int slot, int D, int H, int W,
+                         void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(p && p_prev && op0 && t && m && slot >= 0, "unet_pack_target: bad arguments");
+    conv::k_pack_target<<<ew_blocks((i64)D * H * W), conv::EW, 0, CLB_STREAM(stream)>>>(
+        p, p_prev, op0, inv_s, nx, ny, nz, oi, oj, ok, t, m, slot, D, H, W);
+    CLB_LAUNCH_CHECK("k_pack_target");
+    return 0;
+}
+
+int clb_unet_unpack_output(const float* out, const float* p_prev, const uint8_t* op0, float s, float* p, int nx,
+                           int ny, int nz, int D, int H, int W, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(out && p_prev && op0 && p && D >= nx && H >= ny && W >= nz, "unet_unpack_output: bad arguments");
+    conv::k_unpack_output<<<ew_blocks((i64)nx * ny * nz), conv::EW, 0, CLB_STREAM(stream)>>>(out, p_prev, op0, s, p, nx,
+                                                                                           ny, nz, D, H, W);
+    CLB_LAUNCH_CHECK("k_unpack_output");
+    return 0;
+}
+
+int clb_unet_mse(const float* out, const float* t, const float* m, float* dout, float* loss, int64_t n, float inv_count,
+                 void* stream) {
+    CLB_REQUIRE(out && t && m && dout && loss && n >= 0, "unet_mse: bad arguments");
+    conv::k_mse<<<ew_blocks(n), conv::EW, 0, CLB_STREAM(stream)>>>(out, t, m, dout, loss, n, inv_count);
+    CLB_LAUNCH_CHECK("k_mse");
+    return 0;
+}
+
 // ---- voxelisation ---------------------------------------------------------------------------------
 
 int clb_voxelise_direction(float* out3) {

@@ -388,5 +388,79 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
     }
 }
 
+// Network input from the solver's finest level: channels (b * scale_b, fluid, solid, p * inv_s,
+// 0, 0, 0, 0) of grid cell (oi + z, oj + y, ok + x) into voxel (z, y, x) of batch slot `slot` of a
+// [B][D][H][W][8] volume; cells outside the grid are 0.
+__global__ void k_pack_input(const float* __restrict__ b, const uint8_t* __restrict__ op0,
+                             const uint8_t* __restrict__ solid, const float* __restrict__ p, float scale_b,
+                             float inv_s, int nx, int ny, int nz, int oi, int oj, int ok, __nv_bfloat16* __restrict__ x0,
+                             int slot, int D, int H, int W) {
+    const i64 V = (i64)D * H * W;
+    for (i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (i64)gridDim.x * blockDim.x) {
+        const int xx = (int)(v % W), y = (int)((v / W) % H), z = (int)(v / ((i64)W * H));
+        const int i = oi + z, j = oj + y, k = ok + xx;
+        float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, c3 = 0.0f;
+        if (i >= 0 && i < nx && j >= 0 && j < ny && k >= 0 && k < nz) {
+            const i64 c = ((i64)i * ny + j) * nz + k;
+            const bool fl = (__ldg(op0 + c) & 64u) != 0u;
+            c0 = fl ? __ldg(b + c) * scale_b : 0.0f;
+            c1 = fl ? 1.0f : 0.0f;
+            c2 = (solid && __ldg(solid + c)) ? 1.0f : 0.0f;
+            c3 = fl ? __ldg(p + c) * inv_s : 0.0f;
+        }
+        uint4* dst = reinterpret_cast<uint4*>(x0 + ((i64)slot * V + v) * 8);
+        *dst = make_uint4(pack_bf16x2(c0, c1), pack_bf16x2(c2, c3), 0u, 0u);
+    }
+}
+
+// Training target and loss weight of one batch slot: t = (p - p_prev) * inv_s and m = 1 at fluid
+// cells (the network predicts the change of the pressure since the previous step).
+__global__ void k_pack_target(const float* __restrict__ p, const float* __restrict__ p_prev,
+                              const uint8_t* __restrict__ op0, float inv_s, int nx, int ny, int nz, int oi, int oj,
+                              int ok, float* __restrict__ t, float* __restrict__ m, int slot, int D, int H, int W) {
+    const i64 V = (i64)D * H * W;
+    for (i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (i64)gridDim.x * blockDim.x) {
+        const int xx = (int)(v % W), y = (int)((v / W) % H), z = (int)(v / ((i64)W * H));
+        const int i = oi + z, j = oj + y, k = ok + xx;
+        float tv = 0.0f, mv = 0.0f;
+        if (i >= 0 && i < nx && j >= 0 && j < ny && k >= 0 && k < nz) {
+            const i64 c = ((i64)i * ny + j) * nz + k;
+            if (__ldg(op0 + c) & 64u) {
+                tv = (__ldg(p + c) - __ldg(p_prev + c)) * inv_s;
+                mv = 1.0f;
+            }
+        }
+        t[(i64)slot * V + v] = tv;
+        m[(i64)slot * V + v] = mv;
+    }
+}
+
+// Network output of voxel (i, j, k) (batch slot 0) back to the grid: p = p_prev + out * s at fluid
+// cells (in FP32, so the previous pressure keeps its precision), 0 elsewhere.
+__global__ void k_unpack_output(const float* __restrict__ out, const float* __restrict__ p_prev,
+                                const uint8_t* __restrict__ op0, float s, float* __restrict__ p, int nx, int ny, int nz,
+                                int D, int H, int W) {
+    const i64 C = (i64)nx * ny * nz;
+    for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < C; c += (i64)gridDim.x * blockDim.x) {
+        const int k = (int)(c % nz), j = (int)((c / nz) % ny), i = (int)(c / ((i64)ny * nz));
+        const bool fl = (__ldg(op0 + c) & 64u) != 0u;
+        p[c] = fl ? __ldg(p_prev + c) + __ldg(out + ((i64)i * H + j) * W + k) * s : 0.0f;
+    }
+}
+
+// Masked mean squared error: dout = 2 m (out - t) / count, loss += sum m (out - t)^2 / count.
+__global__ void k_mse(const float* __restrict__ out, const float* __restrict__ t, const float* __restrict__ m,
+                      float* __restrict__ dout, float* loss, i64 n, float inv_count) {
+    float acc = 0.0f;
+    for (i64 v = (i64)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (i64)gridDim.x * blockDim.x) {
+        const float d = (out[v] - t[v]) * m[v];
+        dout[v] = 2.0f * d * inv_count;
+        acc += d * d * inv_count;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc);
+}
+
 }  // namespace conv
 }  // namespace clb

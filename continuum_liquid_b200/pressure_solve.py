@@ -66,6 +66,8 @@ class SolveStats:
     ms: float = 0.0
     history: list = field(default_factory=list)
     events: tuple | None = None  # CUDA events bracketing the solve on its stream
+    warm_start: str = "previous"  # initial guess used: "previous" step's pressure or "learned"
+    learned_rel_residual: float | None = None  # relative residual of the network's guess, when tried
 
     def device_ms(self) -> float:
         """Device time of the solve from its CUDA events (synchronises on the end event)."""
@@ -156,9 +158,13 @@ class PressureSolver:
 
     # -- solves ---------------------------------------------------------------------------------
     def solve(self, velocity, fluid_fraction, pressure, dt, rho, num_vcycles: int = 1, tol: float | None = None,
-              use_graph: bool = True, measure: bool = False) -> SolveStats:
+              use_graph: bool = True, measure: bool = False, warm_start=None, solid=None) -> SolveStats:
         """Solve for ``pressure`` in place (warm-started from its current contents) and apply the
-        Neumann ghost copy. ``tol=None`` runs ``num_vcycles`` W-cycles (reference semantics)."""
+        Neumann ghost copy. ``tol=None`` runs ``num_vcycles`` W-cycles (reference semantics).
+
+        ``warm_start`` (tolerance mode): a callable (rhs, op0, solid, p_prev) -> candidate pressure or
+        None; the candidate replaces the previous-step pressure as the initial guess only when its
+        FP64 relative residual is lower."""
         stats = SolveStats()
         t0 = time.perf_counter()
         stats.events = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -181,6 +187,15 @@ class PressureSolver:
             self.cur = 0
             self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64[0], *self.grid_shape)
             rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
+            if warm_start is not None:
+                guess = warm_start(self.rhs, h.op0, solid, pressure)
+                if guess is not None:
+                    rel_net = self.relative_residual(guess)
+                    stats.learned_rel_residual = rel_net
+                    if rel_net < rel:
+                        self.kernels.call("clb_mg_ir_init", guess, h.op0, self.p64[0], *self.grid_shape)
+                        rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
+                        stats.warm_start = "learned"
             stats.initial_rel_residual = rel
             stats.history.append(rel)
             rate = None

@@ -50,6 +50,7 @@ class StepOptions:
     rho: float = 1000.0
     nu: float = 1.0e-6
     use_graph: bool = True
+    warm_start: object = None  # callable proposing an initial pressure (learned.LearnedWarmStart)
 
 
 class FlipSolver:
@@ -119,7 +120,8 @@ class FlipSolver:
         o = self.options
         stats = self.pressure_solver.solve((self.u, self.v, self.w), self.fluid_fraction, self.pressure, self.dt,
                                            o.rho, num_vcycles=o.num_vcycles if num_vcycles is None else num_vcycles,
-                                           tol=o.tol if tol is None else tol, use_graph=o.use_graph)
+                                           tol=o.tol if tol is None else tol, use_graph=o.use_graph,
+                                           warm_start=o.warm_start, solid=self.obstacle)
         self.last_solve = stats
         return stats
 

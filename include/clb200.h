@@ -290,6 +290,24 @@ int clb_unet_bias_grad(const void* dy, float* db, int voxels, int C, void* strea
 int clb_adam_step(float* p, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2, float eps,
                   int step, void* stream);
 
+/* Network input/output next to the solver (no counterpart in the reference): pack_input writes
+ * channels (b*scale_b, fluid, solid, p*inv_s, 0, 0, 0, 0) of grid cell (oi+z, oj+y, ok+x) into
+ * voxel (z, y, x) of batch slot `slot` of a [B][D][H][W][8] BF16 volume (0 outside the grid; solid
+ * nullable); pack_target writes t = (p - p_prev)*inv_s and the loss weight m = fluid;
+ * unpack_output writes p = p_prev + out*s at fluid cells (0 elsewhere) from batch slot 0 of a
+ * [D][H][W] FP32 volume; mse computes dout = 2 m (out - t) / count and adds
+ * sum m (out - t)^2 / count to *loss. */
+int clb_unet_pack_input(const float* b, const uint8_t* op0, const uint8_t* solid, const float* p, float scale_b,
+                        float inv_s, int nx, int ny, int nz, int oi, int oj, int ok, void* x0, int slot, int D, int H,
+                        int W, void* stream);
+int clb_unet_pack_target(const float* p, const float* p_prev, const uint8_t* op0, float inv_s, int nx, int ny,
+                         int nz, int oi, int oj, int ok, float* t, float* m, int slot, int D, int H, int W,
+                         void* stream);
+int clb_unet_unpack_output(const float* out, const float* p_prev, const uint8_t* op0, float s, float* p, int nx,
+                           int ny, int nz, int D, int H, int W, void* stream);
+int clb_unet_mse(const float* out, const float* t, const float* m, float* dout, float* loss, int64_t n, float inv_count,
+                 void* stream);
+
 /* ---- collider voxelisation (Solver/Kernel/voxelise_mesh.py, OpenCL/voxelise_mesh.cl) ------- */
 
 /* voxelise_mesh.cl:24-48 voxelise_mesh: ORs 1 into mask for interior cells whose centre ray has an
