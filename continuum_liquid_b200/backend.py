@@ -52,6 +52,8 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_pressure_rhs": [P, P, P, P, P, F, F, I, I, I, P],
     "clb_pressure_correction": [P, P, P, P, F, F, I, I, I, P],
     "clb_neumann_domain_bc": [P, I, I, I, P],
+    "clb_pressure_correction_f64": [P, P, P, P, F, F, I, I, I, P],
+    "clb_neumann_domain_bc_f64": [P, I, I, I, P],
     "clb_build_finest_operator": [P, P, P, P, P, I, I, I, P],
     "clb_rbgs_step": [P, P, P, P, P, P, P, F, I, I, I, I, P],
     "clb_restrict_residual": [P] * 14 + [F, I, I, I, I, I, I, P],
@@ -66,6 +68,8 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_residual_norms": [P, I, P, P, F, I, I, I, P, P, P, P],
     "clb_mg_ir_init": [P, P, P, I, I, I, P],
     "clb_mg_ir_step": [P, P, P, P, P, F, I, I, I, P, P, P, P],
+    "clb_mg_fcg_dots": [P, P, P, P, F, I, I, I, P, P, P],
+    "clb_mg_fcg_step": [P, P, P, P, P, P, P, P, F, I, I, I, P, P, P, P],
     "clb_mg_ir_update": [P, P, L, P],
     "clb_mg_ir_store": [P, P, L, P],
     "clb_tc_test_gemm": [P, P, P, I, I, I, I, P],

@@ -21,7 +21,7 @@ using namespace clb;
                 (nz));                                                                                 \
     CLB_REQUIRE((i64)(nx) * (ny) * (nz) < (1ll << 31), "grid %dx%dx%d has more than 2^31 cells", (nx), (ny), (nz))
 
-static const int kAbiVersion = 3;
+static const int kAbiVersion = 4;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 
@@ -326,24 +326,46 @@ int clb_pressure_rhs(const float* u, const float* v, const float* w, const float
     return 0;
 }
 
-int clb_pressure_correction(float* u, float* v, float* w, const float* pressure, float dt_over_rho, float inv_dx,
-                            int nx, int ny, int nz, void* stream) {
+extern "C++" {
+template <typename PT>
+static int pressure_correction_impl(float* u, float* v, float* w, const PT* pressure, float dt_over_rho,
+                                    float inv_dx, int nx, int ny, int nz, void* stream) {
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(u && v && w && pressure, "pressure_correction: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_pressure_correction<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, pressure, dt_over_rho, inv_dx, nx,
-                                                                             ny, nz);
+    k_pressure_correction<PT><<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, pressure, dt_over_rho,
+                                                                                 inv_dx, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_pressure_correction");
     return 0;
 }
 
-int clb_neumann_domain_bc(float* pressure, int nx, int ny, int nz, void* stream) {
+template <typename PT>
+static int neumann_domain_bc_impl(PT* pressure, int nx, int ny, int nz, void* stream) {
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(pressure, "neumann_domain_bc: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_neumann_domain_bc<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(pressure, nx, ny, nz);
+    k_neumann_domain_bc<PT><<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(pressure, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_neumann_domain_bc");
     return 0;
+}
+}  // extern "C++"
+
+int clb_pressure_correction(float* u, float* v, float* w, const float* pressure, float dt_over_rho, float inv_dx,
+                            int nx, int ny, int nz, void* stream) {
+    return pressure_correction_impl<float>(u, v, w, pressure, dt_over_rho, inv_dx, nx, ny, nz, stream);
+}
+
+int clb_pressure_correction_f64(float* u, float* v, float* w, const double* pressure, float dt_over_rho,
+                                float inv_dx, int nx, int ny, int nz, void* stream) {
+    return pressure_correction_impl<double>(u, v, w, pressure, dt_over_rho, inv_dx, nx, ny, nz, stream);
+}
+
+int clb_neumann_domain_bc(float* pressure, int nx, int ny, int nz, void* stream) {
+    return neumann_domain_bc_impl<float>(pressure, nx, ny, nz, stream);
+}
+
+int clb_neumann_domain_bc_f64(double* pressure, int nx, int ny, int nz, void* stream) {
+    return neumann_domain_bc_impl<double>(pressure, nx, ny, nz, stream);
 }
 
 // ---- multigrid, reference layout ----------------------------------------------------------------
@@ -707,11 +729,11 @@ int clb_mg_residual_norms(const void* p, int p_is_double, const float* b, const 
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
     if (p_is_double)
-        k_residual_rows<double, false><<<blocks, RN_THREADS, 0, s>>>((const double*)p, nullptr, nullptr, b, op0,
+        k_residual_rows<double, RES_NORM><<<blocks, RN_THREADS, 0, s>>>((const double*)p, nullptr, nullptr, b, op0,
                                                                      inv_delta2, nx, ny, nz, r_out,
                                                                      (double2*)partials);
     else
-        k_residual_rows<float, false><<<blocks, RN_THREADS, 0, s>>>((const float*)p, nullptr, nullptr, b, op0,
+        k_residual_rows<float, RES_NORM><<<blocks, RN_THREADS, 0, s>>>((const float*)p, nullptr, nullptr, b, op0,
                                                                     inv_delta2, nx, ny, nz, r_out, (double2*)partials);
     CLB_LAUNCH_CHECK("k_residual_rows");
     k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
@@ -728,8 +750,42 @@ int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const 
     const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    k_residual_rows<double, true><<<blocks, RN_THREADS, 0, s>>>(p64_in, e, p64_out, b, op0, inv_delta2, nx, ny, nz,
-                                                                r_out, (double2*)partials);
+    k_residual_rows<double, RES_IR><<<blocks, RN_THREADS, 0, s>>>(p64_in, e, p64_out, b, op0, inv_delta2, nx, ny,
+                                                                  nz, r_out, (double2*)partials);
+    CLB_LAUNCH_CHECK("k_residual_rows");
+    k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
+    CLB_LAUNCH_CHECK("k_reduce_partials");
+    return 0;
+}
+
+int clb_mg_fcg_dots(const float* z, const float* d, const float* r, const uint8_t* op0, float delta, int nx, int ny,
+                    int nz, void* partials4, double* state, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(z && d && r && op0 && partials4 && state, "mg_fcg_dots: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    const int blocks = clb_mg_residual_partials(C);
+    const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
+    cudaStream_t s = CLB_STREAM(stream);
+    k_fcg_dots<<<blocks, RN_THREADS, 0, s>>>(z, d, r, op0, inv_delta2, nx, ny, nz, (Sum4*)partials4);
+    CLB_LAUNCH_CHECK("k_fcg_dots");
+    k_fcg_scalars<<<1, 256, 0, s>>>((const Sum4*)partials4, blocks, state);
+    CLB_LAUNCH_CHECK("k_fcg_scalars");
+    return 0;
+}
+
+int clb_mg_fcg_step(const double* p64_in, const float* z, const float* d_in, double* p64_out, float* d_out,
+                    const double* state, const float* b, const uint8_t* op0, float delta, int nx, int ny, int nz,
+                    float* r_out, void* partials, double* out, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(p64_in && z && d_in && p64_out && d_out && state && b && op0 && r_out && partials && out,
+                "mg_fcg_step: null pointer");
+    CLB_REQUIRE(p64_in != p64_out && d_in != d_out, "mg_fcg_step: outputs must not alias inputs");
+    const i64 C = (i64)nx * ny * nz;
+    const int blocks = clb_mg_residual_partials(C);
+    const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
+    cudaStream_t s = CLB_STREAM(stream);
+    k_residual_rows<double, RES_FCG><<<blocks, RN_THREADS, 0, s>>>(p64_in, z, p64_out, b, op0, inv_delta2, nx, ny,
+                                                                   nz, r_out, (double2*)partials, d_in, d_out, state);
     CLB_LAUNCH_CHECK("k_residual_rows");
     k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");

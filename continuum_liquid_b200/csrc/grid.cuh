@@ -151,9 +151,13 @@ __global__ void __launch_bounds__(GT) k_pressure_rhs(const float* __restrict__ u
     rhs[c] = rhs_at(u, v, w, c, (i64)ny * nz, nz, rho_over_dt, inv_dx);
 }
 
-// pressure_solve.cl:26-47 pressure_correction (helper.cl:25-37 gradient)
+// pressure_solve.cl:26-47 pressure_correction (helper.cl:25-37 gradient). PT = float is the
+// reference's arithmetic; PT = double takes the gradient of an FP64 pressure in FP64 and rounds the
+// updated velocity once (the projection of a refined solve, whose FP64 pressure is the one that
+// meets the residual tolerance).
+template <typename PT>
 __global__ void __launch_bounds__(GT) k_pressure_correction(float* __restrict__ u, float* __restrict__ v,
-                                                             float* __restrict__ w, const float* __restrict__ p,
+                                                             float* __restrict__ w, const PT* __restrict__ p,
                                                              float dt_over_rho, float inv_dx, int nx, int ny, int nz) {
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
@@ -161,17 +165,18 @@ __global__ void __launch_bounds__(GT) k_pressure_correction(float* __restrict__ 
     int i, j, k;
     gcoord(c, ny, nz, i, j, k);
     if (!interior(i, j, k, nx, ny, nz)) return;
-    const float center = __ldg(p + c);
-    const float gx = (__ldg(p + c + (i64)ny * nz) - center) * inv_dx;
-    const float gy = (__ldg(p + c + nz) - center) * inv_dx;
-    const float gz = (__ldg(p + c + 1) - center) * inv_dx;
-    u[c] -= dt_over_rho * gx;
-    v[c] -= dt_over_rho * gy;
-    w[c] -= dt_over_rho * gz;
+    const PT center = __ldg(p + c);
+    const PT gx = (__ldg(p + c + (i64)ny * nz) - center) * (PT)inv_dx;
+    const PT gy = (__ldg(p + c + nz) - center) * (PT)inv_dx;
+    const PT gz = (__ldg(p + c + 1) - center) * (PT)inv_dx;
+    u[c] = (float)((PT)u[c] - (PT)dt_over_rho * gx);
+    v[c] = (float)((PT)v[c] - (PT)dt_over_rho * gy);
+    w[c] = (float)((PT)w[c] - (PT)dt_over_rho * gz);
 }
 
 // boundary_conditions.cl:18-31 neumann_domain_bc (ghosts read interior cells only)
-__global__ void __launch_bounds__(GT) k_neumann_domain_bc(float* p, int nx, int ny, int nz) {
+template <typename PT>
+__global__ void __launch_bounds__(GT) k_neumann_domain_bc(PT* p, int nx, int ny, int nz) {
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
     if (c >= C) return;

@@ -452,25 +452,40 @@ constexpr int RN_THREADS = 256;
 // FP64 residual over the finest level, one (i, j) row per warp (lanes stride along k, so there is no
 // per-cell index division). Per block: sums of r^2 and b^2 over interior fluid cells, with
 // r = b - A p evaluated in FP64 (A is multigrid.cl:25-43 apply_operator).
-//  STEP = false: p is the float or double pressure p_in.
-//  STEP = true:  the refinement update fused in: p = p_in + e is formed on the fly for the cell and
-//                its neighbours and written to p_out (which must not alias p_in).
+//  MODE 0 (RES_NORM): p is the float or double pressure p_in.
+//  MODE 1 (RES_IR):   the refinement update fused in: p = p_in + e is formed on the fly for the cell
+//                     and its neighbours and written to p_out (which must not alias p_in).
+//  MODE 2 (RES_FCG):  the flexible-CG update fused in: the search direction d = e + beta d_in
+//                     (rounded to float, written to d_out) and p = p_in + alpha d, with alpha and
+//                     beta read from state[0] and state[1] (k_fcg_scalars).
 // When r_out is given the residual is stored rounded to float at every cell (0 outside interior
 // fluid cells): it is the right-hand side of the next correction solve.
-template <typename PT, bool STEP>
+enum { RES_NORM = 0, RES_IR = 1, RES_FCG = 2 };
+
+template <typename PT, int MODE>
 __global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restrict__ p_in,
                                                                const float* __restrict__ e,
                                                                double* __restrict__ p_out,
                                                                const float* __restrict__ b,
                                                                const uint8_t* __restrict__ op0, double inv_delta2,
                                                                int nx, int ny, int nz, float* __restrict__ r_out,
-                                                               double2* __restrict__ partials) {
+                                                               double2* __restrict__ partials,
+                                                               const float* __restrict__ d_in = nullptr,
+                                                               float* __restrict__ d_out = nullptr,
+                                                               const double* __restrict__ state = nullptr) {
     __shared__ double2 s_red[RN_THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int sx = ny * nz, sy = nz;
     double rr = 0.0, bb = 0.0;
+    double alpha = 0.0, beta = 0.0;
+    if (MODE == RES_FCG) {
+        alpha = state[0];
+        beta = state[1];
+    }
+    auto dv = [&](int q) -> float { return (float)((double)__ldg(e + q) + beta * (double)__ldg(d_in + q)); };
     auto pv = [&](int q) -> double {
-        if (STEP) return (double)__ldg(p_in + q) + (double)__ldg(e + q);
+        if (MODE == RES_IR) return (double)__ldg(p_in + q) + (double)__ldg(e + q);
+        if (MODE == RES_FCG) return (double)__ldg(p_in + q) + alpha * (double)dv(q);
         return (double)__ldg(p_in + q);
     };
     const int rows = nx * ny;
@@ -481,7 +496,8 @@ __global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restri
         for (int k = lane; k < nz; k += 32) {
             const int c = base + k;
             const double pc = pv(c);
-            if (STEP) p_out[c] = pc;
+            if (MODE != RES_NORM) p_out[c] = pc;
+            if (MODE == RES_FCG) d_out[c] = dv(c);
             const uint32_t o = __ldg(op0 + c);
             float rf = 0.0f;
             if (row_in && k >= 1 && k <= nz - 2 && (o & 64u)) {
@@ -512,6 +528,111 @@ __global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restri
             t.y += s_red[q].y;
         }
         partials[blockIdx.x] = t;
+    }
+}
+
+// Flexible conjugate gradients with the W-cycle as preconditioner (Notay's FCG with truncation 1;
+// no counterpart in the reference, which runs W-cycles only). For the preconditioned residual
+// z = e (one W-cycle on A e = r from e = 0) and the previous direction d, one block's partial sums
+// over interior fluid cells of
+//   x = (A z) . d     (= z . A d, the operator is symmetric)
+//   y = (A z) . z,    z_ = z . r,    w = d . r
+// with A z evaluated in FP64. The next direction is d' = z + beta d, beta = -(z . A d) / (d . A d),
+// so d' . A d' and d' . r follow from these four sums and the previous d . A d without storing A d.
+struct Sum4 {
+    double x, y, z, w;
+};
+
+__global__ void __launch_bounds__(RN_THREADS) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
+                                                          const float* __restrict__ r,
+                                                          const uint8_t* __restrict__ op0, double inv_delta2, int nx,
+                                                          int ny, int nz, Sum4* __restrict__ partials) {
+    __shared__ Sum4 s_red[RN_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sx = ny * nz, sy = nz;
+    Sum4 t = {0.0, 0.0, 0.0, 0.0};
+    const int rows = nx * ny;
+    for (int q = blockIdx.x * (RN_THREADS / 32) + warp; q < rows; q += gridDim.x * (RN_THREADS / 32)) {
+        const int i = q / ny, j = q - i * ny;
+        if (i < 1 || i > nx - 2 || j < 1 || j > ny - 2) continue;
+        const int base = q * nz;
+        for (int k = lane; k < nz; k += 32) {
+            const int c = base + k;
+            const uint32_t o = __ldg(op0 + c);
+            if (k < 1 || k > nz - 2 || !(o & 64u)) continue;
+            const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
+            const double zc = (double)__ldg(z + c);
+            const double ws = (double)bitf(o, 3) * (double)__ldg(z + c + sx) +
+                              (double)bitf(ox, 3) * (double)__ldg(z + c - sx) +
+                              (double)bitf(o, 4) * (double)__ldg(z + c + sy) +
+                              (double)bitf(oy, 4) * (double)__ldg(z + c - sy) +
+                              (double)bitf(o, 5) * (double)__ldg(z + c + 1) +
+                              (double)bitf(oz, 5) * (double)__ldg(z + c - 1);
+            const double az = (ws - (double)(o & 7u) * zc) * inv_delta2;
+            const double dc = (double)__ldg(d + c), rc = (double)__ldg(r + c);
+            t.x += az * dc;
+            t.y += az * zc;
+            t.z += zc * rc;
+            t.w += dc * rc;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+        t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+        t.z += __shfl_xor_sync(0xffffffffu, t.z, o);
+        t.w += __shfl_xor_sync(0xffffffffu, t.w, o);
+    }
+    if (lane == 0) s_red[warp] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Sum4 a = s_red[0];
+        for (int q = 1; q < RN_THREADS / 32; ++q) {
+            a.x += s_red[q].x;
+            a.y += s_red[q].y;
+            a.z += s_red[q].z;
+            a.w += s_red[q].w;
+        }
+        partials[blockIdx.x] = a;
+    }
+}
+
+// Fixed-order sum of the k_fcg_dots partials, then the FCG scalars in
+// state = {alpha, beta, d.Ad of the current direction, 1 once a direction exists}.
+// The first direction is z itself (beta = 0).
+__global__ void k_fcg_scalars(const Sum4* __restrict__ partials, int count, double* __restrict__ state) {
+    __shared__ Sum4 s[256];
+    Sum4 t = {0.0, 0.0, 0.0, 0.0};
+    for (int q = threadIdx.x; q < count; q += 256) {
+        t.x += partials[q].x;
+        t.y += partials[q].y;
+        t.z += partials[q].z;
+        t.w += partials[q].w;
+    }
+    s[threadIdx.x] = t;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s[threadIdx.x].x += s[threadIdx.x + o].x;
+            s[threadIdx.x].y += s[threadIdx.x + o].y;
+            s[threadIdx.x].z += s[threadIdx.x + o].z;
+            s[threadIdx.x].w += s[threadIdx.x + o].w;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const Sum4 a = s[0];
+        const bool has = state[3] != 0.0 && state[2] != 0.0;
+        double beta = 0.0, dad = a.y, dr = a.z;
+        if (has) {
+            beta = -a.x / state[2];
+            dad = a.y + 2.0 * beta * a.x + beta * beta * state[2];
+            dr = a.z + beta * a.w;
+        }
+        state[0] = dad != 0.0 ? dr / dad : 0.0;
+        state[1] = beta;
+        state[2] = dad;
+        state[3] = 1.0;
     }
 }
 

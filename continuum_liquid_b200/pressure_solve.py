@@ -9,9 +9,15 @@ build_finest_operator, ``num_vcycles`` W-cycles, Neumann ghost copy) on the refe
 * tolerance mode (``tol=1e-6``): mixed-precision iterative refinement. The pressure is accumulated
   in FP64; each refinement computes the FP64 residual r = b - A p (and its norm), solves A e = r
   with one FP32 W-cycle from e = 0 and adds e to p, until ||r||_2 / ||b||_2 <= tol over the
-  interior fluid cells. A W-cycle is an affine map, so this is the same iteration as running
-  W-cycles on p, with the rounding of the FP32 residual (which cannot reach 1e-6 by itself)
-  removed.
+  interior fluid cells. A W-cycle is an affine map, so ``method="refine"`` is the same iteration
+  as running W-cycles on p, with the rounding of the FP32 residual (which cannot reach 1e-6 by
+  itself) removed. ``method="fcg"`` (the default) applies the same W-cycle corrections along
+  flexible conjugate-gradient directions (Notay's FCG with truncation 1), which needs fewer
+  W-cycles for the same tolerance; the accumulation, residual and norms stay FP64.
+
+The solution of a tolerance-mode solve is the FP64 pressure (``pressure64``): its float32
+rounding, written to ``pressure``, cannot hold a relative residual of 1e-6 on fine grids, so the
+projection uses the FP64 pressure when one exists.
 """
 
 from __future__ import annotations
@@ -77,22 +83,30 @@ class SolveStats:
         return self.events[0].elapsed_time(self.events[1])
 
 
+METHODS = ("fcg", "refine")
+
+
 class PressureSolver:
     """Packed-layout pressure solve for one grid (allocates its workspace once).
 
-    In tolerance mode one refinement is: e = 0; one W-cycle on A e = r; p64 <- p64 + e fused with
-    the FP64 residual r = b - A p64 and its norms (clb_mg_ir_step). The FP64 pressure alternates
-    between two buffers, so two CUDA graphs (one per direction) capture the refinement. The host
-    reads the residual norm only when the refinement count predicted from the observed contraction
-    rate has run, so most refinements are replayed back to back without a host round trip.
+    In tolerance mode one refinement is: e = 0; one W-cycle on A e = r; then either
+    p64 <- p64 + e (``refine``, clb_mg_ir_step) or the flexible-CG update along d = e + beta d
+    (``fcg``, clb_mg_fcg_dots + clb_mg_fcg_step), each fused with the FP64 residual r = b - A p64
+    and its norms. The FP64 pressure (and the FCG direction) alternate between two buffers, so two
+    CUDA graphs (one per direction) capture the refinement. The host reads the residual norm only
+    when the refinement count predicted from the observed contraction rate has run, so most
+    refinements are replayed back to back without a host round trip.
     """
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100,
-                 autotune: bool = True):
+                 autotune: bool = True, method: str = "fcg"):
+        if method not in METHODS:
+            raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.kernels = kernels
         self.grid_shape = tuple(int(s) for s in grid_shape)
         self.dx = float(dx)
         self.max_cycles = int(max_cycles)
+        self.method = method
         self.hierarchy = multigrid.MultigridHierarchy(kernels, self.grid_shape, dx, min_size)
         device = kernels.device
         self.cells = int(np.prod(self.grid_shape))
@@ -101,6 +115,13 @@ class PressureSolver:
         self.correction = torch.zeros(self.grid_shape, dtype=torch.float32, device=device)
         self.p64 = [torch.zeros(self.grid_shape, dtype=torch.float64, device=device) for _ in range(2)]
         self.cur = 0  # index of the FP64 buffer holding the current pressure
+        # flexible-CG direction (ping-pong like p64), scalars {alpha, beta, d.Ad, has_direction} and
+        # the partial sums of its dot products (4 doubles per block)
+        self.direction = [torch.zeros(self.grid_shape, dtype=torch.float32, device=device) for _ in range(2)]
+        self.fcg_state = torch.zeros(4, dtype=torch.float64, device=device)
+        blocks = kernels.residual_partials(self.cells)
+        self.fcg_partials = torch.zeros(4 * blocks, dtype=torch.float64, device=device)
+        self.solved64 = False  # whether pressure64 holds the last solve's FP64 pressure
         self.norms_host = torch.zeros(2, dtype=torch.float64, pin_memory=True)
         self._graphs: list[torch.cuda.CUDAGraph | None] = [None, None]
         self.autotune = autotune
@@ -124,34 +145,48 @@ class PressureSolver:
         """FP64 ||b - A p|| / ||b|| of a float32 or float64 pressure against the prepared system."""
         return self._relative(self.hierarchy.residual_norms(pressure, self.rhs, queue=queue))
 
+    @property
+    def pressure64(self) -> torch.Tensor:
+        """The FP64 pressure of the last tolerance-mode solve (0 off the interior fluid)."""
+        return self.p64[self.cur]
+
     def refine_once(self, src: int, queue=None) -> None:
         """One refinement from FP64 buffer ``src`` into the other one."""
         h = self.hierarchy
+        delta = float(FIELD_DTYPE(self.dx))
         self.correction.zero_()
         h.w_cycle(self.correction, self.residual, queue=queue)
-        self.kernels.call("clb_mg_ir_step", self.p64[src], self.correction, self.p64[1 - src], self.rhs, h.op0,
-                          float(FIELD_DTYPE(self.dx)), *self.grid_shape, self.residual, h.partials, h.norms,
-                          stream=queue)
+        if self.method == "fcg":
+            self.kernels.call("clb_mg_fcg_dots", self.correction, self.direction[src], self.residual, h.op0, delta,
+                              *self.grid_shape, self.fcg_partials, self.fcg_state, stream=queue)
+            self.kernels.call("clb_mg_fcg_step", self.p64[src], self.correction, self.direction[src],
+                              self.p64[1 - src], self.direction[1 - src], self.fcg_state, self.rhs, h.op0, delta,
+                              *self.grid_shape, self.residual, h.partials, h.norms, stream=queue)
+        else:
+            self.kernels.call("clb_mg_ir_step", self.p64[src], self.correction, self.p64[1 - src], self.rhs, h.op0,
+                              delta, *self.grid_shape, self.residual, h.partials, h.norms, stream=queue)
 
     def _refine(self, use_graph: bool) -> None:
         src = self.cur
         if not use_graph:
             self.refine_once(src)
+        elif self._graphs[src] is None:
+            # the first refinement in this direction runs eagerly on a side stream (warming up the
+            # launches), then is captured without being replayed
+            stream = torch.cuda.current_stream(self.kernels.device)
+            side = torch.cuda.Stream(self.kernels.device)
+            side.wait_stream(stream)
+            with torch.cuda.stream(side):
+                self.refine_once(src)
+            stream.wait_stream(side)
+            graph = torch.cuda.CUDAGraph()
+            before = self.kernels.launch_count()
+            with torch.cuda.graph(graph):
+                self.refine_once(src)
+            # +1: the correction zero-fill is a torch kernel captured with ours
+            self.graph_launches = self.kernels.launch_count() - before + 1
+            self._graphs[src] = graph
         else:
-            if self._graphs[src] is None:
-                stream = torch.cuda.current_stream(self.kernels.device)
-                side = torch.cuda.Stream(self.kernels.device)
-                side.wait_stream(stream)
-                with torch.cuda.stream(side):
-                    self.refine_once(src)  # warm-up outside capture (the result is recomputed below)
-                stream.wait_stream(side)
-                graph = torch.cuda.CUDAGraph()
-                before = self.kernels.launch_count()
-                with torch.cuda.graph(graph):
-                    self.refine_once(src)
-                # +1: the correction zero-fill is a torch kernel captured with ours
-                self.graph_launches = self.kernels.launch_count() - before + 1
-                self._graphs[src] = graph
             self._graphs[src].replay()
             self.graph_replays += 1
         self.cur = 1 - src
@@ -178,6 +213,7 @@ class PressureSolver:
             tune_hierarchy(h, self.correction, self.residual)
             self.tuned = True
         if tol is None:
+            self.solved64 = False
             for _ in range(int(num_vcycles)):
                 h.w_cycle(pressure, self.rhs)
             stats.cycles = int(num_vcycles)
@@ -185,6 +221,9 @@ class PressureSolver:
                 stats.rel_residual = self.relative_residual(pressure)
         else:
             self.cur = 0
+            if self.method == "fcg":
+                self.direction[0].zero_()
+                self.fcg_state.zero_()
             self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64[0], *self.grid_shape)
             rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
             if warm_start is not None:
@@ -214,6 +253,8 @@ class PressureSolver:
                 rate = (rel / previous) ** (1.0 / batch) if previous > 0 and stats.cycles > 1 else None
             stats.rel_residual = rel
             self.kernels.call("clb_mg_ir_store", self.p64[self.cur], pressure, self.cells)
+            self.kernels.call("clb_neumann_domain_bc_f64", self.p64[self.cur], *self.grid_shape)
+            self.solved64 = True
         boundary_conditions.neumann_domain_bc(self.kernels, None, pressure, self.grid_shape)
         stats.events[1].record()
         stats.ms = (time.perf_counter() - t0) * 1e3

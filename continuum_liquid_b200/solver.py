@@ -51,6 +51,7 @@ class StepOptions:
     nu: float = 1.0e-6
     use_graph: bool = True
     warm_start: object = None  # callable proposing an initial pressure (learned.LearnedWarmStart)
+    method: str = "fcg"  # tolerance-mode iteration: "fcg" (W-cycle preconditioned CG) or "refine"
 
 
 class FlipSolver:
@@ -88,7 +89,8 @@ class FlipSolver:
                 else obstacle
             if bool(ob.any()):
                 self.obstacle = ob.to(dev).contiguous()
-        self.pressure_solver = PressureSolver(kernels, self.grid_shape, self.dx, min_size=min_size)
+        self.pressure_solver = PressureSolver(kernels, self.grid_shape, self.dx, min_size=min_size,
+                                              method=self.options.method)
         self.last_solve: SolveStats | None = None
         self.steps_done = 0
 
@@ -129,7 +131,13 @@ class FlipSolver:
         """Stages 6-7: projection, BCs and the fused particle update."""
         k, o, gs = self.kernels, self.options, self.grid_shape
         vel = (self.u, self.v, self.w)
-        pressure_correction(k, queue, vel, self.pressure, self.dx, self.dt, o.rho, gs)
+        ps = self.pressure_solver
+        if ps.solved64:
+            # a tolerance-mode solve: project with the FP64 pressure that meets the tolerance
+            k.call("clb_pressure_correction_f64", *vel, ps.pressure64, float(np.float32(self.dt / o.rho)),
+                   float(np.float32(1.0 / self.dx)), *gs, stream=queue)
+        else:
+            pressure_correction(k, queue, vel, self.pressure, self.dx, self.dt, o.rho, gs)
         boundary_conditions.grid_domain_bc(k, queue, vel, gs)
         if self.obstacle is not None:
             boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)

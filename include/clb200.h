@@ -144,6 +144,13 @@ int clb_pressure_correction(float* u, float* v, float* w, const float* pressure,
 
 /* boundary_conditions.cl:18-31 neumann_domain_bc (boundary_conditions.py:22-33). */
 int clb_neumann_domain_bc(float* pressure, int nx, int ny, int nz, void* stream);
+/* The same two steps on an FP64 pressure (no counterpart in the reference): the gradient is taken
+ * in FP64 and the updated velocity rounded once to float. Used to project with the FP64 pressure
+ * of a refined solve, which is the one that meets the residual tolerance (its float32 rounding
+ * alone leaves a relative residual of order 1e-6 at 48^3 and more on finer grids). */
+int clb_pressure_correction_f64(float* u, float* v, float* w, const double* pressure, float dt_over_rho,
+                                float inv_dx, int nx, int ny, int nz, void* stream);
+int clb_neumann_domain_bc_f64(double* pressure, int nx, int ny, int nz, void* stream);
 
 /* ---- multigrid, reference layout (float32 mask/diagonal/weight arrays per level) -------------- */
 
@@ -245,6 +252,24 @@ int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const 
                    float delta, int nx, int ny, int nz, float* r_out, void* partials, double* out, void* stream);
 int clb_mg_ir_update(double* p64, const float* e, int64_t cells, void* stream);
 int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream);
+
+/* Flexible conjugate gradients preconditioned by one W-cycle (no counterpart in the reference; the
+ * same FP64 accumulation as the refinement steps above, with the correction applied along
+ * conjugate directions). For z = the W-cycle's correction e of the current residual r (float32,
+ * the r_out of the previous step), d_in = the previous direction (float32, zeroed before the
+ * first iteration) and state = double[4] {alpha, beta, d.Ad, has_direction} (zeroed before the
+ * first iteration):
+ *  dots: sums over interior fluid cells of (A z).d, (A z).z, z.r, d.r into partials4
+ *        (clb_mg_residual_partials(cells) * 32 bytes), then beta = -(A z).d / d.Ad (0 for the
+ *        first direction), d' = z + beta d, alpha = d'.r / d'.Ad' into state.
+ *  step: d_out = d' (float32), p64_out = p64_in + alpha d', r_out = b - A p64_out (FP64, rounded
+ *        to float), out = [sum r^2, sum b^2]; outputs must not alias inputs.
+ * With alpha = 1 and beta = 0 the step is clb_mg_ir_step. */
+int clb_mg_fcg_dots(const float* z, const float* d, const float* r, const uint8_t* op0, float delta, int nx, int ny,
+                    int nz, void* partials4, double* state, void* stream);
+int clb_mg_fcg_step(const double* p64_in, const float* z, const float* d_in, double* p64_out, float* d_out,
+                    const double* state, const float* b, const uint8_t* op0, float delta, int nx, int ny, int nz,
+                    float* r_out, void* partials, double* out, void* stream);
 
 /* ---- tensor cores -------------------------------------------------------------------------- */
 

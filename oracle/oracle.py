@@ -325,6 +325,66 @@ def fp64_pressure_solve(rhs, ff, shape, dx, tol=1e-12, max_cycles=200, p0=None):
     return p, history
 
 
+def apply_operator64(p, mask, op0, delta):
+    """A p in FP64 at interior fluid cells (0 elsewhere) for the finest-level operator arrays op0
+    (multigrid.cl:7-43 weighted_neighbor_sum / apply_operator)."""
+    d, wx, wy, wz = (np.asarray(a, np.float64) for a in op0)
+    p = np.asarray(p, np.float64)
+    fluid = np.zeros(p.shape, bool)
+    fluid[1:-1, 1:-1, 1:-1] = np.asarray(mask)[1:-1, 1:-1, 1:-1] > 0
+    ws = np.zeros_like(p)
+    I = (slice(1, -1),) * 3
+    ws[I] = (wx[I] * p[2:, 1:-1, 1:-1] + wx[:-2, 1:-1, 1:-1] * p[:-2, 1:-1, 1:-1]
+             + wy[I] * p[1:-1, 2:, 1:-1] + wy[1:-1, :-2, 1:-1] * p[1:-1, :-2, 1:-1]
+             + wz[I] * p[1:-1, 1:-1, 2:] + wz[1:-1, 1:-1, :-2] * p[1:-1, 1:-1, :-2])
+    return np.where(fluid, (ws - d * p) * (1.0 / (float(delta) * float(delta))), 0.0), fluid
+
+
+def fcg_solve(rhs, ff, shape, dx, p0=None, tol=1e-6, max_cycles=100, flexible=True):
+    """Flexible CG (Notay, truncation 1) preconditioned by one FP32 W-cycle from zero, with the
+    pressure, residual and scalars in FP64 (the product's tolerance-mode iteration; the reference
+    has no counterpart). ``flexible=False`` is plain refinement p += W(r). Returns the FP64
+    pressure and the relative-residual history (one entry per W-cycle, the first for p0)."""
+    levels = Levels(shape)
+    ff32 = c(ff)
+    op32 = build_finest_operator(ff32, shape)
+    op64 = build_finest_operator(c(ff, np.float64), shape, np.float64)
+    fluid = apply_operator64(np.zeros(shape), ff32, op64, dx)[1]
+    b = np.where(fluid, c(rhs, np.float64), 0.0)
+    x = np.zeros(shape) if p0 is None else np.where(fluid, c(p0, np.float64), 0.0)
+    nb = float(np.sqrt(np.sum(b * b)))
+
+    def residual(x):
+        return b - apply_operator64(x, ff32, op64, dx)[0]
+
+    r = residual(x)
+    hist = [float(np.sqrt(np.sum(r * r))) / nb if nb else 0.0]
+    d = np.zeros(shape, np.float32)
+    dad = 0.0
+    while hist[-1] > tol and len(hist) <= max_cycles:
+        r32 = r.astype(np.float32)
+        e = np.zeros(shape, np.float32)
+        levels.w_cycle(e, r32, ff32, op32, F32(float(dx)))
+        z = np.where(fluid, e, np.float32(0)).astype(np.float64)
+        if flexible:
+            az = apply_operator64(z, ff32, op64, dx)[0]
+            sx, sy = float(np.sum(az * d)), float(np.sum(az * z))
+            sz, sw = float(np.sum(z * r32)), float(np.sum(d.astype(np.float64) * r32))
+            if dad != 0.0:
+                beta = -sx / dad
+                dad, dr = sy + 2.0 * beta * sx + beta * beta * dad, sz + beta * sw
+            else:
+                beta, dad, dr = 0.0, sy, sz
+            alpha = dr / dad if dad != 0.0 else 0.0
+            d = (z + beta * d.astype(np.float64)).astype(np.float32)
+            x = x + alpha * d.astype(np.float64)
+        else:
+            x = x + z
+        r = residual(x)
+        hist.append(float(np.sqrt(np.sum(r * r))) / nb)
+    return x, hist
+
+
 # ---- the whole step ----------------------------------------------------------------------------
 class OracleSim:
     """solver.py:308-510 restated step for step on the CPU (obstacle passes always run, as in the

@@ -374,3 +374,40 @@ def test_float32_w_cycle_contracts(oracle):
         rels.append(oracle.relative_residual(p, b, mask, op, dx))
     assert all(r1 < 0.8 * r0 for r0, r1 in zip(rels, rels[1:]))
     assert (mask <= 0).sum() and not p[mask <= 0].any()  # air and ghost pressure held at 0
+
+
+def test_operator_apply_matches_dense_operator(oracle):
+    n, dx = 12, 1.0 / 12.0
+    shape = (n, n, n)
+    mask = liquid_mask(n, 11)
+    rng = np.random.default_rng(12)
+    p = rng.standard_normal(shape) * (mask > 0)
+    op = oracle.build_finest_operator(mask.astype(np.float64), shape, np.float64)
+    got, fluid = oracle.apply_operator64(p, mask, op, dx)
+    A, cells = dense_operator(mask, dx)
+    x = np.array([p[c] for c in cells])
+    want = A @ x
+    assert fluid.sum() == len(cells)
+    np.testing.assert_allclose([got[c] for c in cells], want, rtol=1e-12, atol=1e-9 * np.abs(want).max())
+
+
+def test_fcg_restatement(oracle):
+    """The FCG restatement reports the true FP64 residual of its pressure, reaches the tolerance in
+    fewer W-cycles than refinement, and with flexible=False is exactly W-cycles on the pressure."""
+    n, dx = 18, np.float32(1.0 / 18.0)
+    shape = (n, n, n)
+    mask = liquid_mask(n, 9)
+    rng = np.random.default_rng(13)
+    b = (rng.standard_normal(shape) * (mask > 0)).astype(np.float32)
+    x, hist = oracle.fcg_solve(b, mask, shape, dx, tol=1e-8, max_cycles=60)
+    _, hist_ref = oracle.fcg_solve(b, mask, shape, dx, tol=1e-8, max_cycles=60, flexible=False)
+    op64 = oracle.build_finest_operator(mask.astype(np.float64), shape, np.float64)
+    assert hist[-1] <= 1e-8 and hist_ref[-1] <= 1e-8
+    assert oracle.relative_residual(x, b.astype(np.float64), mask.astype(np.float64), op64, float(dx)) == \
+        pytest.approx(hist[-1], rel=1e-6)
+    assert len(hist) < len(hist_ref)
+    # refinement from zero: its first iterate is one FP32 W-cycle on the pressure
+    x1, _ = oracle.fcg_solve(b, mask, shape, dx, tol=0.0, max_cycles=1, flexible=False)
+    p = np.zeros(shape, np.float32)
+    oracle.Levels(shape).w_cycle(p, b, mask, oracle.build_finest_operator(mask, shape), dx)
+    assert np.array_equal(x1, np.where(mask > 0, p, 0).astype(np.float64))

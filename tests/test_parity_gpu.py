@@ -341,13 +341,14 @@ def test_packed_w_cycle_equals_reference(backend, oracle, shape):
     assert norms[0] == pytest.approx(rr, rel=1e-12) and norms[1] == pytest.approx(bb, rel=1e-12)
 
 
-def test_iterative_refinement_reaches_tolerance(backend, oracle):
+@pytest.mark.parametrize("method", ["fcg", "refine"])
+def test_iterative_refinement_reaches_tolerance(backend, oracle, method):
     shape, dx = (34, 34, 34), F32(1.0 / 34)
     rng = np.random.default_rng(17)
     u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
     ff, _, _ = random_system(shape, 18)
     dt, rho = 1.0 / 240.0, 1000.0
-    ps = pressure_solve.PressureSolver(backend, shape, float(dx))
+    ps = pressure_solve.PressureSolver(backend, shape, float(dx), method=method)
     P = torch.zeros(shape, dtype=torch.float32, device="cuda")
     stats = ps.solve((dev(u), dev(v), dev(w)), dev(ff), P, dt, rho, tol=1e-6)
     assert stats.rel_residual <= 1e-6
@@ -358,11 +359,88 @@ def test_iterative_refinement_reaches_tolerance(backend, oracle):
     interior = ff > 0
     err = np.abs(got[interior] - p64[interior]).max() / np.abs(p64[interior]).max()
     assert err < 1e-5
+    # the FP64 pressure is the solution: its own residual is the reported one
+    assert ps.solved64
+    got64 = host(ps.pressure64)
+    err64 = np.abs(got64[interior] - p64[interior]).max() / np.abs(p64[interior]).max()
+    assert err64 < 1e-5
+    assert ps.relative_residual(ps.pressure64) == pytest.approx(stats.rel_residual, rel=1e-9)
     # air cells inside the domain hold zero pressure; ghosts carry the Neumann copy
     inner = np.zeros(shape, bool)
     inner[1:-1, 1:-1, 1:-1] = True
     assert not got[inner & (ff <= 0)].any()
     assert np.array_equal(got, oracle.neumann_domain_bc(got, shape))
+
+
+@pytest.mark.parametrize("method", ["fcg", "refine"])
+def test_refinement_history_matches_oracle(backend, oracle, method):
+    """Every W-cycle of the GPU iteration against the oracle's restatement (same FP32 W-cycle,
+    FP64 accumulation and scalars; only summation orders differ)."""
+    shape, dx = (34, 30, 38), F32(1.0 / 34)
+    rng = np.random.default_rng(5)
+    u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
+    ff, _, _ = random_system(shape, 6)
+    dt, rho = 1.0 / 240.0, 1000.0
+    ps = pressure_solve.PressureSolver(backend, shape, float(dx), method=method, autotune=False)
+    P = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    ps.solve((dev(u), dev(v), dev(w)), dev(ff), P, dt, rho, tol=1e-3, use_graph=False)  # builds the system
+    h = ps.hierarchy
+    p0 = rng.standard_normal(shape).astype(F32) * 10.0
+    ps.cur = 0
+    backend.call("clb_mg_ir_init", dev(p0), h.op0, ps.p64[0], *shape)
+    got = [ps._relative(h.residual_norms(ps.p64[0], ps.rhs, r_out=ps.residual))]
+    ps.direction[0].zero_()
+    ps.fcg_state.zero_()
+    for _ in range(8):
+        ps._refine(use_graph=False)
+        got.append(ps._relative(h.norms))
+    orhs = oracle.pressure_rhs(u, v, w, ff, dx, dt, rho, shape)
+    x, want = oracle.fcg_solve(orhs, ff, shape, dx, p0=p0, tol=0.0, max_cycles=8, flexible=(method == "fcg"))
+    np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-14)  # FP64 summation orders differ
+    assert want[-1] < 1e-3 * want[0]
+    scale = np.abs(x).max()
+    np.testing.assert_allclose(host(ps.pressure64), x, rtol=0, atol=1e-9 * scale)
+
+
+def test_fcg_needs_fewer_cycles_than_refinement(backend):
+    s = scenes.block(48)
+    counts = {}
+    for method in ("refine", "fcg"):
+        opts = solver.StepOptions(flip_ratio=0.95, tol=1e-6, gravity=s.gravity, method=method)
+        pos, vel = scenes.seed_particles(s)
+        sim = solver.FlipSolver(backend, s.grid_shape, s.dx, pos, vel, dt=s.dt, options=opts)
+        stats = [sim.step() for _ in range(6)]
+        assert all(st.rel_residual <= 1e-6 for st in stats)
+        counts[method] = sum(st.cycles for st in stats)
+    assert counts["fcg"] < counts["refine"], counts
+
+
+def test_fp64_projection_matches_numpy(backend):
+    shape = (20, 18, 22)
+    rng = np.random.default_rng(3)
+    u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
+    p = rng.standard_normal(shape) * 1e3
+    dtr, inv_dx = F32(1.0 / 240.0 / 1000.0), F32(20.0)
+    U, V, W = dev(u), dev(v), dev(w)
+    P = torch.from_numpy(p).cuda()
+    backend.call("clb_neumann_domain_bc_f64", P, *shape)
+    backend.call("clb_pressure_correction_f64", U, V, W, P, float(dtr), float(inv_dx), *shape)
+    q = p.copy()
+    nx, ny, nz = shape
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                if not (0 < i < nx - 1 and 0 < j < ny - 1 and 0 < k < nz - 1):
+                    q[i, j, k] = p[min(max(i, 1), nx - 2), min(max(j, 1), ny - 2), min(max(k, 1), nz - 2)]
+    assert np.array_equal(host(P), q)
+    I = (slice(1, -1),) * 3
+    want = [a.copy() for a in (u, v, w)]
+    grads = (q[2:, 1:-1, 1:-1], q[1:-1, 2:, 1:-1], q[1:-1, 1:-1, 2:])
+    for a, nb in zip(want, grads):
+        g = (nb - q[I]) * np.float64(inv_dx)
+        a[I] = (a[I].astype(np.float64) - np.float64(dtr) * g).astype(F32)
+    for got, a in zip((U, V, W), want):
+        assert np.array_equal(host(got), a)
 
 
 # ---- voxelisation ---------------------------------------------------------------------------------
