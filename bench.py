@@ -58,7 +58,52 @@ def parse_args():
     ap.add_argument("--learned", choices=["auto", "on", "off"], default="auto",
                     help="learned warm start in the timed steps (auto: when trained weights exist)")
     ap.add_argument("--poisson-steps", type=int, default=3, help="steps of the Poisson comparison (0: skip)")
+    ap.add_argument("--case", choices=["step", "sweep0"], default="step",
+                    help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
+                         "(no particles: a small-memory case for profiling the dominant kernel)")
+    ap.add_argument("--sweeps", type=int, default=4, help="red-black iterations of --case sweep0")
     return ap.parse_args()
+
+
+def sweep_case(args):
+    """Level-0 red-black Gauss-Seidel iterations on the block scene's liquid mask (random right-hand side),
+    with the autotuned sweep kind; prints one JSON line with the device time per iteration."""
+    import torch
+
+    from continuum_liquid_b200 import scenes
+    from continuum_liquid_b200.autotune import tune_hierarchy
+    from continuum_liquid_b200.backend import Backend
+    from continuum_liquid_b200.pressure_solve import PressureSolver
+
+    kernels = Backend(0)
+    scene = scenes.block(args.size)
+    centres = [(np.arange(n, dtype=np.float64) + 0.5) * scene.dx for n in scene.grid_shape]
+    X, Y, Z = np.meshgrid(*centres, indexing="ij")
+    liquid = scene.sources[0].region(X, Y, Z)
+    liquid[[0, -1], :, :] = liquid[:, [0, -1], :] = liquid[:, :, [0, -1]] = False
+    ff = torch.from_numpy(liquid.astype(np.float32)).cuda()
+    del X, Y, Z
+    zero = torch.zeros(scene.grid_shape, dtype=torch.float32, device="cuda")
+    ps = PressureSolver(kernels, scene.grid_shape, scene.dx, min_size=scene.min_size, autotune=False)
+    ps.prepare((zero, zero, zero), ff, scene.dt, scene.rho)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    ps.rhs.copy_(torch.randn(scene.grid_shape, device="cuda", generator=gen) * ff)
+    h = ps.hierarchy
+    tune_hierarchy(h, ps.correction, ps.residual)
+    p = torch.zeros_like(zero)
+    h.smooth(0, 2, p, ps.rhs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("sweeps")
+    e0.record()
+    h.smooth(0, args.sweeps, p, ps.rhs)
+    e1.record()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.sweeps
+    cells = scene.cells
+    print(json.dumps({"case": "sweep0", "grid": list(scene.grid_shape), "sweep_kind": h.sweeps()[0],
+                      "ms_per_iteration": ms, "algorithmic_gb_s": 13.0 * cells / (ms * 1e-3) / 1e9}), flush=True)
 
 
 def workload_config(size, n_particles, args):
@@ -291,20 +336,13 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
 
 def our_arm(args):
     import torch
-    import torch.distributed as dist
 
     from continuum_liquid_b200 import scenes, solver
     from continuum_liquid_b200.backend import Backend
+    from continuum_liquid_b200.replicas import ReplicaGroup, throughput
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        torch.cuda.set_device(local)
-        import datetime
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    group = ReplicaGroup("nccl")
+    world, rank, local = group.world, group.rank, group.local_rank
     kernels = Backend(local)
     dev = kernels.device
     scene = scenes.block(args.size)
@@ -317,16 +355,7 @@ def our_arm(args):
                             options=opts, min_size=scene.min_size)
     n = sim.n
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = group.barrier
 
     for _ in range(args.warmup):
         sim.step()
@@ -350,13 +379,12 @@ def our_arm(args):
         torch.cuda.synchronize()
         barrier()
     clock_summary = clocks.summary()
-    elapsed_ms = max_over_ranks(start.elapsed_time(end))
+    value, elapsed_ms = throughput(group, args.steps, start.elapsed_time(end))
     direct_launches = kernels.launch_count() - launches0
     replays = sim.pressure_solver.graph_replays - replays0
     gpu_launches = direct_launches + replays * sim.pressure_solver.graph_launches
     cycles = [s.cycles for s in stats]
     solve_ms = [s.device_ms() for s in stats]
-    value = world * args.steps / (elapsed_ms / 1e3)
 
     # --- Poisson time to 1e-6: timed steps, then each iteration on the same systems ------------
     poisson = {"timed_steps": {"method": args.method, "learned": warm_note, "ms_mean": float(np.mean(solve_ms)),
@@ -392,8 +420,8 @@ def our_arm(args):
         e2.record()
         torch.cuda.synchronize()
         barrier()
-        e2e_ms = max_over_ranks(s2.elapsed_time(e2))
-        e2e = {"value": world * e2e_steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+        e2e_value, _ = throughput(group, e2e_steps, s2.elapsed_time(e2))
+        e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
                "d2h_bytes_per_step": 24 * n, "steps": e2e_steps,
                "path": "FlipSolver.step with the particle state copied from pinned host buffers before and back "
                        "after every step (the reference's per-step host round trip of solver.py:252-306)"}
@@ -465,14 +493,15 @@ def our_arm(args):
             "gpu_launches": int(gpu_launches),
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    group.close()
 
 
 def main():
     args = parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.case == "sweep0":
+        sweep_case(args)
     else:
         our_arm(args)
 

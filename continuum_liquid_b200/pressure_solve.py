@@ -220,42 +220,51 @@ class PressureSolver:
             if measure:
                 stats.rel_residual = self.relative_residual(pressure)
         else:
-            self.cur = 0
-            if self.method == "fcg":
-                self.direction[0].zero_()
-                self.fcg_state.zero_()
-            self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64[0], *self.grid_shape)
-            rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
-            if warm_start is not None:
-                guess = warm_start(self.rhs, h.op0, solid, pressure)
-                if guess is not None:
-                    rel_net = self.relative_residual(guess)
-                    stats.learned_rel_residual = rel_net
-                    if rel_net < rel:
-                        self.kernels.call("clb_mg_ir_init", guess, h.op0, self.p64[0], *self.grid_shape)
-                        rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
-                        stats.warm_start = "learned"
-            stats.initial_rel_residual = rel
-            stats.history.append(rel)
-            rate = None
-            while rel > tol and stats.cycles < self.max_cycles:
-                # refinements to run before the next host check: one less than predicted, at least 1
-                batch = 1
-                if rate is not None and 0.0 < rate < 1.0:
-                    batch = max(1, int(math.ceil(math.log(tol / rel) / math.log(rate))) - 1)
-                batch = min(batch, self.max_cycles - stats.cycles, 8)
-                for _ in range(batch):
-                    self._refine(use_graph)
-                previous = rel
-                stats.cycles += batch
-                rel = self._relative(h.norms)
-                stats.history.append(rel)
-                rate = (rel / previous) ** (1.0 / batch) if previous > 0 and stats.cycles > 1 else None
-            stats.rel_residual = rel
-            self.kernels.call("clb_mg_ir_store", self.p64[self.cur], pressure, self.cells)
-            self.kernels.call("clb_neumann_domain_bc_f64", self.p64[self.cur], *self.grid_shape)
-            self.solved64 = True
+            self.solve_prepared(pressure, tol, use_graph=use_graph, warm_start=warm_start, solid=solid, stats=stats)
         boundary_conditions.neumann_domain_bc(self.kernels, None, pressure, self.grid_shape)
         stats.events[1].record()
         stats.ms = (time.perf_counter() - t0) * 1e3
+        return stats
+
+    def solve_prepared(self, pressure, tol: float, use_graph: bool = True, warm_start=None, solid=None,
+                       stats: SolveStats | None = None) -> SolveStats:
+        """The tolerance-mode iteration on the system already in ``rhs`` and the hierarchy (after
+        ``prepare``), from the initial guess ``pressure`` (float32, updated with the result)."""
+        stats = stats or SolveStats()
+        h = self.hierarchy
+        self.cur = 0
+        if self.method == "fcg":
+            self.direction[0].zero_()
+            self.fcg_state.zero_()
+        self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64[0], *self.grid_shape)
+        rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
+        if warm_start is not None:
+            guess = warm_start(self.rhs, h.op0, solid, pressure)
+            if guess is not None:
+                rel_net = self.relative_residual(guess)
+                stats.learned_rel_residual = rel_net
+                if rel_net < rel:
+                    self.kernels.call("clb_mg_ir_init", guess, h.op0, self.p64[0], *self.grid_shape)
+                    rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
+                    stats.warm_start = "learned"
+        stats.initial_rel_residual = rel
+        stats.history.append(rel)
+        rate = None
+        while rel > tol and stats.cycles < self.max_cycles:
+            # refinements to run before the next host check: one less than predicted, at least 1
+            batch = 1
+            if rate is not None and 0.0 < rate < 1.0:
+                batch = max(1, int(math.ceil(math.log(tol / rel) / math.log(rate))) - 1)
+            batch = min(batch, self.max_cycles - stats.cycles, 8)
+            for _ in range(batch):
+                self._refine(use_graph)
+            previous = rel
+            stats.cycles += batch
+            rel = self._relative(h.norms)
+            stats.history.append(rel)
+            rate = (rel / previous) ** (1.0 / batch) if previous > 0 and stats.cycles > 1 else None
+        stats.rel_residual = rel
+        self.kernels.call("clb_mg_ir_store", self.p64[self.cur], pressure, self.cells)
+        self.kernels.call("clb_neumann_domain_bc_f64", self.p64[self.cur], *self.grid_shape)
+        self.solved64 = True
         return stats
