@@ -58,6 +58,9 @@ def parse_args():
     ap.add_argument("--learned", choices=["auto", "on", "off"], default="auto",
                     help="learned warm start in the timed steps (auto: when trained weights exist)")
     ap.add_argument("--poisson-steps", type=int, default=3, help="steps of the Poisson comparison (0: skip)")
+    ap.add_argument("--coarse-fp16", choices=["auto", "on", "off"], default="auto",
+                    help="FP16 storage of the coarse levels <= 64^3 in the timed steps (auto: when the Poisson "
+                         "comparison shows the convergence factor and time hold)")
     ap.add_argument("--case", choices=["step", "sweep0"], default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
                          "(no particles: a small-memory case for profiling the dominant kernel)")
@@ -264,15 +267,18 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
 
     solvers = {m: PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=min_size, method=m)
                for m in ("refine", "fcg")}
+    solvers["fcg_fp16"] = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg",
+                                         coarse_fp16=True)
     p_tmp = torch.empty_like(sim.pressure)
-    rows = {"refine": [], "fcg": [], "fcg_learned": []}
+    rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": []}
     fp32 = []
     rho = sim.options.rho
     for _ in range(steps):
         sim.pre_solve()
         saved = sim.pressure.clone()
         vel = (sim.u, sim.v, sim.w)
-        variants = [("refine", solvers["refine"], None), ("fcg", solvers["fcg"], None)]
+        variants = [("refine", solvers["refine"], None), ("fcg", solvers["fcg"], None),
+                    ("fcg_fp16", solvers["fcg_fp16"], None)]
         if warm is not None:
             variants.append(("fcg_learned", solvers["fcg"], warm))
         for name, ps, ws in variants:
@@ -281,7 +287,9 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                 st = ps.solve(vel, sim.fluid_fraction, p_tmp, sim.dt, rho, tol=TOL, warm_start=ws, solid=sim.obstacle)
             rows[name].append({"ms": st.device_ms(), "cycles": st.cycles, "rel": st.rel_residual,
                                "guess": st.warm_start, "learned_rel": st.learned_rel_residual,
-                               "initial_rel": st.initial_rel_residual})
+                               "initial_rel": st.initial_rel_residual,
+                               "factor": (st.rel_residual / st.initial_rel_residual) ** (1.0 / st.cycles)
+                               if st.cycles and st.initial_rel_residual else None})
         # the reference method: FP32 W-cycles on the FP32 pressure (FP64 residual read after each)
         ps = solvers["refine"]
         p_tmp.copy_(saved)
@@ -321,13 +329,23 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             continue
         out[name] = {"ms_mean": mean(rs, "ms"), "cycles_mean": mean(rs, "cycles"),
                      "rel_max": max(r["rel"] for r in rs), "cycles": [r["cycles"] for r in rs],
-                     "ms": [round(r["ms"], 3) for r in rs]}
+                     "ms": [round(r["ms"], 3) for r in rs],
+                     "convergence_factor_mean": mean(rs, "factor")}
         if name == "fcg_learned":
             out[name]["guess_used"] = [r["guess"] for r in rs]
             out[name]["learned_rel"] = [r["learned_rel"] for r in rs]
             out[name]["previous_rel"] = [r["initial_rel"] for r in rows["fcg"]]
     if rows["refine"] and rows["fcg"]:
         out["speedup_fcg_vs_refine"] = out["refine"]["ms_mean"] / out["fcg"]["ms_mean"]
+    if rows["fcg_fp16"]:
+        f16, f32 = out["fcg_fp16"], out["fcg"]
+        f16["fp16_levels"] = [list(sh) for sh in solvers["fcg_fp16"].hierarchy.shapes[
+            solvers["fcg_fp16"].hierarchy.fp16_level:]] if solvers["fcg_fp16"].hierarchy.fp16_level else []
+        f16["operator_inexact_entries"] = solvers["fcg_fp16"].hierarchy.fp16_inexact_entries()
+        # the rule: FP16 coarse storage where the measured convergence factor holds (no more cycles) and it
+        # is not slower
+        out["coarse_fp16_holds"] = bool(f16["fp16_levels"]) and f16["cycles_mean"] <= f32["cycles_mean"] and \
+            f16["ms_mean"] <= f32["ms_mean"] * 1.01
     if rows["fcg_learned"]:
         out["speedup_learned_vs_plain_fcg"] = out["fcg"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
         out["speedup_learned_vs_refine"] = out["refine"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
@@ -361,6 +379,25 @@ def our_arm(args):
         sim.step()
     torch.cuda.synchronize()
 
+    # --- Poisson comparison on the next steps' systems; it also decides FP16 coarse storage ----
+    poisson = {}
+    use_fp16 = args.coarse_fp16 == "on"
+    if args.poisson_steps > 0:
+        poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
+        if args.coarse_fp16 == "auto":
+            use_fp16 = poisson.get("coarse_fp16_holds", False)
+    else:
+        poisson["learned_vs_plain"] = "skipped (--poisson-steps 0)"
+    if use_fp16:
+        from continuum_liquid_b200.pressure_solve import PressureSolver
+
+        sim.options.coarse_fp16 = True
+        sim.pressure_solver = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=scene.min_size,
+                                             method=args.method, coarse_fp16=True)
+        for _ in range(2):  # tuning and graph capture of the new solver
+            sim.step()
+        torch.cuda.synchronize()
+
     # --- device-resident timed region -------------------------------------------------------
     stats = []
     solve_ms = []
@@ -386,18 +423,15 @@ def our_arm(args):
     cycles = [s.cycles for s in stats]
     solve_ms = [s.device_ms() for s in stats]
 
-    # --- Poisson time to 1e-6: timed steps, then each iteration on the same systems ------------
-    poisson = {"timed_steps": {"method": args.method, "learned": warm_note, "ms_mean": float(np.mean(solve_ms)),
+    # --- Poisson time to 1e-6 in the timed steps ------------------------------------------------
+    poisson = {"timed_steps": {"method": args.method, "learned": warm_note, "coarse_fp16": use_fp16,
+                               "ms_mean": float(np.mean(solve_ms)),
                                "cycles_mean": float(np.mean(cycles)),
                                "final_rel_residual_max": float(max(s.rel_residual or 0.0 for s in stats)),
                                "initial_rel_residual_mean": float(np.mean([s.initial_rel_residual or 0.0
                                                                            for s in stats])),
                                "guess_used": sorted({s.warm_start for s in stats}),
-                               "history_last_step": [float(x) for x in stats[-1].history]}}
-    if args.poisson_steps > 0:
-        poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
-    else:
-        poisson["learned_vs_plain"] = "skipped (--poisson-steps 0)"
+                               "history_last_step": [float(x) for x in stats[-1].history]}, **poisson}
 
     # --- end to end through the stage API with host buffers ------------------------------------
     e2e = None

@@ -36,12 +36,14 @@ def _time_smooth(h, level, x, rhs, iterations, repeats) -> float:
 def tune_hierarchy(h, x, rhs, iterations: int = 4, repeats: int = 3) -> dict[int, int]:
     """Pick a sweep kind for every level that runs red-black sweeps (``x``/``rhs``: level-0 buffers
     the sweeps may overwrite). Returns {level: kind} and writes it into the hierarchy."""
-    key = (torch.cuda.get_device_name(h.kernels.device), tuple(h.shapes))
+    key = (torch.cuda.get_device_name(h.kernels.device), tuple(h.shapes), getattr(h, "fp16_level", 0))
     choice = _cache.get(key)
     if choice is None:
         choice = {}
         timings = {}
         for level in range(h.levels - 1):
+            if h.is_fp16(level):
+                continue  # FP16 levels have one sweep kind (per-cell)
             candidates = [1, 4] + ([2, 3] if h.alt[level] is not None else [])
             times = {}
             for kind in candidates:

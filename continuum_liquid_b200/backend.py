@@ -106,7 +106,7 @@ class MGHierarchy(ctypes.Structure):
         ("levels", ctypes.c_int32),
         ("shape", (ctypes.c_int32 * 3) * MG_MAX_LEVELS),
         ("delta", ctypes.c_float),
-        ("reserved", ctypes.c_int32),
+        ("fp16_level", ctypes.c_int32),
         ("op0", ctypes.c_void_p),
         ("p", ctypes.c_void_p * MG_MAX_LEVELS),
         ("b", ctypes.c_void_p * MG_MAX_LEVELS),
@@ -114,6 +114,9 @@ class MGHierarchy(ctypes.Structure):
         ("op", ctypes.c_void_p * MG_MAX_LEVELS),
         ("alt", ctypes.c_void_p * MG_MAX_LEVELS),
         ("sweep", ctypes.c_int32 * MG_MAX_LEVELS),
+        ("fp16_scale", ctypes.c_void_p),
+        ("rhs_norms", ctypes.c_void_p),
+        ("fp16_inexact", ctypes.c_void_p),
     ]
 
 

@@ -7,6 +7,7 @@
 #include "multigrid.cuh"
 #include "mg_bottom.cuh"
 #include "mg_sweep.cuh"
+#include "mg_half.cuh"
 #include "voxelise.cuh"
 #include "tc_gemm.cuh"
 #include "conv3d.cuh"
@@ -21,7 +22,7 @@ using namespace clb;
                 (nz));                                                                                 \
     CLB_REQUIRE((i64)(nx) * (ny) * (nz) < (1ll << 31), "grid %dx%dx%d has more than 2^31 cells", (nx), (ny), (nz))
 
-static const int kAbiVersion = 4;
+static const int kAbiVersion = 5;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 
@@ -78,6 +79,10 @@ int clb_init(int device) {
                                         smem_max),
                    "coarse solve attribute"))
         return 1;
+    if (check_call(cudaFuncSetAttribute(k_coarse_solve<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        smem_max),
+                   "coarse solve attribute"))
+        return 1;
     const int bottom_max = (int)kBottomSmemLimit;
     cudaError_t e = cudaSuccess;
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
@@ -85,6 +90,11 @@ int clb_init(int device) {
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<16, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     if (check_call(e, "bottom visit attribute")) return 1;
     if (conv_set_attributes()) return 1;
     return 0;
@@ -485,23 +495,41 @@ static int check_hierarchy(const clb_mg_hierarchy* h) {
         if (l > 0)
             CLB_REQUIRE(h->p[l] && h->b[l] && h->mask[l] && h->op[l], "multigrid: level %d has a null array", l);
     }
+    if (h->fp16_level != 0) {
+        CLB_REQUIRE(h->fp16_level >= 1 && h->fp16_level <= h->levels - 2,
+                    "multigrid: fp16_level %d outside 1..levels-2 (%d)", h->fp16_level, h->levels - 2);
+        CLB_REQUIRE(h->fp16_scale && h->fp16_inexact, "multigrid: FP16 levels need fp16_scale and fp16_inexact");
+        const int* c = h->shape[h->levels - 1];
+        CLB_REQUIRE(c[0] * c[1] * c[2] <= COARSE_SMEM_CELLS, "multigrid: FP16 coarsest level too large (%d cells)",
+                    c[0] * c[1] * c[2]);
+    }
     return 0;
 }
+
+static inline bool is_half(const clb_mg_hierarchy* h, int l) { return h->fp16_level > 0 && l >= h->fp16_level; }
 
 int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream) {
     if (check_hierarchy(h)) return 1;
     cudaStream_t s = CLB_STREAM(stream);
+    if (h->fp16_level > 0 && check_call(cudaMemsetAsync(h->fp16_inexact, 0, sizeof(int32_t), s), "fp16 counter"))
+        return 1;
     for (int l = 1; l < h->levels; ++l) {
         const int* f = h->shape[l - 1];
         const int* c = h->shape[l];
         const i64 C = (i64)c[0] * c[1] * c[2];
-        if (l == 1)
-            k_coarse_operator<true><<<blocks_for(C, MGT), MGT, 0, s>>>(
-                h->op0, nullptr, nullptr, (float4*)h->op[l], h->mask[l], f[0], f[1], f[2], c[0], c[1], c[2]);
-        else
-            k_coarse_operator<false><<<blocks_for(C, MGT), MGT, 0, s>>>(nullptr, (const float4*)h->op[l - 1],
-                                                                         h->mask[l - 1], (float4*)h->op[l], h->mask[l],
-                                                                         f[0], f[1], f[2], c[0], c[1], c[2]);
+        const dim3 grid = blocks_for(C, MGT);
+        const int fs = l == 1 ? 0 : (is_half(h, l - 1) ? 2 : 1);
+        const bool ch = is_half(h, l);
+        const uint8_t* fop0 = l == 1 ? h->op0 : nullptr;
+        const void* fopc = l == 1 ? nullptr : h->op[l - 1];
+        const uint8_t* fmask = l == 1 ? nullptr : h->mask[l - 1];
+#define CLB_COARSE_OP(FS, CH)                                                                                        k_coarse_operator<FS, CH><<<grid, MGT, 0, s>>>(fop0, fopc, fmask, h->op[l], h->mask[l], h->fp16_inexact, f[0],                                                    f[1], f[2], c[0], c[1], c[2])
+        if (fs == 0 && !ch) CLB_COARSE_OP(0, false);
+        else if (fs == 1 && !ch) CLB_COARSE_OP(1, false);
+        else if (fs == 0) CLB_COARSE_OP(0, true);
+        else if (fs == 1) CLB_COARSE_OP(1, true);
+        else CLB_COARSE_OP(2, true);
+#undef CLB_COARSE_OP
         CLB_LAUNCH_CHECK("k_coarse_operator");
     }
     return 0;
@@ -519,11 +547,15 @@ struct LevelView {
     const uint8_t* mask;
     int nx, ny, nz;
     bool l0;
+    bool half;            // FP16 storage (p, b as __half, opc as Half4)
+    const float* scale;   // FP16 scales (mg_half.cuh)
 };
 
 LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rhs) {
     LevelView v;
     v.l0 = (l == 0);
+    v.half = is_half(h, l);
+    v.scale = h->fp16_scale;
     v.alt = h->alt[l];
     v.sweep = h->sweep[l];
     v.p = v.l0 ? x : h->p[l];
@@ -539,6 +571,17 @@ LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rh
 
 int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
     const i64 C = (i64)v.nx * v.ny * v.nz;
+    if (v.half) {  // FP16 levels: one thread per cell
+        for (int it = 0; it < iterations; ++it)
+            for (int parity = 0; parity < 2; ++parity) {
+                k_rbgs_h<<<blocks_for(C, MGT), MGT, 0, s>>>(reinterpret_cast<__half*>(v.p),
+                                                           reinterpret_cast<const __half*>(v.b),
+                                                           reinterpret_cast<const Half4*>(v.opc), v.mask, v.scale,
+                                                           parity, v.nx, v.ny, v.nz);
+                CLB_LAUNCH_CHECK("k_rbgs_h");
+            }
+        return 0;
+    }
     const int kind = v.sweep == 0 ? 1 : v.sweep;
     if (kind == 1) {
         const bool vec4 = (v.nz % 4) == 0 && (((uintptr_t)v.p) & 15) == 0;
@@ -608,6 +651,12 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
 
 int coarse_solve(const LevelView& v, float delta, int iterations, cudaStream_t s) {
     const int C = v.nx * v.ny * v.nz;
+    if (v.half) {  // checked to fit shared memory by check_hierarchy
+        k_coarse_solve<true, false, true><<<1, COARSE_THREADS, coarse_smem_bytes(C), s>>>(
+            v.p, v.b, nullptr, v.opc, v.mask, delta, iterations, v.nx, v.ny, v.nz, v.scale);
+        CLB_LAUNCH_CHECK("k_coarse_solve");
+        return 0;
+    }
     if (C <= COARSE_SMEM_CELLS) {
         const size_t bytes = coarse_smem_bytes(C);
         if (v.l0)
@@ -643,16 +692,23 @@ int bottom_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int co
         return 0;
     const int ka = (ma + BOTTOM_THREADS - 1) / BOTTOM_THREADS;
     const int kb = (mbc + BOTTOM_BTHREADS - 1) / BOTTOM_BTHREADS;
-#define CLB_BOTTOM(KA, KB)                                                                                      \
-    k_bottom_visit<KA, KB><<<1, BOTTOM_THREADS, bytes, s>>>(                                                      \
+#define CLB_BOTTOM(KA, KB, H)                                                                                   \
+    k_bottom_visit<KA, KB, H><<<1, BOTTOM_THREADS, bytes, s>>>(                                                   \
         h->p[level], h->b[level], (const float4*)h->op[level], h->mask[level], a[0], a[1], a[2], h->p[level + 1], \
         h->b[level + 1], (const float4*)h->op[level + 1], h->mask[level + 1], b[0], b[1], b[2], h->delta, pre,  \
-        post, coarse_iters)
-    if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1);
-    else if (ka <= 4 && kb <= 1) CLB_BOTTOM(4, 1);
-    else if (ka <= 8 && kb <= 1) CLB_BOTTOM(8, 1);
-    else if (ka <= 8 && kb <= 2) CLB_BOTTOM(8, 2);
-    else CLB_BOTTOM(16, 4);
+        post, coarse_iters, h->fp16_scale)
+#define CLB_BOTTOM_KINDS(H)                                 \
+    if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1, H);            \
+    else if (ka <= 4 && kb <= 1) CLB_BOTTOM(4, 1, H);       \
+    else if (ka <= 8 && kb <= 1) CLB_BOTTOM(8, 1, H);       \
+    else if (ka <= 8 && kb <= 2) CLB_BOTTOM(8, 2, H);       \
+    else CLB_BOTTOM(16, 4, H);
+    if (is_half(h, level)) {  // the suffix of FP16 levels then holds both bottom levels
+        CLB_BOTTOM_KINDS(true)
+    } else {
+        CLB_BOTTOM_KINDS(false)
+    }
+#undef CLB_BOTTOM_KINDS
 #undef CLB_BOTTOM
     if (check_launch("k_bottom_visit")) return -1;
     return 1;
@@ -668,7 +724,17 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
     if (smooth(v, h->delta, pre, s)) return 1;
     const LevelView c = level_view(h, level + 1, x, rhs);
     const i64 Cc = (i64)c.nx * c.ny * c.nz;
-    if (v.l0)
+    if (c.half) {
+        const dim3 grid = blocks_for(Cc, MGT);
+#define CLB_RESTRICT_H(FS)                                                                                        \
+    k_restrict_h<FS><<<grid, MGT, 0, s>>>(v.p, v.b, v.op0, v.opc, v.mask, reinterpret_cast<__half*>(c.p),          \
+                                          reinterpret_cast<__half*>(const_cast<float*>(c.b)), h->delta, h->fp16_scale, \
+                                          v.nx, v.ny, v.nz, c.nx, c.ny, c.nz)
+        if (v.half) CLB_RESTRICT_H(2);
+        else if (v.l0) CLB_RESTRICT_H(0);
+        else CLB_RESTRICT_H(1);
+#undef CLB_RESTRICT_H
+    } else if (v.l0)
         k_restrict<true><<<blocks_for(Cc, MGT), MGT, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, c.p,
                                                               const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
                                                               c.nx, c.ny, c.nz);
@@ -680,7 +746,19 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
     if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     const i64 Cf = (i64)v.nx * v.ny * v.nz;
-    if (v.l0)
+    if (c.half) {
+        const dim3 grid = blocks_for(Cf, MGT);
+        const __half* ce = reinterpret_cast<const __half*>(c.p);
+        if (v.half)
+            k_prolong_h<2><<<grid, MGT, 0, s>>>(ce, v.p, nullptr, v.mask, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                                 v.nz);
+        else if (v.l0)
+            k_prolong_h<0><<<grid, MGT, 0, s>>>(ce, v.p, v.op0, nullptr, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                                 v.nz);
+        else
+            k_prolong_h<1><<<grid, MGT, 0, s>>>(ce, v.p, nullptr, v.mask, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                                 v.nz);
+    } else if (v.l0)
         k_prolong<true><<<blocks_for(Cf, MGT), MGT, 0, s>>>(c.p, v.p, v.op0, nullptr, c.nx, c.ny, c.nz, v.nx, v.ny,
                                                              v.nz);
     else
@@ -697,7 +775,13 @@ int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pr
     if (check_hierarchy(h)) return 1;
     CLB_REQUIRE(x && rhs, "mg_w_cycle: null level-0 array");
     CLB_REQUIRE(pre_smooth >= 0 && post_smooth >= 0 && coarse_iterations >= 0, "mg_w_cycle: negative sweep count");
-    return w_cycle(h, 0, x, rhs, pre_smooth, post_smooth, coarse_iterations, CLB_STREAM(stream));
+    cudaStream_t s = CLB_STREAM(stream);
+    if (h->fp16_level > 0) {
+        CLB_REQUIRE(h->rhs_norms != nullptr, "mg_w_cycle: FP16 levels need rhs_norms");
+        k_fp16_scale<<<1, 32, 0, s>>>(h->rhs_norms, h->delta, h->fp16_scale);
+        CLB_LAUNCH_CHECK("k_fp16_scale");
+    }
+    return w_cycle(h, 0, x, rhs, pre_smooth, post_smooth, coarse_iterations, s);
 }
 
 int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int iterations, void* stream) {

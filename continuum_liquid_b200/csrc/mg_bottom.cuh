@@ -93,12 +93,15 @@ __device__ __forceinline__ int colour_cell(int r, int colour, int ny, int nz) {
     return (i * ny + j) * nz + k;
 }
 
-template <int KA, int KB>
+// H = true: both levels are stored in FP16 (p, b and operator as __half, scaled values); the visit
+// computes in FP32 in shared memory with kappa = scale[2] in place of delta^2 (mg_half.cuh).
+template <int KA, int KB, bool H = false>
 __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
     k_bottom_visit(float* __restrict__ pa, const float* __restrict__ ba, const float4* __restrict__ opa,
                    const uint8_t* __restrict__ ma, int anx, int any, int anz, float* __restrict__ pb,
                    float* __restrict__ bb, const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx,
-                   int bny, int bnz, float delta, int pre, int post, int coarse_iters) {
+                   int bny, int bnz, float delta, int pre, int post, int coarse_iters,
+                   const float* __restrict__ scale = nullptr) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     auto pad = [](int x) { return (x + 3) & ~3; };  // in floats
@@ -107,18 +110,28 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
     float4* soa = reinterpret_cast<float4*>(sba + pad(CA));
     float* spb = reinterpret_cast<float*>(soa + CA);
     float4* sob = reinterpret_cast<float4*>(spb + pad(CB));
-    const float d2 = delta * delta;
-    const float inv_delta2 = 1.0f / (delta * delta);
+    const float d2 = H ? scale[2] : delta * delta;
+    const float inv_delta2 = H ? scale[3] : 1.0f / (delta * delta);
+    auto ld = [&](const float* a, int c) -> float {
+        return H ? ldh(reinterpret_cast<const __half*>(a), c) : a[c];
+    };
+    auto ld4 = [&](const float4* a, int c) -> float4 {
+        return H ? ld_h4(reinterpret_cast<const Half4*>(a), c) : a[c];
+    };
+    auto st = [&](float* a, int c, float v) {
+        if (H) reinterpret_cast<__half*>(a)[c] = __float2half_rn(v);
+        else a[c] = v;
+    };
 
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
-        spa[c] = pa[c];
-        sba[c] = ba[c];
-        float4 o = opa[c];
+        spa[c] = ld(pa, c);
+        sba[c] = ld(ba, c);
+        float4 o = ld4(opa, c);
         if (!ma[c]) o.x = -1.0f;
         soa[c] = o;
     }
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
-        float4 o = opb[c];
+        float4 o = ld4(opb, c);
         if (!mb[c]) o.x = -1.0f;
         sob[c] = o;
         spb[c] = 0.0f;  // restriction zeroes the coarse pressure (multigrid.cl:114)
@@ -227,18 +240,18 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
     __syncthreads();
     smooth_a(post);
 
-    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) pa[c] = spa[c];
+    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) st(pa, c, spa[c]);
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
-        pb[c] = spb[c];
+        st(pb, c, spb[c]);
         const int I = c / bsx, J = (c / bsy) % bny, K = c % bnz;
-        if (!interior(I, J, K, bnx, bny, bnz)) bb[c] = 0.0f;  // multigrid.cl:115
+        if (!interior(I, J, K, bnx, bny, bnz)) st(bb, c, 0.0f);  // multigrid.cl:115
     }
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KB; ++m) {
             const int r = threadIdx.x + m * BOTTOM_BTHREADS;
-            if (btile && r < MBC) bb[B[colour][m].c] = bvals[colour][m];
+            if (btile && r < MBC) st(bb, B[colour][m].c, bvals[colour][m]);
         }
 }
 

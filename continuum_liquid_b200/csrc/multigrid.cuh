@@ -14,6 +14,7 @@
 // same values as the CPU restatement.
 #pragma once
 #include "common.cuh"
+#include <cuda_fp16.h>
 
 namespace clb {
 
@@ -173,6 +174,27 @@ struct OpC {  // coarse levels: float4 (diag, wx, wy, wz) + mask byte
 
 __device__ __forceinline__ float bitf(uint32_t v, int bit) { return (float)((v >> bit) & 1u); }
 
+// FP16 storage of coarse levels (no counterpart in the reference): p and b as __half, the operator
+// as four __half (diag, wx, wy, wz) in 8 bytes. Values on FP16 levels are scaled (see mg_half.cuh);
+// all arithmetic stays FP32.
+struct __align__(8) Half4 {
+    __half x, y, z, w;
+};
+__device__ __forceinline__ float4 ld_h4(const Half4* __restrict__ op, i64 c) {
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(op) + c);
+    const __half2 a = *reinterpret_cast<const __half2*>(&u.x), b = *reinterpret_cast<const __half2*>(&u.y);
+    return make_float4(__low2float(a), __high2float(a), __low2float(b), __high2float(b));
+}
+__device__ __forceinline__ float ldh(const __half* p, i64 c) { return __half2float(p[c]); }
+__device__ __forceinline__ Half4 to_h4(float4 v) {
+    Half4 h;
+    h.x = __float2half_rn(v.x);
+    h.y = __float2half_rn(v.y);
+    h.z = __float2half_rn(v.z);
+    h.w = __float2half_rn(v.w);
+    return h;
+}
+
 // Weighted neighbour sum (multigrid.cl:7-23) for each layout, same term order.
 template <typename T>
 __device__ __forceinline__ T wsum0(const uint8_t* __restrict__ op, const T* p, i64 c, i64 sx, i64 sy, uint32_t self) {
@@ -215,13 +237,18 @@ __global__ void __launch_bounds__(MGT) k_rhs_op0(const float* __restrict__ u, co
     op0[c] = (uint8_t)bits;
 }
 
-// Operator part of restrict_residual (multigrid.cl:127-179) for one coarse level, from either layout.
-template <bool FINE0>
+// Operator part of restrict_residual (multigrid.cl:127-179) for one coarse level, from any layout:
+// FS = 0 packed finest level, 1 float4 coarse level, 2 FP16 coarse level. CH = true stores the
+// coarse operator in FP16 and counts entries that FP16 does not hold exactly into *inexact (the
+// entries are sums of small integers, exact below 2048).
+template <int FS, bool CH>
 __global__ void __launch_bounds__(MGT) k_coarse_operator(const uint8_t* __restrict__ fop0,
-                                                          const float4* __restrict__ fopc,
-                                                          const uint8_t* __restrict__ fmask, float4* __restrict__ cop,
-                                                          uint8_t* __restrict__ cmask, int fnx, int fny, int fnz,
-                                                          int cnx, int cny, int cnz) {
+                                                          const void* __restrict__ fopc_,
+                                                          const uint8_t* __restrict__ fmask, void* __restrict__ cop_,
+                                                          uint8_t* __restrict__ cmask, int* __restrict__ inexact,
+                                                          int fnx, int fny, int fnz, int cnx, int cny, int cnz) {
+    constexpr bool FINE0 = FS == 0;
+    const float4* __restrict__ fopc = reinterpret_cast<const float4*>(fopc_);
     const i64 C = (i64)cnx * cny * cnz;
     const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
     if (ci >= C) return;
@@ -247,7 +274,7 @@ __global__ void __launch_bounds__(MGT) k_coarse_operator(const uint8_t* __restri
                         wz = bitf(o, 5);
                     } else {
                         if (!__ldg(fmask + f)) continue;
-                        const float4 o = __ldg(fopc + f);
+                        const float4 o = FS == 2 ? ld_h4(reinterpret_cast<const Half4*>(fopc_), f) : __ldg(fopc + f);
                         d = o.x;
                         wx = o.y;
                         wy = o.z;
@@ -269,12 +296,16 @@ __global__ void __launch_bounds__(MGT) k_coarse_operator(const uint8_t* __restri
                     }
                 }
     }
-    if (active > 0) {
-        cop[ci] = make_float4(dsum, cx, cy, cz);
-        cmask[ci] = 1;
+    const float4 v = active > 0 ? make_float4(dsum, cx, cy, cz) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    cmask[ci] = active > 0 ? 1 : 0;
+    if (CH) {
+        const Half4 h = to_h4(v);
+        if (__half2float(h.x) != v.x || __half2float(h.y) != v.y || __half2float(h.z) != v.z ||
+            __half2float(h.w) != v.w)
+            atomicAdd(inexact, 1);
+        reinterpret_cast<Half4*>(cop_)[ci] = h;
     } else {
-        cop[ci] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        cmask[ci] = 0;
+        reinterpret_cast<float4*>(cop_)[ci] = v;
     }
 }
 
@@ -382,29 +413,33 @@ __global__ void __launch_bounds__(MGT) k_prolong(const float* __restrict__ ce, f
 constexpr int COARSE_THREADS = 1024;
 constexpr int COARSE_SMEM_CELLS = 8192;  // 25 bytes per cell -> 200 KB
 
-template <bool SMEM, bool L0>
+// H = true: an FP16 level (p, b, operator as __half, shared-memory path only); its scaled system uses
+// kappa = scale[2] in place of delta^2 (mg_half.cuh).
+template <bool SMEM, bool L0, bool H = false>
 __global__ void __launch_bounds__(COARSE_THREADS) k_coarse_solve(float* p, const float* __restrict__ b,
                                                                   const uint8_t* __restrict__ op0,
                                                                   const float4* __restrict__ opc,
                                                                   const uint8_t* __restrict__ mask, float delta,
-                                                                  int iterations, int nx, int ny, int nz) {
+                                                                  int iterations, int nx, int ny, int nz,
+                                                                  const float* __restrict__ scale = nullptr) {
+    static_assert(!H || (SMEM && !L0), "FP16 levels are coarse levels solved from shared memory");
     extern __shared__ __align__(16) unsigned char smem[];
     const int C = nx * ny * nz;
-    const float d2 = delta * delta;
+    const float d2 = H ? scale[2] : delta * delta;
     const i64 sx = (i64)ny * nz, sy = nz;
     float* sp = reinterpret_cast<float*>(smem);
     float* sb = sp + C;
     float4* so = reinterpret_cast<float4*>(sb + C + ((4 - (2 * C) % 4) % 4));
     if (SMEM) {
         for (int c = threadIdx.x; c < C; c += COARSE_THREADS) {
-            sp[c] = p[c];
-            sb[c] = b[c];
+            sp[c] = H ? ldh(reinterpret_cast<const __half*>(p), c) : p[c];
+            sb[c] = H ? ldh(reinterpret_cast<const __half*>(b), c) : b[c];
             float4 o;
             if (L0) {
                 const uint32_t v = op0[c];
                 o = make_float4((v & 64u) ? (float)(v & 7u) : -1.0f, bitf(v, 3), bitf(v, 4), bitf(v, 5));
             } else {
-                o = opc[c];
+                o = H ? ld_h4(reinterpret_cast<const Half4*>(opc), c) : opc[c];
                 if (!mask[c]) o.x = -1.0f;  // marks "not fluid"; diag itself is never negative
             }
             so[c] = o;
@@ -437,7 +472,10 @@ __global__ void __launch_bounds__(COARSE_THREADS) k_coarse_solve(float* p, const
             __syncthreads();
         }
     if (SMEM)
-        for (int c = threadIdx.x; c < C; c += COARSE_THREADS) p[c] = sp[c];
+        for (int c = threadIdx.x; c < C; c += COARSE_THREADS) {
+            if (H) reinterpret_cast<__half*>(p)[c] = __float2half_rn(sp[c]);
+            else p[c] = sp[c];
+        }
 }
 
 static inline size_t coarse_smem_bytes(int C) {

@@ -120,9 +120,16 @@ class MultigridHierarchy:
     Level 0 is the simulation grid: its operator (``op0``, uint8 per cell) is written by
     ``rhs_operator`` each step. Coarse levels own p, b (float32), mask (uint8) and op (float4 as a
     float32 [..., 4] tensor). ``shapes[l]`` includes the ghost layer, as in the reference.
+
+    ``fp16_max_size`` > 0 stores every coarse level whose largest extent is at most that size in FP16
+    (p, b and op as float16, scaled as described in csrc/mg_half.cuh; no counterpart in the
+    reference), provided at least the two coarsest levels qualify. A W-cycle then needs
+    ``norms[0]`` to hold the squared norm of its right-hand side (the residual kernels leave it
+    there), and those levels use per-cell sweeps.
     """
 
-    def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, fused_min_cells: int = 20**3):
+    def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, fused_min_cells: int = 20**3,
+                 fp16_max_size: int = 0):
         self.kernels = kernels
         self.grid_shape = tuple(int(s) for s in grid_shape)
         self.dx = float(dx)
@@ -130,16 +137,25 @@ class MultigridHierarchy:
         if len(self.shapes) > MG_MAX_LEVELS:
             raise ValueError(f"{len(self.shapes)} multigrid levels exceed the limit of {MG_MAX_LEVELS}")
         device = kernels.device
+        levels = len(self.shapes)
+        self.fp16_level = 0
+        if fp16_max_size > 0:
+            first = next((l for l in range(1, levels) if max(self.shapes[l]) <= fp16_max_size), 0)
+            if 1 <= first <= levels - 2:
+                self.fp16_level = first
         self.op0 = torch.zeros(self.grid_shape, dtype=torch.uint8, device=device)
         self.p: list[torch.Tensor | None] = [None]
         self.b: list[torch.Tensor | None] = [None]
         self.mask: list[torch.Tensor | None] = [None]
         self.op: list[torch.Tensor | None] = [None]
-        for shape in self.shapes[1:]:
-            self.p.append(torch.zeros(shape, dtype=torch.float32, device=device))
-            self.b.append(torch.zeros(shape, dtype=torch.float32, device=device))
+        for l, shape in enumerate(self.shapes[1:], start=1):
+            dt = torch.float16 if self.is_fp16(l) else torch.float32
+            self.p.append(torch.zeros(shape, dtype=dt, device=device))
+            self.b.append(torch.zeros(shape, dtype=dt, device=device))
             self.mask.append(torch.zeros(shape, dtype=torch.uint8, device=device))
-            self.op.append(torch.zeros((*shape, 4), dtype=torch.float32, device=device))
+            self.op.append(torch.zeros((*shape, 4), dtype=dt, device=device))
+        self.fp16_scale = torch.zeros(4, dtype=torch.float32, device=device)
+        self.fp16_inexact = torch.zeros(1, dtype=torch.int32, device=device)
         self.struct = MGHierarchy()
         self.struct.levels = len(self.shapes)
         for l, shape in enumerate(self.shapes):
@@ -157,7 +173,7 @@ class MultigridHierarchy:
         # cells (smaller levels are served by the single-block bottom visit or two-launch sweeps)
         self.alt: list[torch.Tensor | None] = []
         for l, shape in enumerate(self.shapes):
-            big = int(np.prod(shape)) >= fused_min_cells
+            big = int(np.prod(shape)) >= fused_min_cells and not self.is_fp16(l)
             self.alt.append(torch.zeros(shape, dtype=torch.float32, device=device) if big else None)
             if big:
                 self.struct.alt[l] = self.alt[l].data_ptr()
@@ -165,6 +181,20 @@ class MultigridHierarchy:
         cells = int(np.prod(self.grid_shape))
         self.partials = torch.zeros((kernels.residual_partials(cells), 2), dtype=torch.float64, device=device)
         self.norms = torch.zeros(2, dtype=torch.float64, device=device)
+        self.struct.fp16_level = self.fp16_level
+        self.struct.fp16_scale = self.fp16_scale.data_ptr()
+        self.struct.rhs_norms = self.norms.data_ptr()
+        self.struct.fp16_inexact = self.fp16_inexact.data_ptr()
+        for l in range(1, levels):
+            if self.is_fp16(l):
+                self.struct.sweep[l] = 4
+
+    def is_fp16(self, level: int) -> bool:
+        return self.fp16_level > 0 and level >= self.fp16_level
+
+    def fp16_inexact_entries(self) -> int:
+        """Operator entries of the FP16 levels that FP16 does not hold exactly (last build_coarse)."""
+        return int(self.fp16_inexact.item()) if self.fp16_level else 0
 
     @property
     def levels(self) -> int:
@@ -188,8 +218,11 @@ class MultigridHierarchy:
                                     int(coarse_iterations), stream=queue)
 
     def set_sweep(self, level: int, kind: int) -> None:
-        """Red-black sweep implementation of one level (see clb_mg_hierarchy.sweep)."""
-        self.struct.sweep[level] = int(kind)
+        """Red-black sweep implementation of one level (see clb_mg_hierarchy.sweep); FP16 levels
+        always use kind 4."""
+        if self.is_fp16(level) and int(kind) not in (0, 4):
+            raise ValueError(f"level {level} is stored in FP16 and uses sweep kind 4")
+        self.struct.sweep[level] = 4 if self.is_fp16(level) else int(kind)
 
     def sweeps(self) -> list[int]:
         return [int(self.struct.sweep[l]) for l in range(self.levels)]
@@ -209,11 +242,11 @@ class MultigridHierarchy:
         """Host copies of one level (tests and diagnostics)."""
         if level == 0:
             return {"op0": self.op0.cpu().numpy()}
-        return {
-            "p": self.p[level].cpu().numpy(),
-            "b": self.b[level].cpu().numpy(),
+        return {  # FP16 levels are returned as float32 (their p and b in scaled units)
+            "p": self.p[level].float().cpu().numpy(),
+            "b": self.b[level].float().cpu().numpy(),
             "mask": self.mask[level].cpu().numpy(),
-            "op": self.op[level].cpu().numpy(),
+            "op": self.op[level].float().cpu().numpy(),
         }
 
 

@@ -99,15 +99,19 @@ class PressureSolver:
     """
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100,
-                 autotune: bool = True, method: str = "fcg"):
+                 autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
+        self.coarse_fp16 = bool(coarse_fp16)
         self.kernels = kernels
         self.grid_shape = tuple(int(s) for s in grid_shape)
         self.dx = float(dx)
         self.max_cycles = int(max_cycles)
         self.method = method
-        self.hierarchy = multigrid.MultigridHierarchy(kernels, self.grid_shape, dx, min_size)
+        # FP16 storage of the coarse levels of at most fp16_max_size cells per side (tolerance mode only:
+        # the W-cycle then reads the squared norm of its right-hand side from the residual kernels)
+        self.hierarchy = multigrid.MultigridHierarchy(kernels, self.grid_shape, dx, min_size,
+                                                      fp16_max_size=fp16_max_size if coarse_fp16 else 0)
         device = kernels.device
         self.cells = int(np.prod(self.grid_shape))
         self.rhs = torch.zeros(self.grid_shape, dtype=torch.float32, device=device)
@@ -213,6 +217,8 @@ class PressureSolver:
             tune_hierarchy(h, self.correction, self.residual)
             self.tuned = True
         if tol is None:
+            if h.fp16_level:
+                raise ValueError("FP16 coarse levels are a tolerance-mode option (tol=...)")
             self.solved64 = False
             for _ in range(int(num_vcycles)):
                 h.w_cycle(pressure, self.rhs)

@@ -52,6 +52,7 @@ class StepOptions:
     use_graph: bool = True
     warm_start: object = None  # callable proposing an initial pressure (learned.LearnedWarmStart)
     method: str = "fcg"  # tolerance-mode iteration: "fcg" (W-cycle preconditioned CG) or "refine"
+    coarse_fp16: bool = False  # tolerance mode: store the coarse levels of at most 64^3 cells in FP16
 
 
 class FlipSolver:
@@ -90,7 +91,7 @@ class FlipSolver:
             if bool(ob.any()):
                 self.obstacle = ob.to(dev).contiguous()
         self.pressure_solver = PressureSolver(kernels, self.grid_shape, self.dx, min_size=min_size,
-                                              method=self.options.method)
+                                              method=self.options.method, coarse_fp16=self.options.coarse_fp16)
         self.last_solve: SolveStats | None = None
         self.steps_done = 0
 

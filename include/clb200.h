@@ -186,12 +186,15 @@ int clb_coarse_smooth(float* p, const float* b, const float* mask, const float* 
 
 /* A level pyramid as created by multigrid.py:18-50 create_multigrid_levels. Level 0 is the
  * simulation grid; its operator is one byte per cell (bits 0-2 diagonal, 3-5 wx/wy/wz, 6 fluid).
- * Coarse levels l >= 1 hold p, b (float32), a mask byte and a float4 (diagonal, wx, wy, wz). */
+ * Coarse levels l >= 1 hold p, b (float32), a mask byte and a float4 (diagonal, wx, wy, wz).
+ * Levels l >= fp16_level (when fp16_level > 0; no counterpart in the reference) store p and b as
+ * IEEE half and the operator as four halves (8 bytes), with p and b scaled by powers of two taken
+ * from rhs_norms (see clb_mg_w_cycle); such levels use sweep kind 4 and need fp16_scale. */
 typedef struct clb_mg_hierarchy {
     int32_t levels;                      /* including level 0 */
     int32_t shape[CLB_MG_MAX_LEVELS][3]; /* nx, ny, nz per level (ghost layer included) */
     float delta;                         /* grid spacing used by every level (multigrid.py:65) */
-    int32_t reserved;
+    int32_t fp16_level;                  /* first FP16 level (>= 1 and <= levels - 2), 0: none */
     uint8_t* op0;                        /* level 0 packed operator */
     float* p[CLB_MG_MAX_LEVELS];         /* [0] unused: level-0 x is passed per call */
     float* b[CLB_MG_MAX_LEVELS];         /* [0] unused: level-0 rhs is passed per call */
@@ -206,6 +209,13 @@ typedef struct clb_mg_hierarchy {
                                             3 = one fused launch per iteration, 4x4x32 tiles (needs alt),
                                             4 = two colour launches, one thread per cell.
                                             All kinds give identical values. */
+    float* fp16_scale;                   /* device float[4] written by clb_mg_w_cycle: sigma_b,
+                                            1/sigma_p, kappa, 1/kappa (FP16 levels only) */
+    const double* rhs_norms;             /* device: rhs_norms[0] = sum of squares of the level-0
+                                            right-hand side over fluid cells (FP16 levels only; the
+                                            out[0] of clb_mg_residual_norms / ir_step / fcg_step) */
+    int32_t* fp16_inexact;               /* device counter: FP16 operator entries that did not convert
+                                            exactly (clb_mg_build_coarse zeroes and fills it) */
 } clb_mg_hierarchy;
 
 /* pressure_solve.cl:3-24 pressure_rhs fused with multigrid.cl:63-88 build_finest_operator, writing

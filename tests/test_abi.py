@@ -30,7 +30,7 @@ def test_python_signature_table_covers_the_header():
 
 def test_load_library_sets_signatures_and_pure_helpers():
     lib = backend.load_library()
-    assert lib.clb_abi_version() == 4
+    assert lib.clb_abi_version() == 5
     for count in (0, 1, 4096, 4097, 16777216):
         assert lib.clb_scan_scratch_bytes(count) == backend.Backend.scan_scratch_bytes_static(count)
     assert lib.clb_mg_residual_partials(1000) == 4
@@ -40,12 +40,15 @@ def test_load_library_sets_signatures_and_pure_helpers():
 
 
 def test_hierarchy_struct_layout():
-    # int32 levels (0), int32[16][3] (4..196), float delta (196), int32 reserved (200), then
-    # 8-byte-aligned pointers: op0 at 208 and the five pointer tables after it
+    # int32 levels (0), int32[16][3] (4..196), float delta (196), int32 fp16_level (200), then
+    # 8-byte-aligned pointers: op0 at 208, the five pointer tables, int32 sweep[16], then the three
+    # FP16 pointers
     assert backend.MGHierarchy.delta.offset == 196
+    assert backend.MGHierarchy.fp16_level.offset == 200
     assert backend.MGHierarchy.op0.offset == 208
     assert backend.MGHierarchy.p.offset == 216
-    assert ctypes.sizeof(backend.MGHierarchy) == 216 + 5 * 16 * 8 + 16 * 4
+    assert backend.MGHierarchy.fp16_scale.offset == 216 + 5 * 16 * 8 + 16 * 4
+    assert ctypes.sizeof(backend.MGHierarchy) == 216 + 5 * 16 * 8 + 16 * 4 + 3 * 8
 
 
 def test_backend_without_gpu_fails_loudly(monkeypatch):
