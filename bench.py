@@ -40,8 +40,9 @@ METRIC = "steps/s at 256^3; Poisson ms to 1e-6 rel. residual, learned vs plain W
 UNIT = "steps/s"
 TOL = 1e-6
 
-# DRAM bytes per launch of the dominant kernel from one ncu capture (see profiles/); None if not captured.
-NCU_TRAFFIC_BYTES = {}
+# DRAM bytes (read + write) per launch of the dominant kernel from one ncu capture of the same kernel on the
+# same 256^3 system (profiles/k_rbgs_colour_level0_block_256.md); None for kernels not captured.
+NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360}
 
 
 def parse_args():
