@@ -60,6 +60,20 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_prolongate": [P, P, P, I, I, I, I, I, I, P],
     "clb_coarse_smooth": [P, P, P, P, P, P, P, F, I, I, I, I, P],
     "clb_mg_rhs_operator": [P, P, P, P, P, P, F, F, I, I, I, P],
+    "clb_batch_particle_to_grid": [P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, L, F, P],
+    "clb_batch_update_velocity": [P, P, P, P, P, P, P, P, F, F, F, F, F, F, F, F, F, P],
+    "clb_batch_grid_domain_bc": [P, P, P, P, P],
+    "clb_batch_grid_obstacle_bc": [P, P, P, P, P, P, P],
+    "clb_batch_rhs_operator": [P, P, P, P, P, P, P],
+    "clb_batch_w_cycle": [P, P, P, I, I, I, P],
+    "clb_batch_residual_norms": [P, P, I, P, P, P, P, P],
+    "clb_batch_ir_init": [P, P, P, P],
+    "clb_batch_ir_store": [P, P, P, P],
+    "clb_batch_fcg_dots": [P, P, P, P, P, P, P],
+    "clb_batch_fcg_step": [P, P, P, P, P, P, P, P, P, P, P, P],
+    "clb_batch_pressure_correction": [P, P, P, P, P, I, P],
+    "clb_batch_neumann_domain_bc": [P, P, P],
+    "clb_batch_particle_update": [P, P, P, P, P, P, P, P, P, P, F, F, P],
     "clb_mg_build_coarse": [P, P],
     "clb_mg_w_cycle": [P, P, P, I, I, I, P],
     "clb_mg_smooth": [P, I, P, P, I, P],
@@ -117,6 +131,72 @@ class MGHierarchy(ctypes.Structure):
         ("fp16_scale", ctypes.c_void_p),
         ("rhs_norms", ctypes.c_void_p),
         ("fp16_inexact", ctypes.c_void_p),
+    ]
+
+
+BATCH_MAX_SCENES = 64
+
+
+class BatchScene(ctypes.Structure):
+    """Mirror of clb_batch_scene (include/clb200.h)."""
+
+    _fields_ = [
+        ("levels", ctypes.c_int32),
+        ("bottom", ctypes.c_int32),
+        ("shape", (ctypes.c_int32 * 3) * MG_MAX_LEVELS),
+        ("base", ctypes.c_int64 * MG_MAX_LEVELS),
+        ("particle_base", ctypes.c_int64),
+        ("particles", ctypes.c_int64),
+        ("delta", ctypes.c_float),
+        ("inv_dx", ctypes.c_float),
+        ("inv_dx2", ctypes.c_float),
+        ("rho_over_dt", ctypes.c_float),
+        ("dt_over_rho", ctypes.c_float),
+        ("lower", ctypes.c_float),
+        ("upper", ctypes.c_float * 3),
+        ("pad", ctypes.c_int32),
+    ]
+
+
+class BatchList(ctypes.Structure):
+    """Mirror of clb_batch_list."""
+
+    _fields_ = [
+        ("scene", ctypes.c_void_p),
+        ("start", ctypes.c_void_p),
+        ("count", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+        ("total", ctypes.c_int64),
+    ]
+
+
+class Batch(ctypes.Structure):
+    """Mirror of clb_batch."""
+
+    _fields_ = [
+        ("scenes", ctypes.c_int32),
+        ("levels", ctypes.c_int32),
+        ("geom", ctypes.c_void_p),
+        ("geom_host", ctypes.c_void_p),
+        ("particles", BatchList),
+        ("cells", BatchList * MG_MAX_LEVELS),
+        ("recurse", BatchList * MG_MAX_LEVELS),
+        ("recurse_coarse", BatchList * MG_MAX_LEVELS),
+        ("bottom", BatchList * MG_MAX_LEVELS),
+        ("coarse", BatchList * MG_MAX_LEVELS),
+        ("colour0", BatchList),
+        ("sweep0", ctypes.c_int32),
+        ("vec0", ctypes.c_int32),
+        ("reduce_blocks", ctypes.c_int32),
+        ("bottom_ka", ctypes.c_int32),
+        ("bottom_kb", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+        ("bottom_smem", ctypes.c_int64),
+        ("op0", ctypes.c_void_p),
+        ("p", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("b", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("mask", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("op", ctypes.c_void_p * MG_MAX_LEVELS),
     ]
 
 
@@ -200,6 +280,10 @@ class Backend:
 
     def residual_partials(self, cells: int) -> int:
         return int(self.lib.clb_mg_residual_partials(cells))
+
+    def call_batch(self, name: str, batch: "Batch", *args: Any, stream=None) -> None:
+        """Call a clb_batch_* entry point (the batch struct is passed by pointer)."""
+        self.call_hierarchy(name, batch, *args, stream=stream)
 
     def call_hierarchy(self, name: str, hierarchy: MGHierarchy, *args: Any, stream=None) -> None:
         converted = [ptr(a) if isinstance(a, torch.Tensor) or a is None else a for a in args]

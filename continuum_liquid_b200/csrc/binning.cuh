@@ -287,15 +287,14 @@ constexpr int P2G_THREADS = 256;
 
 __device__ __forceinline__ float tent(float s, float f) { return fmaxf(0.0f, 1.0f - fabsf(s - f)); }
 
-__global__ void __launch_bounds__(P2G_THREADS) k_p2g_gather(const float* __restrict__ pos, const float* __restrict__ vel,
-                                                             const int* __restrict__ offsets,
-                                                             const int* __restrict__ counts, float* __restrict__ u,
-                                                             float* __restrict__ v, float* __restrict__ w,
-                                                             float* __restrict__ ff, float inv_dx, float inv_ppc,
-                                                             int nx, int ny, int nz) {
+// Cell `index` of the grid (nothing to do when index >= nx*ny*nz) by lane `lane` of its eight-lane
+// group; every lane of the warp must call it (the partial sums are combined with shuffles).
+__device__ __forceinline__ void p2g_cell(i64 index, int lane, const float* __restrict__ pos,
+                                         const float* __restrict__ vel, const int* __restrict__ offsets,
+                                         const int* __restrict__ counts, float* __restrict__ u, float* __restrict__ v,
+                                         float* __restrict__ w, float* __restrict__ ff, float inv_dx, float inv_ppc,
+                                         int nx, int ny, int nz) {
     const i64 C = (i64)nx * ny * nz;
-    const i64 index = ((i64)blockIdx.x * P2G_THREADS + threadIdx.x) / P2G_LANES;
-    const int lane = threadIdx.x & (P2G_LANES - 1);
     float vs0 = 0.0f, vs1 = 0.0f, vs2 = 0.0f, ws0 = 0.0f, ws1 = 0.0f, ws2 = 0.0f;
     int inside = 0;
     int ci = 0, cj = 0, ck = 0;
@@ -353,6 +352,17 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_gather(const float* __restr
         w[index] = ws2 > 0.0f ? vs2 / ws2 : 0.0f;
         ff[index] = (float)inside * inv_ppc;
     }
+}
+
+__global__ void __launch_bounds__(P2G_THREADS) k_p2g_gather(const float* __restrict__ pos, const float* __restrict__ vel,
+                                                             const int* __restrict__ offsets,
+                                                             const int* __restrict__ counts, float* __restrict__ u,
+                                                             float* __restrict__ v, float* __restrict__ w,
+                                                             float* __restrict__ ff, float inv_dx, float inv_ppc,
+                                                             int nx, int ny, int nz) {
+    const i64 index = ((i64)blockIdx.x * P2G_THREADS + threadIdx.x) / P2G_LANES;
+    p2g_cell(index, threadIdx.x & (P2G_LANES - 1), pos, vel, offsets, counts, u, v, w, ff, inv_dx, inv_ppc, nx, ny,
+             nz);
 }
 
 }  // namespace clb

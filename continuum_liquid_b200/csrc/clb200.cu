@@ -8,6 +8,7 @@
 #include "mg_bottom.cuh"
 #include "mg_sweep.cuh"
 #include "mg_half.cuh"
+#include "batch.cuh"
 #include "voxelise.cuh"
 #include "tc_gemm.cuh"
 #include "conv3d.cuh"
@@ -22,7 +23,7 @@ using namespace clb;
                 (nz));                                                                                 \
     CLB_REQUIRE((i64)(nx) * (ny) * (nz) < (1ll << 31), "grid %dx%dx%d has more than 2^31 cells", (nx), (ny), (nz))
 
-static const int kAbiVersion = 5;
+static const int kAbiVersion = 6;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 
@@ -95,6 +96,12 @@ int clb_init(int device) {
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<16, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_coarse_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     if (check_call(e, "bottom visit attribute")) return 1;
     if (conv_set_attributes()) return 1;
     return 0;
@@ -1179,5 +1186,8 @@ int clb_voxelise_mesh(const float* triangles, uint8_t* mask, int triangle_count,
     CLB_LAUNCH_CHECK("k_voxelise");
     return 0;
 }
+
+// ---- batched scenes --------------------------------------------------------------------------------
+#include "batch_abi.cuh"
 
 }  // extern "C"

@@ -16,15 +16,12 @@ __device__ __forceinline__ float laplacian(const float* __restrict__ f, i64 c, i
 }
 
 // velocity_update.cl:3-43 update_velocity
-__global__ void __launch_bounds__(GT) k_update_velocity(const float* __restrict__ u, const float* __restrict__ v,
+__device__ __forceinline__ void update_velocity_at(i64 c, const float* __restrict__ u, const float* __restrict__ v,
                                                          const float* __restrict__ w, float* __restrict__ ru,
                                                          float* __restrict__ rv, float* __restrict__ rw,
                                                          const float* __restrict__ ff, float gx, float gy, float gz,
                                                          float fx, float fy, float fz, float rho, float nu,
                                                          float inv_dx2, float dt, int nx, int ny, int nz) {
-    const i64 C = (i64)nx * ny * nz;
-    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
-    if (c >= C) return;
     int i, j, k;
     gcoord(c, ny, nz, i, j, k);
     float r0 = __ldg(u + c), r1 = __ldg(v + c), r2 = __ldg(w + c);
@@ -44,13 +41,22 @@ __global__ void __launch_bounds__(GT) k_update_velocity(const float* __restrict_
     rw[c] = r2;
 }
 
-// boundary_conditions.cl:33-67 grid_domain_bc. A ghost copies a component from its clamped
-// interior cell only where the ghost's own wall flag for that component is clear, and the interior
-// source shares that flag, so the source component is never written by the same launch.
-__global__ void __launch_bounds__(GT) k_grid_domain_bc(float* u, float* v, float* w, int nx, int ny, int nz) {
+__global__ void __launch_bounds__(GT) k_update_velocity(const float* __restrict__ u, const float* __restrict__ v,
+                                                         const float* __restrict__ w, float* __restrict__ ru,
+                                                         float* __restrict__ rv, float* __restrict__ rw,
+                                                         const float* __restrict__ ff, float gx, float gy, float gz,
+                                                         float fx, float fy, float fz, float rho, float nu,
+                                                         float inv_dx2, float dt, int nx, int ny, int nz) {
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
     if (c >= C) return;
+    update_velocity_at(c, u, v, w, ru, rv, rw, ff, gx, gy, gz, fx, fy, fz, rho, nu, inv_dx2, dt, nx, ny, nz);
+}
+
+// boundary_conditions.cl:33-67 grid_domain_bc. A ghost copies a component from its clamped
+// interior cell only where the ghost's own wall flag for that component is clear, and the interior
+// source shares that flag, so the source component is never written by the same launch.
+__device__ __forceinline__ void grid_domain_bc_at(i64 c, float* u, float* v, float* w, int nx, int ny, int nz) {
     int i, j, k;
     gcoord(c, ny, nz, i, j, k);
     const bool ghost = !interior(i, j, k, nx, ny, nz);
@@ -68,13 +74,17 @@ __global__ void __launch_bounds__(GT) k_grid_domain_bc(float* u, float* v, float
     if (ww) w[c] = 0.0f;
 }
 
-// boundary_conditions.cl:99-119 grid_obstacle_bc
-__global__ void __launch_bounds__(GT) k_grid_obstacle_bc(float* __restrict__ u, float* __restrict__ v,
-                                                          float* __restrict__ w, float* __restrict__ ff,
-                                                          const uint8_t* __restrict__ obs, int nx, int ny, int nz) {
+__global__ void __launch_bounds__(GT) k_grid_domain_bc(float* u, float* v, float* w, int nx, int ny, int nz) {
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
     if (c >= C) return;
+    grid_domain_bc_at(c, u, v, w, nx, ny, nz);
+}
+
+// boundary_conditions.cl:99-119 grid_obstacle_bc
+__device__ __forceinline__ void grid_obstacle_bc_at(i64 c, float* __restrict__ u, float* __restrict__ v,
+                                                          float* __restrict__ w, float* __restrict__ ff,
+                                                          const uint8_t* __restrict__ obs, int nx, int ny, int nz) {
     int i, j, k;
     gcoord(c, ny, nz, i, j, k);
     const bool self = __ldg(obs + c) != 0;
@@ -87,14 +97,21 @@ __global__ void __launch_bounds__(GT) k_grid_obstacle_bc(float* __restrict__ u, 
     if (zs) w[c] = 0.0f;
 }
 
-// boundary_conditions.cl:121-173 extrapolate_obstacle_velocity (reads non-obstacle cells only and
-// writes obstacle cells only, so one launch has no read/write overlap).
-__global__ void __launch_bounds__(GT) k_extrapolate_obstacle_velocity(float* u, float* v, float* w,
-                                                                       const uint8_t* __restrict__ obs, int nx, int ny,
-                                                                       int nz) {
+__global__ void __launch_bounds__(GT) k_grid_obstacle_bc(float* __restrict__ u, float* __restrict__ v,
+                                                          float* __restrict__ w, float* __restrict__ ff,
+                                                          const uint8_t* __restrict__ obs, int nx, int ny, int nz) {
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
-    if (c >= C || !__ldg(obs + c)) return;
+    if (c >= C) return;
+    grid_obstacle_bc_at(c, u, v, w, ff, obs, nx, ny, nz);
+}
+
+// boundary_conditions.cl:121-173 extrapolate_obstacle_velocity (reads non-obstacle cells only and
+// writes obstacle cells only, so one launch has no read/write overlap).
+__device__ __forceinline__ void extrapolate_obstacle_velocity_at(i64 c, float* u, float* v, float* w,
+                                                                 const uint8_t* __restrict__ obs, int nx, int ny,
+                                                                 int nz) {
+    if (!__ldg(obs + c)) return;
     int i, j, k;
     gcoord(c, ny, nz, i, j, k);
     float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
@@ -123,6 +140,15 @@ __global__ void __launch_bounds__(GT) k_extrapolate_obstacle_velocity(float* u, 
     u[c] = ax ? 0.0f : t0;
     v[c] = ay ? 0.0f : t1;
     w[c] = az ? 0.0f : t2;
+}
+
+__global__ void __launch_bounds__(GT) k_extrapolate_obstacle_velocity(float* u, float* v, float* w,
+                                                                       const uint8_t* __restrict__ obs, int nx, int ny,
+                                                                       int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C) return;
+    extrapolate_obstacle_velocity_at(c, u, v, w, obs, nx, ny, nz);
 }
 
 // pressure_solve.cl:3-24 pressure_rhs (helper.cl:39-52 divergence)
@@ -156,12 +182,9 @@ __global__ void __launch_bounds__(GT) k_pressure_rhs(const float* __restrict__ u
 // updated velocity once (the projection of a refined solve, whose FP64 pressure is the one that
 // meets the residual tolerance).
 template <typename PT>
-__global__ void __launch_bounds__(GT) k_pressure_correction(float* __restrict__ u, float* __restrict__ v,
+__device__ __forceinline__ void pressure_correction_at(i64 c, float* __restrict__ u, float* __restrict__ v,
                                                              float* __restrict__ w, const PT* __restrict__ p,
                                                              float dt_over_rho, float inv_dx, int nx, int ny, int nz) {
-    const i64 C = (i64)nx * ny * nz;
-    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
-    if (c >= C) return;
     int i, j, k;
     gcoord(c, ny, nz, i, j, k);
     if (!interior(i, j, k, nx, ny, nz)) return;
@@ -174,16 +197,31 @@ __global__ void __launch_bounds__(GT) k_pressure_correction(float* __restrict__ 
     w[c] = (float)((PT)w[c] - (PT)dt_over_rho * gz);
 }
 
+template <typename PT>
+__global__ void __launch_bounds__(GT) k_pressure_correction(float* __restrict__ u, float* __restrict__ v,
+                                                             float* __restrict__ w, const PT* __restrict__ p,
+                                                             float dt_over_rho, float inv_dx, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
+    if (c >= C) return;
+    pressure_correction_at<PT>(c, u, v, w, p, dt_over_rho, inv_dx, nx, ny, nz);
+}
+
 // boundary_conditions.cl:18-31 neumann_domain_bc (ghosts read interior cells only)
+template <typename PT>
+__device__ __forceinline__ void neumann_domain_bc_at(i64 c, PT* p, int nx, int ny, int nz) {
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    if (interior(i, j, k, nx, ny, nz)) return;
+    p[c] = p[gidx(clampi(i, 1, nx - 2), clampi(j, 1, ny - 2), clampi(k, 1, nz - 2), ny, nz)];
+}
+
 template <typename PT>
 __global__ void __launch_bounds__(GT) k_neumann_domain_bc(PT* p, int nx, int ny, int nz) {
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
     if (c >= C) return;
-    int i, j, k;
-    gcoord(c, ny, nz, i, j, k);
-    if (interior(i, j, k, nx, ny, nz)) return;
-    p[c] = p[gidx(clampi(i, 1, nx - 2), clampi(j, 1, ny - 2), clampi(k, 1, nz - 2), ny, nz)];
+    neumann_domain_bc_at<PT>(c, p, nx, ny, nz);
 }
 
 }  // namespace clb

@@ -96,12 +96,13 @@ __device__ __forceinline__ int colour_cell(int r, int colour, int ny, int nz) {
 // H = true: both levels are stored in FP16 (p, b and operator as __half, scaled values); the visit
 // computes in FP32 in shared memory with kappa = scale[2] in place of delta^2 (mg_half.cuh).
 template <int KA, int KB, bool H = false>
-__global__ void __launch_bounds__(BOTTOM_THREADS, 1)
-    k_bottom_visit(float* __restrict__ pa, const float* __restrict__ ba, const float4* __restrict__ opa,
-                   const uint8_t* __restrict__ ma, int anx, int any, int anz, float* __restrict__ pb,
-                   float* __restrict__ bb, const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx,
-                   int bny, int bnz, float delta, int pre, int post, int coarse_iters,
-                   const float* __restrict__ scale = nullptr) {
+__device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const float* __restrict__ ba,
+                                                   const float4* __restrict__ opa, const uint8_t* __restrict__ ma,
+                                                   int anx, int any, int anz, float* __restrict__ pb,
+                                                   float* __restrict__ bb, const float4* __restrict__ opb,
+                                                   const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
+                                                   float delta, int pre, int post, int coarse_iters,
+                                                   const float* __restrict__ scale) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     auto pad = [](int x) { return (x + 3) & ~3; };  // in floats
@@ -253,6 +254,17 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
             const int r = threadIdx.x + m * BOTTOM_BTHREADS;
             if (btile && r < MBC) st(bb, B[colour][m].c, bvals[colour][m]);
         }
+}
+
+template <int KA, int KB, bool H = false>
+__global__ void __launch_bounds__(BOTTOM_THREADS, 1)
+    k_bottom_visit(float* __restrict__ pa, const float* __restrict__ ba, const float4* __restrict__ opa,
+                   const uint8_t* __restrict__ ma, int anx, int any, int anz, float* __restrict__ pb,
+                   float* __restrict__ bb, const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx,
+                   int bny, int bnz, float delta, int pre, int post, int coarse_iters,
+                   const float* __restrict__ scale = nullptr) {
+    bottom_visit_block<KA, KB, H>(pa, ba, opa, ma, anx, any, anz, pb, bb, opb, mb, bnx, bny, bnz, delta, pre, post,
+                                  coarse_iters, scale);
 }
 
 }  // namespace clb

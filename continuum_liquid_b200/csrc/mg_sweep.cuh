@@ -144,15 +144,15 @@ namespace clb {
 // row is read with 16-byte loads (needs nz % 4 == 0); every cell of the vector is written back
 // (unchanged cells of the other colour keep their value, cells that are not fluid are set to 0, as
 // rbgs_step does). Each update keeps the reference's term order.
+// Block (bx, by, bz) of the launch described above (block shape (32, 4)).
 template <bool L0, int VEC>
-__global__ void __launch_bounds__(128) k_rbgs_colour(float* p, const float* __restrict__ b,
-                                                      const uint8_t* __restrict__ op0,
-                                                      const float4* __restrict__ opc,
-                                                      const uint8_t* __restrict__ mask, float delta, int parity,
-                                                      int nx, int ny, int nz) {
-    const int k0 = (blockIdx.x * blockDim.x + threadIdx.x) * VEC;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
+__device__ __forceinline__ void rbgs_colour_at(int bx, int by, int bz, float* p, const float* __restrict__ b,
+                                               const uint8_t* __restrict__ op0, const float4* __restrict__ opc,
+                                               const uint8_t* __restrict__ mask, float delta, int parity, int nx,
+                                               int ny, int nz) {
+    const int k0 = (bx * 32 + threadIdx.x) * VEC;
+    const int j = by * 4 + threadIdx.y;
+    const int i = bz;
     if (k0 >= nz || j >= ny) return;
     const int sx = ny * nz, sy = nz;
     const int c0 = i * sx + j * sy + k0;
@@ -224,6 +224,15 @@ __global__ void __launch_bounds__(128) k_rbgs_colour(float* p, const float* __re
         for (int q = 0; q < VEC; ++q)
             if (k0 + q < nz) p[c0 + q] = out[q];
     }
+}
+
+template <bool L0, int VEC>
+__global__ void __launch_bounds__(128) k_rbgs_colour(float* p, const float* __restrict__ b,
+                                                      const uint8_t* __restrict__ op0,
+                                                      const float4* __restrict__ opc,
+                                                      const uint8_t* __restrict__ mask, float delta, int parity,
+                                                      int nx, int ny, int nz) {
+    rbgs_colour_at<L0, VEC>(blockIdx.x, blockIdx.y, blockIdx.z, p, b, op0, opc, mask, delta, parity, nx, ny, nz);
 }
 
 }  // namespace clb

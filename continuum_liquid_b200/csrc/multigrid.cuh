@@ -210,13 +210,10 @@ __device__ __forceinline__ float wsumC(const float4* __restrict__ op, const floa
 
 // Fused pressure_rhs (pressure_solve.cl:3-24) + build_finest_operator (multigrid.cl:63-88) into the
 // packed layout. mask is the fluid fraction, as in pressure_solve.py:299-308.
-__global__ void __launch_bounds__(MGT) k_rhs_op0(const float* __restrict__ u, const float* __restrict__ v,
+__device__ __forceinline__ void rhs_op0_at(i64 c, const float* __restrict__ u, const float* __restrict__ v,
                                                   const float* __restrict__ w, const float* __restrict__ ff,
                                                   float* __restrict__ rhs, uint8_t* __restrict__ op0,
                                                   float rho_over_dt, float inv_dx, int nx, int ny, int nz) {
-    const i64 C = (i64)nx * ny * nz;
-    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
-    if (c >= C) return;
     int i, j, k;
     gcoord(c, ny, nz, i, j, k);
     const i64 sx = (i64)ny * nz, sy = nz;
@@ -237,21 +234,28 @@ __global__ void __launch_bounds__(MGT) k_rhs_op0(const float* __restrict__ u, co
     op0[c] = (uint8_t)bits;
 }
 
+__global__ void __launch_bounds__(MGT) k_rhs_op0(const float* __restrict__ u, const float* __restrict__ v,
+                                                  const float* __restrict__ w, const float* __restrict__ ff,
+                                                  float* __restrict__ rhs, uint8_t* __restrict__ op0,
+                                                  float rho_over_dt, float inv_dx, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    rhs_op0_at(c, u, v, w, ff, rhs, op0, rho_over_dt, inv_dx, nx, ny, nz);
+}
+
 // Operator part of restrict_residual (multigrid.cl:127-179) for one coarse level, from any layout:
 // FS = 0 packed finest level, 1 float4 coarse level, 2 FP16 coarse level. CH = true stores the
 // coarse operator in FP16 and counts entries that FP16 does not hold exactly into *inexact (the
 // entries are sums of small integers, exact below 2048).
 template <int FS, bool CH>
-__global__ void __launch_bounds__(MGT) k_coarse_operator(const uint8_t* __restrict__ fop0,
+__device__ __forceinline__ void coarse_operator_at(i64 ci, const uint8_t* __restrict__ fop0,
                                                           const void* __restrict__ fopc_,
                                                           const uint8_t* __restrict__ fmask, void* __restrict__ cop_,
                                                           uint8_t* __restrict__ cmask, int* __restrict__ inexact,
                                                           int fnx, int fny, int fnz, int cnx, int cny, int cnz) {
     constexpr bool FINE0 = FS == 0;
     const float4* __restrict__ fopc = reinterpret_cast<const float4*>(fopc_);
-    const i64 C = (i64)cnx * cny * cnz;
-    const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
-    if (ci >= C) return;
     int I, J, K;
     gcoord(ci, cny, cnz, I, J, K);
     float dsum = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
@@ -309,14 +313,23 @@ __global__ void __launch_bounds__(MGT) k_coarse_operator(const uint8_t* __restri
     }
 }
 
+template <int FS, bool CH>
+__global__ void __launch_bounds__(MGT) k_coarse_operator(const uint8_t* __restrict__ fop0,
+                                                          const void* __restrict__ fopc_,
+                                                          const uint8_t* __restrict__ fmask, void* __restrict__ cop_,
+                                                          uint8_t* __restrict__ cmask, int* __restrict__ inexact,
+                                                          int fnx, int fny, int fnz, int cnx, int cny, int cnz) {
+    const i64 C = (i64)cnx * cny * cnz;
+    const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (ci >= C) return;
+    coarse_operator_at<FS, CH>(ci, fop0, fopc_, fmask, cop_, cmask, inexact, fnx, fny, fnz, cnx, cny, cnz);
+}
+
 // One red-black Gauss-Seidel colour (multigrid.cl:203-230) on either layout.
 template <bool L0>
-__global__ void __launch_bounds__(MGT) k_rbgs(float* p, const float* __restrict__ b, const uint8_t* __restrict__ op0,
+__device__ __forceinline__ void rbgs_at(i64 c, float* p, const float* __restrict__ b, const uint8_t* __restrict__ op0,
                                                const float4* __restrict__ opc, const uint8_t* __restrict__ mask,
                                                float delta, int parity, int nx, int ny, int nz) {
-    const i64 C = (i64)nx * ny * nz;
-    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
-    if (c >= C) return;
     int i, j, k;
     gcoord(c, ny, nz, i, j, k);
     const i64 sx = (i64)ny * nz, sy = nz;
@@ -341,6 +354,16 @@ __global__ void __launch_bounds__(MGT) k_rbgs(float* p, const float* __restrict_
     }
 }
 
+template <bool L0>
+__global__ void __launch_bounds__(MGT) k_rbgs(float* p, const float* __restrict__ b, const uint8_t* __restrict__ op0,
+                                               const float4* __restrict__ opc, const uint8_t* __restrict__ mask,
+                                               float delta, int parity, int nx, int ny, int nz) {
+    const i64 C = (i64)nx * ny * nz;
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    rbgs_at<L0>(c, p, b, op0, opc, mask, delta, parity, nx, ny, nz);
+}
+
 // Residual (multigrid.cl:45-61) at one fine cell for either layout; 0 contribution when not fluid.
 template <bool L0>
 __device__ __forceinline__ float residual_at(const float* p, const float* __restrict__ b,
@@ -361,14 +384,11 @@ __device__ __forceinline__ float residual_at(const float* p, const float* __rest
 // Right-hand-side part of restrict_residual (multigrid.cl:90-180): coarse b = sum of the eight fine
 // residuals in (di, dj, dk) order, coarse p = 0.
 template <bool L0>
-__global__ void __launch_bounds__(MGT) k_restrict(const float* __restrict__ fp, const float* __restrict__ fb,
+__device__ __forceinline__ void restrict_at(i64 ci, const float* __restrict__ fp, const float* __restrict__ fb,
                                                    const uint8_t* __restrict__ fop0, const float4* __restrict__ fopc,
                                                    const uint8_t* __restrict__ fmask, float* __restrict__ cp,
                                                    float* __restrict__ cb, float delta, int fnx, int fny, int fnz,
                                                    int cnx, int cny, int cnz) {
-    const i64 C = (i64)cnx * cny * cnz;
-    const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
-    if (ci >= C) return;
     cp[ci] = 0.0f;
     int I, J, K;
     gcoord(ci, cny, cnz, I, J, K);
@@ -391,7 +411,31 @@ __global__ void __launch_bounds__(MGT) k_restrict(const float* __restrict__ fp, 
     cb[ci] = rhs;
 }
 
+template <bool L0>
+__global__ void __launch_bounds__(MGT) k_restrict(const float* __restrict__ fp, const float* __restrict__ fb,
+                                                   const uint8_t* __restrict__ fop0, const float4* __restrict__ fopc,
+                                                   const uint8_t* __restrict__ fmask, float* __restrict__ cp,
+                                                   float* __restrict__ cb, float delta, int fnx, int fny, int fnz,
+                                                   int cnx, int cny, int cnz) {
+    const i64 C = (i64)cnx * cny * cnz;
+    const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (ci >= C) return;
+    restrict_at<L0>(ci, fp, fb, fop0, fopc, fmask, cp, cb, delta, fnx, fny, fnz, cnx, cny, cnz);
+}
+
 // prolongate (multigrid.cl:182-201) for either layout
+template <bool L0>
+__device__ __forceinline__ void prolong_at(i64 f, const float* __restrict__ ce, float* __restrict__ fp,
+                                                  const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
+                                                  int cnx, int cny, int cnz, int fnx, int fny, int fnz) {
+    int i, j, k;
+    gcoord(f, fny, fnz, i, j, k);
+    const bool fl = L0 ? ((__ldg(fop0 + f) & 64u) != 0u) : (__ldg(fmask + f) != 0);
+    if (!interior(i, j, k, fnx, fny, fnz) || !fl) return;
+    const int I = min((i - 1) / 2 + 1, cnx - 2), J = min((j - 1) / 2 + 1, cny - 2), K = min((k - 1) / 2 + 1, cnz - 2);
+    fp[f] += __ldg(ce + gidx(I, J, K, cny, cnz));
+}
+
 template <bool L0>
 __global__ void __launch_bounds__(MGT) k_prolong(const float* __restrict__ ce, float* __restrict__ fp,
                                                   const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
@@ -399,12 +443,7 @@ __global__ void __launch_bounds__(MGT) k_prolong(const float* __restrict__ ce, f
     const i64 C = (i64)fnx * fny * fnz;
     const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
     if (f >= C) return;
-    int i, j, k;
-    gcoord(f, fny, fnz, i, j, k);
-    const bool fl = L0 ? ((__ldg(fop0 + f) & 64u) != 0u) : (__ldg(fmask + f) != 0);
-    if (!interior(i, j, k, fnx, fny, fnz) || !fl) return;
-    const int I = min((i - 1) / 2 + 1, cnx - 2), J = min((j - 1) / 2 + 1, cny - 2), K = min((k - 1) / 2 + 1, cnz - 2);
-    fp[f] += __ldg(ce + gidx(I, J, K, cny, cnz));
+    prolong_at<L0>(f, ce, fp, fop0, fmask, cnx, cny, cnz, fnx, fny, fnz);
 }
 
 // coarse_smooth (multigrid.cl:232-264): one block runs all colour sweeps of the coarsest level,
@@ -416,12 +455,10 @@ constexpr int COARSE_SMEM_CELLS = 8192;  // 25 bytes per cell -> 200 KB
 // H = true: an FP16 level (p, b, operator as __half, shared-memory path only); its scaled system uses
 // kappa = scale[2] in place of delta^2 (mg_half.cuh).
 template <bool SMEM, bool L0, bool H = false>
-__global__ void __launch_bounds__(COARSE_THREADS) k_coarse_solve(float* p, const float* __restrict__ b,
-                                                                  const uint8_t* __restrict__ op0,
-                                                                  const float4* __restrict__ opc,
-                                                                  const uint8_t* __restrict__ mask, float delta,
-                                                                  int iterations, int nx, int ny, int nz,
-                                                                  const float* __restrict__ scale = nullptr) {
+__device__ __forceinline__ void coarse_solve_block(float* p, const float* __restrict__ b,
+                                                   const uint8_t* __restrict__ op0, const float4* __restrict__ opc,
+                                                   const uint8_t* __restrict__ mask, float delta, int iterations,
+                                                   int nx, int ny, int nz, const float* __restrict__ scale) {
     static_assert(!H || (SMEM && !L0), "FP16 levels are coarse levels solved from shared memory");
     extern __shared__ __align__(16) unsigned char smem[];
     const int C = nx * ny * nz;
@@ -478,6 +515,16 @@ __global__ void __launch_bounds__(COARSE_THREADS) k_coarse_solve(float* p, const
         }
 }
 
+template <bool SMEM, bool L0, bool H = false>
+__global__ void __launch_bounds__(COARSE_THREADS) k_coarse_solve(float* p, const float* __restrict__ b,
+                                                                  const uint8_t* __restrict__ op0,
+                                                                  const float4* __restrict__ opc,
+                                                                  const uint8_t* __restrict__ mask, float delta,
+                                                                  int iterations, int nx, int ny, int nz,
+                                                                  const float* __restrict__ scale = nullptr) {
+    coarse_solve_block<SMEM, L0, H>(p, b, op0, opc, mask, delta, iterations, nx, ny, nz, scale);
+}
+
 static inline size_t coarse_smem_bytes(int C) {
     return (size_t)C * 8 + (size_t)(((4 - (2 * C) % 4) % 4) * 4) + (size_t)C * 16;
 }
@@ -500,17 +547,15 @@ constexpr int RN_THREADS = 256;
 // fluid cells): it is the right-hand side of the next correction solve.
 enum { RES_NORM = 0, RES_IR = 1, RES_FCG = 2 };
 
+// Block `blk` of `nblk` blocks sharing the rows; its partial sums go to *partial.
 template <typename PT, int MODE>
-__global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restrict__ p_in,
-                                                               const float* __restrict__ e,
-                                                               double* __restrict__ p_out,
-                                                               const float* __restrict__ b,
-                                                               const uint8_t* __restrict__ op0, double inv_delta2,
-                                                               int nx, int ny, int nz, float* __restrict__ r_out,
-                                                               double2* __restrict__ partials,
-                                                               const float* __restrict__ d_in = nullptr,
-                                                               float* __restrict__ d_out = nullptr,
-                                                               const double* __restrict__ state = nullptr) {
+__device__ __forceinline__ void residual_rows_block(int blk, int nblk, const PT* __restrict__ p_in,
+                                                    const float* __restrict__ e, double* __restrict__ p_out,
+                                                    const float* __restrict__ b, const uint8_t* __restrict__ op0,
+                                                    double inv_delta2, int nx, int ny, int nz,
+                                                    float* __restrict__ r_out, double2* __restrict__ partial,
+                                                    const float* __restrict__ d_in, float* __restrict__ d_out,
+                                                    const double* __restrict__ state) {
     __shared__ double2 s_red[RN_THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int sx = ny * nz, sy = nz;
@@ -527,7 +572,7 @@ __global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restri
         return (double)__ldg(p_in + q);
     };
     const int rows = nx * ny;
-    for (int r = blockIdx.x * (RN_THREADS / 32) + warp; r < rows; r += gridDim.x * (RN_THREADS / 32)) {
+    for (int r = blk * (RN_THREADS / 32) + warp; r < rows; r += nblk * (RN_THREADS / 32)) {
         const int i = r / ny, j = r - i * ny;
         const bool row_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
         const int base = r * nz;
@@ -565,8 +610,23 @@ __global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restri
             t.x += s_red[q].x;
             t.y += s_red[q].y;
         }
-        partials[blockIdx.x] = t;
+        *partial = t;
     }
+}
+
+template <typename PT, int MODE>
+__global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restrict__ p_in,
+                                                               const float* __restrict__ e,
+                                                               double* __restrict__ p_out,
+                                                               const float* __restrict__ b,
+                                                               const uint8_t* __restrict__ op0, double inv_delta2,
+                                                               int nx, int ny, int nz, float* __restrict__ r_out,
+                                                               double2* __restrict__ partials,
+                                                               const float* __restrict__ d_in = nullptr,
+                                                               float* __restrict__ d_out = nullptr,
+                                                               const double* __restrict__ state = nullptr) {
+    residual_rows_block<PT, MODE>(blockIdx.x, gridDim.x, p_in, e, p_out, b, op0, inv_delta2, nx, ny, nz, r_out,
+                                  partials + blockIdx.x, d_in, d_out, state);
 }
 
 // Flexible conjugate gradients with the W-cycle as preconditioner (Notay's FCG with truncation 1;
@@ -581,16 +641,16 @@ struct Sum4 {
     double x, y, z, w;
 };
 
-__global__ void __launch_bounds__(RN_THREADS) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
-                                                          const float* __restrict__ r,
-                                                          const uint8_t* __restrict__ op0, double inv_delta2, int nx,
-                                                          int ny, int nz, Sum4* __restrict__ partials) {
+__device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* __restrict__ z,
+                                               const float* __restrict__ d, const float* __restrict__ r,
+                                               const uint8_t* __restrict__ op0, double inv_delta2, int nx, int ny,
+                                               int nz, Sum4* __restrict__ partial) {
     __shared__ Sum4 s_red[RN_THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int sx = ny * nz, sy = nz;
     Sum4 t = {0.0, 0.0, 0.0, 0.0};
     const int rows = nx * ny;
-    for (int q = blockIdx.x * (RN_THREADS / 32) + warp; q < rows; q += gridDim.x * (RN_THREADS / 32)) {
+    for (int q = blk * (RN_THREADS / 32) + warp; q < rows; q += nblk * (RN_THREADS / 32)) {
         const int i = q / ny, j = q - i * ny;
         if (i < 1 || i > nx - 2 || j < 1 || j > ny - 2) continue;
         const int base = q * nz;
@@ -631,14 +691,22 @@ __global__ void __launch_bounds__(RN_THREADS) k_fcg_dots(const float* __restrict
             a.z += s_red[q].z;
             a.w += s_red[q].w;
         }
-        partials[blockIdx.x] = a;
+        *partial = a;
     }
+}
+
+__global__ void __launch_bounds__(RN_THREADS) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
+                                                          const float* __restrict__ r,
+                                                          const uint8_t* __restrict__ op0, double inv_delta2, int nx,
+                                                          int ny, int nz, Sum4* __restrict__ partials) {
+    fcg_dots_block(blockIdx.x, gridDim.x, z, d, r, op0, inv_delta2, nx, ny, nz, partials + blockIdx.x);
 }
 
 // Fixed-order sum of the k_fcg_dots partials, then the FCG scalars in
 // state = {alpha, beta, d.Ad of the current direction, 1 once a direction exists}.
 // The first direction is z itself (beta = 0).
-__global__ void k_fcg_scalars(const Sum4* __restrict__ partials, int count, double* __restrict__ state) {
+__device__ __forceinline__ void fcg_scalars_block(const Sum4* __restrict__ partials, int count,
+                                                  double* __restrict__ state) {
     __shared__ Sum4 s[256];
     Sum4 t = {0.0, 0.0, 0.0, 0.0};
     for (int q = threadIdx.x; q < count; q += 256) {
@@ -674,8 +742,13 @@ __global__ void k_fcg_scalars(const Sum4* __restrict__ partials, int count, doub
     }
 }
 
+__global__ void k_fcg_scalars(const Sum4* __restrict__ partials, int count, double* __restrict__ state) {
+    fcg_scalars_block(partials, count, state);
+}
+
 // Fixed-order reduction of the block partials (deterministic for a given grid size).
-__global__ void k_reduce_partials(const double2* __restrict__ partials, int count, double2* __restrict__ out) {
+__device__ __forceinline__ void reduce_partials_block(const double2* __restrict__ partials, int count,
+                                                      double2* __restrict__ out) {
     __shared__ double2 s[256];
     double2 t = make_double2(0.0, 0.0);
     for (int q = threadIdx.x; q < count; q += 256) {
@@ -694,16 +767,25 @@ __global__ void k_reduce_partials(const double2* __restrict__ partials, int coun
     if (threadIdx.x == 0) *out = s[0];
 }
 
+__global__ void k_reduce_partials(const double2* __restrict__ partials, int count, double2* __restrict__ out) {
+    reduce_partials_block(partials, count, out);
+}
+
 // p64 = warm-start pressure at interior fluid cells, 0 elsewhere (cells that left the liquid since
 // the previous step must not keep a stale pressure).
+__device__ __forceinline__ void ir_init_at(i64 c, const float* __restrict__ p, const uint8_t* __restrict__ op0,
+                                                  double* __restrict__ p64, int nx, int ny, int nz) {
+    int i, j, k;
+    gcoord(c, ny, nz, i, j, k);
+    p64[c] = (interior(i, j, k, nx, ny, nz) && (__ldg(op0 + c) & 64u)) ? (double)__ldg(p + c) : 0.0;
+}
+
 __global__ void __launch_bounds__(MGT) k_ir_init(const float* __restrict__ p, const uint8_t* __restrict__ op0,
                                                   double* __restrict__ p64, int nx, int ny, int nz) {
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c >= C) return;
-    int i, j, k;
-    gcoord(c, ny, nz, i, j, k);
-    p64[c] = (interior(i, j, k, nx, ny, nz) && (__ldg(op0 + c) & 64u)) ? (double)__ldg(p + c) : 0.0;
+    ir_init_at(c, p, op0, p64, nx, ny, nz);
 }
 
 __global__ void __launch_bounds__(MGT) k_ir_update(double* __restrict__ p64, const float* __restrict__ e, i64 C) {

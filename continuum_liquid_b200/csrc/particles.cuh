@@ -182,6 +182,30 @@ __global__ void __launch_bounds__(PT) k_particle_obstacle_bc(float* __restrict__
 // 69-97) and obstacle push-out (boundary_conditions.cl:175-264), in the reference's order, with the
 // particle records staged through shared memory by 16-byte loads and stores. The previous position
 // lives in registers; it is written out only when the caller asks for it.
+// The per-particle part of k_particle_update on registers (prev, when non-null, is this particle's
+// previous-position record).
+__device__ __forceinline__ void particle_update_one(float& p0, float& p1, float& p2, float& v0, float& v1, float& v2,
+                                                    float* __restrict__ prev, const float* u, const float* v,
+                                                    const float* w, const float* ou, const float* ov, const float* ow,
+                                                    const uint8_t* __restrict__ obs, float inv_dx, int nx, int ny,
+                                                    int nz, float flip_ratio, float dt, float lower, float ux,
+                                                    float uy, float uz) {
+    g2p_velocity(v0, v1, v2, p0, p1, p2, u, v, w, ou, ov, ow, inv_dx, nx, ny, nz, flip_ratio);
+    const float q0 = p0, q1 = p1, q2 = p2;
+    if (prev) {
+        prev[0] = q0;
+        prev[1] = q1;
+        prev[2] = q2;
+    }
+    p0 = p0 + dt * v0;
+    p1 = p1 + dt * v1;
+    p2 = p2 + dt * v2;
+    domain_bc_axis(p0, v0, lower, ux);
+    domain_bc_axis(p1, v1, lower, uy);
+    domain_bc_axis(p2, v2, lower, uz);
+    if (obs) obstacle_bc(p0, p1, p2, q0, q1, q2, v0, v1, v2, obs, inv_dx, nx, ny, nz);
+}
+
 __global__ void __launch_bounds__(PT) k_particle_update(float* __restrict__ pos, float* __restrict__ vel,
                                                          float* __restrict__ prev_out, const float* u, const float* v,
                                                          const float* w, const float* ou, const float* ov,
@@ -199,20 +223,8 @@ __global__ void __launch_bounds__(PT) k_particle_update(float* __restrict__ pos,
         const int t = 3 * threadIdx.x;
         float p0 = sp[t], p1 = sp[t + 1], p2 = sp[t + 2];
         float v0 = sv[t], v1 = sv[t + 1], v2 = sv[t + 2];
-        g2p_velocity(v0, v1, v2, p0, p1, p2, u, v, w, ou, ov, ow, inv_dx, nx, ny, nz, flip_ratio);
-        const float q0 = p0, q1 = p1, q2 = p2;
-        if (prev_out) {
-            prev_out[3 * p] = q0;
-            prev_out[3 * p + 1] = q1;
-            prev_out[3 * p + 2] = q2;
-        }
-        p0 = p0 + dt * v0;
-        p1 = p1 + dt * v1;
-        p2 = p2 + dt * v2;
-        domain_bc_axis(p0, v0, lower, ux);
-        domain_bc_axis(p1, v1, lower, uy);
-        domain_bc_axis(p2, v2, lower, uz);
-        if (obs) obstacle_bc(p0, p1, p2, q0, q1, q2, v0, v1, v2, obs, inv_dx, nx, ny, nz);
+        particle_update_one(p0, p1, p2, v0, v1, v2, prev_out ? prev_out + 3 * p : nullptr, u, v, w, ou, ov, ow, obs,
+                            inv_dx, nx, ny, nz, flip_ratio, dt, lower, ux, uy, uz);
         sp[t] = p0;
         sp[t + 1] = p1;
         sp[t + 2] = p2;

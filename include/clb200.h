@@ -355,6 +355,113 @@ int clb_voxelise_mesh(const float* triangles, uint8_t* mask, int triangle_count,
 /* The ray direction of voxelise_mesh.cl:24 as three floats (host helper). */
 int clb_voxelise_direction(float* out3);
 
+/* ---- batched scenes (no counterpart in the reference, which bakes one scene at a time) -------
+ *
+ * Many independent scenes of different grid sizes advance together: every field of a batch holds the
+ * scenes' grids back to back (level 0 for the simulation fields, one array per multigrid level for
+ * the coarse levels), the particles of all scenes are one array, and each stage is one launch over
+ * all scenes. A thread finds its scene from the prefix of the items (cells, particles or blocks) of
+ * the scenes in the launch (a clb_batch_list) and runs the single-scene stage's code on that scene's
+ * part, so each scene's values equal a single-scene run's. Bin keys are offset by each scene's cell
+ * base, so one scan and one stable sort over the whole batch bin every scene at once. */
+#define CLB_BATCH_MAX_SCENES 64
+
+typedef struct clb_batch_scene {
+    int32_t levels;                         /* multigrid levels of this scene */
+    int32_t bottom;                         /* level run as one single-block bottom visit, -1: none */
+    int32_t shape[CLB_MG_MAX_LEVELS][3];    /* per level, ghost layer included */
+    int64_t base[CLB_MG_MAX_LEVELS];        /* first element of this scene's level-l cells */
+    int64_t particle_base;                  /* first particle of this scene */
+    int64_t particles;                      /* particle count */
+    float delta;                            /* float32(dx), the multigrid spacing */
+    float inv_dx;                           /* float32(1/dx) */
+    float inv_dx2;                          /* float32(1/dx^2) */
+    float rho_over_dt;                      /* float32(rho/dt) */
+    float dt_over_rho;                      /* float32(dt/rho) */
+    float lower;                            /* particle domain: float32(1.001 dx) */
+    float upper[3];                         /* float32((n - 1.001) dx) per axis */
+    int32_t pad;
+} clb_batch_scene;
+
+typedef struct clb_batch_list {             /* the scenes of one launch and the prefix of their items */
+    const int32_t* scene;                   /* device int32[count]: scene indices */
+    const int64_t* start;                   /* device int64[count + 1]: item prefix (start[0] = 0) */
+    int32_t count;
+    int32_t pad;
+    int64_t total;                          /* start[count] (host copy) */
+} clb_batch_list;
+
+typedef struct clb_batch {
+    int32_t scenes;
+    int32_t levels;                         /* deepest scene's level count */
+    const clb_batch_scene* geom;            /* device [scenes] */
+    const clb_batch_scene* geom_host;       /* host copy of the same table */
+    clb_batch_list particles;               /* every scene; items = its particles */
+    clb_batch_list cells[CLB_MG_MAX_LEVELS];       /* scenes having level l; items = their level-l cells */
+    clb_batch_list recurse[CLB_MG_MAX_LEVELS];     /* W-cycle: scenes that smooth and recurse at level l;
+                                                      items = level-l cells */
+    clb_batch_list recurse_coarse[CLB_MG_MAX_LEVELS]; /* the same scenes; items = level-(l+1) cells */
+    clb_batch_list bottom[CLB_MG_MAX_LEVELS];      /* scenes whose bottom visit is at level l; items = 1 each */
+    clb_batch_list coarse[CLB_MG_MAX_LEVELS];      /* scenes whose coarsest level l is solved on its own */
+    clb_batch_list colour0;                 /* every scene; items = blocks of the level-0 row sweep */
+    int32_t sweep0;                         /* level-0 sweep: 1 rows (needs colour0), 4 one thread per cell */
+    int32_t vec0;                           /* 4: every scene's nz and level-0 base are multiples of 4 */
+    int32_t reduce_blocks;                  /* blocks per scene of the FP64 reductions */
+    int32_t bottom_ka, bottom_kb;           /* register tiles of the bottom visit (largest scene) */
+    int32_t pad;
+    int64_t bottom_smem;                    /* dynamic shared memory of the bottom visit (largest scene) */
+    uint8_t* op0;                           /* level-0 packed operator of all scenes */
+    float* p[CLB_MG_MAX_LEVELS];            /* levels >= 1 */
+    float* b[CLB_MG_MAX_LEVELS];
+    uint8_t* mask[CLB_MG_MAX_LEVELS];
+    void* op[CLB_MG_MAX_LEVELS];            /* float4 per cell */
+} clb_batch;
+
+/* Stage API over a batch (pointers are the batch-wide arrays; per-scene constants come from geom).
+ * particle_to_grid: zero-fill, count with scene-offset keys, one scan, one stable sort, P2G
+ * (clb_particle_to_grid per scene). Workspace as clb_particle_to_grid for the batch totals. */
+int clb_batch_particle_to_grid(const clb_batch* b, const float* particles, const float* velocity,
+                               float* particles_work, float* velocity_work, float* u, float* v, float* w,
+                               float* fluid_fraction, int32_t* bin_counts, int32_t* bin_offsets, int32_t* keys,
+                               int32_t* ranks, int32_t* perm, int32_t* slot_keys, void* scan_scratch,
+                               int64_t scan_scratch_bytes, float inv_particles_per_cell, void* stream);
+int clb_batch_update_velocity(const clb_batch* b, const float* u, const float* v, const float* w, float* result_u,
+                              float* result_v, float* result_w, const float* fluid_fraction, float gravity_x,
+                              float gravity_y, float gravity_z, float force_x, float force_y, float force_z, float rho,
+                              float nu, float dt, void* stream);
+int clb_batch_grid_domain_bc(const clb_batch* b, float* u, float* v, float* w, void* stream);
+int clb_batch_grid_obstacle_bc(const clb_batch* b, float* u, float* v, float* w, float* fluid_fraction,
+                               const uint8_t* obstacle, void* stream);
+/* pressure rhs + packed finest operator (clb_mg_rhs_operator), then every coarse operator. */
+int clb_batch_rhs_operator(const clb_batch* b, const float* u, const float* v, const float* w,
+                           const float* fluid_fraction, float* rhs, void* stream);
+/* One W-cycle of every scene (clb_mg_w_cycle per scene). */
+int clb_batch_w_cycle(const clb_batch* b, float* x, const float* rhs, int pre_smooth, int post_smooth,
+                      int coarse_iterations, void* stream);
+/* Per-scene FP64 sums (out[2 s] = sum r^2, out[2 s + 1] = sum b^2) of clb_mg_residual_norms;
+ * partials: scenes * reduce_blocks double2. */
+int clb_batch_residual_norms(const clb_batch* b, const void* p, int p_is_double, const float* rhs, float* r_out,
+                             void* partials, double* out, void* stream);
+int clb_batch_ir_init(const clb_batch* b, const float* p32, double* p64, void* stream);
+/* p32 = (float) p64, then the Neumann ghost copy of both (clb_mg_ir_store + clb_neumann_domain_bc[_f64]). */
+int clb_batch_ir_store(const clb_batch* b, double* p64, float* p32, void* stream);
+/* clb_mg_fcg_dots / clb_mg_fcg_step per scene; state: double[4 * scenes]; partials4: scenes *
+ * reduce_blocks * 32 bytes; partials: scenes * reduce_blocks double2; out: double[2 * scenes]. */
+int clb_batch_fcg_dots(const clb_batch* b, const float* z, const float* d, const float* r, void* partials4,
+                       double* state, void* stream);
+int clb_batch_fcg_step(const clb_batch* b, const double* p64_in, const float* z, const float* d_in, double* p64_out,
+                       float* d_out, const double* state, const float* rhs, float* r_out, void* partials, double* out,
+                       void* stream);
+/* pressure_correction (FP32 pressure, p_is_double = 0) or clb_pressure_correction_f64 per scene, and
+ * the FP32 Neumann ghost copy (parity mode). */
+int clb_batch_pressure_correction(const clb_batch* b, float* u, float* v, float* w, const void* pressure,
+                                  int p_is_double, void* stream);
+int clb_batch_neumann_domain_bc(const clb_batch* b, float* pressure, void* stream);
+/* clb_particle_update per scene (obstacle may be an all-zero mask for scenes without a collider). */
+int clb_batch_particle_update(const clb_batch* b, float* particles, float* velocity, const float* u, const float* v,
+                              const float* w, const float* u_old, const float* v_old, const float* w_old,
+                              const uint8_t* obstacle, float flip_ratio, float dt, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

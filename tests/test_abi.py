@@ -30,7 +30,7 @@ def test_python_signature_table_covers_the_header():
 
 def test_load_library_sets_signatures_and_pure_helpers():
     lib = backend.load_library()
-    assert lib.clb_abi_version() == 5
+    assert lib.clb_abi_version() == 6
     for count in (0, 1, 4096, 4097, 16777216):
         assert lib.clb_scan_scratch_bytes(count) == backend.Backend.scan_scratch_bytes_static(count)
     assert lib.clb_mg_residual_partials(1000) == 4
@@ -58,3 +58,36 @@ def test_backend_without_gpu_fails_loudly(monkeypatch):
     monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
     with pytest.raises(RuntimeError, match="CUDA"):
         backend.Backend(0)
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """sizeof/offsetof of the header's structs, as gcc lays them out, against the ctypes mirrors."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or "/usr/bin/gcc"
+    root = Path(__file__).resolve().parents[1]
+    src = tmp_path / "layout.c"
+    fields = {
+        "clb_mg_hierarchy": ["fp16_level", "op0", "sweep", "fp16_scale", "rhs_norms", "fp16_inexact"],
+        "clb_batch_scene": ["base", "particle_base", "delta", "upper", "pad"],
+        "clb_batch_list": ["start", "count", "total"],
+        "clb_batch": ["geom_host", "particles", "cells", "colour0", "sweep0", "bottom_smem", "op0", "op"],
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "clb200.h"', "int main(void) {"]
+    for struct, names in fields.items():
+        lines.append(f'printf("{struct} size %zu\\n", sizeof({struct}));')
+        for n in names:
+            lines.append(f'printf("{struct} {n} %zu\\n", offsetof({struct}, {n}));')
+    lines.append("return 0; }")
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(root / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    mirrors = {"clb_mg_hierarchy": backend.MGHierarchy, "clb_batch_scene": backend.BatchScene,
+               "clb_batch_list": backend.BatchList, "clb_batch": backend.Batch}
+    for line in filter(None, out):
+        struct, name, value = line.split()
+        m = mirrors[struct]
+        got = ctypes.sizeof(m) if name == "size" else getattr(m, name).offset
+        assert got == int(value), (struct, name, got, value)
