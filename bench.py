@@ -62,11 +62,76 @@ def parse_args():
     ap.add_argument("--coarse-fp16", choices=["auto", "on", "off"], default="auto",
                     help="FP16 storage of the coarse levels <= 64^3 in the timed steps (auto: when the Poisson "
                          "comparison shows the convergence factor and time hold)")
-    ap.add_argument("--case", choices=["step", "sweep0"], default="step",
+    ap.add_argument("--case", choices=["step", "sweep0", "batch"], default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
-                         "(no particles: a small-memory case for profiling the dominant kernel)")
+                         "(no particles: a small-memory case for profiling the dominant kernel); batch: the batched "
+                         "uneven-scenes workload (32 scenes of sizes 48-160, one launch per stage)")
+    ap.add_argument("--scenes", type=int, default=32, help="scenes of --case batch")
+    ap.add_argument("--sequential-steps", type=int, default=2,
+                    help="steps of the one-scene-at-a-time comparison of --case batch (0: skip)")
     ap.add_argument("--sweeps", type=int, default=4, help="red-black iterations of --case sweep0")
     return ap.parse_args()
+
+
+def batch_case(args):
+    """Batched uneven scenes: every scene advances one step per batch step, each pressure solve to TOL."""
+    import torch
+
+    from continuum_liquid_b200 import batch, scenes, solver
+    from continuum_liquid_b200.backend import Backend
+
+    kernels = Backend(0)
+    scs = scenes.uneven_batch(args.scenes, seed=0)
+    t0 = time.perf_counter()
+    b = batch.BatchedFlip(kernels, scs, tol=TOL)
+    setup_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        b.step()
+    torch.cuda.synchronize()
+    launches0 = kernels.launch_count()
+    replays0 = b.graph_replays
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(0) as clocks:
+        e0.record()
+        for _ in range(args.steps):
+            stats.append(b.step())
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    line = {
+        "case": "batch", "metric": "scene-steps/s of the batched uneven scenes", "unit": "scene-steps/s",
+        "value": len(scs) * 1e3 / ms, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+        "config": {"workload": f"uneven_batch_{len(scs)}", "sizes": [s.grid_shape[0] for s in scs],
+                   "particles": b.n, "cells": b.C0, "pressure_tolerance": TOL,
+                   "pressure_solver": "per-scene flexible CG with the W-cycle, FP64 accumulation"},
+        "particles_per_s": b.n * 1e3 / ms,
+        "cycles_per_step": [st.cycles for st in stats],
+        "rel_residual_max": max(max(st.rel_residual) for st in stats),
+        "launches_outside_graphs_per_step": (kernels.launch_count() - launches0) / args.steps,
+        "graph_replays_per_step": (b.graph_replays - replays0) / args.steps, "setup_s": setup_s,
+        "clocks": clocks.summary(),
+    }
+    if args.sequential_steps > 0:
+        # the same scenes advanced one at a time by the single-scene solver (graphs in its pressure solve)
+        del b
+        torch.cuda.empty_cache()
+        sims = [solver.scene_solver(kernels, sc, solver.StepOptions(flip_ratio=sc.flip_ratio, tol=TOL,
+                                                                    gravity=sc.gravity, rho=sc.rho, nu=sc.nu))
+                for sc in scs]
+        for sim in sims:
+            sim.step()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.sequential_steps):
+            for sim in sims:
+                sim.step()
+        e1.record()
+        torch.cuda.synchronize()
+        seq_ms = e0.elapsed_time(e1) / args.sequential_steps
+        line["sequential_single_scene"] = {"ms_per_batch_step": seq_ms, "scene_steps_per_s": len(scs) * 1e3 / seq_ms}
+        line["speedup_vs_sequential"] = seq_ms / ms
+    print(json.dumps(line), flush=True)
 
 
 def sweep_case(args):
@@ -537,6 +602,8 @@ def main():
         reference_arm(args)
     elif args.case == "sweep0":
         sweep_case(args)
+    elif args.case == "batch":
+        batch_case(args)
     else:
         our_arm(args)
 
