@@ -62,7 +62,7 @@ def parse_args():
     ap.add_argument("--coarse-fp16", choices=["auto", "on", "off"], default="auto",
                     help="FP16 storage of the coarse levels <= 64^3 in the timed steps (auto: when the Poisson "
                          "comparison shows the convergence factor and time hold)")
-    ap.add_argument("--case", choices=["step", "sweep0", "batch"], default="step",
+    ap.add_argument("--case", choices=["step", "sweep0", "batch", "unet"], default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
                          "(no particles: a small-memory case for profiling the dominant kernel); batch: the batched "
                          "uneven-scenes workload (32 scenes of sizes 48-160, one launch per stage)")
@@ -132,6 +132,75 @@ def batch_case(args):
         line["sequential_single_scene"] = {"ms_per_batch_step": seq_ms, "scene_steps_per_s": len(scs) * 1e3 / seq_ms}
         line["speedup_vs_sequential"] = seq_ms / ms
     print(json.dumps(line), flush=True)
+
+
+def unet_flops_per_voxel() -> float:
+    """Convolution FLOPs of one forward pass per full-resolution voxel (2 * 27 * cin * cout per conv
+    and voxel of its level; levels 1 and 2 have 1/8 and 1/64 of the voxels)."""
+    from continuum_liquid_b200 import learned
+
+    level = {"enc0a": 0, "enc0b": 0, "enc1a": 1, "enc1b": 1, "enc2a": 2, "enc2b": 2, "dec1a": 1, "dec1b": 1,
+             "dec0a": 0, "dec0b": 0}
+    return sum(2.0 * 27 * cin * cout / 8 ** level[name] for name, cin, cout in learned.LAYERS)
+
+
+def unet_case(args):
+    """U-Net of the learned warm start: forward pass at size^3 and one training step (batch 8 of 64^3
+    crops: forward, loss, backward, Adam), device-timed; FLOP rates against the measured BF16 peak."""
+    import torch
+
+    from continuum_liquid_b200 import learned
+    from continuum_liquid_b200.backend import Backend
+
+    kernels = Backend(0)
+    net = learned.UNet(kernels, seed=0)
+    fpv = unet_flops_per_voxel()
+    peak = None
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        peak = json.loads(path.read_text()).get("bf16_tflops")
+    out = {"case": "unet", "flop_per_voxel_forward": fpv, "peak_bf16_tflops": peak}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for n in sorted({64, 128, args.size}):
+        vol = learned.Vol(1, n, n, n)
+        gen = torch.Generator(device="cuda").manual_seed(n)
+        net.buffers(vol)["x0"].copy_(torch.randn(vol.voxels, 8, device="cuda", generator=gen).to(torch.bfloat16))
+        net.forward(vol)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(3):
+            net.forward(vol)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        out[f"forward_{n}^3_ms"] = ms
+        out[f"forward_{n}^3_tflops"] = fpv * vol.voxels / (ms * 1e-3) / 1e12
+        net._buffers.clear()
+        torch.cuda.empty_cache()
+    vol = learned.Vol(8, 64, 64, 64)
+    b = net.buffers(vol)
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    b["x0"].copy_(torch.randn(vol.voxels, 8, device="cuda", generator=gen).to(torch.bfloat16))
+    b["target"].copy_(torch.randn(vol.voxels, device="cuda", generator=gen))
+    b["mask"].fill_(1.0)
+
+    def train_step():
+        net.forward(vol)
+        net.loss_and_grad(vol)
+        net.backward(vol)
+        net.adam_step(1e-4)
+
+    train_step()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(3):
+        train_step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 3
+    out["train_step_batch8_64^3_ms"] = ms
+    out["train_step_tflops"] = 3.0 * fpv * vol.voxels / (ms * 1e-3) / 1e12  # forward + 2x for the backward
+    print(json.dumps(out), flush=True)
 
 
 def sweep_case(args):
@@ -604,6 +673,8 @@ def main():
         sweep_case(args)
     elif args.case == "batch":
         batch_case(args)
+    elif args.case == "unet":
+        unet_case(args)
     else:
         our_arm(args)
 

@@ -12,6 +12,7 @@
 #include "voxelise.cuh"
 #include "tc_gemm.cuh"
 #include "conv3d.cuh"
+#include "conv_win.cuh"
 
 #include <mutex>
 
@@ -28,9 +29,8 @@ static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 
 template <int N, bool DG>
-static cudaError_t conv_rows_attr() {
-    return cudaFuncSetAttribute(conv::k_conv_rows<N, DG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tc::tile_smem_bytes<N>());
+static cudaError_t conv_win_attr() {
+    return cudaFuncSetAttribute(conv::k_conv_win<N, DG>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
 }
 template <int N>
 static cudaError_t conv_wgrad_attr() {
@@ -39,14 +39,14 @@ static cudaError_t conv_wgrad_attr() {
 }
 static int conv_set_attributes() {
     cudaError_t e = cudaSuccess;
-    e = e != cudaSuccess ? e : conv_rows_attr<16, false>();
-    e = e != cudaSuccess ? e : conv_rows_attr<32, false>();
-    e = e != cudaSuccess ? e : conv_rows_attr<64, false>();
-    e = e != cudaSuccess ? e : conv_rows_attr<16, true>();
-    e = e != cudaSuccess ? e : conv_rows_attr<32, true>();
-    e = e != cudaSuccess ? e : conv_rows_attr<48, true>();
-    e = e != cudaSuccess ? e : conv_rows_attr<64, true>();
-    e = e != cudaSuccess ? e : conv_rows_attr<96, true>();
+    e = e != cudaSuccess ? e : conv_win_attr<16, false>();
+    e = e != cudaSuccess ? e : conv_win_attr<32, false>();
+    e = e != cudaSuccess ? e : conv_win_attr<64, false>();
+    e = e != cudaSuccess ? e : conv_win_attr<16, true>();
+    e = e != cudaSuccess ? e : conv_win_attr<32, true>();
+    e = e != cudaSuccess ? e : conv_win_attr<48, true>();
+    e = e != cudaSuccess ? e : conv_win_attr<64, true>();
+    e = e != cudaSuccess ? e : conv_win_attr<96, true>();
     e = e != cudaSuccess ? e : conv_wgrad_attr<16>();
     e = e != cudaSuccess ? e : conv_wgrad_attr<32>();
     e = e != cudaSuccess ? e : conv_wgrad_attr<64>();
@@ -960,24 +960,22 @@ int clb_conv3d_forward(const void* x, const void* wf, const float* bias, void* y
     CLB_REQUIRE(x && wf && y, "conv3d_forward: null pointer");
     CLB_REQUIRE(cin > 0 && cin % 8 == 0, "conv3d_forward: cin=%d must be a positive multiple of 8", cin);
     CLB_REQUIRE(kpad % 64 == 0 && kpad >= 27 * cin, "conv3d_forward: kpad=%d must be a multiple of 64 >= 27*cin", kpad);
+    CLB_REQUIRE(cout == 16 || cout == 32 || cout == 64, "conv3d_forward: cout=%d not supported (16, 32, 64)", cout);
+    conv::WinPlan pl;
+    CLB_REQUIRE(conv::win_plan(D, H, W, cin, cout, B, pl), "conv3d_forward: no block shape fits %dx%dx%d", D, H, W);
     const conv::Vol g{B, D, H, W};
-    const unsigned blocks = (unsigned)(((i64)B * D * H * W + tc::TC_M - 1) / tc::TC_M);
+    const unsigned blocks = (unsigned)((i64)B * D * pl.ytiles * pl.xtiles);
     cudaStream_t s = CLB_STREAM(stream);
     const auto* X = (const __nv_bfloat16*)x;
     const auto* Wf = (const __nv_bfloat16*)wf;
     auto* Y = (__nv_bfloat16*)y;
-    if (cout == 16)
-        conv::k_conv_rows<16, false><<<blocks, tc::TC_THREADS, tc::tile_smem_bytes<16>(), s>>>(X, Wf, bias, nullptr, Y, g,
-                                                                                              cin, kpad, relu);
-    else if (cout == 32)
-        conv::k_conv_rows<32, false><<<blocks, tc::TC_THREADS, tc::tile_smem_bytes<32>(), s>>>(X, Wf, bias, nullptr, Y, g,
-                                                                                              cin, kpad, relu);
-    else if (cout == 64)
-        conv::k_conv_rows<64, false><<<blocks, tc::TC_THREADS, tc::tile_smem_bytes<64>(), s>>>(X, Wf, bias, nullptr, Y, g,
-                                                                                              cin, kpad, relu);
-    else
-        return set_error("conv3d_forward: cout=%d not supported (16, 32, 64)", cout);
-    CLB_LAUNCH_CHECK("k_conv_rows<forward>");
+#define CLB_FW(NN) \
+    conv::k_conv_win<NN, false><<<blocks, conv::CW_THREADS, pl.smem, s>>>(X, Wf, bias, nullptr, Y, g, cin, kpad, relu, pl)
+    if (cout == 16) CLB_FW(16);
+    else if (cout == 32) CLB_FW(32);
+    else CLB_FW(64);
+#undef CLB_FW
+    CLB_LAUNCH_CHECK("k_conv_win<forward>");
     return 0;
 }
 
@@ -987,24 +985,26 @@ int clb_conv3d_dgrad(const void* dy, const void* wd, const void* mask_x, void* d
     CLB_REQUIRE(dy && wd && dx, "conv3d_dgrad: null pointer");
     CLB_REQUIRE(cout > 0 && cout % 8 == 0, "conv3d_dgrad: cout=%d must be a positive multiple of 8", cout);
     CLB_REQUIRE(kpad % 64 == 0 && kpad >= 27 * cout, "conv3d_dgrad: kpad=%d must be a multiple of 64 >= 27*cout", kpad);
+    CLB_REQUIRE(cin == 16 || cin == 32 || cin == 48 || cin == 64 || cin == 96,
+                "conv3d_dgrad: cin=%d not supported (16, 32, 48, 64, 96)", cin);
+    conv::WinPlan pl;
+    CLB_REQUIRE(conv::win_plan(D, H, W, cout, cin, B, pl), "conv3d_dgrad: no block shape fits %dx%dx%d", D, H, W);
     const conv::Vol g{B, D, H, W};
-    const unsigned blocks = (unsigned)(((i64)B * D * H * W + tc::TC_M - 1) / tc::TC_M);
+    const unsigned blocks = (unsigned)((i64)B * D * pl.ytiles * pl.xtiles);
     cudaStream_t s = CLB_STREAM(stream);
     const auto* DY = (const __nv_bfloat16*)dy;
     const auto* Wd = (const __nv_bfloat16*)wd;
     const auto* MX = (const __nv_bfloat16*)mask_x;
     auto* DX = (__nv_bfloat16*)dx;
-#define CLB_DG(NN)                                                                                             \
-    conv::k_conv_rows<NN, true><<<blocks, tc::TC_THREADS, tc::tile_smem_bytes<NN>(), s>>>(DY, Wd, nullptr, MX, DX, g, \
-                                                                                         cout, kpad, 0)
+#define CLB_DG(NN) \
+    conv::k_conv_win<NN, true><<<blocks, conv::CW_THREADS, pl.smem, s>>>(DY, Wd, nullptr, MX, DX, g, cout, kpad, 0, pl)
     if (cin == 16) CLB_DG(16);
     else if (cin == 32) CLB_DG(32);
     else if (cin == 48) CLB_DG(48);
     else if (cin == 64) CLB_DG(64);
-    else if (cin == 96) CLB_DG(96);
-    else return set_error("conv3d_dgrad: cin=%d not supported (16, 32, 48, 64, 96)", cin);
+    else CLB_DG(96);
 #undef CLB_DG
-    CLB_LAUNCH_CHECK("k_conv_rows<dgrad>");
+    CLB_LAUNCH_CHECK("k_conv_win<dgrad>");
     return 0;
 }
 
@@ -1047,8 +1047,9 @@ int clb_conv3d_arrange_weights(const float* w, void* wf, void* wd, int cin, int 
 int clb_unet_avgpool2(const void* x, void* y, int B, int D, int H, int W, int C, void* stream) {
     CLB_VOL_OK(B, D, H, W);
     CLB_REQUIRE(D % 2 == 0 && H % 2 == 0 && W % 2 == 0, "unet_avgpool2: extents must be even");
+    CLB_REQUIRE(C > 0 && C % 8 == 0, "unet_avgpool2: C=%d must be a multiple of 8", C);
     const conv::Vol g{B, D, H, W};
-    conv::k_avgpool2<<<ew_blocks((i64)B * D * H * W * C / 8), conv::EW, 0, CLB_STREAM(stream)>>>(
+    conv::k_avgpool2<<<ew_blocks((i64)B * D * H * W * C / 64), conv::EW, 0, CLB_STREAM(stream)>>>(
         (const __nv_bfloat16*)x, (__nv_bfloat16*)y, g, C);
     CLB_LAUNCH_CHECK("k_avgpool2");
     return 0;
@@ -1057,8 +1058,10 @@ int clb_unet_avgpool2(const void* x, void* y, int B, int D, int H, int W, int C,
 int clb_unet_avgpool2_backward(const void* dy, const void* x, void* dx, int B, int D, int H, int W, int C,
                                void* stream) {
     CLB_VOL_OK(B, D, H, W);
+    CLB_REQUIRE(C > 0 && C % 8 == 0 && D % 2 == 0 && H % 2 == 0 && W % 2 == 0,
+                "unet_avgpool2_backward: C=%d must be a multiple of 8 and extents even", C);
     const conv::Vol g{B, D, H, W};
-    conv::k_avgpool2_backward<<<ew_blocks((i64)B * D * H * W * C), conv::EW, 0, CLB_STREAM(stream)>>>(
+    conv::k_avgpool2_backward<<<ew_blocks((i64)B * D * H * W * C / 8), conv::EW, 0, CLB_STREAM(stream)>>>(
         (const __nv_bfloat16*)dy, (const __nv_bfloat16*)x, (__nv_bfloat16*)dx, g, C);
     CLB_LAUNCH_CHECK("k_avgpool2_backward");
     return 0;
@@ -1067,8 +1070,9 @@ int clb_unet_avgpool2_backward(const void* dy, const void* x, void* dx, int B, i
 int clb_unet_upsample_concat(const void* coarse, const void* skip, void* out, int B, int D, int H, int W, int c1,
                              int c2, void* stream) {
     CLB_VOL_OK(B, D, H, W);
+    CLB_REQUIRE(c1 > 0 && c2 > 0 && c1 % 8 == 0 && c2 % 8 == 0, "unet_upsample_concat: channels must be multiples of 8");
     const conv::Vol g{B, D, H, W};
-    conv::k_upsample_concat<<<ew_blocks((i64)B * D * H * W * (c1 + c2)), conv::EW, 0, CLB_STREAM(stream)>>>(
+    conv::k_upsample_concat<<<ew_blocks((i64)B * D * H * W * (c1 + c2) / 8), conv::EW, 0, CLB_STREAM(stream)>>>(
         (const __nv_bfloat16*)coarse, (const __nv_bfloat16*)skip, (__nv_bfloat16*)out, g, c1, c2);
     CLB_LAUNCH_CHECK("k_upsample_concat");
     return 0;
@@ -1077,8 +1081,10 @@ int clb_unet_upsample_concat(const void* coarse, const void* skip, void* out, in
 int clb_unet_upsample_concat_backward(const void* dout, void* dcoarse, void* dskip, int B, int D, int H, int W,
                                       int c1, int c2, void* stream) {
     CLB_VOL_OK(B, D, H, W);
+    CLB_REQUIRE(c1 > 0 && c2 > 0 && c1 % 8 == 0 && c2 % 8 == 0 && D % 2 == 0 && H % 2 == 0 && W % 2 == 0,
+                "unet_upsample_concat_backward: channels must be multiples of 8 and extents even");
     const conv::Vol g{B, D, H, W};
-    conv::k_upsample_concat_backward<<<ew_blocks((i64)B * D * H * W * (c1 + c2)), conv::EW, 0, CLB_STREAM(stream)>>>(
+    conv::k_upsample_concat_backward<<<ew_blocks((i64)B * D * H * W * (c1 + c2) / 8), conv::EW, 0, CLB_STREAM(stream)>>>(
         (const __nv_bfloat16*)dout, (__nv_bfloat16*)dcoarse, (__nv_bfloat16*)dskip, g, c1, c2);
     CLB_LAUNCH_CHECK("k_upsample_concat_backward");
     return 0;
@@ -1086,7 +1092,7 @@ int clb_unet_upsample_concat_backward(const void* dout, void* dcoarse, void* dsk
 
 int clb_unet_head_forward(const void* h, const float* w, const float* b, float* out, int voxels, int C,
                           void* stream) {
-    CLB_REQUIRE(C > 0 && C <= 16, "unet_head_forward: C=%d must be in 1..16", C);
+    CLB_REQUIRE(C == 16, "unet_head_forward: C=%d must be 16", C);
     conv::k_head_forward<<<ew_blocks(voxels), conv::EW, 0, CLB_STREAM(stream)>>>((const __nv_bfloat16*)h, w, b, out,
                                                                                  voxels, C);
     CLB_LAUNCH_CHECK("k_head_forward");
@@ -1095,7 +1101,7 @@ int clb_unet_head_forward(const void* h, const float* w, const float* b, float* 
 
 int clb_unet_head_backward(const void* h, const float* w, const float* dout, void* dh, float* dw, float* db,
                            int voxels, int C, void* stream) {
-    CLB_REQUIRE(C > 0 && C <= 16, "unet_head_backward: C=%d must be in 1..16", C);
+    CLB_REQUIRE(C == 16, "unet_head_backward: C=%d must be 16", C);
     conv::k_head_backward<<<ew_blocks(voxels), conv::EW, 0, CLB_STREAM(stream)>>>(
         (const __nv_bfloat16*)h, w, dout, (__nv_bfloat16*)dh, dw, db, voxels, C);
     CLB_LAUNCH_CHECK("k_head_backward");
@@ -1103,7 +1109,7 @@ int clb_unet_head_backward(const void* h, const float* w, const float* dout, voi
 }
 
 int clb_unet_bias_grad(const void* dy, float* db, int voxels, int C, void* stream) {
-    CLB_REQUIRE(C > 0 && C <= 256, "unet_bias_grad: C=%d must be in 1..256", C);
+    CLB_REQUIRE(C > 0 && C <= 256 && C % 8 == 0, "unet_bias_grad: C=%d must be a multiple of 8 in 8..256", C);
     conv::k_bias_grad<<<ew_blocks((i64)voxels * C / 16), conv::EW, 0, CLB_STREAM(stream)>>>((const __nv_bfloat16*)dy, db,
                                                                                             voxels, C);
     CLB_LAUNCH_CHECK("k_bias_grad");

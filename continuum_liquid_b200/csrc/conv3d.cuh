@@ -229,48 +229,72 @@ __global__ void k_arrange_weights(const float* __restrict__ w, __nv_bfloat16* __
     }
 }
 
-// 2x2x2 average pooling of a channels-last volume (D, H, W even)
+// Eight BF16 channels (16 bytes) to and from FP32.
+__device__ __forceinline__ void unpack8(const uint4 u, float* f) {
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const float2 t = __bfloat1622float2(h[e]);
+        f[2 * e] = t.x;
+        f[2 * e + 1] = t.y;
+    }
+}
+__device__ __forceinline__ uint4 pack8(const float* f) {
+    return make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]),
+                      pack_bf16x2(f[6], f[7]));
+}
+__device__ __forceinline__ void decode_vox(i64 v, int D, int H, int W, int& b, int& z, int& y, int& x) {
+    x = (int)(v % W);
+    v /= W;
+    y = (int)(v % H);
+    v /= H;
+    z = (int)(v % D);
+    b = (int)(v / D);
+}
+
+// 2x2x2 average pooling of a channels-last volume (D, H, W even); one thread per coarse voxel and
+// group of 8 channels
 __global__ void k_avgpool2(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ y, Vol fine, int C) {
-    const i64 total = (i64)fine.B * (fine.D / 2) * (fine.H / 2) * (fine.W / 2) * C;
+    const int G = C / 8, cD = fine.D / 2, cH = fine.H / 2, cW = fine.W / 2;
+    const i64 total = (i64)fine.B * cD * cH * cW * G;
     for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
-        const int c = (int)(t % C);
-        i64 v = t / C;
-        const int X = (int)(v % (fine.W / 2));
-        v /= fine.W / 2;
-        const int Y = (int)(v % (fine.H / 2));
-        v /= fine.H / 2;
-        const int Z = (int)(v % (fine.D / 2));
-        const int b = (int)(v / (fine.D / 2));
-        float s = 0.0f;
+        const int grp = (int)(t % G);
+        int b, Z, Y, X;
+        decode_vox(t / G, cD, cH, cW, b, Z, Y, X);
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int d = 0; d < 8; ++d) {
             const int z = 2 * Z + (d >> 2), y2 = 2 * Y + ((d >> 1) & 1), x2 = 2 * X + (d & 1);
-            s += __bfloat162float(x[(((i64)(b * fine.D + z) * fine.H + y2) * fine.W + x2) * C + c]);
+            float f[8];
+            unpack8(__ldg(reinterpret_cast<const uint4*>(x + ((((i64)b * fine.D + z) * fine.H + y2) * fine.W + x2) * C) + grp), f);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) s[e] += f[e];
         }
-        y[t] = __float2bfloat16_rn(0.125f * s);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) s[e] *= 0.125f;
+        reinterpret_cast<uint4*>(y)[t] = pack8(s);
     }
 }
 
 // nearest 2x upsampling of `coarse` (C1 channels) written into channels [0, C1) of `out`, and a copy
-// of `skip` (C2 channels) into channels [C1, C1 + C2): the decoder's concatenated input
+// of `skip` (C2 channels) into channels [C1, C1 + C2): the decoder's concatenated input. One thread
+// per fine voxel and group of 8 channels.
 __global__ void k_upsample_concat(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip,
                                   __nv_bfloat16* __restrict__ out, Vol fine, int C1, int C2) {
-    const int C = C1 + C2;
-    const i64 total = (i64)fine.B * fine.D * fine.H * fine.W * C;
+    const int G1 = C1 / 8, G = (C1 + C2) / 8;
+    const i64 total = (i64)fine.B * fine.D * fine.H * fine.W * G;
     for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
-        const int c = (int)(t % C);
-        const i64 v = t / C;
-        if (c < C1) {
-            const int x = (int)(v % fine.W);
-            i64 r = v / fine.W;
-            const int y = (int)(r % fine.H);
-            r /= fine.H;
-            const int z = (int)(r % fine.D);
-            const int b = (int)(r / fine.D);
+        const int grp = (int)(t % G);
+        const i64 v = t / G;
+        uint4 val;
+        if (grp < G1) {
+            int b, z, y, x;
+            decode_vox(v, fine.D, fine.H, fine.W, b, z, y, x);
             const i64 cv = (((i64)b * (fine.D / 2) + z / 2) * (fine.H / 2) + y / 2) * (fine.W / 2) + x / 2;
-            out[t] = coarse[cv * C1 + c];
+            val = __ldg(reinterpret_cast<const uint4*>(coarse + cv * C1) + grp);
         } else {
-            out[t] = skip[v * C2 + (c - C1)];
+            val = __ldg(reinterpret_cast<const uint4*>(skip + v * C2) + (grp - G1));
         }
+        reinterpret_cast<uint4*>(out)[t] = val;
     }
 }
 
@@ -278,31 +302,34 @@ __global__ void k_upsample_concat(const __nv_bfloat16* __restrict__ coarse, cons
 // the copied channels (added to an existing gradient, as the skip tensor also feeds the encoder)
 __global__ void k_upsample_concat_backward(const __nv_bfloat16* __restrict__ dout, __nv_bfloat16* __restrict__ dcoarse,
                                            __nv_bfloat16* __restrict__ dskip, Vol fine, int C1, int C2) {
-    const int C = C1 + C2;
-    const i64 coarse_total = (i64)fine.B * (fine.D / 2) * (fine.H / 2) * (fine.W / 2) * C1;
-    const i64 skip_total = (i64)fine.B * fine.D * fine.H * fine.W * C2;
+    const int C = C1 + C2, G1 = C1 / 8, G2 = C2 / 8, cD = fine.D / 2, cH = fine.H / 2, cW = fine.W / 2;
+    const i64 coarse_total = (i64)fine.B * cD * cH * cW * G1;
+    const i64 skip_total = (i64)fine.B * fine.D * fine.H * fine.W * G2;
     for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < coarse_total + skip_total;
          t += (i64)gridDim.x * blockDim.x) {
         if (t < coarse_total) {
-            const int c = (int)(t % C1);
-            i64 v = t / C1;
-            const int X = (int)(v % (fine.W / 2));
-            v /= fine.W / 2;
-            const int Y = (int)(v % (fine.H / 2));
-            v /= fine.H / 2;
-            const int Z = (int)(v % (fine.D / 2));
-            const int b = (int)(v / (fine.D / 2));
-            float s = 0.0f;
+            const int grp = (int)(t % G1);
+            int b, Z, Y, X;
+            decode_vox(t / G1, cD, cH, cW, b, Z, Y, X);
+            float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             for (int d = 0; d < 8; ++d) {
                 const int z = 2 * Z + (d >> 2), y = 2 * Y + ((d >> 1) & 1), x = 2 * X + (d & 1);
-                s += __bfloat162float(dout[(((i64)(b * fine.D + z) * fine.H + y) * fine.W + x) * C + c]);
+                float f[8];
+                unpack8(__ldg(reinterpret_cast<const uint4*>(dout + ((((i64)b * fine.D + z) * fine.H + y) * fine.W + x) * C) + grp), f);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) s[e] += f[e];
             }
-            dcoarse[t] = __float2bfloat16_rn(s);
+            reinterpret_cast<uint4*>(dcoarse)[t] = pack8(s);
         } else {
             const i64 u = t - coarse_total;
-            const int c = (int)(u % C2);
-            const i64 v = u / C2;
-            dskip[u] = __float2bfloat16_rn(__bfloat162float(dskip[u]) + __bfloat162float(dout[v * C + C1 + c]));
+            const int grp = (int)(u % G2);
+            const i64 v = u / G2;
+            float a[8], f[8];
+            unpack8(reinterpret_cast<const uint4*>(dskip)[u], a);
+            unpack8(__ldg(reinterpret_cast<const uint4*>(dout + v * C + C1) + grp), f);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) a[e] += f[e];
+            reinterpret_cast<uint4*>(dskip)[u] = pack8(a);
         }
     }
 }
@@ -311,65 +338,109 @@ __global__ void k_upsample_concat_backward(const __nv_bfloat16* __restrict__ dou
 // existing gradient and masked by the ReLU of the pooled activation's producer (x > 0)
 __global__ void k_avgpool2_backward(const __nv_bfloat16* __restrict__ dy, const __nv_bfloat16* __restrict__ x,
                                     __nv_bfloat16* __restrict__ dx, Vol fine, int C) {
-    const i64 total = (i64)fine.B * fine.D * fine.H * fine.W * C;
+    const int G = C / 8;
+    const i64 total = (i64)fine.B * fine.D * fine.H * fine.W * G;
     for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (i64)gridDim.x * blockDim.x) {
-        const int c = (int)(t % C);
-        const i64 v = t / C;
-        const int xx = (int)(v % fine.W);
-        i64 r = v / fine.W;
-        const int y = (int)(r % fine.H);
-        r /= fine.H;
-        const int z = (int)(r % fine.D);
-        const int b = (int)(r / fine.D);
+        const int grp = (int)(t % G);
+        int b, z, y, xx;
+        decode_vox(t / G, fine.D, fine.H, fine.W, b, z, y, xx);
         const i64 cv = (((i64)b * (fine.D / 2) + z / 2) * (fine.H / 2) + y / 2) * (fine.W / 2) + xx / 2;
-        float g = __bfloat162float(dx[t]) + 0.125f * __bfloat162float(dy[cv * C + c]);
-        if (!(__bfloat162float(x[t]) > 0.0f)) g = 0.0f;
-        dx[t] = __float2bfloat16_rn(g);
+        float a[8], p[8], xv[8];
+        unpack8(reinterpret_cast<const uint4*>(dx)[t], a);
+        unpack8(__ldg(reinterpret_cast<const uint4*>(dy + cv * C) + grp), p);
+        unpack8(__ldg(reinterpret_cast<const uint4*>(x) + t), xv);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) a[e] = xv[e] > 0.0f ? a[e] + 0.125f * p[e] : 0.0f;
+        reinterpret_cast<uint4*>(dx)[t] = pack8(a);
     }
 }
 
-// 1x1x1 output head: out[v] = sum_c h[v][c] * w[c] + b (C = 16), and its backward
+// 1x1x1 head (C = 16 channels): out[v] = bias + sum_c h[v][c] w[c]
 __global__ void k_head_forward(const __nv_bfloat16* __restrict__ h, const float* __restrict__ w, const float* bias,
                                float* __restrict__ out, int V, int C) {
+    float wr[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) wr[c] = c < C ? __ldg(w + c) : 0.0f;
+    const float b0 = __ldg(bias);
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-        float s = bias[0];
-        for (int c = 0; c < C; ++c) s += __bfloat162float(h[(i64)v * C + c]) * w[c];
+        const uint4* hv = reinterpret_cast<const uint4*>(h + (i64)v * C);
+        float f[16];
+        unpack8(__ldg(hv), f);
+        unpack8(__ldg(hv + 1), f + 8);
+        float s = b0;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) s += f[c] * wr[c];
         out[v] = s;
     }
 }
 
-// dh[v][c] = dout[v] * w[c] masked by (h > 0); dw[c] += sum_v dout[v] h[v][c]; db += sum dout
+// dh[v][c] = dout[v] * w[c] masked by (h > 0); dw[c] += sum_v dout[v] h[v][c]; db += sum dout (C = 16)
 __global__ void k_head_backward(const __nv_bfloat16* __restrict__ h, const float* __restrict__ w,
                                 const float* __restrict__ dout, __nv_bfloat16* __restrict__ dh, float* dw, float* db,
                                 int V, int C) {
-    __shared__ float s_dw[64 + 1];
-    for (int c = threadIdx.x; c <= C; c += blockDim.x) s_dw[c] = 0.0f;
+    __shared__ float s_dw[17];
+    if (threadIdx.x < 17) s_dw[threadIdx.x] = 0.0f;
     __syncthreads();
-    float ldw[16] = {0};
+    float wr[16], ldw[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+        wr[c] = __ldg(w + c);
+        ldw[c] = 0.0f;
+    }
     float ldb = 0.0f;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-        const float g = dout[v];
+        const float g = __ldg(dout + v);
         ldb += g;
-        for (int c = 0; c < C; ++c) {
-            const float hv = __bfloat162float(h[(i64)v * C + c]);
-            ldw[c & 15] += g * hv;
-            dh[(i64)v * C + c] = __float2bfloat16_rn(hv > 0.0f ? g * w[c] : 0.0f);
+        const uint4* hv = reinterpret_cast<const uint4*>(h + (i64)v * C);
+        float f[16], o[16];
+        unpack8(__ldg(hv), f);
+        unpack8(__ldg(hv + 1), f + 8);
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+            ldw[c] += g * f[c];
+            o[c] = f[c] > 0.0f ? g * wr[c] : 0.0f;
         }
+        uint4* dv = reinterpret_cast<uint4*>(dh + (i64)v * C);
+        dv[0] = pack8(o);
+        dv[1] = pack8(o + 8);
     }
-    for (int c = 0; c < C; ++c) atomicAdd(&s_dw[c], ldw[c & 15]);
-    atomicAdd(&s_dw[C], ldb);
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ldw[c] += __shfl_xor_sync(0xffffffffu, ldw[c], o);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ldb += __shfl_xor_sync(0xffffffffu, ldb, o);
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int c = 0; c < 16; ++c) atomicAdd(&s_dw[c], ldw[c]);
+        atomicAdd(&s_dw[16], ldb);
+    }
     __syncthreads();
-    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(dw + c, s_dw[c]);
-    if (threadIdx.x == 0) atomicAdd(db, s_dw[C]);
+    if (threadIdx.x < 16) atomicAdd(dw + threadIdx.x, s_dw[threadIdx.x]);
+    if (threadIdx.x == 16) atomicAdd(db, s_dw[16]);
 }
 
-// bias gradient of a conv: db[co] += sum_v dy[v][co]
+// bias gradient of a conv: db[co] += sum_v dy[v][co]. Thread t of a block sums channel group
+// t % G (8 channels) over voxels t / G, t / G + stride, ... (blockDim is a multiple of G).
 __global__ void k_bias_grad(const __nv_bfloat16* __restrict__ dy, float* db, int V, int C) {
     __shared__ float s[256];
+    const int G = C / 8;
     for (int c = threadIdx.x; c < C; c += blockDim.x) s[c] = 0.0f;
     __syncthreads();
-    for (i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x; t < (i64)V * C; t += (i64)gridDim.x * blockDim.x)
-        atomicAdd(&s[t % C], __bfloat162float(dy[t]));
+    const int per_block = blockDim.x / G;
+    const int grp = threadIdx.x % G, slot = threadIdx.x / G;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (slot < per_block)
+        for (i64 v = (i64)blockIdx.x * per_block + slot; v < V; v += (i64)gridDim.x * per_block) {
+            float f[8];
+            unpack8(__ldg(reinterpret_cast<const uint4*>(dy + v * C) + grp), f);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) acc[e] += f[e];
+        }
+    if (slot < per_block)
+#pragma unroll
+        for (int e = 0; e < 8; ++e) atomicAdd(&s[grp * 8 + e], acc[e]);
     __syncthreads();
     for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(db + c, s[c]);
 }
