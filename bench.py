@@ -57,7 +57,8 @@ def parse_args():
     ap.add_argument("--cpu-cycles", type=int, default=None, help="W-cycles per CPU step (default: measured)")
     ap.add_argument("--method", choices=["fcg", "refine"], default="fcg", help="tolerance-mode pressure iteration")
     ap.add_argument("--learned", choices=["auto", "on", "off"], default="auto",
-                    help="learned warm start in the timed steps (auto: when trained weights exist)")
+                    help="learned warm start in the timed steps (auto: when trained weights exist and the Poisson "
+                         "comparison shows it faster)")
     ap.add_argument("--poisson-steps", type=int, default=3, help="steps of the Poisson comparison (0: skip)")
     ap.add_argument("--coarse-fp16", choices=["auto", "on", "off"], default="auto",
                     help="FP16 storage of the coarse levels <= 64^3 in the timed steps (auto: when the Poisson "
@@ -503,7 +504,7 @@ def our_arm(args):
     positions, velocities = scenes.seed_particles(scene)
     warm, warm_note = load_warm_start(kernels, scene, args.learned)
     opts = solver.StepOptions(flip_ratio=0.95, tol=TOL, gravity=scene.gravity, rho=scene.rho, nu=scene.nu,
-                              method=args.method, warm_start=warm)
+                              method=args.method, warm_start=warm if args.learned == "on" else None)
     sim = solver.FlipSolver(kernels, scene.grid_shape, scene.dx, positions, velocities, obstacle=obstacle, dt=scene.dt,
                             options=opts, min_size=scene.min_size)
     n = sim.n
@@ -517,12 +518,20 @@ def our_arm(args):
     # --- Poisson comparison on the next steps' systems; it also decides FP16 coarse storage ----
     poisson = {}
     use_fp16 = args.coarse_fp16 == "on"
+    use_learned = args.learned == "on"
     if args.poisson_steps > 0:
         poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
         if args.coarse_fp16 == "auto":
             use_fp16 = poisson.get("coarse_fp16_holds", False)
+        if args.learned == "auto" and "fcg_learned" in poisson:
+            # the rule: the learned guess in the timed steps only when it makes the solve faster,
+            # network evaluation included
+            use_learned = poisson["fcg_learned"]["ms_mean"] < poisson["fcg"]["ms_mean"]
     else:
         poisson["learned_vs_plain"] = "skipped (--poisson-steps 0)"
+    sim.options.warm_start = warm if use_learned else None
+    if warm is not None and not use_learned:
+        warm_note += " (not used in the timed steps: no faster than without it in the comparison)"
     if use_fp16:
         from continuum_liquid_b200.pressure_solve import PressureSolver
 

@@ -961,6 +961,7 @@ int clb_conv3d_forward(const void* x, const void* wf, const float* bias, void* y
     CLB_REQUIRE(cin > 0 && cin % 8 == 0, "conv3d_forward: cin=%d must be a positive multiple of 8", cin);
     CLB_REQUIRE(kpad % 64 == 0 && kpad >= 27 * cin, "conv3d_forward: kpad=%d must be a multiple of 64 >= 27*cin", kpad);
     CLB_REQUIRE(cout == 16 || cout == 32 || cout == 64, "conv3d_forward: cout=%d not supported (16, 32, 64)", cout);
+    CLB_REQUIRE(bias == nullptr || ((uintptr_t)bias & 15) == 0, "conv3d_forward: bias must be 16-byte aligned");
     conv::WinPlan pl;
     CLB_REQUIRE(conv::win_plan(D, H, W, cin, cout, B, pl), "conv3d_forward: no block shape fits %dx%dx%d", D, H, W);
     const conv::Vol g{B, D, H, W};

@@ -112,7 +112,9 @@ __global__ void __launch_bounds__(CW_THREADS) k_conv_win(const __nv_bfloat16* __
     bool ok = true;
     for (int q = 0; q < pl.nq && ok; ++q) {
         const int s = q & 1;
-        if (q >= 2) ok = __syncthreads_and(mbar_wait(&bars[s], (uint32_t)(((q - 2) >> 1) & 1))) != 0;
+        // one thread polls the barrier; the others wait at __syncthreads without taking issue slots
+        if (q >= 2)
+            ok = __syncthreads_and(threadIdx.x == 0 ? mbar_wait(&bars[s], (uint32_t)(((q - 2) >> 1) & 1)) : true) != 0;
         if (!ok) break;  // uniform across the block
         stage(q, s);
         cp_async_wait_all();
@@ -120,26 +122,35 @@ __global__ void __launch_bounds__(CW_THREADS) k_conv_win(const __nv_bfloat16* __
         __syncthreads();
         if (threadIdx.x == 0) {
             tc_fence_after();
-            const uint32_t a0 = smem_u32(stage_a[s]), w0 = smem_u32(stage_b[s]);
-            for (int m = 0; m < pl.tiles; ++m)
+            // Descriptors are built once: the start-address field counts 16-byte units, so moving the
+            // window by `off` voxels (16 bytes each) or to the next tap's weights adds to the descriptor
+            // (shared-memory addresses stay below 2^18 bytes, so the 14-bit field never carries).
+            const uint64_t a_base = smem_desc(smem_u32(stage_a[s]) + (uint32_t)(pl.Lbeg + 1) * 16u, plane_bytes, 128u);
+            const uint64_t b_base = smem_desc(smem_u32(stage_b[s]), (uint32_t)(N * 16), 128u);
+            const int slab = TY2 * RW;
+            for (int m = 0; m < pl.tiles; ++m) {
+                const uint64_t am = a_base + (uint64_t)(m * TC_M);
+                const uint32_t dm = tmem + (uint32_t)(m * N);
+#pragma unroll
                 for (int tap = 0; tap < 27; ++tap) {
-                    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-                    int off = (dz * TY2 + dy) * RW + dx;
-                    if (DGRAD) off = -off;
-                    const uint32_t pos = (uint32_t)(pl.Lbeg + m * TC_M + off + 1);
-                    const uint64_t ad = smem_desc(a0 + pos * 16u, plane_bytes, 128u);
-                    const uint64_t bd = smem_desc(w0 + (uint32_t)tap * (uint32_t)(2 * N * 16), (uint32_t)(N * 16), 128u);
-                    mma_bf16(tmem + (uint32_t)(m * N), ad, bd, idesc, (q > 0 || tap > 0) ? 1u : 0u);
+                    const int off = (tap / 9 - 1) * slab + ((tap / 3) % 3 - 1) * RW + (tap % 3 - 1);
+                    const uint64_t ad = am + (uint64_t)(int64_t)(DGRAD ? -off : off);
+                    mma_bf16(dm, ad, b_base + (uint64_t)(tap * 2 * N), idesc, (q > 0 || tap > 0) ? 1u : 0u);
                 }
+            }
             mma_commit(&bars[s]);
         }
     }
     if (ok && pl.nq > 0)
-        ok = __syncthreads_and(mbar_wait(&bars[(pl.nq - 1) & 1], (uint32_t)(((pl.nq - 1) >> 1) & 1))) != 0;
+        ok = __syncthreads_and(threadIdx.x == 0 ? mbar_wait(&bars[(pl.nq - 1) & 1], (uint32_t)(((pl.nq - 1) >> 1) & 1))
+                                                : true) != 0;
     if (!ok) {
-        raise_device_error(4u);
-        mbar_wait(&bars[0], 0);
-        mbar_wait(&bars[1], 0);
+        if (threadIdx.x == 0) {
+            raise_device_error(4u);
+            mbar_wait(&bars[0], 0);
+            mbar_wait(&bars[1], 0);
+        }
+        __syncthreads();
     }
     tc_fence_after();
     if (ok) {
@@ -157,10 +168,22 @@ __global__ void __launch_bounds__(CW_THREADS) k_conv_win(const __nv_bfloat16* __
                 tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(m * N + col), acc);
                 if (!valid) continue;
                 if (!DGRAD) {
+                    float bv[16];
+                    if (bias) {
+                        const float4* b4 = reinterpret_cast<const float4*>(bias + col);
+#pragma unroll
+                        for (int h = 0; h < 4; ++h) {
+                            const float4 t = __ldg(b4 + h);
+                            bv[4 * h] = t.x;
+                            bv[4 * h + 1] = t.y;
+                            bv[4 * h + 2] = t.z;
+                            bv[4 * h + 3] = t.w;
+                        }
+                    }
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
                         float a = acc[e];
-                        if (bias) a += __ldg(bias + col + e);
+                        if (bias) a += bv[e];
                         if (relu) a = fmaxf(a, 0.0f);
                         acc[e] = a;
                     }

@@ -155,7 +155,9 @@ __device__ __forceinline__ void tile_gemm(const Op& op, uint8_t* smem) {
     const int chunks = op.chunks;
     for (int c = 0; c < chunks && ok; ++c) {
         const int s = c & 1;
-        if (c >= 2) ok = __syncthreads_and(mbar_wait(&bars[s], (uint32_t)(((c - 2) >> 1) & 1))) != 0;
+        // one thread polls the barrier; the others wait at __syncthreads without taking issue slots
+        if (c >= 2)
+            ok = __syncthreads_and(threadIdx.x == 0 ? mbar_wait(&bars[s], (uint32_t)(((c - 2) >> 1) & 1)) : true) != 0;
         if (!ok) break;  // uniform across the block
         op.gather_a(a_stage[s], c);
         op.gather_b(b_stage[s], c);
@@ -175,12 +177,16 @@ __device__ __forceinline__ void tile_gemm(const Op& op, uint8_t* smem) {
         }
     }
     if (ok && chunks > 0)
-        ok = __syncthreads_and(mbar_wait(&bars[(chunks - 1) & 1], (uint32_t)(((chunks - 1) >> 1) & 1))) != 0;
+        ok = __syncthreads_and(threadIdx.x == 0 ? mbar_wait(&bars[(chunks - 1) & 1], (uint32_t)(((chunks - 1) >> 1) & 1))
+                                                : true) != 0;
     if (!ok) {
-        raise_device_error(4u);
-        // let MMAs already issued finish before the memory they use is released
-        mbar_wait(&bars[0], 0);
-        mbar_wait(&bars[1], 0);
+        if (threadIdx.x == 0) {
+            raise_device_error(4u);
+            // let MMAs already issued finish before the memory they use is released
+            mbar_wait(&bars[0], 0);
+            mbar_wait(&bars[1], 0);
+        }
+        __syncthreads();
     }
     tc_fence_after();
     if (ok && chunks > 0 && warp < 4) {

@@ -230,8 +230,12 @@ class UNet:
         self.arrange()
 
     # -- persistence -------------------------------------------------------------------------------
-    def save(self, path) -> None:
-        np.savez(path, params=self.params.cpu().numpy(), step=self.step_count)
+    def save(self, path, meta: dict | None = None) -> None:
+        """FP32 master weights (and optional JSON metadata: how they were trained and evaluated)."""
+        import json
+
+        np.savez_compressed(path, params=self.params.cpu().numpy(), step=self.step_count,
+                            meta=np.asarray(json.dumps(meta or {})))
 
     def load(self, path) -> None:
         data = np.load(path)
@@ -254,6 +258,7 @@ class Frame:
     p_conv: torch.Tensor
     dx: float
     scale: float
+    weight: float = 1.0  # loss weight: the relative residual the previous-step pressure starts from
 
 
 def pressure_scale(p: torch.Tensor, op0: torch.Tensor) -> float:
@@ -272,7 +277,8 @@ def pack(net: UNet, vol: Vol, slot: int, rhs, op0, solid, p, dx, s, origin=(0, 0
 
 
 def capture_frames(kernels: Backend, scene, steps: int, tol: float = 1e-6, skip: int = 2) -> list[Frame]:
-    """Run a scene with the plain refined W-cycle and record every solve after the first `skip`."""
+    """Run a scene with the plain solver (previous-step warm start, flexible CG to ``tol``) and record
+    every solve after the first `skip`."""
     from .solver import StepOptions, scene_solver
 
     opts = StepOptions(flip_ratio=scene.flip_ratio, tol=tol, gravity=scene.gravity, rho=scene.rho, nu=scene.nu)
@@ -281,24 +287,27 @@ def capture_frames(kernels: Backend, scene, steps: int, tol: float = 1e-6, skip:
     for step in range(steps):
         sim.pre_solve()
         p_prev = sim.pressure.clone()
-        sim.solve()
+        stats = sim.solve()
         ps = sim.pressure_solver
         if step >= skip:
             s = pressure_scale(p_prev, ps.hierarchy.op0)
             if s > 0:
                 frames.append(Frame(ps.rhs.clone(), ps.hierarchy.op0.clone(),
                                     None if sim.obstacle is None else sim.obstacle, p_prev, sim.pressure.clone(),
-                                    sim.dx, s))
+                                    sim.dx, s, float(stats.initial_rel_residual or 1.0)))
         sim.post_solve()
     return frames
 
 
 def train(net: UNet, frames: list[Frame], iterations: int, batch: int = 8, crop: int = 64, lr: float = 1e-3,
-          seed: int = 0, log_every: int = 0) -> list[float]:
-    """Adam on random crops of the captured solves; returns the loss history."""
+          seed: int = 0, log_every: int = 0, weighted: bool = False) -> list[float]:
+    """Adam on random crops of the captured solves; returns the loss history. ``weighted`` scales each
+    crop's squared error by its frame's weight (relative to the mean weight)."""
     rng = np.random.default_rng(seed)
     vol = Vol(batch, crop, crop, crop)
-    net.buffers(vol)
+    b = net.buffers(vol)
+    per_slot = vol.D * vol.H * vol.W
+    mean_w = float(np.mean([f.weight for f in frames])) or 1.0
     history = []
     for it in range(iterations):
         for slot in range(batch):
@@ -306,6 +315,8 @@ def train(net: UNet, frames: list[Frame], iterations: int, batch: int = 8, crop:
             nx, ny, nz = f.rhs.shape
             origin = tuple(int(rng.integers(0, max(1, n - crop + 1))) for n in (nx, ny, nz))
             pack(net, vol, slot, f.rhs, f.op0, f.solid, f.p_prev, f.dx, f.scale, origin, target=f.p_conv)
+            if weighted:
+                b["mask"][slot * per_slot: (slot + 1) * per_slot].mul_(f.weight / mean_w)
         net.forward(vol)
         loss = net.loss_and_grad(vol)
         net.backward(vol)
@@ -335,6 +346,39 @@ class LearnedWarmStart:
         self.net.k.call("clb_unet_unpack_output", out, p_prev, op0, float(s), self.guess, nx, ny, nz, self.vol.D,
                         self.vol.H, self.vol.W)
         return self.guess
+
+
+def evaluate(kernels: Backend, net: UNet | None, frames: list[Frame], tol: float = 1e-6) -> list[dict]:
+    """Flexible-CG cycles to ``tol`` on each captured system from the previous-step pressure and, with
+    ``net``, from the solver's choice between it and the network's guess (the lower residual)."""
+    from .autotune import tune_hierarchy
+    from .pressure_solve import PressureSolver
+
+    rows = []
+    solvers: dict = {}
+    for f in frames:
+        shape = tuple(f.rhs.shape)
+        if shape not in solvers:
+            ps = PressureSolver(kernels, shape, f.dx)
+            ws = LearnedWarmStart(net, shape, f.dx) if net is not None else None
+            solvers[shape] = (ps, ws)
+        ps, ws = solvers[shape]
+        ps.rhs.copy_(f.rhs)
+        ps.hierarchy.op0.copy_(f.op0)
+        ps.hierarchy.build_coarse()
+        if not ps.tuned:
+            tune_hierarchy(ps.hierarchy, ps.correction, ps.residual)
+            ps.tuned = True
+        row = {"shape": shape}
+        for name, warm in (("previous", None), ("learned", ws)):
+            if name == "learned" and warm is None:
+                continue
+            p = f.p_prev.clone()
+            st = ps.solve_prepared(p, tol, use_graph=False, warm_start=warm, solid=f.solid)
+            row[name] = {"cycles": st.cycles, "initial_rel": st.initial_rel_residual, "guess": st.warm_start,
+                         "learned_rel": st.learned_rel_residual}
+        rows.append(row)
+    return rows
 
 
 def default_weights_path() -> Path:

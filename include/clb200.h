@@ -294,7 +294,9 @@ int clb_tc_test_gemm(const void* a, const void* b, float* c, int M, int N, int K
  * Taps are ordered (dz, dy, dx), dx fastest. Master weights are FP32 [27 * cin][cout].
  *  arrange_weights: wf[cout][kpad] (forward) and, when wd != NULL, wd[cin][kpad2] (data grad), BF16,
  *                   kpad >= 27*cin and kpad2 >= 27*cout multiples of 64, zero-padded.
- *  forward:  y = act(bias + conv(x)), cin % 8 == 0, cout in {16, 32, 64}, relu = 0/1.
+ *  forward:  y = act(bias + conv(x)), cin % 8 == 0, cout in {16, 32, 64}, relu = 0/1; bias (nullable)
+ *            16-byte aligned. Forward and data gradient stage an input tile in shared memory and read
+ *            each tap as a shifted window of it (no per-tap gather).
  *  dgrad:    dx = conv^T(dy) * (mask_x > 0) (mask_x nullable), cout % 8 == 0, cin in {16,32,48,64,96}.
  *  wgrad:    dw[27*cin][cout] += sum over voxels (FP32 atomics; zero dw first), cout in {16, 32, 64};
  *            each block reduces chunks_per_block chunks of 64 voxels. */
