@@ -63,7 +63,7 @@ def parse_args():
     ap.add_argument("--coarse-fp16", choices=["auto", "on", "off"], default="auto",
                     help="FP16 storage of the coarse levels <= 64^3 in the timed steps (auto: when the Poisson "
                          "comparison shows the convergence factor and time hold)")
-    ap.add_argument("--case", choices=["step", "sweep0", "batch", "unet"], default="step",
+    ap.add_argument("--case", choices=["step", "sweep0", "batch", "unet", "collider"], default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
                          "(no particles: a small-memory case for profiling the dominant kernel); batch: the batched "
                          "uneven-scenes workload (32 scenes of sizes 48-160, one launch per stage)")
@@ -133,6 +133,52 @@ def batch_case(args):
         line["sequential_single_scene"] = {"ms_per_batch_step": seq_ms, "scene_steps_per_s": len(scs) * 1e3 / seq_ms}
         line["speedup_vs_sequential"] = seq_ms / ms
     print(json.dumps(line), flush=True)
+
+
+def collider_case(args):
+    """The 128^3 collider pool (a falling sphere of liquid into a pool around an icosphere of 5120
+    triangles) with the collider voxelised again at every step, each pressure solve to TOL."""
+    import torch
+
+    from continuum_liquid_b200 import scenes, solver
+    from continuum_liquid_b200.backend import Backend
+
+    kernels = Backend(0)
+    sc = scenes.collider_pool(128, seed=0, subdivisions=4)
+    opts = solver.StepOptions(flip_ratio=sc.flip_ratio, tol=TOL, gravity=sc.gravity, rho=sc.rho, nu=sc.nu,
+                              revoxelise=True)
+    sim = solver.scene_solver(kernels, sc, opts)
+    triangles = sum(int(t.shape[0]) for t in sim.colliders)
+    for _ in range(args.warmup):
+        sim.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(0) as clocks:
+        e0.record()
+        for _ in range(args.steps):
+            stats.append(sim.step())
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # the voxelisation alone (brick-culled launch, as in the step), averaged over 20 launches
+    e0.record()
+    for _ in range(20):
+        sim.voxelise_colliders()
+    e1.record()
+    torch.cuda.synchronize()
+    vox_ms = e0.elapsed_time(e1) / 20
+    cells = sc.cells
+    print(json.dumps({
+        "case": "collider", "metric": "steps/s of the 128^3 collider pool, collider voxelised every step",
+        "unit": "steps/s", "value": 1e3 / ms, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+        "config": {"workload": "collider_pool_128^3", "grid": list(sc.grid_shape), "particles": sim.n,
+                   "triangles": triangles, "pressure_tolerance": TOL},
+        "particles_per_s": sim.n * 1e3 / ms, "cycles_per_step": [s.cycles for s in stats],
+        "rel_residual_max": max(s.rel_residual for s in stats),
+        "voxelise_ms": vox_ms,
+        "voxelise_ray_triangle_tests_per_s_bruteforce_equivalent": cells * triangles / (vox_ms * 1e-3),
+        "clocks": clocks.summary()}), flush=True)
 
 
 def unet_flops_per_voxel() -> float:
@@ -684,6 +730,8 @@ def main():
         batch_case(args)
     elif args.case == "unet":
         unet_case(args)
+    elif args.case == "collider":
+        collider_case(args)
     else:
         our_arm(args)
 

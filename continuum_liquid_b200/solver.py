@@ -53,6 +53,7 @@ class StepOptions:
     warm_start: object = None  # callable proposing an initial pressure (learned.LearnedWarmStart)
     method: str = "fcg"  # tolerance-mode iteration: "fcg" (W-cycle preconditioned CG) or "refine"
     coarse_fp16: bool = False  # tolerance mode: store the coarse levels of at most 64^3 cells in FP16
+    revoxelise: bool = False  # voxelise the colliders again at every step (moving or deforming meshes)
 
 
 class FlipSolver:
@@ -60,7 +61,7 @@ class FlipSolver:
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, positions, velocities, obstacle=None,
                  dt: float = 1.0 / 240.0, options: StepOptions | None = None, particles_per_cell: int = 8,
-                 min_size: int = 8, capacity: int | None = None):
+                 min_size: int = 8, capacity: int | None = None, colliders=None, origin=(0.0, 0.0, 0.0)):
         self.kernels = kernels
         self.device = kernels.device
         self.grid_shape = tuple(int(s) for s in grid_shape)
@@ -90,15 +91,29 @@ class FlipSolver:
                 else obstacle
             if bool(ob.any()):
                 self.obstacle = ob.to(dev).contiguous()
+        # collider meshes (world-space float32 triangles) for per-step voxelisation
+        self.colliders = [torch.as_tensor(np.ascontiguousarray(t, dtype=np.float32)).to(dev) for t in (colliders or [])]
+        self.origin = tuple(float(o) for o in origin)
+        if self.colliders and self.obstacle is None:
+            self.obstacle = torch.zeros(self.grid_shape, dtype=torch.uint8, device=dev)
         self.pressure_solver = PressureSolver(kernels, self.grid_shape, self.dx, min_size=min_size,
                                               method=self.options.method, coarse_fp16=self.options.coarse_fp16)
         self.last_solve: SolveStats | None = None
         self.steps_done = 0
 
     # -- the step --------------------------------------------------------------------------------
+    def voxelise_colliders(self, queue=None) -> None:
+        """Rebuild the obstacle mask from the collider meshes (voxelise_mesh.py:111-135 per mesh)."""
+        self.obstacle.zero_()
+        for tris in self.colliders:
+            voxelise_mesh.voxelise_triangles(self.kernels, queue, tris, self.obstacle, self.grid_shape, self.dx,
+                                             self.origin)
+
     def pre_solve(self, queue=None) -> None:
         """Stages 1-4: P2G, grid BCs, forces, BCs (everything before the pressure solve)."""
         k, o, gs = self.kernels, self.options, self.grid_shape
+        if o.revoxelise and self.colliders:
+            self.voxelise_colliders(queue)
         (self.particles, self.particle_velocity, self.particle_work, self.particle_velocity_work,
          _, self.fluid_fraction) = particle_methods.particle_to_grid(
             k, queue, self.particles, self.particle_velocity, self.particle_work, self.particle_velocity_work,
@@ -175,7 +190,8 @@ def scene_solver(kernels: Backend, scene, options: StepOptions | None = None) ->
     positions, velocities = seed_particles(scene, obstacle.cpu().numpy())
     opts = options or StepOptions(flip_ratio=scene.flip_ratio, gravity=scene.gravity, rho=scene.rho, nu=scene.nu)
     return FlipSolver(kernels, scene.grid_shape, scene.dx, positions, velocities, obstacle=obstacle, dt=scene.dt,
-                      options=opts, particles_per_cell=scene.particles_per_cell, min_size=scene.min_size)
+                      options=opts, particles_per_cell=scene.particles_per_cell, min_size=scene.min_size,
+                      colliders=scene.obstacles, origin=scene.origin)
 
 
 # ------------------------------------------------------------------------------------------------

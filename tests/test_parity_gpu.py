@@ -560,3 +560,19 @@ def test_every_sweep_kind_matches_oracle(backend, oracle, shape, kind):
     h.w_cycle(P, rhs)
     oracle.Levels(shape).w_cycle(q, orhs, ff, oops, dx)
     assert np.array_equal(host(P), q)
+
+
+def test_revoxelising_a_static_collider_every_step_changes_nothing(backend):
+    s = scenes.collider_pool(32, seed=9, subdivisions=2)
+    sims = []
+    for revox in (False, True):
+        opts = solver.StepOptions(flip_ratio=0.95, num_vcycles=1, gravity=s.gravity, use_graph=False, revoxelise=revox)
+        sims.append(solver.scene_solver(backend, s, opts))
+    assert sims[1].colliders and int(sims[1].obstacle.sum()) > 0
+    mask0 = host(sims[1].obstacle).copy()
+    for _ in range(3):
+        for sim in sims:
+            sim.step()
+        assert np.array_equal(host(sims[1].obstacle), mask0)
+        assert np.array_equal(sims[0].positions(), sims[1].positions())
+        assert np.array_equal(host(sims[0].pressure), host(sims[1].pressure))
