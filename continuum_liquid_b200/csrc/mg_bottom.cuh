@@ -124,18 +124,55 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
         else a[c] = v;
     };
 
-    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
-        spa[c] = ld(pa, c);
-        sba[c] = ld(ba, c);
-        float4 o = ld4(opa, c);
-        if (!ma[c]) o.x = -1.0f;
-        soa[c] = o;
+    // staging: four cells per thread and round, all loads issued before the shared-memory stores
+    constexpr int U = 4;
+    for (int c0 = threadIdx.x; c0 < CA; c0 += U * BOTTOM_THREADS) {
+        float pv[U], bv[U];
+        float4 ov[U];
+        uint8_t mv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int c = c0 + u * BOTTOM_THREADS;
+            if (c < CA) {
+                pv[u] = ld(pa, c);
+                bv[u] = ld(ba, c);
+                ov[u] = ld4(opa, c);
+                mv[u] = ma[c];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int c = c0 + u * BOTTOM_THREADS;
+            if (c < CA) {
+                spa[c] = pv[u];
+                sba[c] = bv[u];
+                float4 o = ov[u];
+                if (!mv[u]) o.x = -1.0f;
+                soa[c] = o;
+            }
+        }
     }
-    for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
-        float4 o = ld4(opb, c);
-        if (!mb[c]) o.x = -1.0f;
-        sob[c] = o;
-        spb[c] = 0.0f;  // restriction zeroes the coarse pressure (multigrid.cl:114)
+    for (int c0 = threadIdx.x; c0 < CB; c0 += U * BOTTOM_THREADS) {
+        float4 ov[U];
+        uint8_t mv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int c = c0 + u * BOTTOM_THREADS;
+            if (c < CB) {
+                ov[u] = ld4(opb, c);
+                mv[u] = mb[c];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int c = c0 + u * BOTTOM_THREADS;
+            if (c < CB) {
+                float4 o = ov[u];
+                if (!mv[u]) o.x = -1.0f;
+                sob[c] = o;
+                spb[c] = 0.0f;  // restriction zeroes the coarse pressure (multigrid.cl:114)
+            }
+        }
     }
     __syncthreads();
 
