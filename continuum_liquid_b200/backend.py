@@ -26,6 +26,7 @@ MG_MAX_LEVELS = 16
 SCAN_TILE = 4096  # elements per scan tile (SCAN_THREADS * SCAN_ITEMS in csrc/binning.cuh)
 
 P, I, L, F, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+U = ctypes.c_uint64
 
 # name -> argument types (every entry point returns int status unless listed in _RESTYPES)
 SIGNATURES: dict[str, list[Any]] = {
@@ -60,6 +61,11 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_prolongate": [P, P, P, I, I, I, I, I, I, P],
     "clb_coarse_smooth": [P, P, P, P, P, P, P, F, I, I, I, I, P],
     "clb_mg_rhs_operator": [P, P, P, P, P, P, F, F, I, I, I, P],
+    "clb_source_cell_counts": [P, L, F, I, I, I, P, P],
+    "clb_source_keep": [P, L, F, I, I, I, P, P, P],
+    "clb_source_compact": [P, P, P, P, L, P, P, P],
+    "clb_source_missing": [P, P, P, I, L, P, P],
+    "clb_source_spawn": [P, P, I, I, I, D, F, F, F, U, U, U, U, P, P, P],
     "clb_batch_particle_to_grid": [P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, L, F, P],
     "clb_batch_update_velocity": [P, P, P, P, P, P, P, P, F, F, F, F, F, F, F, F, F, P],
     "clb_batch_grid_domain_bc": [P, P, P, P, P],

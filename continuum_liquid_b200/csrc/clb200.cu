@@ -9,6 +9,7 @@
 #include "mg_sweep.cuh"
 #include "mg_half.cuh"
 #include "batch.cuh"
+#include "sources.cuh"
 #include "voxelise.cuh"
 #include "tc_gemm.cuh"
 #include "conv3d.cuh"
@@ -24,7 +25,7 @@ using namespace clb;
                 (nz));                                                                                 \
     CLB_REQUIRE((i64)(nx) * (ny) * (nz) < (1ll << 31), "grid %dx%dx%d has more than 2^31 cells", (nx), (ny), (nz))
 
-static const int kAbiVersion = 6;
+static const int kAbiVersion = 7;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 
@@ -1191,6 +1192,64 @@ int clb_voxelise_mesh(const float* triangles, uint8_t* mask, int triangle_count,
         k_voxelise<false><<<grid, VOX_THREADS, 0, CLB_STREAM(stream)>>>(triangles, mask, triangle_count, nx, ny, nz,
                                                                         delta, ox, oy, oz, d[0], d[1], d[2]);
     CLB_LAUNCH_CHECK("k_voxelise");
+    return 0;
+}
+
+// ---- particle sources ------------------------------------------------------------------------------
+
+int clb_source_cell_counts(const float* particles, int64_t n, float delta, int nx, int ny, int nz, int32_t* counts,
+                           void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0 && delta > 0.0f && counts && (n == 0 || particles), "source_cell_counts: bad arguments");
+    if (n == 0) return 0;
+    k_source_cell_counts<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, n, delta, nx, ny, nz, counts);
+    CLB_LAUNCH_CHECK("k_source_cell_counts");
+    return 0;
+}
+
+int clb_source_keep(const float* particles, int64_t n, float delta, int nx, int ny, int nz, const uint8_t* outflow,
+                    int32_t* keep, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0 && delta > 0.0f && outflow && keep && (n == 0 || particles), "source_keep: bad arguments");
+    if (n == 0) return 0;
+    k_source_keep<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, n, delta, nx, ny, nz, outflow, keep);
+    CLB_LAUNCH_CHECK("k_source_keep");
+    return 0;
+}
+
+int clb_source_compact(const float* particles, const float* velocity, const int32_t* keep, const int32_t* slots,
+                       int64_t n, float* particles_out, float* velocity_out, void* stream) {
+    CLB_REQUIRE(n >= 0, "source_compact: negative n");
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && velocity && keep && slots && particles_out && velocity_out,
+                "source_compact: null pointer");
+    CLB_REQUIRE(particles_out != particles && velocity_out != velocity, "source_compact: outputs must not alias");
+    k_source_compact<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, velocity, keep, slots, n,
+                                                                        particles_out, velocity_out);
+    CLB_LAUNCH_CHECK("k_source_compact");
+    return 0;
+}
+
+int clb_source_missing(const int32_t* counts, const uint8_t* source, const uint8_t* solid, int target, int64_t cells,
+                       int32_t* missing, void* stream) {
+    CLB_REQUIRE(counts && source && missing && cells >= 0 && target >= 1, "source_missing: bad arguments");
+    if (cells == 0) return 0;
+    k_source_missing<<<blocks_for(cells, PT), PT, 0, CLB_STREAM(stream)>>>(counts, source, solid, target, cells,
+                                                                            missing);
+    CLB_LAUNCH_CHECK("k_source_missing");
+    return 0;
+}
+
+int clb_source_spawn(const int32_t* missing, const int32_t* offsets, int nx, int ny, int nz, double delta, float vx,
+                     float vy, float vz, uint64_t state_hi, uint64_t state_lo, uint64_t inc_hi, uint64_t inc_lo,
+                     float* particles_out, float* velocity_out, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(missing && offsets && particles_out && velocity_out && delta > 0.0, "source_spawn: bad arguments");
+    const i64 C = (i64)nx * ny * nz;
+    k_source_spawn<<<blocks_for(C, PT), PT, 0, CLB_STREAM(stream)>>>(missing, offsets, C, ny, nz, delta, vx, vy, vz,
+                                                                      state_hi, state_lo, inc_hi, inc_lo,
+                                                                      particles_out, velocity_out);
+    CLB_LAUNCH_CHECK("k_source_spawn");
     return 0;
 }
 

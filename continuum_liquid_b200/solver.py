@@ -102,6 +102,21 @@ class FlipSolver:
         self.steps_done = 0
 
     # -- the step --------------------------------------------------------------------------------
+    def ensure_capacity(self, count: int) -> None:
+        """Grow the particle buffers to hold ``count`` particles (by 1.5x at least, as
+        solver.py:290-303 grows its buffers), keeping the current particles."""
+        cap = self.particles.shape[0]
+        if count <= cap:
+            return
+        new_cap = max(int(count), (cap * 3) // 2)
+        for name in ("particles", "particle_velocity"):
+            old = getattr(self, name)
+            fresh = torch.zeros((new_cap, 3), dtype=torch.float32, device=self.device)
+            fresh[: self.n].copy_(old[: self.n])
+            setattr(self, name, fresh)
+        (self.particle_work, self.particle_velocity_work, self.bin_counts, self.scan_outputs,
+         self.scan_sums) = particle_methods.create_particle_sort_buffers(self.kernels, self.grid_shape, new_cap)
+
     def voxelise_colliders(self, queue=None) -> None:
         """Rebuild the obstacle mask from the collider meshes (voxelise_mesh.py:111-135 per mesh)."""
         self.obstacle.zero_()
@@ -237,6 +252,7 @@ def solver(config: dict, timings=None) -> None:
                                                                   delta)
     sources, obstacle_host = source_particles.download_static_masks(None, sources_dev, obstacle_mask, grid_shape)
     rng = np.random.default_rng(0)
+    device_sources = source_particles.DeviceSources(kernels, sources_dev, obstacle_mask, grid_shape, delta, rng)
     particles_host = np.empty((0, 3), dtype=FIELD_DTYPE)
     velocity_host = np.empty((0, 3), dtype=FIELD_DTYPE)
     particles_host, velocity_host = source_particles.apply_sources(particles_host, velocity_host, sources,
@@ -258,9 +274,8 @@ def solver(config: dict, timings=None) -> None:
             output_frame = (solver_step + 1) // steps_per_frame
             substep_index = solver_step % steps_per_frame
             if dynamic:
-                particles_host, velocity_host = source_particles.apply_sources(
-                    sim.positions(), sim.velocities(), sources, obstacle_host, delta, rng)
-                sim = _resized(sim, particles_host, velocity_host)
+                # the reference's per-step host round trip (solver.py:252-306), on the device
+                device_sources.apply(sim)
             t0 = time.perf_counter()
             stats = sim.step()
             if substep_index == steps_per_frame - 1:
@@ -272,22 +287,3 @@ def solver(config: dict, timings=None) -> None:
                                                                  "ms": (time.perf_counter() - t0) * 1e3}})
     finally:
         output.close_output(writer)
-
-
-def _resized(sim: FlipSolver, positions: np.ndarray, velocities: np.ndarray) -> FlipSolver:
-    """Re-upload host-edited particles (dynamic sources), growing capacity by 1.5x like
-    solver.py:290-303."""
-    n = len(positions)
-    cap = sim.particles.shape[0]
-    if n > cap:
-        new_cap = max(n, (cap * 3) // 2)
-        fresh = FlipSolver(sim.kernels, sim.grid_shape, sim.dx, positions, velocities, obstacle=sim.obstacle,
-                           dt=sim.dt, options=sim.options, particles_per_cell=sim.particles_per_cell,
-                           capacity=new_cap)
-        fresh.pressure.copy_(sim.pressure)
-        return fresh
-    sim.n = n
-    if n:
-        sim.particles[:n].copy_(torch.from_numpy(np.ascontiguousarray(positions, dtype=np.float32)))
-        sim.particle_velocity[:n].copy_(torch.from_numpy(np.ascontiguousarray(velocities, dtype=np.float32)))
-    return sim

@@ -357,6 +357,32 @@ int clb_voxelise_mesh(const float* triangles, uint8_t* mask, int triangle_count,
 /* The ray direction of voxelise_mesh.cl:24 as three floats (host helper). */
 int clb_voxelise_direction(float* out3);
 
+/* ---- particle sources (source_particles.py:21-92, which the reference runs on the host) ------
+ *
+ * Cells are clamp(floor(p / delta), 0, n - 1) per axis (float32 division), as source_particles.py:21-25.
+ *  cell_counts: counts[cell] += particles in it (zero counts first).
+ *  keep:        keep[q] = 0 if particle q lies in an outflow cell, else 1 (source_particles.py:37-39);
+ *               an exclusive scan of keep gives each kept particle's slot and the kept count.
+ *  compact:     kept particles (and velocities) to their slots, order preserved.
+ *  missing:     missing[c] = max(0, target - counts[c]) in non-solid source cells (solid nullable).
+ *  spawn:       source_particles.py:42-75 fill_source: with offsets = exclusive scan of missing, the
+ *               g-th new particle (cells in flat order) is placed at (cell + u) * delta, u the host
+ *               stream's draws 3g..3g+2 after the PCG64 state (state_hi:state_lo, inc_hi:inc_lo) as
+ *               numpy.random.Generator.random gives them (float64, stored as float32); velocity
+ *               (vx, vy, vz). particles_out/velocity_out point at the first new record. The caller
+ *               advances its generator by 3 * (number of new particles). */
+int clb_source_cell_counts(const float* particles, int64_t n, float delta, int nx, int ny, int nz, int32_t* counts,
+                           void* stream);
+int clb_source_keep(const float* particles, int64_t n, float delta, int nx, int ny, int nz, const uint8_t* outflow,
+                    int32_t* keep, void* stream);
+int clb_source_compact(const float* particles, const float* velocity, const int32_t* keep, const int32_t* slots,
+                       int64_t n, float* particles_out, float* velocity_out, void* stream);
+int clb_source_missing(const int32_t* counts, const uint8_t* source, const uint8_t* solid, int target, int64_t cells,
+                       int32_t* missing, void* stream);
+int clb_source_spawn(const int32_t* missing, const int32_t* offsets, int nx, int ny, int nz, double delta, float vx,
+                     float vy, float vz, uint64_t state_hi, uint64_t state_lo, uint64_t inc_hi, uint64_t inc_lo,
+                     float* particles_out, float* velocity_out, void* stream);
+
 /* ---- batched scenes (no counterpart in the reference, which bakes one scene at a time) -------
  *
  * Many independent scenes of different grid sizes advance together: every field of a batch holds the

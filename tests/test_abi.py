@@ -30,7 +30,7 @@ def test_python_signature_table_covers_the_header():
 
 def test_load_library_sets_signatures_and_pure_helpers():
     lib = backend.load_library()
-    assert lib.clb_abi_version() == 6
+    assert lib.clb_abi_version() == 7
     for count in (0, 1, 4096, 4097, 16777216):
         assert lib.clb_scan_scratch_bytes(count) == backend.Backend.scan_scratch_bytes_static(count)
     assert lib.clb_mg_residual_partials(1000) == 4
