@@ -4,9 +4,11 @@ Layout: ``<dir>/particle_cache.json`` (metadata version 2) and ``<dir>/particles
 holding raw float32 (N, 3) positions. Frames are published atomically (written to ``.tmp`` then
 renamed) so a reader polling the directory never sees a partial frame (output.py:46-53).
 
-Device frames are copied into pinned host slots with an asynchronous copy on the solver's stream
-and written by background threads; a writer failure is re-raised on the solver thread at the next
-submit or at close, as ``RuntimeError`` (output.py:91-97).
+Device frames are copied into pinned host slots with an asynchronous copy on the solver's stream and
+written by background threads; the solver thread does not wait for the copy (the writer waits on an
+event recorded after it, and work queued later on the stream cannot overwrite the positions before
+the copy has read them). A writer failure is re-raised on the solver thread at the next submit or at
+close, as ``RuntimeError`` (output.py:91-97).
 """
 
 from __future__ import annotations
@@ -67,12 +69,13 @@ def read_particles(cache_directory, frame) -> np.ndarray:
 
 
 class _Slot:
-    __slots__ = ("host", "count", "frame")
+    __slots__ = ("host", "count", "frame", "ready")
 
     def __init__(self):
         self.host: torch.Tensor | None = None
         self.count = 0
         self.frame = 0
+        self.ready: torch.cuda.Event | None = None  # recorded after the device-to-host copy
 
     def ensure(self, count: int) -> None:
         count = max(1, int(count))
@@ -87,6 +90,9 @@ def _writer_loop(state: dict[str, Any]) -> None:
         try:
             if slot is None:
                 return
+            if slot.ready is not None:
+                slot.ready.synchronize()
+                slot.ready = None
             write_particles(state["cache_directory"], slot.host[: slot.count].numpy(), slot.frame)
         except BaseException as exc:  # noqa: BLE001 - collected and re-raised on the solver thread
             with state["error_lock"]:
@@ -149,13 +155,13 @@ def submit_host(state: dict[str, Any], particles, frame: int) -> None:
 def submit_output(state: dict[str, Any], *, particles: torch.Tensor, particle_count: int, frame: int,
                   queue=None) -> None:
     """output.py:169-186: copy the first ``particle_count`` device positions into a pinned slot
-    (asynchronous copy on the current stream, then an event wait) and queue it for writing."""
+    (asynchronous copy on the current stream) and queue it for writing; the writer thread waits for
+    the copy, the caller does not."""
     slot = _acquire_slot(state, particle_count, frame)
     if particle_count:
         slot.host[:particle_count].copy_(particles[:particle_count], non_blocking=True)
-        event = torch.cuda.Event()
-        event.record()
-        event.synchronize()
+        slot.ready = torch.cuda.Event()
+        slot.ready.record()
     state["write_queue"].put(slot)
 
 
