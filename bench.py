@@ -63,7 +63,7 @@ def parse_args():
     ap.add_argument("--coarse-fp16", choices=["auto", "on", "off"], default="auto",
                     help="FP16 storage of the coarse levels <= 64^3 in the timed steps (auto: when the Poisson "
                          "comparison shows the convergence factor and time hold)")
-    ap.add_argument("--case", choices=["step", "sweep0", "batch", "unet", "collider"], default="step",
+    ap.add_argument("--case", choices=["step", "sweep0", "wcycle", "batch", "unet", "collider"], default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
                          "(no particles: a small-memory case for profiling the dominant kernel); batch: the batched "
                          "uneven-scenes workload (32 scenes of sizes 48-160, one launch per stage)")
@@ -252,7 +252,8 @@ def unet_case(args):
 
 def sweep_case(args):
     """Level-0 red-black Gauss-Seidel iterations on the block scene's liquid mask (random right-hand side),
-    with the autotuned sweep kind; prints one JSON line with the device time per iteration."""
+    with the autotuned sweep kind; prints one JSON line with the device time per iteration. With
+    --case wcycle: whole W-cycles on the same system instead (one per --sweeps)."""
     import torch
 
     from continuum_liquid_b200 import scenes
@@ -279,6 +280,19 @@ def sweep_case(args):
     h.smooth(0, 2, p, ps.rhs)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.case == "wcycle":
+        h.w_cycle(p, ps.rhs)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("sweeps")
+        e0.record()
+        for _ in range(args.sweeps):
+            h.w_cycle(p, ps.rhs)
+        e1.record()
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "wcycle", "grid": list(scene.grid_shape), "levels": [list(x) for x in h.shapes],
+                          "sweep_kinds": h.sweeps(), "ms_per_w_cycle": e0.elapsed_time(e1) / args.sweeps}), flush=True)
+        return
     torch.cuda.nvtx.range_push("sweeps")
     e0.record()
     h.smooth(0, args.sweeps, p, ps.rhs)
@@ -724,7 +738,7 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         reference_arm(args)
-    elif args.case == "sweep0":
+    elif args.case in ("sweep0", "wcycle"):
         sweep_case(args)
     elif args.case == "batch":
         batch_case(args)
