@@ -39,6 +39,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "steps/s at 256^3; Poisson ms to 1e-6 rel. residual, learned vs plain W-cycle"
 UNIT = "steps/s"
 TOL = 1e-6
+COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarsest-level iterations
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu capture of the same kernel on the
 # same 256^3 system (profiles/k_rbgs_colour_level0_block_256.md); None for kernels not captured.
@@ -63,6 +64,10 @@ def parse_args():
     ap.add_argument("--coarse-fp16", choices=["auto", "on", "off"], default="auto",
                     help="FP16 storage of the coarse levels <= 64^3 in the timed steps (auto: when the Poisson "
                          "comparison shows the convergence factor and time hold)")
+    ap.add_argument("--coarse-iterations", default="auto",
+                    help="red-black iterations of each coarsest-level solve in the W-cycle preconditioner of the timed "
+                         "steps (auto: the fastest of 64 (the reference's), 16, 8 and 4 that needs no more FCG cycles "
+                         "than 64 in the Poisson comparison)")
     ap.add_argument("--case", choices=["step", "sweep0", "wcycle", "batch", "unet", "collider"], default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
                          "(no particles: a small-memory case for profiling the dominant kernel); batch: the batched "
@@ -305,7 +310,8 @@ def sweep_case(args):
                       "ms_per_iteration": ms, "algorithmic_gb_s": 13.0 * cells / (ms * 1e-3) / 1e9}), flush=True)
 
 
-def workload_config(size, n_particles, args):
+def workload_config(size, n_particles, args, coarse_iterations=COARSE_ITERATION_CHOICES[0]):
+    k = int(coarse_iterations)
     return {
         "workload": f"flip_step_block_{size}^3",
         "grid": [size, size, size],
@@ -314,9 +320,9 @@ def workload_config(size, n_particles, args):
         "dt": 1.0 / 240.0,
         "flip_ratio": 0.95,
         "pressure_tolerance": TOL,
-        "pressure_solver": ("flexible CG preconditioned by one FP32 W-cycle (pre 2, post 4, coarse 2+64), FP64 "
+        "pressure_solver": (f"flexible CG preconditioned by one FP32 W-cycle (pre 2, post 4, coarse 2+{k}), FP64 "
                             "pressure, residual and norms" if args.method == "fcg" else
-                            "W-cycle (pre 2, post 4, coarse 2+64) in FP64 iterative refinement"),
+                            f"W-cycle (pre 2, post 4, coarse 2+{k}) in FP64 iterative refinement"),
         "multigrid_levels": None,
         "l2": "inputs larger than L2 (particle state 24 B x N, grid fields 4 B x n^3 each)",
         "parallelism": "replicas" if args.gpus > 1 else "single",
@@ -465,16 +471,21 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                for m in ("refine", "fcg")}
     solvers["fcg_fp16"] = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg",
                                          coarse_fp16=True)
+    # fewer coarsest-level iterations in the W-cycle preconditioner, with either coarse storage
+    for k in COARSE_ITERATION_CHOICES[1:]:
+        for fp16 in (False, True):
+            solvers[f"fcg{'_fp16' if fp16 else ''}_c{k}"] = PressureSolver(
+                kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16, coarse_iterations=k)
     p_tmp = torch.empty_like(sim.pressure)
     rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": []}
+    rows.update({name: [] for name in solvers if "_c" in name})
     fp32 = []
     rho = sim.options.rho
     for _ in range(steps):
         sim.pre_solve()
         saved = sim.pressure.clone()
         vel = (sim.u, sim.v, sim.w)
-        variants = [("refine", solvers["refine"], None), ("fcg", solvers["fcg"], None),
-                    ("fcg_fp16", solvers["fcg_fp16"], None)]
+        variants = [(name, ps, None) for name, ps in solvers.items()]
         if warm is not None:
             variants.append(("fcg_learned", solvers["fcg"], warm))
         for name, ps, ws in variants:
@@ -542,6 +553,15 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
         # is not slower
         out["coarse_fp16_holds"] = bool(f16["fp16_levels"]) and f16["cycles_mean"] <= f32["cycles_mean"] and \
             f16["ms_mean"] <= f32["ms_mean"] * 1.01
+    # the rule for the coarsest-level iterations: with the chosen coarse storage, the fastest count that
+    # needs no more cycles than the reference's 64
+    base = "fcg_fp16" if out.get("coarse_fp16_holds") else "fcg"
+    best_k, best_ms = COARSE_ITERATION_CHOICES[0], out[base]["ms_mean"]
+    for k in COARSE_ITERATION_CHOICES[1:]:
+        r = out.get(f"{base}_c{k}")
+        if r and r["cycles_mean"] <= out[base]["cycles_mean"] and r["ms_mean"] < best_ms:
+            best_k, best_ms = k, r["ms_mean"]
+    out["coarse_iterations_chosen"] = best_k
     if rows["fcg_learned"]:
         out["speedup_learned_vs_plain_fcg"] = out["fcg"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
         out["speedup_learned_vs_refine"] = out["refine"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
@@ -579,10 +599,13 @@ def our_arm(args):
     poisson = {}
     use_fp16 = args.coarse_fp16 == "on"
     use_learned = args.learned == "on"
+    coarse_k = COARSE_ITERATION_CHOICES[0] if args.coarse_iterations == "auto" else int(args.coarse_iterations)
     if args.poisson_steps > 0:
         poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
         if args.coarse_fp16 == "auto":
             use_fp16 = poisson.get("coarse_fp16_holds", False)
+        if args.coarse_iterations == "auto":
+            coarse_k = poisson.get("coarse_iterations_chosen", coarse_k)
         if args.learned == "auto" and "fcg_learned" in poisson:
             # the rule: the learned guess in the timed steps only when it makes the solve faster,
             # network evaluation included
@@ -592,12 +615,13 @@ def our_arm(args):
     sim.options.warm_start = warm if use_learned else None
     if warm is not None and not use_learned:
         warm_note += " (not used in the timed steps: no faster than without it in the comparison)"
-    if use_fp16:
+    if use_fp16 or coarse_k != sim.options.coarse_iterations:
         from continuum_liquid_b200.pressure_solve import PressureSolver
 
-        sim.options.coarse_fp16 = True
+        sim.options.coarse_fp16 = use_fp16
+        sim.options.coarse_iterations = coarse_k
         sim.pressure_solver = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=scene.min_size,
-                                             method=args.method, coarse_fp16=True)
+                                             method=args.method, coarse_fp16=use_fp16, coarse_iterations=coarse_k)
         for _ in range(2):  # tuning and graph capture of the new solver
             sim.step()
         torch.cuda.synchronize()
@@ -629,6 +653,7 @@ def our_arm(args):
 
     # --- Poisson time to 1e-6 in the timed steps ------------------------------------------------
     poisson = {"timed_steps": {"method": args.method, "learned": warm_note, "coarse_fp16": use_fp16,
+                               "coarse_iterations": coarse_k,
                                "ms_mean": float(np.mean(solve_ms)),
                                "cycles_mean": float(np.mean(cycles)),
                                "final_rel_residual_max": float(max(s.rel_residual or 0.0 for s in stats)),
@@ -704,7 +729,7 @@ def our_arm(args):
                          f"kernels with {k} FP32 W-cycles (the GPU's mean cycle count)"}
 
     if rank == 0:
-        config = workload_config(args.size, n, args)
+        config = workload_config(args.size, n, args, sim.options.coarse_iterations)
         config["multigrid_levels"] = [list(s) for s in h.shapes]
         config["sweep_kinds"] = h.sweeps()
         config["sweep_tuning_ms_per_iteration"] = h.tuning

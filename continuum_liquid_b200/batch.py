@@ -30,7 +30,7 @@ from .scenes import Scene, seed_particles
 
 F32 = np.float32
 BOTTOM_SMEM_LIMIT = 220 * 1024  # csrc/clb200.cu kBottomSmemLimit
-BOTTOM_THREADS, BOTTOM_BTHREADS, BOTTOM_MAX_A, BOTTOM_MAX_B = 512, 256, 16, 4  # csrc/mg_bottom.cuh
+BOTTOM_THREADS, BOTTOM_BTHREADS, BOTTOM_MAX_A, BOTTOM_MAX_B = 512, 256, 8, 4  # csrc/mg_bottom.cuh
 
 
 def _pad16(x: int) -> int:
@@ -46,13 +46,16 @@ def bottom_plan(shapes) -> tuple[int, int, int, int]:
         return -1, 0, 0, 0
     a, b = shapes[level], shapes[level + 1]
     ca, cb = int(np.prod(a)), int(np.prod(b))
-    ma = (a[0] - 2) * (a[1] - 2) * (a[2] - 2)
-    mbc = (b[0] - 2) * (b[1] - 2) * (b[2] - 2) // 2
+    sa, sb = colour_slots(a), colour_slots(b)
     smem = _pad16(ca * 4) * 2 + ca * 16 + _pad16(cb * 4) + cb * 16
-    if smem > BOTTOM_SMEM_LIMIT or (b[2] - 2) % 2 or mbc > BOTTOM_MAX_B * BOTTOM_BTHREADS or \
-            ma > BOTTOM_MAX_A * BOTTOM_THREADS:
+    if smem > BOTTOM_SMEM_LIMIT or sb > BOTTOM_MAX_B * BOTTOM_BTHREADS or sa > BOTTOM_MAX_A * BOTTOM_THREADS:
         return -1, 0, 0, 0
-    return level, -(-ma // BOTTOM_THREADS), -(-mbc // BOTTOM_BTHREADS), smem
+    return level, -(-sa // BOTTOM_THREADS), -(-sb // BOTTOM_BTHREADS), smem
+
+
+def colour_slots(shape) -> int:
+    """Cells of one colour a thread set must cover on a level (csrc/mg_bottom.cuh colour_slots)."""
+    return (shape[0] - 2) * (shape[1] - 2) * ((shape[2] - 1) // 2)
 
 
 @dataclass
@@ -67,7 +70,7 @@ class BatchedFlip:
 
     def __init__(self, kernels: Backend, scenes: list[Scene], flip_ratio: float | None = None, tol: float | None = 1e-6,
                  num_vcycles: int = 1, reduce_blocks: int = 32, sweep0: int = 1, use_graph: bool = True,
-                 max_cycles: int = 100):
+                 max_cycles: int = 100, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS):
         if not 1 <= len(scenes) <= BATCH_MAX_SCENES:
             raise ValueError(f"a batch holds 1..{BATCH_MAX_SCENES} scenes, got {len(scenes)}")
         first = scenes[0]
@@ -80,6 +83,8 @@ class BatchedFlip:
         self.dt, self.rho, self.nu, self.gravity = first.dt, first.rho, first.nu, tuple(first.gravity)
         self.flip_ratio = first.flip_ratio if flip_ratio is None else float(flip_ratio)
         self.tol, self.num_vcycles, self.max_cycles = tol, int(num_vcycles), int(max_cycles)
+        # coarsest-level iterations of the tolerance mode's W-cycle preconditioner (fixed-cycle mode: 64)
+        self.coarse_iterations = int(coarse_iterations)
         self.ppc = first.particles_per_cell
         self.use_graph = use_graph
         dev = kernels.device
@@ -275,8 +280,8 @@ class BatchedFlip:
         self._pre_work()
         self._swap()
 
-    def _w_cycle(self, x, rhs) -> None:
-        self._call("clb_batch_w_cycle", x, rhs, PRE_SMOOTH, POST_SMOOTH, COARSE_SMOOTH_ITERATIONS)
+    def _w_cycle(self, x, rhs, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS) -> None:
+        self._call("clb_batch_w_cycle", x, rhs, PRE_SMOOTH, POST_SMOOTH, int(coarse_iterations))
 
     def _init_solve(self) -> None:
         self.cur = 0
@@ -287,7 +292,7 @@ class BatchedFlip:
 
     def _iteration(self, src: int) -> None:
         self.correction.zero_()
-        self._w_cycle(self.correction, self.residual)
+        self._w_cycle(self.correction, self.residual, self.coarse_iterations)
         self._call("clb_batch_fcg_dots", self.correction, self.direction[src], self.residual, self.partials4,
                    self.fcg_state)
         self._call("clb_batch_fcg_step", self.p64[src], self.correction, self.direction[src], self.p64[1 - src],

@@ -68,11 +68,11 @@ int batch_bottom(const clb_batch* B, int level, int pre, int post, int coarse_it
         B->p[level + 1], B->b[level + 1], (const float4*)B->op[level + 1], B->mask[level + 1], pre, post,         \
         coarse_iters)
     const int ka = B->bottom_ka, kb = B->bottom_kb;
-    if (ka <= 2 && kb <= 1) CLB_BB(2, 1);
+    if (ka <= 1 && kb <= 1) CLB_BB(1, 1);
+    else if (ka <= 2 && kb <= 1) CLB_BB(2, 1);
     else if (ka <= 4 && kb <= 1) CLB_BB(4, 1);
-    else if (ka <= 8 && kb <= 1) CLB_BB(8, 1);
-    else if (ka <= 8 && kb <= 2) CLB_BB(8, 2);
-    else if (ka <= 16 && kb <= 4) CLB_BB(16, 4);
+    else if (ka <= 4 && kb <= 2) CLB_BB(4, 2);
+    else if (ka <= 8 && kb <= 4) CLB_BB(8, 4);
     else CLB_REQUIRE(false, "batch: bottom visit tiles (%d, %d) too large", ka, kb);
 #undef CLB_BB
     CLB_LAUNCH_CHECK("kb_bottom_visit");

@@ -87,21 +87,21 @@ int clb_init(int device) {
         return 1;
     const int bottom_max = (int)kBottomSmemLimit;
     cudaError_t e = cudaSuccess;
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<1, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<16, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<8, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
-    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_coarse_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     if (check_call(e, "bottom visit attribute")) return 1;
     if (conv_set_attributes()) return 1;
@@ -351,8 +351,8 @@ static int pressure_correction_impl(float* u, float* v, float* w, const PT* pres
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(u && v && w && pressure, "pressure_correction: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_pressure_correction<PT><<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, pressure, dt_over_rho,
-                                                                                 inv_dx, nx, ny, nz);
+    launch(blocks_for(C, GT), GT, 0, CLB_STREAM(stream))(k_pressure_correction<PT>, u, v, w, pressure, dt_over_rho,
+                                                         inv_dx, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_pressure_correction");
     return 0;
 }
@@ -362,7 +362,7 @@ static int neumann_domain_bc_impl(PT* pressure, int nx, int ny, int nz, void* st
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(pressure, "neumann_domain_bc: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_neumann_domain_bc<PT><<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(pressure, nx, ny, nz);
+    launch(blocks_for(C, GT), GT, 0, CLB_STREAM(stream))(k_neumann_domain_bc<PT>, pressure, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_neumann_domain_bc");
     return 0;
 }
@@ -487,8 +487,8 @@ int clb_mg_rhs_operator(const float* u, const float* v, const float* w, const fl
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(u && v && w && fluid_fraction && rhs && op0, "mg_rhs_operator: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_rhs_op0<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(u, v, w, fluid_fraction, rhs, op0, rho_over_dt,
-                                                                   inv_dx, nx, ny, nz);
+    launch(blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream))(k_rhs_op0, u, v, w, fluid_fraction, rhs, op0, rho_over_dt,
+                                                           inv_dx, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_rhs_op0");
     return 0;
 }
@@ -531,7 +531,9 @@ int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream) {
         const uint8_t* fop0 = l == 1 ? h->op0 : nullptr;
         const void* fopc = l == 1 ? nullptr : h->op[l - 1];
         const uint8_t* fmask = l == 1 ? nullptr : h->mask[l - 1];
-#define CLB_COARSE_OP(FS, CH)                                                                                        k_coarse_operator<FS, CH><<<grid, MGT, 0, s>>>(fop0, fopc, fmask, h->op[l], h->mask[l], h->fp16_inexact, f[0],                                                    f[1], f[2], c[0], c[1], c[2])
+#define CLB_COARSE_OP(FS, CH)                                                                             \
+    launch(grid, MGT, 0, s)(k_coarse_operator<FS, CH>, fop0, fopc, fmask, h->op[l], h->mask[l], h->fp16_inexact, \
+                            f[0], f[1], f[2], c[0], c[1], c[2])
         if (fs == 0 && !ch) CLB_COARSE_OP(0, false);
         else if (fs == 1 && !ch) CLB_COARSE_OP(1, false);
         else if (fs == 0) CLB_COARSE_OP(0, true);
@@ -582,10 +584,10 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
     if (v.half) {  // FP16 levels: one thread per cell
         for (int it = 0; it < iterations; ++it)
             for (int parity = 0; parity < 2; ++parity) {
-                k_rbgs_h<<<blocks_for(C, MGT), MGT, 0, s>>>(reinterpret_cast<__half*>(v.p),
-                                                           reinterpret_cast<const __half*>(v.b),
-                                                           reinterpret_cast<const Half4*>(v.opc), v.mask, v.scale,
-                                                           parity, v.nx, v.ny, v.nz);
+                launch(blocks_for(C, MGT), MGT, 0, s)(k_rbgs_h, reinterpret_cast<__half*>(v.p),
+                                                      reinterpret_cast<const __half*>(v.b),
+                                                      reinterpret_cast<const Half4*>(v.opc), v.mask, v.scale,
+                                                      parity, v.nx, v.ny, v.nz);
                 CLB_LAUNCH_CHECK("k_rbgs_h");
             }
         return 0;
@@ -599,17 +601,17 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
         for (int it = 0; it < iterations; ++it)
             for (int parity = 0; parity < 2; ++parity) {
                 if (v.l0 && vec4)
-                    k_rbgs_colour<true, 4><<<grid, block, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta, parity,
-                                                                  v.nx, v.ny, v.nz);
+                    launch(grid, block, 0, s)(k_rbgs_colour<true, 4>, v.p, v.b, v.op0, nullptr, nullptr, delta, parity,
+                                              v.nx, v.ny, v.nz);
                 else if (v.l0)
-                    k_rbgs_colour<true, 1><<<grid, block, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta, parity,
-                                                                  v.nx, v.ny, v.nz);
+                    launch(grid, block, 0, s)(k_rbgs_colour<true, 1>, v.p, v.b, v.op0, nullptr, nullptr, delta, parity,
+                                              v.nx, v.ny, v.nz);
                 else if (vec4)
-                    k_rbgs_colour<false, 4><<<grid, block, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta, parity,
-                                                                   v.nx, v.ny, v.nz);
+                    launch(grid, block, 0, s)(k_rbgs_colour<false, 4>, v.p, v.b, nullptr, v.opc, v.mask, delta, parity,
+                                              v.nx, v.ny, v.nz);
                 else
-                    k_rbgs_colour<false, 1><<<grid, block, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta, parity,
-                                                                   v.nx, v.ny, v.nz);
+                    launch(grid, block, 0, s)(k_rbgs_colour<false, 1>, v.p, v.b, nullptr, v.opc, v.mask, delta, parity,
+                                              v.nx, v.ny, v.nz);
                 CLB_LAUNCH_CHECK("k_rbgs_colour");
             }
         return 0;
@@ -623,17 +625,17 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
         float* other = v.alt;
         for (int it = 0; it < iterations; ++it) {
             if (v.l0 && use_big)
-                k_rbgs_iter<true, 8, 8, 32><<<big, SW_THREADS, 0, s>>>(cur, other, v.b, v.op0, nullptr, nullptr,
-                                                                       delta, v.nx, v.ny, v.nz);
+                launch(big, SW_THREADS, 0, s)(k_rbgs_iter<true, 8, 8, 32>, cur, other, v.b, v.op0, nullptr, nullptr,
+                                              delta, v.nx, v.ny, v.nz);
             else if (v.l0)
-                k_rbgs_iter<true, 4, 4, 32><<<small, SW_THREADS, 0, s>>>(cur, other, v.b, v.op0, nullptr, nullptr,
-                                                                         delta, v.nx, v.ny, v.nz);
+                launch(small, SW_THREADS, 0, s)(k_rbgs_iter<true, 4, 4, 32>, cur, other, v.b, v.op0, nullptr, nullptr,
+                                                delta, v.nx, v.ny, v.nz);
             else if (use_big)
-                k_rbgs_iter<false, 8, 8, 32><<<big, SW_THREADS, 0, s>>>(cur, other, v.b, nullptr, v.opc, v.mask,
-                                                                        delta, v.nx, v.ny, v.nz);
+                launch(big, SW_THREADS, 0, s)(k_rbgs_iter<false, 8, 8, 32>, cur, other, v.b, nullptr, v.opc, v.mask,
+                                              delta, v.nx, v.ny, v.nz);
             else
-                k_rbgs_iter<false, 4, 4, 32><<<small, SW_THREADS, 0, s>>>(cur, other, v.b, nullptr, v.opc, v.mask,
-                                                                          delta, v.nx, v.ny, v.nz);
+                launch(small, SW_THREADS, 0, s)(k_rbgs_iter<false, 4, 4, 32>, cur, other, v.b, nullptr, v.opc, v.mask,
+                                                delta, v.nx, v.ny, v.nz);
             CLB_LAUNCH_CHECK("k_rbgs_iter");
             float* t = cur;
             cur = other;
@@ -647,11 +649,11 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
     for (int it = 0; it < iterations; ++it)
         for (int parity = 0; parity < 2; ++parity) {
             if (v.l0)
-                k_rbgs<true><<<blocks_for(C, MGT), MGT, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta, parity, v.nx,
-                                                                 v.ny, v.nz);
+                launch(blocks_for(C, MGT), MGT, 0, s)(k_rbgs<true>, v.p, v.b, v.op0, nullptr, nullptr, delta, parity, v.nx,
+                                                      v.ny, v.nz);
             else
-                k_rbgs<false><<<blocks_for(C, MGT), MGT, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta, parity, v.nx,
-                                                                  v.ny, v.nz);
+                launch(blocks_for(C, MGT), MGT, 0, s)(k_rbgs<false>, v.p, v.b, nullptr, v.opc, v.mask, delta, parity, v.nx,
+                                                      v.ny, v.nz);
             CLB_LAUNCH_CHECK("k_rbgs");
         }
     return 0;
@@ -660,7 +662,7 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
 int coarse_solve(const LevelView& v, float delta, int iterations, cudaStream_t s) {
     const int C = v.nx * v.ny * v.nz;
     if (v.half) {  // checked to fit shared memory by check_hierarchy
-        k_coarse_solve<true, false, true><<<1, COARSE_THREADS, coarse_smem_bytes(C), s>>>(
+        launch(1, COARSE_THREADS, coarse_smem_bytes(C), s)(k_coarse_solve<true, false, true>,
             v.p, v.b, nullptr, v.opc, v.mask, delta, iterations, v.nx, v.ny, v.nz, v.scale);
         CLB_LAUNCH_CHECK("k_coarse_solve");
         return 0;
@@ -668,18 +670,18 @@ int coarse_solve(const LevelView& v, float delta, int iterations, cudaStream_t s
     if (C <= COARSE_SMEM_CELLS) {
         const size_t bytes = coarse_smem_bytes(C);
         if (v.l0)
-            k_coarse_solve<true, true><<<1, COARSE_THREADS, bytes, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta,
-                                                                         iterations, v.nx, v.ny, v.nz);
+            launch(1, COARSE_THREADS, bytes, s)(k_coarse_solve<true, true>, v.p, v.b, v.op0, nullptr, nullptr, delta,
+                                                iterations, v.nx, v.ny, v.nz, nullptr);
         else
-            k_coarse_solve<true, false><<<1, COARSE_THREADS, bytes, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta,
-                                                                          iterations, v.nx, v.ny, v.nz);
+            launch(1, COARSE_THREADS, bytes, s)(k_coarse_solve<true, false>, v.p, v.b, nullptr, v.opc, v.mask, delta,
+                                                iterations, v.nx, v.ny, v.nz, nullptr);
     } else {
         if (v.l0)
-            k_coarse_solve<false, true><<<1, COARSE_THREADS, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, delta,
-                                                                      iterations, v.nx, v.ny, v.nz);
+            launch(1, COARSE_THREADS, 0, s)(k_coarse_solve<false, true>, v.p, v.b, v.op0, nullptr, nullptr, delta,
+                                            iterations, v.nx, v.ny, v.nz, nullptr);
         else
-            k_coarse_solve<false, false><<<1, COARSE_THREADS, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, delta,
-                                                                       iterations, v.nx, v.ny, v.nz);
+            launch(1, COARSE_THREADS, 0, s)(k_coarse_solve<false, false>, v.p, v.b, nullptr, v.opc, v.mask, delta,
+                                            iterations, v.nx, v.ny, v.nz, nullptr);
     }
     CLB_LAUNCH_CHECK("k_coarse_solve");
     return 0;
@@ -692,25 +694,23 @@ int bottom_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int co
     const int* a = h->shape[level];
     const int* b = h->shape[level + 1];
     const int ca = a[0] * a[1] * a[2], cb = b[0] * b[1] * b[2];
-    const int ma = (a[0] - 2) * (a[1] - 2) * (a[2] - 2), mb = (b[0] - 2) * (b[1] - 2) * (b[2] - 2);
+    const int sa = colour_slots(a[0], a[1], a[2]), sb = colour_slots(b[0], b[1], b[2]);
     const size_t bytes = bottom_smem_bytes(ca, cb);
-    const int mbc = mb / 2;  // cells of each colour (the B extent along k must be even)
-    if (bytes > kBottomSmemLimit || ((b[2] - 2) & 1) || mbc > BOTTOM_MAX_B * BOTTOM_BTHREADS ||
-        ma > BOTTOM_MAX_A * BOTTOM_THREADS)
+    if (bytes > kBottomSmemLimit || sb > BOTTOM_MAX_B * BOTTOM_BTHREADS || sa > BOTTOM_MAX_A * BOTTOM_THREADS)
         return 0;
-    const int ka = (ma + BOTTOM_THREADS - 1) / BOTTOM_THREADS;
-    const int kb = (mbc + BOTTOM_BTHREADS - 1) / BOTTOM_BTHREADS;
+    const int ka = (sa + BOTTOM_THREADS - 1) / BOTTOM_THREADS;
+    const int kb = (sb + BOTTOM_BTHREADS - 1) / BOTTOM_BTHREADS;
 #define CLB_BOTTOM(KA, KB, H)                                                                                   \
-    k_bottom_visit<KA, KB, H><<<1, BOTTOM_THREADS, bytes, s>>>(                                                   \
-        h->p[level], h->b[level], (const float4*)h->op[level], h->mask[level], a[0], a[1], a[2], h->p[level + 1], \
-        h->b[level + 1], (const float4*)h->op[level + 1], h->mask[level + 1], b[0], b[1], b[2], h->delta, pre,  \
-        post, coarse_iters, h->fp16_scale)
+    launch(1, BOTTOM_THREADS, bytes, s)(k_bottom_visit<KA, KB, H>,                                                    \
+        h->p[level], h->b[level], (const float4*)h->op[level], h->mask[level], a[0], a[1], a[2], h->p[level + 1],      \
+        h->b[level + 1], (const float4*)h->op[level + 1], h->mask[level + 1], b[0], b[1], b[2], h->delta, pre,         \
+                                        post, coarse_iters, h->fp16_scale)
 #define CLB_BOTTOM_KINDS(H)                                 \
-    if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1, H);            \
+    if (ka <= 1 && kb <= 1) CLB_BOTTOM(1, 1, H);            \
+    else if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1, H);       \
     else if (ka <= 4 && kb <= 1) CLB_BOTTOM(4, 1, H);       \
-    else if (ka <= 8 && kb <= 1) CLB_BOTTOM(8, 1, H);       \
-    else if (ka <= 8 && kb <= 2) CLB_BOTTOM(8, 2, H);       \
-    else CLB_BOTTOM(16, 4, H);
+    else if (ka <= 4 && kb <= 2) CLB_BOTTOM(4, 2, H);       \
+    else CLB_BOTTOM(8, 4, H);
     if (is_half(h, level)) {  // the suffix of FP16 levels then holds both bottom levels
         CLB_BOTTOM_KINDS(true)
     } else {
@@ -735,21 +735,21 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
     if (c.half) {
         const dim3 grid = blocks_for(Cc, MGT);
 #define CLB_RESTRICT_H(FS)                                                                                        \
-    k_restrict_h<FS><<<grid, MGT, 0, s>>>(v.p, v.b, v.op0, v.opc, v.mask, reinterpret_cast<__half*>(c.p),          \
-                                          reinterpret_cast<__half*>(const_cast<float*>(c.b)), h->delta, h->fp16_scale, \
-                                          v.nx, v.ny, v.nz, c.nx, c.ny, c.nz)
+    launch(grid, MGT, 0, s)(k_restrict_h<FS>, v.p, v.b, v.op0, v.opc, v.mask, reinterpret_cast<__half*>(c.p),          \
+                            reinterpret_cast<__half*>(const_cast<float*>(c.b)), h->delta, h->fp16_scale,               \
+                            v.nx, v.ny, v.nz, c.nx, c.ny, c.nz)
         if (v.half) CLB_RESTRICT_H(2);
         else if (v.l0) CLB_RESTRICT_H(0);
         else CLB_RESTRICT_H(1);
 #undef CLB_RESTRICT_H
     } else if (v.l0)
-        k_restrict<true><<<blocks_for(Cc, MGT), MGT, 0, s>>>(v.p, v.b, v.op0, nullptr, nullptr, c.p,
-                                                              const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
-                                                              c.nx, c.ny, c.nz);
+        launch(blocks_for(Cc, MGT), MGT, 0, s)(k_restrict<true>, v.p, v.b, v.op0, nullptr, nullptr, c.p,
+                                               const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
+                                               c.nx, c.ny, c.nz);
     else
-        k_restrict<false><<<blocks_for(Cc, MGT), MGT, 0, s>>>(v.p, v.b, nullptr, v.opc, v.mask, c.p,
-                                                               const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
-                                                               c.nx, c.ny, c.nz);
+        launch(blocks_for(Cc, MGT), MGT, 0, s)(k_restrict<false>, v.p, v.b, nullptr, v.opc, v.mask, c.p,
+                                               const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
+                                               c.nx, c.ny, c.nz);
     CLB_LAUNCH_CHECK("k_restrict");
     if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
@@ -758,20 +758,20 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
         const dim3 grid = blocks_for(Cf, MGT);
         const __half* ce = reinterpret_cast<const __half*>(c.p);
         if (v.half)
-            k_prolong_h<2><<<grid, MGT, 0, s>>>(ce, v.p, nullptr, v.mask, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                                 v.nz);
+            launch(grid, MGT, 0, s)(k_prolong_h<2>, ce, v.p, nullptr, v.mask, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                    v.nz);
         else if (v.l0)
-            k_prolong_h<0><<<grid, MGT, 0, s>>>(ce, v.p, v.op0, nullptr, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                                 v.nz);
+            launch(grid, MGT, 0, s)(k_prolong_h<0>, ce, v.p, v.op0, nullptr, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                    v.nz);
         else
-            k_prolong_h<1><<<grid, MGT, 0, s>>>(ce, v.p, nullptr, v.mask, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                                 v.nz);
+            launch(grid, MGT, 0, s)(k_prolong_h<1>, ce, v.p, nullptr, v.mask, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                    v.nz);
     } else if (v.l0)
-        k_prolong<true><<<blocks_for(Cf, MGT), MGT, 0, s>>>(c.p, v.p, v.op0, nullptr, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                                             v.nz);
+        launch(blocks_for(Cf, MGT), MGT, 0, s)(k_prolong<true>, c.p, v.p, v.op0, nullptr, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                               v.nz);
     else
-        k_prolong<false><<<blocks_for(Cf, MGT), MGT, 0, s>>>(c.p, v.p, nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                                              v.nz);
+        launch(blocks_for(Cf, MGT), MGT, 0, s)(k_prolong<false>, c.p, v.p, nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny,
+                                               v.nz);
     CLB_LAUNCH_CHECK("k_prolong");
     return smooth(v, h->delta, post, s);
 }
@@ -786,7 +786,7 @@ int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pr
     cudaStream_t s = CLB_STREAM(stream);
     if (h->fp16_level > 0) {
         CLB_REQUIRE(h->rhs_norms != nullptr, "mg_w_cycle: FP16 levels need rhs_norms");
-        k_fp16_scale<<<1, 32, 0, s>>>(h->rhs_norms, h->delta, h->fp16_scale);
+        launch(1, 32, 0, s)(k_fp16_scale, h->rhs_norms, h->delta, h->fp16_scale);
         CLB_LAUNCH_CHECK("k_fp16_scale");
     }
     return w_cycle(h, 0, x, rhs, pre_smooth, post_smooth, coarse_iterations, s);
@@ -801,8 +801,9 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
 }
 
 int clb_mg_set_option(int option, int value) {
-    CLB_REQUIRE(option == 0, "mg_set_option: unknown option %d", option);
-    g_use_bottom = value != 0;
+    CLB_REQUIRE(option == 0 || option == 1, "mg_set_option: unknown option %d", option);
+    if (option == 0) g_use_bottom = value != 0;
+    else g_use_pdl = value != 0;
     return 0;
 }
 
@@ -821,14 +822,15 @@ int clb_mg_residual_norms(const void* p, int p_is_double, const float* b, const 
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
     if (p_is_double)
-        k_residual_rows<double, RES_NORM><<<blocks, RN_THREADS, 0, s>>>((const double*)p, nullptr, nullptr, b, op0,
-                                                                     inv_delta2, nx, ny, nz, r_out,
-                                                                     (double2*)partials);
+        launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_NORM>, (const double*)p, nullptr, nullptr, b, op0,
+                                         inv_delta2, nx, ny, nz, r_out,
+                                         (double2*)partials, nullptr, nullptr, nullptr);
     else
-        k_residual_rows<float, RES_NORM><<<blocks, RN_THREADS, 0, s>>>((const float*)p, nullptr, nullptr, b, op0,
-                                                                    inv_delta2, nx, ny, nz, r_out, (double2*)partials);
+        launch(blocks, RN_THREADS, 0, s)(k_residual_rows<float, RES_NORM>, (const float*)p, nullptr, nullptr, b, op0,
+                                         inv_delta2, nx, ny, nz, r_out, (double2*)partials,
+                                         nullptr, nullptr, nullptr);
     CLB_LAUNCH_CHECK("k_residual_rows");
-    k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
+    launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
     return 0;
 }
@@ -842,10 +844,10 @@ int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const 
     const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    k_residual_rows<double, RES_IR><<<blocks, RN_THREADS, 0, s>>>(p64_in, e, p64_out, b, op0, inv_delta2, nx, ny,
-                                                                  nz, r_out, (double2*)partials);
+    launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_IR>, p64_in, e, p64_out, b, op0, inv_delta2, nx, ny,
+                                     nz, r_out, (double2*)partials, nullptr, nullptr, nullptr);
     CLB_LAUNCH_CHECK("k_residual_rows");
-    k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
+    launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
     return 0;
 }
@@ -858,9 +860,9 @@ int clb_mg_fcg_dots(const float* z, const float* d, const float* r, const uint8_
     const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    k_fcg_dots<<<blocks, RN_THREADS, 0, s>>>(z, d, r, op0, inv_delta2, nx, ny, nz, (Sum4*)partials4);
+    launch(blocks, RN_THREADS, 0, s)(k_fcg_dots, z, d, r, op0, inv_delta2, nx, ny, nz, (Sum4*)partials4);
     CLB_LAUNCH_CHECK("k_fcg_dots");
-    k_fcg_scalars<<<1, 256, 0, s>>>((const Sum4*)partials4, blocks, state);
+    launch(1, 256, 0, s)(k_fcg_scalars, (const Sum4*)partials4, blocks, state);
     CLB_LAUNCH_CHECK("k_fcg_scalars");
     return 0;
 }
@@ -876,10 +878,10 @@ int clb_mg_fcg_step(const double* p64_in, const float* z, const float* d_in, dou
     const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    k_residual_rows<double, RES_FCG><<<blocks, RN_THREADS, 0, s>>>(p64_in, z, p64_out, b, op0, inv_delta2, nx, ny,
-                                                                   nz, r_out, (double2*)partials, d_in, d_out, state);
+    launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_FCG>, p64_in, z, p64_out, b, op0, inv_delta2, nx, ny,
+                                     nz, r_out, (double2*)partials, d_in, d_out, state);
     CLB_LAUNCH_CHECK("k_residual_rows");
-    k_reduce_partials<<<1, 256, 0, s>>>((const double2*)partials, blocks, (double2*)out);
+    launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
     return 0;
 }
@@ -888,7 +890,7 @@ int clb_mg_ir_init(const float* p32, const uint8_t* op0, double* p64, int nx, in
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(p32 && op0 && p64, "mg_ir_init: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_ir_init<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(p32, op0, p64, nx, ny, nz);
+    launch(blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_init, p32, op0, p64, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_ir_init");
     return 0;
 }
@@ -896,7 +898,7 @@ int clb_mg_ir_init(const float* p32, const uint8_t* op0, double* p64, int nx, in
 int clb_mg_ir_update(double* p64, const float* e, int64_t cells, void* stream) {
     CLB_REQUIRE(p64 && e && cells >= 0, "mg_ir_update: bad arguments");
     if (cells == 0) return 0;
-    k_ir_update<<<blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream)>>>(p64, e, cells);
+    launch(blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_update, p64, e, cells);
     CLB_LAUNCH_CHECK("k_ir_update");
     return 0;
 }
@@ -904,7 +906,7 @@ int clb_mg_ir_update(double* p64, const float* e, int64_t cells, void* stream) {
 int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream) {
     CLB_REQUIRE(p64 && p32 && cells >= 0, "mg_ir_store: bad arguments");
     if (cells == 0) return 0;
-    k_ir_store<<<blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream)>>>(p64, p32, cells);
+    launch(blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_store, p64, p32, cells);
     CLB_LAUNCH_CHECK("k_ir_store");
     return 0;
 }

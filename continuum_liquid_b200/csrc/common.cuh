@@ -78,6 +78,48 @@ static inline unsigned int blocks_for(i64 n, int threads) { return (unsigned int
 // Number of SMs on the current device (cached per process; the library serves one GPU).
 static int g_sm_count = 0;
 
+// Programmatic dependent launch. The pressure-solve kernels are launched with programmatic stream
+// serialisation (launch()), so a kernel's blocks may be scheduled while its predecessor in the stream
+// is still running; each such kernel calls pdl_begin() before its first memory access. pdl_begin
+// waits until the predecessor grid has completed and its writes are visible (griddepcontrol.wait:
+// immediate when the kernel was launched without the attribute), then allows the next kernel of the
+// stream to be scheduled. A grid completes only after every block has passed its own wait, so
+// dependences on kernels further back in the stream hold as well. The waiting blocks are placed only
+// after all blocks of the running grid have started, so they never take an SM a running grid needs.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+static bool g_use_pdl = true;  // clb_mg_set_option(1, ...) switches programmatic dependent launch off
+
+// launch(grid, block, smem, stream)(kernel, args...): the kernel launch with programmatic stream
+// serialisation (when enabled); the kernel must start with pdl_begin(). Errors are left for
+// check_launch (cudaGetLastError).
+struct Launch {
+    dim3 grid, block;
+    size_t smem;
+    cudaStream_t stream;
+    template <typename... P, typename... A>
+    void operator()(void (*kernel)(P...), A&&... args) const {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = g_use_pdl ? 1 : 0;
+        (void)cudaLaunchKernelEx(&cfg, kernel, static_cast<A&&>(args)...);
+    }
+};
+
+static inline Launch launch(dim3 grid, dim3 block, size_t smem, cudaStream_t stream) {
+    return Launch{grid, block, smem, stream};
+}
+
 }  // namespace clb
 
 #define CLB_REQUIRE(cond, ...)                  \

@@ -201,6 +201,7 @@ template <typename PT>
 __global__ void __launch_bounds__(GT) k_pressure_correction(float* __restrict__ u, float* __restrict__ v,
                                                              float* __restrict__ w, const PT* __restrict__ p,
                                                              float dt_over_rho, float inv_dx, int nx, int ny, int nz) {
+    pdl_begin();
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
     if (c >= C) return;
@@ -218,6 +219,7 @@ __device__ __forceinline__ void neumann_domain_bc_at(i64 c, PT* p, int nx, int n
 
 template <typename PT>
 __global__ void __launch_bounds__(GT) k_neumann_domain_bc(PT* p, int nx, int ny, int nz) {
+    pdl_begin();
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
     if (c >= C) return;

@@ -7,19 +7,19 @@
 // launches these are bound by launch latency; here one block of 512 threads runs the whole visit
 // with both levels in shared memory and block barriers between phases.
 //
-// Each thread owns a fixed set of A cells and B cells (interior cells in index order, strided by the
-// block size); the cell index, diagonal and delta^2 * b of each owned cell stay in registers across
-// all sweeps (the neighbour weights are read from shared memory). The update formula and every summation order
-// are those of multigrid.cl (rbgs_step, restrict_residual, prolongate), so the result is identical
-// to the launch-per-kernel W-cycle.
+// Each thread owns a fixed set of A cells and B cells of either colour (colour slots, below); the
+// cell index, diagonal and delta^2 * b of each owned cell stay in registers across all sweeps (the
+// neighbour weights of A cells are read from shared memory, those of B cells are registers too). The
+// update formula and every summation order are those of multigrid.cl (rbgs_step, restrict_residual,
+// prolongate), so the result is identical to the launch-per-kernel W-cycle.
 #pragma once
 #include "multigrid.cuh"
 
 namespace clb {
 
 constexpr int BOTTOM_THREADS = 512;
-constexpr int BOTTOM_MAX_A = 16;  // A cells per thread
-constexpr int BOTTOM_MAX_B = 4;  // B cells of each colour per B thread
+constexpr int BOTTOM_MAX_A = 8;  // A slots of each colour per thread
+constexpr int BOTTOM_MAX_B = 4;  // B slots of each colour per B thread
 
 static inline size_t bottom_smem_bytes(int ca, int cb) {
     // A: p, b, op(float4); B: p, op(float4); each region padded to 16 bytes
@@ -27,31 +27,33 @@ static inline size_t bottom_smem_bytes(int ca, int cb) {
     return pad((size_t)ca * 4) * 2 + (size_t)ca * 16 + pad((size_t)cb * 4) + (size_t)cb * 16;
 }
 
-// Constants of one owned cell: smem index, diagonal (< 0: not fluid, never updated), delta^2 * b
-// and colour (2 for threads without a cell).
+// Cells of one colour are numbered by slots: the interior rows (i, j) in index order, ceil(mz / 2)
+// slots per row, slot s of a row being its (s+1)-th cell of the colour, k = k0 + 2 s with k0 the
+// row's first such k (1 or 2). With an odd interior extent along k the last slot of every other row
+// is empty. A colour phase updates cells of one colour only, and those are independent of each other,
+// so any assignment of cells to threads gives the same result; numbering by colour keeps every lane
+// of a warp busy in every phase.
+__host__ __device__ __forceinline__ int colour_slots(int nx, int ny, int nz) {
+    return (nx - 2) * (ny - 2) * ((nz - 1) / 2);
+}
+
+// smem / grid index of slot r of colour `colour`, or -1 for an empty slot or r past the last slot
+__device__ __forceinline__ int colour_cell(int r, int colour, int nx, int ny, int nz) {
+    const int half = (nz - 1) / 2, my = ny - 2;
+    const int row = r / half, s = r - row * half;
+    const int i = 1 + row / my, j = 1 + row % my;
+    const int k = 1 + 2 * s + ((i + j + 1 + colour) & 1);
+    if (i > nx - 2 || k > nz - 2) return -1;
+    return (i * ny + j) * nz + k;
+}
+
+// Constants of one owned cell of the second-coarsest level: smem index, diagonal (<= 0: not updated;
+// -1 marks cells that are not fluid or slots without a cell) and delta^2 * b.
 struct OwnedCell {
     int c;
     float d;
     float d2b;
-    int colour;
 };
-
-__device__ __forceinline__ void owned_cell(int q, int nx, int ny, int nz, const float4* so, bool valid, OwnedCell& o) {
-    const int my = ny - 2, mz = nz - 2;
-    o.d = -1.0f;
-    o.c = 0;
-    o.colour = 2;
-    if (!valid) return;
-    const int i = 1 + q / (my * mz), rem = q % (my * mz), j = 1 + rem / mz, k = 1 + rem % mz;
-    (void)nx;
-    const int sx = ny * nz, sy = nz;
-    const int c = (i * ny + j) * nz + k;
-    o.c = c;
-    o.colour = (i + j + k) & 1;
-    (void)sx;
-    (void)sy;
-    o.d = so[c].x;  // -1 when not fluid
-}
 
 // Owned coarsest-level cell with its neighbour weights in registers (constant for the whole visit).
 struct OwnedCellW {
@@ -77,24 +79,15 @@ __device__ __forceinline__ void relax(const OwnedCell& o, float* sp, const float
 }
 
 // The coarsest level B runs on BOTTOM_BTHREADS threads (8 warps) that synchronise with a named
-// barrier: each owns the r-th red and the r-th black interior cell (r = thread, thread + 256, ...), so
-// every thread updates one cell per colour phase. This needs an even interior extent along k (each
-// row then holds the same number of cells of either colour).
+// barrier; each owns slots r = thread, thread + 256, ... of both colours, so every thread updates
+// its cells of one colour per phase.
 constexpr int BOTTOM_BTHREADS = 256;
 
 __device__ __forceinline__ void bar_b() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
-// interior cell of colour `colour` with ordinal r (rows of mz/2 cells of each colour, index order)
-__device__ __forceinline__ int colour_cell(int r, int colour, int ny, int nz) {
-    const int half = (nz - 2) / 2, my = ny - 2;
-    const int row = r / half, m = r - row * half;
-    const int i = 1 + row / my, j = 1 + row % my;
-    const int k = 1 + 2 * m + ((i + j + 1 + colour) & 1);
-    return (i * ny + j) * nz + k;
-}
-
 // H = true: both levels are stored in FP16 (p, b and operator as __half, scaled values); the visit
 // computes in FP32 in shared memory with kappa = scale[2] in place of delta^2 (mg_half.cuh).
+// KA: A slots of each colour per thread (of BOTTOM_THREADS); KB: B slots of each colour per B thread.
 template <int KA, int KB, bool H = false>
 __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const float* __restrict__ ba,
                                                    const float4* __restrict__ opa, const uint8_t* __restrict__ ma,
@@ -177,29 +170,30 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
     __syncthreads();
 
     const int asx = any * anz, asy = anz, bsx = bny * bnz, bsy = bnz;
-    const int MA = (anx - 2) * (any - 2) * (anz - 2);
-    const int MBC = (bnx - 2) * (bny - 2) * (bnz - 2) / 2;  // cells of each colour on B
-    OwnedCell A[KA];
+    OwnedCell A[2][KA];  // [colour][m]
 #pragma unroll
-    for (int m = 0; m < KA; ++m) {
-        const int q = threadIdx.x + m * BOTTOM_THREADS;
-        owned_cell(q, anx, any, anz, soa, q < MA, A[m]);
-        A[m].d2b = q < MA ? d2 * sba[A[m].c] : 0.0f;
-    }
+    for (int colour = 0; colour < 2; ++colour)
+#pragma unroll
+        for (int m = 0; m < KA; ++m) {
+            const int c = colour_cell(threadIdx.x + m * BOTTOM_THREADS, colour, anx, any, anz);
+            OwnedCell& o = A[colour][m];
+            o.c = c < 0 ? 0 : c;
+            o.d = c < 0 ? -1.0f : soa[c].x;  // -1 when not fluid
+            o.d2b = c < 0 ? 0.0f : d2 * sba[c];
+        }
     const bool btile = threadIdx.x < BOTTOM_BTHREADS;
     OwnedCellW B[2][KB];  // [colour][m]
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KB; ++m) {
-            const int r = threadIdx.x + m * BOTTOM_BTHREADS;
+            const int c = btile ? colour_cell(threadIdx.x + m * BOTTOM_BTHREADS, colour, bnx, bny, bnz) : -1;
             OwnedCellW& o = B[colour][m];
             o.d2b = 0.0f;
             o.c = 0;
             o.d = -1.0f;
             o.wxp = o.wxm = o.wyp = o.wym = o.wzp = o.wzm = 0.0f;
-            if (btile && r < MBC) {
-                const int c = colour_cell(r, colour, bny, bnz);
+            if (c >= 0) {
                 const float4 self = sob[c];
                 o.c = c;
                 o.d = self.x;
@@ -214,10 +208,11 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
 
     auto smooth_a = [&](int iterations) {
         for (int it = 0; it < iterations; ++it)
-            for (int parity = 0; parity < 2; ++parity) {
+#pragma unroll
+            for (int colour = 0; colour < 2; ++colour) {
 #pragma unroll
                 for (int m = 0; m < KA; ++m)
-                    if (A[m].colour == parity && A[m].d > 0.0f) relax(A[m], spa, soa, asx, asy);
+                    if (A[colour][m].d > 0.0f) relax(A[colour][m], spa, soa, asx, asy);
                 __syncthreads();
             }
     };
@@ -229,9 +224,8 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KB; ++m) {
-            const int r = threadIdx.x + m * BOTTOM_BTHREADS;
             float rhs = 0.0f;
-            if (btile && r < MBC) {
+            if (B[colour][m].d >= 0.0f) {  // a fluid cell (slots without a cell and air cells hold -1)
                 const int c = B[colour][m].c;
                 const int I = c / bsx, J = (c / bsy) % bny, K = c % bnz;
                 const int si = 1 + 2 * (I - 1), sj = 1 + 2 * (J - 1), sk = 1 + 2 * (K - 1);
@@ -267,14 +261,16 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
     __syncthreads();
     // prolongation (multigrid.cl:182-201)
 #pragma unroll
-    for (int m = 0; m < KA; ++m) {
-        if (A[m].d < 0.0f) continue;  // interior fluid cells only
-        const int c = A[m].c;
-        const int i = c / asx, j = (c / asy) % any, k = c % anz;
-        const int I = min((i - 1) / 2 + 1, bnx - 2), J = min((j - 1) / 2 + 1, bny - 2),
-                  K = min((k - 1) / 2 + 1, bnz - 2);
-        spa[c] += spb[(I * bny + J) * bnz + K];
-    }
+    for (int colour = 0; colour < 2; ++colour)
+#pragma unroll
+        for (int m = 0; m < KA; ++m) {
+            if (A[colour][m].d < 0.0f) continue;  // interior fluid cells only
+            const int c = A[colour][m].c;
+            const int i = c / asx, j = (c / asy) % any, k = c % anz;
+            const int I = min((i - 1) / 2 + 1, bnx - 2), J = min((j - 1) / 2 + 1, bny - 2),
+                      K = min((k - 1) / 2 + 1, bnz - 2);
+            spa[c] += spb[(I * bny + J) * bnz + K];
+        }
     __syncthreads();
     smooth_a(post);
 
@@ -287,10 +283,9 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
-        for (int m = 0; m < KB; ++m) {
-            const int r = threadIdx.x + m * BOTTOM_BTHREADS;
-            if (btile && r < MBC) st(bb, B[colour][m].c, bvals[colour][m]);
-        }
+        for (int m = 0; m < KB; ++m)
+            if (btile && colour_cell(threadIdx.x + m * BOTTOM_BTHREADS, colour, bnx, bny, bnz) >= 0)
+                st(bb, B[colour][m].c, bvals[colour][m]);
 }
 
 template <int KA, int KB, bool H = false>
@@ -300,6 +295,7 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
                    float* __restrict__ bb, const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx,
                    int bny, int bnz, float delta, int pre, int post, int coarse_iters,
                    const float* __restrict__ scale = nullptr) {
+    pdl_begin();
     bottom_visit_block<KA, KB, H>(pa, ba, opa, ma, anx, any, anz, pb, bb, opb, mb, bnx, bny, bnz, delta, pre, post,
                                   coarse_iters, scale);
 }

@@ -23,6 +23,7 @@ namespace clb {
 
 // scale = {sigma_b, 1 / sigma_p, kappa, 1 / kappa} from rhs_norms[0] = ||r||_2^2 (one thread).
 __global__ void k_fp16_scale(const double* __restrict__ rhs_norms, float delta, float* __restrict__ scale) {
+    pdl_begin();
     if (threadIdx.x != 0) return;
     const double nrm = sqrt(fmax(rhs_norms[0], 0.0));
     int eb = 0;
@@ -42,6 +43,7 @@ __global__ void k_fp16_scale(const double* __restrict__ rhs_norms, float delta, 
 __global__ void __launch_bounds__(MGT) k_rbgs_h(__half* p, const __half* __restrict__ b, const Half4* __restrict__ op,
                                                  const uint8_t* __restrict__ mask, const float* __restrict__ scale,
                                                  int parity, int nx, int ny, int nz) {
+    pdl_begin();
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c >= C) return;
@@ -79,6 +81,7 @@ __global__ void __launch_bounds__(MGT) k_restrict_h(const void* __restrict__ fp,
                                                      __half* __restrict__ cb, float delta,
                                                      const float* __restrict__ scale, int fnx, int fny, int fnz,
                                                      int cnx, int cny, int cnz) {
+    pdl_begin();
     const i64 C = (i64)cnx * cny * cnz;
     const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
     if (ci >= C) return;
@@ -117,6 +120,7 @@ __global__ void __launch_bounds__(MGT) k_prolong_h(const __half* __restrict__ ce
                                                     const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
                                                     const float* __restrict__ scale, int cnx, int cny, int cnz,
                                                     int fnx, int fny, int fnz) {
+    pdl_begin();
     const i64 C = (i64)fnx * fny * fnz;
     const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
     if (f >= C) return;

@@ -27,6 +27,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_rbgs_iter(const float* __restric
                                                            const float4* __restrict__ opc,
                                                            const uint8_t* __restrict__ mask, float delta, int nx,
                                                            int ny, int nz) {
+    pdl_begin();
     constexpr int SW_PI = SW_TI + 4, SW_PJ = SW_TJ + 4, SW_PK = SW_TK + 4;  // p region (halo 2)
     constexpr int SW_BI = SW_TI + 2, SW_BJ = SW_TJ + 2, SW_BK = SW_TK + 2;  // b region (halo 1)
     constexpr int SW_PCELLS = SW_PI * SW_PJ * SW_PK;
@@ -232,6 +233,7 @@ __global__ void __launch_bounds__(128) k_rbgs_colour(float* p, const float* __re
                                                       const float4* __restrict__ opc,
                                                       const uint8_t* __restrict__ mask, float delta, int parity,
                                                       int nx, int ny, int nz) {
+    pdl_begin();
     rbgs_colour_at<L0, VEC>(blockIdx.x, blockIdx.y, blockIdx.z, p, b, op0, opc, mask, delta, parity, nx, ny, nz);
 }
 

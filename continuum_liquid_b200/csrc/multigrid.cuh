@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(MGT) k_rhs_op0(const float* __restrict__ u, co
                                                   const float* __restrict__ w, const float* __restrict__ ff,
                                                   float* __restrict__ rhs, uint8_t* __restrict__ op0,
                                                   float rho_over_dt, float inv_dx, int nx, int ny, int nz) {
+    pdl_begin();
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c >= C) return;
@@ -319,6 +320,7 @@ __global__ void __launch_bounds__(MGT) k_coarse_operator(const uint8_t* __restri
                                                           const uint8_t* __restrict__ fmask, void* __restrict__ cop_,
                                                           uint8_t* __restrict__ cmask, int* __restrict__ inexact,
                                                           int fnx, int fny, int fnz, int cnx, int cny, int cnz) {
+    pdl_begin();
     const i64 C = (i64)cnx * cny * cnz;
     const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
     if (ci >= C) return;
@@ -358,6 +360,7 @@ template <bool L0>
 __global__ void __launch_bounds__(MGT) k_rbgs(float* p, const float* __restrict__ b, const uint8_t* __restrict__ op0,
                                                const float4* __restrict__ opc, const uint8_t* __restrict__ mask,
                                                float delta, int parity, int nx, int ny, int nz) {
+    pdl_begin();
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c >= C) return;
@@ -417,6 +420,7 @@ __global__ void __launch_bounds__(MGT) k_restrict(const float* __restrict__ fp, 
                                                    const uint8_t* __restrict__ fmask, float* __restrict__ cp,
                                                    float* __restrict__ cb, float delta, int fnx, int fny, int fnz,
                                                    int cnx, int cny, int cnz) {
+    pdl_begin();
     const i64 C = (i64)cnx * cny * cnz;
     const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
     if (ci >= C) return;
@@ -440,6 +444,7 @@ template <bool L0>
 __global__ void __launch_bounds__(MGT) k_prolong(const float* __restrict__ ce, float* __restrict__ fp,
                                                   const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
                                                   int cnx, int cny, int cnz, int fnx, int fny, int fnz) {
+    pdl_begin();
     const i64 C = (i64)fnx * fny * fnz;
     const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
     if (f >= C) return;
@@ -522,6 +527,7 @@ __global__ void __launch_bounds__(COARSE_THREADS) k_coarse_solve(float* p, const
                                                                   const uint8_t* __restrict__ mask, float delta,
                                                                   int iterations, int nx, int ny, int nz,
                                                                   const float* __restrict__ scale = nullptr) {
+    pdl_begin();
     coarse_solve_block<SMEM, L0, H>(p, b, op0, opc, mask, delta, iterations, nx, ny, nz, scale);
 }
 
@@ -625,6 +631,7 @@ __global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restri
                                                                const float* __restrict__ d_in = nullptr,
                                                                float* __restrict__ d_out = nullptr,
                                                                const double* __restrict__ state = nullptr) {
+    pdl_begin();
     residual_rows_block<PT, MODE>(blockIdx.x, gridDim.x, p_in, e, p_out, b, op0, inv_delta2, nx, ny, nz, r_out,
                                   partials + blockIdx.x, d_in, d_out, state);
 }
@@ -699,6 +706,7 @@ __global__ void __launch_bounds__(RN_THREADS) k_fcg_dots(const float* __restrict
                                                           const float* __restrict__ r,
                                                           const uint8_t* __restrict__ op0, double inv_delta2, int nx,
                                                           int ny, int nz, Sum4* __restrict__ partials) {
+    pdl_begin();
     fcg_dots_block(blockIdx.x, gridDim.x, z, d, r, op0, inv_delta2, nx, ny, nz, partials + blockIdx.x);
 }
 
@@ -743,6 +751,7 @@ __device__ __forceinline__ void fcg_scalars_block(const Sum4* __restrict__ parti
 }
 
 __global__ void k_fcg_scalars(const Sum4* __restrict__ partials, int count, double* __restrict__ state) {
+    pdl_begin();
     fcg_scalars_block(partials, count, state);
 }
 
@@ -768,6 +777,7 @@ __device__ __forceinline__ void reduce_partials_block(const double2* __restrict_
 }
 
 __global__ void k_reduce_partials(const double2* __restrict__ partials, int count, double2* __restrict__ out) {
+    pdl_begin();
     reduce_partials_block(partials, count, out);
 }
 
@@ -782,6 +792,7 @@ __device__ __forceinline__ void ir_init_at(i64 c, const float* __restrict__ p, c
 
 __global__ void __launch_bounds__(MGT) k_ir_init(const float* __restrict__ p, const uint8_t* __restrict__ op0,
                                                   double* __restrict__ p64, int nx, int ny, int nz) {
+    pdl_begin();
     const i64 C = (i64)nx * ny * nz;
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c >= C) return;
@@ -789,11 +800,13 @@ __global__ void __launch_bounds__(MGT) k_ir_init(const float* __restrict__ p, co
 }
 
 __global__ void __launch_bounds__(MGT) k_ir_update(double* __restrict__ p64, const float* __restrict__ e, i64 C) {
+    pdl_begin();
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c < C) p64[c] += (double)__ldg(e + c);
 }
 
 __global__ void __launch_bounds__(MGT) k_ir_store(const double* __restrict__ p64, float* __restrict__ p, i64 C) {
+    pdl_begin();
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c < C) p[c] = (float)__ldg(p64 + c);
 }

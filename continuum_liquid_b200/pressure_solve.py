@@ -99,7 +99,8 @@ class PressureSolver:
     """
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100,
-                 autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64):
+                 autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64,
+                 coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.coarse_fp16 = bool(coarse_fp16)
@@ -108,6 +109,11 @@ class PressureSolver:
         self.dx = float(dx)
         self.max_cycles = int(max_cycles)
         self.method = method
+        # red-black iterations (beyond pre-smoothing) of each coarsest-level solve inside the tolerance
+        # mode's W-cycle; the reference's 64 by default (fixed-cycle mode always uses 64)
+        self.coarse_iterations = int(coarse_iterations)
+        if self.coarse_iterations < 0:
+            raise ValueError("coarse_iterations must be >= 0")
         # FP16 storage of the coarse levels of at most fp16_max_size cells per side (tolerance mode only:
         # the W-cycle then reads the squared norm of its right-hand side from the residual kernels)
         self.hierarchy = multigrid.MultigridHierarchy(kernels, self.grid_shape, dx, min_size,
@@ -159,7 +165,7 @@ class PressureSolver:
         h = self.hierarchy
         delta = float(FIELD_DTYPE(self.dx))
         self.correction.zero_()
-        h.w_cycle(self.correction, self.residual, queue=queue)
+        h.w_cycle(self.correction, self.residual, coarse_iterations=self.coarse_iterations, queue=queue)
         if self.method == "fcg":
             self.kernels.call("clb_mg_fcg_dots", self.correction, self.direction[src], self.residual, h.op0, delta,
                               *self.grid_shape, self.fcg_partials, self.fcg_state, stream=queue)

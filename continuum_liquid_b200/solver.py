@@ -53,6 +53,9 @@ class StepOptions:
     warm_start: object = None  # callable proposing an initial pressure (learned.LearnedWarmStart)
     method: str = "fcg"  # tolerance-mode iteration: "fcg" (W-cycle preconditioned CG) or "refine"
     coarse_fp16: bool = False  # tolerance mode: store the coarse levels of at most 64^3 cells in FP16
+    # tolerance mode: red-black iterations of each coarsest-level solve in the W-cycle preconditioner
+    # beyond its pre-smoothing (the reference's fixed-cycle W-cycle uses 64, multigrid.py defaults)
+    coarse_iterations: int = 64
     revoxelise: bool = False  # voxelise the colliders again at every step (moving or deforming meshes)
 
 
@@ -97,7 +100,8 @@ class FlipSolver:
         if self.colliders and self.obstacle is None:
             self.obstacle = torch.zeros(self.grid_shape, dtype=torch.uint8, device=dev)
         self.pressure_solver = PressureSolver(kernels, self.grid_shape, self.dx, min_size=min_size,
-                                              method=self.options.method, coarse_fp16=self.options.coarse_fp16)
+                                              method=self.options.method, coarse_fp16=self.options.coarse_fp16,
+                                              coarse_iterations=self.options.coarse_iterations)
         self.last_solve: SolveStats | None = None
         self.steps_done = 0
 

@@ -238,7 +238,10 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
 /* Process-wide multigrid options (host-side switches, no device work):
  *  option 0: 1 (default) runs each visit of the second-coarsest level, including both coarse solves,
  *            as one single-block launch from shared memory; 0 launches one kernel per sweep as the
- *            reference does. Both give identical results. */
+ *            reference does. Both give identical results.
+ *  option 1: 1 (default) launches the pressure-solve kernels with programmatic dependent launch (a
+ *            kernel's blocks are scheduled while its predecessor drains and wait for its completion
+ *            on the device); 0 launches them with ordinary stream serialisation. Identical results. */
 int clb_mg_set_option(int option, int value);
 
 /* Block-partial count used by clb_mg_residual_norms for a grid of `cells` cells. */

@@ -411,3 +411,16 @@ def test_fcg_restatement(oracle):
     p = np.zeros(shape, np.float32)
     oracle.Levels(shape).w_cycle(p, b, mask, oracle.build_finest_operator(mask, shape), dx)
     assert np.array_equal(x1, np.where(mask > 0, p, 0).astype(np.float64))
+
+
+def test_fcg_with_fewer_coarse_iterations(oracle):
+    """The FCG restatement still converges with a weak coarsest-level solve in its W-cycle."""
+    n, dx = 18, np.float32(1.0 / 18.0)
+    shape = (n, n, n)
+    mask = liquid_mask(n, 9)
+    rng = np.random.default_rng(14)
+    b = (rng.standard_normal(shape) * (mask > 0)).astype(np.float32)
+    _, hist64 = oracle.fcg_solve(b, mask, shape, dx, tol=1e-8, max_cycles=60)
+    _, hist4 = oracle.fcg_solve(b, mask, shape, dx, tol=1e-8, max_cycles=60, coarse_iterations=4)
+    assert hist4[-1] <= 1e-8
+    assert len(hist4) <= len(hist64) + 3

@@ -372,16 +372,18 @@ def test_iterative_refinement_reaches_tolerance(backend, oracle, method):
     assert np.array_equal(got, oracle.neumann_domain_bc(got, shape))
 
 
-@pytest.mark.parametrize("method", ["fcg", "refine"])
-def test_refinement_history_matches_oracle(backend, oracle, method):
-    """Every W-cycle of the GPU iteration against the oracle's restatement (same FP32 W-cycle,
-    FP64 accumulation and scalars; only summation orders differ)."""
+@pytest.mark.parametrize("method,coarse", [("fcg", 64), ("refine", 64), ("fcg", 4), ("fcg", 0)])
+def test_refinement_history_matches_oracle(backend, oracle, method, coarse):
+    """Every W-cycle of the GPU iteration against the oracle's restatement (same FP32 W-cycle, with
+    the reference's or fewer coarsest-level iterations, FP64 accumulation and scalars; only summation
+    orders differ)."""
     shape, dx = (34, 30, 38), F32(1.0 / 34)
     rng = np.random.default_rng(5)
     u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
     ff, _, _ = random_system(shape, 6)
     dt, rho = 1.0 / 240.0, 1000.0
-    ps = pressure_solve.PressureSolver(backend, shape, float(dx), method=method, autotune=False)
+    ps = pressure_solve.PressureSolver(backend, shape, float(dx), method=method, autotune=False,
+                                       coarse_iterations=coarse)
     P = torch.zeros(shape, dtype=torch.float32, device="cuda")
     ps.solve((dev(u), dev(v), dev(w)), dev(ff), P, dt, rho, tol=1e-3, use_graph=False)  # builds the system
     h = ps.hierarchy
@@ -395,7 +397,8 @@ def test_refinement_history_matches_oracle(backend, oracle, method):
         ps._refine(use_graph=False)
         got.append(ps._relative(h.norms))
     orhs = oracle.pressure_rhs(u, v, w, ff, dx, dt, rho, shape)
-    x, want = oracle.fcg_solve(orhs, ff, shape, dx, p0=p0, tol=0.0, max_cycles=8, flexible=(method == "fcg"))
+    x, want = oracle.fcg_solve(orhs, ff, shape, dx, p0=p0, tol=0.0, max_cycles=8, flexible=(method == "fcg"),
+                               coarse_iterations=coarse)
     np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-14)  # FP64 summation orders differ
     assert want[-1] < 1e-3 * want[0]
     scale = np.abs(x).max()
@@ -491,13 +494,16 @@ def test_bad_arguments_raise(backend):
         backend.call("clb_rbgs_step", t, t, t, t, t, t, t, 1.0, 3, 4, 4, 4)
 
 
+@pytest.mark.parametrize("pdl", [1, 0])
 @pytest.mark.parametrize("bottom", [1, 0])
 @pytest.mark.parametrize("shape", [(66, 66, 66), (34, 40, 30)])
-def test_w_cycle_paths_agree(backend, oracle, shape, bottom):
-    """The single-block bottom visit and the fused red-black iterations give the reference values."""
+def test_w_cycle_paths_agree(backend, oracle, shape, bottom, pdl):
+    """The single-block bottom visit and the fused red-black iterations give the reference values,
+    with and without programmatic dependent launch."""
     dx = F32(1.0 / shape[0])
     ff, b, p0 = random_system(shape, 21)
     backend.lib.clb_mg_set_option(0, bottom)
+    backend.lib.clb_mg_set_option(1, pdl)
     try:
         h = multigrid.MultigridHierarchy(backend, shape, float(dx))
         h.op0.copy_(torch.zeros_like(h.op0))
@@ -514,6 +520,32 @@ def test_w_cycle_paths_agree(backend, oracle, shape, bottom):
         assert np.array_equal(host(P), q)
     finally:
         backend.lib.clb_mg_set_option(0, 1)
+        backend.lib.clb_mg_set_option(1, 1)
+
+
+def test_programmatic_launch_changes_nothing(backend):
+    """Tolerance-mode solves (flexible CG, CUDA graphs) give bit-identical FP64 pressures and cycle
+    counts with programmatic dependent launch on and off."""
+    shape = (96, 80, 72)
+    dx = 1.0 / 96
+    ff, _, _ = random_system(shape, 31)
+    rng = np.random.default_rng(32)
+    vel = [dev(rng.standard_normal(shape).astype(F32)) for _ in range(3)]
+    results = {}
+    try:
+        for pdl in (0, 1):
+            backend.lib.clb_mg_set_option(1, pdl)
+            ps = pressure_solve.PressureSolver(backend, shape, dx, autotune=False)
+            p = torch.zeros(shape, dtype=torch.float32, device="cuda")
+            stats = [ps.solve(vel, dev(ff), p, 1.0 / 240.0, 1000.0, tol=1e-6) for _ in range(3)]
+            assert all(st.rel_residual <= 1e-6 for st in stats)
+            results[pdl] = (host(ps.pressure64), host(p), [st.cycles for st in stats])
+    finally:
+        backend.lib.clb_mg_set_option(1, 1)
+    assert np.array_equal(results[0][0], results[1][0])
+    assert np.array_equal(results[0][1], results[1][1])
+    assert results[0][2] == results[1][2]
+    assert backend.device_error() == 0
 
 
 @pytest.mark.parametrize("iterations", [1, 3])
@@ -576,3 +608,21 @@ def test_revoxelising_a_static_collider_every_step_changes_nothing(backend):
         assert np.array_equal(host(sims[1].obstacle), mask0)
         assert np.array_equal(sims[0].positions(), sims[1].positions())
         assert np.array_equal(host(sims[0].pressure), host(sims[1].pressure))
+
+
+
+def test_steps_with_fewer_coarse_iterations(backend):
+    """Tolerance-mode steps with 4 instead of the reference's 64 coarsest-level iterations in the
+    W-cycle preconditioner reach the tolerance every step in about as many cycles."""
+    s = scenes.block(48)
+    pos, vel = scenes.seed_particles(s)
+    totals = {}
+    for k in (64, 4):
+        opts = solver.StepOptions(flip_ratio=0.95, tol=1e-6, gravity=s.gravity, coarse_iterations=k)
+        sim = solver.FlipSolver(backend, s.grid_shape, s.dx, pos, vel, dt=s.dt, options=opts)
+        stats = [sim.step() for _ in range(4)]
+        assert all(st.rel_residual <= 1e-6 for st in stats)
+        assert sim.pressure_solver.coarse_iterations == k
+        totals[k] = sum(st.cycles for st in stats)
+    assert totals[4] <= totals[64] + 4, totals
+    assert backend.device_error() == 0
