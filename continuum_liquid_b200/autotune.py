@@ -15,6 +15,8 @@ KINDS = {
     2: "fused iteration, 8x8x32 tiles",
     3: "fused iteration, 4x4x32 tiles",
     4: "two colour launches, one thread per cell",
+    5: "fused pairs of iterations, 8x8x32 tiles",
+    6: "fused pairs of iterations, 4x4x32 tiles",
 }
 
 _cache: dict[tuple, dict[int, int]] = {}
@@ -42,9 +44,9 @@ def tune_hierarchy(h, x, rhs, iterations: int = 4, repeats: int = 3) -> dict[int
         choice = {}
         timings = {}
         for level in range(h.levels - 1):
-            if h.is_fp16(level):
-                continue  # FP16 levels have one sweep kind (per-cell)
-            candidates = [1, 4] + ([2, 3] if h.alt[level] is not None else [])
+            # FP32 coarse levels have no two-iteration 8x8x32 tile (kind 5 runs as 6 there)
+            fused = ([2, 3, 5, 6] if level == 0 or h.is_fp16(level) else [2, 3, 6]) if h.alt[level] is not None else []
+            candidates = ([4] if h.is_fp16(level) else [1, 4]) + fused
             times = {}
             for kind in candidates:
                 h.set_sweep(level, kind)

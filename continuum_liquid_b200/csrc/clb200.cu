@@ -8,6 +8,7 @@
 #include "mg_bottom.cuh"
 #include "mg_sweep.cuh"
 #include "mg_half.cuh"
+#include "mg_cluster.cuh"
 #include "batch.cuh"
 #include "sources.cuh"
 #include "voxelise.cuh"
@@ -28,6 +29,40 @@ using namespace clb;
 static const int kAbiVersion = 7;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
+static bool g_use_cluster = true;  // clb_mg_set_option(2, ...) switches the cluster visit off
+
+template <bool L0, bool H, int TI, int TJ, int T>
+static cudaError_t rbgs_iter_attr_one() {
+    return cudaFuncSetAttribute(k_rbgs_iter<L0, H, TI, TJ, 32, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)SweepTile<L0, H, TI, TJ, 32, T>::smem());
+}
+// every tile and iteration count dispatched for one level kind (FP32 coarse levels have no
+// two-iteration 8 x 8 x 32 tile: its staged operator would exceed the shared memory)
+template <bool L0, bool H>
+static cudaError_t rbgs_iter_attr() {
+    cudaError_t e = rbgs_iter_attr_one<L0, H, 4, 4, 1>();
+    e = e != cudaSuccess ? e : rbgs_iter_attr_one<L0, H, 4, 4, 2>();
+    e = e != cudaSuccess ? e : rbgs_iter_attr_one<L0, H, 8, 8, 1>();
+    if (L0 || H) e = e != cudaSuccess ? e : rbgs_iter_attr_one<L0, H, 8, 8, (L0 || H) ? 2 : 1>();
+    return e;
+}
+
+template <int NS, int KA, int KB, bool H>
+static cudaError_t cluster_visit_attr_one() {
+    cudaError_t e = cudaFuncSetAttribute(k_cluster_visit<NS, KA, KB, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kBottomSmemLimit);
+    return e != cudaSuccess ? e
+                            : cudaFuncSetAttribute(k_cluster_visit<NS, KA, KB, H>,
+                                                   cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+template <bool H>
+static cudaError_t cluster_visit_attr() {
+    cudaError_t e = cluster_visit_attr_one<2, 4, 1, H>();
+    e = e != cudaSuccess ? e : cluster_visit_attr_one<4, 4, 1, H>();
+    e = e != cudaSuccess ? e : cluster_visit_attr_one<8, 4, 1, H>();
+    e = e != cudaSuccess ? e : cluster_visit_attr_one<4, 2, 1, H>();
+    return e;
+}
 
 template <int N, bool DG>
 static cudaError_t conv_win_attr() {
@@ -87,6 +122,12 @@ int clb_init(int device) {
         return 1;
     const int bottom_max = (int)kBottomSmemLimit;
     cudaError_t e = cudaSuccess;
+    // the fused sweeps stage more than the default 48 KB of shared memory
+    e = e != cudaSuccess ? e : rbgs_iter_attr<true, false>();
+    e = e != cudaSuccess ? e : rbgs_iter_attr<false, false>();
+    e = e != cudaSuccess ? e : rbgs_iter_attr<false, true>();
+    e = e != cudaSuccess ? e : cluster_visit_attr<false>();
+    e = e != cudaSuccess ? e : cluster_visit_attr<true>();
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_bottom_visit<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
@@ -579,9 +620,56 @@ LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rh
     return v;
 }
 
+extern "C++" {
+// One launch of k_rbgs_iter: T iterations on big (8 x 8 x 32) or small (4 x 4 x 32) tiles.
+template <bool L0, bool H, int TI, int TJ, int T>
+static void launch_rbgs_iter(const LevelView& v, const float* in, float* out, float delta, cudaStream_t s) {
+    const dim3 grid((v.nz + 31) / 32, (v.ny + TJ - 1) / TJ, (v.nx + TI - 1) / TI);
+    launch(grid, SW_THREADS, SweepTile<L0, H, TI, TJ, 32, T>::smem(), s)(
+        k_rbgs_iter<L0, H, TI, TJ, 32, T>, in, out, v.b, L0 ? v.op0 : nullptr, L0 ? nullptr : v.opc,
+        L0 ? nullptr : v.mask, delta, v.scale, v.nx, v.ny, v.nz);
+}
+
+template <bool L0, bool H>
+static void launch_rbgs_iter(const LevelView& v, bool big, int t, const float* in, float* out, float delta,
+                             cudaStream_t s) {
+    if (big && t == 2 && (L0 || H)) launch_rbgs_iter<L0, H, 8, 8, (L0 || H) ? 2 : 1>(v, in, out, delta, s);
+    else if (t == 2) launch_rbgs_iter<L0, H, 4, 4, 2>(v, in, out, delta, s);  // FP32 coarse: no big pair tile
+    else if (big) launch_rbgs_iter<L0, H, 8, 8, 1>(v, in, out, delta, s);
+    else launch_rbgs_iter<L0, H, 4, 4, 1>(v, in, out, delta, s);
+}
+}  // extern "C++"
+
+// clb_mg_hierarchy.sweep kinds: 1 two colour launches with 16-byte row vectors (FP32 levels), 2/3 one
+// fused launch per iteration on 8x8x32 / 4x4x32 tiles, 4 two colour launches with one thread per
+// cell, 5/6 one fused launch per two iterations on 8x8x32 / 4x4x32 tiles (on FP32 coarse levels kind 5
+// runs as 6). Kinds 2, 3, 5 and 6 need the level's second buffer. All give identical values.
 int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
     const i64 C = (i64)v.nx * v.ny * v.nz;
-    if (v.half) {  // FP16 levels: one thread per cell
+    const int kind = v.sweep == 0 ? (v.half ? 4 : 1) : v.sweep;
+    if ((kind == 2 || kind == 3 || kind == 5 || kind == 6) && v.alt != nullptr && iterations > 0) {
+        // fused iterations, alternating between the level's buffer and its second buffer
+        const bool big = kind == 2 || kind == 5;
+        const int per = kind >= 5 ? 2 : 1;
+        float* cur = v.p;
+        float* other = v.alt;
+        for (int left = iterations; left > 0;) {
+            const int t = left >= per ? per : 1;
+            if (v.l0) launch_rbgs_iter<true, false>(v, big, t, cur, other, delta, s);
+            else if (v.half) launch_rbgs_iter<false, true>(v, big, t, cur, other, delta, s);
+            else launch_rbgs_iter<false, false>(v, big, t, cur, other, delta, s);
+            CLB_LAUNCH_CHECK("k_rbgs_iter");
+            float* tmp = cur;
+            cur = other;
+            other = tmp;
+            left -= t;
+        }
+        const size_t bytes = (size_t)C * (v.half ? 2 : 4);
+        if (cur != v.p && check_call(cudaMemcpyAsync(v.p, cur, bytes, cudaMemcpyDeviceToDevice, s), "smooth copy-back"))
+            return 1;
+        return 0;
+    }
+    if (v.half) {  // FP16 levels otherwise: one thread per cell
         for (int it = 0; it < iterations; ++it)
             for (int parity = 0; parity < 2; ++parity) {
                 launch(blocks_for(C, MGT), MGT, 0, s)(k_rbgs_h, reinterpret_cast<__half*>(v.p),
@@ -592,7 +680,6 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
             }
         return 0;
     }
-    const int kind = v.sweep == 0 ? 1 : v.sweep;
     if (kind == 1) {
         const bool vec4 = (v.nz % 4) == 0 && (((uintptr_t)v.p) & 15) == 0;
         const int vec = vec4 ? 4 : 1;
@@ -614,36 +701,6 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
                                               v.nx, v.ny, v.nz);
                 CLB_LAUNCH_CHECK("k_rbgs_colour");
             }
-        return 0;
-    }
-    if ((kind == 2 || kind == 3) && v.alt != nullptr && iterations > 0) {
-        // fused iterations, alternating between the level's buffer and its second buffer
-        const dim3 big((v.nz + 31) / 32, (v.ny + 7) / 8, (v.nx + 7) / 8);
-        const dim3 small((v.nz + 31) / 32, (v.ny + 3) / 4, (v.nx + 3) / 4);
-        const bool use_big = kind == 2;
-        float* cur = v.p;
-        float* other = v.alt;
-        for (int it = 0; it < iterations; ++it) {
-            if (v.l0 && use_big)
-                launch(big, SW_THREADS, 0, s)(k_rbgs_iter<true, 8, 8, 32>, cur, other, v.b, v.op0, nullptr, nullptr,
-                                              delta, v.nx, v.ny, v.nz);
-            else if (v.l0)
-                launch(small, SW_THREADS, 0, s)(k_rbgs_iter<true, 4, 4, 32>, cur, other, v.b, v.op0, nullptr, nullptr,
-                                                delta, v.nx, v.ny, v.nz);
-            else if (use_big)
-                launch(big, SW_THREADS, 0, s)(k_rbgs_iter<false, 8, 8, 32>, cur, other, v.b, nullptr, v.opc, v.mask,
-                                              delta, v.nx, v.ny, v.nz);
-            else
-                launch(small, SW_THREADS, 0, s)(k_rbgs_iter<false, 4, 4, 32>, cur, other, v.b, nullptr, v.opc, v.mask,
-                                                delta, v.nx, v.ny, v.nz);
-            CLB_LAUNCH_CHECK("k_rbgs_iter");
-            float* t = cur;
-            cur = other;
-            other = t;
-        }
-        if (cur != v.p && check_call(cudaMemcpyAsync(v.p, cur, sizeof(float) * C, cudaMemcpyDeviceToDevice, s),
-                                     "smooth copy-back"))
-            return 1;
         return 0;
     }
     for (int it = 0; it < iterations; ++it)
@@ -687,6 +744,91 @@ int coarse_solve(const LevelView& v, float delta, int iterations, cudaStream_t s
     return 0;
 }
 
+extern "C++" {
+template <int NS, int KA, int KB, bool H>
+static int launch_cluster_visit(const clb_mg_hierarchy* h, int level, int csize, size_t bytes, int pre, int post,
+                                int coarse_iters, cudaStream_t s) {
+    auto kernel = k_cluster_visit<NS, KA, KB, H>;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(csize);
+    cfg.blockDim = dim3(BOTTOM_THREADS);
+    cfg.dynamicSmemBytes = bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    // a cluster of this size and shared memory must be schedulable (checked once per shape)
+    static std::mutex mu;
+    static int cached_csize = -1, cached_ok = 0;
+    static size_t cached_bytes = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (cached_csize != csize || cached_bytes != bytes) {
+            int clusters = 0;
+            cached_ok = cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) == cudaSuccess && clusters >= 1;
+            (void)cudaGetLastError();
+            cached_csize = csize;
+            cached_bytes = bytes;
+        }
+        if (!cached_ok) return 0;
+    }
+    cfg.numAttrs = g_use_pdl ? 2 : 1;
+    const int* c = h->shape[level];
+    const int* a = h->shape[level + 1];
+    const int* b = h->shape[level + 2];
+    (void)cudaLaunchKernelEx(&cfg, kernel, h->p[level], (const float*)h->b[level], (const void*)h->op[level],
+                             (const uint8_t*)h->mask[level], c[0], c[1], c[2], h->p[level + 1],
+                             (const float4*)h->op[level + 1], (const uint8_t*)h->mask[level + 1], a[0], a[1], a[2],
+                             (const float4*)h->op[level + 2], (const uint8_t*)h->mask[level + 2], b[0], b[1], b[2],
+                             h->delta, pre, post, coarse_iters, (const float*)h->fp16_scale);
+    return check_launch("k_cluster_visit") ? -1 : 1;
+}
+}  // extern "C++"
+
+// One cluster launch for a whole visit of the third-coarsest level with its two bottom visits
+// (mg_cluster.cuh) when the three levels share their storage type and fit; returns 1 if it launched,
+// 0 if the caller must go on level by level, -1 on error.
+int cluster_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int coarse_iters, cudaStream_t s) {
+    if (!g_use_cluster || !g_use_bottom || level < 1 || level != h->levels - 3) return 0;
+    const bool half = is_half(h, level);
+    if (is_half(h, level + 1) != half || is_half(h, level + 2) != half) return 0;
+    const int* c = h->shape[level];
+    const int* a = h->shape[level + 1];
+    const int* b = h->shape[level + 2];
+    const int sa = colour_slots(a[0], a[1], a[2]), sb = colour_slots(b[0], b[1], b[2]);
+    const int ka = (sa + BOTTOM_THREADS - 1) / BOTTOM_THREADS, kb = (sb + BOTTOM_BTHREADS - 1) / BOTTOM_BTHREADS;
+    if (kb > 1 || ka > 4) return 0;
+    const int pairs = (c[0] - 1) / 2;
+    const int cs = pairs < CLUSTER_MAX - 1 ? pairs : CLUSTER_MAX - 1;
+    if (cs < 1) return 0;
+    const ClusterLayout L = cluster_layout(cs, c[0], c[1], c[2], half);
+    const size_t bottom = bottom_smem_bytes(a[0] * a[1] * a[2], b[0] * b[1] * b[2]);
+    const size_t bytes = L.slab_bytes > bottom ? L.slab_bytes : bottom;
+    if (bytes > kBottomSmemLimit) return 0;
+    const long long slots = (long long)L.own_max * (c[1] - 2) * ((c[2] - 1) / 2);
+    const int ns = (int)((slots + BOTTOM_THREADS - 1) / BOTTOM_THREADS);
+#define CLB_CLUSTER(NS, KA, H) launch_cluster_visit<NS, KA, 1, H>(h, level, cs + 1, bytes, pre, post, coarse_iters, s)
+#define CLB_CLUSTER_KINDS(H)                                  \
+    if (ka <= 2 && ns <= 4) return CLB_CLUSTER(4, 2, H);      \
+    if (ns <= 2) return CLB_CLUSTER(2, 4, H);                 \
+    if (ns <= 4) return CLB_CLUSTER(4, 4, H);                 \
+    if (ns <= 8) return CLB_CLUSTER(8, 4, H);                 \
+    return 0;
+    if (half) {
+        CLB_CLUSTER_KINDS(true)
+    } else {
+        CLB_CLUSTER_KINDS(false)
+    }
+#undef CLB_CLUSTER_KINDS
+#undef CLB_CLUSTER
+}
+
 // One launch for a whole visit of the second-coarsest level when both bottom levels fit in shared
 // memory (mg_bottom.cuh); returns 1 if it launched, 0 if the caller must recurse, -1 on error.
 int bottom_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int coarse_iters, cudaStream_t s) {
@@ -727,6 +869,8 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
             cudaStream_t s) {
     const LevelView v = level_view(h, level, x, rhs);
     if (level == h->levels - 1) return coarse_solve(v, h->delta, pre + coarse_iters, s);
+    const int cluster = cluster_visit(h, level, pre, post, coarse_iters, s);
+    if (cluster != 0) return cluster < 0 ? 1 : 0;
     const int bottom = bottom_visit(h, level, pre, post, coarse_iters, s);
     if (bottom != 0) return bottom < 0 ? 1 : 0;
     if (smooth(v, h->delta, pre, s)) return 1;
@@ -801,9 +945,10 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
 }
 
 int clb_mg_set_option(int option, int value) {
-    CLB_REQUIRE(option == 0 || option == 1, "mg_set_option: unknown option %d", option);
+    CLB_REQUIRE(option >= 0 && option <= 2, "mg_set_option: unknown option %d", option);
     if (option == 0) g_use_bottom = value != 0;
-    else g_use_pdl = value != 0;
+    else if (option == 1) g_use_pdl = value != 0;
+    else g_use_cluster = value != 0;
     return 0;
 }
 

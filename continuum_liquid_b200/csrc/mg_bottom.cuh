@@ -85,39 +85,40 @@ constexpr int BOTTOM_BTHREADS = 256;
 
 __device__ __forceinline__ void bar_b() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
-// H = true: both levels are stored in FP16 (p, b and operator as __half, scaled values); the visit
-// computes in FP32 in shared memory with kappa = scale[2] in place of delta^2 (mg_half.cuh).
-// KA: A slots of each colour per thread (of BOTTOM_THREADS); KB: B slots of each colour per B thread.
-template <int KA, int KB, bool H = false>
-__device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const float* __restrict__ ba,
-                                                   const float4* __restrict__ opa, const uint8_t* __restrict__ ma,
-                                                   int anx, int any, int anz, float* __restrict__ pb,
-                                                   float* __restrict__ bb, const float4* __restrict__ opb,
-                                                   const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
-                                                   float delta, int pre, int post, int coarse_iters,
-                                                   const float* __restrict__ scale) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int CA = anx * any * anz, CB = bnx * bny * bnz;
+// Shared-memory arrays of a bottom visit: A's p, b and operator (float4, diagonal -1 where not
+// fluid), B's p and operator; each region padded to 16 bytes (bottom_smem_bytes).
+struct BottomSmem {
+    float* spa;
+    float* sba;
+    float4* soa;
+    float* spb;
+    float4* sob;
+};
+
+__device__ __forceinline__ BottomSmem bottom_smem(unsigned char* base, int CA, int CB) {
     auto pad = [](int x) { return (x + 3) & ~3; };  // in floats
-    float* spa = reinterpret_cast<float*>(smem);
-    float* sba = spa + pad(CA);
-    float4* soa = reinterpret_cast<float4*>(sba + pad(CA));
-    float* spb = reinterpret_cast<float*>(soa + CA);
-    float4* sob = reinterpret_cast<float4*>(spb + pad(CB));
-    const float d2 = H ? scale[2] : delta * delta;
-    const float inv_delta2 = H ? scale[3] : 1.0f / (delta * delta);
+    BottomSmem S;
+    S.spa = reinterpret_cast<float*>(base);
+    S.sba = S.spa + pad(CA);
+    S.soa = reinterpret_cast<float4*>(S.sba + pad(CA));
+    S.spb = reinterpret_cast<float*>(S.soa + CA);
+    S.sob = reinterpret_cast<float4*>(S.spb + pad(CB));
+    return S;
+}
+
+// Staging of the operators of both levels and, when pa / ba are given, of A's p and b (FP16 levels
+// are converted to FP32). Four cells per thread and round, all loads issued before the stores.
+template <bool H>
+__device__ __forceinline__ void bottom_stage(const BottomSmem& S, const float* __restrict__ pa,
+                                             const float* __restrict__ ba, const float4* __restrict__ opa,
+                                             const uint8_t* __restrict__ ma, int CA, const float4* __restrict__ opb,
+                                             const uint8_t* __restrict__ mb, int CB) {
     auto ld = [&](const float* a, int c) -> float {
         return H ? ldh(reinterpret_cast<const __half*>(a), c) : a[c];
     };
     auto ld4 = [&](const float4* a, int c) -> float4 {
         return H ? ld_h4(reinterpret_cast<const Half4*>(a), c) : a[c];
     };
-    auto st = [&](float* a, int c, float v) {
-        if (H) reinterpret_cast<__half*>(a)[c] = __float2half_rn(v);
-        else a[c] = v;
-    };
-
-    // staging: four cells per thread and round, all loads issued before the shared-memory stores
     constexpr int U = 4;
     for (int c0 = threadIdx.x; c0 < CA; c0 += U * BOTTOM_THREADS) {
         float pv[U], bv[U];
@@ -127,8 +128,8 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
         for (int u = 0; u < U; ++u) {
             const int c = c0 + u * BOTTOM_THREADS;
             if (c < CA) {
-                pv[u] = ld(pa, c);
-                bv[u] = ld(ba, c);
+                pv[u] = pa ? ld(pa, c) : 0.0f;
+                bv[u] = ba ? ld(ba, c) : 0.0f;
                 ov[u] = ld4(opa, c);
                 mv[u] = ma[c];
             }
@@ -137,11 +138,11 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
         for (int u = 0; u < U; ++u) {
             const int c = c0 + u * BOTTOM_THREADS;
             if (c < CA) {
-                spa[c] = pv[u];
-                sba[c] = bv[u];
+                if (pa) S.spa[c] = pv[u];
+                if (ba) S.sba[c] = bv[u];
                 float4 o = ov[u];
                 if (!mv[u]) o.x = -1.0f;
-                soa[c] = o;
+                S.soa[c] = o;
             }
         }
     }
@@ -162,12 +163,32 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
             if (c < CB) {
                 float4 o = ov[u];
                 if (!mv[u]) o.x = -1.0f;
-                sob[c] = o;
-                spb[c] = 0.0f;  // restriction zeroes the coarse pressure (multigrid.cl:114)
+                S.sob[c] = o;
             }
         }
     }
-    __syncthreads();
+}
+
+// One visit of A from staged shared memory: pre-smoothing of
+// A, restriction into B (B's p zeroed, multigrid.cl:114), the two coarse solves of B, prolongation,
+// post-smoothing of A. bb (nullable): B's right-hand side is stored there (FP16 when H). KA: A slots of
+// each colour per thread (of BOTTOM_THREADS); KB: B slots of each colour per B thread.
+template <int KA, int KB, bool H>
+__device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int any, int anz, int bnx, int bny, int bnz,
+                                            float d2, float inv_delta2, int pre, int post, int coarse_iters,
+                                            float* __restrict__ bb) {
+    float* spa = S.spa;
+    const float* sba = S.sba;
+    const float4* soa = S.soa;
+    float* spb = S.spb;
+    const float4* sob = S.sob;
+    const int CB = bnx * bny * bnz;
+    auto st = [&](float* a, int c, float v) {
+        if (H) reinterpret_cast<__half*>(a)[c] = __float2half_rn(v);
+        else a[c] = v;
+    };
+    __syncthreads();  // staging and the caller's writes to shared memory are complete
+    for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) spb[c] = 0.0f;  // multigrid.cl:114
 
     const int asx = any * anz, asy = anz, bsx = bny * bnz, bsy = bnz;
     OwnedCell A[2][KA];  // [colour][m]
@@ -217,6 +238,7 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
             }
     };
 
+    __syncthreads();
     smooth_a(pre);
     // restriction of the residual (multigrid.cl:90-180, right-hand-side part) into B's owners
     float bvals[2][KB];
@@ -273,19 +295,44 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
         }
     __syncthreads();
     smooth_a(post);
+    if (bb) {
+#pragma unroll
+        for (int colour = 0; colour < 2; ++colour)
+#pragma unroll
+            for (int m = 0; m < KB; ++m)
+                if (btile && colour_cell(threadIdx.x + m * BOTTOM_BTHREADS, colour, bnx, bny, bnz) >= 0)
+                    st(bb, B[colour][m].c, bvals[colour][m]);
+    }
+}
 
-    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) st(pa, c, spa[c]);
+// H = true: both levels are stored in FP16 (p, b and operator as __half, scaled values); the visit
+// computes in FP32 in shared memory with kappa = scale[2] in place of delta^2 (mg_half.cuh).
+template <int KA, int KB, bool H = false>
+__device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const float* __restrict__ ba,
+                                                   const float4* __restrict__ opa, const uint8_t* __restrict__ ma,
+                                                   int anx, int any, int anz, float* __restrict__ pb,
+                                                   float* __restrict__ bb, const float4* __restrict__ opb,
+                                                   const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
+                                                   float delta, int pre, int post, int coarse_iters,
+                                                   const float* __restrict__ scale) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int CA = anx * any * anz, CB = bnx * bny * bnz;
+    const BottomSmem S = bottom_smem(smem, CA, CB);
+    const float d2 = H ? scale[2] : delta * delta;
+    const float inv_delta2 = H ? scale[3] : 1.0f / (delta * delta);
+    auto st = [&](float* a, int c, float v) {
+        if (H) reinterpret_cast<__half*>(a)[c] = __float2half_rn(v);
+        else a[c] = v;
+    };
+    bottom_stage<H>(S, pa, ba, opa, ma, CA, opb, mb, CB);
+    bottom_core<KA, KB, H>(S, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, bb);
+    const int bsx = bny * bnz, bsy = bnz;
+    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) st(pa, c, S.spa[c]);
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
-        st(pb, c, spb[c]);
+        st(pb, c, S.spb[c]);
         const int I = c / bsx, J = (c / bsy) % bny, K = c % bnz;
         if (!interior(I, J, K, bnx, bny, bnz)) st(bb, c, 0.0f);  // multigrid.cl:115
     }
-#pragma unroll
-    for (int colour = 0; colour < 2; ++colour)
-#pragma unroll
-        for (int m = 0; m < KB; ++m)
-            if (btile && colour_cell(threadIdx.x + m * BOTTOM_BTHREADS, colour, bnx, bny, bnz) >= 0)
-                st(bb, B[colour][m].c, bvals[colour][m]);
 }
 
 template <int KA, int KB, bool H = false>

@@ -55,11 +55,14 @@ __global__ void __launch_bounds__(MGT) k_rbgs_h(__half* p, const __half* __restr
         if (!fluid) p[c] = __float2half_rn(0.0f);
         return;
     }
+    // a fluid cell of the colour: the operator, neighbour weights, neighbours and b in one round trip
     const float4 o = ld_h4(op, c);
+    const float wxm = ld_h4(op, c - sx).y, wym = ld_h4(op, c - sy).z, wzm = ld_h4(op, c - 1).w;
+    const float pxp = ldh(p, c + sx), pxm = ldh(p, c - sx), pyp = ldh(p, c + sy), pym = ldh(p, c - sy);
+    const float pzp = ldh(p, c + 1), pzm = ldh(p, c - 1), bc = ldh(b, c), kappa = scale[2];
     if (!(o.x > 0.0f)) return;
-    const float ws = o.y * ldh(p, c + sx) + ld_h4(op, c - sx).y * ldh(p, c - sx) + o.z * ldh(p, c + sy) +
-                     ld_h4(op, c - sy).z * ldh(p, c - sy) + o.w * ldh(p, c + 1) + ld_h4(op, c - 1).w * ldh(p, c - 1);
-    p[c] = __float2half_rn((ws - scale[2] * ldh(b, c)) / o.x);
+    const float ws = o.y * pxp + wxm * pxm + o.z * pyp + wym * pym + o.w * pzp + wzm * pzm;
+    p[c] = __float2half_rn((ws - kappa * bc) / o.x);
 }
 
 // Residual at an FP16 fine cell in scaled units: b_s - (sum w p_s - diag p_s) / kappa.

@@ -351,8 +351,13 @@ __device__ __forceinline__ void rbgs_at(i64 c, float* p, const float* __restrict
             if (!fluid) p[c] = 0.0f;
             return;
         }
+        // a fluid cell of the colour: the operator, neighbour weights, neighbours and b in one round trip
         const float4 o = __ldg(opc + c);
-        if (o.x > 0.0f) p[c] = (wsumC(opc, p, c, sx, sy, o) - d2 * __ldg(b + c)) / o.x;
+        const float wxm = __ldg(opc + c - sx).y, wym = __ldg(opc + c - sy).z, wzm = __ldg(opc + c - 1).w;
+        const float pxp = p[c + sx], pxm = p[c - sx], pyp = p[c + sy], pym = p[c - sy], pzp = p[c + 1], pzm = p[c - 1];
+        const float bc = __ldg(b + c);
+        const float ws = o.y * pxp + wxm * pxm + o.z * pyp + wym * pym + o.w * pzp + wzm * pzm;
+        if (o.x > 0.0f) p[c] = (ws - d2 * bc) / o.x;
     }
 }
 

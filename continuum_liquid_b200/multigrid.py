@@ -125,7 +125,7 @@ class MultigridHierarchy:
     (p, b and op as float16, scaled as described in csrc/mg_half.cuh; no counterpart in the
     reference), provided at least the two coarsest levels qualify. A W-cycle then needs
     ``norms[0]`` to hold the squared norm of its right-hand side (the residual kernels leave it
-    there), and those levels use per-cell sweeps.
+    there), and those levels use the per-cell or the fused sweep kinds (not the row-vector kind 1).
     """
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, fused_min_cells: int = 20**3,
@@ -173,8 +173,9 @@ class MultigridHierarchy:
         # cells (smaller levels are served by the single-block bottom visit or two-launch sweeps)
         self.alt: list[torch.Tensor | None] = []
         for l, shape in enumerate(self.shapes):
-            big = int(np.prod(shape)) >= fused_min_cells and not self.is_fp16(l)
-            self.alt.append(torch.zeros(shape, dtype=torch.float32, device=device) if big else None)
+            big = int(np.prod(shape)) >= fused_min_cells
+            dt = torch.float16 if self.is_fp16(l) else torch.float32
+            self.alt.append(torch.zeros(shape, dtype=dt, device=device) if big else None)
             if big:
                 self.struct.alt[l] = self.alt[l].data_ptr()
         self.tuning: dict | None = None  # per-level sweep timings from the autotuner (ms per iteration)
@@ -218,11 +219,14 @@ class MultigridHierarchy:
                                     int(coarse_iterations), stream=queue)
 
     def set_sweep(self, level: int, kind: int) -> None:
-        """Red-black sweep implementation of one level (see clb_mg_hierarchy.sweep); FP16 levels
-        always use kind 4."""
-        if self.is_fp16(level) and int(kind) not in (0, 4):
-            raise ValueError(f"level {level} is stored in FP16 and uses sweep kind 4")
-        self.struct.sweep[level] = 4 if self.is_fp16(level) else int(kind)
+        """Red-black sweep implementation of one level (see clb_mg_hierarchy.sweep); FP16 levels take
+        kinds 2-6 (0 means 4)."""
+        kind = int(kind)
+        if kind not in (0, 1, 2, 3, 4, 5, 6):
+            raise ValueError(f"unknown sweep kind {kind}")
+        if self.is_fp16(level) and kind == 1:
+            raise ValueError(f"level {level} is stored in FP16: sweep kinds 2-6")
+        self.struct.sweep[level] = 4 if self.is_fp16(level) and kind == 0 else kind
 
     def sweeps(self) -> list[int]:
         return [int(self.struct.sweep[l]) for l in range(self.levels)]

@@ -189,7 +189,8 @@ int clb_coarse_smooth(float* p, const float* b, const float* mask, const float* 
  * Coarse levels l >= 1 hold p, b (float32), a mask byte and a float4 (diagonal, wx, wy, wz).
  * Levels l >= fp16_level (when fp16_level > 0; no counterpart in the reference) store p and b as
  * IEEE half and the operator as four halves (8 bytes), with p and b scaled by powers of two taken
- * from rhs_norms (see clb_mg_w_cycle); such levels use sweep kind 4 and need fp16_scale. */
+ * from rhs_norms (see clb_mg_w_cycle); such levels use sweep kinds 2-6 (0 and 1 mean 4), an alt
+ * buffer of halves, and need fp16_scale. */
 typedef struct clb_mg_hierarchy {
     int32_t levels;                      /* including level 0 */
     int32_t shape[CLB_MG_MAX_LEVELS][3]; /* nx, ny, nz per level (ghost layer included) */
@@ -200,14 +201,18 @@ typedef struct clb_mg_hierarchy {
     float* b[CLB_MG_MAX_LEVELS];         /* [0] unused: level-0 rhs is passed per call */
     uint8_t* mask[CLB_MG_MAX_LEVELS];    /* [0] unused */
     void* op[CLB_MG_MAX_LEVELS];         /* [0] unused; float4 per cell */
-    float* alt[CLB_MG_MAX_LEVELS];       /* optional second buffer per level (level 0 included), used
-                                            by the fused sweep kinds */
+    float* alt[CLB_MG_MAX_LEVELS];       /* optional second buffer per level (level 0 included, the
+                                            level's element type), used by the fused sweep kinds */
     int32_t sweep[CLB_MG_MAX_LEVELS];    /* red-black sweep implementation per level:
                                             0 = default (two colour launches),
                                             1 = two colour launches, 16-byte row vectors when nz % 4 == 0,
                                             2 = one fused launch per iteration, 8x8x32 tiles (needs alt),
                                             3 = one fused launch per iteration, 4x4x32 tiles (needs alt),
-                                            4 = two colour launches, one thread per cell.
+                                            4 = two colour launches, one thread per cell,
+                                            5 = one fused launch per two iterations, 8x8x32 tiles
+                                                (needs alt; on FP32 coarse levels it runs as 6),
+                                            6 = one fused launch per two iterations, 4x4x32 tiles
+                                                (needs alt).
                                             All kinds give identical values. */
     float* fp16_scale;                   /* device float[4] written by clb_mg_w_cycle: sigma_b,
                                             1/sigma_p, kappa, 1/kappa (FP16 levels only) */
@@ -241,7 +246,11 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
  *            reference does. Both give identical results.
  *  option 1: 1 (default) launches the pressure-solve kernels with programmatic dependent launch (a
  *            kernel's blocks are scheduled while its predecessor drains and wait for its completion
- *            on the device); 0 launches them with ordinary stream serialisation. Identical results. */
+ *            on the device); 0 launches them with ordinary stream serialisation. Identical results.
+ *  option 2: 1 (default) runs each visit of the third-coarsest level, with its two bottom visits, as
+ *            one launch of a thread-block cluster (up to 16 CTAs, distributed shared memory) when the
+ *            three levels share their storage type and fit; 0 goes level by level. Identical
+ *            results. */
 int clb_mg_set_option(int option, int value);
 
 /* Block-partial count used by clb_mg_residual_norms for a grid of `cells` cells. */

@@ -102,3 +102,60 @@ def test_full_steps_with_fp16_coarse_levels(backend):
             assert sim.pressure_solver.hierarchy.fp16_level > 0
     assert totals[True] <= totals[False] + 5, totals
     assert backend.device_error() == 0
+
+
+@pytest.mark.parametrize("kind", [2, 3, 5, 6])
+def test_fp16_fused_sweeps_equal_per_cell_sweeps(backend, kind):
+    """The fused FP16 sweep kinds round every update to FP16 as the per-cell kind stores it: the same
+    values on every FP16 level, for odd and even iteration counts."""
+    shape = (80, 70, 60)
+    dx = 1.0 / 80
+    ff, vel = liquid_system(shape, 11)
+    rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    h = multigrid.MultigridHierarchy(backend, shape, dx, fp16_max_size=64, fused_min_cells=1)
+    h.rhs_operator(vel, ff, rhs, 1.0 / 240.0, 1000.0)
+    h.build_coarse()
+    h.residual_norms(torch.zeros_like(rhs), rhs)
+    e = torch.zeros_like(rhs)
+    h.w_cycle(e, rhs)  # fills every level's p and b with scaled FP16 values
+    levels = [l for l in range(1, h.levels - 1) if h.is_fp16(l)]
+    assert levels
+    for level in levels:
+        start_p = h.p[level].clone()
+        for iterations in (1, 2, 3):
+            results = {}
+            for k in (4, kind):
+                h.set_sweep(level, k)
+                h.p[level].copy_(start_p)
+                h.smooth(level, iterations)
+                results[k] = h.p[level].clone()
+            assert torch.equal(results[4], results[kind]), (level, iterations)
+            assert results[4].abs().max() > 0
+    assert backend.device_error() == 0
+
+
+@pytest.mark.parametrize("shape", [(130, 130, 130), (134, 120, 125)])
+def test_fp16_cluster_visit_equals_level_by_level(backend, shape):
+    """With FP16 storage the cluster visit of the third-coarsest level (and its bottom visits) rounds
+    exactly where the level-by-level kernels store FP16: W-cycles agree bit for bit."""
+    dx = 1.0 / shape[0]
+    ff, vel = liquid_system(shape, 13)
+    rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    h = multigrid.MultigridHierarchy(backend, shape, dx, fp16_max_size=64)
+    assert h.fp16_level == h.levels - 3
+    h.rhs_operator(vel, ff, rhs, 1.0 / 240.0, 1000.0)
+    h.build_coarse()
+    h.residual_norms(torch.zeros_like(rhs), rhs)
+    out = {}
+    try:
+        for cluster in (0, 1):
+            backend.lib.clb_mg_set_option(2, cluster)
+            e = torch.zeros_like(rhs)
+            for _ in range(2):
+                h.w_cycle(e, rhs)
+            out[cluster] = e
+    finally:
+        backend.lib.clb_mg_set_option(2, 1)
+    assert torch.equal(out[0], out[1])
+    assert out[1].abs().max() > 0
+    assert backend.device_error() == 0

@@ -494,16 +494,18 @@ def test_bad_arguments_raise(backend):
         backend.call("clb_rbgs_step", t, t, t, t, t, t, t, 1.0, 3, 4, 4, 4)
 
 
+@pytest.mark.parametrize("cluster", [1, 0])
 @pytest.mark.parametrize("pdl", [1, 0])
 @pytest.mark.parametrize("bottom", [1, 0])
-@pytest.mark.parametrize("shape", [(66, 66, 66), (34, 40, 30)])
-def test_w_cycle_paths_agree(backend, oracle, shape, bottom, pdl):
-    """The single-block bottom visit and the fused red-black iterations give the reference values,
-    with and without programmatic dependent launch."""
+@pytest.mark.parametrize("shape", [(66, 66, 66), (34, 40, 30), (70, 66, 61)])
+def test_w_cycle_paths_agree(backend, oracle, shape, bottom, pdl, cluster):
+    """The cluster visit, the single-block bottom visit and the fused red-black iterations give the
+    reference values, with and without programmatic dependent launch."""
     dx = F32(1.0 / shape[0])
     ff, b, p0 = random_system(shape, 21)
     backend.lib.clb_mg_set_option(0, bottom)
     backend.lib.clb_mg_set_option(1, pdl)
+    backend.lib.clb_mg_set_option(2, cluster)
     try:
         h = multigrid.MultigridHierarchy(backend, shape, float(dx))
         h.op0.copy_(torch.zeros_like(h.op0))
@@ -521,6 +523,7 @@ def test_w_cycle_paths_agree(backend, oracle, shape, bottom, pdl):
     finally:
         backend.lib.clb_mg_set_option(0, 1)
         backend.lib.clb_mg_set_option(1, 1)
+        backend.lib.clb_mg_set_option(2, 1)
 
 
 def test_programmatic_launch_changes_nothing(backend):
@@ -568,7 +571,7 @@ def test_fused_smoothing_odd_iterations(backend, oracle, iterations):
     assert np.array_equal(host(P), q)
 
 
-@pytest.mark.parametrize("kind", [1, 2, 3, 4])
+@pytest.mark.parametrize("kind", [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("shape", [(40, 36, 44), (33, 33, 33)])
 def test_every_sweep_kind_matches_oracle(backend, oracle, shape, kind):
     dx = F32(1.0 / shape[0])
