@@ -85,6 +85,7 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_smooth": [P, I, P, P, I, P],
     "clb_mg_set_option": [I, I],
     "clb_mg_residual_partials": [L],
+    "clb_mg_tile_capacity": [I, I, I, I],
     "clb_mg_residual_norms": [P, I, P, P, F, I, I, I, P, P, P, P],
     "clb_mg_ir_init": [P, P, P, I, I, I, P],
     "clb_mg_ir_step": [P, P, P, P, P, F, I, I, I, P, P, P, P],
@@ -116,6 +117,7 @@ _RESTYPES = {
     "clb_last_error": ctypes.c_char_p,
     "clb_scan_scratch_bytes": ctypes.c_int64,
     "clb_launch_count": ctypes.c_int64,
+    "clb_mg_tile_capacity": ctypes.c_int64,
 }
 
 
@@ -137,6 +139,9 @@ class MGHierarchy(ctypes.Structure):
         ("fp16_scale", ctypes.c_void_p),
         ("rhs_norms", ctypes.c_void_p),
         ("fp16_inexact", ctypes.c_void_p),
+        ("tiles", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("tile_counts", ctypes.c_void_p),
+        ("zero_outside", ctypes.c_int32),
     ]
 
 

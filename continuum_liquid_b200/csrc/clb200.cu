@@ -9,6 +9,7 @@
 #include "mg_sweep.cuh"
 #include "mg_half.cuh"
 #include "mg_cluster.cuh"
+#include "mg_tiles.cuh"
 #include "batch.cuh"
 #include "sources.cuh"
 #include "voxelise.cuh"
@@ -26,7 +27,7 @@ using namespace clb;
                 (nz));                                                                                 \
     CLB_REQUIRE((i64)(nx) * (ny) * (nz) < (1ll << 31), "grid %dx%dx%d has more than 2^31 cells", (nx), (ny), (nz))
 
-static const int kAbiVersion = 7;
+static const int kAbiVersion = 8;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 static bool g_use_cluster = true;  // clb_mg_set_option(2, ...) switches the cluster visit off
@@ -582,8 +583,35 @@ int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream) {
         else CLB_COARSE_OP(2, true);
 #undef CLB_COARSE_OP
         CLB_LAUNCH_CHECK("k_coarse_operator");
+        // coarse p and b start at 0: cells without fluid keep it for the whole solve (mg_tiles.cuh)
+        const size_t bytes = (size_t)C * (ch ? 2 : 4);
+        if (check_call(cudaMemsetAsync(h->p[l], 0, bytes, s), "coarse p") ||
+            check_call(cudaMemsetAsync(h->b[l], 0, bytes, s), "coarse b"))
+            return 1;
+    }
+    if (h->tile_counts) {
+        if (check_call(cudaMemsetAsync(h->tile_counts, 0, sizeof(int32_t) * CLB_MG_MAX_LEVELS, s), "tile counts"))
+            return 1;
+        for (int l = 0; l < h->levels; ++l) {
+            if (!h->tiles[l]) continue;
+            const int* n = h->shape[l];
+            const i64 tiles = tile_capacity(n[0], n[1], n[2], l == 0);
+            const unsigned grid = blocks_for(tiles * 32, 256);
+            if (l == 0)
+                launch(grid, 256, 0, s)(k_mg_tiles<true>, (const uint8_t*)h->op0, n[0], n[1], n[2], h->tiles[l],
+                                        h->tile_counts + l);
+            else
+                launch(grid, 256, 0, s)(k_mg_tiles<false>, (const uint8_t*)h->mask[l], n[0], n[1], n[2], h->tiles[l],
+                                        h->tile_counts + l);
+            CLB_LAUNCH_CHECK("k_mg_tiles");
+        }
     }
     return 0;
+}
+
+int64_t clb_mg_tile_capacity(int nx, int ny, int nz, int finest) {
+    if (nx <= 0 || ny <= 0 || nz <= 0) return 0;
+    return tile_capacity(nx, ny, nz, finest != 0);
 }
 
 namespace {
@@ -600,6 +628,8 @@ struct LevelView {
     bool l0;
     bool half;            // FP16 storage (p, b as __half, opc as Half4)
     const float* scale;   // FP16 scales (mg_half.cuh)
+    const int* tiles;     // fluid tiles (mg_tiles.cuh) or null
+    const int* tile_count;
 };
 
 LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rhs) {
@@ -617,7 +647,16 @@ LevelView level_view(const clb_mg_hierarchy* h, int l, float* x, const float* rh
     v.nx = h->shape[l][0];
     v.ny = h->shape[l][1];
     v.nz = h->shape[l][2];
+    v.tiles = h->tile_counts ? h->tiles[l] : nullptr;
+    v.tile_count = h->tile_counts ? h->tile_counts + l : nullptr;
     return v;
+}
+
+// Blocks of the tile-list kernels: enough to fill the GPU, never more than there are tiles.
+static unsigned tile_grid(const LevelView& v) {
+    const i64 cap = tile_capacity(v.nx, v.ny, v.nz, v.l0);
+    const i64 most = (i64)(g_sm_count > 0 ? g_sm_count : 148) * 16;
+    return (unsigned)(cap < most ? (cap > 0 ? cap : 1) : most);
 }
 
 extern "C++" {
@@ -644,9 +683,30 @@ static void launch_rbgs_iter(const LevelView& v, bool big, int t, const float* i
 // fused launch per iteration on 8x8x32 / 4x4x32 tiles, 4 two colour launches with one thread per
 // cell, 5/6 one fused launch per two iterations on 8x8x32 / 4x4x32 tiles (on FP32 coarse levels kind 5
 // runs as 6). Kinds 2, 3, 5 and 6 need the level's second buffer. All give identical values.
-int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s) {
+// sparse: every cell without fluid holds 0 (inside a W-cycle, mg_tiles.cuh), so an FP32 level with a
+// tile list is swept on its fluid tiles only.
+int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s, bool sparse = false) {
     const i64 C = (i64)v.nx * v.ny * v.nz;
     const int kind = v.sweep == 0 ? (v.half ? 4 : 1) : v.sweep;
+    const int vec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
+    if (sparse && v.tiles && !v.half && (vec == 1 || (((uintptr_t)v.p) & 15) == 0)) {
+        const unsigned grid = tile_grid(v);
+        const dim3 block(32, 4);
+        for (int it = 0; it < iterations; ++it)
+            for (int parity = 0; parity < 2; ++parity) {
+                if (v.l0 && vec == 4)
+                    launch(grid, block, 0, s)(k_rbgs_colour_tiles<true, 4>, v.tiles, v.tile_count, v.p, v.b, v.op0,
+                                              nullptr, nullptr, delta, parity, v.nx, v.ny, v.nz);
+                else if (v.l0)
+                    launch(grid, block, 0, s)(k_rbgs_colour_tiles<true, 1>, v.tiles, v.tile_count, v.p, v.b, v.op0,
+                                              nullptr, nullptr, delta, parity, v.nx, v.ny, v.nz);
+                else
+                    launch(grid, block, 0, s)(k_rbgs_colour_tiles<false, 1>, v.tiles, v.tile_count, v.p, v.b,
+                                              nullptr, v.opc, v.mask, delta, parity, v.nx, v.ny, v.nz);
+                CLB_LAUNCH_CHECK("k_rbgs_colour_tiles");
+            }
+        return 0;
+    }
     if ((kind == 2 || kind == 3 || kind == 5 || kind == 6) && v.alt != nullptr && iterations > 0) {
         // fused iterations, alternating between the level's buffer and its second buffer
         const bool big = kind == 2 || kind == 5;
@@ -873,10 +933,22 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
     if (cluster != 0) return cluster < 0 ? 1 : 0;
     const int bottom = bottom_visit(h, level, pre, post, coarse_iters, s);
     if (bottom != 0) return bottom < 0 ? 1 : 0;
-    if (smooth(v, h->delta, pre, s)) return 1;
+    // coarse levels hold 0 outside the fluid (zeroed by clb_mg_build_coarse and the restriction);
+    // level 0 does when the caller says so
+    const bool sparse = level > 0 || h->zero_outside != 0;
+    if (smooth(v, h->delta, pre, s, sparse)) return 1;
     const LevelView c = level_view(h, level + 1, x, rhs);
     const i64 Cc = (i64)c.nx * c.ny * c.nz;
-    if (c.half) {
+    if (!c.half && !v.half && c.tiles) {  // restriction of the coarse fluid tiles (inactive cells hold 0)
+        if (v.l0)
+            launch(tile_grid(c), dim3(32, 4), 0, s)(k_restrict_tiles<true>, c.tiles, c.tile_count, v.p, v.b, v.op0,
+                                                    nullptr, nullptr, c.p, const_cast<float*>(c.b), h->delta, v.nx,
+                                                    v.ny, v.nz, c.nx, c.ny, c.nz);
+        else
+            launch(tile_grid(c), dim3(32, 4), 0, s)(k_restrict_tiles<false>, c.tiles, c.tile_count, v.p, v.b,
+                                                    nullptr, v.opc, v.mask, c.p, const_cast<float*>(c.b), h->delta,
+                                                    v.nx, v.ny, v.nz, c.nx, c.ny, c.nz);
+    } else if (c.half) {
         const dim3 grid = blocks_for(Cc, MGT);
 #define CLB_RESTRICT_H(FS)                                                                                        \
     launch(grid, MGT, 0, s)(k_restrict_h<FS>, v.p, v.b, v.op0, v.opc, v.mask, reinterpret_cast<__half*>(c.p),          \
@@ -898,7 +970,18 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
     if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     const i64 Cf = (i64)v.nx * v.ny * v.nz;
-    if (c.half) {
+    const int fvec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
+    if (!c.half && !v.half && v.tiles) {  // prolongation into the fine fluid tiles
+        if (v.l0 && fvec == 4)
+            launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<true, 4>, v.tiles, v.tile_count, c.p, v.p, v.op0,
+                                                    nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
+        else if (v.l0)
+            launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<true, 1>, v.tiles, v.tile_count, c.p, v.p, v.op0,
+                                                    nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
+        else
+            launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<false, 1>, v.tiles, v.tile_count, c.p, v.p,
+                                                    nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
+    } else if (c.half) {
         const dim3 grid = blocks_for(Cf, MGT);
         const __half* ce = reinterpret_cast<const __half*>(c.p);
         if (v.half)
@@ -917,7 +1000,7 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
         launch(blocks_for(Cf, MGT), MGT, 0, s)(k_prolong<false>, c.p, v.p, nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny,
                                                v.nz);
     CLB_LAUNCH_CHECK("k_prolong");
-    return smooth(v, h->delta, post, s);
+    return smooth(v, h->delta, post, s, sparse);
 }
 
 }  // namespace

@@ -129,7 +129,7 @@ class MultigridHierarchy:
     """
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, fused_min_cells: int = 20**3,
-                 fp16_max_size: int = 0):
+                 fp16_max_size: int = 0, fluid_tiles: bool = True):
         self.kernels = kernels
         self.grid_shape = tuple(int(s) for s in grid_shape)
         self.dx = float(dx)
@@ -186,6 +186,16 @@ class MultigridHierarchy:
         self.struct.fp16_scale = self.fp16_scale.data_ptr()
         self.struct.rhs_norms = self.norms.data_ptr()
         self.struct.fp16_inexact = self.fp16_inexact.data_ptr()
+        # fluid tiles per level (csrc/mg_tiles.cuh): inside a W-cycle the FP32 levels' sweeps,
+        # restrictions and prolongations visit only the tiles that hold fluid
+        self.tiles: list[torch.Tensor] = []
+        self.tile_counts = torch.zeros(MG_MAX_LEVELS, dtype=torch.int32, device=device)
+        if fluid_tiles:
+            for l, shape in enumerate(self.shapes):
+                cap = int(kernels.lib.clb_mg_tile_capacity(*shape, 1 if l == 0 else 0))
+                self.tiles.append(torch.zeros(max(cap, 1), dtype=torch.int32, device=device))
+                self.struct.tiles[l] = self.tiles[l].data_ptr()
+            self.struct.tile_counts = self.tile_counts.data_ptr()
         for l in range(1, levels):
             if self.is_fp16(l):
                 self.struct.sweep[l] = 4
@@ -213,8 +223,11 @@ class MultigridHierarchy:
         self.kernels.call_hierarchy("clb_mg_build_coarse", self.struct, stream=queue)
 
     def w_cycle(self, x, rhs, pre_smooth=PRE_SMOOTH, post_smooth=POST_SMOOTH,
-                coarse_iterations=COARSE_SMOOTH_ITERATIONS, queue=None) -> None:
-        """One W-cycle on level-0 unknown ``x`` and right-hand side ``rhs``."""
+                coarse_iterations=COARSE_SMOOTH_ITERATIONS, queue=None, x_zero_outside: bool = False) -> None:
+        """One W-cycle on level-0 unknown ``x`` and right-hand side ``rhs``. ``x_zero_outside``: the
+        caller guarantees that ``x`` is 0 at every cell that is not fluid (a zeroed correction), so the
+        level-0 sweeps may skip the tiles without fluid."""
+        self.struct.zero_outside = 1 if x_zero_outside else 0
         self.kernels.call_hierarchy("clb_mg_w_cycle", self.struct, x, rhs, int(pre_smooth), int(post_smooth),
                                     int(coarse_iterations), stream=queue)
 

@@ -165,7 +165,8 @@ class PressureSolver:
         h = self.hierarchy
         delta = float(FIELD_DTYPE(self.dx))
         self.correction.zero_()
-        h.w_cycle(self.correction, self.residual, coarse_iterations=self.coarse_iterations, queue=queue)
+        h.w_cycle(self.correction, self.residual, coarse_iterations=self.coarse_iterations, queue=queue,
+                  x_zero_outside=True)
         if self.method == "fcg":
             self.kernels.call("clb_mg_fcg_dots", self.correction, self.direction[src], self.residual, h.op0, delta,
                               *self.grid_shape, self.fcg_partials, self.fcg_state, stream=queue)

@@ -221,7 +221,22 @@ typedef struct clb_mg_hierarchy {
                                             out[0] of clb_mg_residual_norms / ir_step / fcg_step) */
     int32_t* fp16_inexact;               /* device counter: FP16 operator entries that did not convert
                                             exactly (clb_mg_build_coarse zeroes and fills it) */
+    /* No counterpart in the reference: fluid tiles (NULL tiles / tile_counts: every sweep covers the
+     * whole level). A tile is one plane i, four rows j and 32 cells k (128 on the finest level when
+     * nz % 4 == 0), numbered (i * ceil(ny / 4) + j / 4) * ceil(nz / tile_k) + k / tile_k.
+     * clb_mg_build_coarse lists the tiles that hold a fluid cell and zeroes every coarse p and b;
+     * inside clb_mg_w_cycle the sweeps, restrictions and prolongations of FP32 levels then visit the
+     * listed tiles only (cells that are not fluid keep the 0 the reference's sweeps would write). */
+    int32_t* tiles[CLB_MG_MAX_LEVELS];   /* per level: clb_mg_tile_capacity(shape, level == 0) entries */
+    int32_t* tile_counts;                /* device int32[CLB_MG_MAX_LEVELS]: listed tiles per level */
+    int32_t zero_outside;                /* 1: level-0 x is 0 at every cell that is not fluid when
+                                            clb_mg_w_cycle is called (the correction of the tolerance
+                                            mode), so level-0 sweeps may skip tiles without fluid;
+                                            0: level-0 sweeps cover the whole grid */
 } clb_mg_hierarchy;
+
+/* Number of tiles of a level of nx x ny x nz cells (finest != 0: the finest level's tile shape). */
+int64_t clb_mg_tile_capacity(int nx, int ny, int nz, int finest);
 
 /* pressure_solve.cl:3-24 pressure_rhs fused with multigrid.cl:63-88 build_finest_operator, writing
  * the packed level-0 operator. */

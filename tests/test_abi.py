@@ -30,7 +30,7 @@ def test_python_signature_table_covers_the_header():
 
 def test_load_library_sets_signatures_and_pure_helpers():
     lib = backend.load_library()
-    assert lib.clb_abi_version() == 7
+    assert lib.clb_abi_version() == 8
     for count in (0, 1, 4096, 4097, 16777216):
         assert lib.clb_scan_scratch_bytes(count) == backend.Backend.scan_scratch_bytes_static(count)
     assert lib.clb_mg_residual_partials(1000) == 4
@@ -41,14 +41,17 @@ def test_load_library_sets_signatures_and_pure_helpers():
 
 def test_hierarchy_struct_layout():
     # int32 levels (0), int32[16][3] (4..196), float delta (196), int32 fp16_level (200), then
-    # 8-byte-aligned pointers: op0 at 208, the five pointer tables, int32 sweep[16], then the three
-    # FP16 pointers
+    # 8-byte-aligned pointers: op0 at 208, the five pointer tables, int32 sweep[16], the three FP16
+    # pointers, the tile table, the tile counts and the int32 zero_outside flag (padded to 8 bytes)
     assert backend.MGHierarchy.delta.offset == 196
     assert backend.MGHierarchy.fp16_level.offset == 200
     assert backend.MGHierarchy.op0.offset == 208
     assert backend.MGHierarchy.p.offset == 216
     assert backend.MGHierarchy.fp16_scale.offset == 216 + 5 * 16 * 8 + 16 * 4
-    assert ctypes.sizeof(backend.MGHierarchy) == 216 + 5 * 16 * 8 + 16 * 4 + 3 * 8
+    tiles = 216 + 5 * 16 * 8 + 16 * 4 + 3 * 8
+    assert backend.MGHierarchy.tiles.offset == tiles
+    assert backend.MGHierarchy.zero_outside.offset == tiles + 16 * 8 + 8
+    assert ctypes.sizeof(backend.MGHierarchy) == tiles + 16 * 8 + 8 + 8
 
 
 def test_backend_without_gpu_fails_loudly(monkeypatch):
@@ -69,7 +72,8 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
     root = Path(__file__).resolve().parents[1]
     src = tmp_path / "layout.c"
     fields = {
-        "clb_mg_hierarchy": ["fp16_level", "op0", "sweep", "fp16_scale", "rhs_norms", "fp16_inexact"],
+        "clb_mg_hierarchy": ["fp16_level", "op0", "sweep", "fp16_scale", "rhs_norms", "fp16_inexact", "tiles",
+                             "tile_counts", "zero_outside"],
         "clb_batch_scene": ["base", "particle_base", "delta", "upper", "pad"],
         "clb_batch_list": ["start", "count", "total"],
         "clb_batch": ["geom_host", "particles", "cells", "colour0", "sweep0", "bottom_smem", "op0", "op"],

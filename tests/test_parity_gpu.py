@@ -629,3 +629,44 @@ def test_steps_with_fewer_coarse_iterations(backend):
         totals[k] = sum(st.cycles for st in stats)
     assert totals[4] <= totals[64] + 4, totals
     assert backend.device_error() == 0
+
+
+def corner_block_system(shape, seed):
+    """A liquid block in one corner (most tiles hold no fluid) and a random right-hand side."""
+    rng = np.random.default_rng(seed)
+    ff = np.zeros(shape, F32)
+    nx, ny, nz = shape
+    ff[1 : nx // 2, 1 : (7 * ny) // 10, 1 : nz // 2] = 1.0
+    ff[rng.random(shape) < 0.03] = 0
+    return ff
+
+
+@pytest.mark.parametrize("shape", [(66, 70, 68), (66, 66, 66), (40, 36, 44)])
+def test_fluid_tile_w_cycle_matches_oracle(backend, oracle, shape):
+    """W-cycles that visit only the tiles holding fluid (level 0 included: a zero correction) give the
+    reference's values, and the same values as with the tile lists switched off."""
+    dx = F32(1.0 / shape[0])
+    ff = corner_block_system(shape, 41)
+    u, v, w = (np.random.default_rng(42 + a).standard_normal(shape).astype(F32) for a in range(3))
+    orhs = oracle.pressure_rhs(u, v, w, ff, dx, 1.0 / 240.0, 1000.0, shape)
+    oops = oracle.build_finest_operator(ff, shape)
+    results = {}
+    for tiles in (True, False):
+        h = multigrid.MultigridHierarchy(backend, shape, float(dx), fluid_tiles=tiles)
+        rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+        h.rhs_operator((dev(u), dev(v), dev(w)), dev(ff), rhs, 1.0 / 240.0, 1000.0)
+        h.build_coarse()
+        if tiles:
+            counts = h.tile_counts.cpu().numpy()[: h.levels]
+            assert 0 < counts[0] < int(backend.lib.clb_mg_tile_capacity(*shape, 1))
+        P = torch.zeros(shape, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            h.w_cycle(P, rhs, x_zero_outside=True, coarse_iterations=8)
+        results[tiles] = host(P)
+    q = np.zeros(shape, F32)
+    levels = oracle.Levels(shape)
+    for _ in range(2):
+        levels.w_cycle(q, orhs, ff, oops, dx, coarse=8)
+    assert np.array_equal(results[True], q)
+    assert np.array_equal(results[False], q)
+    assert backend.device_error() == 0
