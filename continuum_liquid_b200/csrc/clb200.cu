@@ -31,6 +31,7 @@ static const int kAbiVersion = 8;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 static bool g_use_cluster = true;  // clb_mg_set_option(2, ...) switches the cluster visit off
+static bool g_skip_air = true;     // clb_mg_set_option(3, ...): refinement/FCG steps skip cells without fluid
 
 template <bool L0, bool H, int TI, int TJ, int T>
 static cudaError_t rbgs_iter_attr_one() {
@@ -1028,10 +1029,11 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
 }
 
 int clb_mg_set_option(int option, int value) {
-    CLB_REQUIRE(option >= 0 && option <= 2, "mg_set_option: unknown option %d", option);
+    CLB_REQUIRE(option >= 0 && option <= 3, "mg_set_option: unknown option %d", option);
     if (option == 0) g_use_bottom = value != 0;
     else if (option == 1) g_use_pdl = value != 0;
-    else g_use_cluster = value != 0;
+    else if (option == 2) g_use_cluster = value != 0;
+    else g_skip_air = value != 0;
     return 0;
 }
 
@@ -1072,8 +1074,12 @@ int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const 
     const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_IR>, p64_in, e, p64_out, b, op0, inv_delta2, nx, ny,
-                                     nz, r_out, (double2*)partials, nullptr, nullptr, nullptr);
+    if (g_skip_air)
+        launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_IR, true>, p64_in, e, p64_out, b, op0, inv_delta2,
+                                         nx, ny, nz, r_out, (double2*)partials, nullptr, nullptr, nullptr);
+    else
+        launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_IR, false>, p64_in, e, p64_out, b, op0,
+                                         inv_delta2, nx, ny, nz, r_out, (double2*)partials, nullptr, nullptr, nullptr);
     CLB_LAUNCH_CHECK("k_residual_rows");
     launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
@@ -1106,8 +1112,12 @@ int clb_mg_fcg_step(const double* p64_in, const float* z, const float* d_in, dou
     const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_FCG>, p64_in, z, p64_out, b, op0, inv_delta2, nx, ny,
-                                     nz, r_out, (double2*)partials, d_in, d_out, state);
+    if (g_skip_air)
+        launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_FCG, true>, p64_in, z, p64_out, b, op0,
+                                         inv_delta2, nx, ny, nz, r_out, (double2*)partials, d_in, d_out, state);
+    else
+        launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_FCG, false>, p64_in, z, p64_out, b, op0,
+                                         inv_delta2, nx, ny, nz, r_out, (double2*)partials, d_in, d_out, state);
     CLB_LAUNCH_CHECK("k_residual_rows");
     launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");

@@ -556,10 +556,14 @@ constexpr int RN_THREADS = 256;
 //                     beta read from state[0] and state[1] (k_fcg_scalars).
 // When r_out is given the residual is stored rounded to float at every cell (0 outside interior
 // fluid cells): it is the right-hand side of the next correction solve.
+// SKIP (refinement and FCG steps): cells that are not interior fluid cells are neither read nor
+// written. Every value there is 0 when the caller keeps the invariant (e, d_in, p_in, and the
+// outputs zeroed outside the fluid once per solve), so the outputs and sums are those of the full
+// pass; the per-lane summation order over fluid cells is unchanged.
 enum { RES_NORM = 0, RES_IR = 1, RES_FCG = 2 };
 
 // Block `blk` of `nblk` blocks sharing the rows; its partial sums go to *partial.
-template <typename PT, int MODE>
+template <typename PT, int MODE, bool SKIP = false>
 __device__ __forceinline__ void residual_rows_block(int blk, int nblk, const PT* __restrict__ p_in,
                                                     const float* __restrict__ e, double* __restrict__ p_out,
                                                     const float* __restrict__ b, const uint8_t* __restrict__ op0,
@@ -589,6 +593,7 @@ __device__ __forceinline__ void residual_rows_block(int blk, int nblk, const PT*
         const int base = r * nz;
         for (int k = lane; k < nz; k += 32) {
             const int c = base + k;
+            if (SKIP && MODE != RES_NORM && !(row_in && k >= 1 && k <= nz - 2 && (__ldg(op0 + c) & 64u))) continue;
             const double pc = pv(c);
             if (MODE != RES_NORM) p_out[c] = pc;
             if (MODE == RES_FCG) d_out[c] = dv(c);
@@ -625,7 +630,7 @@ __device__ __forceinline__ void residual_rows_block(int blk, int nblk, const PT*
     }
 }
 
-template <typename PT, int MODE>
+template <typename PT, int MODE, bool SKIP = false>
 __global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restrict__ p_in,
                                                                const float* __restrict__ e,
                                                                double* __restrict__ p_out,
@@ -637,7 +642,7 @@ __global__ void __launch_bounds__(RN_THREADS) k_residual_rows(const PT* __restri
                                                                float* __restrict__ d_out = nullptr,
                                                                const double* __restrict__ state = nullptr) {
     pdl_begin();
-    residual_rows_block<PT, MODE>(blockIdx.x, gridDim.x, p_in, e, p_out, b, op0, inv_delta2, nx, ny, nz, r_out,
+    residual_rows_block<PT, MODE, SKIP>(blockIdx.x, gridDim.x, p_in, e, p_out, b, op0, inv_delta2, nx, ny, nz, r_out,
                                   partials + blockIdx.x, d_in, d_out, state);
 }
 

@@ -248,7 +248,10 @@ class PressureSolver:
         self.cur = 0
         if self.method == "fcg":
             self.direction[0].zero_()
+            self.direction[1].zero_()
             self.fcg_state.zero_()
+        # the step kernels skip cells outside the fluid: both FP64 buffers start at 0 there
+        self.p64[1].zero_()
         self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64[0], *self.grid_shape)
         rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
         if warm_start is not None:

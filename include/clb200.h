@@ -265,7 +265,12 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
  *  option 2: 1 (default) runs each visit of the third-coarsest level, with its two bottom visits, as
  *            one launch of a thread-block cluster (up to 16 CTAs, distributed shared memory) when the
  *            three levels share their storage type and fit; 0 goes level by level. Identical
- *            results. */
+ *            results.
+ *  option 3: 1 (default) lets clb_mg_ir_step and clb_mg_fcg_step skip the cells that are not
+ *            interior fluid cells (neither read nor written); the caller keeps p64_out, d_out and
+ *            r_out at 0 there (zero them once per solve: clb_mg_ir_init and clb_mg_residual_norms
+ *            with r_out do so for their outputs). 0 writes every cell. Identical results when the
+ *            caller keeps that invariant. */
 int clb_mg_set_option(int option, int value);
 
 /* Block-partial count used by clb_mg_residual_norms for a grid of `cells` cells. */
