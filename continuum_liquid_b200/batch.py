@@ -47,7 +47,7 @@ def bottom_plan(shapes) -> tuple[int, int, int, int]:
     a, b = shapes[level], shapes[level + 1]
     ca, cb = int(np.prod(a)), int(np.prod(b))
     sa, sb = colour_slots(a), colour_slots(b)
-    smem = _pad16(ca * 4) * 2 + ca * 16 + _pad16(cb * 4) + cb * 16
+    smem = _pad16(ca * 4) * 2 + ca * 16 + _pad16(cb * 4) + cb * 16 + _pad16((ca + cb + 8) * 4)
     if smem > BOTTOM_SMEM_LIMIT or sb > BOTTOM_MAX_B * BOTTOM_BTHREADS or sa > BOTTOM_MAX_A * BOTTOM_THREADS:
         return -1, 0, 0, 0
     return level, -(-sa // BOTTOM_THREADS), -(-sb // BOTTOM_BTHREADS), smem

@@ -22,9 +22,11 @@ constexpr int BOTTOM_MAX_A = 8;  // A slots of each colour per thread
 constexpr int BOTTOM_MAX_B = 4;  // B slots of each colour per B thread
 
 static inline size_t bottom_smem_bytes(int ca, int cb) {
-    // A: p, b, op(float4); B: p, op(float4); each region padded to 16 bytes
+    // A: p, b, op(float4); B: p, op(float4); the fluid-cell lists of both colours of both levels and
+    // their four counts; each region padded to 16 bytes
     auto pad = [](size_t x) { return (x + 15) & ~(size_t)15; };
-    return pad((size_t)ca * 4) * 2 + (size_t)ca * 16 + pad((size_t)cb * 4) + (size_t)cb * 16;
+    return pad((size_t)ca * 4) * 2 + (size_t)ca * 16 + pad((size_t)cb * 4) + (size_t)cb * 16 +
+           pad((size_t)(ca + cb + 8) * 4);
 }
 
 // Cells of one colour are numbered by slots: the interior rows (i, j) in index order, ceil(mz / 2)
@@ -86,13 +88,17 @@ constexpr int BOTTOM_BTHREADS = 256;
 __device__ __forceinline__ void bar_b() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 // Shared-memory arrays of a bottom visit: A's p, b and operator (float4, diagonal -1 where not
-// fluid), B's p and operator; each region padded to 16 bytes (bottom_smem_bytes).
+// fluid), B's p and operator, and the fluid cells of each colour of both levels; each region padded to
+// 16 bytes (bottom_smem_bytes).
 struct BottomSmem {
     float* spa;
     float* sba;
     float4* soa;
     float* spb;
     float4* sob;
+    int* count;   // fluid cells: A colour 0, A colour 1, B colour 0, B colour 1
+    int* list_a;  // two lists of CA / 2 + 1 entries
+    int* list_b;  // two lists of CB / 2 + 1 entries
 };
 
 __device__ __forceinline__ BottomSmem bottom_smem(unsigned char* base, int CA, int CB) {
@@ -103,7 +109,35 @@ __device__ __forceinline__ BottomSmem bottom_smem(unsigned char* base, int CA, i
     S.soa = reinterpret_cast<float4*>(S.sba + pad(CA));
     S.spb = reinterpret_cast<float*>(S.soa + CA);
     S.sob = reinterpret_cast<float4*>(S.spb + pad(CB));
+    S.count = reinterpret_cast<int*>(S.sob + CB);
+    S.list_a = S.count + 4;
+    S.list_b = S.list_a + 2 * (CA / 2 + 1);
     return S;
+}
+
+// Lists the fluid interior cells of each colour of both levels (after the operators are staged and
+// the block has synchronised). Their order is arbitrary -- cells of one colour are independent -- and
+// the threads take them in turn, so a warp's owned cells are fluid but for the last ones and the empty
+// slots beyond the count are empty in whole warps: a phase costs what the fluid needs, not what the
+// level's size does.
+__device__ __forceinline__ void bottom_lists(const BottomSmem& S, int anx, int any, int anz, int bnx, int bny,
+                                             int bnz) {
+    const int CA = anx * any * anz, CB = bnx * bny * bnz;
+    const int la = CA / 2 + 1, lb = CB / 2 + 1;
+    if (threadIdx.x < 4) S.count[threadIdx.x] = 0;
+    __syncthreads();
+    const int sa = colour_slots(anx, any, anz), sb = colour_slots(bnx, bny, bnz);
+    for (int colour = 0; colour < 2; ++colour) {
+        for (int r = threadIdx.x; r < sa; r += BOTTOM_THREADS) {
+            const int c = colour_cell(r, colour, anx, any, anz);
+            if (c >= 0 && S.soa[c].x >= 0.0f) S.list_a[colour * la + atomicAdd(S.count + colour, 1)] = c;
+        }
+        for (int r = threadIdx.x; r < sb; r += BOTTOM_THREADS) {
+            const int c = colour_cell(r, colour, bnx, bny, bnz);
+            if (c >= 0 && S.sob[c].x >= 0.0f) S.list_b[colour * lb + atomicAdd(S.count + 2 + colour, 1)] = c;
+        }
+    }
+    __syncthreads();
 }
 
 // Staging of the operators of both levels and, when pa / ba are given, of A's p and b (FP16 levels
@@ -191,15 +225,17 @@ __device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int an
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) spb[c] = 0.0f;  // multigrid.cl:114
 
     const int asx = any * anz, asy = anz, bsx = bny * bnz, bsy = bnz;
-    OwnedCell A[2][KA];  // [colour][m]
+    const int la = (anx * any * anz) / 2 + 1, lb = CB / 2 + 1;
+    OwnedCell A[2][KA];  // [colour][m]: the thread's fluid cells (bottom_lists)
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KA; ++m) {
-            const int c = colour_cell(threadIdx.x + m * BOTTOM_THREADS, colour, anx, any, anz);
+            const int r = threadIdx.x + m * BOTTOM_THREADS;
+            const int c = r < S.count[colour] ? S.list_a[colour * la + r] : -1;
             OwnedCell& o = A[colour][m];
             o.c = c < 0 ? 0 : c;
-            o.d = c < 0 ? -1.0f : soa[c].x;  // -1 when not fluid
+            o.d = c < 0 ? -1.0f : soa[c].x;  // fluid: >= 0
             o.d2b = c < 0 ? 0.0f : d2 * sba[c];
         }
     const bool btile = threadIdx.x < BOTTOM_BTHREADS;
@@ -208,7 +244,8 @@ __device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int an
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KB; ++m) {
-            const int c = btile ? colour_cell(threadIdx.x + m * BOTTOM_BTHREADS, colour, bnx, bny, bnz) : -1;
+            const int r = threadIdx.x + m * BOTTOM_BTHREADS;
+            const int c = btile && r < S.count[2 + colour] ? S.list_b[colour * lb + r] : -1;
             OwnedCellW& o = B[colour][m];
             o.d2b = 0.0f;
             o.c = 0;
@@ -300,8 +337,7 @@ __device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int an
         for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
             for (int m = 0; m < KB; ++m)
-                if (btile && colour_cell(threadIdx.x + m * BOTTOM_BTHREADS, colour, bnx, bny, bnz) >= 0)
-                    st(bb, B[colour][m].c, bvals[colour][m]);
+                if (B[colour][m].d >= 0.0f) st(bb, B[colour][m].c, bvals[colour][m]);  // fluid cells
     }
 }
 
@@ -325,13 +361,15 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
         else a[c] = v;
     };
     bottom_stage<H>(S, pa, ba, opa, ma, CA, opb, mb, CB);
+    bottom_lists(S, anx, any, anz, bnx, bny, bnz);
     bottom_core<KA, KB, H>(S, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, bb);
     const int bsx = bny * bnz, bsy = bnz;
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) st(pa, c, S.spa[c]);
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
         st(pb, c, S.spb[c]);
         const int I = c / bsx, J = (c / bsy) % bny, K = c % bnz;
-        if (!interior(I, J, K, bnx, bny, bnz)) st(bb, c, 0.0f);  // multigrid.cl:115
+        // multigrid.cl:115 zeroes b off the interior; cells that are not fluid restrict to 0
+        if (!interior(I, J, K, bnx, bny, bnz) || S.sob[c].x < 0.0f) st(bb, c, 0.0f);
     }
 }
 

@@ -59,6 +59,8 @@ struct ClusterLayout {
     size_t op_off;   // operator: (own_max + 2) planes
     size_t p_off;    // p: (own_max + 2) planes
     size_t b_off;    // b: own_max planes
+    size_t list_off; // fluid cells of each colour: list_len ints each, then two counts
+    int list_len;
     size_t slab_bytes;
 };
 
@@ -73,7 +75,9 @@ __host__ __device__ __forceinline__ ClusterLayout cluster_layout(int cs, int nx,
     L.op_off = 0;
     L.p_off = pad((size_t)(L.own_max + 2) * plane * op_bytes);
     L.b_off = L.p_off + pad((size_t)(L.own_max + 2) * plane * 4);
-    L.slab_bytes = L.b_off + pad((size_t)L.own_max * plane * 4);
+    L.list_off = L.b_off + pad((size_t)L.own_max * plane * 4);
+    L.list_len = (int)((size_t)L.own_max * plane / 2 + 1);
+    L.slab_bytes = L.list_off + pad((size_t)(2 * L.list_len + 2) * 4);
     return L;
 }
 
@@ -126,15 +130,28 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
     }
     __syncthreads();
 
-    // owned cells by colour slots of the slab seen as a level of np planes (global colour: the local
-    // plane il is global plane il + i_lo - 1)
+    // owned cells: the slab's fluid cells of each colour (the slab seen as a level of np planes; the
+    // local plane il is global plane il + i_lo - 1), listed in arbitrary order and taken in turn by the
+    // threads, so only a warp's last owned slots can be empty (bottom_lists)
     const int flip = (sl.i_lo - 1) & 1;
+    int* list = reinterpret_cast<int*>(smem + L.list_off);
+    int* count = list + 2 * L.list_len;
+    if (threadIdx.x < 2) count[threadIdx.x] = 0;
+    __syncthreads();
+    const int slots = colour_slots(np, ny, nz);
+    for (int colour = 0; colour < 2; ++colour)
+        for (int r = threadIdx.x; r < slots; r += BOTTOM_THREADS) {
+            const int c = colour_cell(r, colour ^ flip, np, ny, nz);
+            if (c >= 0 && op4(c).x >= 0.0f) list[colour * L.list_len + atomicAdd(count + colour, 1)] = c;
+        }
+    __syncthreads();
     SlabCell C[2][NS];
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < NS; ++m) {
-            const int c = colour_cell(threadIdx.x + m * BOTTOM_THREADS, colour ^ flip, np, ny, nz);
+            const int r = threadIdx.x + m * BOTTOM_THREADS;
+            const int c = r < count[colour] ? list[colour * L.list_len + r] : -1;
             SlabCell& o = C[colour][m];
             o.c = c < 0 ? 0 : c;
             o.d = c < 0 ? -1.0f : op4(c).x;
@@ -250,6 +267,7 @@ __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __rest
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     const BottomSmem S = bottom_smem(smem, CA, CB);
     bottom_stage<H>(S, nullptr, nullptr, opa, ma, CA, opb, mb, CB);
+    bottom_lists(S, anx, any, anz, bnx, bny, bnz);
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
         S.spa[c] = 0.0f;  // restriction zeroes the coarse pressure (multigrid.cl:114)
         S.sba[c] = 0.0f;  // cells the restriction does not write (non-interior) hold 0
