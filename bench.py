@@ -43,7 +43,9 @@ COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarses
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu capture of the same kernel on the
 # same 256^3 system (profiles/k_rbgs_colour_level0_block_256.md); None for kernels not captured.
-NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360}
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
+NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
+                     "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
 
 
 def parse_args():
@@ -282,7 +284,7 @@ def sweep_case(args):
     h = ps.hierarchy
     tune_hierarchy(h, ps.correction, ps.residual)
     p = torch.zeros_like(zero)
-    h.smooth(0, 2, p, ps.rhs)
+    h.smooth(0, 2, p, ps.rhs, zero_outside=True)  # p is 0 outside the fluid: the fluid-tile sweep
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.case == "wcycle":
@@ -300,13 +302,14 @@ def sweep_case(args):
         return
     torch.cuda.nvtx.range_push("sweeps")
     e0.record()
-    h.smooth(0, args.sweeps, p, ps.rhs)
+    h.smooth(0, args.sweeps, p, ps.rhs, zero_outside=True)
     e1.record()
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.sweeps
-    cells = scene.cells
-    print(json.dumps({"case": "sweep0", "grid": list(scene.grid_shape), "sweep_kind": h.sweeps()[0],
+    tiles0 = int(h.tile_counts[0].item())
+    cells = tiles0 * 4 * (128 if scene.grid_shape[2] % 4 == 0 else 32)
+    print(json.dumps({"case": "sweep0", "grid": list(scene.grid_shape), "fluid_tiles": tiles0, "tile_cells": cells,
                       "ms_per_iteration": ms, "algorithmic_gb_s": 13.0 * cells / (ms * 1e-3) / 1e9}), flush=True)
 
 
@@ -689,32 +692,32 @@ def our_arm(args):
                "path": "FlipSolver.step with the particle state copied from pinned host buffers before and back "
                        "after every step (the reference's per-step host round trip of solver.py:252-306)"}
 
-    # --- roofline: level-0 red-black Gauss-Seidel sweep, timed alone on the stream ------------
+    # --- roofline: the level-0 red-black sweep as the timed steps run it (on the fluid tiles), timed
+    # alone on the stream ---------------------------------------------------------------------------
     ps = sim.pressure_solver
     h = ps.hierarchy
     iters = 20
     torch.cuda.synchronize()
     ps.correction.zero_()
-    h.smooth(0, 2, ps.correction, ps.residual)
+    h.smooth(0, 2, ps.correction, ps.residual, zero_outside=True)
     s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s3.record()
-    h.smooth(0, iters, ps.correction, ps.residual)
+    h.smooth(0, iters, ps.correction, ps.residual, zero_outside=True)
     e3.record()
     torch.cuda.synchronize()
-    kind0 = h.sweeps()[0] or 1
-    fused = kind0 in (2, 3)
-    launches_timed = iters if fused else 2 * iters
-    per_launch_s = s3.elapsed_time(e3) / 1e3 / launches_timed
-    cells = int(np.prod(scene.grid_shape))
-    # p read + write 8 B, b 4 B, packed operator 1 B per cell per red-black iteration
-    algorithmic = 13.0 * cells if fused else 13.0 * cells / 2.0
+    per_launch_s = s3.elapsed_time(e3) / 1e3 / (2 * iters)
+    vec = scene.grid_shape[2] % 4 == 0
+    tiles0 = int(h.tile_counts[0].item())
+    cells = tiles0 * 4 * (128 if vec else 32)  # the cells of the fluid tiles a launch streams
+    # p read + write 8 B, b 4 B, packed operator 1 B per cell per red-black iteration; one colour per launch
+    algorithmic = 13.0 * cells / 2.0
     achieved = algorithmic / per_launch_s / 1e9
     peak, peak_kind = measured_peak_hbm()
-    kernel = {1: "k_rbgs_colour<true,4>", 2: "k_rbgs_iter<true,8,8,32>", 3: "k_rbgs_iter<true,4,4,32>",
-              4: "k_rbgs<true>"}[kind0]
+    kernel = "k_rbgs_colour_tiles<true,4>" if vec else "k_rbgs_colour_tiles<true,1>"
     traffic = NCU_TRAFFIC_BYTES.get(kernel)
-    roofline = {"kernel": f"{kernel} (level-0 red-black Gauss-Seidel, {'one iteration' if fused else 'one colour'} "
-                          "per launch)", "bound": "hbm",
+    roofline = {"kernel": f"{kernel} (level-0 red-black Gauss-Seidel on the {tiles0} fluid tiles of "
+                          f"{int(h.kernels.lib.clb_mg_tile_capacity(*scene.grid_shape, 1))}, one colour per launch)",
+                "bound": "hbm", "tile_cells": cells,
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                 "traffic": traffic, "algorithmic_bytes_per_launch": algorithmic, "launch_us": per_launch_s * 1e6}

@@ -1025,7 +1025,8 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
     CLB_REQUIRE(level >= 0 && level < h->levels, "mg_smooth: level %d outside 0..%d", level, h->levels - 1);
     CLB_REQUIRE(iterations >= 0, "mg_smooth: negative iterations");
     CLB_REQUIRE(level > 0 || (x && rhs), "mg_smooth: null level-0 array");
-    return smooth(level_view(h, level, x, rhs), h->delta, iterations, CLB_STREAM(stream));
+    return smooth(level_view(h, level, x, rhs), h->delta, iterations, CLB_STREAM(stream),
+                  h->zero_outside != 0 && h->tile_counts != nullptr);
 }
 
 int clb_mg_set_option(int option, int value) {

@@ -244,8 +244,11 @@ class MultigridHierarchy:
     def sweeps(self) -> list[int]:
         return [int(self.struct.sweep[l]) for l in range(self.levels)]
 
-    def smooth(self, level: int, iterations: int, x=None, rhs=None, queue=None) -> None:
-        """``iterations`` red-black Gauss-Seidel iterations on one level."""
+    def smooth(self, level: int, iterations: int, x=None, rhs=None, queue=None, zero_outside: bool = False) -> None:
+        """``iterations`` red-black Gauss-Seidel iterations on one level. ``zero_outside``: the caller
+        guarantees that the level's p (``x`` on level 0) is 0 at every cell that is not fluid, so an
+        FP32 level is swept on its fluid tiles only (the values are the same)."""
+        self.struct.zero_outside = 1 if zero_outside else 0
         self.kernels.call_hierarchy("clb_mg_smooth", self.struct, int(level), x, rhs, int(iterations), stream=queue)
 
     def residual_norms(self, p, rhs, r_out=None, queue=None) -> torch.Tensor:

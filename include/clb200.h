@@ -252,7 +252,9 @@ int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pr
                    int coarse_iterations, void* stream);
 
 /* multigrid.py:190-220 smooth: `iterations` red-black Gauss-Seidel iterations on one level (level 0
- * uses x and rhs; coarse levels their own p and b). */
+ * uses x and rhs; coarse levels their own p and b). With h->zero_outside = 1 and tile lists built by
+ * clb_mg_build_coarse, the caller guarantees that the level's p (x on level 0) is 0 at every cell
+ * that is not fluid, and an FP32 level is swept on its fluid tiles only (same values). */
 int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int iterations, void* stream);
 
 /* Process-wide multigrid options (host-side switches, no device work):
