@@ -354,15 +354,93 @@ __device__ __forceinline__ void p2g_cell(i64 index, int lane, const float* __res
     }
 }
 
+// The same gather with the lanes laid out by warp: block b handles cells 32 b .. 32 b + 31, warp w
+// is lane w of all 32 cells (thread t of the warp: cell 32 b + t). The warp's threads then visit bins
+// with the same offset at the same time, so the exact-zero cases above are uniform across the warp:
+// a bin one above the cell on exactly one axis feeds only that axis's face component and never the
+// inside count, and it skips the other two components' weights and the count. Each lane still
+// visits bins w, w+8, w+16, w+24 and their particles in order and accumulates as above; the eight
+// partial sums of a cell are combined in shared memory in the order of the offset-4, 2, 1 tree
+// ((l0 + l4) + (l2 + l6)) + ((l1 + l5) + (l3 + l7)), so the values are the same as p2g_cell's.
 __global__ void __launch_bounds__(P2G_THREADS) k_p2g_gather(const float* __restrict__ pos, const float* __restrict__ vel,
                                                              const int* __restrict__ offsets,
                                                              const int* __restrict__ counts, float* __restrict__ u,
                                                              float* __restrict__ v, float* __restrict__ w,
                                                              float* __restrict__ ff, float inv_dx, float inv_ppc,
                                                              int nx, int ny, int nz) {
-    const i64 index = ((i64)blockIdx.x * P2G_THREADS + threadIdx.x) / P2G_LANES;
-    p2g_cell(index, threadIdx.x & (P2G_LANES - 1), pos, vel, offsets, counts, u, v, w, ff, inv_dx, inv_ppc, nx, ny,
-             nz);
+    __shared__ float s_sum[6][P2G_LANES][32];
+    __shared__ int s_inside[P2G_LANES][32];
+    const i64 C = (i64)nx * ny * nz;
+    const int lane = threadIdx.x >> 5, t = threadIdx.x & 31;
+    const i64 index = (i64)blockIdx.x * 32 + t;
+    float vs0 = 0.0f, vs1 = 0.0f, vs2 = 0.0f, ws0 = 0.0f, ws1 = 0.0f, ws2 = 0.0f;
+    int inside = 0;
+    if (index < C) {
+        int ci, cj, ck;
+        gcoord(index, ny, nz, ci, cj, ck);
+        const float gx = (float)ci, gy = (float)cj, gz = (float)ck;
+        const float x1 = gx + 1.0f, xh = gx + 0.5f, y1 = gy + 1.0f, yh = gy + 0.5f, z1 = gz + 1.0f, zh = gz + 0.5f;
+        for (int nb = lane; nb < 27; nb += P2G_LANES) {  // the same nb in the whole warp
+            const int ox = nb / 9 - 1, oy = (nb / 3) % 3 - 1, oz = nb % 3 - 1;
+            const int up = (ox > 0) + (oy > 0) + (oz > 0);
+            if (up >= 2) continue;  // every weight of this bin is zero
+            const bool du = oy <= 0 && oz <= 0, dv = ox <= 0 && oz <= 0, dw = ox <= 0 && oy <= 0, din = up == 0;
+            const int bx = ci + ox, by = cj + oy, bz = ck + oz;
+            if (bx < 0 || bx >= nx - 1 || by < 0 || by >= ny - 1 || bz < 0 || bz >= nz - 1) continue;
+            const i64 bin = gidx(bx, by, bz, ny, nz);
+            const int begin = __ldg(offsets + bin);
+            const int end = begin + __ldg(counts + bin);
+            for (int q = begin; q < end; ++q) {
+                const float* P = pos + 3 * (i64)q;
+                const float* V = vel + 3 * (i64)q;
+                const float s0 = __ldg(P) * inv_dx, s1 = __ldg(P + 1) * inv_dx, s2 = __ldg(P + 2) * inv_dx;
+                if (din) {
+                    const int pc0 = clampi((int)s0, 1, nx - 2);
+                    const int pc1 = clampi((int)s1, 1, ny - 2);
+                    const int pc2 = clampi((int)s2, 1, nz - 2);
+                    inside += (pc0 == ci && pc1 == cj && pc2 == ck) ? 1 : 0;
+                }
+                if (du) {
+                    const float wu = tent(s0, x1) * tent(s1, yh) * tent(s2, zh);
+                    vs0 += wu * __ldg(V);
+                    ws0 += wu;
+                }
+                if (dv) {
+                    const float wv = tent(s0, xh) * tent(s1, y1) * tent(s2, zh);
+                    vs1 += wv * __ldg(V + 1);
+                    ws1 += wv;
+                }
+                if (dw) {
+                    const float ww = tent(s0, xh) * tent(s1, yh) * tent(s2, z1);
+                    vs2 += ww * __ldg(V + 2);
+                    ws2 += ww;
+                }
+            }
+        }
+    }
+    s_sum[0][lane][t] = vs0;
+    s_sum[1][lane][t] = vs1;
+    s_sum[2][lane][t] = vs2;
+    s_sum[3][lane][t] = ws0;
+    s_sum[4][lane][t] = ws1;
+    s_sum[5][lane][t] = ws2;
+    s_inside[lane][t] = inside;
+    __syncthreads();
+    if (lane == 0 && index < C) {
+        float r[6];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+            const float* l = &s_sum[a][0][t];
+            r[a] = ((l[0] + l[4 * 32]) + (l[2 * 32] + l[6 * 32])) + ((l[1 * 32] + l[5 * 32]) + (l[3 * 32] + l[7 * 32]));
+        }
+        int n = 0;
+#pragma unroll
+        for (int q = 0; q < P2G_LANES; ++q) n += s_inside[q][t];
+        u[index] = r[3] > 0.0f ? r[0] / r[3] : 0.0f;
+        v[index] = r[4] > 0.0f ? r[1] / r[4] : 0.0f;
+        w[index] = r[5] > 0.0f ? r[2] / r[5] : 0.0f;
+        ff[index] = (float)n * inv_ppc;
+    }
 }
 
 }  // namespace clb
