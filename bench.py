@@ -40,9 +40,7 @@ METRIC = "steps/s at 256^3; Poisson ms to 1e-6 rel. residual, learned vs plain W
 UNIT = "steps/s"
 TOL = 1e-6
 COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarsest-level iterations
-
-# DRAM bytes (read + write) per launch of the dominant kernel from one ncu capture of the same kernel on the
-# same 256^3 system (profiles/k_rbgs_colour_level0_block_256.md); None for kernels not captured.
+SMOOTHING_CHOICES = ((2, 4), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
                      "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
@@ -70,6 +68,10 @@ def parse_args():
                     help="red-black iterations of each coarsest-level solve in the W-cycle preconditioner of the timed "
                          "steps (auto: the fastest of 64 (the reference's), 16, 8 and 4 that needs no more FCG cycles "
                          "than 64 in the Poisson comparison)")
+    ap.add_argument("--smoothing", default="auto",
+                    help="red-black iterations before,after the coarse-grid correction in the W-cycle preconditioner "
+                         "of the timed steps, e.g. 2,4 (auto: the fastest of 2,4 (the reference's), 1,2 and 1,1 to the "
+                         "tolerance in the Poisson comparison, with 4 coarsest-level iterations)")
     ap.add_argument("--case", choices=["step", "sweep0", "wcycle", "batch", "unet", "collider"], default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
                          "(no particles: a small-memory case for profiling the dominant kernel); batch: the batched "
@@ -321,8 +323,10 @@ def sweep_case(args):
                       "ms_per_iteration": ms, "algorithmic_gb_s": 13.0 * cells / (ms * 1e-3) / 1e9}), flush=True)
 
 
-def workload_config(size, n_particles, args, coarse_iterations=COARSE_ITERATION_CHOICES[0]):
+def workload_config(size, n_particles, args, coarse_iterations=COARSE_ITERATION_CHOICES[0],
+                    smoothing=SMOOTHING_CHOICES[0]):
     k = int(coarse_iterations)
+    pre, post = smoothing
     return {
         "workload": f"flip_step_block_{size}^3",
         "grid": [size, size, size],
@@ -331,9 +335,9 @@ def workload_config(size, n_particles, args, coarse_iterations=COARSE_ITERATION_
         "dt": 1.0 / 240.0,
         "flip_ratio": 0.95,
         "pressure_tolerance": TOL,
-        "pressure_solver": (f"flexible CG preconditioned by one FP32 W-cycle (pre 2, post 4, coarse 2+{k}), FP64 "
-                            "pressure, residual and norms" if args.method == "fcg" else
-                            f"W-cycle (pre 2, post 4, coarse 2+{k}) in FP64 iterative refinement"),
+        "pressure_solver": (f"flexible CG preconditioned by one FP32 W-cycle (pre {pre}, post {post}, coarse "
+                            f"{pre}+{k}), FP64 pressure, residual and norms" if args.method == "fcg" else
+                            f"W-cycle (pre {pre}, post {post}, coarse {pre}+{k}) in FP64 iterative refinement"),
         "multigrid_levels": None,
         "l2": "inputs larger than L2 (particle state 24 B x N, grid fields 4 B x n^3 each)",
         "parallelism": "replicas" if args.gpus > 1 else "single",
@@ -487,6 +491,12 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
         for fp16 in (False, True):
             solvers[f"fcg{'_fp16' if fp16 else ''}_c{k}"] = PressureSolver(
                 kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16, coarse_iterations=k)
+    # fewer smoothing sweeps per level, with 4 coarsest-level iterations and either coarse storage
+    for pre, post in SMOOTHING_CHOICES[1:]:
+        for fp16 in (False, True):
+            solvers[f"fcg{'_fp16' if fp16 else ''}_c4_s{pre}{post}"] = PressureSolver(
+                kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16, coarse_iterations=4,
+                pre_smooth=pre, post_smooth=post)
     p_tmp = torch.empty_like(sim.pressure)
     rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": []}
     rows.update({name: [] for name in solvers if "_c" in name})
@@ -573,6 +583,16 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
         if r and r["cycles_mean"] <= out[base]["cycles_mean"] and r["ms_mean"] < best_ms:
             best_k, best_ms = k, r["ms_mean"]
     out["coarse_iterations_chosen"] = best_k
+    # the rule for the smoothing counts (with 4 coarsest-level iterations chosen): the fastest to the
+    # tolerance
+    best_s = SMOOTHING_CHOICES[0]
+    if best_k == 4:
+        best_ms = out[f"{base}_c4"]["ms_mean"]
+        for pre, post in SMOOTHING_CHOICES[1:]:
+            r = out.get(f"{base}_c4_s{pre}{post}")
+            if r and r["ms_mean"] < best_ms:
+                best_s, best_ms = (pre, post), r["ms_mean"]
+    out["smoothing_chosen"] = list(best_s)
     if rows["fcg_learned"]:
         out["speedup_learned_vs_plain_fcg"] = out["fcg"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
         out["speedup_learned_vs_refine"] = out["refine"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
@@ -611,12 +631,15 @@ def our_arm(args):
     use_fp16 = args.coarse_fp16 == "on"
     use_learned = args.learned == "on"
     coarse_k = COARSE_ITERATION_CHOICES[0] if args.coarse_iterations == "auto" else int(args.coarse_iterations)
+    smoothing = SMOOTHING_CHOICES[0] if args.smoothing == "auto" else tuple(int(x) for x in args.smoothing.split(","))
     if args.poisson_steps > 0:
         poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
         if args.coarse_fp16 == "auto":
             use_fp16 = poisson.get("coarse_fp16_holds", False)
         if args.coarse_iterations == "auto":
             coarse_k = poisson.get("coarse_iterations_chosen", coarse_k)
+        if args.smoothing == "auto":
+            smoothing = tuple(poisson.get("smoothing_chosen", smoothing))
         if args.learned == "auto" and "fcg_learned" in poisson:
             # the rule: the learned guess in the timed steps only when it makes the solve faster,
             # network evaluation included
@@ -626,13 +649,16 @@ def our_arm(args):
     sim.options.warm_start = warm if use_learned else None
     if warm is not None and not use_learned:
         warm_note += " (not used in the timed steps: no faster than without it in the comparison)"
-    if use_fp16 or coarse_k != sim.options.coarse_iterations:
+    if use_fp16 or coarse_k != sim.options.coarse_iterations or \
+            smoothing != (sim.options.pre_smooth, sim.options.post_smooth):
         from continuum_liquid_b200.pressure_solve import PressureSolver
 
         sim.options.coarse_fp16 = use_fp16
         sim.options.coarse_iterations = coarse_k
+        sim.options.pre_smooth, sim.options.post_smooth = smoothing
         sim.pressure_solver = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=scene.min_size,
-                                             method=args.method, coarse_fp16=use_fp16, coarse_iterations=coarse_k)
+                                             method=args.method, coarse_fp16=use_fp16, coarse_iterations=coarse_k,
+                                             pre_smooth=smoothing[0], post_smooth=smoothing[1])
         for _ in range(2):  # tuning and graph capture of the new solver
             sim.step()
         torch.cuda.synchronize()
@@ -664,7 +690,7 @@ def our_arm(args):
 
     # --- Poisson time to 1e-6 in the timed steps ------------------------------------------------
     poisson = {"timed_steps": {"method": args.method, "learned": warm_note, "coarse_fp16": use_fp16,
-                               "coarse_iterations": coarse_k,
+                               "coarse_iterations": coarse_k, "smoothing": list(smoothing),
                                "ms_mean": float(np.mean(solve_ms)),
                                "cycles_mean": float(np.mean(cycles)),
                                "final_rel_residual_max": float(max(s.rel_residual or 0.0 for s in stats)),
@@ -740,7 +766,8 @@ def our_arm(args):
                          f"kernels with {k} FP32 W-cycles (the GPU's mean cycle count)"}
 
     if rank == 0:
-        config = workload_config(args.size, n, args, sim.options.coarse_iterations)
+        config = workload_config(args.size, n, args, sim.options.coarse_iterations,
+                                 (sim.options.pre_smooth, sim.options.post_smooth))
         config["multigrid_levels"] = [list(s) for s in h.shapes]
         config["sweep_kinds"] = h.sweeps()
         config["sweep_tuning_ms_per_iteration"] = h.tuning

@@ -100,7 +100,8 @@ class PressureSolver:
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100,
                  autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64,
-                 coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS):
+                 coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS,
+                 pre_smooth: int = multigrid.PRE_SMOOTH, post_smooth: int = multigrid.POST_SMOOTH):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.coarse_fp16 = bool(coarse_fp16)
@@ -114,6 +115,12 @@ class PressureSolver:
         self.coarse_iterations = int(coarse_iterations)
         if self.coarse_iterations < 0:
             raise ValueError("coarse_iterations must be >= 0")
+        # red-black iterations before and after the coarse-grid correction on every level of the
+        # tolerance mode's W-cycle preconditioner; the reference's 2 and 4 by default (fixed-cycle mode
+        # always uses those)
+        self.pre_smooth, self.post_smooth = int(pre_smooth), int(post_smooth)
+        if self.pre_smooth < 0 or self.post_smooth < 0 or self.pre_smooth + self.post_smooth == 0:
+            raise ValueError("pre_smooth and post_smooth must be >= 0 and not both 0")
         # FP16 storage of the coarse levels of at most fp16_max_size cells per side (tolerance mode only:
         # the W-cycle then reads the squared norm of its right-hand side from the residual kernels)
         self.hierarchy = multigrid.MultigridHierarchy(kernels, self.grid_shape, dx, min_size,
@@ -165,8 +172,8 @@ class PressureSolver:
         h = self.hierarchy
         delta = float(FIELD_DTYPE(self.dx))
         self.correction.zero_()
-        h.w_cycle(self.correction, self.residual, coarse_iterations=self.coarse_iterations, queue=queue,
-                  x_zero_outside=True)
+        h.w_cycle(self.correction, self.residual, pre_smooth=self.pre_smooth, post_smooth=self.post_smooth,
+                  coarse_iterations=self.coarse_iterations, queue=queue, x_zero_outside=True)
         if self.method == "fcg":
             self.kernels.call("clb_mg_fcg_dots", self.correction, self.direction[src], self.residual, h.op0, delta,
                               *self.grid_shape, self.fcg_partials, self.fcg_state, stream=queue)

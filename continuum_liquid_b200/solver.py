@@ -56,6 +56,10 @@ class StepOptions:
     # tolerance mode: red-black iterations of each coarsest-level solve in the W-cycle preconditioner
     # beyond its pre-smoothing (the reference's fixed-cycle W-cycle uses 64, multigrid.py defaults)
     coarse_iterations: int = 64
+    # tolerance mode: red-black iterations before / after the coarse-grid correction in the W-cycle
+    # preconditioner (the reference's 2 and 4)
+    pre_smooth: int = 2
+    post_smooth: int = 4
     revoxelise: bool = False  # voxelise the colliders again at every step (moving or deforming meshes)
 
 
@@ -101,7 +105,9 @@ class FlipSolver:
             self.obstacle = torch.zeros(self.grid_shape, dtype=torch.uint8, device=dev)
         self.pressure_solver = PressureSolver(kernels, self.grid_shape, self.dx, min_size=min_size,
                                               method=self.options.method, coarse_fp16=self.options.coarse_fp16,
-                                              coarse_iterations=self.options.coarse_iterations)
+                                              coarse_iterations=self.options.coarse_iterations,
+                                              pre_smooth=self.options.pre_smooth,
+                                              post_smooth=self.options.post_smooth)
         self.last_solve: SolveStats | None = None
         self.steps_done = 0
 

@@ -340,11 +340,13 @@ def apply_operator64(p, mask, op0, delta):
     return np.where(fluid, (ws - d * p) * (1.0 / (float(delta) * float(delta))), 0.0), fluid
 
 
-def fcg_solve(rhs, ff, shape, dx, p0=None, tol=1e-6, max_cycles=100, flexible=True, coarse_iterations=64):
+def fcg_solve(rhs, ff, shape, dx, p0=None, tol=1e-6, max_cycles=100, flexible=True, coarse_iterations=64,
+              pre_smooth=2, post_smooth=4):
     """Flexible CG (Notay, truncation 1) preconditioned by one FP32 W-cycle from zero, with the
     pressure, residual and scalars in FP64 (the product's tolerance-mode iteration; the reference
     has no counterpart). ``flexible=False`` is plain refinement p += W(r). ``coarse_iterations``:
-    red-black iterations of each coarsest-level solve in the W-cycle (the reference's 64 by default).
+    red-black iterations of each coarsest-level solve in the W-cycle (the reference's 64 by default);
+    ``pre_smooth``/``post_smooth``: its smoothing sweeps per level (the reference's 2 and 4).
     Returns the FP64 pressure and the relative-residual history (one entry per W-cycle, the first
     for p0)."""
     levels = Levels(shape)
@@ -366,7 +368,8 @@ def fcg_solve(rhs, ff, shape, dx, p0=None, tol=1e-6, max_cycles=100, flexible=Tr
     while hist[-1] > tol and len(hist) <= max_cycles:
         r32 = r.astype(np.float32)
         e = np.zeros(shape, np.float32)
-        levels.w_cycle(e, r32, ff32, op32, F32(float(dx)), coarse=int(coarse_iterations))
+        levels.w_cycle(e, r32, ff32, op32, F32(float(dx)), pre=int(pre_smooth), post=int(post_smooth),
+                       coarse=int(coarse_iterations))
         z = np.where(fluid, e, np.float32(0)).astype(np.float64)
         if flexible:
             az = apply_operator64(z, ff32, op64, dx)[0]

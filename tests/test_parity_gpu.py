@@ -372,8 +372,9 @@ def test_iterative_refinement_reaches_tolerance(backend, oracle, method):
     assert np.array_equal(got, oracle.neumann_domain_bc(got, shape))
 
 
-@pytest.mark.parametrize("method,coarse", [("fcg", 64), ("refine", 64), ("fcg", 4), ("fcg", 0)])
-def test_refinement_history_matches_oracle(backend, oracle, method, coarse):
+@pytest.mark.parametrize("method,coarse,smooth", [("fcg", 64, (2, 4)), ("refine", 64, (2, 4)), ("fcg", 4, (2, 4)),
+                                                  ("fcg", 0, (2, 4)), ("fcg", 4, (1, 1)), ("fcg", 4, (1, 2))])
+def test_refinement_history_matches_oracle(backend, oracle, method, coarse, smooth):
     """Every W-cycle of the GPU iteration against the oracle's restatement (same FP32 W-cycle, with
     the reference's or fewer coarsest-level iterations, FP64 accumulation and scalars; only summation
     orders differ)."""
@@ -383,7 +384,7 @@ def test_refinement_history_matches_oracle(backend, oracle, method, coarse):
     ff, _, _ = random_system(shape, 6)
     dt, rho = 1.0 / 240.0, 1000.0
     ps = pressure_solve.PressureSolver(backend, shape, float(dx), method=method, autotune=False,
-                                       coarse_iterations=coarse)
+                                       coarse_iterations=coarse, pre_smooth=smooth[0], post_smooth=smooth[1])
     P = torch.zeros(shape, dtype=torch.float32, device="cuda")
     ps.solve((dev(u), dev(v), dev(w)), dev(ff), P, dt, rho, tol=1e-3, use_graph=False)  # builds the system
     h = ps.hierarchy
@@ -398,7 +399,7 @@ def test_refinement_history_matches_oracle(backend, oracle, method, coarse):
         got.append(ps._relative(h.norms))
     orhs = oracle.pressure_rhs(u, v, w, ff, dx, dt, rho, shape)
     x, want = oracle.fcg_solve(orhs, ff, shape, dx, p0=p0, tol=0.0, max_cycles=8, flexible=(method == "fcg"),
-                               coarse_iterations=coarse)
+                               coarse_iterations=coarse, pre_smooth=smooth[0], post_smooth=smooth[1])
     np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-14)  # FP64 summation orders differ
     assert want[-1] < 1e-3 * want[0]
     scale = np.abs(x).max()
@@ -614,18 +615,22 @@ def test_revoxelising_a_static_collider_every_step_changes_nothing(backend):
 
 
 
-def test_steps_with_fewer_coarse_iterations(backend):
+@pytest.mark.parametrize("smooth", [(2, 4), (1, 1)])
+def test_steps_with_fewer_coarse_iterations(backend, smooth):
     """Tolerance-mode steps with 4 instead of the reference's 64 coarsest-level iterations in the
-    W-cycle preconditioner reach the tolerance every step in about as many cycles."""
+    W-cycle preconditioner (and with fewer smoothing sweeps) reach the tolerance every step in about as
+    many cycles."""
     s = scenes.block(48)
     pos, vel = scenes.seed_particles(s)
     totals = {}
     for k in (64, 4):
-        opts = solver.StepOptions(flip_ratio=0.95, tol=1e-6, gravity=s.gravity, coarse_iterations=k)
+        opts = solver.StepOptions(flip_ratio=0.95, tol=1e-6, gravity=s.gravity, coarse_iterations=k,
+                                  pre_smooth=smooth[0], post_smooth=smooth[1])
         sim = solver.FlipSolver(backend, s.grid_shape, s.dx, pos, vel, dt=s.dt, options=opts)
         stats = [sim.step() for _ in range(4)]
         assert all(st.rel_residual <= 1e-6 for st in stats)
         assert sim.pressure_solver.coarse_iterations == k
+        assert (sim.pressure_solver.pre_smooth, sim.pressure_solver.post_smooth) == smooth
         totals[k] = sum(st.cycles for st in stats)
     assert totals[4] <= totals[64] + 4, totals
     assert backend.device_error() == 0
