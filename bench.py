@@ -44,6 +44,9 @@ SMOOTHING_CHOICES = ((2, 4), (1, 2), (1, 1))  # (pre, post); (2, 4): the referen
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
                      "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
+# fluid tiles listed when the tile sweep above was captured (bench.py --case sweep0): its traffic is scaled to
+# the tile count of the measured launch (the sweep streams each listed tile and its stencil neighbours)
+NCU_TILES_AT_CAPTURE = {"k_rbgs_colour_tiles<true,4>": 5715}
 
 
 def parse_args():
@@ -749,6 +752,8 @@ def our_arm(args):
     peak, peak_kind = measured_peak_hbm()
     kernel = "k_rbgs_colour_tiles<true,4>" if vec else "k_rbgs_colour_tiles<true,1>"
     traffic = NCU_TRAFFIC_BYTES.get(kernel)
+    if traffic is not None and kernel in NCU_TILES_AT_CAPTURE:
+        traffic = int(round(traffic * tiles0 / NCU_TILES_AT_CAPTURE[kernel]))
     roofline = {"kernel": f"{kernel} (level-0 red-black Gauss-Seidel on the {tiles0} fluid tiles of "
                           f"{int(h.kernels.lib.clb_mg_tile_capacity(*scene.grid_shape, 1))}, one colour per launch)",
                 "bound": "hbm", "tile_cells": cells,
