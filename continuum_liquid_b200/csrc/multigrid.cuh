@@ -562,6 +562,28 @@ constexpr int RN_THREADS = 256;
 // pass; the per-lane summation order over fluid cells is unchanged.
 enum { RES_NORM = 0, RES_IR = 1, RES_FCG = 2 };
 
+// Whether row `base` (nz cells of the packed finest operator) holds a fluid cell, for the whole warp:
+// one 8-byte load per lane per 256 cells (when the row starts 8-byte aligned) instead of the per-cell
+// byte loads a row without fluid would otherwise cost. Skipping such a row changes no sum: none of its
+// cells contributes.
+__device__ __forceinline__ bool row_has_fluid(const uint8_t* __restrict__ op0, i64 base, int nz, int lane) {
+    bool any = false;
+    if ((((uintptr_t)(op0 + base)) & 7) == 0) {
+        for (int k = lane * 8; k < nz; k += 256) {
+            const int n = nz - k < 8 ? nz - k : 8;
+            if (n == 8) {
+                const uint2 w = __ldg(reinterpret_cast<const uint2*>(op0 + base + k));
+                any |= ((w.x | w.y) & 0x40404040u) != 0u;
+            } else {
+                for (int q = 0; q < n; ++q) any |= (__ldg(op0 + base + k + q) & 64u) != 0u;
+            }
+        }
+    } else {
+        for (int k = lane; k < nz; k += 32) any |= (__ldg(op0 + base + k) & 64u) != 0u;
+    }
+    return __any_sync(0xffffffffu, any);
+}
+
 // Block `blk` of `nblk` blocks sharing the rows; its partial sums go to *partial.
 template <typename PT, int MODE, bool SKIP = false>
 __device__ __forceinline__ void residual_rows_block(int blk, int nblk, const PT* __restrict__ p_in,
@@ -591,6 +613,7 @@ __device__ __forceinline__ void residual_rows_block(int blk, int nblk, const PT*
         const int i = r / ny, j = r - i * ny;
         const bool row_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
         const int base = r * nz;
+        if (SKIP && MODE != RES_NORM && (!row_in || !row_has_fluid(op0, base, nz, lane))) continue;
         for (int k = lane; k < nz; k += 32) {
             const int c = base + k;
             if (SKIP && MODE != RES_NORM && !(row_in && k >= 1 && k <= nz - 2 && (__ldg(op0 + c) & 64u))) continue;
@@ -671,6 +694,7 @@ __device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* _
         const int i = q / ny, j = q - i * ny;
         if (i < 1 || i > nx - 2 || j < 1 || j > ny - 2) continue;
         const int base = q * nz;
+        if (!row_has_fluid(op0, base, nz, lane)) continue;
         for (int k = lane; k < nz; k += 32) {
             const int c = base + k;
             const uint32_t o = __ldg(op0 + c);
