@@ -222,7 +222,6 @@ __device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int an
         else a[c] = v;
     };
     __syncthreads();  // staging and the caller's writes to shared memory are complete
-    for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) spb[c] = 0.0f;  // multigrid.cl:114
 
     const int asx = any * anz, asy = anz, bsx = bny * bnz, bsy = bnz;
     const int la = (anx * any * anz) / 2 + 1, lb = CB / 2 + 1;
@@ -277,34 +276,61 @@ __device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int an
 
     __syncthreads();
     smooth_a(pre);
-    // restriction of the residual (multigrid.cl:90-180, right-hand-side part) into B's owners
+    // restriction of the residual (multigrid.cl:90-180, right-hand-side part) of B's fluid cells (both
+    // lists): eight threads per coarse cell, thread l forms the residual of child l = 4 di + 2 dj + dk
+    // (interior fluid children only), and the group's first thread adds them in that order, as one
+    // thread running over di, dj, dk does. The sums go to B's p (free until the coarse solves), from
+    // which B's owners take them.
+    {
+        const int lane = threadIdx.x & 31, l = threadIdx.x & 7;
+        const int n0 = S.count[2], nb = n0 + S.count[3];
+        for (int g0 = 0; g0 < nb; g0 += BOTTOM_THREADS / 8) {  // the same trip count in every thread
+            const int g = g0 + (int)(threadIdx.x >> 3);
+            int cb = -1;
+            float r = 0.0f;
+            bool present = false;
+            if (g < nb) {
+                cb = g < n0 ? S.list_b[g] : S.list_b[lb + g - n0];
+                const int I = cb / bsx, J = (cb / bsy) % bny, K = cb % bnz;
+                const int i = 2 * I - 1 + (l >> 2), j = 2 * J - 1 + ((l >> 1) & 1), k = 2 * K - 1 + (l & 1);
+                if (interior(i, j, k, anx, any, anz)) {
+                    const int f = (i * any + j) * anz + k;
+                    const float4 o = soa[f];
+                    if (o.x >= 0.0f) {
+                        const float ws = o.y * spa[f + asx] + soa[f - asx].y * spa[f - asx] + o.z * spa[f + asy] +
+                                         soa[f - asy].z * spa[f - asy] + o.w * spa[f + 1] + soa[f - 1].w * spa[f - 1];
+                        r = sba[f] - (ws - o.x * spa[f]) * inv_delta2;
+                        present = true;
+                    }
+                }
+            }
+            const unsigned have = __ballot_sync(0xffffffffu, present) >> (lane & ~7);
+            float v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = __shfl_sync(0xffffffffu, r, (lane & ~7) + q);
+            if (l == 0 && cb >= 0) {
+                float rhs = 0.0f;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if ((have >> q) & 1u) rhs += v[q];
+                spb[cb] = rhs;
+            }
+        }
+    }
+    __syncthreads();
     float bvals[2][KB];
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KB; ++m) {
-            float rhs = 0.0f;
-            if (B[colour][m].d >= 0.0f) {  // a fluid cell (slots without a cell and air cells hold -1)
-                const int c = B[colour][m].c;
-                const int I = c / bsx, J = (c / bsy) % bny, K = c % bnz;
-                const int si = 1 + 2 * (I - 1), sj = 1 + 2 * (J - 1), sk = 1 + 2 * (K - 1);
-                for (int di = 0; di < 2; ++di)
-                    for (int dj = 0; dj < 2; ++dj)
-                        for (int dk = 0; dk < 2; ++dk) {
-                            const int i = si + di, j = sj + dj, k = sk + dk;
-                            if (!interior(i, j, k, anx, any, anz)) continue;
-                            const int f = (i * any + j) * anz + k;
-                            const float4 o = soa[f];
-                            if (o.x < 0.0f) continue;
-                            const float ws = o.y * spa[f + asx] + soa[f - asx].y * spa[f - asx] + o.z * spa[f + asy] +
-                                             soa[f - asy].z * spa[f - asy] + o.w * spa[f + 1] +
-                                             soa[f - 1].w * spa[f - 1];
-                            rhs += sba[f] - (ws - o.x * spa[f]) * inv_delta2;
-                        }
-            }
+            // a fluid cell (slots without a cell and air cells hold -1)
+            const float rhs = B[colour][m].d >= 0.0f ? spb[B[colour][m].c] : 0.0f;
             bvals[colour][m] = rhs;
             B[colour][m].d2b = d2 * rhs;
         }
+    __syncthreads();
+    for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) spb[c] = 0.0f;  // multigrid.cl:114
+    __syncthreads();
     if (btile) {
         // two coarse solves of the W (multigrid.py:127-170), pre + coarse_iters iterations each
         const int iterations = 2 * (pre + coarse_iters);
