@@ -1044,6 +1044,28 @@ int clb_mg_residual_partials(int64_t cells) {
     return (int)(need < cap ? (need > 0 ? need : 1) : cap);
 }
 
+extern "C++" {
+namespace {
+// Grid of a row kernel (k_residual_rows, k_fcg_dots): at most the blocks that are resident on the
+// device at once, so that no partial second wave waits for the first (the rows are spread over the
+// blocks' warps in any case). Never more than clb_mg_residual_partials, the callers' partial count.
+template <auto KERNEL>
+int row_grid(i64 cells) {
+    static const int per_sm = [] {  // once per kernel
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, KERNEL, RN_THREADS, 0) != cudaSuccess) {
+            (void)cudaGetLastError();
+            n = 0;
+        }
+        return n;
+    }();
+    const int want = clb_mg_residual_partials(cells);
+    const int resident = per_sm * (g_sm_count > 0 ? g_sm_count : 148);
+    return resident >= 1 && resident < want ? resident : want;
+}
+}  // namespace
+}  // extern "C++"
+
 int clb_mg_residual_norms(const void* p, int p_is_double, const float* b, const uint8_t* op0, float delta, int nx,
                           int ny, int nz, float* r_out, void* partials, double* out, void* stream) {
     CLB_GRID_ARGS_OK(nx, ny, nz);
@@ -1072,15 +1094,18 @@ int clb_mg_ir_step(const double* p64_in, const float* e, double* p64_out, const 
     CLB_REQUIRE(p64_in && e && p64_out && b && op0 && r_out && partials && out, "mg_ir_step: null pointer");
     CLB_REQUIRE(p64_in != p64_out, "mg_ir_step: p64_out must not alias p64_in");
     const i64 C = (i64)nx * ny * nz;
-    const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    if (g_skip_air)
+    int blocks;
+    if (g_skip_air) {
+        blocks = row_grid<k_residual_rows<double, RES_IR, true>>(C);
         launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_IR, true>, p64_in, e, p64_out, b, op0, inv_delta2,
                                          nx, ny, nz, r_out, (double2*)partials, nullptr, nullptr, nullptr);
-    else
+    } else {
+        blocks = clb_mg_residual_partials(C);
         launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_IR, false>, p64_in, e, p64_out, b, op0,
                                          inv_delta2, nx, ny, nz, r_out, (double2*)partials, nullptr, nullptr, nullptr);
+    }
     CLB_LAUNCH_CHECK("k_residual_rows");
     launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
@@ -1092,7 +1117,7 @@ int clb_mg_fcg_dots(const float* z, const float* d, const float* r, const uint8_
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(z && d && r && op0 && partials4 && state, "mg_fcg_dots: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    const int blocks = clb_mg_residual_partials(C);
+    const int blocks = row_grid<k_fcg_dots>(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
     launch(blocks, RN_THREADS, 0, s)(k_fcg_dots, z, d, r, op0, inv_delta2, nx, ny, nz, (Sum4*)partials4);
@@ -1110,15 +1135,18 @@ int clb_mg_fcg_step(const double* p64_in, const float* z, const float* d_in, dou
                 "mg_fcg_step: null pointer");
     CLB_REQUIRE(p64_in != p64_out && d_in != d_out, "mg_fcg_step: outputs must not alias inputs");
     const i64 C = (i64)nx * ny * nz;
-    const int blocks = clb_mg_residual_partials(C);
     const double inv_delta2 = 1.0 / ((double)delta * (double)delta);
     cudaStream_t s = CLB_STREAM(stream);
-    if (g_skip_air)
+    int blocks;
+    if (g_skip_air) {
+        blocks = row_grid<k_residual_rows<double, RES_FCG, true>>(C);
         launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_FCG, true>, p64_in, z, p64_out, b, op0,
                                          inv_delta2, nx, ny, nz, r_out, (double2*)partials, d_in, d_out, state);
-    else
+    } else {
+        blocks = clb_mg_residual_partials(C);
         launch(blocks, RN_THREADS, 0, s)(k_residual_rows<double, RES_FCG, false>, p64_in, z, p64_out, b, op0,
                                          inv_delta2, nx, ny, nz, r_out, (double2*)partials, d_in, d_out, state);
+    }
     CLB_LAUNCH_CHECK("k_residual_rows");
     launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
