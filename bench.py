@@ -327,9 +327,10 @@ def sweep_case(args):
 
 
 def workload_config(size, n_particles, args, coarse_iterations=COARSE_ITERATION_CHOICES[0],
-                    smoothing=SMOOTHING_CHOICES[0]):
+                    smoothing=SMOOTHING_CHOICES[0], fp16_levels=None):
     k = int(coarse_iterations)
     pre, post = smoothing
+    storage = (f", levels {fp16_levels[0][0]}^3 and coarser stored in FP16" if fp16_levels else "")
     return {
         "workload": f"flip_step_block_{size}^3",
         "grid": [size, size, size],
@@ -338,9 +339,10 @@ def workload_config(size, n_particles, args, coarse_iterations=COARSE_ITERATION_
         "dt": 1.0 / 240.0,
         "flip_ratio": 0.95,
         "pressure_tolerance": TOL,
-        "pressure_solver": (f"flexible CG preconditioned by one FP32 W-cycle (pre {pre}, post {post}, coarse "
-                            f"{pre}+{k}), FP64 pressure, residual and norms" if args.method == "fcg" else
-                            f"W-cycle (pre {pre}, post {post}, coarse {pre}+{k}) in FP64 iterative refinement"),
+        "pressure_solver": (f"flexible CG preconditioned by one W-cycle computed in FP32 (pre {pre}, post {post}, "
+                            f"coarse {pre}+{k}{storage}), FP64 pressure, residual and norms" if args.method == "fcg"
+                            else f"W-cycle computed in FP32 (pre {pre}, post {post}, coarse {pre}+{k}{storage}) in "
+                                 f"FP64 iterative refinement"),
         "multigrid_levels": None,
         "l2": "inputs larger than L2 (particle state 24 B x N, grid fields 4 B x n^3 each)",
         "parallelism": "replicas" if args.gpus > 1 else "single",
@@ -772,7 +774,8 @@ def our_arm(args):
 
     if rank == 0:
         config = workload_config(args.size, n, args, sim.options.coarse_iterations,
-                                 (sim.options.pre_smooth, sim.options.post_smooth))
+                                 (sim.options.pre_smooth, sim.options.post_smooth),
+                                 [list(s) for s in h.shapes[h.fp16_level:]] if h.fp16_level else None)
         config["multigrid_levels"] = [list(s) for s in h.shapes]
         config["sweep_kinds"] = h.sweeps()
         config["sweep_tuning_ms_per_iteration"] = h.tuning
