@@ -196,6 +196,60 @@ class FlipSolver:
         self.steps_done += 1
         return stats
 
+    def step_host(self, positions: torch.Tensor, velocities: torch.Tensor, chunks: int = 8) -> SolveStats:
+        """One step with the particle state making the host round trip that solver.py:252-306 makes
+        every step: ``positions`` and ``velocities`` (pinned float32 host tensors of shape (n, 3)) are
+        uploaded, the step runs, and the new state is downloaded into the same tensors.
+
+        The copies run in ``chunks`` pieces on two copy streams. In back-to-back calls a piece's upload
+        waits only for the previous call's download of that piece (which followed that call's step), so
+        the download of one call and the upload of the next overlap piece by piece: the link carries
+        both directions at once. The call returns once the work is enqueued: the host tensors hold the
+        new state after ``torch.cuda.synchronize()``. Work on the current stream after the call waits
+        for the download; between calls, the caller synchronises before it reads or changes the host
+        tensors or the particle state by other means."""
+        n = self.n
+        for name, t in (("positions", positions), ("velocities", velocities)):
+            if t.device.type != "cpu" or not t.is_pinned() or t.dtype != torch.float32 or tuple(t.shape) != (n, 3) \
+                    or not t.is_contiguous():
+                raise ValueError(f"step_host: {name} must be a contiguous pinned float32 host tensor of shape ({n}, 3)")
+        chunks = max(1, min(int(chunks), max(n, 1)))
+        if getattr(self, "_host_streams", None) is None:
+            self._host_streams = (torch.cuda.Stream(self.device), torch.cuda.Stream(self.device))
+            self._host_events: list = []
+        up, down = self._host_streams
+        compute = torch.cuda.current_stream(self.device)
+        bounds = [(n * c) // chunks for c in range(chunks + 1)]
+        previous = self._host_events if len(self._host_events) == chunks else None
+        if previous is None:
+            # the first call (or another piece count): the upload waits for all work so far
+            up.wait_stream(compute)
+            up.wait_stream(down)
+        with torch.cuda.stream(up):
+            for c in range(chunks):
+                a, b = bounds[c], bounds[c + 1]
+                if previous is not None:
+                    up.wait_event(previous[c])
+                self.particles[a:b].copy_(positions[a:b], non_blocking=True)
+                self.particle_velocity[a:b].copy_(velocities[a:b], non_blocking=True)
+        compute.wait_stream(up)
+        stats = self.step()
+        if self.n != n:
+            raise RuntimeError("step_host: the step changed the particle count; use step() with sources")
+        down.wait_stream(compute)
+        events = []
+        with torch.cuda.stream(down):
+            for c in range(chunks):
+                a, b = bounds[c], bounds[c + 1]
+                positions[a:b].copy_(self.particles[a:b], non_blocking=True)
+                velocities[a:b].copy_(self.particle_velocity[a:b], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(down)
+                events.append(ev)
+        self._host_events = events
+        compute.wait_stream(down)
+        return stats
+
     # -- host views -------------------------------------------------------------------------------
     def positions(self) -> np.ndarray:
         return self.particles[: self.n].cpu().numpy()
