@@ -358,7 +358,11 @@ int clb_grid_domain_bc(float* u, float* v, float* w, int nx, int ny, int nz, voi
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(u && v && w, "grid_domain_bc: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_grid_domain_bc<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, nx, ny, nz);
+    if (nx >= 3 && ny >= 3 && nz >= 3)  // the shell of cells the conditions change
+        k_grid_domain_bc_shell<<<blocks_for(shell_cells(nx, ny, nz, 1, 2), GT), GT, 0, CLB_STREAM(stream)>>>(
+            u, v, w, nx, ny, nz);
+    else
+        k_grid_domain_bc<<<blocks_for(C, GT), GT, 0, CLB_STREAM(stream)>>>(u, v, w, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_grid_domain_bc");
     return 0;
 }
@@ -405,7 +409,11 @@ static int neumann_domain_bc_impl(PT* pressure, int nx, int ny, int nz, void* st
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(pressure, "neumann_domain_bc: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    launch(blocks_for(C, GT), GT, 0, CLB_STREAM(stream))(k_neumann_domain_bc<PT>, pressure, nx, ny, nz);
+    if (nx >= 2 && ny >= 2 && nz >= 2)  // the shell of non-interior cells
+        launch(blocks_for(shell_cells(nx, ny, nz, 1, 1), GT), GT, 0, CLB_STREAM(stream))(
+            k_neumann_domain_bc_shell<PT>, pressure, nx, ny, nz);
+    else
+        launch(blocks_for(C, GT), GT, 0, CLB_STREAM(stream))(k_neumann_domain_bc<PT>, pressure, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_neumann_domain_bc");
     return 0;
 }

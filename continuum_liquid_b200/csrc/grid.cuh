@@ -81,6 +81,46 @@ __global__ void __launch_bounds__(GT) k_grid_domain_bc(float* u, float* v, float
     grid_domain_bc_at(c, u, v, w, nx, ny, nz);
 }
 
+// The shell of a grid: the cells within `lo` planes of a low face or `hi` planes of a high face on
+// some axis, counted without repeats (needs every extent >= lo + hi). The domain boundary conditions
+// change only such cells (grid_domain_bc: lo 1, hi 2; neumann_domain_bc: lo 1, hi 1), and since
+// their writes never feed their own reads, a launch over the shell alone leaves the same values as
+// one over the whole grid for a few percent of the threads.
+__host__ __device__ __forceinline__ i64 shell_cells(int nx, int ny, int nz, int lo, int hi) {
+    const i64 w = lo + hi;
+    return w * ny * nz + (nx - w) * w * nz + (nx - w) * (ny - w) * w;
+}
+
+// Shell cell t (< shell_cells): the lo + hi face planes of x, then the face rows of y in the other
+// planes, then the face cells of z in the other rows.
+__device__ __forceinline__ i64 shell_cell(i64 t, int nx, int ny, int nz, int lo, int hi) {
+    const int w = lo + hi;
+    auto side = [&](int q, int n) { return q < lo ? q : n - hi + (q - lo); };
+    const i64 a = (i64)w * ny * nz;
+    if (t < a) {
+        const i64 plane = (i64)ny * nz;
+        const int p = (int)(t / plane), r = (int)(t - p * plane);
+        return gidx(side(p, nx), r / nz, r % nz, ny, nz);
+    }
+    t -= a;
+    const i64 b = (i64)(nx - w) * w * nz;
+    if (t < b) {
+        const i64 slab = (i64)w * nz;
+        const int p = (int)(t / slab), r = (int)(t - p * slab);
+        return gidx(lo + p, side(r / nz, ny), r % nz, ny, nz);
+    }
+    t -= b;
+    const i64 rows = (i64)(ny - w) * w;
+    const int p = (int)(t / rows), r = (int)(t - p * rows);
+    return gidx(lo + p, lo + r / w, side(r % w, nz), ny, nz);
+}
+
+__global__ void __launch_bounds__(GT) k_grid_domain_bc_shell(float* u, float* v, float* w, int nx, int ny, int nz) {
+    const i64 t = (i64)blockIdx.x * GT + threadIdx.x;
+    if (t >= shell_cells(nx, ny, nz, 1, 2)) return;
+    grid_domain_bc_at(shell_cell(t, nx, ny, nz, 1, 2), u, v, w, nx, ny, nz);
+}
+
 // boundary_conditions.cl:99-119 grid_obstacle_bc
 __device__ __forceinline__ void grid_obstacle_bc_at(i64 c, float* __restrict__ u, float* __restrict__ v,
                                                           float* __restrict__ w, float* __restrict__ ff,
@@ -224,6 +264,15 @@ __global__ void __launch_bounds__(GT) k_neumann_domain_bc(PT* p, int nx, int ny,
     const i64 c = (i64)blockIdx.x * GT + threadIdx.x;
     if (c >= C) return;
     neumann_domain_bc_at<PT>(c, p, nx, ny, nz);
+}
+
+// The same over the grid's shell of non-interior cells only (shell_cells with lo = hi = 1).
+template <typename PT>
+__global__ void __launch_bounds__(GT) k_neumann_domain_bc_shell(PT* p, int nx, int ny, int nz) {
+    pdl_begin();
+    const i64 t = (i64)blockIdx.x * GT + threadIdx.x;
+    if (t >= shell_cells(nx, ny, nz, 1, 1)) return;
+    neumann_domain_bc_at<PT>(shell_cell(t, nx, ny, nz, 1, 1), p, nx, ny, nz);
 }
 
 }  // namespace clb
