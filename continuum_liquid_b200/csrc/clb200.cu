@@ -694,16 +694,32 @@ static void launch_rbgs_iter(const LevelView& v, bool big, int t, const float* i
 // runs as 6). Kinds 2, 3, 5 and 6 need the level's second buffer. All give identical values.
 // sparse: every cell without fluid holds 0 (inside a W-cycle, mg_tiles.cuh), so an FP32 level with a
 // tile list is swept on its fluid tiles only.
-int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s, bool sparse = false) {
+// Whether smooth(..., sparse = true) takes the fluid-tile colour sweeps on this level.
+bool tile_sweeps(const LevelView& v) {
+    const int vec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
+    return v.tiles && !v.half && (vec == 1 || (((uintptr_t)v.p) & 15) == 0);
+}
+
+// from_zero (level 0, tile sweeps, iterations >= 1): the first colour treats p as 0 (clb_mg_hierarchy
+// zero_outside = 2).
+int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s, bool sparse = false,
+           bool from_zero = false) {
     const i64 C = (i64)v.nx * v.ny * v.nz;
     const int kind = v.sweep == 0 ? (v.half ? 4 : 1) : v.sweep;
     const int vec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
-    if (sparse && v.tiles && !v.half && (vec == 1 || (((uintptr_t)v.p) & 15) == 0)) {
+    if (sparse && tile_sweeps(v)) {
         const unsigned grid = tile_grid(v);
         const dim3 block(32, 4);
         for (int it = 0; it < iterations; ++it)
             for (int parity = 0; parity < 2; ++parity) {
-                if (v.l0 && vec == 4)
+                if (from_zero && v.l0 && it == 0 && parity == 0) {
+                    if (vec == 4)
+                        launch(grid, block, 0, s)(k_rbgs_colour_tiles<true, 4, true>, v.tiles, v.tile_count, v.p,
+                                                  v.b, v.op0, nullptr, nullptr, delta, parity, v.nx, v.ny, v.nz);
+                    else
+                        launch(grid, block, 0, s)(k_rbgs_colour_tiles<true, 1, true>, v.tiles, v.tile_count, v.p,
+                                                  v.b, v.op0, nullptr, nullptr, delta, parity, v.nx, v.ny, v.nz);
+                } else if (v.l0 && vec == 4)
                     launch(grid, block, 0, s)(k_rbgs_colour_tiles<true, 4>, v.tiles, v.tile_count, v.p, v.b, v.op0,
                                               nullptr, nullptr, delta, parity, v.nx, v.ny, v.nz);
                 else if (v.l0)
@@ -934,18 +950,32 @@ int bottom_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int co
 }
 
 // multigrid.py:53-187 w_cycle
+// zero_outside = 2 on level 0: x counts as 0 inside the fluid tiles (and is 0 outside them). When the
+// first thing done to level 0 is a fluid-tile colour sweep, that sweep ignores x (from_zero);
+// otherwise x is zeroed here.
+int level0_zero(const clb_mg_hierarchy* h, const LevelView& v, int first_sweeps, bool sweep_first, bool sparse,
+                cudaStream_t s, bool& from_zero) {
+    from_zero = false;
+    if (h->zero_outside != 2) return 0;
+    from_zero = sweep_first && sparse && first_sweeps >= 1 && tile_sweeps(v);
+    if (from_zero) return 0;
+    return check_call(cudaMemsetAsync(v.p, 0, (size_t)v.nx * v.ny * v.nz * sizeof(float), s), "zero level-0 x");
+}
+
 int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int pre, int post, int coarse_iters,
             cudaStream_t s) {
     const LevelView v = level_view(h, level, x, rhs);
+    // coarse levels hold 0 outside the fluid (zeroed by clb_mg_build_coarse and the restriction);
+    // level 0 does when the caller says so
+    const bool sparse = level > 0 || h->zero_outside != 0;
+    bool from_zero = false;
+    if (level == 0 && level0_zero(h, v, pre, level != h->levels - 1, sparse, s, from_zero)) return 1;
     if (level == h->levels - 1) return coarse_solve(v, h->delta, pre + coarse_iters, s);
     const int cluster = cluster_visit(h, level, pre, post, coarse_iters, s);
     if (cluster != 0) return cluster < 0 ? 1 : 0;
     const int bottom = bottom_visit(h, level, pre, post, coarse_iters, s);
     if (bottom != 0) return bottom < 0 ? 1 : 0;
-    // coarse levels hold 0 outside the fluid (zeroed by clb_mg_build_coarse and the restriction);
-    // level 0 does when the caller says so
-    const bool sparse = level > 0 || h->zero_outside != 0;
-    if (smooth(v, h->delta, pre, s, sparse)) return 1;
+    if (smooth(v, h->delta, pre, s, sparse, from_zero)) return 1;
     const LevelView c = level_view(h, level + 1, x, rhs);
     const i64 Cc = (i64)c.nx * c.ny * c.nz;
     if (!c.half && !v.half && c.tiles) {  // restriction of the coarse fluid tiles (inactive cells hold 0)
@@ -1033,8 +1063,11 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
     CLB_REQUIRE(level >= 0 && level < h->levels, "mg_smooth: level %d outside 0..%d", level, h->levels - 1);
     CLB_REQUIRE(iterations >= 0, "mg_smooth: negative iterations");
     CLB_REQUIRE(level > 0 || (x && rhs), "mg_smooth: null level-0 array");
-    return smooth(level_view(h, level, x, rhs), h->delta, iterations, CLB_STREAM(stream),
-                  h->zero_outside != 0 && h->tile_counts != nullptr);
+    const LevelView v = level_view(h, level, x, rhs);
+    const bool sparse = h->zero_outside != 0 && h->tile_counts != nullptr;
+    bool from_zero = false;
+    if (level == 0 && level0_zero(h, v, iterations, true, sparse, CLB_STREAM(stream), from_zero)) return 1;
+    return smooth(v, h->delta, iterations, CLB_STREAM(stream), sparse, from_zero);
 }
 
 int clb_mg_set_option(int option, int value) {

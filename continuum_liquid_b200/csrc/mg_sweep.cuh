@@ -216,8 +216,11 @@ namespace clb {
 // row is read with 16-byte loads (needs nz % 4 == 0); every cell of the vector is written back
 // (unchanged cells of the other colour keep their value, cells that are not fluid are set to 0, as
 // rbgs_step does). Each update keeps the reference's term order.
+// Z: the colour runs as if p held 0 at every cell (p is written but not read): the updated cells get
+// (0 - delta^2 b) / d, which is the update's value when every neighbour is 0 (each weighted term is
+// +0), and every other cell of the vector is set to 0.
 // Block (bx, by, bz) of the launch described above (block shape (32, 4)).
-template <bool L0, int VEC>
+template <bool L0, int VEC, bool Z = false>
 __device__ __forceinline__ void rbgs_colour_at(int bx, int by, int bz, float* p, const float* __restrict__ b,
                                                const uint8_t* __restrict__ op0, const float4* __restrict__ opc,
                                                const uint8_t* __restrict__ mask, float delta, int parity, int nx,
@@ -232,7 +235,10 @@ __device__ __forceinline__ void rbgs_colour_at(int bx, int by, int bz, float* p,
     const float d2 = delta * delta;
     float pc[VEC], out[VEC];
     uint32_t fl[VEC];
-    if (VEC == 4) {
+    if (Z) {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) pc[q] = 0.0f;
+    } else if (VEC == 4) {
         const float4 v = *reinterpret_cast<const float4*>(p + c0);
         pc[0] = v.x;
         pc[1] = v.y;
@@ -282,10 +288,12 @@ __device__ __forceinline__ void rbgs_colour_at(int bx, int by, int bz, float* p,
                 wzm = __ldg(opc + c - 1).w;
             }
             if (!(d > 0.0f)) continue;
-            const float kp = (q + 1 < VEC) ? pc[q + 1] : p[c + 1];
-            const float km = (q > 0) ? pc[q - 1] : p[c - 1];
-            const float ws = wxp * p[c + sx] + wxm * p[c - sx] + wyp * p[c + sy] + wym * p[c - sy] + wzp * kp +
-                             wzm * km;
+            float ws = 0.0f;
+            if (!Z) {
+                const float kp = (q + 1 < VEC) ? pc[q + 1] : p[c + 1];
+                const float km = (q > 0) ? pc[q - 1] : p[c - 1];
+                ws = wxp * p[c + sx] + wxm * p[c - sx] + wyp * p[c + sy] + wym * p[c - sy] + wzp * kp + wzm * km;
+            }
             out[q] = (ws - d2 * __ldg(b + c)) / d;
         }
     }

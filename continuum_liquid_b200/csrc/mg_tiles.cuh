@@ -51,8 +51,9 @@ __global__ void __launch_bounds__(256) k_mg_tiles(const uint8_t* __restrict__ fl
 }
 
 // Red-black colour on the listed tiles: block b handles tiles b, b + gridDim.x, ... with the body of
-// the dense colour sweep (rbgs_colour_at; VEC = 4 on the finest level when its tiles are 128 cells).
-template <bool L0, int VEC>
+// the dense colour sweep (rbgs_colour_at; VEC = 4 on the finest level when its tiles are 128 cells;
+// Z: as if p were 0 on entry).
+template <bool L0, int VEC, bool Z = false>
 __global__ void __launch_bounds__(128) k_rbgs_colour_tiles(const int* __restrict__ list, const int* __restrict__ count,
                                                             float* p, const float* __restrict__ b,
                                                             const uint8_t* __restrict__ op0,
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(128) k_rbgs_colour_tiles(const int* __restrict
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
         const int tile = __ldg(list + t);
         const int kb = tile % kg, rest = tile / kg;
-        rbgs_colour_at<L0, VEC>(kb, rest % jg, rest / jg, p, b, op0, opc, mask, delta, parity, nx, ny, nz);
+        rbgs_colour_at<L0, VEC, Z>(kb, rest % jg, rest / jg, p, b, op0, opc, mask, delta, parity, nx, ny, nz);
     }
 }
 

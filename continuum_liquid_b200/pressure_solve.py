@@ -171,9 +171,11 @@ class PressureSolver:
         """One refinement from FP64 buffer ``src`` into the other one."""
         h = self.hierarchy
         delta = float(FIELD_DTYPE(self.dx))
-        self.correction.zero_()
+        # the correction starts from 0: its buffer is 0 outside the fluid (zeroed once per solve, and
+        # the W-cycle writes 0 to every cell that is not fluid), so the W-cycle's first sweep ignores
+        # the previous correction at fluid cells instead of a fill of the whole buffer
         h.w_cycle(self.correction, self.residual, pre_smooth=self.pre_smooth, post_smooth=self.post_smooth,
-                  coarse_iterations=self.coarse_iterations, queue=queue, x_zero_outside=True)
+                  coarse_iterations=self.coarse_iterations, queue=queue, x_from_zero=True)
         if self.method == "fcg":
             self.kernels.call("clb_mg_fcg_dots", self.correction, self.direction[src], self.residual, h.op0, delta,
                               *self.grid_shape, self.fcg_partials, self.fcg_state, stream=queue)
@@ -201,8 +203,7 @@ class PressureSolver:
             before = self.kernels.launch_count()
             with torch.cuda.graph(graph):
                 self.refine_once(src)
-            # +1: the correction zero-fill is a torch kernel captured with ours
-            self.graph_launches = self.kernels.launch_count() - before + 1
+            self.graph_launches = self.kernels.launch_count() - before
             self._graphs[src] = graph
         else:
             self._graphs[src].replay()
@@ -257,8 +258,10 @@ class PressureSolver:
             self.direction[0].zero_()
             self.direction[1].zero_()
             self.fcg_state.zero_()
-        # the step kernels skip cells outside the fluid: both FP64 buffers start at 0 there
+        # the step kernels skip cells outside the fluid: both FP64 buffers start at 0 there; so does
+        # the correction (the fluid of the last solve may have moved)
         self.p64[1].zero_()
+        self.correction.zero_()
         self.kernels.call("clb_mg_ir_init", pressure, h.op0, self.p64[0], *self.grid_shape)
         rel = self._relative(h.residual_norms(self.p64[0], self.rhs, r_out=self.residual))
         if warm_start is not None:

@@ -232,6 +232,10 @@ typedef struct clb_mg_hierarchy {
     int32_t zero_outside;                /* 1: level-0 x is 0 at every cell that is not fluid when
                                             clb_mg_w_cycle is called (the correction of the tolerance
                                             mode), so level-0 sweeps may skip tiles without fluid;
+                                            2: as 1, and x counts as 0 inside the level-0 fluid tiles
+                                            too (a correction from zero whose buffer still holds the
+                                            previous one there): the first colour sweep ignores x, or
+                                            x is zeroed first;
                                             0: level-0 sweeps cover the whole grid */
 } clb_mg_hierarchy;
 
@@ -254,7 +258,8 @@ int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pr
 /* multigrid.py:190-220 smooth: `iterations` red-black Gauss-Seidel iterations on one level (level 0
  * uses x and rhs; coarse levels their own p and b). With h->zero_outside = 1 and tile lists built by
  * clb_mg_build_coarse, the caller guarantees that the level's p (x on level 0) is 0 at every cell
- * that is not fluid, and an FP32 level is swept on its fluid tiles only (same values). */
+ * that is not fluid, and an FP32 level is swept on its fluid tiles only (same values); with 2, level-0
+ * x counts as 0 inside the fluid tiles as well. */
 int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int iterations, void* stream);
 
 /* Process-wide multigrid options (host-side switches, no device work):

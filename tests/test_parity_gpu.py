@@ -675,3 +675,27 @@ def test_fluid_tile_w_cycle_matches_oracle(backend, oracle, shape):
     assert np.array_equal(results[True], q)
     assert np.array_equal(results[False], q)
     assert backend.device_error() == 0
+
+
+@pytest.mark.parametrize("shape,pre", [((66, 70, 68), 1), ((40, 36, 44), 2), ((40, 36, 44), 0)])
+def test_w_cycle_from_zero_ignores_the_previous_correction(backend, oracle, shape, pre):
+    """A W-cycle told that the correction starts from zero (x_from_zero: its first level-0 sweep ignores
+    x, or x is zeroed when no sweep comes first) gives the reference's W-cycle from a zero x, although
+    the buffer still holds a previous correction at the fluid cells."""
+    dx = F32(1.0 / shape[0])
+    ff = corner_block_system(shape, 43)
+    u, v, w = (np.random.default_rng(52 + a).standard_normal(shape).astype(F32) for a in range(3))
+    orhs = oracle.pressure_rhs(u, v, w, ff, dx, 1.0 / 240.0, 1000.0, shape)
+    oops = oracle.build_finest_operator(ff, shape)
+    h = multigrid.MultigridHierarchy(backend, shape, float(dx))
+    rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    h.rhs_operator((dev(u), dev(v), dev(w)), dev(ff), rhs, 1.0 / 240.0, 1000.0)
+    h.build_coarse()
+    P = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    h.w_cycle(P, rhs, pre_smooth=pre, coarse_iterations=8, x_zero_outside=True)  # a previous correction
+    assert P.abs().max() > 0
+    h.w_cycle(P, rhs, pre_smooth=pre, coarse_iterations=8, x_from_zero=True)
+    q = np.zeros(shape, F32)
+    oracle.Levels(shape).w_cycle(q, orhs, ff, oops, dx, pre=pre, coarse=8)
+    assert np.array_equal(host(P), q)
+    assert backend.device_error() == 0
