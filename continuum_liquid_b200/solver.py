@@ -168,8 +168,10 @@ class FlipSolver:
         self.last_solve = stats
         return stats
 
-    def post_solve(self, queue=None) -> None:
-        """Stages 6-7: projection, BCs and the fused particle update."""
+    def post_solve(self, queue=None, piece_bounds=None, piece_done=None) -> None:
+        """Stages 6-7: projection, BCs and the fused particle update. ``piece_bounds`` (ascending
+        particle indices from 0 to n) splits the particle update into one launch per piece, each
+        followed by ``piece_done(piece)`` (the update of one particle does not depend on another's)."""
         k, o, gs = self.kernels, self.options, self.grid_shape
         vel = (self.u, self.v, self.w)
         ps = self.pressure_solver
@@ -182,9 +184,18 @@ class FlipSolver:
         boundary_conditions.grid_domain_bc(k, queue, vel, gs)
         if self.obstacle is not None:
             boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)
-        particle_methods.particle_update(k, queue, self.particles, self.particle_velocity, vel,
-                                         (self.u_work, self.v_work, self.w_work), self.obstacle, self.n, gs, self.dx,
-                                         self.dt, o.flip_ratio)
+        if piece_bounds is None:
+            particle_methods.particle_update(k, queue, self.particles, self.particle_velocity, vel,
+                                             (self.u_work, self.v_work, self.w_work), self.obstacle, self.n, gs,
+                                             self.dx, self.dt, o.flip_ratio)
+            return
+        for c in range(len(piece_bounds) - 1):
+            a, b = piece_bounds[c], piece_bounds[c + 1]
+            if b > a:
+                particle_methods.particle_update(k, queue, self.particles[a:b], self.particle_velocity[a:b], vel,
+                                                 (self.u_work, self.v_work, self.w_work), self.obstacle, b - a, gs,
+                                                 self.dx, self.dt, o.flip_ratio)
+            piece_done(c)
 
     def step(self) -> SolveStats:
         if self.n == 0:
@@ -201,9 +212,10 @@ class FlipSolver:
         every step: ``positions`` and ``velocities`` (pinned float32 host tensors of shape (n, 3)) are
         uploaded, the step runs, and the new state is downloaded into the same tensors.
 
-        The copies run in ``chunks`` pieces on two copy streams. In back-to-back calls a piece's upload
-        waits only for the previous call's download of that piece (which followed that call's step), so
-        the download of one call and the upload of the next overlap piece by piece: the link carries
+        The copies run in ``chunks`` pieces on two copy streams. The step's last stage, the particle
+        update, runs one launch per piece, and a piece's download starts once its update is done. In
+        back-to-back calls a piece's upload waits only for the previous call's download of that piece,
+        so the download of one call and the upload of the next overlap piece by piece: the link carries
         both directions at once. The call returns once the work is enqueued: the host tensors hold the
         new state after ``torch.cuda.synchronize()``. Work on the current stream after the call waits
         for the download; between calls, the caller synchronises before it reads or changes the host
@@ -233,14 +245,30 @@ class FlipSolver:
                 self.particles[a:b].copy_(positions[a:b], non_blocking=True)
                 self.particle_velocity[a:b].copy_(velocities[a:b], non_blocking=True)
         compute.wait_stream(up)
-        stats = self.step()
+        updated = []
+
+        def piece_done(c: int) -> None:
+            ev = torch.cuda.Event()
+            ev.record(compute)
+            updated.append(ev)
+
+        if n == 0:
+            stats = self.step()
+        else:
+            self.pre_solve()
+            stats = self.solve()
+            self.post_solve(piece_bounds=bounds, piece_done=piece_done)
+            self.steps_done += 1
         if self.n != n:
             raise RuntimeError("step_host: the step changed the particle count; use step() with sources")
-        down.wait_stream(compute)
+        if len(updated) != chunks:
+            down.wait_stream(compute)
         events = []
         with torch.cuda.stream(down):
             for c in range(chunks):
                 a, b = bounds[c], bounds[c + 1]
+                if len(updated) == chunks:
+                    down.wait_event(updated[c])
                 positions[a:b].copy_(self.particles[a:b], non_blocking=True)
                 velocities[a:b].copy_(self.particle_velocity[a:b], non_blocking=True)
                 ev = torch.cuda.Event()
