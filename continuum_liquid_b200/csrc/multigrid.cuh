@@ -405,16 +405,28 @@ __device__ __forceinline__ void restrict_at(i64 ci, const float* __restrict__ fp
         const int si = 1 + 2 * (I - 1), sj = 1 + 2 * (J - 1), sk = 1 + 2 * (K - 1);
         const float inv_delta2 = 1.0f / (delta * delta);
         const i64 sx = (i64)fny * fnz, sy = fnz;
-        for (int di = 0; di < 2; ++di)
-            for (int dj = 0; dj < 2; ++dj)
-                for (int dk = 0; dk < 2; ++dk) {
-                    const int i = si + di, j = sj + dj, k = sk + dk;
-                    if (!interior(i, j, k, fnx, fny, fnz)) continue;
-                    const i64 f = gidx(i, j, k, fny, fnz);
-                    const bool fl = L0 ? ((__ldg(fop0 + f) & 64u) != 0u) : (__ldg(fmask + f) != 0);
-                    if (!fl) continue;
-                    rhs += residual_at<L0>(fp, fb, fop0, fopc, fmask, inv_delta2, f, sx, sy);
-                }
+        // the eight children's fluid flags first, all loads at once; then the fluid children's
+        // residuals in (di, dj, dk) order
+        uint32_t flag[8];
+#pragma unroll
+        for (int ch = 0; ch < 8; ++ch) {
+            const int i = si + (ch >> 2), j = sj + ((ch >> 1) & 1), k = sk + (ch & 1);
+            const i64 f = gidx(i, j, k, fny, fnz);
+            flag[ch] = !interior(i, j, k, fnx, fny, fnz) ? 0u
+                       : L0 ? (uint32_t)__ldg(fop0 + f) : (__ldg(fmask + f) != 0 ? 64u : 0u);
+        }
+#pragma unroll
+        for (int ch = 0; ch < 8; ++ch) {
+            if (!(flag[ch] & 64u)) continue;
+            const i64 f = gidx(si + (ch >> 2), sj + ((ch >> 1) & 1), sk + (ch & 1), fny, fnz);
+            if (L0) {  // residual_at<true> with the operator byte already loaded
+                const uint32_t o = flag[ch];
+                const float ap = (wsum0<float>(fop0, fp, f, sx, sy, o) - (float)(o & 7u) * fp[f]) * inv_delta2;
+                rhs += __ldg(fb + f) - ap;
+            } else {
+                rhs += residual_at<false>(fp, fb, fop0, fopc, fmask, inv_delta2, f, sx, sy);
+            }
+        }
     }
     cb[ci] = rhs;
 }
