@@ -293,12 +293,13 @@ def sweep_case(args):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.case == "wcycle":
-        # as the tolerance mode runs it: a zeroed correction, fluid tiles on every level
+        # as the tolerance mode runs it: a correction from zero (the buffer zeroed once, each W-cycle's
+        # first sweep ignoring the previous correction), fluid tiles on every level
         k = 4 if args.coarse_iterations == "auto" else int(args.coarse_iterations)
+        p.zero_()
 
         def cycle():
-            p.zero_()
-            h.w_cycle(p, ps.rhs, coarse_iterations=k, x_zero_outside=True)
+            h.w_cycle(p, ps.rhs, coarse_iterations=k, x_from_zero=True)
 
         cycle()
         torch.cuda.synchronize()
