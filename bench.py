@@ -441,6 +441,9 @@ def reference_arm(args):
         run_cpu_steps(scene, positions, velocities, 1, cycles)
     sec, threads = run_cpu_steps(scene, positions, velocities, steps, cycles)
     value = 1.0 / sec
+    config = workload_config(args.size, len(positions), args)
+    config["pressure_solver"] = (f"the reference's fixed count of {cycles} W-cycles per step in FP32 (pre 2, post 4, "
+                                 f"coarse 2+64)")
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -455,7 +458,7 @@ def reference_arm(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": workload_config(args.size, len(positions), args),
+        "config": config,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{steps} full step(s) of the {args.size}^3 block scene ({len(positions)} particles) "
                                    f"with {cycles} FP32 W-cycles per step (the reference method: fixed cycle count; "
