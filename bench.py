@@ -730,8 +730,8 @@ def our_arm(args):
                "d2h_bytes_per_step": 24 * n, "steps": e2e_steps,
                "path": "FlipSolver.step_host: the particle state copied from pinned host buffers before and back "
                        "after every step (the reference's per-step host round trip of solver.py:252-306), in 8 "
-                       "pieces per direction on two copy streams, one step's download overlapping the next "
-                       "step's upload"}
+                       "pieces per direction on two copy streams: a piece's download starts once the particle "
+                       "update of that piece is done and overlaps the next step's upload of earlier pieces"}
 
     # --- roofline: the level-0 red-black sweep as the timed steps run it (on the fluid tiles), timed
     # alone on the stream ---------------------------------------------------------------------------
