@@ -1198,7 +1198,10 @@ int clb_mg_ir_init(const float* p32, const uint8_t* op0, double* p64, int nx, in
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(p32 && op0 && p64, "mg_ir_init: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    launch(blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_init, p32, op0, p64, nx, ny, nz);
+    if (nz % 4 == 0 && (((uintptr_t)p32 | (uintptr_t)p64) & 15) == 0 && (((uintptr_t)op0) & 3) == 0)
+        launch(blocks_for(C / 4, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_init4, p32, op0, p64, nx, ny, nz);
+    else
+        launch(blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_init, p32, op0, p64, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_ir_init");
     return 0;
 }
@@ -1214,7 +1217,10 @@ int clb_mg_ir_update(double* p64, const float* e, int64_t cells, void* stream) {
 int clb_mg_ir_store(const double* p64, float* p32, int64_t cells, void* stream) {
     CLB_REQUIRE(p64 && p32 && cells >= 0, "mg_ir_store: bad arguments");
     if (cells == 0) return 0;
-    launch(blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_store, p64, p32, cells);
+    if (cells % 4 == 0 && (((uintptr_t)p32 | (uintptr_t)p64) & 15) == 0)
+        launch(blocks_for(cells / 4, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_store4, p64, p32, cells / 4);
+    else
+        launch(blocks_for(cells, MGT), MGT, 0, CLB_STREAM(stream))(k_ir_store, p64, p32, cells);
     CLB_LAUNCH_CHECK("k_ir_store");
     return 0;
 }
