@@ -39,7 +39,7 @@ def scene_particles(n, seed=0, jitter_vel=True, shape=None):
     return s, pos, vel
 
 
-@pytest.fixture(params=[(16, 16, 16), (33, 33, 33), (40, 24, 31)], ids=lambda s: "x".join(map(str, s)))
+@pytest.fixture(params=[(16, 16, 16), (33, 33, 33), (40, 24, 31), (24, 20, 32)], ids=lambda s: "x".join(map(str, s)))
 def case(request):
     shape = request.param
     n = shape[0]
@@ -111,10 +111,12 @@ def test_particle_to_grid_stage_bit_exact(backend, oracle, case):
         assert np.array_equal(host(g), o)
 
 
-def test_dense_bins_and_outside_particles(backend, oracle):
-    """Many particles in one bin (slow path of the stable sort) and particles outside the grid
-    (clamped bins), as the reference allows."""
-    shape, dx = (12, 12, 12), F32(1.0 / 12)
+@pytest.mark.parametrize("shape", [(12, 12, 12), (12, 12, 32)])
+def test_dense_bins_and_outside_particles(backend, oracle, shape):
+    """Many particles in one bin (slow path of the stable sort), in grids whose rows are and are not a
+    multiple of the 32-cell gather block, and particles outside the grid (clamped bins), as the
+    reference allows."""
+    dx = F32(1.0 / 12)
     rng = np.random.default_rng(5)
     dense = (np.array([5.6, 5.6, 5.6]) + rng.random((300, 3)) * 0.3) * dx
     outside = np.array([[-0.2, 0.5, 0.5], [0.5, 1.7, 0.5], [0.5, 0.5, -3.0]])
