@@ -192,7 +192,8 @@ int clb_exclusive_prefix_sum(const int32_t* values, int32_t* output, int32_t* to
 // 16 + 8 * 16384 bytes, held on every GPU that loads the library until the process exits.
 //
 // In host code the array's name only stands for it; its device address is obtained once per device
-// with cudaGetSymbolAddress, on the first call made while that device is current.
+// with cudaGetSymbolAddress, on the first call made while that device is current, and kept for the
+// life of the process (a device reset would invalidate it; the header tells callers not to reset).
 static constexpr i64 kScanStaticTiles = (CLB_SCAN_STATIC_MAX_COUNT + SCAN_TILE - 1) / SCAN_TILE;
 static __device__ __align__(256) unsigned char g_scan_static_scratch[16 + 8 * kScanStaticTiles];
 static std::mutex g_scan_static_mutex;

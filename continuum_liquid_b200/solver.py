@@ -342,23 +342,23 @@ def solver(config: dict, timings=None) -> None:
 
     sources_dev, obstacle_mask = voxelise_mesh.build_static_masks(kernels, None, kernels, simulation, grid_shape,
                                                                   delta)
-    sources, obstacle_host = source_particles.download_static_masks(None, sources_dev, obstacle_mask, grid_shape)
+    # the reference seeds on the host from default_rng(0) (solver.py:146-158); the device sources
+    # draw the same stream, so the particles equal the reference's without leaving the GPU
     rng = np.random.default_rng(0)
+    empty = np.empty((0, 3), dtype=FIELD_DTYPE)
+    sim = FlipSolver(kernels, grid_shape, delta, empty, empty, obstacle=obstacle_mask, dt=dt, options=options,
+                     particles_per_cell=8)
+    source_particles.DeviceSources(kernels, sources_dev, obstacle_mask, grid_shape, delta, rng,
+                                   initial=True).apply(sim)
     device_sources = source_particles.DeviceSources(kernels, sources_dev, obstacle_mask, grid_shape, delta, rng)
-    particles_host = np.empty((0, 3), dtype=FIELD_DTYPE)
-    velocity_host = np.empty((0, 3), dtype=FIELD_DTYPE)
-    particles_host, velocity_host = source_particles.apply_sources(particles_host, velocity_host, sources,
-                                                                   obstacle_host, delta, rng, initial=True)
-    sim = FlipSolver(kernels, grid_shape, delta, particles_host, velocity_host, obstacle=obstacle_mask, dt=dt,
-                     options=options, particles_per_cell=8)
 
     output_dir.mkdir(parents=True, exist_ok=True)
     cache = output.create_cache(output_dir, fps=fps, start_frame=start_frame, end_frame=end_frame)
     writer = output.create_output(cache)
     try:
-        output.submit_host(writer, particles_host, frame=start_frame)
+        output.submit_output(writer, particles=sim.particles, particle_count=sim.n, frame=start_frame)
         emit_message({"type": "stats", "frame": 0, "total_frames": total_frames, "particle_count": sim.n})
-        dynamic = any(source.get("type") in {"INFLOW", "OUTFLOW"} for source in sources)
+        dynamic = any(source.get("type") in {"INFLOW", "OUTFLOW"} for source in sources_dev)
         for solver_step in range(total_solver_steps):
             if cancel_event is not None and cancel_event.is_set():
                 print("Bake cancellation requested. Stopping the simulation cleanly...")

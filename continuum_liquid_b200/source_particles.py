@@ -1,7 +1,10 @@
-"""Host-side particle sources (mirrors Solver/Kernel/source_particles.py).
+"""Particle sources (the stage of Solver/Kernel/source_particles.py) on the device.
 
-Sources are voxelised on the device and their masks downloaded once; seeding, inflow top-up and
-outflow removal then run on the host with numpy, exactly where the reference runs them.
+The reference voxelises its source meshes on the device, downloads the masks once and then seeds,
+tops up and removes particles on the host with numpy, copying every particle to the host and back
+before each step (solver.py:252-306). Here the initial fill, the inflows and the outflows run on the
+GPU (``DeviceSources``) and draw the reference's random stream, so the particles are the ones the
+reference's host code makes, bit for bit, without leaving the device.
 """
 
 from __future__ import annotations
@@ -22,77 +25,22 @@ def download_static_masks(queue, sources, obstacle_mask_device, grid_shape):
     return result, obstacle
 
 
-def particle_cells(positions, delta, grid_shape):
-    """source_particles.py:21-25: clamp(floor(p / delta), 0, n - 1)."""
-    if len(positions) == 0:
-        return np.empty((0, 3), dtype=np.int32)
-    cells = np.floor(np.asarray(positions) / delta).astype(np.int32)
-    return np.clip(cells, 0, np.asarray(grid_shape, dtype=np.int32) - 1)
-
-
-def mask_membership(positions, mask, delta):
-    """source_particles.py:28-34."""
-    cells = particle_cells(positions, delta, mask.shape)
-    if len(cells) == 0:
-        return np.zeros(0, dtype=np.bool_)
-    return mask[cells[:, 0], cells[:, 1], cells[:, 2]]
-
-
-def remove_masked(particles, velocities, mask, delta):
-    """source_particles.py:37-39: drop particles inside an outflow mask."""
-    keep = ~mask_membership(particles, mask, delta)
-    return particles[keep], velocities[keep]
-
-
-def fill_source(particles, velocities, source, obstacle_mask, delta, rng):
-    """source_particles.py:42-75: top every non-solid source cell up to ``particle_density``
-    particles, each new one uniform in its cell, with the source velocity."""
-    target = max(1, int(source.get("particle_density", 8)))
-    source_mask = np.asarray(source["mask"], dtype=np.bool_) & ~obstacle_mask
-    cells = np.argwhere(source_mask)
-    if len(cells) == 0:
-        return particles, velocities
-    counts = np.zeros(source_mask.shape, dtype=np.int64)
-    occupied = particle_cells(particles, delta, source_mask.shape)
-    if len(occupied):
-        flat = np.ravel_multi_index(occupied.T, source_mask.shape)
-        counts.flat[:] = np.bincount(flat, minlength=source_mask.size)
-    missing = np.maximum(0, target - counts[tuple(cells.T)])
-    spawn = np.repeat(cells, missing, axis=0)
-    if len(spawn) == 0:
-        return particles, velocities
-    new_positions = (spawn + rng.random((len(spawn), 3))) * delta
-    velocity = np.asarray(source.get("velocity", (0.0, 0.0, 0.0)), dtype=FIELD_DTYPE)
-    new_velocities = np.broadcast_to(velocity, new_positions.shape)
-    return (
-        np.ascontiguousarray(np.concatenate((particles, new_positions)), dtype=FIELD_DTYPE),
-        np.ascontiguousarray(np.concatenate((velocities, new_velocities)), dtype=FIELD_DTYPE),
-    )
-
-
-def apply_sources(particles, velocities, sources, obstacle_mask, delta, rng, initial=False):
-    """source_particles.py:78-92: outflows first, then inflows (and geometry sources initially)."""
-    for source in sources:
-        if source.get("type") == "OUTFLOW":
-            particles, velocities = remove_masked(particles, velocities, source["mask"], delta)
-    for source in sources:
-        kind = source.get("type")
-        if kind == "INFLOW" or (initial and kind == "GEOMETRY"):
-            particles, velocities = fill_source(particles, velocities, source, obstacle_mask, delta, rng)
-    return particles, velocities
-
-
 class DeviceSources:
-    """Outflow removal and inflow top-up on the device, for the sources of a running simulation
-    (apply_sources without ``initial``: outflows first, then each inflow in order). The results equal
-    apply_sources on the host with the same random generator, which this class advances by the draws
-    it uses; the particles never leave the GPU (only the counts are read back, to size the buffers).
+    """The reference's ``apply_sources`` (source_particles.py:78-92) on the device: every outflow
+    first, then each inflow in order, and with ``initial`` each geometry source too (the initial
+    fill, solver.py:146-158). A source cell that is not solid is topped up to the source's density;
+    the new particles of a cell are placed in flat cell order, each at (cell + three consecutive
+    draws of the generator) * delta in float64, rounded to float32, which is what the reference's
+    numpy code computes. This class advances ``rng`` by the draws it uses, so host and device stay
+    interchangeable; the particles never leave the GPU (only the counts are read back, to size the
+    buffers).
 
-    ``sources``: dicts with ``type`` ("INFLOW" / "OUTFLOW"), ``mask_device`` (uint8 grid tensor),
-    ``particle_density`` and ``velocity`` as in the reference; ``obstacle``: uint8 grid tensor or None.
+    ``sources``: dicts with ``type`` ("GEOMETRY" / "INFLOW" / "OUTFLOW"), ``mask_device`` (uint8 grid
+    tensor), ``particle_density`` and ``velocity`` as in the reference; ``obstacle``: uint8 grid
+    tensor or None.
     """
 
-    def __init__(self, kernels, sources, obstacle, grid_shape, delta, rng):
+    def __init__(self, kernels, sources, obstacle, grid_shape, delta, rng, initial: bool = False):
         import torch
 
         self.k = kernels
@@ -112,7 +60,8 @@ class DeviceSources:
             self.outflow = combined
         self.inflows = [(src["mask_device"].to(torch.uint8).contiguous(), max(1, int(src.get("particle_density", 8))),
                          tuple(float(FIELD_DTYPE(c)) for c in src.get("velocity", (0.0, 0.0, 0.0))))
-                        for src in sources if src.get("type") == "INFLOW"]
+                        for src in sources
+                        if src.get("type") == "INFLOW" or (initial and src.get("type") == "GEOMETRY")]
         self.counts = torch.zeros(cells, dtype=torch.int32, device=dev)
         self.missing = torch.zeros(cells, dtype=torch.int32, device=dev)
         self.offsets = torch.zeros(cells, dtype=torch.int32, device=dev)
@@ -165,5 +114,4 @@ class DeviceSources:
         sim.n = n
 
 
-__all__ = ["download_static_masks", "particle_cells", "mask_membership", "remove_masked", "fill_source",
-           "apply_sources", "DeviceSources"]
+__all__ = ["download_static_masks", "DeviceSources"]

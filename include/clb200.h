@@ -64,7 +64,9 @@ int clb_exclusive_prefix_sum(const int32_t* values, int32_t* output, int32_t* to
  * (16 + 8 * 16384 bytes, held on every GPU that loads the library until the process exits), so at
  * most CLB_SCAN_STATIC_MAX_COUNT elements are accepted; larger counts fail with an error. The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture. Every call clears the part of the array
+ * current; make that first call before any stream capture. The address is kept for the life of the
+ * process, so a caller that resets a device (cudaDeviceReset) must not call this function on that
+ * device afterwards: the array may then live elsewhere. Every call clears the part of the array
  * it uses and all calls share it: calls whose work overlaps on the GPU (different streams, or
  * different host threads on one device) race and must be serialised by the caller. */
 #define CLB_SCAN_STATIC_MAX_COUNT 67108864LL

@@ -5,9 +5,12 @@ liboracle.so (flip_oracle.cpp, one function per reference OpenCL kernel) and a n
 of the host orchestration in Solver/Kernel/solver.py:243-529, particles.py:73-171,
 multigrid.py:18-187 and pressure_solve.py:10-85.
 
-Parity status: unpinned by the reference itself -- the reference has no tests or golden vectors
-and its OpenCL programs cannot run here (no OpenCL runtime). The restatement is pinned by
-hand-derived known-answer tests (tests/test_oracle_kats.py) instead.
+Parity status: pinned to the reference itself. The reference ships no tests or golden vectors and
+no OpenCL runtime exists here, so oracle/reference_run.py runs the reference's own host code and
+OpenCL kernels on the CPU (oracle/pyopencl_shim, oracle/ref_build.py -> oracle/_ref/); the bakes it
+produced are committed as tests/golden/ref_*, and tests/test_reference_golden.py checks this
+restatement against them bit for bit (every frame and every intermediate of the first step).
+Hand-derived known-answer tests (tests/test_oracle_kats.py) check it as well.
 """
 
 from __future__ import annotations
@@ -411,13 +414,15 @@ class OracleSim:
     def step(self):
         s, dx, dt = self.shape, self.dx, self.dt
         pos_s, vel_s, u, v, w, ff, counts, offsets = particle_to_grid(self.pos, self.vel, dx, s, self.ppc)
-        self.trace.update(counts=counts, offsets=offsets, sorted_pos=pos_s, p2g_u=u, p2g_ff=ff)
+        self.trace.update(counts=counts, offsets=offsets, sorted_pos=pos_s, sorted_vel=vel_s, p2g_u=u, p2g_v=v,
+                          p2g_w=w, p2g_ff=ff)
         u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s)
         u, v, w = grid_domain_bc(u, v, w, s)
         uo, vo, wo = u, v, w
         u, v, w = update_velocity(u, v, w, ff, self.gravity, (0.0, 0.0, 0.0), self.rho, self.nu, dx, dt, s)
         u, v, w = grid_domain_bc(u, v, w, s)
         u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s)
+        self.trace.update(pre_u=u, pre_v=v, pre_w=w, pressure_in=self.pressure.copy())
         self.pressure, rhs, op0 = pressure_solve(u, v, w, ff, self.pressure, dx, dt, self.rho, self.num_vcycles, s,
                                                  self.levels)
         self.trace.update(rhs=rhs, ff=ff, pressure=self.pressure.copy())
@@ -426,6 +431,7 @@ class OracleSim:
         u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s)
         self.trace.update(u=u, v=v, w=w)
         vel = grid_to_particle(vel_s, pos_s, (u, v, w), (uo, vo, wo), dx, s, self.flip_ratio)
+        self.trace.update(vel_g2p=vel)
         prev = pos_s.copy()
         pos = advect(pos_s, vel, dt)
         pos, vel = particle_domain_bc(pos, vel, dx, s)
