@@ -58,7 +58,6 @@ def parse_args():
     ap.add_argument("--size", type=int, default=256, help="grid size n of the n^3 block scene")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-cycles", type=int, default=None, help="W-cycles per CPU step (default: measured)")
     ap.add_argument("--method", choices=["fcg", "refine"], default="fcg", help="tolerance-mode pressure iteration")
     ap.add_argument("--learned", choices=["auto", "on", "off"], default="auto",
                     help="learned warm start in the timed steps (auto: when trained weights exist and the Poisson "
@@ -327,27 +326,31 @@ def sweep_case(args):
                       "ms_per_iteration": ms, "algorithmic_gb_s": 13.0 * cells / (ms * 1e-3) / 1e9}), flush=True)
 
 
-def workload_config(size, n_particles, args, coarse_iterations=COARSE_ITERATION_CHOICES[0],
-                    smoothing=SMOOTHING_CHOICES[0], fp16_levels=None):
-    k = int(coarse_iterations)
-    pre, post = smoothing
-    storage = (f", levels {fp16_levels[0][0]}^3 and coarser stored in FP16" if fp16_levels else "")
+def workload_config(size, n_particles, args):
+    """The workload, identical in both arms' lines (how each arm solves is in its "solver" key)."""
     return {
         "workload": f"flip_step_block_{size}^3",
         "grid": [size, size, size],
         "particles": int(n_particles),
         "liquid_block": [[0, 0, 0], [0.5, 0.7, 0.5]],
+        "seeding": "8 particles per liquid cell, one uniform in each 2x2x2 sub-cell, numpy default_rng(0)",
         "dt": 1.0 / 240.0,
+        "gravity": [0.0, -9.81, 0.0],
         "flip_ratio": 0.95,
         "pressure_tolerance": TOL,
-        "pressure_solver": (f"flexible CG preconditioned by one W-cycle computed in FP32 (pre {pre}, post {post}, "
-                            f"coarse {pre}+{k}{storage}), FP64 pressure, residual and norms" if args.method == "fcg"
-                            else f"W-cycle computed in FP32 (pre {pre}, post {post}, coarse {pre}+{k}{storage}) in "
-                                 f"FP64 iterative refinement"),
-        "multigrid_levels": None,
+        "pressure_residual": "FP64 ||b - A p||_2 / ||b||_2 over the interior fluid cells, checked every step",
         "l2": "inputs larger than L2 (particle state 24 B x N, grid fields 4 B x n^3 each)",
         "parallelism": "replicas" if args.gpus > 1 else "single",
     }
+
+
+def solver_description(method, pre, post, k, fp16_levels=None):
+    storage = f", levels {fp16_levels[0][0]}^3 and coarser stored in FP16" if fp16_levels else ""
+    if method == "fcg":
+        return (f"flexible CG preconditioned by one W-cycle computed in FP32 (pre {pre}, post {post}, coarse "
+                f"{pre}+{k}{storage}), FP64 pressure, residual and norms")
+    return (f"W-cycle computed in FP32 (pre {pre}, post {post}, coarse {pre}+{k}{storage}) in FP64 iterative "
+            f"refinement")
 
 
 class ClockSampler:
@@ -411,22 +414,63 @@ def measured_peak_hbm():
 
 
 # ------------------------------------------------------------------------------------------------
-def run_cpu_steps(scene, positions, velocities, steps, cycles, threads_note=True):
-    """The reference algorithm on the host cores (oracle restatement, OpenMP): `steps` full steps
-    with `cycles` W-cycles each; returns seconds per step and the cycle count used."""
+# the tolerance-mode preconditioner settings the GPU's Poisson comparison picks at 256^3 (4 coarsest-level
+# iterations, one smoothing sweep before and after): the CPU solves to the tolerance with the same iteration
+CPU_FCG = {"coarse_iterations": 4, "pre_smooth": 1, "post_smooth": 1}
+REFERENCE_FIXED_CYCLES = 6
+
+
+def cpu_sim(scene, positions, velocities, tol=TOL, cycles=None):
+    """The reference algorithm on the host cores: the oracle (every reference kernel restated in C++
+    with OpenMP, the step order of solver.py:243-529). With ``tol`` each pressure is solved to that
+    FP64 relative residual by the flexible CG with the reference's W-cycle as preconditioner (the same
+    work as the GPU's timed step); with ``cycles`` by the reference's own method, that fixed number of
+    FP32 W-cycles."""
     from oracle import oracle
 
-    sim = oracle.OracleSim(scene.grid_shape, scene.dx, positions, velocities, dt=scene.dt, flip_ratio=0.95,
-                           gravity=scene.gravity, num_vcycles=cycles)
-    times = []
+    return oracle.OracleSim(scene.grid_shape, scene.dx, positions, velocities, dt=scene.dt, flip_ratio=0.95,
+                            gravity=scene.gravity, rho=scene.rho, nu=scene.nu, min_size=scene.min_size,
+                            num_vcycles=cycles or 1, tol=None if cycles else tol, **CPU_FCG)
+
+
+def cpu_steps(sim, steps):
+    """Seconds and pressure cycles of each of ``steps`` full steps."""
+    times, cycles = [], []
     for _ in range(steps):
         t0 = time.perf_counter()
         sim.step()
         times.append(time.perf_counter() - t0)
-    return float(np.mean(times)), oracle.lib().orc_num_threads()
+        cycles.append(int(sim.last_cycles))
+    return times, cycles
+
+
+def cpu_threads():
+    from oracle import oracle
+
+    return int(oracle.lib().orc_num_threads())
+
+
+def reference_method_step(sim):
+    """One more step of ``sim`` with the reference's own pressure method (a fixed count of FP32 W-cycles
+    from the previous pressure): its time and the FP64 relative residual it leaves."""
+    from oracle import oracle
+
+    sim.tol, sim.num_vcycles = None, REFERENCE_FIXED_CYCLES
+    t0 = time.perf_counter()
+    sim.step()
+    sec = time.perf_counter() - t0
+    ff = sim.trace["ff"]
+    rel = oracle.relative_residual(sim.trace["pressure"], sim.trace["rhs"], ff,
+                                   oracle.build_finest_operator(ff, sim.shape), np.float32(sim.dx))
+    return {"ms_per_step": sec * 1e3, "w_cycles": REFERENCE_FIXED_CYCLES, "rel_residual": rel,
+            "reaches_tolerance": bool(rel <= TOL),
+            "method": f"the reference's pressure solve (pressure_solve.py:61-83): {REFERENCE_FIXED_CYCLES} FP32 "
+                      f"W-cycles (pre 2, post 4, coarse 2+64) from the previous pressure, no residual check"}
 
 
 def reference_arm(args):
+    """The reference's CPU implementation of the step (the oracle; the OpenCL original needs an OpenCL
+    device, which this host lacks) on the same workload, steps and warm-up as this backend's arm."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -434,35 +478,38 @@ def reference_arm(args):
 
     scene = scenes.block(args.size)
     positions, velocities = scenes.seed_particles(scene)
-    cycles = args.cpu_cycles or 6
-    steps = max(1, min(args.steps, 2))
-    warm = 1 if args.warmup > 0 else 0
-    if warm:
-        run_cpu_steps(scene, positions, velocities, 1, cycles)
-    sec, threads = run_cpu_steps(scene, positions, velocities, steps, cycles)
+    sim = cpu_sim(scene, positions, velocities)
+    cpu_steps(sim, args.warmup)
+    times, cycles = cpu_steps(sim, args.steps)
+    sec = float(np.mean(times))
     value = 1.0 / sec
-    config = workload_config(args.size, len(positions), args)
-    config["pressure_solver"] = (f"the reference's fixed count of {cycles} W-cycles per step in FP32 (pre 2, post 4, "
-                                 f"coarse 2+64)")
+    threads = cpu_threads()
+    fixed = reference_method_step(sim)
+    solver = (f"the reference's kernels (oracle restatement, OpenMP) with each pressure solved to {TOL:g} by flexible "
+              f"CG preconditioned by the reference W-cycle in FP32 (pre {CPU_FCG['pre_smooth']}, post "
+              f"{CPU_FCG['post_smooth']}, coarse {CPU_FCG['pre_smooth']}+{CPU_FCG['coarse_iterations']}), FP64 "
+              f"pressure and residual")
     line = {
         "impl": "reference",
         "metric": METRIC,
         "value": value,
         "unit": UNIT,
         "n_gpus": args.gpus,
-        "steps": steps,
-        "warmup": warm,
+        "steps": args.steps,
+        "warmup": args.warmup,
         "ms_per_step": sec * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": config,
+        "config": workload_config(args.size, len(positions), args),
+        "solver": solver,
+        "cycles_per_step": cycles,
+        "reference_method": fixed,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{steps} full step(s) of the {args.size}^3 block scene ({len(positions)} particles) "
-                                   f"with {cycles} FP32 W-cycles per step (the reference method: fixed cycle count; "
-                                   f"the OpenCL original cannot run on this host)"},
+                         "sample": f"{args.steps} full steps (after {args.warmup} warm-up steps) of the {args.size}^3 "
+                                   f"block scene ({len(positions)} particles), each pressure to {TOL:g}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -483,6 +530,133 @@ def load_warm_start(kernels, scene, mode):
     net = learned.UNet(kernels)
     net.load(path)
     return learned.LearnedWarmStart(net, scene.grid_shape, scene.dx), str(path.name)
+
+
+AUDIT_TOL = 1e-11  # the FP64 reference solution: the same FP64 iteration run this much further
+
+
+def first_step_parity(sim, positions, velocities, scene):
+    """The first step's binning, counting sort and P2G on the GPU (the product path) against the oracle
+    on the same seeded particles: per-cell counts, offsets, sorted particles and the P2G grid velocity
+    and fluid fraction, compared value for value."""
+    from continuum_liquid_b200 import particles as pm
+    from oracle import oracle
+
+    k, gs, n = sim.kernels, sim.grid_shape, sim.n
+    (sim.particles, sim.particle_velocity, sim.particle_work, sim.particle_velocity_work, _,
+     sim.fluid_fraction) = pm.particle_to_grid(k, None, sim.particles, sim.particle_velocity, sim.particle_work,
+                                               sim.particle_velocity_work, (sim.u, sim.v, sim.w), sim.bin_counts,
+                                               sim.scan_outputs, sim.scan_sums, sim.fluid_fraction, n, gs, sim.dx,
+                                               sim.particles_per_cell)
+    host = lambda t: t.detach().cpu().numpy()  # noqa: E731
+    got = {"counts": host(sim.bin_counts).reshape(gs), "offsets": host(sim.scan_outputs[0]).reshape(gs),
+           "sorted_positions": sim.positions(), "sorted_velocities": sim.velocities(), "p2g_u": host(sim.u),
+           "p2g_v": host(sim.v), "p2g_w": host(sim.w), "fluid_fraction": host(sim.fluid_fraction)}
+    t0 = time.perf_counter()
+    pos_s, vel_s, u, v, w, ff, counts, offsets = oracle.particle_to_grid(positions, velocities, scene.dx, gs)
+    oracle_s = time.perf_counter() - t0
+    ref = {"counts": counts.reshape(gs), "offsets": offsets.reshape(gs), "sorted_positions": pos_s,
+           "sorted_velocities": vel_s, "p2g_u": u, "p2g_v": v, "p2g_w": w, "fluid_fraction": ff}
+    exact = {name: bool(np.array_equal(got[name], ref[name])) for name in ref}
+    return {"scene": f"the first step of the timed scene ({n} particles, {gs[0]}^3)", "bit_exact": exact,
+            "all_bit_exact": all(exact.values()), "oracle_s": round(oracle_s, 2),
+            "oracle": "CPU restatement of particles.cl:44-227 (pinned to the reference's own bakes by "
+                      "tests/test_reference_golden.py)"}
+
+
+def pressure_error_audit(sim, snapshot, end_positions, steps, min_size):
+    """Replays the timed steps from the state they started in, and after each step's pressure solve
+    (the timed steps' settings, to TOL) solves the same system once more, in the same FP64 iteration,
+    to AUDIT_TOL: the FP64 reference solution. Reports each step's pressure error against it and whether
+    the replay reproduced the timed steps bit for bit (the particle positions after the last step)."""
+    import torch
+
+    from continuum_liquid_b200.pressure_solve import PressureSolver
+
+    n, pos, vel, pressure = snapshot
+    sim.n = n
+    sim.particles[:n].copy_(pos)
+    sim.particle_velocity[:n].copy_(vel)
+    sim.pressure.copy_(pressure)
+    ref = PressureSolver(sim.kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", max_cycles=300)
+    p_tmp = torch.empty_like(sim.pressure)
+    rows = []
+    for _ in range(steps):
+        p_prev = sim.pressure.clone()
+        sim.pre_solve()
+        st = sim.solve()
+        p_tmp.copy_(p_prev)
+        rst = ref.solve((sim.u, sim.v, sim.w), sim.fluid_fraction, p_tmp, sim.dt, sim.options.rho, tol=AUDIT_TOL)
+        p, p_star = sim.pressure_solver.pressure64, ref.pressure64
+        diff = p - p_star
+        rows.append({"cycles": st.cycles, "rel_residual": st.rel_residual,
+                     "rel_l2_error": float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(p_star)),
+                     "rel_max_error": float(diff.abs().max() / p_star.abs().max()),
+                     "reference_rel_residual": rst.rel_residual, "reference_cycles": rst.cycles})
+        sim.post_solve()
+    torch.cuda.synchronize()
+    replay_exact = bool(torch.equal(sim.particles[:n], end_positions))
+    return {"reference": f"the FP64-accumulated flexible CG run to {AUDIT_TOL:g} on each step's system (FP64 pressure "
+                         f"and residual; its FP32 W-cycle preconditioner sets only the convergence rate); checked "
+                         f"against the oracle's FP64-only W-cycle solve by tests/test_fp64_reference_gpu.py",
+            "steps": rows, "rel_l2_error_max": max(r["rel_l2_error"] for r in rows),
+            "rel_max_error_max": max(r["rel_max_error"] for r in rows),
+            "replay_bit_exact": replay_exact}
+
+
+def kernel_rooflines(sim, peak, ms_per_step, reps=5):
+    """Device time of each particle stage launched alone (CUDA events on the launching stream, the mean
+    of ``reps`` launches on the scene's current state) against its algorithmic bytes."""
+    import torch
+
+    from continuum_liquid_b200 import particles as pm
+
+    k, gs, n = sim.kernels, sim.grid_shape, sim.n
+    C = int(np.prod(gs))
+    scratch = sim.scan_sums[0]
+    inv_dx = float(np.float32(1.0 / sim.dx))
+    tiled = sim.options.tiled_p2g()
+    stages = []
+
+    def timed(name, kernel, bytes_, fn, prepare=None):
+        times = []
+        for _ in range(reps + 1):
+            if prepare is not None:
+                prepare()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = float(np.mean(times[1:]))
+        gbs = bytes_ / (ms * 1e-3) / 1e9
+        stages.append({"stage": name, "kernels": kernel, "ms": ms, "algorithmic_bytes": int(bytes_),
+                       "achieved": gbs, "unit": "GB/s", "frac": gbs / peak, "share_of_step": ms / ms_per_step})
+
+    pos, vel = sim.particles, sim.particle_velocity
+    timed("count", "k_bin_count", 20 * n + 4 * C,
+          lambda: k.call("clb_count_particles_per_cell", pos, sim.bin_counts, scratch.keys, scratch.ranks, n, inv_dx,
+                         *gs), prepare=sim.bin_counts.zero_)
+    timed("scan", "k_scan_lookback", 8 * C,
+          lambda: pm.exclusive_prefix_sum(k, None, sim.bin_counts, sim.scan_outputs, sim.scan_sums, C))
+    timed("sort", "k_scatter_perm + k_stable_gather", 56 * n + 4 * C,
+          lambda: pm.sort_particles(k, None, pos, vel, sim.particle_work, sim.particle_velocity_work,
+                                    sim.scan_outputs[0], sim.bin_counts, scratch, n))
+    timed("p2g", "k_p2g_tiled" if tiled else "k_p2g_gather", 24 * n + 24 * C,
+          lambda: pm.particle_to_grid_gather(k, None, sim.particle_work, sim.particle_velocity_work,
+                                             sim.scan_outputs[0], sim.bin_counts, (sim.u, sim.v, sim.w),
+                                             sim.fluid_fraction, gs, sim.dx, sim.particles_per_cell, tiled=tiled))
+
+    def restore():
+        sim.particle_work[:n].copy_(pos[:n])
+        sim.particle_velocity_work[:n].copy_(vel[:n])
+
+    timed("particle_update", "k_particle_update (G2P, FLIP/PIC blend, advection, particle BCs)", 48 * n + 24 * C,
+          lambda: pm.particle_update(k, None, sim.particle_work, sim.particle_velocity_work, (sim.u, sim.v, sim.w),
+                                     (sim.u_work, sim.v_work, sim.w_work), sim.obstacle, n, gs, sim.dx, sim.dt,
+                                     sim.options.flip_ratio), prepare=restore)
+    return stages
 
 
 def poisson_comparison(kernels, sim, steps, warm, min_size):
@@ -628,6 +802,7 @@ def our_arm(args):
     sim = solver.FlipSolver(kernels, scene.grid_shape, scene.dx, positions, velocities, obstacle=obstacle, dt=scene.dt,
                             options=opts, min_size=scene.min_size)
     n = sim.n
+    parity = first_step_parity(sim, positions, velocities, scene) if rank == 0 else None
 
     barrier = group.barrier
 
@@ -673,6 +848,7 @@ def our_arm(args):
         torch.cuda.synchronize()
 
     # --- device-resident timed region -------------------------------------------------------
+    snapshot = (sim.n, sim.particles[:n].clone(), sim.particle_velocity[:n].clone(), sim.pressure.clone())
     stats = []
     solve_ms = []
     launches0 = kernels.launch_count()
@@ -690,6 +866,7 @@ def our_arm(args):
         torch.cuda.synchronize()
         barrier()
     clock_summary = clocks.summary()
+    end_positions = sim.particles[:n].clone()
     value, elapsed_ms = throughput(group, args.steps, start.elapsed_time(end))
     direct_launches = kernels.launch_count() - launches0
     replays = sim.pressure_solver.graph_replays - replays0
@@ -733,6 +910,10 @@ def our_arm(args):
                        "pieces per direction on two copy streams: a piece's download starts once the particle "
                        "update of that piece is done and overlaps the next step's upload of earlier pieces"}
 
+    # --- each timed step's pressure error against an FP64 reference solution (replayed steps) -------
+    audit = pressure_error_audit(sim, snapshot, end_positions, args.steps, scene.min_size)
+    del snapshot
+
     # --- roofline: the level-0 red-black sweep as the timed steps run it (on the fluid tiles), timed
     # alone on the stream ---------------------------------------------------------------------------
     ps = sim.pressure_solver
@@ -765,22 +946,27 @@ def our_arm(args):
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                 "traffic": traffic, "algorithmic_bytes_per_launch": algorithmic, "launch_us": per_launch_s * 1e6}
 
+    rooflines = [dict(roofline, stage="level0_sweep", ms=per_launch_s * 1e3,
+                      share_of_step=per_launch_s * 1e3 / (elapsed_ms / args.steps))]
+    rooflines += kernel_rooflines(sim, peak, elapsed_ms / args.steps)
+
     # --- CPU baseline (rank 0, N = 1): the reference algorithm on the host cores ---------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        k = args.cpu_cycles or max(1, int(round(float(np.mean(cycles)))))
-        sec, threads = run_cpu_steps(scene, positions, velocities, 1, k)
-        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"1 full step of the same scene ({n} particles) by the CPU restatement of the reference "
-                         f"kernels with {k} FP32 W-cycles (the GPU's mean cycle count)"}
+        cpu_times, cpu_cycles = cpu_steps(cpu_sim(scene, positions, velocities), 1)
+        cpu = {"value": 1.0 / cpu_times[0], "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+               "sample": f"the first step of the same scene ({n} particles) by the CPU restatement of the reference "
+                         f"kernels, its pressure solved to {TOL:g} ({cpu_cycles[0]} cycles of the same iteration)"}
 
     if rank == 0:
-        config = workload_config(args.size, n, args, sim.options.coarse_iterations,
-                                 (sim.options.pre_smooth, sim.options.post_smooth),
-                                 [list(s) for s in h.shapes[h.fp16_level:]] if h.fp16_level else None)
-        config["multigrid_levels"] = [list(s) for s in h.shapes]
-        config["sweep_kinds"] = h.sweeps()
-        config["sweep_tuning_ms_per_iteration"] = h.tuning
+        config = workload_config(args.size, n, args)
+        fp16_levels = [list(s) for s in h.shapes[h.fp16_level:]] if h.fp16_level else None
+        solver_info = {"pressure": solver_description(args.method, sim.options.pre_smooth, sim.options.post_smooth,
+                                                      sim.options.coarse_iterations, fp16_levels),
+                       "p2g": "tiled scatter (k_p2g_tiled)" if sim.options.tiled_p2g() else
+                              "reference-order gather (k_p2g_gather)",
+                       "multigrid_levels": [list(s) for s in h.shapes], "sweep_kinds": h.sweeps(),
+                       "sweep_tuning_ms_per_iteration": h.tuning}
         line = {
             "metric": METRIC,
             "value": value,
@@ -795,10 +981,14 @@ def our_arm(args):
             "dtype": "f32",
             "data": "synthetic",
             "config": config,
+            "solver": solver_info,
             "particles_per_s": value * n,
+            "parity": parity,
+            "pressure_error": audit,
             "poisson": poisson,
             "e2e": e2e,
             "roofline": roofline,
+            "rooflines": rooflines,
             "cpu_baseline": cpu,
             "clocks": clock_summary,
             "gpu_launches": int(gpu_launches),

@@ -42,6 +42,8 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_sort_particles": [P, P, P, P, P, P, P, P, P, P, L, P],
     "clb_particle_to_grid_gather": [P, P, P, P, P, P, P, P, F, F, I, I, I, P],
     "clb_particle_to_grid": [P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, L, L, F, F, I, I, I, P],
+    "clb_particle_to_grid_gather_tiled": [P, P, P, P, P, P, P, P, F, F, I, I, I, P],
+    "clb_particle_to_grid_tiled": [P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, L, L, F, F, I, I, I, P],
     "clb_grid_to_particle": [P, P, P, P, P, P, P, P, L, F, I, I, I, F, P],
     "clb_advect_particles": [P, P, L, F, P],
     "clb_particle_domain_bc": [P, P, L, F, F, F, F, P],

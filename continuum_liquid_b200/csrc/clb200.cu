@@ -2,6 +2,7 @@
 // included below; this file validates arguments, picks launch shapes and enqueues the kernels.
 #include "../../include/clb200.h"
 #include "binning.cuh"
+#include "p2g_tiled.cuh"
 #include "particles.cuh"
 #include "grid.cuh"
 #include "multigrid.cuh"
@@ -147,6 +148,9 @@ int clb_init(int device) {
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_bottom_visit<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bottom_max);
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_coarse_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     if (check_call(e, "bottom visit attribute")) return 1;
+    if (check_call(cudaFuncSetAttribute(k_p2g_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, P2GT_SMEM),
+                   "tiled P2G attribute"))
+        return 1;
     if (conv_set_attributes()) return 1;
     return 0;
 }
@@ -257,11 +261,29 @@ int clb_particle_to_grid_gather(const float* particles, const float* velocity, c
     return 0;
 }
 
-int clb_particle_to_grid(const float* particles, const float* velocity, float* particles_work, float* velocity_work,
-                         float* u, float* v, float* w, float* fluid_fraction, int32_t* bin_counts,
-                         int32_t* bin_offsets, int32_t* keys, int32_t* ranks, int32_t* perm, int32_t* slot_keys,
-                         void* scan_scratch, int64_t scan_scratch_bytes_, int64_t n, float inv_dx,
-                         float inv_ppc, int nx, int ny, int nz, void* stream) {
+int clb_particle_to_grid_gather_tiled(const float* particles, const float* velocity, const int32_t* bin_offsets,
+                                      const int32_t* bin_counts, float* u, float* v, float* w, float* fluid_fraction,
+                                      float inv_dx, float inv_particles_per_cell, int nx, int ny, int nz,
+                                      void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(bin_offsets && bin_counts && u && v && w && fluid_fraction,
+                "particle_to_grid_gather_tiled: null pointer");
+    int tiles_j = 0, tiles_k = 0;
+    const int tiles = p2g_tiled_tiles(nx, ny, nz, &tiles_j, &tiles_k);
+    k_p2g_tiled<<<tiles, P2GT_THREADS, P2GT_SMEM, CLB_STREAM(stream)>>>(particles, velocity, bin_offsets, bin_counts,
+                                                                          u, v, w, fluid_fraction, inv_dx,
+                                                                          inv_particles_per_cell, nx, ny, nz, tiles_j,
+                                                                          tiles_k);
+    CLB_LAUNCH_CHECK("k_p2g_tiled");
+    return 0;
+}
+
+static int particle_to_grid_impl(const float* particles, const float* velocity, float* particles_work,
+                                 float* velocity_work, float* u, float* v, float* w, float* fluid_fraction,
+                                 int32_t* bin_counts, int32_t* bin_offsets, int32_t* keys, int32_t* ranks,
+                                 int32_t* perm, int32_t* slot_keys, void* scan_scratch, int64_t scan_scratch_bytes_,
+                                 int64_t n, float inv_dx, float inv_ppc, int nx, int ny, int nz, void* stream,
+                                 bool tiled) {
     CLB_GRID_ARGS_OK(nx, ny, nz);
     CLB_REQUIRE(inv_dx > 0.0f && inv_ppc > 0.0f, "particle_to_grid: inv_dx and inv_particles_per_cell must be > 0");
     CLB_REQUIRE(n >= 0 && n < (1ll << 31), "particle_to_grid: n=%lld out of range", (long long)n);
@@ -274,8 +296,31 @@ int clb_particle_to_grid(const float* particles, const float* velocity, float* p
     if (clb_sort_particles(particles, velocity, particles_work, velocity_work, bin_offsets, bin_counts, keys, ranks,
                            perm, slot_keys, n, stream))
         return 1;
+    if (tiled)
+        return clb_particle_to_grid_gather_tiled(particles_work, velocity_work, bin_offsets, bin_counts, u, v, w,
+                                                 fluid_fraction, inv_dx, inv_ppc, nx, ny, nz, stream);
     return clb_particle_to_grid_gather(particles_work, velocity_work, bin_offsets, bin_counts, u, v, w, fluid_fraction,
                                        inv_dx, inv_ppc, nx, ny, nz, stream);
+}
+
+int clb_particle_to_grid(const float* particles, const float* velocity, float* particles_work, float* velocity_work,
+                         float* u, float* v, float* w, float* fluid_fraction, int32_t* bin_counts,
+                         int32_t* bin_offsets, int32_t* keys, int32_t* ranks, int32_t* perm, int32_t* slot_keys,
+                         void* scan_scratch, int64_t scan_scratch_bytes_, int64_t n, float inv_dx,
+                         float inv_ppc, int nx, int ny, int nz, void* stream) {
+    return particle_to_grid_impl(particles, velocity, particles_work, velocity_work, u, v, w, fluid_fraction,
+                                 bin_counts, bin_offsets, keys, ranks, perm, slot_keys, scan_scratch,
+                                 scan_scratch_bytes_, n, inv_dx, inv_ppc, nx, ny, nz, stream, false);
+}
+
+int clb_particle_to_grid_tiled(const float* particles, const float* velocity, float* particles_work,
+                               float* velocity_work, float* u, float* v, float* w, float* fluid_fraction,
+                               int32_t* bin_counts, int32_t* bin_offsets, int32_t* keys, int32_t* ranks,
+                               int32_t* perm, int32_t* slot_keys, void* scan_scratch, int64_t scan_scratch_bytes_,
+                               int64_t n, float inv_dx, float inv_ppc, int nx, int ny, int nz, void* stream) {
+    return particle_to_grid_impl(particles, velocity, particles_work, velocity_work, u, v, w, fluid_fraction,
+                                 bin_counts, bin_offsets, keys, ranks, perm, slot_keys, scan_scratch,
+                                 scan_scratch_bytes_, n, inv_dx, inv_ppc, nx, ny, nz, stream, true);
 }
 
 int clb_grid_to_particle(float* velocity, const float* particles, const float* u, const float* v, const float* w,

@@ -89,11 +89,14 @@ def sort_particles(kernels: Backend, queue, particles, particle_velocity, partic
 
 
 def particle_to_grid_gather(kernels: Backend, queue, particles, particle_velocity, bin_offsets, bin_counts, velocity,
-                            fluid_fraction, grid_shape, dx, particles_per_cell):
-    """particles.cl:135-227 (dispatched as particles.py:194-215)."""
+                            fluid_fraction, grid_shape, dx, particles_per_cell, tiled: bool = False):
+    """particles.cl:135-227 (dispatched as particles.py:194-215). ``tiled``: the tiled scatter that
+    visits each particle once (every weight the reference's, each cell's sums in another fixed order:
+    equal to float rounding, not bit for bit)."""
     nx, ny, nz = grid_shape
     u, v, w = velocity
-    kernels.call("clb_particle_to_grid_gather", particles, particle_velocity, bin_offsets, bin_counts, u, v, w,
+    name = "clb_particle_to_grid_gather_tiled" if tiled else "clb_particle_to_grid_gather"
+    kernels.call(name, particles, particle_velocity, bin_offsets, bin_counts, u, v, w,
                  fluid_fraction, float(FIELD_DTYPE(1.0 / float(dx))), float(FIELD_DTYPE(1.0 / particles_per_cell)), nx, ny,
                  nz, stream=queue)
 
@@ -114,17 +117,19 @@ def particle_to_grid(
     grid_shape,
     dx,
     particles_per_cell,
+    tiled: bool = False,
 ):
     """particles.py:73-171: count, scan, sort into the work buffers, swap, gather.
 
     Returns ``(particles, particle_velocity, particle_work, particle_velocity_work, velocity,
-    fluid_fraction)`` with the particle buffers swapped, exactly like the reference.
+    fluid_fraction)`` with the particle buffers swapped, exactly like the reference. ``tiled`` selects
+    the tiled gather (see ``particle_to_grid_gather``); binning and sort are the same either way.
     """
     nx, ny, nz = grid_shape
     u, v, w = velocity
     scratch: SortScratch = particle_bin_scan_sums[0]
     kernels.call(
-        "clb_particle_to_grid",
+        "clb_particle_to_grid_tiled" if tiled else "clb_particle_to_grid",
         particles,
         particle_velocity,
         particle_work,

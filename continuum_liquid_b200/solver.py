@@ -61,6 +61,15 @@ class StepOptions:
     pre_smooth: int = 2
     post_smooth: int = 4
     revoxelise: bool = False  # voxelise the colliders again at every step (moving or deforming meshes)
+    # P2G gather: "exact" (the reference's summation order, bit for bit), "tiled" (each particle visited
+    # once; equal to float rounding) or "auto" (exact in the reference's fixed-cycle mode, tiled when
+    # the pressure is solved to a tolerance)
+    p2g: str = "auto"
+
+    def tiled_p2g(self) -> bool:
+        if self.p2g not in ("auto", "exact", "tiled"):
+            raise ValueError(f"p2g must be 'auto', 'exact' or 'tiled', not {self.p2g!r}")
+        return self.p2g == "tiled" or (self.p2g == "auto" and self.tol is not None)
 
 
 class FlipSolver:
@@ -143,7 +152,7 @@ class FlipSolver:
          _, self.fluid_fraction) = particle_methods.particle_to_grid(
             k, queue, self.particles, self.particle_velocity, self.particle_work, self.particle_velocity_work,
             (self.u, self.v, self.w), self.bin_counts, self.scan_outputs, self.scan_sums, self.fluid_fraction, self.n,
-            gs, self.dx, self.particles_per_cell)
+            gs, self.dx, self.particles_per_cell, tiled=o.tiled_p2g())
         vel = (self.u, self.v, self.w)
         if self.obstacle is not None:
             boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)

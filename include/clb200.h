@@ -96,6 +96,25 @@ int clb_particle_to_grid(const float* particles, const float* velocity, float* p
                          void* scan_scratch, int64_t scan_scratch_bytes, int64_t n, float inv_dx,
                          float inv_particles_per_cell, int nx, int ny, int nz, void* stream);
 
+/* particles.cl:135-227 particle_to_grid_gather, the same inputs and outputs, computed as a tiled
+ * scatter that visits each particle once (the tolerance-mode path). Every weight is the reference's;
+ * the sums of a cell are added in a different (fixed) order, so velocities agree with
+ * clb_particle_to_grid_gather to float rounding (not bit for bit); the fluid fraction and the set of
+ * zero faces are identical. Deterministic: the same inputs give the same bits on every run. */
+int clb_particle_to_grid_gather_tiled(const float* particles, const float* velocity, const int32_t* bin_offsets,
+                                      const int32_t* bin_counts, float* u, float* v, float* w, float* fluid_fraction,
+                                      float inv_dx, float inv_particles_per_cell, int nx, int ny, int nz,
+                                      void* stream);
+
+/* clb_particle_to_grid with the tiled gather (particles.py:73-171 with
+ * clb_particle_to_grid_gather_tiled as its last stage); same arguments. */
+int clb_particle_to_grid_tiled(const float* particles, const float* velocity, float* particles_work,
+                               float* velocity_work, float* u, float* v, float* w, float* fluid_fraction,
+                               int32_t* bin_counts, int32_t* bin_offsets, int32_t* keys, int32_t* ranks,
+                               int32_t* perm, int32_t* slot_keys, void* scan_scratch, int64_t scan_scratch_bytes,
+                               int64_t n, float inv_dx, float inv_particles_per_cell, int nx, int ny, int nz,
+                               void* stream);
+
 /* particles.cl:229-262 grid_to_particle (particles.py:174-206), plus a FLIP/PIC blend:
  * flip_ratio = 1 is the reference's pure FLIP update. */
 int clb_grid_to_particle(float* velocity, const float* particles, const float* u, const float* v, const float* w,

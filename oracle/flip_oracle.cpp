@@ -890,6 +890,77 @@ void orc_residual_norms_f64(const double* p, const double* b, const double* m, c
                             double* bb) {
     residual_norms<double>(p, b, m, d, wx, wy, wz, delta, nx, ny, nz, rr, bb);
 }
+// One flexible-CG update of the tolerance-mode iteration (oracle.fcg_solve), in FP64 with OpenMP:
+// z = the W-cycle correction e at interior fluid cells (mask > 0), 0 elsewhere; with `flexible`
+// the four dot products of Notay's truncated flexible CG (A z . d, A z . z, z . r32, d . r32), the
+// scalars beta, d.Ad (*dad, carried between calls, 0 = no direction yet) and alpha, the new float32
+// direction d = z + beta d and x += alpha d; without it x += z. Then r = b - A x (FP64), r32 = r
+// rounded to float32 and *rr = sum r^2. A is the FP64 finest operator (d, wx, wy, wz).
+void orc_fcg_update(const float* e, float* dir, double* x, double* r, float* r32, const double* b, const float* m,
+                    const double* dg, const double* wx, const double* wy, const double* wz, double dx, int nx, int ny,
+                    int nz, int flexible, double* dad, double* rr) {
+    const i64 C = (i64)nx * ny * nz, syz = (i64)ny * nz;
+    const double inv = 1.0 / (dx * dx);
+    auto fluid = [&](i64 c, int i, int j, int k) { return interior(i, j, k, nx, ny, nz) && m[c] > 0.0f; };
+    auto zval = [&](i64 c) {
+        int i, j, k;
+        gcoord(c, ny, nz, i, j, k);
+        return fluid(c, i, j, k) ? (double)e[c] : 0.0;
+    };
+    auto apply = [&](auto&& val, i64 c) {
+        const double ws = wx[c] * val(c + syz) + wx[c - syz] * val(c - syz) + wy[c] * val(c + nz) +
+                          wy[c - nz] * val(c - nz) + wz[c] * val(c + 1) + wz[c - 1] * val(c - 1);
+        return (ws - dg[c] * val(c)) * inv;
+    };
+    if (flexible) {
+        double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : sx, sy, sz, sw)
+        for (i64 c = 0; c < C; ++c) {
+            int i, j, k;
+            gcoord(c, ny, nz, i, j, k);
+            if (!fluid(c, i, j, k)) continue;
+            const double z = (double)e[c];
+            const double az = apply(zval, c);
+            sx += az * (double)dir[c];
+            sy += az * z;
+            sz += z * (double)r32[c];
+            sw += (double)dir[c] * (double)r32[c];
+        }
+        double beta, dr;
+        if (*dad != 0.0) {
+            beta = -sx / *dad;
+            dr = sz + beta * sw;
+            *dad = sy + 2.0 * beta * sx + beta * beta * *dad;
+        } else {
+            beta = 0.0;
+            *dad = sy;
+            dr = sz;
+        }
+        const double alpha = *dad != 0.0 ? dr / *dad : 0.0;
+#pragma omp parallel for schedule(static)
+        for (i64 c = 0; c < C; ++c) {
+            const float dn = (float)(zval(c) + beta * (double)dir[c]);
+            dir[c] = dn;
+            x[c] = x[c] + alpha * (double)dn;
+        }
+    } else {
+#pragma omp parallel for schedule(static)
+        for (i64 c = 0; c < C; ++c) x[c] = x[c] + zval(c);
+    }
+    auto xval = [&](i64 c) { return x[c]; };
+    double sr = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : sr)
+    for (i64 c = 0; c < C; ++c) {
+        int i, j, k;
+        gcoord(c, ny, nz, i, j, k);
+        const double rc = fluid(c, i, j, k) ? b[c] - apply(xval, c) : 0.0;
+        r[c] = rc;
+        r32[c] = (float)rc;
+        sr += rc * rc;
+    }
+    *rr = sr;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

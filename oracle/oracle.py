@@ -61,6 +61,8 @@ _SIGS = {
     "orc_w_cycle_f64": [_P] * 7 + [_P, _I, _D, _I, _I, _I],
     "orc_residual_norms_f32": [_f32p] * 7 + [_F, _I, _I, _I, _P, _P],
     "orc_residual_norms_f64": [_f64p] * 7 + [_D, _I, _I, _I, _P, _P],
+    "orc_fcg_update": [_f32p, _f32p, _f64p, _f64p, _f32p, _f64p, _f32p, _f64p, _f64p, _f64p, _f64p, _D, _I, _I, _I,
+                       _I, _P, _P],
     "orc_num_threads": [],
 }
 
@@ -360,36 +362,24 @@ def fcg_solve(rhs, ff, shape, dx, p0=None, tol=1e-6, max_cycles=100, flexible=Tr
     b = np.where(fluid, c(rhs, np.float64), 0.0)
     x = np.zeros(shape) if p0 is None else np.where(fluid, c(p0, np.float64), 0.0)
     nb = float(np.sqrt(np.sum(b * b)))
-
-    def residual(x):
-        return b - apply_operator64(x, ff32, op64, dx)[0]
-
-    r = residual(x)
-    hist = [float(np.sqrt(np.sum(r * r))) / nb if nb else 0.0]
+    r = np.zeros(shape, np.float64)
+    r32 = np.zeros(shape, np.float32)
     d = np.zeros(shape, np.float32)
-    dad = 0.0
+    e = np.zeros(shape, np.float32)
+    dad, rr = ctypes.c_double(0.0), ctypes.c_double(0.0)
+
+    def update(flex):
+        # orc_fcg_update: the CG scalars, direction and iterate, then r = b - A x and sum r^2 (FP64)
+        lib().orc_fcg_update(e, d, x, r, r32, b, ff32, *op64, float(dx), *shape, int(flex), ctypes.addressof(dad),
+                             ctypes.addressof(rr))
+        return float(np.sqrt(rr.value)) / nb if nb else 0.0
+
+    hist = [update(False)]  # e = 0: only the initial residual
     while hist[-1] > tol and len(hist) <= max_cycles:
-        r32 = r.astype(np.float32)
-        e = np.zeros(shape, np.float32)
-        levels.w_cycle(e, r32, ff32, op32, F32(float(dx)), pre=int(pre_smooth), post=int(post_smooth),
+        e[...] = 0.0
+        levels.w_cycle(e, r32.copy(), ff32, op32, F32(float(dx)), pre=int(pre_smooth), post=int(post_smooth),
                        coarse=int(coarse_iterations))
-        z = np.where(fluid, e, np.float32(0)).astype(np.float64)
-        if flexible:
-            az = apply_operator64(z, ff32, op64, dx)[0]
-            sx, sy = float(np.sum(az * d)), float(np.sum(az * z))
-            sz, sw = float(np.sum(z * r32)), float(np.sum(d.astype(np.float64) * r32))
-            if dad != 0.0:
-                beta = -sx / dad
-                dad, dr = sy + 2.0 * beta * sx + beta * beta * dad, sz + beta * sw
-            else:
-                beta, dad, dr = 0.0, sy, sz
-            alpha = dr / dad if dad != 0.0 else 0.0
-            d = (z + beta * d.astype(np.float64)).astype(np.float32)
-            x = x + alpha * d.astype(np.float64)
-        else:
-            x = x + z
-        r = residual(x)
-        hist.append(float(np.sqrt(np.sum(r * r))) / nb)
+        hist.append(update(flexible))
     return x, hist
 
 
@@ -399,11 +389,18 @@ class OracleSim:
     reference; an empty mask makes them no-ops)."""
 
     def __init__(self, shape, dx, positions, velocities, obstacle=None, dt=1.0 / 240.0, flip_ratio=1.0,
-                 gravity=(0.0, 0.0, -9.81), rho=1000.0, nu=1.0e-6, ppc=8, min_size=8, num_vcycles=1):
+                 gravity=(0.0, 0.0, -9.81), rho=1000.0, nu=1.0e-6, ppc=8, min_size=8, num_vcycles=1, tol=None,
+                 coarse_iterations=64, pre_smooth=2, post_smooth=4):
         self.shape = tuple(int(s) for s in shape)
         self.dx, self.dt, self.flip_ratio = float(dx), float(dt), float(flip_ratio)
         self.gravity, self.rho, self.nu, self.ppc = tuple(gravity), float(rho), float(nu), ppc
         self.num_vcycles = num_vcycles
+        # tol: solve each pressure to this FP64 relative residual with fcg_solve (the product's
+        # tolerance mode, W-cycle preconditioner with these coarse and smoothing counts) instead of
+        # the reference's fixed num_vcycles W-cycles
+        self.tol = tol
+        self.fcg_options = dict(coarse_iterations=coarse_iterations, pre_smooth=pre_smooth, post_smooth=post_smooth)
+        self.last_cycles = 0
         self.pos = c(positions).copy()
         self.vel = c(velocities).copy()
         self.obstacle = np.zeros(self.shape, np.uint8) if obstacle is None else c(obstacle, np.uint8)
@@ -423,8 +420,15 @@ class OracleSim:
         u, v, w = grid_domain_bc(u, v, w, s)
         u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s)
         self.trace.update(pre_u=u, pre_v=v, pre_w=w, pressure_in=self.pressure.copy())
-        self.pressure, rhs, op0 = pressure_solve(u, v, w, ff, self.pressure, dx, dt, self.rho, self.num_vcycles, s,
-                                                 self.levels)
+        if self.tol is None:
+            self.pressure, rhs, op0 = pressure_solve(u, v, w, ff, self.pressure, dx, dt, self.rho, self.num_vcycles,
+                                                     s, self.levels)
+            self.last_cycles = self.num_vcycles
+        else:
+            rhs = pressure_rhs(u, v, w, ff, dx, dt, self.rho, s)
+            p64, hist = fcg_solve(rhs, ff, s, dx, p0=self.pressure, tol=self.tol, **self.fcg_options)
+            self.pressure = neumann_domain_bc(p64.astype(np.float32), s)
+            self.last_cycles = len(hist) - 1
         self.trace.update(rhs=rhs, ff=ff, pressure=self.pressure.copy())
         u, v, w = pressure_correction(u, v, w, self.pressure, dx, dt, self.rho, s)
         u, v, w = grid_domain_bc(u, v, w, s)
