@@ -74,7 +74,8 @@ def parse_args():
                     help="red-black iterations before,after the coarse-grid correction in the W-cycle preconditioner "
                          "of the timed steps, e.g. 2,4 (auto: the fastest of 2,4 (the reference's), 1,2 and 1,1 to the "
                          "tolerance in the Poisson comparison, with 4 coarsest-level iterations)")
-    ap.add_argument("--case", choices=["step", "sweep0", "wcycle", "batch", "unet", "collider"], default="step",
+    ap.add_argument("--case", choices=["step", "sweep0", "wcycle", "batch", "unet", "collider", "particles"],
+                    default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
                          "(no particles: a small-memory case for profiling the dominant kernel); batch: the batched "
                          "uneven-scenes workload (32 scenes of sizes 48-160, one launch per stage)")
@@ -190,6 +191,39 @@ def collider_case(args):
         "voxelise_ms": vox_ms,
         "voxelise_ray_triangle_tests_per_s_bruteforce_equivalent": cells * triangles / (vox_ms * 1e-3),
         "clocks": clocks.summary()}), flush=True)
+
+
+def particles_case(args):
+    """The particle stages of one step launched alone on the block scene at --size^3 (after one full
+    step, so the particles are sorted and moving): count, scan, sort, the reference-order and the tiled
+    P2G gather, the fused particle update; device time per launch and algorithmic GB/s. A small-memory
+    case for profiling these kernels."""
+    import torch
+
+    from continuum_liquid_b200 import scenes, solver
+    from continuum_liquid_b200.backend import Backend
+
+    kernels = Backend(0)
+    scene = scenes.block(args.size)
+    positions, velocities = scenes.seed_particles(scene)
+    sim = solver.FlipSolver(kernels, scene.grid_shape, scene.dx, positions, velocities, dt=scene.dt,
+                            options=solver.StepOptions(flip_ratio=0.95, tol=TOL, gravity=scene.gravity, rho=scene.rho,
+                                                       nu=scene.nu), min_size=scene.min_size)
+    for _ in range(max(1, args.warmup)):
+        sim.step()
+    torch.cuda.synchronize()
+    peak, peak_kind = measured_peak_hbm()
+    out = {"case": "particles", "grid": list(scene.grid_shape), "particles": sim.n, "peak_gbs": peak,
+           "peak_source": peak_kind}
+    torch.cuda.nvtx.range_push("stages")
+    rows = kernel_rooflines(sim, peak, 1.0, reps=max(1, args.steps))
+    sim.options.p2g = "exact"
+    rows += [dict(r, stage="p2g_exact") for r in kernel_rooflines(sim, peak, 1.0, reps=max(1, args.steps))
+             if r["stage"] == "p2g"]
+    torch.cuda.nvtx.range_pop()
+    out["stages"] = [{k: r[k] for k in ("stage", "kernels", "ms", "algorithmic_bytes", "achieved", "frac")}
+                     for r in rows]
+    print(json.dumps(out), flush=True)
 
 
 def unet_flops_per_voxel() -> float:
@@ -1009,6 +1043,8 @@ def main():
         unet_case(args)
     elif args.case == "collider":
         collider_case(args)
+    elif args.case == "particles":
+        particles_case(args)
     else:
         our_arm(args)
 

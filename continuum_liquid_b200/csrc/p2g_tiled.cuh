@@ -1,8 +1,8 @@
 // P2G as a tiled, deterministic scatter (the tolerance-mode path; the reference-order gather of
 // binning.cuh stays the parity path). Same results as particles.cl:135-227 up to the order in which
 // each cell's weighted sums are added: every weight is computed exactly as the reference computes
-// it, the fluid fraction (an integer count) is identical, and a face velocity is 0 exactly when the
-// reference's is.
+// it, the fluid fraction (an integer count) is identical, and a face that no particle weighs is 0 in
+// both.
 //
 // Why: the reference visits each particle from the 27 cells around its bin (27 tent evaluations per
 // particle per face type). Here each particle is visited once. A particle in bin b (b = floor(s -

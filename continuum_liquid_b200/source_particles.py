@@ -103,6 +103,7 @@ class DeviceSources:
             added = int(self.total.item())
             if added == 0:
                 continue
+            sim.n = n  # the particles so far (outflows and earlier fills) survive a reallocation
             sim.ensure_capacity(n + added)
             st = self.rng.bit_generator.state["state"]
             state, inc = int(st["state"]), int(st["inc"])

@@ -99,8 +99,8 @@ int clb_particle_to_grid(const float* particles, const float* velocity, float* p
 /* particles.cl:135-227 particle_to_grid_gather, the same inputs and outputs, computed as a tiled
  * scatter that visits each particle once (the tolerance-mode path). Every weight is the reference's;
  * the sums of a cell are added in a different (fixed) order, so velocities agree with
- * clb_particle_to_grid_gather to float rounding (not bit for bit); the fluid fraction and the set of
- * zero faces are identical. Deterministic: the same inputs give the same bits on every run. */
+ * clb_particle_to_grid_gather to float rounding (not bit for bit); the fluid fraction is identical
+ * and a face that no particle weighs is 0 in both. Deterministic: the same inputs give the same bits on every run. */
 int clb_particle_to_grid_gather_tiled(const float* particles, const float* velocity, const int32_t* bin_offsets,
                                       const int32_t* bin_counts, float* u, float* v, float* w, float* fluid_fraction,
                                       float inv_dx, float inv_particles_per_cell, int nx, int ny, int nz,

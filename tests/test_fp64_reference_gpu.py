@@ -27,7 +27,9 @@ def test_fp64_reference_solution_matches_fp64_only_wcycle(backend, oracle, name)
     assert st.rel_residual <= 1e-11
     p_gpu = ps.pressure64.cpu().numpy()
     rhs, ff = ps.rhs.cpu().numpy(), sim.fluid_fraction.cpu().numpy()
-    p_ref, hist = oracle.fp64_pressure_solve(rhs, ff, scene.grid_shape, scene.dx, tol=1e-12, max_cycles=400)
+    # the operator's cell size as the solver passes it (float32, as the reference passes FIELD_DTYPE(dx))
+    delta = float(np.float32(scene.dx))
+    p_ref, hist = oracle.fp64_pressure_solve(rhs, ff, scene.grid_shape, delta, tol=1e-12, max_cycles=400)
     assert hist[-1] <= 1e-12
     fluid = np.zeros(scene.grid_shape, bool)
     fluid[1:-1, 1:-1, 1:-1] = ff[1:-1, 1:-1, 1:-1] > 0

@@ -1,7 +1,8 @@
 """The tiled P2G (each particle visited once, the tolerance-mode path) against the reference-order
-gather and the oracle: the fluid fraction and the set of zero faces bit for bit, the face velocities
-within 1e-5 of the field's largest magnitude (only the order of each cell's sums differs), the same
-bits on every run; at 64^3 and at the 256^3 block of the benchmark."""
+gather and the oracle: the fluid fraction bit for bit, the face velocities within 1e-5 of the field's
+largest magnitude (only the order of each cell's sums differs, so a sum that cancels can come out as
+an exact 0 in one order and a tiny value in the other), the same bits on every run; at 64^3 and at
+the 256^3 block of the benchmark."""
 
 from __future__ import annotations
 
@@ -30,7 +31,6 @@ def bin_and_gather(backend, pos, vel, shape, dx, tiled):
 
 def check_close(got, ref):
     for a, b in zip(got, ref):
-        assert np.array_equal(a == 0, b == 0)
         scale = float(np.abs(b).max()) or 1.0
         assert float(np.abs(a.astype(np.float64) - b).max()) <= TOL * scale
 
