@@ -715,7 +715,7 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                 kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16, coarse_iterations=4,
                 pre_smooth=pre, post_smooth=post)
     p_tmp = torch.empty_like(sim.pressure)
-    rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": []}
+    rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": [], "fcg_tuned_learned": []}
     rows.update({name: [] for name in solvers if "_c" in name})
     fp32 = []
     rho = sim.options.rho
@@ -726,6 +726,9 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
         variants = [(name, ps, None) for name, ps in solvers.items()]
         if warm is not None:
             variants.append(("fcg_learned", solvers["fcg"], warm))
+            # the same guess with the preconditioner settings the timed steps use (FP16 coarse levels,
+            # 4 coarsest-level iterations, one smoothing sweep each way): the comparison that decides
+            variants.append(("fcg_tuned_learned", solvers["fcg_fp16_c4_s11"], warm))
         for name, ps, ws in variants:
             for rep in range(2):  # the first run captures graphs and tunes; the second is timed
                 p_tmp.copy_(saved)
@@ -776,7 +779,7 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                      "rel_max": max(r["rel"] for r in rs), "cycles": [r["cycles"] for r in rs],
                      "ms": [round(r["ms"], 3) for r in rs],
                      "convergence_factor_mean": mean(rs, "factor")}
-        if name == "fcg_learned":
+        if name in ("fcg_learned", "fcg_tuned_learned"):
             out[name]["guess_used"] = [r["guess"] for r in rs]
             out[name]["learned_rel"] = [r["learned_rel"] for r in rs]
             out[name]["previous_rel"] = [r["initial_rel"] for r in rows["fcg"]]
@@ -813,6 +816,16 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
     if rows["fcg_learned"]:
         out["speedup_learned_vs_plain_fcg"] = out["fcg"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
         out["speedup_learned_vs_refine"] = out["refine"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
+    if rows["fcg_tuned_learned"]:
+        tuned = out["fcg_fp16_c4_s11"]
+        learned = out["fcg_tuned_learned"]
+        out["learned_at_timed_settings"] = {
+            "speedup": tuned["ms_mean"] / learned["ms_mean"], "ms_plain": tuned["ms_mean"],
+            "ms_learned": learned["ms_mean"], "cycles_plain": tuned["cycles_mean"],
+            "cycles_learned": learned["cycles_mean"],
+            "cycles_saved_ms": (tuned["cycles_mean"] - learned["cycles_mean"]) * tuned["ms_mean"] /
+            max(tuned["cycles_mean"], 1.0),
+        }
     return out
 
 
@@ -858,10 +871,10 @@ def our_arm(args):
             coarse_k = poisson.get("coarse_iterations_chosen", coarse_k)
         if args.smoothing == "auto":
             smoothing = tuple(poisson.get("smoothing_chosen", smoothing))
-        if args.learned == "auto" and "fcg_learned" in poisson:
+        if args.learned == "auto" and "fcg_tuned_learned" in poisson:
             # the rule: the learned guess in the timed steps only when it makes the solve faster,
             # network evaluation included
-            use_learned = poisson["fcg_learned"]["ms_mean"] < poisson["fcg"]["ms_mean"]
+            use_learned = poisson["fcg_tuned_learned"]["ms_mean"] < poisson["fcg_fp16_c4_s11"]["ms_mean"]
     else:
         poisson["learned_vs_plain"] = "skipped (--poisson-steps 0)"
     sim.options.warm_start = warm if use_learned else None

@@ -57,11 +57,12 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_neumann_domain_bc": [P, I, I, I, P],
     "clb_pressure_correction_f64": [P, P, P, P, F, F, I, I, I, P],
     "clb_neumann_domain_bc_f64": [P, I, I, I, P],
-    "clb_build_finest_operator": [P, P, P, P, P, I, I, I, P],
-    "clb_rbgs_step": [P, P, P, P, P, P, P, F, I, I, I, I, P],
-    "clb_restrict_residual": [P] * 14 + [F, I, I, I, I, I, I, P],
-    "clb_prolongate": [P, P, P, I, I, I, I, I, I, P],
-    "clb_coarse_smooth": [P, P, P, P, P, P, P, F, I, I, I, I, P],
+    "clb_mg_pack_finest": [P, P, P, P, P, P, P, I, I, I, P],
+    "clb_mg_unpack_finest": [P, P, P, P, P, I, I, I, P],
+    "clb_mg_pack_level": [P, P, P, P, P, P, P, I, I, I, P],
+    "clb_mg_unpack_level": [P, P, P, P, P, P, P, I, I, I, P],
+    "clb_mg_smooth_level": [P, P, P, P, F, I, I, I, I, P],
+    "clb_mg_coarse_solve_level": [P, P, P, P, F, I, I, I, I, P],
     "clb_mg_rhs_operator": [P, P, P, P, P, P, F, F, I, I, I, P],
     "clb_source_cell_counts": [P, L, F, I, I, I, P, P],
     "clb_source_keep": [P, L, F, I, I, I, P, P, P],

@@ -483,97 +483,90 @@ int clb_neumann_domain_bc_f64(double* pressure, int nx, int ny, int nz, void* st
     return neumann_domain_bc_impl<double>(pressure, nx, ny, nz, stream);
 }
 
-// ---- multigrid, reference layout ----------------------------------------------------------------
+// ---- multigrid: the reference's level arrays through the product kernels -----------------------
 
-int clb_build_finest_operator(const float* mask, float* diagonal, float* weight_x, float* weight_y, float* weight_z,
-                              int nx, int ny, int nz, void* stream) {
+int clb_mg_pack_finest(const float* mask, const float* diagonal, const float* weight_x, const float* weight_y,
+                       const float* weight_z, uint8_t* op0, int32_t* invalid, int nx, int ny, int nz, void* stream) {
     CLB_GRID_ARGS_OK(nx, ny, nz);
-    CLB_REQUIRE(mask && diagonal && weight_x && weight_y && weight_z, "build_finest_operator: null pointer");
+    CLB_REQUIRE(mask && diagonal && weight_x && weight_y && weight_z && op0 && invalid, "mg_pack_finest: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_ref_build_finest_operator<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(mask, diagonal, weight_x, weight_y,
-                                                                                     weight_z, nx, ny, nz);
-    CLB_LAUNCH_CHECK("k_ref_build_finest_operator");
+    k_pack_finest<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(mask, diagonal, weight_x, weight_y, weight_z,
+                                                                        op0, invalid, C);
+    CLB_LAUNCH_CHECK("k_pack_finest");
     return 0;
 }
 
-int clb_rbgs_step(float* p, const float* b, const float* mask, const float* diagonal, const float* weight_x,
-                  const float* weight_y, const float* weight_z, float delta, int parity, int nx, int ny, int nz,
-                  void* stream) {
+int clb_mg_unpack_finest(const uint8_t* op0, float* diagonal, float* weight_x, float* weight_y, float* weight_z,
+                         int nx, int ny, int nz, void* stream) {
     CLB_GRID_ARGS_OK(nx, ny, nz);
-    CLB_REQUIRE(parity == 0 || parity == 1, "rbgs_step: parity must be 0 or 1");
-    CLB_REQUIRE(p && b && mask && diagonal && weight_x && weight_y && weight_z, "rbgs_step: null pointer");
+    CLB_REQUIRE(op0 && diagonal && weight_x && weight_y && weight_z, "mg_unpack_finest: null pointer");
     const i64 C = (i64)nx * ny * nz;
-    k_ref_rbgs_step<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(p, b, mask, diagonal, weight_x, weight_y,
-                                                                         weight_z, delta, parity, nx, ny, nz);
-    CLB_LAUNCH_CHECK("k_ref_rbgs_step");
+    k_unpack_finest<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(op0, diagonal, weight_x, weight_y, weight_z, C);
+    CLB_LAUNCH_CHECK("k_unpack_finest");
     return 0;
 }
 
-int clb_restrict_residual(const float* fine_p, const float* fine_b, const float* fine_mask, const float* fine_diagonal,
-                          const float* fine_weight_x, const float* fine_weight_y, const float* fine_weight_z,
-                          float* coarse_p, float* coarse_b, float* coarse_mask, float* coarse_diagonal,
-                          float* coarse_weight_x, float* coarse_weight_y, float* coarse_weight_z, float delta,
-                          int fine_nx, int fine_ny, int fine_nz, int coarse_nx, int coarse_ny, int coarse_nz,
-                          void* stream) {
-    CLB_GRID_ARGS_OK(fine_nx, fine_ny, fine_nz);
-    CLB_GRID_ARGS_OK(coarse_nx, coarse_ny, coarse_nz);
-    CLB_REQUIRE(fine_p && fine_b && fine_mask && fine_diagonal && fine_weight_x && fine_weight_y && fine_weight_z &&
-                    coarse_p && coarse_b && coarse_mask && coarse_diagonal && coarse_weight_x && coarse_weight_y &&
-                    coarse_weight_z,
-                "restrict_residual: null pointer");
-    const i64 C = (i64)coarse_nx * coarse_ny * coarse_nz;
-    k_ref_restrict_residual<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(
-        fine_p, fine_b, fine_mask, fine_diagonal, fine_weight_x, fine_weight_y, fine_weight_z, coarse_p, coarse_b,
-        coarse_mask, coarse_diagonal, coarse_weight_x, coarse_weight_y, coarse_weight_z, delta, fine_nx, fine_ny,
-        fine_nz, coarse_nx, coarse_ny, coarse_nz);
-    CLB_LAUNCH_CHECK("k_ref_restrict_residual");
+int clb_mg_pack_level(const float* mask, const float* diagonal, const float* weight_x, const float* weight_y,
+                      const float* weight_z, float* op4, uint8_t* mask_out, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(mask && diagonal && weight_x && weight_y && weight_z && op4 && mask_out, "mg_pack_level: null pointer");
+    CLB_REQUIRE((((uintptr_t)op4) & 15) == 0, "mg_pack_level: op4 must be 16-byte aligned");
+    const i64 C = (i64)nx * ny * nz;
+    k_pack_level<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(mask, diagonal, weight_x, weight_y, weight_z,
+                                                                       reinterpret_cast<float4*>(op4), mask_out, C);
+    CLB_LAUNCH_CHECK("k_pack_level");
     return 0;
 }
 
-int clb_prolongate(const float* coarse_error, float* fine_p, const float* fine_mask, int coarse_nx, int coarse_ny,
-                   int coarse_nz, int fine_nx, int fine_ny, int fine_nz, void* stream) {
-    CLB_GRID_ARGS_OK(fine_nx, fine_ny, fine_nz);
-    CLB_GRID_ARGS_OK(coarse_nx, coarse_ny, coarse_nz);
-    CLB_REQUIRE(coarse_error && fine_p && fine_mask, "prolongate: null pointer");
-    const i64 C = (i64)fine_nx * fine_ny * fine_nz;
-    k_ref_prolongate<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(coarse_error, fine_p, fine_mask, coarse_nx,
-                                                                          coarse_ny, coarse_nz, fine_nx, fine_ny,
-                                                                          fine_nz);
-    CLB_LAUNCH_CHECK("k_ref_prolongate");
+int clb_mg_unpack_level(const float* op4, const uint8_t* mask_in, float* mask, float* diagonal, float* weight_x,
+                        float* weight_y, float* weight_z, int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(op4 && mask_in && mask && diagonal && weight_x && weight_y && weight_z, "mg_unpack_level: null pointer");
+    CLB_REQUIRE((((uintptr_t)op4) & 15) == 0, "mg_unpack_level: op4 must be 16-byte aligned");
+    const i64 C = (i64)nx * ny * nz;
+    k_unpack_level<<<blocks_for(C, MGT), MGT, 0, CLB_STREAM(stream)>>>(reinterpret_cast<const float4*>(op4), mask_in,
+                                                                         mask, diagonal, weight_x, weight_y, weight_z,
+                                                                         C);
+    CLB_LAUNCH_CHECK("k_unpack_level");
     return 0;
 }
 
-// The reference-layout coarse smooth runs one block of 1024 threads directly on the float arrays:
-// rbgs_step's update formula in a loop with block barriers, like multigrid.cl:232-264.
-__global__ void __launch_bounds__(COARSE_THREADS) k_ref_coarse_smooth(float* p, const float* b, const float* mask,
-                                                                       const float* diag, const float* wx,
-                                                                       const float* wy, const float* wz, float delta,
-                                                                       int iterations, int nx, int ny, int nz) {
-    const int C = nx * ny * nz;
-    const float d2 = delta * delta;
-    const i64 sx = (i64)ny * nz, sy = nz;
+int clb_mg_smooth_level(float* p, const float* b, const float* op4, const uint8_t* mask, float delta, int iterations,
+                        int nx, int ny, int nz, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(iterations >= 0, "mg_smooth_level: negative iterations");
+    CLB_REQUIRE(p && b && op4 && mask, "mg_smooth_level: null pointer");
+    CLB_REQUIRE((((uintptr_t)op4) & 15) == 0, "mg_smooth_level: op4 must be 16-byte aligned");
+    const i64 C = (i64)nx * ny * nz;
+    const float4* opc = reinterpret_cast<const float4*>(op4);
+    cudaStream_t s = CLB_STREAM(stream);
     for (int it = 0; it < iterations; ++it)
         for (int parity = 0; parity < 2; ++parity) {
-            for (int c = threadIdx.x; c < C; c += COARSE_THREADS) {
-                int i, j, k;
-                gcoord(c, ny, nz, i, j, k);
-                if (!interior(i, j, k, nx, ny, nz) || mask[c] <= 0.0f || ((i + j + k) & 1) != parity) continue;
-                const float d = diag[c];
-                if (d > 0.0f) p[c] = (ref_wsum(p, wx, wy, wz, c, sx, sy) - d2 * b[c]) / d;
-            }
-            __syncthreads();
+            launch(blocks_for(C, MGT), MGT, 0, s)(k_rbgs<false>, p, b, (const uint8_t*)nullptr, opc, mask, delta,
+                                                  parity, nx, ny, nz);
+            CLB_LAUNCH_CHECK("k_rbgs");
         }
+    return 0;
 }
 
-int clb_coarse_smooth(float* p, const float* b, const float* mask, const float* diagonal, const float* weight_x,
-                      const float* weight_y, const float* weight_z, float delta, int iterations, int nx, int ny,
-                      int nz, void* stream) {
+int clb_mg_coarse_solve_level(float* p, const float* b, const float* op4, const uint8_t* mask, float delta,
+                              int iterations, int nx, int ny, int nz, void* stream) {
     CLB_GRID_ARGS_OK(nx, ny, nz);
-    CLB_REQUIRE(iterations >= 0, "coarse_smooth: negative iterations");
-    CLB_REQUIRE(p && b && mask && diagonal && weight_x && weight_y && weight_z, "coarse_smooth: null pointer");
-    k_ref_coarse_smooth<<<1, COARSE_THREADS, 0, CLB_STREAM(stream)>>>(p, b, mask, diagonal, weight_x, weight_y,
-                                                                       weight_z, delta, iterations, nx, ny, nz);
-    CLB_LAUNCH_CHECK("k_ref_coarse_smooth");
+    CLB_REQUIRE(iterations >= 0, "mg_coarse_solve_level: negative iterations");
+    CLB_REQUIRE(p && b && op4 && mask, "mg_coarse_solve_level: null pointer");
+    CLB_REQUIRE((((uintptr_t)op4) & 15) == 0, "mg_coarse_solve_level: op4 must be 16-byte aligned");
+    const i64 C = (i64)nx * ny * nz;
+    CLB_REQUIRE(C < (1ll << 31), "mg_coarse_solve_level: level too large");
+    const float4* opc = reinterpret_cast<const float4*>(op4);
+    cudaStream_t s = CLB_STREAM(stream);
+    if (C <= COARSE_SMEM_CELLS)
+        launch(1, COARSE_THREADS, coarse_smem_bytes((int)C), s)(k_coarse_solve<true, false>, p, b,
+                                                                (const uint8_t*)nullptr, opc, mask, delta, iterations,
+                                                                nx, ny, nz, (const float*)nullptr);
+    else
+        launch(1, COARSE_THREADS, 0, s)(k_coarse_solve<false, false>, p, b, (const uint8_t*)nullptr, opc, mask, delta,
+                                        iterations, nx, ny, nz, (const float*)nullptr);
+    CLB_LAUNCH_CHECK("k_coarse_solve");
     return 0;
 }
 

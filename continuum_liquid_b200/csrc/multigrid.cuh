@@ -21,141 +21,63 @@ namespace clb {
 constexpr int MGT = 256;
 constexpr int MG_MAX_LEVELS = 16;
 
-// multigrid.cl:3-5 domain_diagonal
-__device__ __forceinline__ float domain_diagonal(int i, int j, int k, int nx, int ny, int nz) {
-    return 6.0f - (float)(i == 1) - (float)(i == nx - 2) - (float)(j == 1) - (float)(j == ny - 2) - (float)(k == 1) -
-           (float)(k == nz - 2);
-}
-
 // ------------------------------------------------------------------------------------------------
-// Reference layout kernels
+// The reference's level arrays (float32 mask, diagonal, weight_x, weight_y, weight_z per level,
+// multigrid.py:18-50) converted to and from the product's level formats, so that the stage functions
+// that take the reference's arrays (multigrid.w_cycle, smooth, coarse_smooth, pressure_solve) run the
+// product kernels: the finest level packed into one byte per cell, a coarse level into a float4
+// (diagonal, wx, wy, wz) plus a mask byte. A cell is fluid where its mask is > 0, as the reference
+// tests it (multigrid.cl:38, 220, 251).
 // ------------------------------------------------------------------------------------------------
-__device__ __forceinline__ float ref_wsum(const float* p, const float* wx, const float* wy, const float* wz, i64 c,
-                                          i64 sx, i64 sy) {
-    return wx[c] * p[c + sx] + wx[c - sx] * p[c - sx] + wy[c] * p[c + sy] + wy[c - sy] * p[c - sy] + wz[c] * p[c + 1] +
-           wz[c - 1] * p[c - 1];
-}
-
-// multigrid.cl:63-88 build_finest_operator
-__global__ void __launch_bounds__(MGT) k_ref_build_finest_operator(const float* __restrict__ mask, float* diag,
-                                                                    float* wx, float* wy, float* wz, int nx, int ny,
-                                                                    int nz) {
-    const i64 C = (i64)nx * ny * nz;
+__global__ void __launch_bounds__(MGT) k_pack_finest(const float* __restrict__ mask, const float* __restrict__ diag,
+                                                      const float* __restrict__ wx, const float* __restrict__ wy,
+                                                      const float* __restrict__ wz, uint8_t* __restrict__ op0,
+                                                      int* __restrict__ invalid, i64 C) {
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c >= C) return;
-    diag[c] = 0.0f;
-    wx[c] = 0.0f;
-    wy[c] = 0.0f;
-    wz[c] = 0.0f;
-    int i, j, k;
-    gcoord(c, ny, nz, i, j, k);
-    if (!interior(i, j, k, nx, ny, nz) || mask[c] <= 0.0f) return;
-    diag[c] = domain_diagonal(i, j, k, nx, ny, nz);
-    if (i < nx - 2) wx[c] = mask[c + (i64)ny * nz] > 0.0f ? 1.0f : 0.0f;
-    if (j < ny - 2) wy[c] = mask[c + nz] > 0.0f ? 1.0f : 0.0f;
-    if (k < nz - 2) wz[c] = mask[c + 1] > 0.0f ? 1.0f : 0.0f;
+    const float d = __ldg(diag + c), x = __ldg(wx + c), y = __ldg(wy + c), z = __ldg(wz + c);
+    // the byte holds a diagonal 0..7 and 0/1 weights, which is what build_finest_operator produces
+    const bool ok = d >= 0.0f && d <= 7.0f && d == floorf(d) && (x == 0.0f || x == 1.0f) &&
+                    (y == 0.0f || y == 1.0f) && (z == 0.0f || z == 1.0f);
+    if (!ok) atomicAdd(invalid, 1);
+    op0[c] = (uint8_t)(((uint32_t)d & 7u) | ((uint32_t)(x == 1.0f) << 3) | ((uint32_t)(y == 1.0f) << 4) |
+                       ((uint32_t)(z == 1.0f) << 5) | ((uint32_t)(__ldg(mask + c) > 0.0f) << 6));
 }
 
-// multigrid.cl:203-230 rbgs_step (one colour; zeroes p wherever mask <= 0)
-__global__ void __launch_bounds__(MGT) k_ref_rbgs_step(float* p, const float* __restrict__ b,
-                                                        const float* __restrict__ mask, const float* __restrict__ diag,
-                                                        const float* __restrict__ wx, const float* __restrict__ wy,
-                                                        const float* __restrict__ wz, float delta, int parity, int nx,
-                                                        int ny, int nz) {
-    const i64 C = (i64)nx * ny * nz;
+__global__ void __launch_bounds__(MGT) k_unpack_finest(const uint8_t* __restrict__ op0, float* __restrict__ diag,
+                                                        float* __restrict__ wx, float* __restrict__ wy,
+                                                        float* __restrict__ wz, i64 C) {
     const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
     if (c >= C) return;
-    int i, j, k;
-    gcoord(c, ny, nz, i, j, k);
-    const float m = mask[c];
-    if (!interior(i, j, k, nx, ny, nz) || m <= 0.0f || ((i + j + k) & 1) != parity) {
-        if (m <= 0.0f) p[c] = 0.0f;
-        return;
-    }
-    const float d = diag[c];
-    if (d > 0.0f) p[c] = (ref_wsum(p, wx, wy, wz, c, (i64)ny * nz, nz) - delta * delta * b[c]) / d;
+    const uint32_t o = __ldg(op0 + c);
+    diag[c] = (float)(o & 7u);
+    wx[c] = (float)((o >> 3) & 1u);
+    wy[c] = (float)((o >> 4) & 1u);
+    wz[c] = (float)((o >> 5) & 1u);
 }
 
-// multigrid.cl:25-61 residual on the reference layout
-__device__ __forceinline__ float ref_residual(const float* p, const float* b, const float* mask, const float* diag,
-                                              const float* wx, const float* wy, const float* wz, float inv_delta2,
-                                              int i, int j, int k, int nx, int ny, int nz) {
-    const i64 c = gidx(i, j, k, ny, nz);
-    float ap = 0.0f;
-    if (interior(i, j, k, nx, ny, nz) && !(mask[c] <= 0.0f))
-        ap = (ref_wsum(p, wx, wy, wz, c, (i64)ny * nz, nz) - diag[c] * p[c]) * inv_delta2;
-    return b[c] - ap;
+__global__ void __launch_bounds__(MGT) k_pack_level(const float* __restrict__ mask, const float* __restrict__ diag,
+                                                     const float* __restrict__ wx, const float* __restrict__ wy,
+                                                     const float* __restrict__ wz, float4* __restrict__ op,
+                                                     uint8_t* __restrict__ mask_out, i64 C) {
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    op[c] = make_float4(__ldg(diag + c), __ldg(wx + c), __ldg(wy + c), __ldg(wz + c));
+    mask_out[c] = __ldg(mask + c) > 0.0f ? 1 : 0;
 }
 
-// multigrid.cl:90-180 restrict_residual
-__global__ void __launch_bounds__(MGT) k_ref_restrict_residual(
-    const float* __restrict__ fp, const float* __restrict__ fb, const float* __restrict__ fm,
-    const float* __restrict__ fd, const float* __restrict__ fwx, const float* __restrict__ fwy,
-    const float* __restrict__ fwz, float* cp, float* cb, float* cm, float* cd, float* cwx, float* cwy, float* cwz,
-    float delta, int fnx, int fny, int fnz, int cnx, int cny, int cnz) {
-    const i64 C = (i64)cnx * cny * cnz;
-    const i64 ci = (i64)blockIdx.x * MGT + threadIdx.x;
-    if (ci >= C) return;
-    cp[ci] = 0.0f;
-    cb[ci] = 0.0f;
-    cm[ci] = 0.0f;
-    cd[ci] = 0.0f;
-    cwx[ci] = 0.0f;
-    cwy[ci] = 0.0f;
-    cwz[ci] = 0.0f;
-    int I, J, K;
-    gcoord(ci, cny, cnz, I, J, K);
-    if (!interior(I, J, K, cnx, cny, cnz)) return;
-    const int si = 1 + 2 * (I - 1), sj = 1 + 2 * (J - 1), sk = 1 + 2 * (K - 1);
-    const float inv_delta2 = 1.0f / (delta * delta);
-    float rhs = 0.0f, dsum = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    int active = 0;
-    for (int di = 0; di < 2; ++di)
-        for (int dj = 0; dj < 2; ++dj)
-            for (int dk = 0; dk < 2; ++dk) {
-                const int i = si + di, j = sj + dj, k = sk + dk;
-                if (!interior(i, j, k, fnx, fny, fnz)) continue;
-                const i64 f = gidx(i, j, k, fny, fnz);
-                if (fm[f] <= 0.0f) continue;
-                ++active;
-                rhs += ref_residual(fp, fb, fm, fd, fwx, fwy, fwz, inv_delta2, i, j, k, fnx, fny, fnz);
-                dsum += fd[f];
-                const float wx = fwx[f], wy = fwy[f], wz = fwz[f];
-                if (wx > 0.0f) {
-                    if (di == 0) dsum -= 2.0f * wx;
-                    else cx += wx;
-                }
-                if (wy > 0.0f) {
-                    if (dj == 0) dsum -= 2.0f * wy;
-                    else cy += wy;
-                }
-                if (wz > 0.0f) {
-                    if (dk == 0) dsum -= 2.0f * wz;
-                    else cz += wz;
-                }
-            }
-    if (active > 0) {
-        cb[ci] = rhs;
-        cm[ci] = 1.0f;
-        cd[ci] = dsum;
-        cwx[ci] = cx;
-        cwy[ci] = cy;
-        cwz[ci] = cz;
-    }
-}
-
-// multigrid.cl:182-201 prolongate
-__global__ void __launch_bounds__(MGT) k_ref_prolongate(const float* __restrict__ ce, float* fp,
-                                                         const float* __restrict__ fm, int cnx, int cny, int cnz,
-                                                         int fnx, int fny, int fnz) {
-    const i64 C = (i64)fnx * fny * fnz;
-    const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
-    if (f >= C) return;
-    int i, j, k;
-    gcoord(f, fny, fnz, i, j, k);
-    if (!interior(i, j, k, fnx, fny, fnz) || fm[f] <= 0.0f) return;
-    const int I = min((i - 1) / 2 + 1, cnx - 2), J = min((j - 1) / 2 + 1, cny - 2), K = min((k - 1) / 2 + 1, cnz - 2);
-    fp[f] += ce[gidx(I, J, K, cny, cnz)];
+__global__ void __launch_bounds__(MGT) k_unpack_level(const float4* __restrict__ op, const uint8_t* __restrict__ m,
+                                                       float* __restrict__ mask, float* __restrict__ diag,
+                                                       float* __restrict__ wx, float* __restrict__ wy,
+                                                       float* __restrict__ wz, i64 C) {
+    const i64 c = (i64)blockIdx.x * MGT + threadIdx.x;
+    if (c >= C) return;
+    const float4 o = __ldg(op + c);
+    mask[c] = __ldg(m + c) ? 1.0f : 0.0f;
+    diag[c] = o.x;
+    wx[c] = o.y;
+    wy[c] = o.z;
+    wz[c] = o.w;
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -1,15 +1,17 @@
 """Multigrid W-cycle (mirrors Solver/Kernel/multigrid.py).
 
-Two forms are provided:
+The reference keeps five float32 arrays per level (mask, diagonal, wx, wy, wz) plus p and b, and its
+host code walks the W-cycle recursion one OpenCL kernel per step. Here:
 
-* the reference's own form: ``create_multigrid_levels`` returns per-level float32 arrays (p, b,
-  mask, and the (diagonal, wx, wy, wz) operator tuple) and ``w_cycle``/``smooth``/``coarse_smooth``
-  dispatch one CUDA kernel per reference kernel, with the reference's recursion;
-* the packed form used by the solver: ``MultigridHierarchy`` keeps the finest operator in one byte
-  per cell and the coarse operators as float4 + mask byte, builds the Galerkin coarse operators once
-  per solve, and runs a whole W-cycle with one library call (capturable in a CUDA graph).
+* ``MultigridHierarchy`` is the product path: the finest operator in one byte per cell, the coarse
+  operators as float4 + mask byte, built once per solve, a whole W-cycle in one library call
+  (capturable in a CUDA graph), fluid tiles, cluster and bottom visits;
+* the reference's stage functions keep their names and arguments (``create_multigrid_levels``,
+  ``w_cycle``, ``smooth``, ``coarse_smooth``) for callers that hold the reference's level arrays:
+  they pack those arrays into the product formats, run the product kernels and write the coarse
+  operators back where the reference's restriction leaves them.
 
-Both give the same values as the CPU restatement of the reference.
+Both give the reference's values bit for bit (tests compare them with the CPU restatement).
 """
 
 from __future__ import annotations
@@ -59,58 +61,90 @@ def create_multigrid_levels(context, shape, min_size: int = 8):
     return p_levels, b_levels, mask_levels, operator_levels, level_shapes
 
 
+def _stage_cache(kernels: Backend) -> dict:
+    """Per-backend workspace of the stage functions (packed hierarchies and level buffers)."""
+    cache = getattr(kernels, "_stage_cache", None)
+    if cache is None:
+        cache = {}
+        kernels._stage_cache = cache
+    return cache
+
+
+def stage_min_size(shape, level_shapes) -> int:
+    """The ``min_size`` of ``create_multigrid_levels`` that produced ``level_shapes`` for ``shape``."""
+    wanted = [tuple(int(x) for x in s) for s in level_shapes]
+    for m in (8, *range(2, 65)):
+        if level_shapes_for(shape, m) == wanted:
+            return m
+    raise ValueError(f"level shapes {wanted} are not a multigrid pyramid of {tuple(shape)}")
+
+
+def _stage_hierarchy(kernels: Backend, shape, level_shapes, delta) -> "MultigridHierarchy":
+    key = ("hierarchy", tuple(int(s) for s in shape), tuple(tuple(s) for s in level_shapes), float(FIELD_DTYPE(delta)))
+    cache = _stage_cache(kernels)
+    if key not in cache:
+        cache[key] = MultigridHierarchy(kernels, shape, float(delta), stage_min_size(shape, level_shapes))
+    return cache[key]
+
+
+def _packed_level(kernels: Backend, shape):
+    key = ("level", tuple(int(s) for s in shape))
+    cache = _stage_cache(kernels)
+    if key not in cache:
+        cache[key] = (torch.zeros((*shape, 4), dtype=torch.float32, device=kernels.device),
+                      torch.zeros(tuple(shape), dtype=torch.uint8, device=kernels.device))
+    return cache[key]
+
+
+def write_coarse_operators(kernels: Backend, queue, hierarchy: "MultigridHierarchy", mask_levels,
+                           operator_levels) -> None:
+    """The hierarchy's coarse operators into the reference's level arrays (mask as 1.0 / 0.0, then
+    diagonal, wx, wy, wz): what restrict_residual (multigrid.cl:90-180) leaves there."""
+    for level in range(1, hierarchy.levels):
+        kernels.call("clb_mg_unpack_level", hierarchy.op[level], hierarchy.mask[level], mask_levels[level - 1],
+                     *operator_levels[level - 1], *hierarchy.shapes[level], stream=queue)
+
+
 def w_cycle(kernels: Backend, queue, level, p_levels, b_levels, mask_levels, operator_levels, p_level0, b_level0,
             mask_level0, operator_level0, base_delta, level_shapes, level0_shape, pre_smooth, post_smooth,
             coarse_smooth_iterations) -> None:
-    """multigrid.py:53-187: one dense multigrid W-cycle for laplace(p) = b (reference layout)."""
-    if level == 0:
-        p, b, mask, operator, shape = p_level0, b_level0, mask_level0, operator_level0, level0_shape
-    else:
-        current = level - 1
-        p, b, mask = p_levels[current], b_levels[current], mask_levels[current]
-        operator, shape = operator_levels[current], level_shapes[current]
+    """multigrid.py:53-187: one W-cycle for laplace(p) = b on the reference's level arrays.
 
-    if level == len(p_levels):
-        coarse_smooth(kernels, queue, p, b, mask, operator, base_delta, pre_smooth + coarse_smooth_iterations, shape)
-        return
-
-    smooth(kernels, queue, p, b, mask, operator, base_delta, pre_smooth, shape)
-    coarse = level
-    coarse_shape = level_shapes[coarse]
-    kernels.call(
-        "clb_restrict_residual",
-        p,
-        b,
-        mask,
-        *operator,
-        p_levels[coarse],
-        b_levels[coarse],
-        mask_levels[coarse],
-        *operator_levels[coarse],
-        float(FIELD_DTYPE(base_delta)),
-        *shape,
-        *coarse_shape,
-        stream=queue,
-    )
-    args = (p_levels, b_levels, mask_levels, operator_levels, p_level0, b_level0, mask_level0, operator_level0,
-            base_delta, level_shapes, level0_shape, pre_smooth, post_smooth, coarse_smooth_iterations)
-    w_cycle(kernels, queue, level + 1, *args)
-    w_cycle(kernels, queue, level + 1, *args)
-    kernels.call("clb_prolongate", p_levels[coarse], p, mask, *coarse_shape, *shape, stream=queue)
-    smooth(kernels, queue, p, b, mask, operator, base_delta, post_smooth, shape)
+    The finest operator (``operator_level0`` with ``mask_level0``, as build_finest_operator writes
+    them) is packed into one byte per cell and the W-cycle runs on the product hierarchy; ``p_level0``
+    is updated in place with the reference's values. The coarse levels' operators and masks are
+    written to ``operator_levels`` / ``mask_levels`` as the reference's restriction leaves them; their
+    ``p_levels`` and ``b_levels`` are the W-cycle's workspace and are not written. The reference's
+    callers start a W-cycle at level 0 only (pressure_solve.py:61-83); so does this function."""
+    if int(level) != 0:
+        raise ValueError("w_cycle runs whole W-cycles from level 0 (the level argument of the reference's "
+                         "recursion); coarse levels are visited inside it")
+    h = _stage_hierarchy(kernels, level0_shape, level_shapes, base_delta)
+    invalid = torch.zeros(1, dtype=torch.int32, device=kernels.device)
+    kernels.call("clb_mg_pack_finest", mask_level0, *operator_level0, h.op0, invalid, *level0_shape, stream=queue)
+    if int(invalid.item()):
+        raise ValueError(f"operator_level0 is not a finest-level operator at {int(invalid.item())} cells "
+                         "(diagonal 0..7 and 0/1 weights, as build_finest_operator writes them)")
+    h.build_coarse(queue=queue)
+    h.w_cycle(p_level0, b_level0, pre_smooth, post_smooth, coarse_smooth_iterations, queue=queue)
+    write_coarse_operators(kernels, queue, h, mask_levels, operator_levels)
 
 
 def smooth(kernels: Backend, queue, p, b, mask, operator, delta, iterations, shape) -> None:
-    """multigrid.py:190-220: red-black Gauss-Seidel, two colour launches per iteration."""
-    for _ in range(iterations):
-        for parity in (0, 1):
-            kernels.call("clb_rbgs_step", p, b, mask, *operator, float(FIELD_DTYPE(delta)), parity, *shape,
-                         stream=queue)
+    """multigrid.py:190-220: red-black Gauss-Seidel on one level of the reference's arrays (packed
+    into the product's coarse-level format for the product sweep kernel)."""
+    op4, mask8 = _packed_level(kernels, shape)
+    kernels.call("clb_mg_pack_level", mask, *operator, op4, mask8, *shape, stream=queue)
+    kernels.call("clb_mg_smooth_level", p, b, op4, mask8, float(FIELD_DTYPE(delta)), int(iterations), *shape,
+                 stream=queue)
 
 
 def coarse_smooth(kernels: Backend, queue, p, b, mask, operator, delta, iterations, shape) -> None:
-    """multigrid.py:223-249: the coarsest level smoothed in one single-block launch."""
-    kernels.call("clb_coarse_smooth", p, b, mask, *operator, float(FIELD_DTYPE(delta)), int(iterations), *shape,
+    """multigrid.py:223-249: the coarsest level smoothed in one single-block launch (the product's
+    coarse solve on the packed level)."""
+    op4, mask8 = _packed_level(kernels, shape)
+    kernels.call("clb_mg_pack_level", mask, *operator, op4, mask8, *shape, stream=queue)
+    kernels.call("clb_mg_coarse_solve_level", p, b, op4, mask8, float(FIELD_DTYPE(delta)), int(iterations), *shape,
                  stream=queue)
 
 

@@ -1,7 +1,9 @@
 """Pressure solve and projection (mirrors Solver/Kernel/pressure_solve.py).
 
 ``pressure_solve`` keeps the reference's signature and algorithm (pressure_rhs,
-build_finest_operator, ``num_vcycles`` W-cycles, Neumann ghost copy) on the reference layout.
+build_finest_operator, ``num_vcycles`` W-cycles, Neumann ghost copy) and runs it through
+``PressureSolver``, writing the reference's outputs (``rhs``, the finest operator arrays and the coarse
+operators) into the caller's arrays.
 
 ``PressureSolver`` is the product path behind the same stage: the packed multigrid hierarchy plus
 
@@ -38,17 +40,24 @@ FIELD_DTYPE = np.float32
 def pressure_solve(kernels: Backend, multigrid_kernels, boundary_kernels, queue, velocity, fluid_fraction, pressure,
                    rhs, p_levels, b_levels, mask_levels, operator_level0, operator_levels, multigrid_level_shapes, dx,
                    dt, rho, num_vcycles, grid_shape):
-    """pressure_solve.py:10-85 on the reference layout (one kernel per reference kernel)."""
-    nx, ny, nz = grid_shape
-    u, v, w = velocity
-    kernels.call("clb_pressure_rhs", u, v, w, fluid_fraction, rhs, float(FIELD_DTYPE(float(rho) / float(dt))),
-                 float(FIELD_DTYPE(1.0 / float(dx))), nx, ny, nz, stream=queue)
-    kernels.call("clb_build_finest_operator", fluid_fraction, *operator_level0, nx, ny, nz, stream=queue)
-    for _ in range(num_vcycles):
-        multigrid.w_cycle(kernels, queue, 0, p_levels, b_levels, mask_levels, operator_levels, pressure, rhs,
-                          fluid_fraction, operator_level0, dx, multigrid_level_shapes, grid_shape,
-                          multigrid.PRE_SMOOTH, multigrid.POST_SMOOTH, multigrid.COARSE_SMOOTH_ITERATIONS)
-    boundary_conditions.neumann_domain_bc(kernels, queue, pressure, grid_shape)
+    """pressure_solve.py:10-85: right-hand side, finest operator, ``num_vcycles`` W-cycles on the
+    previous pressure and the Neumann ghost copy, by the product solver (the packed hierarchy, its
+    W-cycle bit for bit the reference's). ``rhs`` and ``operator_level0`` receive what the reference's
+    pressure_rhs and build_finest_operator write, ``operator_levels`` / ``mask_levels`` the coarse
+    operators; ``p_levels`` and ``b_levels`` are workspace and are not written."""
+    key = ("solver", tuple(int(s) for s in grid_shape), tuple(tuple(s) for s in multigrid_level_shapes),
+           float(FIELD_DTYPE(dx)))
+    cache = multigrid._stage_cache(kernels)
+    if key not in cache:
+        cache[key] = PressureSolver(kernels, grid_shape, float(dx),
+                                    min_size=multigrid.stage_min_size(grid_shape, multigrid_level_shapes))
+    ps = cache[key]
+    stream = queue if queue is not None else torch.cuda.current_stream(kernels.device)
+    with torch.cuda.stream(stream):
+        ps.solve(velocity, fluid_fraction, pressure, dt, rho, num_vcycles=int(num_vcycles), tol=None)
+        rhs.copy_(ps.rhs)
+        kernels.call("clb_mg_unpack_finest", ps.hierarchy.op0, *operator_level0, *grid_shape)
+        multigrid.write_coarse_operators(kernels, None, ps.hierarchy, mask_levels, operator_levels)
     return pressure
 
 

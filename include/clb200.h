@@ -173,33 +173,36 @@ int clb_pressure_correction_f64(float* u, float* v, float* w, const double* pres
                                 float inv_dx, int nx, int ny, int nz, void* stream);
 int clb_neumann_domain_bc_f64(double* pressure, int nx, int ny, int nz, void* stream);
 
-/* ---- multigrid, reference layout (float32 mask/diagonal/weight arrays per level) -------------- */
+/* ---- multigrid: the reference's level arrays through the product kernels -------------------- */
+/* The reference keeps five float32 arrays per level (mask, diagonal, weight_x, weight_y, weight_z;
+ * multigrid.py:18-50, built by multigrid.cl:63-88 build_finest_operator and :90-180
+ * restrict_residual). The stage functions that take those arrays (multigrid.py:53-249 w_cycle,
+ * smooth, coarse_smooth; pressure_solve.py:10-85) convert them with these calls and run the
+ * product kernels: the finest level as one byte per cell (see clb_mg_hierarchy), a coarse level as a
+ * float4 (diagonal, wx, wy, wz) per cell (op4, 16-byte aligned) and a mask byte. A cell is fluid
+ * where its mask is > 0, the reference's test. */
 
-/* multigrid.cl:63-88 build_finest_operator (pressure_solve.py:50-59). */
-int clb_build_finest_operator(const float* mask, float* diagonal, float* weight_x, float* weight_y, float* weight_z,
-                              int nx, int ny, int nz, void* stream);
-
-/* multigrid.cl:203-230 rbgs_step (one colour; multigrid.py:190-220 calls it twice per iteration). */
-int clb_rbgs_step(float* p, const float* b, const float* mask, const float* diagonal, const float* weight_x,
-                  const float* weight_y, const float* weight_z, float delta, int parity, int nx, int ny, int nz,
-                  void* stream);
-
-/* multigrid.cl:90-180 restrict_residual (multigrid.py:106-125). */
-int clb_restrict_residual(const float* fine_p, const float* fine_b, const float* fine_mask, const float* fine_diagonal,
-                          const float* fine_weight_x, const float* fine_weight_y, const float* fine_weight_z,
-                          float* coarse_p, float* coarse_b, float* coarse_mask, float* coarse_diagonal,
-                          float* coarse_weight_x, float* coarse_weight_y, float* coarse_weight_z, float delta,
-                          int fine_nx, int fine_ny, int fine_nz, int coarse_nx, int coarse_ny, int coarse_nz,
-                          void* stream);
-
-/* multigrid.cl:182-201 prolongate (multigrid.py:172-185). */
-int clb_prolongate(const float* coarse_error, float* fine_p, const float* fine_mask, int coarse_nx, int coarse_ny,
-                   int coarse_nz, int fine_nx, int fine_ny, int fine_nz, void* stream);
-
-/* multigrid.cl:232-264 coarse_smooth (multigrid.py:223-249): one block, all sweeps. */
-int clb_coarse_smooth(float* p, const float* b, const float* mask, const float* diagonal, const float* weight_x,
-                      const float* weight_y, const float* weight_z, float delta, int iterations, int nx, int ny,
-                      int nz, void* stream);
+/* Finest level -> packed bytes. Counts into *invalid (device int, zeroed by the caller) the cells
+ * whose diagonal is not an integer 0..7 or whose weights are not 0 or 1: such an operator is not a
+ * finest operator and has no byte form. */
+int clb_mg_pack_finest(const float* mask, const float* diagonal, const float* weight_x, const float* weight_y,
+                       const float* weight_z, uint8_t* op0, int32_t* invalid, int nx, int ny, int nz, void* stream);
+/* Packed bytes -> the finest operator arrays (what build_finest_operator writes). */
+int clb_mg_unpack_finest(const uint8_t* op0, float* diagonal, float* weight_x, float* weight_y, float* weight_z,
+                         int nx, int ny, int nz, void* stream);
+/* Coarse level arrays -> float4 operator + mask byte, and back (mask written as 1.0 / 0.0). */
+int clb_mg_pack_level(const float* mask, const float* diagonal, const float* weight_x, const float* weight_y,
+                      const float* weight_z, float* op4, uint8_t* mask_out, int nx, int ny, int nz, void* stream);
+int clb_mg_unpack_level(const float* op4, const uint8_t* mask_in, float* mask, float* diagonal, float* weight_x,
+                        float* weight_y, float* weight_z, int nx, int ny, int nz, void* stream);
+/* multigrid.py:190-220 smooth on a packed coarse-format level: `iterations` red-black iterations
+ * (multigrid.cl:203-230 per colour; cells whose mask is 0 are set to 0). */
+int clb_mg_smooth_level(float* p, const float* b, const float* op4, const uint8_t* mask, float delta, int iterations,
+                        int nx, int ny, int nz, void* stream);
+/* multigrid.py:223-249 coarse_smooth on a packed coarse-format level: `iterations` red-black
+ * iterations in one block (multigrid.cl:232-264). */
+int clb_mg_coarse_solve_level(float* p, const float* b, const float* op4, const uint8_t* mask, float delta,
+                              int iterations, int nx, int ny, int nz, void* stream);
 
 /* ---- multigrid, packed layout (product path) ------------------------------------------------ */
 

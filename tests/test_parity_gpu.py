@@ -250,37 +250,36 @@ def random_system(shape, seed):
     return ff, b, p0
 
 
-def test_reference_layout_kernels(backend, oracle, case):
+def test_reference_layout_stage_functions(backend, oracle, case):
+    """multigrid.smooth / coarse_smooth on the reference's level arrays (packed for the product kernels)
+    equal the oracle's rbgs_step and coarse_smooth; the finest operator survives the byte packing."""
     shape, dx, _, _ = case
     ff, b, p0 = random_system(shape, 12)
-    ops = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(4)]
-    backend.call("clb_build_finest_operator", dev(ff), *ops, *shape)
     oops = oracle.build_finest_operator(ff, shape)
-    for a, o in zip(ops, oops):
+    op0 = torch.zeros(shape, dtype=torch.uint8, device="cuda")
+    invalid = torch.zeros(1, dtype=torch.int32, device="cuda")
+    backend.call("clb_mg_pack_finest", dev(ff), *(dev(o) for o in oops), op0, invalid, *shape)
+    back = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(4)]
+    backend.call("clb_mg_unpack_finest", op0, *back, *shape)
+    assert int(invalid.item()) == 0
+    for a, o in zip(back, oops):
         assert np.array_equal(host(a), o)
+    ops = tuple(dev(o) for o in oops)
     P = dev(p0)
-    for parity in (0, 1, 0):
-        backend.call("clb_rbgs_step", P, dev(b), dev(ff), *ops, float(dx), parity, *shape)
+    multigrid.smooth(backend, None, P, dev(b), dev(ff), ops, float(dx), 2, shape)
     q = p0.copy()
-    for parity in (0, 1, 0):
+    for parity in (0, 1, 0, 1):
         oracle.lib().orc_rbgs_step_f32(q, b, ff, *oops, dx, parity, *shape)
     assert np.array_equal(host(P), q)
+    # a coarse level as the reference's restriction makes it, then its coarse smooth
     cshape = tuple(oracle.coarse_grid_size(s) for s in shape)
-    carr = [torch.zeros(cshape, dtype=torch.float32, device="cuda") for _ in range(7)]
-    backend.call("clb_restrict_residual", P, dev(b), dev(ff), *ops, *carr, float(dx), *shape, *cshape)
     oc = [np.zeros(cshape, F32) for _ in range(7)]
     oracle.lib().orc_restrict_residual_f32(q, b, ff, *oops, *oc, dx, *shape, *cshape)
-    for a, o in zip(carr, oc):
-        assert np.array_equal(host(a), o)
-    ce = np.random.default_rng(13).standard_normal(cshape).astype(F32)
-    backend.call("clb_prolongate", dev(ce), P, dev(ff), *cshape, *shape)
-    oracle.lib().orc_prolongate_f32(ce, q, ff, *cshape, *shape)
-    assert np.array_equal(host(P), q)
-    # coarse smooth on the coarse level produced by restriction
-    cp = carr[0]
-    backend.call("clb_coarse_smooth", cp, *carr[1:], float(dx), 66, *cshape)
-    ocp = oc[0].copy()
-    oracle.lib().orc_coarse_smooth_f32(ocp, *oc[1:], dx, 66, *cshape)
+    cp = dev(np.random.default_rng(13).standard_normal(cshape).astype(F32) * (oc[2] > 0))
+    ocp = host(cp).copy()
+    multigrid.coarse_smooth(backend, None, cp, dev(oc[1]), dev(oc[2]), tuple(dev(o) for o in oc[3:]), float(dx), 66,
+                            cshape)
+    oracle.lib().orc_coarse_smooth_f32(ocp, oc[1], oc[2], *oc[3:], dx, 66, *cshape)
     assert np.array_equal(host(cp), ocp)
 
 
@@ -288,11 +287,10 @@ def test_reference_layout_w_cycle(backend, oracle):
     shape, dx = (34, 34, 34), F32(1.0 / 34)
     ff, b, p0 = random_system(shape, 14)
     lv = multigrid.create_multigrid_levels(backend, shape)
-    ops = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(4)]
-    backend.call("clb_build_finest_operator", dev(ff), *ops, *shape)
+    ops = tuple(dev(o) for o in oracle.build_finest_operator(ff, shape))
     P = dev(p0)
     for _ in range(2):
-        multigrid.w_cycle(backend, None, 0, lv[0], lv[1], lv[2], lv[3], P, dev(b), dev(ff), tuple(ops), float(dx),
+        multigrid.w_cycle(backend, None, 0, lv[0], lv[1], lv[2], lv[3], P, dev(b), dev(ff), ops, float(dx),
                           lv[4], shape, 2, 4, 64)
     levels = oracle.Levels(shape)
     q = p0.copy()
@@ -300,6 +298,40 @@ def test_reference_layout_w_cycle(backend, oracle):
     for _ in range(2):
         levels.w_cycle(q, b, ff, oops, dx)
     assert np.array_equal(host(P), q)
+    # the coarse operators and masks, where the reference's restriction leaves them
+    for l in range(1, len(levels.shapes)):
+        assert np.array_equal(host(lv[2][l - 1]), levels.m[l]), f"mask {l}"
+        for a, o in zip(lv[3][l - 1], levels.ops[l]):
+            assert np.array_equal(host(a), o), f"operator {l}"
+    with pytest.raises(ValueError, match="level 0"):
+        multigrid.w_cycle(backend, None, 1, lv[0], lv[1], lv[2], lv[3], P, dev(b), dev(ff), ops, float(dx), lv[4],
+                          shape, 2, 4, 64)
+    bad = (dev(oops[0] * 0.5), *ops[1:])
+    with pytest.raises(ValueError, match="finest-level operator"):
+        multigrid.w_cycle(backend, None, 0, lv[0], lv[1], lv[2], lv[3], P, dev(b), dev(ff), bad, float(dx), lv[4],
+                          shape, 2, 4, 64)
+
+
+def test_reference_layout_pressure_solve(backend, oracle):
+    """pressure_solve.pressure_solve (the stage the add-on calls, on the reference's arrays) equals the
+    oracle's pressure_solve: pressure, right-hand side and finest operator."""
+    from continuum_liquid_b200 import pressure_solve as ps_mod
+
+    shape, dx, dt, rho = (34, 30, 38), 1.0 / 34, 1.0 / 240, 1000.0
+    rng = np.random.default_rng(21)
+    u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
+    ff, _, p0 = random_system(shape, 22)
+    lv = multigrid.create_multigrid_levels(backend, shape)
+    rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    op0 = tuple(torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(4))
+    P = dev(p0)
+    ps_mod.pressure_solve(backend, backend, backend, None, (dev(u), dev(v), dev(w)), dev(ff), P, rhs, lv[0], lv[1],
+                          lv[2], op0, lv[3], lv[4], dx, dt, rho, 2, shape)
+    p_ref, rhs_ref, op_ref = oracle.pressure_solve(u, v, w, ff, p0, dx, dt, rho, 2, shape)
+    assert np.array_equal(host(P), p_ref)
+    assert np.array_equal(host(rhs), rhs_ref)
+    for a, o in zip(op0, op_ref):
+        assert np.array_equal(host(a), o)
 
 
 @pytest.mark.parametrize("shape", [(34, 34, 34), (66, 66, 66), (48, 40, 56)])
@@ -493,8 +525,8 @@ def test_bad_arguments_raise(backend):
     t = torch.zeros(8, dtype=torch.float32, device="cuda")
     with pytest.raises(RuntimeError, match="grid"):
         backend.call("clb_grid_domain_bc", t, t, t, 2, 2, 2)
-    with pytest.raises(RuntimeError, match="parity"):
-        backend.call("clb_rbgs_step", t, t, t, t, t, t, t, 1.0, 3, 4, 4, 4)
+    with pytest.raises(RuntimeError, match="negative iterations"):
+        backend.call("clb_mg_smooth_level", t, t, t, t, 1.0, -1, 4, 4, 4)
 
 
 @pytest.mark.parametrize("cluster", [1, 0])
