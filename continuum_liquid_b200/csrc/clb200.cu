@@ -871,7 +871,7 @@ int coarse_solve(const LevelView& v, float delta, int iterations, cudaStream_t s
 extern "C++" {
 template <int NS, int KA, int KB, bool H>
 static int launch_cluster_visit(const clb_mg_hierarchy* h, int level, int csize, size_t bytes, int pre, int post,
-                                int coarse_iters, cudaStream_t s) {
+                                int coarse_iters, int visits, cudaStream_t s) {
     auto kernel = k_cluster_visit<NS, KA, KB, H>;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(csize);
@@ -910,15 +910,16 @@ static int launch_cluster_visit(const clb_mg_hierarchy* h, int level, int csize,
                              (const uint8_t*)h->mask[level], c[0], c[1], c[2], h->p[level + 1],
                              (const float4*)h->op[level + 1], (const uint8_t*)h->mask[level + 1], a[0], a[1], a[2],
                              (const float4*)h->op[level + 2], (const uint8_t*)h->mask[level + 2], b[0], b[1], b[2],
-                             h->delta, pre, post, coarse_iters, (const float*)h->fp16_scale);
+                             h->delta, pre, post, coarse_iters, (const float*)h->fp16_scale, visits);
     return check_launch("k_cluster_visit") ? -1 : 1;
 }
 }  // extern "C++"
 
-// One cluster launch for a whole visit of the third-coarsest level with its two bottom visits
-// (mg_cluster.cuh) when the three levels share their storage type and fit; returns 1 if it launched,
-// 0 if the caller must go on level by level, -1 on error.
-int cluster_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int coarse_iters, cudaStream_t s) {
+// One cluster launch for `visits` consecutive visits of the third-coarsest level, each with its two
+// bottom visits (mg_cluster.cuh), when the three levels share their storage type and fit; returns 1
+// if it launched, 0 if the caller must go on level by level, -1 on error.
+int cluster_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int coarse_iters, cudaStream_t s,
+                  int visits = 1) {
     if (!g_use_cluster || !g_use_bottom || level < 1 || level != h->levels - 3) return 0;
     const bool half = is_half(h, level);
     if (is_half(h, level + 1) != half || is_half(h, level + 2) != half) return 0;
@@ -937,7 +938,8 @@ int cluster_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int c
     if (bytes > kBottomSmemLimit) return 0;
     const long long slots = (long long)L.own_max * (c[1] - 2) * ((c[2] - 1) / 2);
     const int ns = (int)((slots + BOTTOM_THREADS - 1) / BOTTOM_THREADS);
-#define CLB_CLUSTER(NS, KA, H) launch_cluster_visit<NS, KA, 1, H>(h, level, cs + 1, bytes, pre, post, coarse_iters, s)
+#define CLB_CLUSTER(NS, KA, H) \
+    launch_cluster_visit<NS, KA, 1, H>(h, level, cs + 1, bytes, pre, post, coarse_iters, visits, s)
 #define CLB_CLUSTER_KINDS(H)                                  \
     if (ka <= 2 && ns <= 4) return CLB_CLUSTER(4, 2, H);      \
     if (ns <= 2) return CLB_CLUSTER(2, 4, H);                 \
@@ -1045,8 +1047,13 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
                                                const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
                                                c.nx, c.ny, c.nz);
     CLB_LAUNCH_CHECK("k_restrict");
-    if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
-    if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+    // the two visits of the level below: one cluster launch for both when it takes the cluster path
+    const int both = cluster_visit(h, level + 1, pre, post, coarse_iters, s, 2);
+    if (both < 0) return 1;
+    if (both == 0) {
+        if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+        if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+    }
     const i64 Cf = (i64)v.nx * v.ny * v.nz;
     const int fvec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
     if (!c.half && !v.half && v.tiles) {  // prolongation into the fine fluid tiles

@@ -1,5 +1,6 @@
 // One visit of the third-coarsest level C = L-3 together with both visits of the level below it
-// (its two bottom visits, mg_bottom.cuh), as one launch of a thread-block cluster.
+// (its two bottom visits, mg_bottom.cuh), as one launch of a thread-block cluster; or the two visits
+// of C that the level above makes back to back, in one launch (`visits` = 2).
 //
 // A W-cycle visits C 2^(L-3) times, and each visit (multigrid.py:53-187) is pre-smoothing of C,
 // restriction to A = C+1, two visits of A (each: smoothing, restriction to B, two coarse solves,
@@ -92,7 +93,7 @@ template <int NS, bool H>
 __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, float* __restrict__ pc_out,
                                   const float* __restrict__ bc, const void* __restrict__ opc_,
                                   const uint8_t* __restrict__ mc, int nx, int ny, int nz, int anx, int any, int anz,
-                                  float d2, float inv_delta2, int pre, int post) {
+                                  float d2, float inv_delta2, int pre, int post, int visits) {
     namespace cgx = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem[];
     using OpT = typename std::conditional<H, uint2, float4>::type;
@@ -190,6 +191,10 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
         push();
     };
 
+    // consecutive visits of C (the two a W-cycle makes from the level above) keep C's planes, lists and
+    // operands in shared memory: a visit starts from the p the previous one left, exactly as a
+    // separate launch that staged it again would
+    for (int visit = 0; visit < visits; ++visit) {
     cluster_barrier();  // every CTA staged (the first CTA zeroed A's p and b)
     for (int it = 0; it < pre; ++it) {
         phase(0);
@@ -249,6 +254,7 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
         phase(0);
         phase(1);
     }
+    }  // visits
 
     // the owned planes back to C's p
     for (int q = threadIdx.x; q < own * PL; q += BOTTOM_THREADS) {
@@ -262,17 +268,19 @@ template <int KA, int KB, bool H>
 __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __restrict__ opa,
                                     const uint8_t* __restrict__ ma, int anx, int any, int anz,
                                     const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny,
-                                    int bnz, float d2, float inv_delta2, int pre, int post, int coarse_iters) {
+                                    int bnz, float d2, float inv_delta2, int pre, int post, int coarse_iters,
+                                    int visits) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     const BottomSmem S = bottom_smem(smem, CA, CB);
     bottom_stage<H>(S, nullptr, nullptr, opa, ma, CA, opb, mb, CB);
     bottom_lists(S, anx, any, anz, bnx, bny, bnz);
+    for (int visit_c = 0; visit_c < visits; ++visit_c) {
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
         S.spa[c] = 0.0f;  // restriction zeroes the coarse pressure (multigrid.cl:114)
         S.sba[c] = 0.0f;  // cells the restriction does not write (non-interior) hold 0
     }
-    cluster_barrier();  // staged
+    cluster_barrier();  // staged (for a later visit of C: the slabs finished reading A's p)
     for (int it = 0; it < 2 * pre; ++it) cluster_barrier();  // the C-level pre-smoothing phases
     cluster_barrier();  // A's right-hand side is complete
     for (int visit = 0; visit < 2; ++visit) {
@@ -285,6 +293,7 @@ __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __rest
     cluster_barrier();  // both visits done; the slabs read A's p next
     cluster_barrier();  // prolongation done
     for (int it = 0; it < 2 * post; ++it) cluster_barrier();  // the C-level post-smoothing phases
+    }  // visits of C
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
         if (H) reinterpret_cast<__half*>(pa)[c] = __float2half_rn(S.spa[c]);
         else pa[c] = S.spa[c];
@@ -298,7 +307,8 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
                     const uint8_t* __restrict__ mc, int nx, int ny, int nz, float* __restrict__ pa,
                     const float4* __restrict__ opa, const uint8_t* __restrict__ ma, int anx, int any, int anz,
                     const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
-                    float delta, int pre, int post, int coarse_iters, const float* __restrict__ scale) {
+                    float delta, int pre, int post, int coarse_iters, const float* __restrict__ scale,
+                    int visits) {
     pdl_begin();
     const float d2 = H ? scale[2] : delta * delta;
     const float inv_delta2 = H ? scale[3] : 1.0f / (delta * delta);
@@ -306,10 +316,10 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
     const int cs = (int)cooperative_groups::this_cluster().num_blocks() - 1;
     if (rank == 0)
         cluster_bottom_path<KA, KB, H>(pa, opa, ma, anx, any, anz, opb, mb, bnx, bny, bnz, d2, inv_delta2, pre, post,
-                                       coarse_iters);
+                                       coarse_iters, visits);
     else
         cluster_slab_path<NS, H>((int)rank - 1, cs, pc, pc, bc, opc, mc, nx, ny, nz, anx, any, anz, d2, inv_delta2,
-                                 pre, post);
+                                 pre, post, visits);
 }
 
 }  // namespace clb

@@ -17,7 +17,7 @@
 // along k, one warp per row, one lane per bin. Rows run in 9 phases by (row i mod 3, row j mod 3):
 // rows of one phase are at least 3 apart in i or j, so their candidate cells are disjoint and no two
 // warps add to the same cell at the same time. Inside a row the lanes add one candidate offset at a
-// time (distinct cells per step, __syncwarp between steps). Every cell therefore receives its terms
+// time (distinct cells of each array per step, __syncwarp between steps). Every cell therefore receives its terms
 // in a fixed order: no floating-point atomics (the counts use integer shared-memory atomics, which
 // commute), and the same result on every run.
 #pragma once
@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(P2GT_THREADS, 2)
                     begin = __ldg(offsets + bin);
                     end = begin + __ldg(counts + bin);
                 }
+                if (!__any_sync(0xffffffffu, end > begin)) continue;  // a row without particles adds nothing
                 float vu[12], wu[12], vv[12], wv[12], vw[12], ww[12];
 #pragma unroll
                 for (int a = 0; a < 12; ++a) vu[a] = wu[a] = vv[a] = wv[a] = vw[a] = ww[a] = 0.0f;
@@ -123,7 +124,9 @@ __global__ void __launch_bounds__(P2GT_THREADS, 2)
                         atomicAdd(s_cnt + (ci * P2GT_TJ + cj) * P2GT_TK + ck, 1);
                 }
                 __syncwarp();
-                // add the bin's sums to the tile's cells, one candidate offset at a time
+                // add the bin's sums to the tile's cells, one candidate offset at a time: within a step the
+                // lanes write distinct cells of each array (u, v and w sums are separate arrays), and a
+                // __syncwarp orders the steps, which can reach the same cell from neighbouring lanes
                 auto add = [&](float* sv, float* sw, int di, int dj, int dk, float val, float wgt) {
                     const int ci = li + di, cj = lj + dj, ck = lk + dk;
                     if (bin_ok && ci >= 0 && ci < P2GT_TI && cj >= 0 && cj < P2GT_TJ && ck >= 0 && ck < P2GT_TK) {
@@ -131,7 +134,6 @@ __global__ void __launch_bounds__(P2GT_THREADS, 2)
                         sv[c] += val;
                         sw[c] += wgt;
                     }
-                    __syncwarp();
                 };
 #pragma unroll
                 for (int a = 0; a < 3; ++a)
@@ -143,6 +145,7 @@ __global__ void __launch_bounds__(P2GT_THREADS, 2)
                             add(s_vel, s_wgt, a - 1, b, c, vu[t], wu[t]);
                             add(s_vel + P2GT_CELLS, s_wgt + P2GT_CELLS, b, a - 1, c, vv[t], wv[t]);
                             add(s_vel + 2 * P2GT_CELLS, s_wgt + 2 * P2GT_CELLS, b, c, a - 1, vw[t], ww[t]);
+                            __syncwarp();
                         }
             }
             __syncthreads();
