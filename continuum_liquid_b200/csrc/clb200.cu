@@ -362,7 +362,7 @@ int clb_particle_obstacle_bc(float* particles, const float* previous, float* vel
     CLB_REQUIRE(n >= 0, "particle_obstacle_bc: negative n");
     if (n == 0) return 0;
     CLB_REQUIRE(particles && previous && velocity && obstacle, "particle_obstacle_bc: null pointer");
-    k_particle_obstacle_bc<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, previous, velocity, obstacle, n,
+    k_particle_obstacle_bc<false><<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(particles, previous, velocity, obstacle, n,
                                                                               inv_dx, nx, ny, nz);
     CLB_LAUNCH_CHECK("k_particle_obstacle_bc");
     return 0;
@@ -376,10 +376,61 @@ int clb_particle_update(float* particles, float* velocity, float* previous_out, 
     CLB_REQUIRE(n >= 0, "particle_update: negative n");
     if (n == 0) return 0;
     CLB_REQUIRE(particles && velocity && u && v && w && u_old && v_old && w_old, "particle_update: null pointer");
-    k_particle_update<<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(
+    k_particle_update<false><<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(
         particles, velocity, previous_out, u, v, w, u_old, v_old, w_old, obstacle, n, inv_dx, nx, ny, nz, flip_ratio,
         dt, lower, upper_x, upper_y, upper_z);
     CLB_LAUNCH_CHECK("k_particle_update");
+    return 0;
+}
+
+// ---- moving colliders (no counterpart in the reference) ------------------------------------------
+
+static RigidMotion motion_of(const float* m) {
+    return RigidMotion{m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8]};
+}
+
+int clb_particle_obstacle_bc_moving(float* particles, const float* previous, float* velocity,
+                                    const uint8_t* obstacle, int64_t n, float inv_dx, int nx, int ny, int nz,
+                                    const float* motion, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0, "particle_obstacle_bc_moving: negative n");
+    CLB_REQUIRE(motion != nullptr, "particle_obstacle_bc_moving: null motion");
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && previous && velocity && obstacle, "particle_obstacle_bc_moving: null pointer");
+    k_particle_obstacle_bc<true><<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(
+        particles, previous, velocity, obstacle, n, inv_dx, nx, ny, nz, motion_of(motion));
+    CLB_LAUNCH_CHECK("k_particle_obstacle_bc");
+    return 0;
+}
+
+int clb_particle_update_moving(float* particles, float* velocity, float* previous_out, const float* u, const float* v,
+                               const float* w, const float* u_old, const float* v_old, const float* w_old,
+                               const uint8_t* obstacle, int64_t n, float inv_dx, int nx, int ny, int nz,
+                               float flip_ratio, float dt, float lower, float upper_x, float upper_y, float upper_z,
+                               const float* motion, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0, "particle_update_moving: negative n");
+    CLB_REQUIRE(motion != nullptr && obstacle != nullptr, "particle_update_moving: null motion or obstacle");
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && velocity && u && v && w && u_old && v_old && w_old, "particle_update_moving: null pointer");
+    k_particle_update<true><<<blocks_for(n, PT), PT, 0, CLB_STREAM(stream)>>>(
+        particles, velocity, previous_out, u, v, w, u_old, v_old, w_old, obstacle, n, inv_dx, nx, ny, nz, flip_ratio,
+        dt, lower, upper_x, upper_y, upper_z, motion_of(motion));
+    CLB_LAUNCH_CHECK("k_particle_update");
+    return 0;
+}
+
+int clb_grid_obstacle_bc_moving(float* u, float* v, float* w, float* fluid_fraction, const uint8_t* obstacle, int nx,
+                                int ny, int nz, const float* motion, float dx, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(u && v && w && fluid_fraction && obstacle && motion, "grid_obstacle_bc_moving: null pointer");
+    const i64 C = (i64)nx * ny * nz;
+    cudaStream_t s = CLB_STREAM(stream);
+    const RigidMotion m = motion_of(motion);
+    k_grid_obstacle_bc_moving<<<blocks_for(C, 256), 256, 0, s>>>(u, v, w, fluid_fraction, obstacle, nx, ny, nz, m, dx);
+    CLB_LAUNCH_CHECK("k_grid_obstacle_bc_moving");
+    k_extrapolate_obstacle_velocity_moving<<<blocks_for(C, 256), 256, 0, s>>>(u, v, w, obstacle, nx, ny, nz, m, dx);
+    CLB_LAUNCH_CHECK("k_extrapolate_obstacle_velocity_moving");
     return 0;
 }
 

@@ -2,6 +2,7 @@
 // (Solver/Kernel/OpenCL/particles.cl:229-276, boundary_conditions.cl:69-97 and 175-264).
 #pragma once
 #include "binning.cuh"
+#include "moving.cuh"
 
 namespace clb {
 
@@ -69,10 +70,12 @@ __device__ __forceinline__ void domain_bc_axis(float& x, float& vel, float lower
 
 __device__ __forceinline__ int cell_of(float x, float inv_dx, int n) { return clampi((int)(x * inv_dx), 0, n - 1); }
 
-// boundary_conditions.cl:175-264 particle_obstacle_bc.
+// boundary_conditions.cl:175-264 particle_obstacle_bc. MOVING (no counterpart in the reference): the
+// collider moves with `motion`, and only the velocity relative to it loses its inward component.
+template <bool MOVING = false>
 __device__ __forceinline__ void obstacle_bc(float& p0, float& p1, float& p2, float q0, float q1, float q2, float& v0,
                                             float& v1, float& v2, const uint8_t* __restrict__ obs, float inv_dx,
-                                            int nx, int ny, int nz) {
+                                            int nx, int ny, int nz, RigidMotion motion = RigidMotion{}) {
     const int c0 = cell_of(p0, inv_dx, nx), c1 = cell_of(p1, inv_dx, ny), c2 = cell_of(p2, inv_dx, nz);
     if (!__ldg(obs + gidx(c0, c1, c2, ny, nz))) return;
     const int r0 = cell_of(q0, inv_dx, nx), r1 = cell_of(q1, inv_dx, ny), r2 = cell_of(q2, inv_dx, nz);
@@ -107,7 +110,15 @@ __device__ __forceinline__ void obstacle_bc(float& p0, float& p1, float& p2, flo
             n2 = 1.0f;
         }
     }
-    const float vn = v0 * n0 + v1 * n1 + v2 * n2;
+    float vn;
+    if constexpr (MOVING) {
+        float s0, s1, s2;
+        rigid_velocity(motion, p0, p1, p2, s0, s1, s2);
+        const float r0 = v0 - s0, r1 = v1 - s1, r2 = v2 - s2;
+        vn = r0 * n0 + r1 * n1 + r2 * n2;
+    } else {
+        vn = v0 * n0 + v1 * n1 + v2 * n2;
+    }
     if (vn < 0.0f) {
         v0 = v0 - vn * n0;
         v1 = v1 - vn * n1;
@@ -161,14 +172,17 @@ __global__ void __launch_bounds__(PT) k_particle_domain_bc(float* __restrict__ p
     domain_bc_axis(pos[3 * p + 2], vel[3 * p + 2], lower, uz);
 }
 
+template <bool MOVING = false>
 __global__ void __launch_bounds__(PT) k_particle_obstacle_bc(float* __restrict__ pos, const float* __restrict__ prev,
                                                               float* __restrict__ vel, const uint8_t* __restrict__ obs,
-                                                              i64 n, float inv_dx, int nx, int ny, int nz) {
+                                                              i64 n, float inv_dx, int nx, int ny, int nz,
+                                                              RigidMotion motion = RigidMotion{}) {
     const i64 p = (i64)blockIdx.x * PT + threadIdx.x;
     if (p >= n) return;
     float p0 = pos[3 * p], p1 = pos[3 * p + 1], p2 = pos[3 * p + 2];
     float v0 = vel[3 * p], v1 = vel[3 * p + 1], v2 = vel[3 * p + 2];
-    obstacle_bc(p0, p1, p2, prev[3 * p], prev[3 * p + 1], prev[3 * p + 2], v0, v1, v2, obs, inv_dx, nx, ny, nz);
+    obstacle_bc<MOVING>(p0, p1, p2, prev[3 * p], prev[3 * p + 1], prev[3 * p + 2], v0, v1, v2, obs, inv_dx, nx, ny, nz,
+                        motion);
     pos[3 * p] = p0;
     pos[3 * p + 1] = p1;
     pos[3 * p + 2] = p2;
@@ -184,12 +198,13 @@ __global__ void __launch_bounds__(PT) k_particle_obstacle_bc(float* __restrict__
 // lives in registers; it is written out only when the caller asks for it.
 // The per-particle part of k_particle_update on registers (prev, when non-null, is this particle's
 // previous-position record).
+template <bool MOVING = false>
 __device__ __forceinline__ void particle_update_one(float& p0, float& p1, float& p2, float& v0, float& v1, float& v2,
                                                     float* __restrict__ prev, const float* u, const float* v,
                                                     const float* w, const float* ou, const float* ov, const float* ow,
                                                     const uint8_t* __restrict__ obs, float inv_dx, int nx, int ny,
                                                     int nz, float flip_ratio, float dt, float lower, float ux,
-                                                    float uy, float uz) {
+                                                    float uy, float uz, RigidMotion motion = RigidMotion{}) {
     g2p_velocity(v0, v1, v2, p0, p1, p2, u, v, w, ou, ov, ow, inv_dx, nx, ny, nz, flip_ratio);
     const float q0 = p0, q1 = p1, q2 = p2;
     if (prev) {
@@ -203,15 +218,17 @@ __device__ __forceinline__ void particle_update_one(float& p0, float& p1, float&
     domain_bc_axis(p0, v0, lower, ux);
     domain_bc_axis(p1, v1, lower, uy);
     domain_bc_axis(p2, v2, lower, uz);
-    if (obs) obstacle_bc(p0, p1, p2, q0, q1, q2, v0, v1, v2, obs, inv_dx, nx, ny, nz);
+    if (obs) obstacle_bc<MOVING>(p0, p1, p2, q0, q1, q2, v0, v1, v2, obs, inv_dx, nx, ny, nz, motion);
 }
 
+template <bool MOVING = false>
 __global__ void __launch_bounds__(PT) k_particle_update(float* __restrict__ pos, float* __restrict__ vel,
                                                          float* __restrict__ prev_out, const float* u, const float* v,
                                                          const float* w, const float* ou, const float* ov,
                                                          const float* ow, const uint8_t* __restrict__ obs, i64 n,
                                                          float inv_dx, int nx, int ny, int nz, float flip_ratio,
-                                                         float dt, float lower, float ux, float uy, float uz) {
+                                                         float dt, float lower, float ux, float uy, float uz,
+                                                         RigidMotion motion = RigidMotion{}) {
     __shared__ __align__(16) float sp[3 * PT];
     __shared__ __align__(16) float sv[3 * PT];
     const i64 first = (i64)blockIdx.x * PT;
@@ -223,8 +240,8 @@ __global__ void __launch_bounds__(PT) k_particle_update(float* __restrict__ pos,
         const int t = 3 * threadIdx.x;
         float p0 = sp[t], p1 = sp[t + 1], p2 = sp[t + 2];
         float v0 = sv[t], v1 = sv[t + 1], v2 = sv[t + 2];
-        particle_update_one(p0, p1, p2, v0, v1, v2, prev_out ? prev_out + 3 * p : nullptr, u, v, w, ou, ov, ow, obs,
-                            inv_dx, nx, ny, nz, flip_ratio, dt, lower, ux, uy, uz);
+        particle_update_one<MOVING>(p0, p1, p2, v0, v1, v2, prev_out ? prev_out + 3 * p : nullptr, u, v, w, ou, ov,
+                                    ow, obs, inv_dx, nx, ny, nz, flip_ratio, dt, lower, ux, uy, uz, motion);
         sp[t] = p0;
         sp[t + 1] = p1;
         sp[t + 2] = p2;

@@ -13,6 +13,7 @@ import numpy as np
 import torch
 
 from .backend import Backend
+from .colliders import motion_arg
 
 FIELD_DTYPE = np.float32
 
@@ -178,17 +179,20 @@ def advect_particles(kernels: Backend, queue, particles, particle_velocity, part
 
 
 def particle_update(kernels: Backend, queue, particles, particle_velocity, velocity, old_velocity, obstacle,
-                    particle_count_total, grid_shape, dx, dt, flip_ratio: float = 1.0, previous_particles=None):
+                    particle_count_total, grid_shape, dx, dt, flip_ratio: float = 1.0, previous_particles=None,
+                    motion=None):
     """solver.py:453-510 fused: G2P, previous-position copy, advection, domain and obstacle BCs.
 
     ``obstacle`` may be None when the scene has no collider (the obstacle BC is then a no-op in the
     reference as well). ``previous_particles`` receives the pre-advection positions when given.
+    ``motion`` (with an obstacle): the collider moves rigidly (``colliders.RigidMotion.parameters``).
     """
     nx, ny, nz = grid_shape
     u, v, w = velocity
     ou, ov, ow = old_velocity
+    extra = () if motion is None else (motion_arg(motion),)
     kernels.call(
-        "clb_particle_update",
+        "clb_particle_update" if motion is None else "clb_particle_update_moving",
         particles,
         particle_velocity,
         previous_particles,
@@ -210,6 +214,7 @@ def particle_update(kernels: Backend, queue, particles, particle_velocity, veloc
         float(FIELD_DTYPE((grid_shape[0] - 1.001) * float(dx))),
         float(FIELD_DTYPE((grid_shape[1] - 1.001) * float(dx))),
         float(FIELD_DTYPE((grid_shape[2] - 1.001) * float(dx))),
+        *extra,
         stream=queue,
     )
     return particles, particle_velocity

@@ -77,7 +77,8 @@ class FlipSolver:
 
     def __init__(self, kernels: Backend, grid_shape, dx: float, positions, velocities, obstacle=None,
                  dt: float = 1.0 / 240.0, options: StepOptions | None = None, particles_per_cell: int = 8,
-                 min_size: int = 8, capacity: int | None = None, colliders=None, origin=(0.0, 0.0, 0.0)):
+                 min_size: int = 8, capacity: int | None = None, colliders=None, origin=(0.0, 0.0, 0.0),
+                 collider_motion=None):
         self.kernels = kernels
         self.device = kernels.device
         self.grid_shape = tuple(int(s) for s in grid_shape)
@@ -110,6 +111,13 @@ class FlipSolver:
         # collider meshes (world-space float32 triangles) for per-step voxelisation
         self.colliders = [torch.as_tensor(np.ascontiguousarray(t, dtype=np.float32)).to(dev) for t in (colliders or [])]
         self.origin = tuple(float(o) for o in origin)
+        # a rigid motion of the colliders (colliders.RigidMotion; no counterpart in the reference): every
+        # step voxelises them at their pose and uses the solid's velocity in the obstacle conditions
+        self.collider_motion = collider_motion
+        self._collider_rest = [np.ascontiguousarray(t, dtype=np.float32) for t in (colliders or [])]
+        self._motion = None  # this step's motion parameters (grid-local), set by pre_solve
+        if collider_motion is not None and not self.colliders:
+            raise ValueError("collider_motion needs the collider meshes (colliders=...)")
         if self.colliders and self.obstacle is None:
             self.obstacle = torch.zeros(self.grid_shape, dtype=torch.uint8, device=dev)
         self.pressure_solver = PressureSolver(kernels, self.grid_shape, self.dx, min_size=min_size,
@@ -146,7 +154,16 @@ class FlipSolver:
     def pre_solve(self, queue=None) -> None:
         """Stages 1-4: P2G, grid BCs, forces, BCs (everything before the pressure solve)."""
         k, o, gs = self.kernels, self.options, self.grid_shape
-        if o.revoxelise and self.colliders:
+        self._motion = None
+        if self.collider_motion is not None:
+            # the pose at the step's start time; the rest triangles moved on the host (float64, rounded
+            # once), voxelised on the device
+            t = self.steps_done * self.dt
+            for dev_tris, rest in zip(self.colliders, self._collider_rest):
+                dev_tris.copy_(torch.from_numpy(self.collider_motion.transform(rest, t)))
+            self.voxelise_colliders(queue)
+            self._motion = self.collider_motion.parameters(t, self.origin)
+        elif o.revoxelise and self.colliders:
             self.voxelise_colliders(queue)
         (self.particles, self.particle_velocity, self.particle_work, self.particle_velocity_work,
          _, self.fluid_fraction) = particle_methods.particle_to_grid(
@@ -155,7 +172,8 @@ class FlipSolver:
             gs, self.dx, self.particles_per_cell, tiled=o.tiled_p2g())
         vel = (self.u, self.v, self.w)
         if self.obstacle is not None:
-            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)
+            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs,
+                                                 self._motion, self.dx)
         boundary_conditions.grid_domain_bc(k, queue, vel, gs)
         velocity_update.update_velocity(k, queue, vel, (self.u_work, self.v_work, self.w_work), self.fluid_fraction,
                                         o.gravity, *o.force, o.rho, o.nu, self.dx, self.dt, gs)
@@ -165,7 +183,8 @@ class FlipSolver:
         vel = (self.u, self.v, self.w)
         boundary_conditions.grid_domain_bc(k, queue, vel, gs)
         if self.obstacle is not None:
-            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)
+            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs,
+                                                 self._motion, self.dx)
 
     def solve(self, tol: float | None = None, num_vcycles: int | None = None) -> SolveStats:
         """Stage 5: the pressure solve, warm-started from the previous step's pressure."""
@@ -192,18 +211,19 @@ class FlipSolver:
             pressure_correction(k, queue, vel, self.pressure, self.dx, self.dt, o.rho, gs)
         boundary_conditions.grid_domain_bc(k, queue, vel, gs)
         if self.obstacle is not None:
-            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs)
+            boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs,
+                                                 self._motion, self.dx)
         if piece_bounds is None:
             particle_methods.particle_update(k, queue, self.particles, self.particle_velocity, vel,
                                              (self.u_work, self.v_work, self.w_work), self.obstacle, self.n, gs,
-                                             self.dx, self.dt, o.flip_ratio)
+                                             self.dx, self.dt, o.flip_ratio, motion=self._motion)
             return
         for c in range(len(piece_bounds) - 1):
             a, b = piece_bounds[c], piece_bounds[c + 1]
             if b > a:
                 particle_methods.particle_update(k, queue, self.particles[a:b], self.particle_velocity[a:b], vel,
                                                  (self.u_work, self.v_work, self.w_work), self.obstacle, b - a, gs,
-                                                 self.dx, self.dt, o.flip_ratio)
+                                                 self.dx, self.dt, o.flip_ratio, motion=self._motion)
             piece_done(c)
 
     def step(self) -> SolveStats:
@@ -310,6 +330,23 @@ def scene_solver(kernels: Backend, scene, options: StepOptions | None = None) ->
                       colliders=scene.obstacles, origin=scene.origin)
 
 
+def moving_colliders(simulation: dict):
+    """The obstacles' world triangles and their rigid motion when the config gives one (an obstacle's
+    "motion": {"velocity", "angular_velocity", "pivot"}; no counterpart in the reference). All
+    obstacles of a scene then move together: one motion, given on every obstacle."""
+    from .colliders import RigidMotion
+
+    obstacles = simulation.get("obstacles") or ()
+    motions = [RigidMotion.from_config(o.get("motion")) for o in obstacles]
+    if all(m is None for m in motions):
+        return [], None
+    if any(m != motions[0] for m in motions):
+        raise ValueError("moving obstacles: every obstacle of a scene must give the same motion (one rigid body)")
+    bake_path = simulation.get("output_path", ".")
+    tris = [voxelise_mesh._entry_triangles(entry, bake_path) for o in obstacles for entry in o.get("geometry_inputs") or ()]
+    return [t for t in tris if t.size], motions[0]
+
+
 # ------------------------------------------------------------------------------------------------
 # solver(config): the reference's entry point (solver.py:22-531)
 # ------------------------------------------------------------------------------------------------
@@ -355,8 +392,12 @@ def solver(config: dict, timings=None) -> None:
     # draw the same stream, so the particles equal the reference's without leaving the GPU
     rng = np.random.default_rng(0)
     empty = np.empty((0, 3), dtype=FIELD_DTYPE)
+    colliders, motion = moving_colliders(simulation)
+    size = domain_size
+    origin = (-0.5 * float(size["x"]), -0.5 * float(size["y"]), 0.0)
     sim = FlipSolver(kernels, grid_shape, delta, empty, empty, obstacle=obstacle_mask, dt=dt, options=options,
-                     particles_per_cell=8)
+                     particles_per_cell=8, colliders=colliders if motion is not None else None, origin=origin,
+                     collider_motion=motion)
     source_particles.DeviceSources(kernels, sources_dev, obstacle_mask, grid_shape, delta, rng,
                                    initial=True).apply(sim)
     device_sources = source_particles.DeviceSources(kernels, sources_dev, obstacle_mask, grid_shape, delta, rng)

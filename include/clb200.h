@@ -173,6 +173,32 @@ int clb_pressure_correction_f64(float* u, float* v, float* w, const double* pres
                                 float inv_dx, int nx, int ny, int nz, void* stream);
 int clb_neumann_domain_bc_f64(double* pressure, int nx, int ny, int nz, void* stream);
 
+/* ---- moving colliders ------------------------------------------------------------------------- */
+/* No counterpart in the reference: its colliders are voxelised once and stay at rest
+ * (solver.py:132-139), so its obstacle conditions set solid faces and solid velocities to 0
+ * (boundary_conditions.cl:99-264). Here a collider may move as a rigid body. `motion` points to 9
+ * host floats (vx, vy, vz, wx, wy, wz, cx, cy, cz): velocity, angular velocity (rad/s) and the pivot
+ * at the step's time in grid-local coordinates; the solid's velocity at x is V + W x (x - C). The
+ * obstacle mask is the collider voxelised at its pose (clb_voxelise_mesh). With V = W = 0 each call
+ * gives exactly what its static counterpart gives. */
+
+/* clb_grid_obstacle_bc with solid faces set to the solid's velocity component at the face centre
+ * (the u face of cell (i, j, k) at ((i+1) dx, (j+0.5) dx, (k+0.5) dx)), and solid cells next to
+ * fluid given the solid's normal component (the fluid's averaged tangential velocity as before). */
+int clb_grid_obstacle_bc_moving(float* u, float* v, float* w, float* fluid_fraction, const uint8_t* obstacle, int nx,
+                                int ny, int nz, const float* motion, float dx, void* stream);
+/* clb_particle_obstacle_bc where only the velocity relative to the solid (at the particle's
+ * position) loses its inward normal component. */
+int clb_particle_obstacle_bc_moving(float* particles, const float* previous, float* velocity,
+                                    const uint8_t* obstacle, int64_t n, float inv_dx, int nx, int ny, int nz,
+                                    const float* motion, void* stream);
+/* clb_particle_update with the moving obstacle condition above (obstacle must not be null). */
+int clb_particle_update_moving(float* particles, float* velocity, float* previous_out, const float* u, const float* v,
+                               const float* w, const float* u_old, const float* v_old, const float* w_old,
+                               const uint8_t* obstacle, int64_t n, float inv_dx, int nx, int ny, int nz,
+                               float flip_ratio, float dt, float lower, float upper_x, float upper_y, float upper_z,
+                               const float* motion, void* stream);
+
 /* ---- multigrid: the reference's level arrays through the product kernels -------------------- */
 /* The reference keeps five float32 arrays per level (mask, diagonal, weight_x, weight_y, weight_z;
  * multigrid.py:18-50, built by multigrid.cl:63-88 build_finest_operator and :90-180

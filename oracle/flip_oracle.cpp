@@ -573,6 +573,170 @@ void orc_particle_obstacle_bc(float* pos, const float* prev, float* vel, const u
     }
 }
 
+// ---- moving colliders (no counterpart in the reference, whose colliders are static) ------------
+// A rigid motion m[9] = (V, W, C) in grid-local coordinates: velocity, angular velocity (rad/s) and
+// pivot. The solid's velocity at x is V + W x (x - C), evaluated in this order (separately rounded).
+static inline void rigid_velocity(const float* m, float x, float y, float z, float out[3]) {
+    const float rx = x - m[6], ry = y - m[7], rz = z - m[8];
+    out[0] = m[0] + (m[4] * rz - m[5] * ry);
+    out[1] = m[1] + (m[5] * rx - m[3] * rz);
+    out[2] = m[2] + (m[3] * ry - m[4] * rx);
+}
+
+// grid_obstacle_bc with a moving solid: a solid face takes the solid's velocity component at the face
+// centre (u face of cell (i, j, k) at ((i+1) dx, (j+0.5) dx, (k+0.5) dx), v and w likewise) instead of 0.
+void orc_grid_obstacle_bc_moving(float* u, float* v, float* w, float* ff, const uint8_t* obs, int nx, int ny, int nz,
+                                 const float* m, float dx) {
+    const i64 C = (i64)nx * ny * nz;
+#pragma omp parallel for schedule(static)
+    for (i64 index = 0; index < C; ++index) {
+        int i, j, k;
+        gcoord(index, ny, nz, i, j, k);
+        if (obs[index]) ff[index] = 0.0f;
+        const bool xs = obs[index] || (i + 1 < nx && obs[gidx(i + 1, j, k, ny, nz)]);
+        const bool ys = obs[index] || (j + 1 < ny && obs[gidx(i, j + 1, k, ny, nz)]);
+        const bool zs = obs[index] || (k + 1 < nz && obs[gidx(i, j, k + 1, ny, nz)]);
+        const float fi = (float)i, fj = (float)j, fk = (float)k;
+        float sv[3];
+        if (xs) {
+            rigid_velocity(m, (fi + 1.0f) * dx, (fj + 0.5f) * dx, (fk + 0.5f) * dx, sv);
+            u[index] = sv[0];
+        }
+        if (ys) {
+            rigid_velocity(m, (fi + 0.5f) * dx, (fj + 1.0f) * dx, (fk + 0.5f) * dx, sv);
+            v[index] = sv[1];
+        }
+        if (zs) {
+            rigid_velocity(m, (fi + 0.5f) * dx, (fj + 0.5f) * dx, (fk + 1.0f) * dx, sv);
+            w[index] = sv[2];
+        }
+    }
+}
+
+// extrapolate_obstacle_velocity with a moving solid: a solid cell next to fluid keeps the fluid's
+// averaged tangential velocity and takes the solid's normal component at its face centre.
+void orc_extrapolate_obstacle_velocity_moving(float* u, float* v, float* w, const uint8_t* obs, int nx, int ny,
+                                              int nz, const float* m, float dx) {
+    const i64 C = (i64)nx * ny * nz;
+#pragma omp parallel for schedule(static)
+    for (i64 index = 0; index < C; ++index) {
+        if (!obs[index]) continue;
+        int i, j, k;
+        gcoord(index, ny, nz, i, j, k);
+        float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
+        int n = 0;
+        int ax = 0, ay = 0, az = 0;
+        auto acc = [&](int a, int b, int c, int& axis) {
+            const i64 q = gidx(a, b, c, ny, nz);
+            if (!obs[q]) {
+                t0 += u[q];
+                t1 += v[q];
+                t2 += w[q];
+                n += 1;
+                axis = 1;
+            }
+        };
+        if (i > 0) acc(i - 1, j, k, ax);
+        if (i + 1 < nx) acc(i + 1, j, k, ax);
+        if (j > 0) acc(i, j - 1, k, ay);
+        if (j + 1 < ny) acc(i, j + 1, k, ay);
+        if (k > 0) acc(i, j, k - 1, az);
+        if (k + 1 < nz) acc(i, j, k + 1, az);
+        if (n == 0) continue;
+        const float fn = (float)n;
+        t0 /= fn;
+        t1 /= fn;
+        t2 /= fn;
+        const float fi = (float)i, fj = (float)j, fk = (float)k;
+        float sv[3];
+        if (ax) rigid_velocity(m, (fi + 1.0f) * dx, (fj + 0.5f) * dx, (fk + 0.5f) * dx, sv);
+        u[index] = ax ? sv[0] : t0;
+        if (ay) rigid_velocity(m, (fi + 0.5f) * dx, (fj + 1.0f) * dx, (fk + 0.5f) * dx, sv);
+        v[index] = ay ? sv[1] : t1;
+        if (az) rigid_velocity(m, (fi + 0.5f) * dx, (fj + 0.5f) * dx, (fk + 1.0f) * dx, sv);
+        w[index] = az ? sv[2] : t2;
+    }
+}
+
+// particle_obstacle_bc with a moving solid: the same normal and push-out, but only the particle's
+// velocity relative to the solid (at the particle's position) loses its inward normal component.
+void orc_particle_obstacle_bc_moving(float* pos, const float* prev, float* vel, const uint8_t* obs, i64 n,
+                                     float inv_dx, int nx, int ny, int nz, const float* m) {
+#pragma omp parallel for schedule(static)
+    for (i64 p = 0; p < n; ++p) {
+        float* P = pos + 3 * p;
+        const float* Q = prev + 3 * p;
+        float* V = vel + 3 * p;
+        const int c0 = clampi((int)(P[0] * inv_dx), 0, nx - 1);
+        const int c1 = clampi((int)(P[1] * inv_dx), 0, ny - 1);
+        const int c2 = clampi((int)(P[2] * inv_dx), 0, nz - 1);
+        if (!obs[gidx(c0, c1, c2, ny, nz)]) continue;
+        const int p0 = clampi((int)(Q[0] * inv_dx), 0, nx - 1);
+        const int p1 = clampi((int)(Q[1] * inv_dx), 0, ny - 1);
+        const int p2 = clampi((int)(Q[2] * inv_dx), 0, nz - 1);
+        float nrm[3] = {0.0f, 0.0f, 0.0f};
+        if ((p0 != c0 || p1 != c1 || p2 != c2) && !obs[gidx(p0, p1, p2, ny, nz)]) {
+            nrm[0] = (float)(p0 - c0);
+            nrm[1] = (float)(p1 - c1);
+            nrm[2] = (float)(p2 - c2);
+        } else {
+            if (c0 > 0 && !obs[gidx(c0 - 1, c1, c2, ny, nz)]) nrm[0] -= 1.0f;
+            if (c0 + 1 < nx && !obs[gidx(c0 + 1, c1, c2, ny, nz)]) nrm[0] += 1.0f;
+            if (c1 > 0 && !obs[gidx(c0, c1 - 1, c2, ny, nz)]) nrm[1] -= 1.0f;
+            if (c1 + 1 < ny && !obs[gidx(c0, c1 + 1, c2, ny, nz)]) nrm[1] += 1.0f;
+            if (c2 > 0 && !obs[gidx(c0, c1, c2 - 1, ny, nz)]) nrm[2] -= 1.0f;
+            if (c2 + 1 < nz && !obs[gidx(c0, c1, c2 + 1, ny, nz)]) nrm[2] += 1.0f;
+        }
+        const float len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        if (len > 0.0f) {
+            nrm[0] /= len;
+            nrm[1] /= len;
+            nrm[2] /= len;
+        } else {
+            const float fb[3] = {Q[0] - P[0], Q[1] - P[1], Q[2] - P[2]};
+            const float fl = std::sqrt(fb[0] * fb[0] + fb[1] * fb[1] + fb[2] * fb[2]);
+            if (fl > 0.0f) {
+                nrm[0] = fb[0] / fl;
+                nrm[1] = fb[1] / fl;
+                nrm[2] = fb[2] / fl;
+            } else {
+                nrm[0] = 0.0f;
+                nrm[1] = 0.0f;
+                nrm[2] = 1.0f;
+            }
+        }
+        float sv[3];
+        rigid_velocity(m, P[0], P[1], P[2], sv);
+        const float r0 = V[0] - sv[0], r1 = V[1] - sv[1], r2 = V[2] - sv[2];
+        const float vn = r0 * nrm[0] + r1 * nrm[1] + r2 * nrm[2];
+        if (vn < 0.0f) {
+            V[0] -= vn * nrm[0];
+            V[1] -= vn * nrm[1];
+            V[2] -= vn * nrm[2];
+        }
+        const float dx = 1.0f / inv_dx;
+        const int cc[3] = {c0, c1, c2};
+        float cor[3] = {P[0], P[1], P[2]};
+        for (int a = 0; a < 3; ++a) {
+            if (nrm[a] < 0.0f)
+                cor[a] = 2.0f * ((float)cc[a] * dx) - P[a];
+            else if (nrm[a] > 0.0f)
+                cor[a] = 2.0f * ((float)(cc[a] + 1) * dx) - P[a];
+        }
+        const int k0 = clampi((int)(cor[0] * inv_dx), 0, nx - 1);
+        const int k1 = clampi((int)(cor[1] * inv_dx), 0, ny - 1);
+        const int k2 = clampi((int)(cor[2] * inv_dx), 0, nz - 1);
+        if (obs[gidx(k0, k1, k2, ny, nz)]) {
+            cor[0] = Q[0];
+            cor[1] = Q[1];
+            cor[2] = Q[2];
+        }
+        P[0] = cor[0];
+        P[1] = cor[1];
+        P[2] = cor[2];
+    }
+}
+
 // pressure_solve.cl:3-24 pressure_rhs
 void orc_pressure_rhs(const float* u, const float* v, const float* w, const float* ff, float* rhs, float rho_over_dt,
                       float inv_dx, int nx, int ny, int nz) {

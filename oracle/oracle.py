@@ -63,6 +63,9 @@ _SIGS = {
     "orc_residual_norms_f64": [_f64p] * 7 + [_D, _I, _I, _I, _P, _P],
     "orc_fcg_update": [_f32p, _f32p, _f64p, _f64p, _f32p, _f64p, _f32p, _f64p, _f64p, _f64p, _f64p, _D, _I, _I, _I,
                        _I, _P, _P],
+    "orc_grid_obstacle_bc_moving": [_f32p, _f32p, _f32p, _f32p, _u8p, _I, _I, _I, _f32p, _F],
+    "orc_extrapolate_obstacle_velocity_moving": [_f32p, _f32p, _f32p, _u8p, _I, _I, _I, _f32p, _F],
+    "orc_particle_obstacle_bc_moving": [_f32p, _f32p, _f32p, _u8p, _L, _F, _I, _I, _I, _f32p],
     "orc_num_threads": [],
 }
 
@@ -163,9 +166,14 @@ def particle_domain_bc(pos, vel, dx, shape):
     return pos, vel
 
 
-def particle_obstacle_bc(pos, prev, vel, obstacle, dx, shape):
+def particle_obstacle_bc(pos, prev, vel, obstacle, dx, shape, motion=None):
     pos, vel = c(pos).copy(), c(vel).copy()
-    lib().orc_particle_obstacle_bc(pos, c(prev), vel, c(obstacle, np.uint8), len(pos), F32(1.0 / float(dx)), *shape)
+    if motion is None:
+        lib().orc_particle_obstacle_bc(pos, c(prev), vel, c(obstacle, np.uint8), len(pos), F32(1.0 / float(dx)),
+                                       *shape)
+    else:
+        lib().orc_particle_obstacle_bc_moving(pos, c(prev), vel, c(obstacle, np.uint8), len(pos),
+                                              F32(1.0 / float(dx)), *shape, c(motion))
     return pos, vel
 
 
@@ -199,12 +207,19 @@ def grid_domain_bc(u, v, w, shape):
     return u, v, w
 
 
-def grid_obstacle_bc(u, v, w, ff, obstacle, shape):
-    """boundary_conditions.py:53-79: grid_obstacle_bc then extrapolate_obstacle_velocity."""
+def grid_obstacle_bc(u, v, w, ff, obstacle, shape, motion=None, dx=None):
+    """boundary_conditions.py:53-79: grid_obstacle_bc then extrapolate_obstacle_velocity. ``motion``
+    (9 floats: velocity, angular velocity, pivot in grid-local coordinates; with the cell size ``dx``):
+    a moving collider (no counterpart in the reference)."""
     u, v, w, ff = c(u).copy(), c(v).copy(), c(w).copy(), c(ff).copy()
     ob = c(obstacle, np.uint8)
-    lib().orc_grid_obstacle_bc(u, v, w, ff, ob, *shape)
-    lib().orc_extrapolate_obstacle_velocity(u, v, w, ob, *shape)
+    if motion is None:
+        lib().orc_grid_obstacle_bc(u, v, w, ff, ob, *shape)
+        lib().orc_extrapolate_obstacle_velocity(u, v, w, ob, *shape)
+    else:
+        m = c(motion)
+        lib().orc_grid_obstacle_bc_moving(u, v, w, ff, ob, *shape, m, F32(dx))
+        lib().orc_extrapolate_obstacle_velocity_moving(u, v, w, ob, *shape, m, F32(dx))
     return u, v, w, ff
 
 
@@ -390,7 +405,7 @@ class OracleSim:
 
     def __init__(self, shape, dx, positions, velocities, obstacle=None, dt=1.0 / 240.0, flip_ratio=1.0,
                  gravity=(0.0, 0.0, -9.81), rho=1000.0, nu=1.0e-6, ppc=8, min_size=8, num_vcycles=1, tol=None,
-                 coarse_iterations=64, pre_smooth=2, post_smooth=4):
+                 coarse_iterations=64, pre_smooth=2, post_smooth=4, collider_pose=None, origin=(0.0, 0.0, 0.0)):
         self.shape = tuple(int(s) for s in shape)
         self.dx, self.dt, self.flip_ratio = float(dx), float(dt), float(flip_ratio)
         self.gravity, self.rho, self.nu, self.ppc = tuple(gravity), float(rho), float(nu), ppc
@@ -401,6 +416,11 @@ class OracleSim:
         self.tol = tol
         self.fcg_options = dict(coarse_iterations=coarse_iterations, pre_smooth=pre_smooth, post_smooth=post_smooth)
         self.last_cycles = 0
+        # moving colliders: collider_pose(t) -> (world triangle arrays at time t, the 9 motion parameters
+        # in grid-local coordinates); each step voxelises them at the step's start time
+        self.collider_pose = collider_pose
+        self.origin = tuple(origin)
+        self.steps_done = 0
         self.pos = c(positions).copy()
         self.vel = c(velocities).copy()
         self.obstacle = np.zeros(self.shape, np.uint8) if obstacle is None else c(obstacle, np.uint8)
@@ -410,15 +430,23 @@ class OracleSim:
 
     def step(self):
         s, dx, dt = self.shape, self.dx, self.dt
+        motion = None
+        if self.collider_pose is not None:
+            tris, motion = self.collider_pose(self.steps_done * dt)
+            mask = np.zeros(s, np.uint8)
+            for t in tris:
+                mask = voxelise(t, s, dx, self.origin, mask)
+            self.obstacle = mask
+        self.steps_done += 1
         pos_s, vel_s, u, v, w, ff, counts, offsets = particle_to_grid(self.pos, self.vel, dx, s, self.ppc)
         self.trace.update(counts=counts, offsets=offsets, sorted_pos=pos_s, sorted_vel=vel_s, p2g_u=u, p2g_v=v,
                           p2g_w=w, p2g_ff=ff)
-        u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s)
+        u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s, motion, dx)
         u, v, w = grid_domain_bc(u, v, w, s)
         uo, vo, wo = u, v, w
         u, v, w = update_velocity(u, v, w, ff, self.gravity, (0.0, 0.0, 0.0), self.rho, self.nu, dx, dt, s)
         u, v, w = grid_domain_bc(u, v, w, s)
-        u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s)
+        u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s, motion, dx)
         self.trace.update(pre_u=u, pre_v=v, pre_w=w, pressure_in=self.pressure.copy())
         if self.tol is None:
             self.pressure, rhs, op0 = pressure_solve(u, v, w, ff, self.pressure, dx, dt, self.rho, self.num_vcycles,
@@ -432,13 +460,13 @@ class OracleSim:
         self.trace.update(rhs=rhs, ff=ff, pressure=self.pressure.copy())
         u, v, w = pressure_correction(u, v, w, self.pressure, dx, dt, self.rho, s)
         u, v, w = grid_domain_bc(u, v, w, s)
-        u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s)
+        u, v, w, ff = grid_obstacle_bc(u, v, w, ff, self.obstacle, s, motion, dx)
         self.trace.update(u=u, v=v, w=w)
         vel = grid_to_particle(vel_s, pos_s, (u, v, w), (uo, vo, wo), dx, s, self.flip_ratio)
         self.trace.update(vel_g2p=vel)
         prev = pos_s.copy()
         pos = advect(pos_s, vel, dt)
         pos, vel = particle_domain_bc(pos, vel, dx, s)
-        pos, vel = particle_obstacle_bc(pos, prev, vel, self.obstacle, dx, s)
+        pos, vel = particle_obstacle_bc(pos, prev, vel, self.obstacle, dx, s, motion)
         self.pos, self.vel = pos, vel
         return self
