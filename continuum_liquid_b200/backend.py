@@ -89,9 +89,11 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_build_coarse": [P, P],
     "clb_mg_w_cycle": [P, P, P, I, I, I, P],
     "clb_mg_smooth": [P, I, P, P, I, P],
+    "clb_mg_level0_iteration": [P, P, P, P, I, P],
     "clb_mg_set_option": [I, I],
     "clb_mg_residual_partials": [L],
     "clb_mg_tile_capacity": [I, I, I, I],
+    "clb_mg_fused_tile_capacity": [I, I, I],
     "clb_mg_residual_norms": [P, I, P, P, F, I, I, I, P, P, P, P],
     "clb_mg_ir_init": [P, P, P, I, I, I, P],
     "clb_mg_ir_step": [P, P, P, P, P, F, I, I, I, P, P, P, P],
@@ -124,6 +126,7 @@ _RESTYPES = {
     "clb_scan_scratch_bytes": ctypes.c_int64,
     "clb_launch_count": ctypes.c_int64,
     "clb_mg_tile_capacity": ctypes.c_int64,
+    "clb_mg_fused_tile_capacity": ctypes.c_int64,
 }
 
 
@@ -148,6 +151,8 @@ class MGHierarchy(ctypes.Structure):
         ("tiles", ctypes.c_void_p * MG_MAX_LEVELS),
         ("tile_counts", ctypes.c_void_p),
         ("zero_outside", ctypes.c_int32),
+        ("fused_tiles", ctypes.c_void_p),
+        ("fused_tile_count", ctypes.c_void_p),
     ]
 
 

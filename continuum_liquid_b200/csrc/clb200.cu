@@ -11,6 +11,7 @@
 #include "mg_half.cuh"
 #include "mg_cluster.cuh"
 #include "mg_tiles.cuh"
+#include "mg_level0.cuh"
 #include "batch.cuh"
 #include "sources.cuh"
 #include "voxelise.cuh"
@@ -151,6 +152,19 @@ int clb_init(int device) {
     if (check_call(cudaFuncSetAttribute(k_p2g_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, P2GT_SMEM),
                    "tiled P2G attribute"))
         return 1;
+    e = cudaFuncSetAttribute(k_l0_iter_tiles<L0F_ZERO | L0F_RESTRICT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)L0Region<3>::smem());
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_l0_iter_tiles<L0F_RESTRICT>,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)L0Region<3>::smem());
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_l0_iter_tiles<L0F_ZERO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)L0Region<2>::smem());
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_l0_iter_tiles<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)L0Region<2>::smem());
+    e = e != cudaSuccess ? e : cudaFuncSetAttribute(k_l0_iter_tiles<L0F_PROLONG>,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)L0Region<2>::smem());
+    if (check_call(e, "level-0 fused iteration attribute")) return 1;
     if (conv_set_attributes()) return 1;
     return 0;
 }
@@ -705,6 +719,17 @@ int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream) {
             CLB_LAUNCH_CHECK("k_mg_tiles");
         }
     }
+    if (h->fused_tiles) {
+        CLB_REQUIRE(h->fused_tile_count != nullptr, "multigrid: fused_tiles without fused_tile_count");
+        const int* n = h->shape[0];
+        const i64 tiles = l0_tile_capacity(n[0], n[1], n[2]);
+        if (check_call(cudaMemsetAsync(h->fused_tile_count, 0, sizeof(int32_t), s), "fused tile count")) return 1;
+        if (tiles > 0) {
+            launch((unsigned)tiles, L0T_THREADS, 0, s)(k_l0_fused_tiles, (const uint8_t*)h->op0, n[0], n[1], n[2],
+                                                      h->fused_tiles, h->fused_tile_count);
+            CLB_LAUNCH_CHECK("k_l0_fused_tiles");
+        }
+    }
     return 0;
 }
 
@@ -712,6 +737,8 @@ int64_t clb_mg_tile_capacity(int nx, int ny, int nz, int finest) {
     if (nx <= 0 || ny <= 0 || nz <= 0) return 0;
     return tile_capacity(nx, ny, nz, finest != 0);
 }
+
+int64_t clb_mg_fused_tile_capacity(int nx, int ny, int nz) { return l0_tile_capacity(nx, ny, nz); }
 
 namespace {
 
@@ -795,7 +822,7 @@ bool tile_sweeps(const LevelView& v) {
 int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s, bool sparse = false,
            bool from_zero = false) {
     const i64 C = (i64)v.nx * v.ny * v.nz;
-    const int kind = v.sweep == 0 ? (v.half ? 4 : 1) : v.sweep;
+    const int kind = v.sweep == 0 || v.sweep == 7 ? (v.half ? 4 : 1) : v.sweep;  // 7: see level0_fused
     const int vec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
     if (sparse && tile_sweeps(v)) {
         const unsigned grid = tile_grid(v);
@@ -1055,7 +1082,79 @@ int level0_zero(const clb_mg_hierarchy* h, const LevelView& v, int first_sweeps,
 }
 
 int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int pre, int post, int coarse_iters,
+            cudaStream_t s);
+
+// Whether level 0 of this W-cycle runs as the fused tile launches of mg_level0.cuh: sweep kind 7 on
+// level 0, its 3-D fluid tiles and second buffer, a correction from zero (zero_outside = 2), at least
+// one pre- and one post-smoothing iteration, and an FP32 level 1 below.
+bool level0_fused(const clb_mg_hierarchy* h, int pre, int post) {
+    return h->sweep[0] == 7 && h->fused_tiles && h->fused_tile_count && h->alt[0] && h->zero_outside == 2 &&
+           pre >= 1 && post >= 1 && h->levels >= 2 && !is_half(h, 1);
+}
+
+extern "C++" {
+template <int MODE>
+void launch_l0_iter(const clb_mg_hierarchy* h, const float* in, float* out, const float* rhs, cudaStream_t s) {
+    const int* n = h->shape[0];
+    const int* c = h->shape[1];
+    const i64 cap = l0_tile_capacity(n[0], n[1], n[2]);
+    static const int per_sm = [] {  // once per mode
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_l0_iter_tiles<MODE>, L0T_THREADS,
+                                                          L0Region<(MODE & L0F_RESTRICT) ? 3 : 2>::smem()) !=
+            cudaSuccess) {
+            (void)cudaGetLastError();
+            b = 0;
+        }
+        return b > 0 ? b : 1;
+    }();
+    const i64 most = (i64)per_sm * (g_sm_count > 0 ? g_sm_count : 148);
+    const unsigned grid = (unsigned)(cap < most ? (cap > 0 ? cap : 1) : most);
+    launch(grid, L0T_THREADS, L0Region<(MODE & L0F_RESTRICT) ? 3 : 2>::smem(), s)(
+        k_l0_iter_tiles<MODE>, h->fused_tiles, h->fused_tile_count, in, out, rhs, h->op0, h->delta, n[0], n[1], n[2],
+        h->p[1], h->b[1], h->p[1], c[0], c[1], c[2]);
+}
+}  // extern "C++"
+
+// Level 0 of a W-cycle from a zero correction in pre + post fused launches: the first pre-smoothing
+// iteration reads no x, the last one restricts, the first post-smoothing one prolongs. The launches
+// alternate between x and the level's second buffer, the first writing the one that makes the last
+// write land in x.
+int w_cycle_level0_fused(const clb_mg_hierarchy* h, float* x, const float* rhs, int pre, int post, int coarse_iters,
+                         cudaStream_t s) {
+    float* buf[2] = {x, h->alt[0]};
+    int dst = (pre + post) % 2 == 1 ? 0 : 1;
+    const float* src = nullptr;
+    for (int it = 0; it < pre; ++it) {
+        const bool first = it == 0, last = it == pre - 1;
+        if (first && last) launch_l0_iter<L0F_ZERO | L0F_RESTRICT>(h, src, buf[dst], rhs, s);
+        else if (first) launch_l0_iter<L0F_ZERO>(h, src, buf[dst], rhs, s);
+        else if (last) launch_l0_iter<L0F_RESTRICT>(h, src, buf[dst], rhs, s);
+        else launch_l0_iter<0>(h, src, buf[dst], rhs, s);
+        CLB_LAUNCH_CHECK("k_l0_iter_tiles");
+        src = buf[dst];
+        dst ^= 1;
+    }
+    const int both = cluster_visit(h, 1, pre, post, coarse_iters, s, 2);
+    if (both < 0) return 1;
+    if (both == 0) {
+        if (w_cycle(h, 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+        if (w_cycle(h, 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+    }
+    for (int it = 0; it < post; ++it) {
+        if (it == 0) launch_l0_iter<L0F_PROLONG>(h, src, buf[dst], rhs, s);
+        else launch_l0_iter<0>(h, src, buf[dst], rhs, s);
+        CLB_LAUNCH_CHECK("k_l0_iter_tiles");
+        src = buf[dst];
+        dst ^= 1;
+    }
+    CLB_REQUIRE(src == x, "mg_w_cycle: fused level-0 iterations ended outside x");
+    return 0;
+}
+
+int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int pre, int post, int coarse_iters,
             cudaStream_t s) {
+    if (level == 0 && level0_fused(h, pre, post)) return w_cycle_level0_fused(h, x, rhs, pre, post, coarse_iters, s);
     const LevelView v = level_view(h, level, x, rhs);
     // coarse levels hold 0 outside the fluid (zeroed by clb_mg_build_coarse and the restriction);
     // level 0 does when the caller says so
@@ -1153,6 +1252,26 @@ int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pr
         CLB_LAUNCH_CHECK("k_fp16_scale");
     }
     return w_cycle(h, 0, x, rhs, pre_smooth, post_smooth, coarse_iterations, s);
+}
+
+int clb_mg_level0_iteration(const clb_mg_hierarchy* h, const float* x_in, float* x_out, const float* rhs, int mode,
+                            void* stream) {
+    if (check_hierarchy(h)) return 1;
+    CLB_REQUIRE(h->fused_tiles && h->fused_tile_count, "mg_level0_iteration: no fused tiles");
+    CLB_REQUIRE(h->levels >= 2 && !is_half(h, 1), "mg_level0_iteration: level 1 must exist and be FP32");
+    CLB_REQUIRE(x_out && rhs && ((mode & L0F_ZERO) || x_in), "mg_level0_iteration: null array");
+    CLB_REQUIRE((mode & L0F_ZERO) || x_in != x_out, "mg_level0_iteration: x_in and x_out must differ");
+    cudaStream_t s = CLB_STREAM(stream);
+    switch (mode) {
+        case 0: launch_l0_iter<0>(h, x_in, x_out, rhs, s); break;
+        case L0F_ZERO: launch_l0_iter<L0F_ZERO>(h, nullptr, x_out, rhs, s); break;
+        case L0F_RESTRICT: launch_l0_iter<L0F_RESTRICT>(h, x_in, x_out, rhs, s); break;
+        case L0F_ZERO | L0F_RESTRICT: launch_l0_iter<L0F_ZERO | L0F_RESTRICT>(h, nullptr, x_out, rhs, s); break;
+        case L0F_PROLONG: launch_l0_iter<L0F_PROLONG>(h, x_in, x_out, rhs, s); break;
+        default: return set_error("mg_level0_iteration: mode %d is not 0, 1, 2, 3 or 4", mode);
+    }
+    CLB_LAUNCH_CHECK("k_l0_iter_tiles");
+    return 0;
 }
 
 int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int iterations, void* stream) {

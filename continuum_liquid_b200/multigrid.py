@@ -230,6 +230,12 @@ class MultigridHierarchy:
                 self.tiles.append(torch.zeros(max(cap, 1), dtype=torch.int32, device=device))
                 self.struct.tiles[l] = self.tiles[l].data_ptr()
             self.struct.tile_counts = self.tile_counts.data_ptr()
+            # 3-D fluid tiles of level 0 for the fused level-0 visit (sweep kind 7, csrc/mg_level0.cuh)
+            cap = int(kernels.lib.clb_mg_fused_tile_capacity(*self.grid_shape))
+            self.fused_tiles = torch.zeros(max(cap, 1), dtype=torch.int32, device=device)
+            self.fused_tile_count = torch.zeros(1, dtype=torch.int32, device=device)
+            self.struct.fused_tiles = self.fused_tiles.data_ptr()
+            self.struct.fused_tile_count = self.fused_tile_count.data_ptr()
         for l in range(1, levels):
             if self.is_fp16(l):
                 self.struct.sweep[l] = 4
@@ -270,16 +276,37 @@ class MultigridHierarchy:
 
     def set_sweep(self, level: int, kind: int) -> None:
         """Red-black sweep implementation of one level (see clb_mg_hierarchy.sweep); FP16 levels take
-        kinds 2-6 (0 means 4)."""
+        kinds 2-6 (0 means 4); kind 7 on level 0 runs the W-cycle's level-0 visit as fused tile launches
+        (tolerance-mode W-cycles from a zero correction)."""
         kind = int(kind)
-        if kind not in (0, 1, 2, 3, 4, 5, 6):
+        if kind not in (0, 1, 2, 3, 4, 5, 6, 7):
             raise ValueError(f"unknown sweep kind {kind}")
+        if kind == 7 and level != 0:
+            raise ValueError("sweep kind 7 (the fused level-0 visit) is for level 0 only")
         if self.is_fp16(level) and kind == 1:
             raise ValueError(f"level {level} is stored in FP16: sweep kinds 2-6")
         self.struct.sweep[level] = 4 if self.is_fp16(level) and kind == 0 else kind
 
     def sweeps(self) -> list[int]:
         return [int(self.struct.sweep[l]) for l in range(self.levels)]
+
+    def level0_iteration(self, x_in, x_out, rhs, mode: int, queue=None) -> None:
+        """One launch of the fused level-0 kernel (clb_mg_level0_iteration): mode 1 = from zero, 2 = with
+        the restriction into level 1, 3 = both, 4 = with the prolongation of level 1's p, 0 = neither."""
+        self.kernels.call_hierarchy("clb_mg_level0_iteration", self.struct, x_in, x_out, rhs, int(mode),
+                                    stream=queue)
+
+    def fused_tile_cells(self) -> int:
+        """Grid cells covered by the listed fused level-0 tiles (after build_coarse)."""
+        n = int(self.fused_tile_count.item())
+        if n == 0:
+            return 0
+        nx, ny, nz = self.grid_shape
+        tj, tk = -(-(ny - 2) // 8), -(-(nz - 2) // 32)
+        t = self.fused_tiles[:n].cpu().numpy().astype(np.int64)
+        a, b, c = t // (tj * tk), (t // tk) % tj, t % tk
+        ext = lambda start, size, n_: np.minimum(start + size, n_) - start
+        return int(np.sum(ext(1 + 8 * a, 8, nx) * ext(1 + 8 * b, 8, ny) * ext(1 + 32 * c, 32, nz)))
 
     def smooth(self, level: int, iterations: int, x=None, rhs=None, queue=None, zero_outside: bool = False) -> None:
         """``iterations`` red-black Gauss-Seidel iterations on one level. ``zero_outside``: the caller

@@ -110,7 +110,8 @@ class PressureSolver:
     def __init__(self, kernels: Backend, grid_shape, dx: float, min_size: int = 8, max_cycles: int = 100,
                  autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64,
                  coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS,
-                 pre_smooth: int = multigrid.PRE_SMOOTH, post_smooth: int = multigrid.POST_SMOOTH):
+                 pre_smooth: int = multigrid.PRE_SMOOTH, post_smooth: int = multigrid.POST_SMOOTH,
+                 fused_level0: bool = True):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.coarse_fp16 = bool(coarse_fp16)
@@ -128,6 +129,9 @@ class PressureSolver:
         # tolerance mode's W-cycle preconditioner; the reference's 2 and 4 by default (fixed-cycle mode
         # always uses those)
         self.pre_smooth, self.post_smooth = int(pre_smooth), int(post_smooth)
+        # the tolerance mode's W-cycles run level 0 as fused tile launches (sweep kind 7,
+        # csrc/mg_level0.cuh); the values are those of the launch-per-step path
+        self.fused_level0 = bool(fused_level0)
         if self.pre_smooth < 0 or self.post_smooth < 0 or self.pre_smooth + self.post_smooth == 0:
             raise ValueError("pre_smooth and post_smooth must be >= 0 and not both 0")
         # FP16 storage of the coarse levels of at most fp16_max_size cells per side (tolerance mode only:
@@ -183,8 +187,14 @@ class PressureSolver:
         # the correction starts from 0: its buffer is 0 outside the fluid (zeroed once per solve, and
         # the W-cycle writes 0 to every cell that is not fluid), so the W-cycle's first sweep ignores
         # the previous correction at fluid cells instead of a fill of the whole buffer
-        h.w_cycle(self.correction, self.residual, pre_smooth=self.pre_smooth, post_smooth=self.post_smooth,
-                  coarse_iterations=self.coarse_iterations, queue=queue, x_from_zero=True)
+        kind0 = int(h.struct.sweep[0])
+        if self.fused_level0:
+            h.struct.sweep[0] = 7
+        try:
+            h.w_cycle(self.correction, self.residual, pre_smooth=self.pre_smooth, post_smooth=self.post_smooth,
+                      coarse_iterations=self.coarse_iterations, queue=queue, x_from_zero=True)
+        finally:
+            h.struct.sweep[0] = kind0
         if self.method == "fcg":
             self.kernels.call("clb_mg_fcg_dots", self.correction, self.direction[src], self.residual, h.op0, delta,
                               *self.grid_shape, self.fcg_partials, self.fcg_state, stream=queue)

@@ -262,7 +262,14 @@ typedef struct clb_mg_hierarchy {
                                             5 = one fused launch per two iterations, 8x8x32 tiles
                                                 (needs alt; on FP32 coarse levels it runs as 6),
                                             6 = one fused launch per two iterations, 4x4x32 tiles
-                                                (needs alt).
+                                                (needs alt),
+                                            7 = level 0 only: inside clb_mg_w_cycle, the whole level-0
+                                                visit in pre + post launches on 3-D fluid tiles (the
+                                                last pre-smoothing iteration fused with the residual and
+                                                the restriction, the first post-smoothing one with the
+                                                prolongation), when fused_tiles, alt[0] and an FP32
+                                                level 1 are given, zero_outside is 2 and pre, post >= 1;
+                                                otherwise as 1.
                                             All kinds give identical values. */
     float* fp16_scale;                   /* device float[4] written by clb_mg_w_cycle: sigma_b,
                                             1/sigma_p, kappa, 1/kappa (FP16 levels only) */
@@ -287,10 +294,17 @@ typedef struct clb_mg_hierarchy {
                                             previous one there): the first colour sweep ignores x, or
                                             x is zeroed first;
                                             0: level-0 sweeps cover the whole grid */
+    /* No counterpart in the reference: the 3-D fluid tiles of level 0 (8 x 8 x 32 cells starting at
+     * cell (1, 1, 1)) that sweep kind 7 walks; clb_mg_build_coarse lists them. NULL: kind 7 runs as 1. */
+    int32_t* fused_tiles;                /* clb_mg_fused_tile_capacity(level-0 shape) entries */
+    int32_t* fused_tile_count;           /* device int32: listed tiles */
 } clb_mg_hierarchy;
 
 /* Number of tiles of a level of nx x ny x nz cells (finest != 0: the finest level's tile shape). */
 int64_t clb_mg_tile_capacity(int nx, int ny, int nz, int finest);
+
+/* Number of 3-D fluid tiles of level 0 (clb_mg_hierarchy.fused_tiles) for nx x ny x nz cells. */
+int64_t clb_mg_fused_tile_capacity(int nx, int ny, int nz);
 
 /* pressure_solve.cl:3-24 pressure_rhs fused with multigrid.cl:63-88 build_finest_operator, writing
  * the packed level-0 operator. */
@@ -304,6 +318,15 @@ int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream);
  * as pressure_solve.py:61-83: 2, 4, 64). */
 int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pre_smooth, int post_smooth,
                    int coarse_iterations, void* stream);
+
+/* No counterpart in the reference: one launch of sweep kind 7's level-0 kernel on the fused tiles
+ * (clb_mg_build_coarse lists them): x_out = one red-black iteration of x_in on level 0, with
+ *   mode 1: x_in counts as 0 (not read),
+ *   mode 2: also the residual of the result restricted into level 1 (p = 0, b = the children's sum),
+ *   mode 3: both, mode 4: x_in plus level 1's p prolonged first (multigrid.cl:182-201), mode 0: neither.
+ * Cells of tiles that are not listed are not written. x_in and x_out must differ. */
+int clb_mg_level0_iteration(const clb_mg_hierarchy* h, const float* x_in, float* x_out, const float* rhs, int mode,
+                            void* stream);
 
 /* multigrid.py:190-220 smooth: `iterations` red-black Gauss-Seidel iterations on one level (level 0
  * uses x and rhs; coarse levels their own p and b). With h->zero_outside = 1 and tile lists built by

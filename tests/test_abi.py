@@ -42,7 +42,8 @@ def test_load_library_sets_signatures_and_pure_helpers():
 def test_hierarchy_struct_layout():
     # int32 levels (0), int32[16][3] (4..196), float delta (196), int32 fp16_level (200), then
     # 8-byte-aligned pointers: op0 at 208, the five pointer tables, int32 sweep[16], the three FP16
-    # pointers, the tile table, the tile counts and the int32 zero_outside flag (padded to 8 bytes)
+    # pointers, the tile table, the tile counts, the int32 zero_outside flag (padded to 8 bytes) and the
+    # two fused-tile pointers
     assert backend.MGHierarchy.delta.offset == 196
     assert backend.MGHierarchy.fp16_level.offset == 200
     assert backend.MGHierarchy.op0.offset == 208
@@ -51,7 +52,8 @@ def test_hierarchy_struct_layout():
     tiles = 216 + 5 * 16 * 8 + 16 * 4 + 3 * 8
     assert backend.MGHierarchy.tiles.offset == tiles
     assert backend.MGHierarchy.zero_outside.offset == tiles + 16 * 8 + 8
-    assert ctypes.sizeof(backend.MGHierarchy) == tiles + 16 * 8 + 8 + 8
+    assert backend.MGHierarchy.fused_tiles.offset == tiles + 16 * 8 + 8 + 8
+    assert ctypes.sizeof(backend.MGHierarchy) == tiles + 16 * 8 + 8 + 8 + 2 * 8
 
 
 def test_backend_without_gpu_fails_loudly(monkeypatch):
