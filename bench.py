@@ -41,12 +41,14 @@ UNIT = "steps/s"
 TOL = 1e-6
 COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarsest-level iterations
 SMOOTHING_CHOICES = ((2, 4), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
-# DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/), and the
-# grid cells of the listed tiles when it was captured (bench.py --case sweep0, the block at rest): the
-# traffic is scaled to the tile cells of the measured launch (a launch streams its listed tiles)
-NCU_TRAFFIC_BYTES: dict[str, int] = {}
-NCU_CELLS_AT_CAPTURE: dict[str, int] = {}
-# algorithmic bytes per grid cell of the listed level-0 tiles: the pre-smoothing launch reads b 4 and the
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
+NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
+                     "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
+# fluid tiles listed when the tile sweep above was captured (bench.py --case sweep0): its traffic is scaled to
+# the tile count of the measured launch (the sweep streams each listed tile and its stencil neighbours)
+NCU_TILES_AT_CAPTURE = {"k_rbgs_colour_tiles<true,4>": 5715}
+# algorithmic bytes per grid cell of the listed fused level-0 tiles (--case sweep0 --fused-level0): the
+# pre-smoothing launch reads b 4 and the
 # operator 1, writes x 4 and level 1's p and b (8 per coarse cell = 1 per fine cell); the post-smoothing
 # launch reads x 4, the operator 1, b 4 and level 1's p (4 per coarse cell = 0.5 per fine cell), writes x 4
 LEVEL0_PRE_BYTES, LEVEL0_POST_BYTES = 10.0, 13.5
@@ -79,14 +81,18 @@ def parse_args():
                          "tolerance in the Poisson comparison, with 4 coarsest-level iterations)")
     ap.add_argument("--case", choices=["step", "sweep0", "wcycle", "batch", "unet", "collider", "particles"],
                     default="step",
-                    help="step: the benchmark; sweep0: only the level-0 part of the W-cycle (the fused pre- and "
-                         "post-smoothing launches) on the scene's pressure system (no particles: a small-memory case "
-                         "for profiling); wcycle: whole W-cycles on that system; batch: the batched "
+                    help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
+                         "(no particles: a small-memory case for profiling); wcycle: whole W-cycles on that system; "
+                         "batch: the batched "
                          "uneven-scenes workload (32 scenes of sizes 48-160, one launch per stage)")
     ap.add_argument("--scenes", type=int, default=32, help="scenes of --case batch")
     ap.add_argument("--sequential-steps", type=int, default=2,
                     help="steps of the one-scene-at-a-time comparison of --case batch (0: skip)")
-    ap.add_argument("--sweeps", type=int, default=4, help="launch pairs of --case sweep0, W-cycles of --case wcycle")
+    ap.add_argument("--sweeps", type=int, default=4,
+                    help="red-black iterations (with --fused-level0: launch pairs) of --case sweep0, W-cycles of "
+                         "--case wcycle")
+    ap.add_argument("--fused-level0", action="store_true",
+                    help="--case sweep0/wcycle: level 0 of the W-cycle as the fused tile launches (sweep kind 7)")
     return ap.parse_args()
 
 
@@ -325,8 +331,10 @@ def sweep_case(args):
     ps.rhs.copy_(torch.randn(scene.grid_shape, device="cuda", generator=gen) * ff)
     h = ps.hierarchy
     tune_hierarchy(h, ps.correction, ps.residual)
-    h.set_sweep(0, 7)  # the tolerance mode's level-0 visit: fused tile launches
+    if args.fused_level0:
+        h.set_sweep(0, 7)  # level 0 of the W-cycle as the fused tile launches of csrc/mg_level0.cuh
     p = torch.zeros_like(zero)
+    h.smooth(0, 2, p, ps.rhs, zero_outside=True)  # p is 0 outside the fluid: the fluid-tile sweep
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.case == "wcycle":
@@ -351,8 +359,22 @@ def sweep_case(args):
                           "sweep_kinds": h.sweeps(), "coarse_iterations": k,
                           "ms_per_w_cycle": e0.elapsed_time(e1) / args.sweeps}), flush=True)
         return
-    # the level-0 part of a W-cycle: the pre-smoothing launch (from zero, with the restriction) and the
-    # post-smoothing launch (with the prolongation), alternating between x and the second buffer
+    if not args.fused_level0:
+        torch.cuda.nvtx.range_push("sweeps")
+        e0.record()
+        h.smooth(0, args.sweeps, p, ps.rhs, zero_outside=True)
+        e1.record()
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.sweeps
+        tiles0 = int(h.tile_counts[0].item())
+        cells = tiles0 * 4 * (128 if scene.grid_shape[2] % 4 == 0 else 32)
+        print(json.dumps({"case": "sweep0", "grid": list(scene.grid_shape), "fluid_tiles": tiles0,
+                          "tile_cells": cells, "ms_per_iteration": ms,
+                          "algorithmic_gb_s": 13.0 * cells / (ms * 1e-3) / 1e9}), flush=True)
+        return
+    # the fused level-0 part of a W-cycle: the pre-smoothing launch (from zero, with the restriction) and
+    # the post-smoothing launch (with the prolongation), alternating between x and the second buffer
     alt = h.alt[0]
 
     def pair():
@@ -978,46 +1000,39 @@ def our_arm(args):
     audit = pressure_error_audit(sim, snapshot, end_positions, args.steps, scene.min_size)
     del snapshot
 
-    # --- roofline: the level-0 part of the W-cycle as the timed steps run it (the fused pre- and
-    # post-smoothing launches on the level-0 fluid tiles), timed alone on the stream -----------------
+    # --- roofline: the level-0 red-black sweep as the timed steps run it (on the fluid tiles), timed
+    # alone on the stream ---------------------------------------------------------------------------
     ps = sim.pressure_solver
     h = ps.hierarchy
     iters = 20
-    alt = h.alt[0]
-
-    def level0_pair():
-        h.level0_iteration(None, alt, ps.residual, 3)
-        h.level0_iteration(alt, ps.correction, ps.residual, 4)
-
     torch.cuda.synchronize()
-    level0_pair()
+    ps.correction.zero_()
+    h.smooth(0, 2, ps.correction, ps.residual, zero_outside=True)
     s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s3.record()
-    for _ in range(iters):
-        level0_pair()
+    h.smooth(0, iters, ps.correction, ps.residual, zero_outside=True)
     e3.record()
     torch.cuda.synchronize()
-    per_pair_s = s3.elapsed_time(e3) / 1e3 / iters
-    tiles0 = int(h.fused_tile_count.item())
-    cells = h.fused_tile_cells()
-    algorithmic = (LEVEL0_PRE_BYTES + LEVEL0_POST_BYTES) * cells / 2.0  # per launch, the pair's mean
-    per_launch_s = per_pair_s / 2.0
+    per_launch_s = s3.elapsed_time(e3) / 1e3 / (2 * iters)
+    vec = scene.grid_shape[2] % 4 == 0
+    tiles0 = int(h.tile_counts[0].item())
+    cells = tiles0 * 4 * (128 if vec else 32)  # the cells of the fluid tiles a launch streams
+    # p read + write 8 B, b 4 B, packed operator 1 B per cell per red-black iteration; one colour per launch
+    algorithmic = 13.0 * cells / 2.0
     achieved = algorithmic / per_launch_s / 1e9
     peak, peak_kind = measured_peak_hbm()
-    kernel = "k_l0_iter_tiles<3> + k_l0_iter_tiles<4>"
+    kernel = "k_rbgs_colour_tiles<true,4>" if vec else "k_rbgs_colour_tiles<true,1>"
     traffic = NCU_TRAFFIC_BYTES.get(kernel)
-    if traffic is not None and kernel in NCU_CELLS_AT_CAPTURE:
-        traffic = int(round(traffic * cells / NCU_CELLS_AT_CAPTURE[kernel]))
-    roofline = {"kernel": f"{kernel} (level 0 of the W-cycle: a red-black iteration with the residual and its "
-                          f"restriction, then the prolongation with a red-black iteration, on the {tiles0} listed "
-                          f"8x8x32 fluid tiles of {int(h.kernels.lib.clb_mg_fused_tile_capacity(*scene.grid_shape))};"
-                          f" figures per launch, the pair's mean)",
+    if traffic is not None and kernel in NCU_TILES_AT_CAPTURE:
+        traffic = int(round(traffic * tiles0 / NCU_TILES_AT_CAPTURE[kernel]))
+    roofline = {"kernel": f"{kernel} (level-0 red-black Gauss-Seidel on the {tiles0} fluid tiles of "
+                          f"{int(h.kernels.lib.clb_mg_tile_capacity(*scene.grid_shape, 1))}, one colour per launch)",
                 "bound": "hbm", "tile_cells": cells,
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                 "traffic": traffic, "algorithmic_bytes_per_launch": algorithmic, "launch_us": per_launch_s * 1e6}
 
-    rooflines = [dict(roofline, stage="level0_visit", ms=per_launch_s * 1e3,
+    rooflines = [dict(roofline, stage="level0_sweep", ms=per_launch_s * 1e3,
                       share_of_step=per_launch_s * 1e3 / (elapsed_ms / args.steps))]
     rooflines += kernel_rooflines(sim, peak, elapsed_ms / args.steps)
 

@@ -111,7 +111,7 @@ class PressureSolver:
                  autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64,
                  coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS,
                  pre_smooth: int = multigrid.PRE_SMOOTH, post_smooth: int = multigrid.POST_SMOOTH,
-                 fused_level0: bool = True):
+                 fused_level0: bool = False):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.coarse_fp16 = bool(coarse_fp16)
@@ -129,8 +129,9 @@ class PressureSolver:
         # tolerance mode's W-cycle preconditioner; the reference's 2 and 4 by default (fixed-cycle mode
         # always uses those)
         self.pre_smooth, self.post_smooth = int(pre_smooth), int(post_smooth)
-        # the tolerance mode's W-cycles run level 0 as fused tile launches (sweep kind 7,
-        # csrc/mg_level0.cuh); the values are those of the launch-per-step path
+        # fused_level0: the tolerance mode's W-cycles run level 0 as fused tile launches (sweep kind 7,
+        # csrc/mg_level0.cuh), with the values of the launch-per-step path. Off by default: at 256^3 the
+        # recomputed halo costs more instructions than the four launches it saves
         self.fused_level0 = bool(fused_level0)
         if self.pre_smooth < 0 or self.post_smooth < 0 or self.pre_smooth + self.post_smooth == 0:
             raise ValueError("pre_smooth and post_smooth must be >= 0 and not both 0")
