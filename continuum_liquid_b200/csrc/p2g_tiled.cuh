@@ -1,8 +1,11 @@
 // P2G as a tiled, deterministic scatter (the tolerance-mode path; the reference-order gather of
-// binning.cuh stays the parity path). Same results as particles.cl:135-227 up to the order in which
-// each cell's weighted sums are added: every weight is computed exactly as the reference computes
-// it, the fluid fraction (an integer count) is identical, and a face that no particle weighs is 0 in
-// both.
+// binning.cuh stays the parity path). Same results as particles.cl:135-227 up to the order and
+// rounding with which each cell's weighted sums are added: every weight is computed exactly as the
+// reference computes it, the fluid fraction (an integer count) is identical, and a face that no
+// particle weighs is 0 in both.
+//
+// The weights are the reference's, rounded as it rounds them; each velocity term is added with one
+// fused multiply-add (one rounding instead of two).
 //
 // Why: the reference visits each particle from the 27 cells around its bin (27 tent evaluations per
 // particle per face type). Here each particle is visited once. A particle in bin b (b = floor(s -
@@ -109,11 +112,13 @@ __global__ void __launch_bounds__(P2GT_THREADS, 2)
                                 const float gu = fx[a] * hy[b] * hz[c];  // u: (a, b, c) = (x, y, z)
                                 const float gv = hx[b] * fy[a] * hz[c];  // v: (b, a, c)
                                 const float gw = hx[b] * hy[c] * fz[a];  // w: (b, c, a)
-                                vu[t] += gu * v0;
+                                // the velocity sums as one fused multiply-add per term (this kernel is
+                                // the tolerance mode's: its sums already differ from the reference's order)
+                                vu[t] = __fmaf_rn(gu, v0, vu[t]);
                                 wu[t] += gu;
-                                vv[t] += gv * v1;
+                                vv[t] = __fmaf_rn(gv, v1, vv[t]);
                                 wv[t] += gv;
-                                vw[t] += gw * v2;
+                                vw[t] = __fmaf_rn(gw, v2, vw[t]);
                                 ww[t] += gw;
                             }
                     // the particle's cell for the fluid fraction (b or b + 1 on each axis): integer adds

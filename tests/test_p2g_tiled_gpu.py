@@ -1,7 +1,7 @@
 """The tiled P2G (each particle visited once, the tolerance-mode path) against the reference-order
 gather and the oracle: the fluid fraction bit for bit, the face velocities within 1e-5 of the field's
-largest magnitude (only the order of each cell's sums differs, so a sum that cancels can come out as
-an exact 0 in one order and a tiny value in the other), the same bits on every run; at 64^3 and at
+largest magnitude (only the order and rounding of each cell's sums differ, so a sum that cancels can
+come out as an exact 0 in one order and a tiny value in the other), the same bits on every run; at 64^3 and at
 the 256^3 block of the benchmark."""
 
 from __future__ import annotations
