@@ -41,6 +41,7 @@ UNIT = "steps/s"
 TOL = 1e-6
 COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarsest-level iterations
 SMOOTHING_CHOICES = ((2, 4), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
+SINGLE_VISIT_CHOICES = (0, 3, 2)  # first level visited once per parent visit; 0: the reference's W-cycle
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
                      "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
@@ -79,6 +80,11 @@ def parse_args():
                     help="red-black iterations before,after the coarse-grid correction in the W-cycle preconditioner "
                          "of the timed steps, e.g. 2,4 (auto: the fastest of 2,4 (the reference's), 1,2 and 1,1 to the "
                          "tolerance in the Poisson comparison, with 4 coarsest-level iterations)")
+    ap.add_argument("--single-visit", default="auto",
+                    help="first multigrid level visited once (not twice) per visit of the level above in the W-cycle "
+                         "preconditioner of the timed steps; 0 = the reference's W-cycle (auto: the fastest of 0, 3 "
+                         "and 2 in the Poisson comparison, with 4 coarsest-level iterations and one smoothing sweep "
+                         "each way)")
     ap.add_argument("--case", choices=["step", "sweep0", "wcycle", "batch", "unet", "collider", "particles"],
                     default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
@@ -331,6 +337,7 @@ def sweep_case(args):
     ps.rhs.copy_(torch.randn(scene.grid_shape, device="cuda", generator=gen) * ff)
     h = ps.hierarchy
     tune_hierarchy(h, ps.correction, ps.residual)
+    kernels.call("clb_mg_set_option", 4, 0 if args.single_visit == "auto" else int(args.single_visit))
     if args.fused_level0:
         h.set_sweep(0, 7)  # level 0 of the W-cycle as the fused tile launches of csrc/mg_level0.cuh
     p = torch.zeros_like(zero)
@@ -417,12 +424,13 @@ def workload_config(size, n_particles, args):
     }
 
 
-def solver_description(method, pre, post, k, fp16_levels=None):
+def solver_description(method, pre, post, k, fp16_levels=None, single_from=0):
     storage = f", levels {fp16_levels[0][0]}^3 and coarser stored in FP16" if fp16_levels else ""
+    cycle = "W-cycle" if not single_from else f"W-cycle (levels {single_from}+ visited once per parent visit)"
     if method == "fcg":
-        return (f"flexible CG preconditioned by one W-cycle computed in FP32 (pre {pre}, post {post}, coarse "
+        return (f"flexible CG preconditioned by one {cycle} computed in FP32 (pre {pre}, post {post}, coarse "
                 f"{pre}+{k}{storage}), FP64 pressure, residual and norms")
-    return (f"W-cycle computed in FP32 (pre {pre}, post {post}, coarse {pre}+{k}{storage}) in FP64 iterative "
+    return (f"{cycle} computed in FP32 (pre {pre}, post {post}, coarse {pre}+{k}{storage}) in FP64 iterative "
             f"refinement")
 
 
@@ -753,6 +761,14 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             solvers[f"fcg{'_fp16' if fp16 else ''}_c4_s{pre}{post}"] = PressureSolver(
                 kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16, coarse_iterations=4,
                 pre_smooth=pre, post_smooth=post)
+    # one visit instead of two of every level from l on (clb_mg_set_option 4), with the settings above
+    single = {}
+    for level in SINGLE_VISIT_CHOICES[1:]:
+        for fp16 in (False, True):
+            name = f"fcg{'_fp16' if fp16 else ''}_c4_s11_v{level}"
+            single[name] = level
+            solvers[name] = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg",
+                                           coarse_fp16=fp16, coarse_iterations=4, pre_smooth=1, post_smooth=1)
     p_tmp = torch.empty_like(sim.pressure)
     rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": [], "fcg_tuned_learned": []}
     rows.update({name: [] for name in solvers if "_c" in name})
@@ -769,9 +785,11 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             # 4 coarsest-level iterations, one smoothing sweep each way): the comparison that decides
             variants.append(("fcg_tuned_learned", solvers["fcg_fp16_c4_s11"], warm))
         for name, ps, ws in variants:
+            kernels.call("clb_mg_set_option", 4, single.get(name, 0))
             for rep in range(2):  # the first run captures graphs and tunes; the second is timed
                 p_tmp.copy_(saved)
                 st = ps.solve(vel, sim.fluid_fraction, p_tmp, sim.dt, rho, tol=TOL, warm_start=ws, solid=sim.obstacle)
+            kernels.call("clb_mg_set_option", 4, 0)
             rows[name].append({"ms": st.device_ms(), "cycles": st.cycles, "rel": st.rel_residual,
                                "guess": st.warm_start, "learned_rel": st.learned_rel_residual,
                                "initial_rel": st.initial_rel_residual,
@@ -852,6 +870,16 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             if r and r["ms_mean"] < best_ms:
                 best_s, best_ms = (pre, post), r["ms_mean"]
     out["smoothing_chosen"] = list(best_s)
+    # the rule for single visits (with 4 coarsest-level iterations and one smoothing sweep each way
+    # chosen): the fastest to the tolerance
+    best_v = 0
+    if best_k == 4 and tuple(best_s) == (1, 1):
+        best_ms = out[f"{base}_c4_s11"]["ms_mean"]
+        for level in SINGLE_VISIT_CHOICES[1:]:
+            r = out.get(f"{base}_c4_s11_v{level}")
+            if r and r["ms_mean"] < best_ms:
+                best_v, best_ms = level, r["ms_mean"]
+    out["single_visit_from_chosen"] = best_v
     if rows["fcg_learned"]:
         out["speedup_learned_vs_plain_fcg"] = out["fcg"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
         out["speedup_learned_vs_refine"] = out["refine"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
@@ -902,6 +930,7 @@ def our_arm(args):
     use_learned = args.learned == "on"
     coarse_k = COARSE_ITERATION_CHOICES[0] if args.coarse_iterations == "auto" else int(args.coarse_iterations)
     smoothing = SMOOTHING_CHOICES[0] if args.smoothing == "auto" else tuple(int(x) for x in args.smoothing.split(","))
+    single_from = 0 if args.single_visit == "auto" else int(args.single_visit)
     if args.poisson_steps > 0:
         poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
         if args.coarse_fp16 == "auto":
@@ -910,6 +939,8 @@ def our_arm(args):
             coarse_k = poisson.get("coarse_iterations_chosen", coarse_k)
         if args.smoothing == "auto":
             smoothing = tuple(poisson.get("smoothing_chosen", smoothing))
+        if args.single_visit == "auto":
+            single_from = poisson.get("single_visit_from_chosen", 0)
         if args.learned == "auto" and "fcg_tuned_learned" in poisson:
             # the rule: the learned guess in the timed steps only when it makes the solve faster,
             # network evaluation included
@@ -919,7 +950,8 @@ def our_arm(args):
     sim.options.warm_start = warm if use_learned else None
     if warm is not None and not use_learned:
         warm_note += " (not used in the timed steps: no faster than without it in the comparison)"
-    if use_fp16 or coarse_k != sim.options.coarse_iterations or \
+    kernels.call("clb_mg_set_option", 4, single_from)  # read when the timed solver captures its graphs
+    if use_fp16 or coarse_k != sim.options.coarse_iterations or single_from or \
             smoothing != (sim.options.pre_smooth, sim.options.post_smooth):
         from continuum_liquid_b200.pressure_solve import PressureSolver
 
@@ -1048,7 +1080,7 @@ def our_arm(args):
         config = workload_config(args.size, n, args)
         fp16_levels = [list(s) for s in h.shapes[h.fp16_level:]] if h.fp16_level else None
         solver_info = {"pressure": solver_description(args.method, sim.options.pre_smooth, sim.options.post_smooth,
-                                                      sim.options.coarse_iterations, fp16_levels),
+                                                      sim.options.coarse_iterations, fp16_levels, single_from),
                        "p2g": "tiled scatter (k_p2g_tiled)" if sim.options.tiled_p2g() else
                               "reference-order gather (k_p2g_gather)",
                        "multigrid_levels": [list(s) for s in h.shapes], "sweep_kinds": h.sweeps(),

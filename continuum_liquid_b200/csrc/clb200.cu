@@ -34,6 +34,10 @@ static const int kAbiVersion = 8;
 static const size_t kBottomSmemLimit = 220 * 1024;
 static bool g_use_bottom = true;  // clb_mg_set_option(0, ...) switches the single-block bottom visit off
 static bool g_use_cluster = true;  // clb_mg_set_option(2, ...) switches the cluster visit off
+static int g_single_from = 0;      // clb_mg_set_option(4, l): levels >= l (> 0) are visited once per parent visit
+
+// Visits of `level` per visit of the level above: the reference's two, or one from the single-visit level on.
+static inline int visits_of(int level) { return g_single_from > 0 && level >= g_single_from ? 1 : 2; }
 static bool g_skip_air = true;     // clb_mg_set_option(3, ...): refinement/FCG steps skip cells without fluid
 
 template <bool L0, bool H, int TI, int TJ, int T>
@@ -990,7 +994,8 @@ static int launch_cluster_visit(const clb_mg_hierarchy* h, int level, int csize,
                              (const uint8_t*)h->mask[level], c[0], c[1], c[2], h->p[level + 1],
                              (const float4*)h->op[level + 1], (const uint8_t*)h->mask[level + 1], a[0], a[1], a[2],
                              (const float4*)h->op[level + 2], (const uint8_t*)h->mask[level + 2], b[0], b[1], b[2],
-                             h->delta, pre, post, coarse_iters, (const float*)h->fp16_scale, visits);
+                             h->delta, pre, post, coarse_iters, (const float*)h->fp16_scale, visits,
+                             visits_of(level + 1), visits_of(level + 2));
     return check_launch("k_cluster_visit") ? -1 : 1;
 }
 }  // extern "C++"
@@ -1052,7 +1057,7 @@ int bottom_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int co
     launch(1, BOTTOM_THREADS, bytes, s)(k_bottom_visit<KA, KB, H>,                                                    \
         h->p[level], h->b[level], (const float4*)h->op[level], h->mask[level], a[0], a[1], a[2], h->p[level + 1],      \
         h->b[level + 1], (const float4*)h->op[level + 1], h->mask[level + 1], b[0], b[1], b[2], h->delta, pre,         \
-                                        post, coarse_iters, h->fp16_scale)
+                                        post, coarse_iters, h->fp16_scale, visits_of(level + 1))
 #define CLB_BOTTOM_KINDS(H)                                 \
     if (ka <= 1 && kb <= 1) CLB_BOTTOM(1, 1, H);            \
     else if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1, H);       \
@@ -1137,12 +1142,12 @@ int w_cycle_level0_fused(const clb_mg_hierarchy* h, float* x, const float* rhs, 
         src = buf[dst];
         dst ^= 1;
     }
-    const int both = cluster_visit(h, 1, pre, post, coarse_iters, s, 2);
+    const int visits = visits_of(1);
+    const int both = cluster_visit(h, 1, pre, post, coarse_iters, s, visits);
     if (both < 0) return 1;
-    if (both == 0) {
-        if (w_cycle(h, 1, x, rhs, pre, post, coarse_iters, s)) return 1;
-        if (w_cycle(h, 1, x, rhs, pre, post, coarse_iters, s)) return 1;
-    }
+    if (both == 0)
+        for (int v2 = 0; v2 < visits; ++v2)
+            if (w_cycle(h, 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     for (int it = 0; it < post; ++it) {
         if (it == 0) launch_l0_iter<L0F_PROLONG>(h, src, buf[dst], rhs, s);
         else launch_l0_iter<0>(h, src, buf[dst], rhs, s);
@@ -1199,13 +1204,14 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
                                                const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz,
                                                c.nx, c.ny, c.nz);
     CLB_LAUNCH_CHECK("k_restrict");
-    // the two visits of the level below: one cluster launch for both when it takes the cluster path
-    const int both = cluster_visit(h, level + 1, pre, post, coarse_iters, s, 2);
+    // the visits of the level below (two, or one from the single-visit level on): one cluster launch
+    // for them when it takes the cluster path
+    const int visits = visits_of(level + 1);
+    const int both = cluster_visit(h, level + 1, pre, post, coarse_iters, s, visits);
     if (both < 0) return 1;
-    if (both == 0) {
-        if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
-        if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
-    }
+    if (both == 0)
+        for (int v2 = 0; v2 < visits; ++v2)
+            if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     const i64 Cf = (i64)v.nx * v.ny * v.nz;
     const int fvec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
     if (!c.half && !v.half && v.tiles) {  // prolongation into the fine fluid tiles
@@ -1289,11 +1295,13 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
 }
 
 int clb_mg_set_option(int option, int value) {
-    CLB_REQUIRE(option >= 0 && option <= 3, "mg_set_option: unknown option %d", option);
+    CLB_REQUIRE(option >= 0 && option <= 4, "mg_set_option: unknown option %d", option);
+    CLB_REQUIRE(option != 4 || value >= 0, "mg_set_option: negative single-visit level");
     if (option == 0) g_use_bottom = value != 0;
     else if (option == 1) g_use_pdl = value != 0;
     else if (option == 2) g_use_cluster = value != 0;
-    else g_skip_air = value != 0;
+    else if (option == 3) g_skip_air = value != 0;
+    else g_single_from = value;
     return 0;
 }
 

@@ -210,7 +210,7 @@ __device__ __forceinline__ void bottom_stage(const BottomSmem& S, const float* _
 template <int KA, int KB, bool H>
 __device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int any, int anz, int bnx, int bny, int bnz,
                                             float d2, float inv_delta2, int pre, int post, int coarse_iters,
-                                            float* __restrict__ bb) {
+                                            float* __restrict__ bb, int b_solves = 2) {
     float* spa = S.spa;
     const float* sba = S.sba;
     const float4* soa = S.soa;
@@ -332,8 +332,9 @@ __device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int an
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) spb[c] = 0.0f;  // multigrid.cl:114
     __syncthreads();
     if (btile) {
-        // two coarse solves of the W (multigrid.py:127-170), pre + coarse_iters iterations each
-        const int iterations = 2 * (pre + coarse_iters);
+        // two coarse solves of the W (multigrid.py:127-170; b_solves: one when the coarsest level is
+        // visited once), pre + coarse_iters iterations each
+        const int iterations = b_solves * (pre + coarse_iters);
         for (int it = 0; it < iterations; ++it)
 #pragma unroll
             for (int colour = 0; colour < 2; ++colour) {
@@ -376,7 +377,7 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
                                                    float* __restrict__ bb, const float4* __restrict__ opb,
                                                    const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
                                                    float delta, int pre, int post, int coarse_iters,
-                                                   const float* __restrict__ scale) {
+                                                   const float* __restrict__ scale, int b_solves = 2) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     const BottomSmem S = bottom_smem(smem, CA, CB);
@@ -388,7 +389,7 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
     };
     bottom_stage<H>(S, pa, ba, opa, ma, CA, opb, mb, CB);
     bottom_lists(S, anx, any, anz, bnx, bny, bnz);
-    bottom_core<KA, KB, H>(S, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, bb);
+    bottom_core<KA, KB, H>(S, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, bb, b_solves);
     const int bsx = bny * bnz, bsy = bnz;
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) st(pa, c, S.spa[c]);
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
@@ -405,10 +406,10 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
                    const uint8_t* __restrict__ ma, int anx, int any, int anz, float* __restrict__ pb,
                    float* __restrict__ bb, const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx,
                    int bny, int bnz, float delta, int pre, int post, int coarse_iters,
-                   const float* __restrict__ scale = nullptr) {
+                   const float* __restrict__ scale = nullptr, int b_solves = 2) {
     pdl_begin();
     bottom_visit_block<KA, KB, H>(pa, ba, opa, ma, anx, any, anz, pb, bb, opb, mb, bnx, bny, bnz, delta, pre, post,
-                                  coarse_iters, scale);
+                                  coarse_iters, scale, b_solves);
 }
 
 }  // namespace clb

@@ -1,6 +1,8 @@
 // One visit of the third-coarsest level C = L-3 together with both visits of the level below it
 // (its two bottom visits, mg_bottom.cuh), as one launch of a thread-block cluster; or the two visits
-// of C that the level above makes back to back, in one launch (`visits` = 2).
+// of C that the level above makes back to back, in one launch (`visits` = 2). `a_visits` and
+// `b_solves` (2 in the reference's W-cycle, 1 for a level visited once per parent visit) are the
+// visits of A per visit of C and the coarse solves of B per visit of A.
 //
 // A W-cycle visits C 2^(L-3) times, and each visit (multigrid.py:53-187) is pre-smoothing of C,
 // restriction to A = C+1, two visits of A (each: smoothing, restriction to B, two coarse solves,
@@ -269,7 +271,7 @@ __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __rest
                                     const uint8_t* __restrict__ ma, int anx, int any, int anz,
                                     const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny,
                                     int bnz, float d2, float inv_delta2, int pre, int post, int coarse_iters,
-                                    int visits) {
+                                    int visits, int a_visits, int b_solves) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     const BottomSmem S = bottom_smem(smem, CA, CB);
@@ -283,8 +285,9 @@ __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __rest
     cluster_barrier();  // staged (for a later visit of C: the slabs finished reading A's p)
     for (int it = 0; it < 2 * pre; ++it) cluster_barrier();  // the C-level pre-smoothing phases
     cluster_barrier();  // A's right-hand side is complete
-    for (int visit = 0; visit < 2; ++visit) {
-        bottom_core<KA, KB, H>(S, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, nullptr);
+    for (int visit = 0; visit < a_visits; ++visit) {  // two, or one when A is visited once
+        bottom_core<KA, KB, H>(S, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, nullptr,
+                               b_solves);
         __syncthreads();
         if (H)  // A's p as the bottom visit stores it (FP16) before it is read again
             for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) S.spa[c] = __half2float(__float2half_rn(S.spa[c]));
@@ -308,7 +311,7 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
                     const float4* __restrict__ opa, const uint8_t* __restrict__ ma, int anx, int any, int anz,
                     const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
                     float delta, int pre, int post, int coarse_iters, const float* __restrict__ scale,
-                    int visits) {
+                    int visits, int a_visits, int b_solves) {
     pdl_begin();
     const float d2 = H ? scale[2] : delta * delta;
     const float inv_delta2 = H ? scale[3] : 1.0f / (delta * delta);
@@ -316,7 +319,7 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
     const int cs = (int)cooperative_groups::this_cluster().num_blocks() - 1;
     if (rank == 0)
         cluster_bottom_path<KA, KB, H>(pa, opa, ma, anx, any, anz, opb, mb, bnx, bny, bnz, d2, inv_delta2, pre, post,
-                                       coarse_iters, visits);
+                                       coarse_iters, visits, a_visits, b_solves);
     else
         cluster_slab_path<NS, H>((int)rank - 1, cs, pc, pc, bc, opc, mc, nx, ny, nz, anx, any, anz, d2, inv_delta2,
                                  pre, post, visits);

@@ -350,7 +350,12 @@ int clb_mg_smooth(const clb_mg_hierarchy* h, int level, float* x, const float* r
  *            interior fluid cells (neither read nor written); the caller keeps p64_out, d_out and
  *            r_out at 0 there (zero them once per solve: clb_mg_ir_init and clb_mg_residual_norms
  *            with r_out do so for their outputs). 0 writes every cell. Identical results when the
- *            caller keeps that invariant. */
+ *            caller keeps that invariant.
+ *  option 4: l > 0 makes clb_mg_w_cycle visit every level from l on once per visit of the level above
+ *            (a V-cycle below level l - 1; the coarsest level then gets one coarse solve per visit of
+ *            the level above), on every path (level by level, bottom and cluster launches); 0 (default)
+ *            keeps the reference's two visits. A different preconditioner for the tolerance mode:
+ *            values change. Read when a W-cycle is enqueued (and so fixed in a captured graph). */
 int clb_mg_set_option(int option, int value);
 
 /* Block-partial count used by clb_mg_residual_norms for a grid of `cells` cells. */

@@ -956,8 +956,10 @@ struct Levels {
 };
 
 // multigrid.py:53-187 w_cycle (recursive). Level 0 is the fine grid; level count-1 is the coarsest.
+// single_from > 0 (no counterpart in the reference): levels from single_from on are visited once per
+// visit of the level above instead of twice (the solver's clb_mg_set_option 4).
 template <typename T>
-void w_cycle(const Levels<T>& L, int level, T delta, int pre, int post, int coarse_iters) {
+void w_cycle(const Levels<T>& L, int level, T delta, int pre, int post, int coarse_iters, int single_from = 0) {
     const int* s = L.shape + 3 * level;
     if (level == L.count - 1) {
         coarse_smooth<T>(L.p[level], L.b[level], L.m[level], L.d[level], L.wx[level], L.wy[level], L.wz[level], delta,
@@ -973,8 +975,8 @@ void w_cycle(const Levels<T>& L, int level, T delta, int pre, int post, int coar
     restrict_residual<T>(L.p[level], L.b[level], L.m[level], L.d[level], L.wx[level], L.wy[level], L.wz[level], L.p[c],
                          L.b[c], L.m[c], L.d[c], L.wx[c], L.wy[c], L.wz[c], delta, s[0], s[1], s[2], cs[0], cs[1],
                          cs[2]);
-    w_cycle<T>(L, c, delta, pre, post, coarse_iters);
-    w_cycle<T>(L, c, delta, pre, post, coarse_iters);
+    const int visits = single_from > 0 && c >= single_from ? 1 : 2;
+    for (int v = 0; v < visits; ++v) w_cycle<T>(L, c, delta, pre, post, coarse_iters, single_from);
     prolongate<T>(L.p[c], L.p[level], L.m[level], cs[0], cs[1], cs[2], s[0], s[1], s[2]);
     for (int it = 0; it < post; ++it)
         for (int parity = 0; parity < 2; ++parity)
@@ -1035,14 +1037,14 @@ void orc_coarse_smooth_f32(float* p, const float* b, const float* m, const float
 
 // W-cycle over a level list whose arrays are given as pointer tables (level 0 = finest).
 void orc_w_cycle_f32(float** p, float** b, float** m, float** d, float** wx, float** wy, float** wz, const int* shapes,
-                     int levels, float delta, int pre, int post, int coarse_iters) {
+                     int levels, float delta, int pre, int post, int coarse_iters, int single_from) {
     Levels<float> L{p, b, m, d, wx, wy, wz, shapes, levels};
-    w_cycle<float>(L, 0, delta, pre, post, coarse_iters);
+    w_cycle<float>(L, 0, delta, pre, post, coarse_iters, single_from);
 }
 void orc_w_cycle_f64(double** p, double** b, double** m, double** d, double** wx, double** wy, double** wz,
-                     const int* shapes, int levels, double delta, int pre, int post, int coarse_iters) {
+                     const int* shapes, int levels, double delta, int pre, int post, int coarse_iters, int single_from) {
     Levels<double> L{p, b, m, d, wx, wy, wz, shapes, levels};
-    w_cycle<double>(L, 0, delta, pre, post, coarse_iters);
+    w_cycle<double>(L, 0, delta, pre, post, coarse_iters, single_from);
 }
 void orc_residual_norms_f32(const float* p, const float* b, const float* m, const float* d, const float* wx,
                             const float* wy, const float* wz, float delta, int nx, int ny, int nz, double* rr,

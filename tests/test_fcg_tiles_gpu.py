@@ -58,6 +58,11 @@ def test_tile_step_and_dots_match_rows(backend, shape):
     p_in = field(3.0, np.float64)
     state = torch.tensor([0.7, -0.3, 5.0, 1.0], dtype=torch.float64, device="cuda")
 
+    # the scalars the steps use: the row dots' (each path's own dots differ in the last bits)
+    common = state.clone()
+    part4 = torch.zeros(4 * blocks, dtype=torch.float64, device="cuda")
+    backend.call("clb_mg_fcg_dots", z, d, r, h.op0, delta, *shape, part4, common)
+
     def outputs(tiles: bool):
         p_out = torch.zeros(shape, dtype=torch.float64, device="cuda")
         d_out = torch.zeros(shape, dtype=torch.float32, device="cuda")
@@ -68,10 +73,12 @@ def test_tile_step_and_dots_match_rows(backend, shape):
         st = state.clone()
         if tiles:
             backend.call_hierarchy("clb_mg_fcg_dots_tiles", h.struct, z, d, r, part4, st)
-            backend.call_hierarchy("clb_mg_fcg_step_tiles", h.struct, p_in, z, d, p_out, d_out, st, rhs, r_out, part, out)
+            backend.call_hierarchy("clb_mg_fcg_step_tiles", h.struct, p_in, z, d, p_out, d_out, common, rhs, r_out,
+                                   part, out)
         else:
             backend.call("clb_mg_fcg_dots", z, d, r, h.op0, delta, *shape, part4, st)
-            backend.call("clb_mg_fcg_step", p_in, z, d, p_out, d_out, st, rhs, h.op0, delta, *shape, r_out, part, out)
+            backend.call("clb_mg_fcg_step", p_in, z, d, p_out, d_out, common, rhs, h.op0, delta, *shape, r_out, part,
+                         out)
         ir_out = torch.zeros(shape, dtype=torch.float64, device="cuda")
         ir_r = torch.zeros(shape, dtype=torch.float32, device="cuda")
         ir_norms = torch.zeros(2, dtype=torch.float64, device="cuda")

@@ -424,3 +424,28 @@ def test_fcg_with_fewer_coarse_iterations(oracle):
     _, hist4 = oracle.fcg_solve(b, mask, shape, dx, tol=1e-8, max_cycles=60, coarse_iterations=4)
     assert hist4[-1] <= 1e-8
     assert len(hist4) <= len(hist64) + 3
+
+
+def test_single_visit_levels(oracle):
+    """The single-visit variant of the W-cycle: from a level past the coarsest it is the reference's
+    W-cycle; from the coarsest it runs one coarse solve per visit of the level above, which is the
+    reference W-cycle with half the coarsest-level iterations there when pre-smoothing is 0."""
+    shape = (34, 30, 38)
+    rng = np.random.default_rng(11)
+    ff = np.zeros(shape, np.float32)
+    ff[1:-1, 1:20, 1:-1] = 1.0
+    ff[rng.random(shape) < 0.05] = 0
+    b = (rng.standard_normal(shape) * (ff > 0)).astype(np.float32)
+    dx = np.float32(1.0 / 34)
+    ops = oracle.build_finest_operator(ff, shape)
+    levels = oracle.Levels(shape)
+    n = len(levels.shapes)
+    results = {}
+    for single in (0, n, n - 1):
+        q = np.zeros(shape, np.float32)
+        oracle.Levels(shape).w_cycle(q, b, ff, ops, dx, pre=0, post=2, coarse=8, single_from=single)
+        results[single] = q
+    assert np.array_equal(results[0], results[n])
+    q = np.zeros(shape, np.float32)
+    oracle.Levels(shape).w_cycle(q, b, ff, ops, dx, pre=0, post=2, coarse=4)
+    assert np.array_equal(results[n - 1], q)
