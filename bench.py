@@ -41,7 +41,6 @@ UNIT = "steps/s"
 TOL = 1e-6
 COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarsest-level iterations
 SMOOTHING_CHOICES = ((2, 4), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
-SINGLE_VISIT_CHOICES = (0, 3, 2)  # first level visited once per parent visit; 0: the reference's W-cycle
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
                      "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
@@ -80,11 +79,10 @@ def parse_args():
                     help="red-black iterations before,after the coarse-grid correction in the W-cycle preconditioner "
                          "of the timed steps, e.g. 2,4 (auto: the fastest of 2,4 (the reference's), 1,2 and 1,1 to the "
                          "tolerance in the Poisson comparison, with 4 coarsest-level iterations)")
-    ap.add_argument("--single-visit", default="auto",
+    ap.add_argument("--single-visit", type=int, default=0,
                     help="first multigrid level visited once (not twice) per visit of the level above in the W-cycle "
-                         "preconditioner of the timed steps; 0 = the reference's W-cycle (auto: the fastest of 0, 3 "
-                         "and 2 in the Poisson comparison, with 4 coarsest-level iterations and one smoothing sweep "
-                         "each way)")
+                         "preconditioner (0 = the reference's W-cycle; at 256^3 levels 3 and 2 need 20 and 27 FCG "
+                         "cycles against 13)")
     ap.add_argument("--case", choices=["step", "sweep0", "wcycle", "batch", "unet", "collider", "particles"],
                     default="step",
                     help="step: the benchmark; sweep0: only level-0 red-black sweeps on the scene's pressure system "
@@ -337,7 +335,7 @@ def sweep_case(args):
     ps.rhs.copy_(torch.randn(scene.grid_shape, device="cuda", generator=gen) * ff)
     h = ps.hierarchy
     tune_hierarchy(h, ps.correction, ps.residual)
-    kernels.call("clb_mg_set_option", 4, 0 if args.single_visit == "auto" else int(args.single_visit))
+    kernels.call("clb_mg_set_option", 4, args.single_visit)
     if args.fused_level0:
         h.set_sweep(0, 7)  # level 0 of the W-cycle as the fused tile launches of csrc/mg_level0.cuh
     p = torch.zeros_like(zero)
@@ -761,14 +759,7 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             solvers[f"fcg{'_fp16' if fp16 else ''}_c4_s{pre}{post}"] = PressureSolver(
                 kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16, coarse_iterations=4,
                 pre_smooth=pre, post_smooth=post)
-    # one visit instead of two of every level from l on (clb_mg_set_option 4), with the settings above
-    single = {}
-    for level in SINGLE_VISIT_CHOICES[1:]:
-        for fp16 in (False, True):
-            name = f"fcg{'_fp16' if fp16 else ''}_c4_s11_v{level}"
-            single[name] = level
-            solvers[name] = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg",
-                                           coarse_fp16=fp16, coarse_iterations=4, pre_smooth=1, post_smooth=1)
+    single = {}  # variant name -> first level visited once (clb_mg_set_option 4); none by default
     p_tmp = torch.empty_like(sim.pressure)
     rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": [], "fcg_tuned_learned": []}
     rows.update({name: [] for name in solvers if "_c" in name})
@@ -870,16 +861,6 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             if r and r["ms_mean"] < best_ms:
                 best_s, best_ms = (pre, post), r["ms_mean"]
     out["smoothing_chosen"] = list(best_s)
-    # the rule for single visits (with 4 coarsest-level iterations and one smoothing sweep each way
-    # chosen): the fastest to the tolerance
-    best_v = 0
-    if best_k == 4 and tuple(best_s) == (1, 1):
-        best_ms = out[f"{base}_c4_s11"]["ms_mean"]
-        for level in SINGLE_VISIT_CHOICES[1:]:
-            r = out.get(f"{base}_c4_s11_v{level}")
-            if r and r["ms_mean"] < best_ms:
-                best_v, best_ms = level, r["ms_mean"]
-    out["single_visit_from_chosen"] = best_v
     if rows["fcg_learned"]:
         out["speedup_learned_vs_plain_fcg"] = out["fcg"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
         out["speedup_learned_vs_refine"] = out["refine"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
@@ -930,7 +911,7 @@ def our_arm(args):
     use_learned = args.learned == "on"
     coarse_k = COARSE_ITERATION_CHOICES[0] if args.coarse_iterations == "auto" else int(args.coarse_iterations)
     smoothing = SMOOTHING_CHOICES[0] if args.smoothing == "auto" else tuple(int(x) for x in args.smoothing.split(","))
-    single_from = 0 if args.single_visit == "auto" else int(args.single_visit)
+    single_from = int(args.single_visit)
     if args.poisson_steps > 0:
         poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
         if args.coarse_fp16 == "auto":
@@ -939,8 +920,6 @@ def our_arm(args):
             coarse_k = poisson.get("coarse_iterations_chosen", coarse_k)
         if args.smoothing == "auto":
             smoothing = tuple(poisson.get("smoothing_chosen", smoothing))
-        if args.single_visit == "auto":
-            single_from = poisson.get("single_visit_from_chosen", 0)
         if args.learned == "auto" and "fcg_tuned_learned" in poisson:
             # the rule: the learned guess in the timed steps only when it makes the solve faster,
             # network evaluation included

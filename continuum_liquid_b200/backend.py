@@ -90,9 +90,6 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_w_cycle": [P, P, P, I, I, I, P],
     "clb_mg_smooth": [P, I, P, P, I, P],
     "clb_mg_level0_iteration": [P, P, P, P, I, P],
-    "clb_mg_ir_step_tiles": [P, P, P, P, P, P, P, P, P],
-    "clb_mg_fcg_dots_tiles": [P, P, P, P, P, P, P],
-    "clb_mg_fcg_step_tiles": [P, P, P, P, P, P, P, P, P, P, P, P],
     "clb_mg_set_option": [I, I],
     "clb_mg_residual_partials": [L],
     "clb_mg_tile_capacity": [I, I, I, I],

@@ -12,7 +12,6 @@
 #include "mg_cluster.cuh"
 #include "mg_tiles.cuh"
 #include "mg_level0.cuh"
-#include "mg_fcg_tiles.cuh"
 #include "batch.cuh"
 #include "sources.cuh"
 #include "voxelise.cuh"
@@ -715,11 +714,10 @@ int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream) {
             const int* n = h->shape[l];
             const i64 tiles = tile_capacity(n[0], n[1], n[2], l == 0);
             const unsigned grid = blocks_for(tiles * 32, 256);
-            if (l == 0) {  // ascending order: flags, then one block compacts them
-                launch(grid, 256, 0, s)(k_mg_tile_flags0, (const uint8_t*)h->op0, n[0], n[1], n[2], h->tiles[l]);
-                CLB_LAUNCH_CHECK("k_mg_tile_flags0");
-                launch(1, COMPACT_THREADS, 0, s)(k_compact_tiles, h->tiles[l], (int)tiles, h->tile_counts + l);
-            } else
+            if (l == 0)
+                launch(grid, 256, 0, s)(k_mg_tiles<true>, (const uint8_t*)h->op0, n[0], n[1], n[2], h->tiles[l],
+                                        h->tile_counts + l);
+            else
                 launch(grid, 256, 0, s)(k_mg_tiles<false>, (const uint8_t*)h->mask[l], n[0], n[1], n[2], h->tiles[l],
                                         h->tile_counts + l);
             CLB_LAUNCH_CHECK("k_mg_tiles");
@@ -1415,120 +1413,6 @@ int clb_mg_fcg_step(const double* p64_in, const float* z, const float* d_in, dou
                                          inv_delta2, nx, ny, nz, r_out, (double2*)partials, d_in, d_out, state);
     }
     CLB_LAUNCH_CHECK("k_residual_rows");
-    launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
-    CLB_LAUNCH_CHECK("k_reduce_partials");
-    return 0;
-}
-
-extern "C++" {
-namespace {
-// Grid of the tile kernels of mg_fcg_tiles.cuh: the resident blocks, at most the partials the caller
-// holds (clb_mg_residual_partials) and the tiles there can be.
-template <auto KERNEL>
-int fcg_tile_grid(i64 cells, i64 tiles) {
-    static const int per_sm = [] {
-        int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, KERNEL, FT_THREADS, 0) != cudaSuccess) {
-            (void)cudaGetLastError();
-            n = 0;
-        }
-        return n > 0 ? n : 1;
-    }();
-    i64 g = (i64)per_sm * (g_sm_count > 0 ? g_sm_count : 148);
-    const i64 cap = clb_mg_residual_partials(cells);
-    if (g > cap) g = cap;
-    if (g > tiles) g = tiles;
-    return (int)(g > 0 ? g : 1);
-}
-
-bool fcg_tiles_ok(const clb_mg_hierarchy* h) { return g_skip_air && h->tiles[0] && h->tile_counts; }
-}  // namespace
-}  // extern "C++"
-
-int clb_mg_ir_step_tiles(const clb_mg_hierarchy* h, const double* p64_in, const float* e, double* p64_out,
-                         const float* b, float* r_out, void* partials, double* out, void* stream) {
-    if (check_hierarchy(h)) return 1;
-    const int* n = h->shape[0];
-    if (!fcg_tiles_ok(h))
-        return clb_mg_ir_step(p64_in, e, p64_out, b, h->op0, h->delta, n[0], n[1], n[2], r_out, partials, out, stream);
-    CLB_REQUIRE(p64_in && e && p64_out && b && r_out && partials && out, "mg_ir_step_tiles: null pointer");
-    CLB_REQUIRE(p64_in != p64_out, "mg_ir_step_tiles: p64_out must not alias p64_in");
-    const i64 C = (i64)n[0] * n[1] * n[2];
-    const double inv_delta2 = 1.0 / ((double)h->delta * (double)h->delta);
-    cudaStream_t s = CLB_STREAM(stream);
-    const i64 tiles = tile_capacity(n[0], n[1], n[2], true);
-    int blocks;
-    if (tile_k(n[2], true) == 128) {
-        blocks = fcg_tile_grid<k_step_tiles<RES_IR, 128>>(C, tiles);
-        launch(blocks, FT_THREADS, 0, s)(k_step_tiles<RES_IR, 128>, h->tiles[0], h->tile_counts, p64_in, e, p64_out, b,
-                                         h->op0, inv_delta2, n[0], n[1], n[2], r_out, (double2*)partials, nullptr,
-                                         nullptr, nullptr);
-    } else {
-        blocks = fcg_tile_grid<k_step_tiles<RES_IR, 32>>(C, tiles);
-        launch(blocks, FT_THREADS, 0, s)(k_step_tiles<RES_IR, 32>, h->tiles[0], h->tile_counts, p64_in, e, p64_out, b,
-                                         h->op0, inv_delta2, n[0], n[1], n[2], r_out, (double2*)partials, nullptr,
-                                         nullptr, nullptr);
-    }
-    CLB_LAUNCH_CHECK("k_step_tiles");
-    launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
-    CLB_LAUNCH_CHECK("k_reduce_partials");
-    return 0;
-}
-
-int clb_mg_fcg_dots_tiles(const clb_mg_hierarchy* h, const float* z, const float* d, const float* r, void* partials4,
-                          double* state, void* stream) {
-    if (check_hierarchy(h)) return 1;
-    const int* n = h->shape[0];
-    if (!fcg_tiles_ok(h)) return clb_mg_fcg_dots(z, d, r, h->op0, h->delta, n[0], n[1], n[2], partials4, state, stream);
-    CLB_REQUIRE(z && d && r && partials4 && state, "mg_fcg_dots_tiles: null pointer");
-    const i64 C = (i64)n[0] * n[1] * n[2];
-    const double inv_delta2 = 1.0 / ((double)h->delta * (double)h->delta);
-    cudaStream_t s = CLB_STREAM(stream);
-    const i64 tiles = tile_capacity(n[0], n[1], n[2], true);
-    int blocks;
-    if (tile_k(n[2], true) == 128) {
-        blocks = fcg_tile_grid<k_fcg_dots_tiles<128>>(C, tiles);
-        launch(blocks, FT_THREADS, 0, s)(k_fcg_dots_tiles<128>, h->tiles[0], h->tile_counts, z, d, r, h->op0, inv_delta2,
-                                         n[0], n[1], n[2], (Sum4*)partials4);
-    } else {
-        blocks = fcg_tile_grid<k_fcg_dots_tiles<32>>(C, tiles);
-        launch(blocks, FT_THREADS, 0, s)(k_fcg_dots_tiles<32>, h->tiles[0], h->tile_counts, z, d, r, h->op0, inv_delta2,
-                                         n[0], n[1], n[2], (Sum4*)partials4);
-    }
-    CLB_LAUNCH_CHECK("k_fcg_dots_tiles");
-    launch(1, 256, 0, s)(k_fcg_scalars, (const Sum4*)partials4, blocks, state);
-    CLB_LAUNCH_CHECK("k_fcg_scalars");
-    return 0;
-}
-
-int clb_mg_fcg_step_tiles(const clb_mg_hierarchy* h, const double* p64_in, const float* z, const float* d_in,
-                          double* p64_out, float* d_out, const double* state, const float* b, float* r_out,
-                          void* partials, double* out, void* stream) {
-    if (check_hierarchy(h)) return 1;
-    const int* n = h->shape[0];
-    if (!fcg_tiles_ok(h))
-        return clb_mg_fcg_step(p64_in, z, d_in, p64_out, d_out, state, b, h->op0, h->delta, n[0], n[1], n[2], r_out,
-                               partials, out, stream);
-    CLB_REQUIRE(p64_in && z && d_in && p64_out && d_out && state && b && r_out && partials && out,
-                "mg_fcg_step_tiles: null pointer");
-    CLB_REQUIRE(p64_in != p64_out && d_in != d_out, "mg_fcg_step_tiles: outputs must not alias inputs");
-    const i64 C = (i64)n[0] * n[1] * n[2];
-    const double inv_delta2 = 1.0 / ((double)h->delta * (double)h->delta);
-    cudaStream_t s = CLB_STREAM(stream);
-    const i64 tiles = tile_capacity(n[0], n[1], n[2], true);
-    int blocks;
-    if (tile_k(n[2], true) == 128) {
-        blocks = fcg_tile_grid<k_step_tiles<RES_FCG, 128>>(C, tiles);
-        launch(blocks, FT_THREADS, 0, s)(k_step_tiles<RES_FCG, 128>, h->tiles[0], h->tile_counts, p64_in, z, p64_out,
-                                         b, h->op0, inv_delta2, n[0], n[1], n[2], r_out, (double2*)partials, d_in,
-                                         d_out, state);
-    } else {
-        blocks = fcg_tile_grid<k_step_tiles<RES_FCG, 32>>(C, tiles);
-        launch(blocks, FT_THREADS, 0, s)(k_step_tiles<RES_FCG, 32>, h->tiles[0], h->tile_counts, p64_in, z, p64_out,
-                                         b, h->op0, inv_delta2, n[0], n[1], n[2], r_out, (double2*)partials, d_in,
-                                         d_out, state);
-    }
-    CLB_LAUNCH_CHECK("k_step_tiles");
     launch(1, 256, 0, s)(k_reduce_partials, (const double2*)partials, blocks, (double2*)out);
     CLB_LAUNCH_CHECK("k_reduce_partials");
     return 0;

@@ -11,9 +11,8 @@
 //
 // A tile is one plane i, four rows j and TK cells along k (TK = 128 on the finest level when
 // nz % 4 == 0, matching the 16-byte-vector colour sweep; 32 otherwise), i.e. exactly one block of the
-// (32, 4)-thread colour sweep. The lists are rebuilt once per solve; the coarse levels' order is
-// arbitrary (tiles are independent within a colour phase), level 0's is ascending (its FP64 sums,
-// mg_fcg_tiles.cuh, follow the list).
+// (32, 4)-thread colour sweep. The lists are rebuilt once per solve; their order is arbitrary (tiles
+// are independent within a colour phase).
 #pragma once
 #include "multigrid.cuh"
 #include "mg_sweep.cuh"
@@ -49,78 +48,6 @@ __global__ void __launch_bounds__(256) k_mg_tiles(const uint8_t* __restrict__ fl
     }
     const unsigned any = __ballot_sync(0xffffffffu, fluid);
     if (lane == 0 && t < tiles && any) list[atomicAdd(count, 1)] = (int)t;
-}
-
-// Level 0's list in ascending tile order (the FP64 sums of mg_fcg_tiles.cuh walk it, so its order must
-// not change from run to run): one warp per tile writes its fluid flag to list[t], then one block
-// compacts the flags in place (k_compact_tiles).
-__global__ void __launch_bounds__(256) k_mg_tile_flags0(const uint8_t* __restrict__ op0, int nx, int ny, int nz,
-                                                        int* __restrict__ list) {
-    pdl_begin();
-    const int tk = tile_k(nz, true), jg = (ny + 3) / 4, kg = (nz + tk - 1) / tk;
-    const i64 tiles = (i64)nx * jg * kg;
-    const i64 t = ((i64)blockIdx.x * 256 + threadIdx.x) / 32;
-    const int lane = threadIdx.x & 31;
-    bool fluid = false;
-    if (t < tiles) {
-        const int kb = (int)(t % kg), jb = (int)((t / kg) % jg), i = (int)(t / ((i64)kg * jg));
-        const int j = jb * 4 + lane / 8;
-        if (j < ny)
-            for (int k = kb * tk + (lane & 7); k < kb * tk + tk && k < nz; k += 8)
-                fluid |= (__ldg(op0 + gidx(i, j, k, ny, nz)) & 64u) != 0u;
-    }
-    const unsigned any = __ballot_sync(0xffffffffu, fluid);
-    if (lane == 0 && t < tiles) list[t] = any ? 1 : 0;
-}
-
-constexpr int COMPACT_THREADS = 1024, COMPACT_PER = 8;
-
-// In-place ordered compaction of 0/1 flags into the indices of the set ones; *count = their number.
-// Chunk by chunk: every flag of a chunk is read before any index is written, and an index lands at or
-// before its own position, so no unread flag is overwritten.
-__global__ void __launch_bounds__(COMPACT_THREADS) k_compact_tiles(int* __restrict__ list, int n, int* __restrict__ count) {
-    pdl_begin();
-    __shared__ int s_warp[COMPACT_THREADS / 32];
-    __shared__ int s_base;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) s_base = 0;
-    __syncthreads();
-    for (int start = 0; start < n; start += COMPACT_THREADS * COMPACT_PER) {
-        int f[COMPACT_PER], mine = 0;
-#pragma unroll
-        for (int u = 0; u < COMPACT_PER; ++u) {
-            const int idx = start + threadIdx.x * COMPACT_PER + u;
-            f[u] = idx < n ? (list[idx] != 0) : 0;
-            mine += f[u];
-        }
-        int incl = mine;  // inclusive scan within the warp
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        if (lane == 31) s_warp[warp] = incl;
-        __syncthreads();  // also: every flag of the chunk has been read
-        if (warp == 0) {
-            int w = s_warp[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += v;
-            }
-            s_warp[lane] = w;  // inclusive over warps
-        }
-        __syncthreads();
-        int pos = s_base + (warp > 0 ? s_warp[warp - 1] : 0) + incl - mine;
-#pragma unroll
-        for (int u = 0; u < COMPACT_PER; ++u)
-            if (f[u]) list[pos++] = start + threadIdx.x * COMPACT_PER + u;
-        const int total = s_warp[COMPACT_THREADS / 32 - 1];
-        __syncthreads();  // s_base and s_warp read by all
-        if (threadIdx.x == 0) s_base += total;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *count = s_base;
 }
 
 // Red-black colour on the listed tiles: block b handles tiles b, b + gridDim.x, ... with the body of

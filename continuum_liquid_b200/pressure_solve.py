@@ -195,17 +195,16 @@ class PressureSolver:
                       coarse_iterations=self.coarse_iterations, queue=queue, x_from_zero=True)
         finally:
             h.struct.sweep[0] = kind0
-        # the dots and the step walk the level-0 fluid tiles (csrc/mg_fcg_tiles.cuh; rows when the
-        # hierarchy has no tiles)
+        delta = float(FIELD_DTYPE(self.dx))
         if self.method == "fcg":
-            self.kernels.call_hierarchy("clb_mg_fcg_dots_tiles", h.struct, self.correction, self.direction[src],
-                                        self.residual, self.fcg_partials, self.fcg_state, stream=queue)
-            self.kernels.call_hierarchy("clb_mg_fcg_step_tiles", h.struct, self.p64[src], self.correction,
-                                        self.direction[src], self.p64[1 - src], self.direction[1 - src],
-                                        self.fcg_state, self.rhs, self.residual, h.partials, h.norms, stream=queue)
+            self.kernels.call("clb_mg_fcg_dots", self.correction, self.direction[src], self.residual, h.op0, delta,
+                              *self.grid_shape, self.fcg_partials, self.fcg_state, stream=queue)
+            self.kernels.call("clb_mg_fcg_step", self.p64[src], self.correction, self.direction[src],
+                              self.p64[1 - src], self.direction[1 - src], self.fcg_state, self.rhs, h.op0, delta,
+                              *self.grid_shape, self.residual, h.partials, h.norms, stream=queue)
         else:
-            self.kernels.call_hierarchy("clb_mg_ir_step_tiles", h.struct, self.p64[src], self.correction,
-                                        self.p64[1 - src], self.rhs, self.residual, h.partials, h.norms, stream=queue)
+            self.kernels.call("clb_mg_ir_step", self.p64[src], self.correction, self.p64[1 - src], self.rhs, h.op0,
+                              delta, *self.grid_shape, self.residual, h.partials, h.norms, stream=queue)
 
     def _refine(self, use_graph: bool) -> None:
         src = self.cur

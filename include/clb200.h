@@ -398,19 +398,6 @@ int clb_mg_fcg_step(const double* p64_in, const float* z, const float* d_in, dou
                     const double* state, const float* b, const uint8_t* op0, float delta, int nx, int ny, int nz,
                     float* r_out, void* partials, double* out, void* stream);
 
-/* The same three steps on the level-0 fluid tiles of a hierarchy (clb_mg_build_coarse lists them, in
- * ascending order): each block loads a tile and the neighbours its cells read into shared memory
- * before any use, instead of walking rows. Op0, delta and the shape come from h. Per cell the values
- * are those of the calls above; the FP64 sums add the cells in another (fixed) order. Without fluid
- * tiles in h, or with option 3 off, they run the calls above. */
-int clb_mg_ir_step_tiles(const clb_mg_hierarchy* h, const double* p64_in, const float* e, double* p64_out,
-                         const float* b, float* r_out, void* partials, double* out, void* stream);
-int clb_mg_fcg_dots_tiles(const clb_mg_hierarchy* h, const float* z, const float* d, const float* r, void* partials4,
-                          double* state, void* stream);
-int clb_mg_fcg_step_tiles(const clb_mg_hierarchy* h, const double* p64_in, const float* z, const float* d_in,
-                          double* p64_out, float* d_out, const double* state, const float* b, float* r_out,
-                          void* partials, double* out, void* stream);
-
 /* ---- tensor cores -------------------------------------------------------------------------- */
 
 /* No counterpart in the reference (the learned warm start is new). Check of the tcgen05 GEMM core
