@@ -70,7 +70,8 @@ class BatchedFlip:
 
     def __init__(self, kernels: Backend, scenes: list[Scene], flip_ratio: float | None = None, tol: float | None = 1e-6,
                  num_vcycles: int = 1, reduce_blocks: int = 32, sweep0: int = 1, use_graph: bool = True,
-                 max_cycles: int = 100, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS):
+                 max_cycles: int = 100, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS,
+                 pre_smooth: int = PRE_SMOOTH, post_smooth: int = POST_SMOOTH):
         if not 1 <= len(scenes) <= BATCH_MAX_SCENES:
             raise ValueError(f"a batch holds 1..{BATCH_MAX_SCENES} scenes, got {len(scenes)}")
         first = scenes[0]
@@ -85,6 +86,11 @@ class BatchedFlip:
         self.tol, self.num_vcycles, self.max_cycles = tol, int(num_vcycles), int(max_cycles)
         # coarsest-level iterations of the tolerance mode's W-cycle preconditioner (fixed-cycle mode: 64)
         self.coarse_iterations = int(coarse_iterations)
+        # smoothing sweeps per level of the tolerance mode's W-cycle preconditioner (fixed-cycle mode:
+        # the reference's 2 and 4)
+        self.pre_smooth, self.post_smooth = int(pre_smooth), int(post_smooth)
+        if self.pre_smooth < 0 or self.post_smooth < 0 or self.pre_smooth + self.post_smooth == 0:
+            raise ValueError("pre_smooth and post_smooth must be >= 0 and not both 0")
         self.ppc = first.particles_per_cell
         self.use_graph = use_graph
         dev = kernels.device
@@ -280,8 +286,9 @@ class BatchedFlip:
         self._pre_work()
         self._swap()
 
-    def _w_cycle(self, x, rhs, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS) -> None:
-        self._call("clb_batch_w_cycle", x, rhs, PRE_SMOOTH, POST_SMOOTH, int(coarse_iterations))
+    def _w_cycle(self, x, rhs, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS, pre: int = PRE_SMOOTH,
+                 post: int = POST_SMOOTH) -> None:
+        self._call("clb_batch_w_cycle", x, rhs, int(pre), int(post), int(coarse_iterations))
 
     def _init_solve(self) -> None:
         self.cur = 0
@@ -292,7 +299,7 @@ class BatchedFlip:
 
     def _iteration(self, src: int) -> None:
         self.correction.zero_()
-        self._w_cycle(self.correction, self.residual, self.coarse_iterations)
+        self._w_cycle(self.correction, self.residual, self.coarse_iterations, self.pre_smooth, self.post_smooth)
         self._call("clb_batch_fcg_dots", self.correction, self.direction[src], self.residual, self.partials4,
                    self.fcg_state)
         self._call("clb_batch_fcg_step", self.p64[src], self.correction, self.direction[src], self.p64[1 - src],

@@ -55,10 +55,12 @@ def test_reference_mode_matches_single_scenes(backend, use_graph):
     assert backend.device_error() == 0
 
 
-def test_tolerance_mode_solves_every_scene(backend):
+@pytest.mark.parametrize("wset", [{}, {"coarse_iterations": 4, "pre_smooth": 1, "post_smooth": 1}],
+                         ids=["reference-cycle", "c4-s11"])
+def test_tolerance_mode_solves_every_scene(backend, wset):
     sc = mixed_scenes()
-    b = batch.BatchedFlip(backend, sc, flip_ratio=0.95, tol=1e-6)
-    sims = [single(backend, s, tol=1e-6) for s in sc]
+    b = batch.BatchedFlip(backend, sc, flip_ratio=0.95, tol=1e-6, **wset)
+    sims = [single(backend, s, tol=1e-6, **wset) for s in sc]
     for step in range(4):
         st = b.step()
         assert len(st.rel_residual) == len(sc) and max(st.rel_residual) <= 1e-6
