@@ -212,7 +212,7 @@ class Batch(ctypes.Structure):
         ("reduce_blocks", ctypes.c_int32),
         ("bottom_ka", ctypes.c_int32),
         ("bottom_kb", ctypes.c_int32),
-        ("pad", ctypes.c_int32),
+        ("p2g_tiled", ctypes.c_int32),
         ("bottom_smem", ctypes.c_int64),
         ("op0", ctypes.c_void_p),
         ("p", ctypes.c_void_p * MG_MAX_LEVELS),

@@ -71,7 +71,7 @@ class BatchedFlip:
     def __init__(self, kernels: Backend, scenes: list[Scene], flip_ratio: float | None = None, tol: float | None = 1e-6,
                  num_vcycles: int = 1, reduce_blocks: int = 32, sweep0: int = 1, use_graph: bool = True,
                  max_cycles: int = 100, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS,
-                 pre_smooth: int = PRE_SMOOTH, post_smooth: int = POST_SMOOTH):
+                 pre_smooth: int = PRE_SMOOTH, post_smooth: int = POST_SMOOTH, tiled_p2g: bool | None = None):
         if not 1 <= len(scenes) <= BATCH_MAX_SCENES:
             raise ValueError(f"a batch holds 1..{BATCH_MAX_SCENES} scenes, got {len(scenes)}")
         first = scenes[0]
@@ -205,6 +205,9 @@ class BatchedFlip:
         b.colour0 = self._list(rec0, blocks)
         b.sweep0 = int(sweep0)
         b.vec0 = vec
+        # P2G: the tiled scatter in tolerance mode (each particle visited once; the same values as the
+        # single-scene tiled P2G), the reference-order gather in the fixed-cycle mode (None: by mode)
+        b.p2g_tiled = int(tol is not None if tiled_p2g is None else bool(tiled_p2g))
         b.reduce_blocks = int(reduce_blocks)
         used = [p for p in self.plans if p[0] >= 0]
         b.bottom_ka = max((p[1] for p in used), default=0)

@@ -14,6 +14,7 @@
 #include "mg_bottom.cuh"
 #include "mg_sweep.cuh"
 #include "multigrid.cuh"
+#include "p2g_tiled.cuh"
 #include "particles.cuh"
 
 namespace clb {
@@ -115,6 +116,43 @@ __global__ void __launch_bounds__(P2G_THREADS) kb_p2g(BList L, i64 total, const 
     const i64 C = (i64)g.shape[0][0] * g.shape[0][1] * g.shape[0][2];
     p2g_cell(local >= 0 ? local : C, threadIdx.x & (P2G_LANES - 1), pos, vel, offsets + o, counts + o, u + o, v + o,
              w + o, ff + o, g.inv_dx, inv_ppc, CLB_DIMS(g, 0));
+}
+
+// k_p2g_tiled over the batch: the scenes' tiles are numbered scene after scene (in list order), block b
+// runs tile b of that numbering on its scene; bin offsets are batch-wide particle indices.
+__global__ void __launch_bounds__(P2GT_THREADS, 2) kb_p2g_tiled(BList L, const clb_batch_scene* __restrict__ G,
+                                                                 const float* __restrict__ pos,
+                                                                 const float* __restrict__ vel,
+                                                                 const int* __restrict__ offsets,
+                                                                 const int* __restrict__ counts, float* __restrict__ u,
+                                                                 float* __restrict__ v, float* __restrict__ w,
+                                                                 float* __restrict__ ff, float inv_ppc) {
+    __shared__ i64 s_start[CLB_BATCH_MAX_SCENES + 1];
+    for (int q = threadIdx.x; q < L.count; q += P2GT_THREADS) {
+        const clb_batch_scene& g = G[L.scene[q]];
+        int tj, tk;
+        s_start[q + 1] = p2g_tiled_tiles(CLB_DIMS(g, 0), &tj, &tk);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_start[0] = 0;
+        for (int q = 1; q <= L.count; ++q) s_start[q] += s_start[q - 1];
+    }
+    __syncthreads();
+    const i64 b = blockIdx.x;
+    if (b >= s_start[L.count]) return;  // the whole block leaves together
+    int lo = 0, hi = L.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_start[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const clb_batch_scene& g = G[L.scene[lo]];
+    const i64 o = g.base[0];
+    int tj, tk;
+    p2g_tiled_tiles(CLB_DIMS(g, 0), &tj, &tk);
+    p2g_tile((int)(b - s_start[lo]), pos, vel, offsets + o, counts + o, u + o, v + o, w + o, ff + o, g.inv_dx, inv_ppc,
+             CLB_DIMS(g, 0), tj, tk);
 }
 
 // k_particle_update over the batch (records staged through shared memory per block).

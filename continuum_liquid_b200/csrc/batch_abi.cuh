@@ -156,6 +156,19 @@ int clb_batch_particle_to_grid(const clb_batch* b, const float* particles, const
     if (clb_sort_particles(particles, velocity, particles_work, velocity_work, bin_offsets, bin_counts, keys, ranks,
                            perm, slot_keys, n, stream))
         return 1;
+    if (b->p2g_tiled) {  // each particle visited once per tile (the tolerance mode's P2G)
+        i64 tiles = 0;
+        for (int q = 0; q < b->scenes; ++q) {
+            const clb_batch_scene& g = b->geom_host[q];
+            int tj, tk;
+            tiles += p2g_tiled_tiles(g.shape[0][0], g.shape[0][1], g.shape[0][2], &tj, &tk);
+        }
+        kb_p2g_tiled<<<(unsigned)tiles, P2GT_THREADS, P2GT_SMEM, s>>>(blist(b->cells[0]), b->geom, particles_work,
+                                                                      velocity_work, bin_offsets, bin_counts, u, v, w,
+                                                                      fluid_fraction, inv_ppc);
+        CLB_LAUNCH_CHECK("kb_p2g_tiled");
+        return 0;
+    }
     kb_p2g<<<blocks_for(C * P2G_LANES, P2G_THREADS), P2G_THREADS, 0, s>>>(
         blist(b->cells[0]), C, b->geom, particles_work, velocity_work, bin_offsets, bin_counts, u, v, w,
         fluid_fraction, inv_ppc);

@@ -154,7 +154,9 @@ int clb_init(int device) {
     e = e != cudaSuccess ? e : cudaFuncSetAttribute(kb_coarse_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
     if (check_call(e, "bottom visit attribute")) return 1;
     if (check_call(cudaFuncSetAttribute(k_p2g_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, P2GT_SMEM),
-                   "tiled P2G attribute"))
+                   "tiled P2G attribute") ||
+        check_call(cudaFuncSetAttribute(kb_p2g_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, P2GT_SMEM),
+                   "batched tiled P2G attribute"))
         return 1;
     e = cudaFuncSetAttribute(k_l0_iter_tiles<L0F_ZERO | L0F_RESTRICT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)L0Region<3>::smem());

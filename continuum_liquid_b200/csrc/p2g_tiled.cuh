@@ -40,16 +40,17 @@ static_assert(P2GT_ROWS_I % 3 == 0 && P2GT_ROWS_J % 3 == 0, "phases split the ro
 
 __device__ __forceinline__ float p2gt_tent(float s, float f) { return fmaxf(0.0f, 1.0f - fabsf(s - f)); }
 
-__global__ void __launch_bounds__(P2GT_THREADS, 2)
-    k_p2g_tiled(const float* __restrict__ pos, const float* __restrict__ vel, const int* __restrict__ offsets,
-                const int* __restrict__ counts, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
-                float* __restrict__ ff, float inv_dx, float inv_ppc, int nx, int ny, int nz, int tiles_j,
-                int tiles_k) {
+// One block's tile (the body of k_p2g_tiled; also run per scene by the batched P2G). The particle
+// indices in offsets are indices into pos and vel.
+__device__ __forceinline__ void p2g_tile(int tile, const float* __restrict__ pos, const float* __restrict__ vel,
+                                         const int* __restrict__ offsets, const int* __restrict__ counts,
+                                         float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+                                         float* __restrict__ ff, float inv_dx, float inv_ppc, int nx, int ny, int nz,
+                                         int tiles_j, int tiles_k) {
     extern __shared__ __align__(16) float p2gt_smem[];
     float* s_vel = p2gt_smem;                    // [3][CELLS]
     float* s_wgt = p2gt_smem + 3 * P2GT_CELLS;  // [3][CELLS]
     int* s_cnt = reinterpret_cast<int*>(p2gt_smem + 6 * P2GT_CELLS);
-    const int tile = blockIdx.x;
     const int tk = tile % tiles_k, tj = (tile / tiles_k) % tiles_j, ti = tile / (tiles_k * tiles_j);
     const int i0 = ti * P2GT_TI, j0 = tj * P2GT_TJ, k0 = tk * P2GT_TK;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -173,7 +174,15 @@ __global__ void __launch_bounds__(P2GT_THREADS, 2)
     }
 }
 
-static inline int p2g_tiled_tiles(int nx, int ny, int nz, int* tiles_j, int* tiles_k) {
+__global__ void __launch_bounds__(P2GT_THREADS, 2)
+    k_p2g_tiled(const float* __restrict__ pos, const float* __restrict__ vel, const int* __restrict__ offsets,
+                const int* __restrict__ counts, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w,
+                float* __restrict__ ff, float inv_dx, float inv_ppc, int nx, int ny, int nz, int tiles_j,
+                int tiles_k) {
+    p2g_tile(blockIdx.x, pos, vel, offsets, counts, u, v, w, ff, inv_dx, inv_ppc, nx, ny, nz, tiles_j, tiles_k);
+}
+
+__host__ __device__ __forceinline__ int p2g_tiled_tiles(int nx, int ny, int nz, int* tiles_j, int* tiles_k) {
     const int ti = (nx + P2GT_TI - 1) / P2GT_TI;
     *tiles_j = (ny + P2GT_TJ - 1) / P2GT_TJ;
     *tiles_k = (nz + P2GT_TK - 1) / P2GT_TK;

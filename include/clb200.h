@@ -553,7 +553,8 @@ typedef struct clb_batch {
     int32_t vec0;                           /* 4: every scene's nz and level-0 base are multiples of 4 */
     int32_t reduce_blocks;                  /* blocks per scene of the FP64 reductions */
     int32_t bottom_ka, bottom_kb;           /* register tiles of the bottom visit (largest scene) */
-    int32_t pad;
+    int32_t p2g_tiled;                      /* 1: P2G by the tiled scatter (clb_particle_to_grid_tiled), 0:
+                                               the reference-order gather */
     int64_t bottom_smem;                    /* dynamic shared memory of the bottom visit (largest scene) */
     uint8_t* op0;                           /* level-0 packed operator of all scenes */
     float* p[CLB_MG_MAX_LEVELS];            /* levels >= 1 */
@@ -564,7 +565,8 @@ typedef struct clb_batch {
 
 /* Stage API over a batch (pointers are the batch-wide arrays; per-scene constants come from geom).
  * particle_to_grid: zero-fill, count with scene-offset keys, one scan, one stable sort, P2G
- * (clb_particle_to_grid per scene). Workspace as clb_particle_to_grid for the batch totals. */
+ * (clb_particle_to_grid per scene, or clb_particle_to_grid_tiled when b->p2g_tiled is 1). Workspace as
+ * clb_particle_to_grid for the batch totals. */
 int clb_batch_particle_to_grid(const clb_batch* b, const float* particles, const float* velocity,
                                float* particles_work, float* velocity_work, float* u, float* v, float* w,
                                float* fluid_fraction, int32_t* bin_counts, int32_t* bin_offsets, int32_t* keys,

@@ -71,3 +71,22 @@ def test_tolerance_mode_solves_every_scene(backend, wset):
             assert diff <= 1e-5 * sc[s].grid_shape[0] * sc[s].dx, (step, s, diff)
     assert b.graph_replays > 0
     assert backend.device_error() == 0
+
+
+@pytest.mark.parametrize("tiled", [True, False])
+def test_batched_p2g_matches_single_scenes(backend, tiled):
+    """The batch's P2G (the tiled scatter in tolerance mode, the reference-order gather otherwise) gives
+    each scene exactly the single-scene P2G's grid: the stages up to the pressure solve, bit for bit."""
+    sc = mixed_scenes()
+    b = batch.BatchedFlip(backend, sc, flip_ratio=0.95, tol=1e-6 if tiled else None, use_graph=False)
+    assert b.batch.p2g_tiled == int(tiled)
+    sims = [single(backend, s, tol=1e-6 if tiled else None) for s in sc]
+    assert all(sim.options.tiled_p2g() == tiled for sim in sims)
+    b.pre_solve()
+    host = lambda t: t.detach().cpu().numpy()  # noqa: E731
+    for s, sim in enumerate(sims):
+        sim.pre_solve()
+        for got, want, name in ((b.u, sim.u, "u"), (b.v, sim.v, "v"), (b.w, sim.w, "w"),
+                                (b.fluid_fraction, sim.fluid_fraction, "fluid fraction")):
+            assert np.array_equal(host(b.scene_view(got, s)), host(want)), (s, name)
+    assert backend.device_error() == 0
