@@ -50,6 +50,7 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_particle_obstacle_bc": [P, P, P, P, L, F, I, I, I, P],
     "clb_particle_update": [P, P, P, P, P, P, P, P, P, P, L, F, I, I, I, F, F, F, F, F, F, P],
     "clb_particle_update_moving": [P, P, P, P, P, P, P, P, P, P, L, F, I, I, I, F, F, F, F, F, F, P, P],
+    "clb_particle_update_tiled": [P, P, P, P, P, P, P, P, P, P, P, P, L, F, I, I, I, F, F, F, F, F, F, P, P],
     "clb_particle_obstacle_bc_moving": [P, P, P, P, L, F, I, I, I, P, P],
     "clb_grid_obstacle_bc_moving": [P, P, P, P, P, I, I, I, P, F, P],
     "clb_update_velocity": [P, P, P, P, P, P, P, F, F, F, F, F, F, F, F, F, F, I, I, I, P],

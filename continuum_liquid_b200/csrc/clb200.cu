@@ -4,6 +4,7 @@
 #include "binning.cuh"
 #include "p2g_tiled.cuh"
 #include "particles.cuh"
+#include "g2p_tiled.cuh"
 #include "grid.cuh"
 #include "multigrid.cuh"
 #include "mg_bottom.cuh"
@@ -156,7 +157,13 @@ int clb_init(int device) {
     if (check_call(cudaFuncSetAttribute(k_p2g_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, P2GT_SMEM),
                    "tiled P2G attribute") ||
         check_call(cudaFuncSetAttribute(kb_p2g_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, P2GT_SMEM),
-                   "batched tiled P2G attribute"))
+                   "batched tiled P2G attribute") ||
+        check_call(cudaFuncSetAttribute(k_particle_update_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        PUT_SMEM),
+                   "tiled particle update attribute") ||
+        check_call(cudaFuncSetAttribute(k_particle_update_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        PUT_SMEM),
+                   "tiled particle update attribute"))
         return 1;
     e = cudaFuncSetAttribute(k_l0_iter_tiles<L0F_ZERO | L0F_RESTRICT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)L0Region<3>::smem());
@@ -403,11 +410,36 @@ int clb_particle_update(float* particles, float* velocity, float* previous_out, 
     return 0;
 }
 
-// ---- moving colliders (no counterpart in the reference) ------------------------------------------
-
 static RigidMotion motion_of(const float* m) {
     return RigidMotion{m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8]};
 }
+
+int clb_particle_update_tiled(float* particles, float* velocity, float* previous_out, const float* u, const float* v,
+                              const float* w, const float* u_old, const float* v_old, const float* w_old,
+                              const uint8_t* obstacle, const int32_t* bin_offsets, const int32_t* bin_counts,
+                              int64_t n, float inv_dx, int nx, int ny, int nz, float flip_ratio, float dt, float lower,
+                              float upper_x, float upper_y, float upper_z, const float* motion, void* stream) {
+    CLB_GRID_ARGS_OK(nx, ny, nz);
+    CLB_REQUIRE(n >= 0 && n < (1ll << 31), "particle_update_tiled: n=%lld out of range", (long long)n);
+    if (n == 0) return 0;
+    CLB_REQUIRE(particles && velocity && u && v && w && u_old && v_old && w_old && bin_offsets && bin_counts,
+                "particle_update_tiled: null pointer");
+    CLB_REQUIRE(motion == nullptr || obstacle != nullptr, "particle_update_tiled: a motion needs an obstacle");
+    int tiles_j = 0, tiles_k = 0;
+    const int tiles = particle_update_tiles(nx, ny, nz, &tiles_j, &tiles_k);
+    if (motion)
+        k_particle_update_tiled<true><<<tiles, PUT_THREADS, PUT_SMEM, CLB_STREAM(stream)>>>(
+            particles, velocity, previous_out, u, v, w, u_old, v_old, w_old, obstacle, bin_offsets, bin_counts, inv_dx,
+            nx, ny, nz, flip_ratio, dt, lower, upper_x, upper_y, upper_z, tiles_j, tiles_k, motion_of(motion));
+    else
+        k_particle_update_tiled<false><<<tiles, PUT_THREADS, PUT_SMEM, CLB_STREAM(stream)>>>(
+            particles, velocity, previous_out, u, v, w, u_old, v_old, w_old, obstacle, bin_offsets, bin_counts, inv_dx,
+            nx, ny, nz, flip_ratio, dt, lower, upper_x, upper_y, upper_z, tiles_j, tiles_k, RigidMotion{});
+    CLB_LAUNCH_CHECK("k_particle_update_tiled");
+    return 0;
+}
+
+// ---- moving colliders (no counterpart in the reference) ------------------------------------------
 
 int clb_particle_obstacle_bc_moving(float* particles, const float* previous, float* velocity,
                                     const uint8_t* obstacle, int64_t n, float inv_dx, int nx, int ny, int nz,

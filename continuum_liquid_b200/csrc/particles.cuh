@@ -6,11 +6,13 @@
 
 namespace clb {
 
-// particles.cl:12-42 staggered_interpolation_base/fraction + sample_field for one face component.
+// particles.cl:12-42 staggered_interpolation_base/fraction + sample_field for one face component of
+// the current and the old grid at once. `fetch(i, j, k)` returns {cur, old} at node (i, j, k).
 // Returns the sample of `cur` and writes the sample of `old` into *old_sample.
-__device__ __forceinline__ float sample_pair(const float* __restrict__ cur, const float* __restrict__ old, float px,
-                                             float py, float pz, float inv_dx, float offx, float offy, float offz,
-                                             int nx, int ny, int nz, float* old_sample) {
+template <class Fetch>
+__device__ __forceinline__ float sample_pair_with(Fetch&& fetch, float px, float py, float pz, float inv_dx,
+                                                  float offx, float offy, float offz, int nx, int ny, int nz,
+                                                  float* old_sample) {
     const float sx = px * inv_dx - offx, sy = py * inv_dx - offy, sz = pz * inv_dx - offz;
     const int bx = clampi((int)floorf(sx), 0, nx - 2);
     const int by = clampi((int)floorf(sy), 0, ny - 2);
@@ -26,24 +28,33 @@ __device__ __forceinline__ float sample_pair(const float* __restrict__ cur, cons
 #pragma unroll
             for (int oz = 0; oz <= 1; ++oz) {
                 const float wgt = (ox ? fx : 1.0f - fx) * (oy ? fy : 1.0f - fy) * (oz ? fz : 1.0f - fz);
-                const i64 c = gidx(bx + ox, by + oy, bz + oz, ny, nz);
-                a += wgt * __ldg(cur + c);
-                b += wgt * __ldg(old + c);
+                const float2 val = fetch(bx + ox, by + oy, bz + oz);
+                a += wgt * val.x;
+                b += wgt * val.y;
             }
     *old_sample = b;
     return a;
 }
 
+__device__ __forceinline__ float sample_pair(const float* __restrict__ cur, const float* __restrict__ old, float px,
+                                             float py, float pz, float inv_dx, float offx, float offy, float offz,
+                                             int nx, int ny, int nz, float* old_sample) {
+    auto fetch = [&](int i, int j, int k) {
+        const i64 c = gidx(i, j, k, ny, nz);
+        return make_float2(__ldg(cur + c), __ldg(old + c));
+    };
+    return sample_pair_with(fetch, px, py, pz, inv_dx, offx, offy, offz, nx, ny, nz, old_sample);
+}
+
 // particles.cl:229-262 grid_to_particle with the FLIP/PIC blend extension (flip_ratio == 1 is the
-// reference's pure FLIP update v += I(u) - I(u_old)).
-__device__ __forceinline__ void g2p_velocity(float& v0, float& v1, float& v2, float px, float py, float pz,
-                                             const float* u, const float* v, const float* w, const float* ou,
-                                             const float* ov, const float* ow, float inv_dx, int nx, int ny, int nz,
-                                             float flip_ratio) {
+// reference's pure FLIP update v += I(u) - I(u_old)). `sample(axis, offx, offy, offz, &old)` samples
+// face component `axis` of the current and the old grid.
+template <class Sample>
+__device__ __forceinline__ void g2p_velocity_with(float& v0, float& v1, float& v2, Sample&& sample, float flip_ratio) {
     float o0, o1, o2;
-    const float c0 = sample_pair(u, ou, px, py, pz, inv_dx, 1.0f, 0.5f, 0.5f, nx, ny, nz, &o0);
-    const float c1 = sample_pair(v, ov, px, py, pz, inv_dx, 0.5f, 1.0f, 0.5f, nx, ny, nz, &o1);
-    const float c2 = sample_pair(w, ow, px, py, pz, inv_dx, 0.5f, 0.5f, 1.0f, nx, ny, nz, &o2);
+    const float c0 = sample(0, 1.0f, 0.5f, 0.5f, &o0);
+    const float c1 = sample(1, 0.5f, 1.0f, 0.5f, &o1);
+    const float c2 = sample(2, 0.5f, 0.5f, 1.0f, &o2);
     const float f0 = v0 + (c0 - o0), f1 = v1 + (c1 - o1), f2 = v2 + (c2 - o2);
     if (flip_ratio == 1.0f) {
         v0 = f0;
@@ -55,6 +66,18 @@ __device__ __forceinline__ void g2p_velocity(float& v0, float& v1, float& v2, fl
         v1 = flip_ratio * f1 + pic * c1;
         v2 = flip_ratio * f2 + pic * c2;
     }
+}
+
+__device__ __forceinline__ void g2p_velocity(float& v0, float& v1, float& v2, float px, float py, float pz,
+                                             const float* u, const float* v, const float* w, const float* ou,
+                                             const float* ov, const float* ow, float inv_dx, int nx, int ny, int nz,
+                                             float flip_ratio) {
+    auto sample = [&](int axis, float offx, float offy, float offz, float* old) {
+        const float* cur = axis == 0 ? u : (axis == 1 ? v : w);
+        const float* prev = axis == 0 ? ou : (axis == 1 ? ov : ow);
+        return sample_pair(cur, prev, px, py, pz, inv_dx, offx, offy, offz, nx, ny, nz, old);
+    };
+    g2p_velocity_with(v0, v1, v2, sample, flip_ratio);
 }
 
 // boundary_conditions.cl:69-97 particle_domain_bc for one component.
@@ -198,6 +221,29 @@ __global__ void __launch_bounds__(PT) k_particle_obstacle_bc(float* __restrict__
 // lives in registers; it is written out only when the caller asks for it.
 // The per-particle part of k_particle_update on registers (prev, when non-null, is this particle's
 // previous-position record).
+// The same with the grid velocity sampled by `sample` (g2p_velocity_with).
+template <bool MOVING, class Sample>
+__device__ __forceinline__ void particle_update_with(float& p0, float& p1, float& p2, float& v0, float& v1, float& v2,
+                                                     float* __restrict__ prev, Sample&& sample,
+                                                     const uint8_t* __restrict__ obs, float inv_dx, int nx, int ny,
+                                                     int nz, float flip_ratio, float dt, float lower, float ux,
+                                                     float uy, float uz, RigidMotion motion) {
+    g2p_velocity_with(v0, v1, v2, sample, flip_ratio);
+    const float q0 = p0, q1 = p1, q2 = p2;
+    if (prev) {
+        prev[0] = q0;
+        prev[1] = q1;
+        prev[2] = q2;
+    }
+    p0 = p0 + dt * v0;
+    p1 = p1 + dt * v1;
+    p2 = p2 + dt * v2;
+    domain_bc_axis(p0, v0, lower, ux);
+    domain_bc_axis(p1, v1, lower, uy);
+    domain_bc_axis(p2, v2, lower, uz);
+    if (obs) obstacle_bc<MOVING>(p0, p1, p2, q0, q1, q2, v0, v1, v2, obs, inv_dx, nx, ny, nz, motion);
+}
+
 template <bool MOVING = false>
 __device__ __forceinline__ void particle_update_one(float& p0, float& p1, float& p2, float& v0, float& v1, float& v2,
                                                     float* __restrict__ prev, const float* u, const float* v,

@@ -180,16 +180,27 @@ def advect_particles(kernels: Backend, queue, particles, particle_velocity, part
 
 def particle_update(kernels: Backend, queue, particles, particle_velocity, velocity, old_velocity, obstacle,
                     particle_count_total, grid_shape, dx, dt, flip_ratio: float = 1.0, previous_particles=None,
-                    motion=None):
+                    motion=None, bins=None):
     """solver.py:453-510 fused: G2P, previous-position copy, advection, domain and obstacle BCs.
 
     ``obstacle`` may be None when the scene has no collider (the obstacle BC is then a no-op in the
     reference as well). ``previous_particles`` receives the pre-advection positions when given.
     ``motion`` (with an obstacle): the collider moves rigidly (``colliders.RigidMotion.parameters``).
+    ``bins``: ``(bin_offsets, bin_counts)`` of the particles' counting sort when they are still sorted
+    by bin; the update then walks the bins tile by tile (``clb_particle_update_tiled``, same values).
     """
     nx, ny, nz = grid_shape
     u, v, w = velocity
     ou, ov, ow = old_velocity
+    if bins is not None:
+        offsets, counts = bins
+        kernels.call("clb_particle_update_tiled", particles, particle_velocity, previous_particles, u, v, w, ou, ov, ow,
+                     obstacle, offsets, counts, int(particle_count_total), float(FIELD_DTYPE(1.0 / float(dx))), nx, ny,
+                     nz, float(FIELD_DTYPE(flip_ratio)), float(FIELD_DTYPE(dt)),
+                     float(FIELD_DTYPE(1.001 * float(dx))), float(FIELD_DTYPE((nx - 1.001) * float(dx))),
+                     float(FIELD_DTYPE((ny - 1.001) * float(dx))), float(FIELD_DTYPE((nz - 1.001) * float(dx))),
+                     None if motion is None else motion_arg(motion), stream=queue)
+        return particles, particle_velocity
     extra = () if motion is None else (motion_arg(motion),)
     kernels.call(
         "clb_particle_update" if motion is None else "clb_particle_update_moving",

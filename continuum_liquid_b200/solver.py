@@ -214,9 +214,11 @@ class FlipSolver:
             boundary_conditions.grid_obstacle_bc(k, queue, vel, self.fluid_fraction, self.obstacle, gs,
                                                  self._motion, self.dx)
         if piece_bounds is None:
+            # the particles are still sorted by bin from this step's P2G: the tiled update (same values)
             particle_methods.particle_update(k, queue, self.particles, self.particle_velocity, vel,
                                              (self.u_work, self.v_work, self.w_work), self.obstacle, self.n, gs,
-                                             self.dx, self.dt, o.flip_ratio, motion=self._motion)
+                                             self.dx, self.dt, o.flip_ratio, motion=self._motion,
+                                             bins=(self.scan_outputs[0], self.bin_counts))
             return
         for c in range(len(piece_bounds) - 1):
             a, b = piece_bounds[c], piece_bounds[c + 1]

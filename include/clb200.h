@@ -192,6 +192,17 @@ int clb_grid_obstacle_bc_moving(float* u, float* v, float* w, float* fluid_fract
 int clb_particle_obstacle_bc_moving(float* particles, const float* previous, float* velocity,
                                     const uint8_t* obstacle, int64_t n, float inv_dx, int nx, int ny, int nz,
                                     const float* motion, void* stream);
+/* No counterpart in the reference: clb_particle_update (or, with motion non-NULL, the moving-obstacle
+ * form below; motion as there) walking the bins of 8 x 8 x 30-bin tiles: particles must be sorted by
+ * bin, bin_offsets / bin_counts describing them (the counting sort of clb_particle_to_grid, before any
+ * particle moves). Each block stages the six grid arrays its bins' particles sample in shared memory.
+ * The same values as clb_particle_update, bit for bit. */
+int clb_particle_update_tiled(float* particles, float* velocity, float* previous_out, const float* u, const float* v,
+                              const float* w, const float* u_old, const float* v_old, const float* w_old,
+                              const uint8_t* obstacle, const int32_t* bin_offsets, const int32_t* bin_counts,
+                              int64_t n, float inv_dx, int nx, int ny, int nz, float flip_ratio, float dt, float lower,
+                              float upper_x, float upper_y, float upper_z, const float* motion, void* stream);
+
 /* clb_particle_update with the moving obstacle condition above (obstacle must not be null). */
 int clb_particle_update_moving(float* particles, float* velocity, float* previous_out, const float* u, const float* v,
                                const float* w, const float* u_old, const float* v_old, const float* w_old,
