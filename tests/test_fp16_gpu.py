@@ -161,7 +161,7 @@ def test_fp16_cluster_visit_equals_level_by_level(backend, shape):
     assert backend.device_error() == 0
 
 
-@pytest.mark.parametrize("shape", [(130, 130, 130), (100, 90, 120)])
+@pytest.mark.parametrize("shape", [(130, 130, 130), (140, 130, 150)])
 def test_fp16_tile_transfers_equal_full_grid(backend, shape):
     """Restriction into and prolongation from an FP16 level on the fluid tiles (k_restrict_h_tiles,
     k_prolong_h_tiles) give the full-grid kernels' values: W-cycles with and without fluid tiles agree
