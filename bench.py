@@ -731,14 +731,20 @@ def kernel_rooflines(sim, peak, ms_per_step, reps=5):
                                              sim.scan_outputs[0], sim.bin_counts, (sim.u, sim.v, sim.w),
                                              sim.fluid_fraction, gs, sim.dx, sim.particles_per_cell, tiled=tiled))
 
-    def restore():
-        sim.particle_work[:n].copy_(pos[:n])
-        sim.particle_velocity_work[:n].copy_(vel[:n])
+    # the sort left the particles sorted by bin in the work buffers, with the bins of the scan above: the
+    # state the step's particle update runs on
+    sorted_pos, sorted_vel = sim.particle_work[:n].clone(), sim.particle_velocity_work[:n].clone()
 
-    timed("particle_update", "k_particle_update (G2P, FLIP/PIC blend, advection, particle BCs)", 48 * n + 24 * C,
+    def restore():
+        sim.particle_work[:n].copy_(sorted_pos)
+        sim.particle_velocity_work[:n].copy_(sorted_vel)
+
+    timed("particle_update", "k_particle_update_tiled (G2P, FLIP/PIC blend, advection, particle BCs)",
+          48 * n + 24 * C,
           lambda: pm.particle_update(k, None, sim.particle_work, sim.particle_velocity_work, (sim.u, sim.v, sim.w),
                                      (sim.u_work, sim.v_work, sim.w_work), sim.obstacle, n, gs, sim.dx, sim.dt,
-                                     sim.options.flip_ratio), prepare=restore)
+                                     sim.options.flip_ratio, bins=(sim.scan_outputs[0], sim.bin_counts)),
+          prepare=restore)
     return stages
 
 

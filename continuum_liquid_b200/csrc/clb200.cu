@@ -1217,11 +1217,6 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
             launch(tile_grid(c), dim3(32, 4), 0, s)(k_restrict_tiles<false>, c.tiles, c.tile_count, v.p, v.b,
                                                     nullptr, v.opc, v.mask, c.p, const_cast<float*>(c.b), h->delta,
                                                     v.nx, v.ny, v.nz, c.nx, c.ny, c.nz);
-    } else if (c.half && !v.half && !v.l0 && c.tiles) {  // FP32 coarse level into an FP16 one, coarse fluid tiles
-        launch(tile_grid(c), dim3(32, 4), 0, s)(k_restrict_h_tiles<1>, c.tiles, c.tile_count, v.p, v.b, nullptr, v.opc,
-                                                v.mask, reinterpret_cast<__half*>(c.p),
-                                                reinterpret_cast<__half*>(const_cast<float*>(c.b)), h->delta,
-                                                h->fp16_scale, v.nx, v.ny, v.nz, c.nx, c.ny, c.nz);
     } else if (c.half) {
         const dim3 grid = blocks_for(Cc, MGT);
 #define CLB_RESTRICT_H(FS)                                                                                        \
@@ -1261,10 +1256,6 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
         else
             launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<false, 1>, v.tiles, v.tile_count, c.p, v.p,
                                                     nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
-    } else if (c.half && !v.half && !v.l0 && v.tiles) {  // into the fine FP32 level's fluid tiles
-        launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_h_tiles, v.tiles, v.tile_count,
-                                                reinterpret_cast<const __half*>(c.p), v.p, v.mask, h->fp16_scale,
-                                                c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
     } else if (c.half) {
         const dim3 grid = blocks_for(Cf, MGT);
         const __half* ce = reinterpret_cast<const __half*>(c.p);

@@ -125,31 +125,6 @@ __global__ void __launch_bounds__(MGT) k_restrict_h(const void* __restrict__ fp,
     restrict_h_at<FS>(ci, fp, fb, fop0, fopc, fmask, cp, cb, delta, scale, fnx, fny, fnz, cnx, cny, cnz);
 }
 
-// The same on the listed fluid tiles of the FP16 coarse level (one plane, four rows, 32 cells; block
-// shape (32, 4)): cells of tiles without fluid keep the 0 that clb_mg_build_coarse wrote, which is
-// what the restriction writes there.
-template <int FS>
-__global__ void __launch_bounds__(128) k_restrict_h_tiles(const int* __restrict__ list, const int* __restrict__ count,
-                                                           const void* __restrict__ fp, const void* __restrict__ fb,
-                                                           const uint8_t* __restrict__ fop0,
-                                                           const void* __restrict__ fopc,
-                                                           const uint8_t* __restrict__ fmask, __half* __restrict__ cp,
-                                                           __half* __restrict__ cb, float delta,
-                                                           const float* __restrict__ scale, int fnx, int fny, int fnz,
-                                                           int cnx, int cny, int cnz) {
-    pdl_begin();
-    const int jg = (cny + 3) / 4, kg = (cnz + 31) / 32;
-    const int n = *count;
-    for (int t = blockIdx.x; t < n; t += gridDim.x) {
-        const int tile = __ldg(list + t);
-        const int kb = tile % kg, rest = tile / kg, i = rest / jg, j = (rest % jg) * 4 + threadIdx.y;
-        const int k = kb * 32 + threadIdx.x;
-        if (j < cny && k < cnz)
-            restrict_h_at<FS>(gidx(i, j, k, cny, cnz), fp, fb, fop0, fopc, fmask, cp, cb, delta, scale, fnx, fny, fnz,
-                              cnx, cny, cnz);
-    }
-}
-
 // Prolongation (multigrid.cl:182-201) from an FP16 coarse level into a fine level of layout FS; into
 // an FP32 level the coarse value is unscaled by 1 / sigma_p.
 template <int FS>
@@ -181,25 +156,6 @@ __global__ void __launch_bounds__(MGT) k_prolong_h(const __half* __restrict__ ce
     const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
     if (f >= C) return;
     prolong_h_at<FS>(f, ce, fp, fop0, fmask, scale, cnx, cny, cnz, fnx, fny, fnz);
-}
-
-// The same into the listed fluid tiles of an FP32 coarse fine level (FS = 1; 32-cell tiles, block
-// shape (32, 4)): only fluid cells change, and every fluid cell lies in a listed tile.
-__global__ void __launch_bounds__(128) k_prolong_h_tiles(const int* __restrict__ list, const int* __restrict__ count,
-                                                          const __half* __restrict__ ce, float* __restrict__ fp,
-                                                          const uint8_t* __restrict__ fmask,
-                                                          const float* __restrict__ scale, int cnx, int cny, int cnz,
-                                                          int fnx, int fny, int fnz) {
-    pdl_begin();
-    const int jg = (fny + 3) / 4, kg = (fnz + 31) / 32;
-    const int n = *count;
-    for (int t = blockIdx.x; t < n; t += gridDim.x) {
-        const int tile = __ldg(list + t);
-        const int kb = tile % kg, rest = tile / kg, i = rest / jg, j = (rest % jg) * 4 + threadIdx.y;
-        const int k = kb * 32 + threadIdx.x;
-        if (j < fny && k < fnz)
-            prolong_h_at<1>(gidx(i, j, k, fny, fnz), ce, fp, nullptr, fmask, scale, cnx, cny, cnz, fnx, fny, fnz);
-    }
 }
 
 }  // namespace clb

@@ -160,26 +160,3 @@ def test_fp16_cluster_visit_equals_level_by_level(backend, shape):
     assert out[1].abs().max() > 0
     assert backend.device_error() == 0
 
-
-@pytest.mark.parametrize("shape", [(130, 130, 130), (140, 130, 150)])
-def test_fp16_tile_transfers_equal_full_grid(backend, shape):
-    """Restriction into and prolongation from an FP16 level on the fluid tiles (k_restrict_h_tiles,
-    k_prolong_h_tiles) give the full-grid kernels' values: W-cycles with and without fluid tiles agree
-    bit for bit."""
-    dx = 1.0 / shape[0]
-    ff, vel = liquid_system(shape, 14)
-    out = {}
-    for tiles in (False, True):
-        h = multigrid.MultigridHierarchy(backend, shape, dx, fp16_max_size=64, fluid_tiles=tiles)
-        assert h.fp16_level == 2  # level 1 is FP32: its transfers to level 2 take the tile kernels
-        rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
-        h.rhs_operator(vel, ff, rhs, 1.0 / 240.0, 1000.0)
-        h.build_coarse()
-        h.residual_norms(torch.zeros_like(rhs), rhs)
-        e = torch.zeros_like(rhs)
-        for _ in range(2):
-            h.w_cycle(e, rhs, pre_smooth=1, post_smooth=1, coarse_iterations=4, x_zero_outside=tiles)
-        out[tiles] = e
-    assert torch.equal(out[False], out[True])
-    assert out[True].abs().max() > 0
-    assert backend.device_error() == 0
