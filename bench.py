@@ -95,6 +95,9 @@ def parse_args():
     ap.add_argument("--sweeps", type=int, default=4,
                     help="red-black iterations (with --fused-level0: launch pairs) of --case sweep0, W-cycles of "
                          "--case wcycle")
+    ap.add_argument("--level-kinds", default="",
+                    help="--case sweep0/wcycle: red-black sweep kinds per level after tuning, e.g. 1:3,2:3 (a fused "
+                         "kind 2, 3, 5 or 6 on a coarse level runs over the whole level instead of its fluid tiles)")
     ap.add_argument("--fused-level0", action="store_true",
                     help="--case sweep0/wcycle: level 0 of the W-cycle as the fused tile launches (sweep kind 7)")
     return ap.parse_args()
@@ -339,6 +342,9 @@ def sweep_case(args):
     ps.rhs.copy_(torch.randn(scene.grid_shape, device="cuda", generator=gen) * ff)
     h = ps.hierarchy
     tune_hierarchy(h, ps.correction, ps.residual)
+    for item in filter(None, args.level_kinds.split(",")):
+        level, kind = (int(x) for x in item.split(":"))
+        h.set_sweep(level, kind)
     kernels.call("clb_mg_set_option", 4, args.single_visit)
     if args.fused_level0:
         h.set_sweep(0, 7)  # level 0 of the W-cycle as the fused tile launches of csrc/mg_level0.cuh
@@ -350,10 +356,11 @@ def sweep_case(args):
         # as the tolerance mode runs it: a correction from zero (the buffer zeroed once, each W-cycle's
         # first sweep ignoring the previous correction), fluid tiles on every level
         k = 4 if args.coarse_iterations == "auto" else int(args.coarse_iterations)
+        pre, post = (2, 4) if args.smoothing == "auto" else (int(x) for x in args.smoothing.split(","))
         p.zero_()
 
         def cycle():
-            h.w_cycle(p, ps.rhs, coarse_iterations=k, x_from_zero=True)
+            h.w_cycle(p, ps.rhs, pre_smooth=pre, post_smooth=post, coarse_iterations=k, x_from_zero=True)
 
         cycle()
         torch.cuda.synchronize()
@@ -365,7 +372,7 @@ def sweep_case(args):
         torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         print(json.dumps({"case": "wcycle", "grid": list(scene.grid_shape), "levels": [list(x) for x in h.shapes],
-                          "sweep_kinds": h.sweeps(), "coarse_iterations": k,
+                          "sweep_kinds": h.sweeps(), "coarse_iterations": k, "smoothing": [pre, post],
                           "ms_per_w_cycle": e0.elapsed_time(e1) / args.sweeps}), flush=True)
         return
     if not args.fused_level0:
