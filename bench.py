@@ -95,9 +95,6 @@ def parse_args():
     ap.add_argument("--sweeps", type=int, default=4,
                     help="red-black iterations (with --fused-level0: launch pairs) of --case sweep0, W-cycles of "
                          "--case wcycle")
-    ap.add_argument("--level-kinds", default="",
-                    help="--case sweep0/wcycle: red-black sweep kinds per level after tuning, e.g. 1:3,2:3 (a fused "
-                         "kind 2, 3, 5 or 6 on a coarse level runs over the whole level instead of its fluid tiles)")
     ap.add_argument("--fused-level0", action="store_true",
                     help="--case sweep0/wcycle: level 0 of the W-cycle as the fused tile launches (sweep kind 7)")
     return ap.parse_args()
@@ -342,9 +339,6 @@ def sweep_case(args):
     ps.rhs.copy_(torch.randn(scene.grid_shape, device="cuda", generator=gen) * ff)
     h = ps.hierarchy
     tune_hierarchy(h, ps.correction, ps.residual)
-    for item in filter(None, args.level_kinds.split(",")):
-        level, kind = (int(x) for x in item.split(":"))
-        h.set_sweep(level, kind)
     kernels.call("clb_mg_set_option", 4, args.single_visit)
     if args.fused_level0:
         h.set_sweep(0, 7)  # level 0 of the W-cycle as the fused tile launches of csrc/mg_level0.cuh

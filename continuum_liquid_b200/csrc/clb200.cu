@@ -862,9 +862,7 @@ int smooth(const LevelView& v, float delta, int iterations, cudaStream_t s, bool
     const i64 C = (i64)v.nx * v.ny * v.nz;
     const int kind = v.sweep == 0 || v.sweep == 7 ? (v.half ? 4 : 1) : v.sweep;  // 7: see level0_fused
     const int vec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
-    // a fused kind on a coarse level runs over the whole level instead of the fluid-tile colour sweeps
-    const bool fused_kind = !v.l0 && (kind == 2 || kind == 3 || kind == 5 || kind == 6) && v.alt != nullptr;
-    if (sparse && tile_sweeps(v) && !fused_kind) {
+    if (sparse && tile_sweeps(v)) {
         const unsigned grid = tile_grid(v);
         const dim3 block(32, 4);
         for (int it = 0; it < iterations; ++it)
