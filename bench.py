@@ -961,6 +961,7 @@ def our_arm(args):
     solve_ms = []
     launches0 = kernels.launch_count()
     replays0 = sim.pressure_solver.graph_replays
+    loop0 = sim.pressure_solver.loop_refinements
     with ClockSampler(dev.index) as clocks:
         barrier()
         torch.cuda.synchronize()
@@ -978,7 +979,10 @@ def our_arm(args):
     value, elapsed_ms = throughput(group, args.steps, start.elapsed_time(end))
     direct_launches = kernels.launch_count() - launches0
     replays = sim.pressure_solver.graph_replays - replays0
-    gpu_launches = direct_launches + replays * sim.pressure_solver.graph_launches
+    # refinements replayed from graphs (the host loop's or the device loop's), plus the device loop's
+    # one check kernel per refinement
+    gpu_launches = direct_launches + replays * sim.pressure_solver.graph_launches + \
+        (sim.pressure_solver.loop_refinements - loop0)
     cycles = [s.cycles for s in stats]
     solve_ms = [s.device_ms() for s in stats]
 

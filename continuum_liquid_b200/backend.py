@@ -91,6 +91,10 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_w_cycle": [P, P, P, I, I, I, P],
     "clb_mg_smooth": [P, I, P, P, I, P],
     "clb_mg_level0_iteration": [P, P, P, P, I, P],
+    "clb_solve_loop_create": [P, P, P, P, P, P, P, P, P, P, P, P, I, I, I, I, D, I, P, P, I, P],
+    "clb_solve_loop_launch": [P, P, P],
+    "clb_solve_loop_launches": [P],
+    "clb_solve_loop_destroy": [P],
     "clb_mg_set_option": [I, I],
     "clb_mg_residual_partials": [L],
     "clb_mg_tile_capacity": [I, I, I, I],

@@ -1827,6 +1827,9 @@ int clb_source_spawn(const int32_t* missing, const int32_t* offsets, int nx, int
     return 0;
 }
 
+// ---- the tolerance-mode iteration looping on the device --------------------------------------------
+#include "solve_loop.cuh"
+
 // ---- batched scenes --------------------------------------------------------------------------------
 #include "batch_abi.cuh"
 

@@ -95,6 +95,10 @@ class SolveStats:
 METHODS = ("fcg", "refine")
 
 
+def ptr_of(t: torch.Tensor) -> int:
+    return t.data_ptr()
+
+
 class PressureSolver:
     """Packed-layout pressure solve for one grid (allocates its workspace once).
 
@@ -111,7 +115,7 @@ class PressureSolver:
                  autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64,
                  coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS,
                  pre_smooth: int = multigrid.PRE_SMOOTH, post_smooth: int = multigrid.POST_SMOOTH,
-                 fused_level0: bool = False):
+                 fused_level0: bool = False, device_loop: bool = True):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.coarse_fp16 = bool(coarse_fp16)
@@ -133,6 +137,12 @@ class PressureSolver:
         # csrc/mg_level0.cuh), with the values of the launch-per-step path. Off by default: at 256^3 the
         # recomputed halo costs more instructions than the four launches it saves
         self.fused_level0 = bool(fused_level0)
+        # device_loop: with CUDA graphs, tolerance-mode solves after the first run as one graph that
+        # loops on the device until the tolerance (clb_solve_loop_*, a WHILE conditional node): no host
+        # round trip between refinements
+        self.device_loop = bool(device_loop)
+        self._loop = None  # ctypes handle of the loop graph
+        self._loop_key = None
         if self.pre_smooth < 0 or self.post_smooth < 0 or self.pre_smooth + self.post_smooth == 0:
             raise ValueError("pre_smooth and post_smooth must be >= 0 and not both 0")
         # FP16 storage of the coarse levels of at most fp16_max_size cells per side (tolerance mode only:
@@ -157,8 +167,13 @@ class PressureSolver:
         self._graphs: list[torch.cuda.CUDAGraph | None] = [None, None]
         self.autotune = autotune
         self.tuned = False
-        self.graph_replays = 0  # refinement-graph replays so far
+        self.graph_replays = 0  # refinements replayed from graphs so far (host-loop graphs and the device loop)
         self.graph_launches = 0  # kernels inside one refinement graph
+        self.host_batch = 8  # most refinements the host loop runs between two reads of the residual
+        self.loop_refinements = 0  # refinements run by the device loop (each also runs one check kernel)
+        self.loop_cycles = torch.zeros(1, dtype=torch.int32, device=device)
+        self.loop_history = torch.zeros(self.max_cycles + 2, dtype=torch.float64, device=device)
+        self._loop_host = torch.zeros(self.max_cycles + 3, dtype=torch.float64, pin_memory=True)
 
     # -- pieces ---------------------------------------------------------------------------------
     def prepare(self, velocity, fluid_fraction, dt, rho, queue=None) -> None:
@@ -295,13 +310,18 @@ class PressureSolver:
                     stats.warm_start = "learned"
         stats.initial_rel_residual = rel
         stats.history.append(rel)
+        if use_graph and self.device_loop and self._loop is not None and self._loop_key == self._key(tol):
+            if rel > tol:
+                rel = self._run_loop(stats)
+            stats.rel_residual = rel
+            return self._finish(pressure, stats)
         rate = None
         while rel > tol and stats.cycles < self.max_cycles:
             # refinements to run before the next host check: one less than predicted, at least 1
             batch = 1
             if rate is not None and 0.0 < rate < 1.0:
                 batch = max(1, int(math.ceil(math.log(tol / rel) / math.log(rate))) - 1)
-            batch = min(batch, self.max_cycles - stats.cycles, 8)
+            batch = min(batch, self.max_cycles - stats.cycles, self.host_batch)
             for _ in range(batch):
                 self._refine(use_graph)
             previous = rel
@@ -310,7 +330,75 @@ class PressureSolver:
             stats.history.append(rel)
             rate = (rel / previous) ** (1.0 / batch) if previous > 0 and stats.cycles > 1 else None
         stats.rel_residual = rel
+        if use_graph and self.device_loop and self._loop_key != self._key(tol):
+            self._build_loop(tol)  # later solves loop on the device (the launches are warm now)
+        return self._finish(pressure, stats)
+
+    def _finish(self, pressure, stats: SolveStats) -> SolveStats:
         self.kernels.call("clb_mg_ir_store", self.p64[self.cur], pressure, self.cells)
         self.kernels.call("clb_neumann_domain_bc_f64", self.p64[self.cur], *self.grid_shape)
         self.solved64 = True
         return stats
+
+    # -- the device loop ------------------------------------------------------------------------
+    def _key(self, tol: float):
+        return (float(tol), self.max_cycles, self.method, self.pre_smooth, self.post_smooth, self.coarse_iterations,
+                self.fused_level0)
+
+    def _build_loop(self, tol: float) -> None:
+        import ctypes
+
+        self.release_loop()
+        h = self.hierarchy
+        kind0 = int(h.struct.sweep[0])
+        if self.fused_level0:
+            h.struct.sweep[0] = 7
+        out = ctypes.c_void_p()
+        from .backend import ptr
+
+        try:
+            status = self.kernels.lib.clb_solve_loop_create(
+                ctypes.byref(h.struct), ptr(self.correction), ptr(self.residual), ptr(self.direction[0]),
+                ptr(self.direction[1]), ptr(self.p64[0]), ptr(self.p64[1]), ptr(self.rhs), ptr(self.fcg_state),
+                ptr(self.fcg_partials), ptr(h.partials), ptr(h.norms), 0 if self.method == "fcg" else 1,
+                self.pre_smooth, self.post_smooth, self.coarse_iterations, float(tol), self.max_cycles,
+                ptr(self.loop_cycles), ptr(self.loop_history), int(self.loop_history.numel()), ctypes.byref(out))
+        finally:
+            h.struct.sweep[0] = kind0
+        if status != 0:  # the host loop stays in use
+            self.loop_error = (self.kernels.lib.clb_last_error() or b"").decode(errors="replace")
+            return
+        self._loop = out
+        self._loop_key = self._key(tol)
+        self.loop_launches = int(self.kernels.lib.clb_solve_loop_launches(out))
+
+    def _run_loop(self, stats: SolveStats) -> float:
+        """Runs the loop graph from the prepared state (buffer 0); returns the final relative residual."""
+        k = self.kernels
+        k._check(k.lib.clb_solve_loop_launch(self._loop, ptr_of(self.loop_cycles), k.stream_handle(None)),
+                 "clb_solve_loop_launch")
+        host = self._loop_host
+        host[0:1].copy_(self.loop_cycles.to(torch.float64), non_blocking=True)
+        host[1:].copy_(self.loop_history, non_blocking=True)
+        torch.cuda.current_stream(k.device).synchronize()
+        cycles = int(host[0])
+        stats.cycles = cycles
+        hist = [float(x) for x in host[2 : 2 + cycles]]  # history[1..cycles]
+        stats.history.extend(hist)
+        self.cur = cycles % 2
+        self.graph_replays += cycles
+        self.loop_refinements += cycles
+        return hist[-1] if hist else stats.history[0]
+
+    def release_loop(self) -> None:
+        """Destroys the loop graph (it is rebuilt on the next solve that needs it)."""
+        if self._loop is not None:
+            self.kernels.lib.clb_solve_loop_destroy(self._loop)
+            self._loop = None
+            self._loop_key = None
+
+    def __del__(self):
+        try:
+            self.release_loop()
+        except Exception:
+            pass

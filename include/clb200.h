@@ -409,6 +409,28 @@ int clb_mg_fcg_step(const double* p64_in, const float* z, const float* d_in, dou
                     const double* state, const float* b, const uint8_t* op0, float delta, int nx, int ny, int nz,
                     float* r_out, void* partials, double* out, void* stream);
 
+/* No counterpart in the reference: the tolerance-mode iteration as one CUDA graph that loops on the
+ * device. A WHILE conditional node runs refinement after refinement (clb_mg_w_cycle from a zero
+ * correction, then clb_mg_fcg_dots + clb_mg_fcg_step for method 0 or clb_mg_ir_step for method 1),
+ * the FP64 buffers and directions alternating 0 -> 1 -> 0 ..., until the relative residual
+ * sqrt(out[0] / out[1]) of a refinement is <= tol or max_cycles refinements have run; no host
+ * round trip inside. After each refinement k (from 1) *cycles = k and history[k] = its relative
+ * residual (k < history_len). The caller prepares the system and the initial residual, direction 0,
+ * FCG state and the zeroed buffers as for the calls it replaces; after the graph ran the pressure is
+ * in p64_0 if *cycles is even, else p64_1. Buffers and settings are fixed at creation (the hierarchy
+ * is read then). */
+typedef struct clb_solve_loop clb_solve_loop;
+int clb_solve_loop_create(const clb_mg_hierarchy* h, float* correction, float* residual, float* direction0,
+                          float* direction1, double* p64_0, double* p64_1, const float* rhs, double* fcg_state,
+                          void* fcg_partials, void* partials, double* norms, int method, int pre_smooth,
+                          int post_smooth, int coarse_iterations, double tol, int max_cycles, int* cycles,
+                          double* history, int history_len, clb_solve_loop** out);
+/* Resets *cycles to 0 and launches the loop on the stream (asynchronous). */
+int clb_solve_loop_launch(clb_solve_loop* loop, int* cycles, void* stream);
+/* Kernels one refinement of the loop launches (as clb_launch_count counts them). */
+int clb_solve_loop_launches(const clb_solve_loop* loop);
+int clb_solve_loop_destroy(clb_solve_loop* loop);
+
 /* ---- tensor cores -------------------------------------------------------------------------- */
 
 /* No counterpart in the reference (the learned warm start is new). Check of the tcgen05 GEMM core
