@@ -115,7 +115,7 @@ class PressureSolver:
                  autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64,
                  coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS,
                  pre_smooth: int = multigrid.PRE_SMOOTH, post_smooth: int = multigrid.POST_SMOOTH,
-                 fused_level0: bool = False, device_loop: bool = True):
+                 fused_level0: bool = False, device_loop: bool = False):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.coarse_fp16 = bool(coarse_fp16)
@@ -139,7 +139,9 @@ class PressureSolver:
         self.fused_level0 = bool(fused_level0)
         # device_loop: with CUDA graphs, tolerance-mode solves after the first run as one graph that
         # loops on the device until the tolerance (clb_solve_loop_*, a WHILE conditional node): no host
-        # round trip between refinements
+        # round trip between refinements. Off by default: at 256^3 it is as fast as the host loop (the
+        # loop's device-side body launches cost what the host's few residual reads did), and a profiler
+        # sees no kernel inside it
         self.device_loop = bool(device_loop)
         self._loop = None  # ctypes handle of the loop graph
         self._loop_key = None
