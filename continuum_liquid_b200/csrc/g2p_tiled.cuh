@@ -98,21 +98,45 @@ __global__ void __launch_bounds__(PUT_THREADS, 2)
         const int begin = __ldg(offsets + gidx(bx, by, k0, ny, nz));
         const i64 last = gidx(bx, by, k_last, ny, nz);
         const int end = __ldg(offsets + last) + __ldg(counts + last);
-        for (int p = begin + lane; p < end; p += 32) {
-            float p0 = pos[3 * (i64)p], p1 = pos[3 * (i64)p + 1], p2 = pos[3 * (i64)p + 2];
-            float v0 = vel[3 * (i64)p], v1 = vel[3 * (i64)p + 1], v2 = vel[3 * (i64)p + 2];
-            const float x0 = p0, x1 = p1, x2 = p2;  // the sampling position (pre-advection)
-            auto at = [&](int axis, float offx, float offy, float offz, float* old) {
-                return sample(axis, offx, offy, offz, old, x0, x1, x2);
+        // two particles per lane and round, both records loaded before either is updated (more loads in
+        // flight at this occupancy)
+        for (int p = begin + lane; p < end; p += 64) {
+            const int q = p + 32;
+            const bool two = q < end;
+            float a[6], c[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                a[t] = pos[3 * (i64)p + t];
+                a[3 + t] = vel[3 * (i64)p + t];
+            }
+            if (two)
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    c[t] = pos[3 * (i64)q + t];
+                    c[3 + t] = vel[3 * (i64)q + t];
+                }
+            auto update = [&](float* r, int idx) {
+                const float x0 = r[0], x1 = r[1], x2 = r[2];  // the sampling position (pre-advection)
+                auto at = [&](int axis, float offx, float offy, float offz, float* old) {
+                    return sample(axis, offx, offy, offz, old, x0, x1, x2);
+                };
+                particle_update_with<MOVING>(r[0], r[1], r[2], r[3], r[4], r[5],
+                                             prev_out ? prev_out + 3 * (i64)idx : nullptr, at, obs, inv_dx, nx, ny,
+                                             nz, flip_ratio, dt, lower, ux, uy, uz, motion);
             };
-            particle_update_with<MOVING>(p0, p1, p2, v0, v1, v2, prev_out ? prev_out + 3 * (i64)p : nullptr, at, obs,
-                                         inv_dx, nx, ny, nz, flip_ratio, dt, lower, ux, uy, uz, motion);
-            pos[3 * (i64)p] = p0;
-            pos[3 * (i64)p + 1] = p1;
-            pos[3 * (i64)p + 2] = p2;
-            vel[3 * (i64)p] = v0;
-            vel[3 * (i64)p + 1] = v1;
-            vel[3 * (i64)p + 2] = v2;
+            update(a, p);
+            if (two) update(c, q);
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                pos[3 * (i64)p + t] = a[t];
+                vel[3 * (i64)p + t] = a[3 + t];
+            }
+            if (two)
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    pos[3 * (i64)q + t] = c[t];
+                    vel[3 * (i64)q + t] = c[3 + t];
+                }
         }
     }
 }
