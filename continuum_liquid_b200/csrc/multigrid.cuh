@@ -548,13 +548,25 @@ __device__ __forceinline__ void residual_rows_block(int blk, int nblk, const PT*
         const bool row_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
         const int base = r * nz;
         if (SKIP && MODE != RES_NORM && (!row_in || !row_has_fluid(op0, base, nz, lane))) continue;
-        for (int k = lane; k < nz; k += 32) {
+        // a lane's operator bytes of 8 consecutive steps are loaded together, so a step waits on one
+        // round of loads (its stencil), not two (the byte that says whether the cell is fluid first)
+        for (int k0 = 0; k0 < nz; k0 += 256) {
+        unsigned long long ops = 0ull;  // byte m: the operator of step m
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int k = k0 + lane + 32 * m;
+            if (k < nz) ops |= (unsigned long long)__ldg(op0 + base + k) << (8 * m);
+        }
+#pragma unroll 1
+        for (int m = 0; m < 8; ++m) {
+            const int k = k0 + lane + 32 * m;
+            if (k >= nz) continue;
             const int c = base + k;
-            if (SKIP && MODE != RES_NORM && !(row_in && k >= 1 && k <= nz - 2 && (__ldg(op0 + c) & 64u))) continue;
+            const uint32_t o = (uint32_t)(ops >> (8 * m)) & 0xffu;
+            if (SKIP && MODE != RES_NORM && !(row_in && k >= 1 && k <= nz - 2 && (o & 64u))) continue;
             const double pc = pv(c);
             if (MODE != RES_NORM) p_out[c] = pc;
             if (MODE == RES_FCG) d_out[c] = dv(c);
-            const uint32_t o = __ldg(op0 + c);
             float rf = 0.0f;
             if (row_in && k >= 1 && k <= nz - 2 && (o & 64u)) {
                 const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
@@ -568,6 +580,7 @@ __device__ __forceinline__ void residual_rows_block(int blk, int nblk, const PT*
                 rf = (float)res;
             }
             if (r_out) r_out[c] = rf;
+        }
         }
     }
 #pragma unroll
@@ -629,9 +642,18 @@ __device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* _
         if (i < 1 || i > nx - 2 || j < 1 || j > ny - 2) continue;
         const int base = q * nz;
         if (!row_has_fluid(op0, base, nz, lane)) continue;
-        for (int k = lane; k < nz; k += 32) {
+        for (int k0 = 0; k0 < nz; k0 += 256) {  // operator bytes of 8 steps first, as in the step kernel
+        unsigned long long ops = 0ull;  // byte m: the operator of step m
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int k = k0 + lane + 32 * m;
+            if (k < nz) ops |= (unsigned long long)__ldg(op0 + base + k) << (8 * m);
+        }
+#pragma unroll 1
+        for (int m = 0; m < 8; ++m) {
+            const int k = k0 + lane + 32 * m;
             const int c = base + k;
-            const uint32_t o = __ldg(op0 + c);
+            const uint32_t o = (uint32_t)(ops >> (8 * m)) & 0xffu;
             if (k < 1 || k > nz - 2 || !(o & 64u)) continue;
             const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
             const double zc = (double)__ldg(z + c);
@@ -647,6 +669,7 @@ __device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* _
             t.y += az * zc;
             t.z += zc * rc;
             t.w += dc * rc;
+        }
         }
     }
 #pragma unroll
@@ -670,7 +693,7 @@ __device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* _
     }
 }
 
-__global__ void __launch_bounds__(RN_THREADS) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
+__global__ void __launch_bounds__(RN_THREADS, 4) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
                                                           const float* __restrict__ r,
                                                           const uint8_t* __restrict__ op0, double inv_delta2, int nx,
                                                           int ny, int nz, Sum4* __restrict__ partials) {

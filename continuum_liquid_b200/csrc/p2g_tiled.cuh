@@ -89,27 +89,11 @@ __device__ __forceinline__ void p2g_tile(int tile, const float* __restrict__ pos
                 for (int a = 0; a < 12; ++a) vu[a] = wu[a] = vv[a] = wv[a] = vw[a] = ww[a] = 0.0f;
                 const float fbx = (float)bx, fby = (float)by, fbz = (float)bz;
                 const int li = bx - i0, lj = by - j0, lk = bz - k0;
-                // the next particle's record is loaded while this one is added
-                float np0 = 0.0f, np1 = 0.0f, np2 = 0.0f, nv0 = 0.0f, nv1 = 0.0f, nv2 = 0.0f;
-                if (begin < end) {
-                    np0 = __ldg(pos + 3 * (i64)begin);
-                    np1 = __ldg(pos + 3 * (i64)begin + 1);
-                    np2 = __ldg(pos + 3 * (i64)begin + 2);
-                    nv0 = __ldg(vel + 3 * (i64)begin);
-                    nv1 = __ldg(vel + 3 * (i64)begin + 1);
-                    nv2 = __ldg(vel + 3 * (i64)begin + 2);
-                }
                 for (int q = begin; q < end; ++q) {
-                    const float sx = np0 * inv_dx, sy = np1 * inv_dx, sz = np2 * inv_dx;
-                    const float v0 = nv0, v1 = nv1, v2 = nv2;
-                    if (q + 1 < end) {
-                        np0 = __ldg(pos + 3 * (i64)(q + 1));
-                        np1 = __ldg(pos + 3 * (i64)(q + 1) + 1);
-                        np2 = __ldg(pos + 3 * (i64)(q + 1) + 2);
-                        nv0 = __ldg(vel + 3 * (i64)(q + 1));
-                        nv1 = __ldg(vel + 3 * (i64)(q + 1) + 1);
-                        nv2 = __ldg(vel + 3 * (i64)(q + 1) + 2);
-                    }
+                    const float* P = pos + 3 * (i64)q;
+                    const float* V = vel + 3 * (i64)q;
+                    const float sx = __ldg(P) * inv_dx, sy = __ldg(P + 1) * inv_dx, sz = __ldg(P + 2) * inv_dx;
+                    const float v0 = __ldg(V), v1 = __ldg(V + 1), v2 = __ldg(V + 2);
                     // the reference's face positions: cell c's u face at c + 1 on x, its v and w faces
                     // at c + 0.5; here c = b - 1, b, b + 1 (full) and b, b + 1 (half)
                     const float fx[3] = {p2gt_tent(sx, fbx), p2gt_tent(sx, fbx + 1.0f), p2gt_tent(sx, fbx + 2.0f)};
