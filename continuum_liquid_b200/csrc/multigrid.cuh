@@ -693,7 +693,7 @@ __device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* _
     }
 }
 
-__global__ void __launch_bounds__(RN_THREADS, 4) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
+__global__ void __launch_bounds__(RN_THREADS, 5) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
                                                           const float* __restrict__ r,
                                                           const uint8_t* __restrict__ op0, double inv_delta2, int nx,
                                                           int ny, int nz, Sum4* __restrict__ partials) {
