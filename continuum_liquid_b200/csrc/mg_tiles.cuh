@@ -63,8 +63,11 @@ __global__ void __launch_bounds__(128) k_rbgs_colour_tiles(const int* __restrict
     pdl_begin();
     const int tk = 32 * VEC, jg = (ny + 3) / 4, kg = (nz + tk - 1) / tk;
     const int n = *count;
+    // the next tile's index is loaded while this tile is swept
+    int next = blockIdx.x < n ? __ldg(list + blockIdx.x) : 0;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
-        const int tile = __ldg(list + t);
+        const int tile = next;
+        if (t + (int)gridDim.x < n) next = __ldg(list + t + gridDim.x);
         const int kb = tile % kg, rest = tile / kg;
         rbgs_colour_at<L0, VEC, Z>(kb, rest % jg, rest / jg, p, b, op0, opc, mask, delta, parity, nx, ny, nz);
     }
@@ -82,8 +85,10 @@ __global__ void __launch_bounds__(128) k_restrict_tiles(const int* __restrict__ 
     pdl_begin();
     const int jg = (cny + 3) / 4, kg = (cnz + 31) / 32;
     const int n = *count;
+    int next = blockIdx.x < n ? __ldg(list + blockIdx.x) : 0;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
-        const int tile = __ldg(list + t);
+        const int tile = next;
+        if (t + (int)gridDim.x < n) next = __ldg(list + t + gridDim.x);
         const int kb = tile % kg, rest = tile / kg, i = rest / jg, j = (rest % jg) * 4 + threadIdx.y;
         const int k = kb * 32 + threadIdx.x;
         if (j < cny && k < cnz)
@@ -102,8 +107,10 @@ __global__ void __launch_bounds__(128) k_prolong_tiles(const int* __restrict__ l
     pdl_begin();
     const int tk = 32 * VEC, jg = (fny + 3) / 4, kg = (fnz + tk - 1) / tk;
     const int n = *count;
+    int next = blockIdx.x < n ? __ldg(list + blockIdx.x) : 0;
     for (int t = blockIdx.x; t < n; t += gridDim.x) {
-        const int tile = __ldg(list + t);
+        const int tile = next;
+        if (t + (int)gridDim.x < n) next = __ldg(list + t + gridDim.x);
         const int kb = tile % kg, rest = tile / kg, i = rest / jg, j = (rest % jg) * 4 + threadIdx.y;
         if (j >= fny) continue;
 #pragma unroll

@@ -642,18 +642,9 @@ __device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* _
         if (i < 1 || i > nx - 2 || j < 1 || j > ny - 2) continue;
         const int base = q * nz;
         if (!row_has_fluid(op0, base, nz, lane)) continue;
-        for (int k0 = 0; k0 < nz; k0 += 256) {  // operator bytes of 8 steps first, as in the step kernel
-        unsigned long long ops = 0ull;  // byte m: the operator of step m
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            const int k = k0 + lane + 32 * m;
-            if (k < nz) ops |= (unsigned long long)__ldg(op0 + base + k) << (8 * m);
-        }
-#pragma unroll 1
-        for (int m = 0; m < 8; ++m) {
-            const int k = k0 + lane + 32 * m;
+        for (int k = lane; k < nz; k += 32) {
             const int c = base + k;
-            const uint32_t o = (uint32_t)(ops >> (8 * m)) & 0xffu;
+            const uint32_t o = __ldg(op0 + c);
             if (k < 1 || k > nz - 2 || !(o & 64u)) continue;
             const uint32_t ox = __ldg(op0 + c - sx), oy = __ldg(op0 + c - sy), oz = __ldg(op0 + c - 1);
             const double zc = (double)__ldg(z + c);
@@ -669,7 +660,6 @@ __device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* _
             t.y += az * zc;
             t.z += zc * rc;
             t.w += dc * rc;
-        }
         }
     }
 #pragma unroll
@@ -693,7 +683,7 @@ __device__ __forceinline__ void fcg_dots_block(int blk, int nblk, const float* _
     }
 }
 
-__global__ void __launch_bounds__(RN_THREADS, 5) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
+__global__ void __launch_bounds__(RN_THREADS) k_fcg_dots(const float* __restrict__ z, const float* __restrict__ d,
                                                           const float* __restrict__ r,
                                                           const uint8_t* __restrict__ op0, double inv_delta2, int nx,
                                                           int ny, int nz, Sum4* __restrict__ partials) {
