@@ -1247,7 +1247,10 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
     const i64 Cf = (i64)v.nx * v.ny * v.nz;
     const int fvec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
     if (!c.half && !v.half && v.tiles) {  // prolongation into the fine fluid tiles
-        if (v.l0 && fvec == 4)
+        if (v.l0 && fvec == 4 && ((((uintptr_t)v.p) & 15) | (((uintptr_t)v.op0) & 3)) == 0)
+            launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<true, 4, true>, v.tiles, v.tile_count, c.p, v.p,
+                                                    v.op0, nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
+        else if (v.l0 && fvec == 4)
             launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<true, 4>, v.tiles, v.tile_count, c.p, v.p, v.op0,
                                                     nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
         else if (v.l0)

@@ -98,7 +98,9 @@ __global__ void __launch_bounds__(128) k_restrict_tiles(const int* __restrict__ 
 }
 
 // Prolongation (prolong_at) into the fine cells of the listed fine tiles (TK = 32 VEC cells along k).
-template <bool L0, int VEC>
+// V4 (finest level, VEC = 4; the caller checked that x is 16-byte and the operator 4-byte aligned):
+// each thread's four cells as vectors.
+template <bool L0, int VEC, bool V4 = false>
 __global__ void __launch_bounds__(128) k_prolong_tiles(const int* __restrict__ list, const int* __restrict__ count,
                                                         const float* __restrict__ ce, float* __restrict__ fp,
                                                         const uint8_t* __restrict__ fop0,
@@ -113,10 +115,31 @@ __global__ void __launch_bounds__(128) k_prolong_tiles(const int* __restrict__ l
         if (t + (int)gridDim.x < n) next = __ldg(list + t + gridDim.x);
         const int kb = tile % kg, rest = tile / kg, i = rest / jg, j = (rest % jg) * 4 + threadIdx.y;
         if (j >= fny) continue;
+        if constexpr (V4) {
+            static_assert(L0 && VEC == 4, "the vector form is the finest level's");
+            // the thread's four cells at once (nz % 4 == 0, 16-byte aligned rows): their operator bytes,
+            // x and the parents' corrections in one round of loads; prolong_at's update per cell
+            const int k0 = (kb * 32 + threadIdx.x) * 4;
+            if (k0 >= fnz || i < 1 || i > fnx - 2 || j < 1 || j > fny - 2) continue;
+            const i64 c0 = gidx(i, j, k0, fny, fnz);
+            const uchar4 o = *reinterpret_cast<const uchar4*>(fop0 + c0);
+            if (!((o.x | o.y | o.z | o.w) & 64u)) continue;
+            float4 x = *reinterpret_cast<const float4*>(fp + c0);
+            const i64 cb = gidx(min((i - 1) / 2 + 1, cnx - 2), min((j - 1) / 2 + 1, cny - 2), 0, cny, cnz);
+            auto parent = [&](int k) { return __ldg(ce + cb + min((k - 1) / 2 + 1, cnz - 2)); };
+            const float e0 = parent(k0), e1 = parent(k0 + 1), e2 = parent(k0 + 2), e3 = parent(k0 + 3);
+            auto live = [&](unsigned ob, int k) { return (ob & 64u) && k >= 1 && k <= fnz - 2; };
+            if (live(o.x, k0)) x.x += e0;
+            if (live(o.y, k0 + 1)) x.y += e1;
+            if (live(o.z, k0 + 2)) x.z += e2;
+            if (live(o.w, k0 + 3)) x.w += e3;
+            *reinterpret_cast<float4*>(fp + c0) = x;
+        } else {
 #pragma unroll
-        for (int q = 0; q < VEC; ++q) {
-            const int k = (kb * 32 + threadIdx.x) * VEC + q;
-            if (k < fnz) prolong_at<L0>(gidx(i, j, k, fny, fnz), ce, fp, fop0, fmask, cnx, cny, cnz, fnx, fny, fnz);
+            for (int q = 0; q < VEC; ++q) {
+                const int k = (kb * 32 + threadIdx.x) * VEC + q;
+                if (k < fnz) prolong_at<L0>(gidx(i, j, k, fny, fnz), ce, fp, fop0, fmask, cnx, cny, cnz, fnx, fny, fnz);
+            }
         }
     }
 }
