@@ -1209,10 +1209,10 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
     const LevelView c = level_view(h, level + 1, x, rhs);
     const i64 Cc = (i64)c.nx * c.ny * c.nz;
     if (!c.half && !v.half && c.tiles) {  // restriction of the coarse fluid tiles (inactive cells hold 0)
-        if (v.l0)  // the fine neighbourhood of each coarse tile staged in shared memory first
-            launch(tile_grid(c), dim3(32, 4), 0, s)(k_restrict_tiles_l0, c.tiles, c.tile_count, v.p, v.b, v.op0, c.p,
-                                                    const_cast<float*>(c.b), h->delta, v.nx, v.ny, v.nz, c.nx, c.ny,
-                                                    c.nz);
+        if (v.l0)
+            launch(tile_grid(c), dim3(32, 4), 0, s)(k_restrict_tiles<true>, c.tiles, c.tile_count, v.p, v.b, v.op0,
+                                                    nullptr, nullptr, c.p, const_cast<float*>(c.b), h->delta, v.nx,
+                                                    v.ny, v.nz, c.nx, c.ny, c.nz);
         else
             launch(tile_grid(c), dim3(32, 4), 0, s)(k_restrict_tiles<false>, c.tiles, c.tile_count, v.p, v.b,
                                                     nullptr, v.opc, v.mask, c.p, const_cast<float*>(c.b), h->delta,

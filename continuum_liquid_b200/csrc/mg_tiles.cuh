@@ -97,101 +97,6 @@ __global__ void __launch_bounds__(128) k_restrict_tiles(const int* __restrict__ 
     }
 }
 
-// Restriction from the finest level into the cells of the listed coarse tiles (one plane I, rows
-// J0 .. J0 + 3, cells K0 .. K0 + 31; block shape (32, 4)) with the fine neighbourhood staged first:
-// the block loads x and the packed operator over fine planes 2I - 2 .. 2I + 1, rows 2 J0 - 2 .. 2 J0 + 7
-// and cells 2 K0 - 2 .. 2 K0 + 63, and b over the children, in one round of loads, then each thread
-// forms its coarse cell's eight child residuals from shared memory. restrict_at<true>'s arithmetic and
-// order, so the same values; cells outside the fine grid are staged as 0 and never read as children.
-constexpr int RS_PI = 4, RS_PJ = 10, RS_PK = 66, RS_P = RS_PI * RS_PJ * RS_PK;
-constexpr int RS_BI = 2, RS_BJ = 8, RS_BK = 64, RS_B = RS_BI * RS_BJ * RS_BK;
-
-__global__ void __launch_bounds__(128) k_restrict_tiles_l0(const int* __restrict__ list, const int* __restrict__ count,
-                                                            const float* __restrict__ fp, const float* __restrict__ fb,
-                                                            const uint8_t* __restrict__ fop0, float* __restrict__ cp,
-                                                            float* __restrict__ cb, float delta, int fnx, int fny,
-                                                            int fnz, int cnx, int cny, int cnz) {
-    pdl_begin();
-    __shared__ float s_p[RS_P];
-    __shared__ float s_b[RS_B];
-    __shared__ uint8_t s_o[RS_P];
-    const int jg = (cny + 3) / 4, kg = (cnz + 31) / 32;
-    const int n = *count;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    const i64 sxg = (i64)fny * fnz;
-    const float inv_delta2 = 1.0f / (delta * delta);
-    int next = blockIdx.x < n ? __ldg(list + blockIdx.x) : 0;
-    for (int t = blockIdx.x; t < n; t += gridDim.x) {
-        const int tile = next;
-        if (t + (int)gridDim.x < n) next = __ldg(list + t + gridDim.x);
-        const int kb = tile % kg, rest = tile / kg, I = rest / jg, J0 = (rest % jg) * 4, K0 = kb * 32;
-        const int gi = 2 * I - 2, gj = 2 * J0 - 2, gk = 2 * K0 - 2;  // staged region origin
-        __syncthreads();  // the previous tile's reads of shared memory are done
-        constexpr int UP = (RS_P + 127) / 128, UB = (RS_B + 127) / 128;
-        float pv[UP], bv[UB];
-        uint32_t ov[UP];
-#pragma unroll
-        for (int u = 0; u < UP; ++u) {
-            const int q = tid + u * 128;
-            const int a = q / (RS_PJ * RS_PK), r = q - a * (RS_PJ * RS_PK), bj = r / RS_PK, ck = r - bj * RS_PK;
-            const int i = gi + a, j = gj + bj, k = gk + ck;
-            pv[u] = 0.0f;
-            ov[u] = 0u;
-            if (q < RS_P && i >= 0 && i < fnx && j >= 0 && j < fny && k >= 0 && k < fnz) {
-                const i64 c = i * sxg + (i64)j * fnz + k;
-                pv[u] = __ldg(fp + c);
-                ov[u] = __ldg(fop0 + c);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < UB; ++u) {
-            const int q = tid + u * 128;
-            const int a = q / (RS_BJ * RS_BK), r = q - a * (RS_BJ * RS_BK), bj = r / RS_BK, ck = r - bj * RS_BK;
-            const int i = gi + 1 + a, j = gj + 1 + bj, k = gk + 1 + ck;
-            bv[u] = 0.0f;
-            if (q < RS_B && i >= 0 && i < fnx && j >= 0 && j < fny && k >= 0 && k < fnz)
-                bv[u] = __ldg(fb + i * sxg + (i64)j * fnz + k);
-        }
-#pragma unroll
-        for (int u = 0; u < UP; ++u) {
-            const int q = tid + u * 128;
-            if (q < RS_P) {
-                s_p[q] = pv[u];
-                s_o[q] = (uint8_t)ov[u];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < UB; ++u) {
-            const int q = tid + u * 128;
-            if (q < RS_B) s_b[q] = bv[u];
-        }
-        __syncthreads();
-        const int J = J0 + threadIdx.y, K = K0 + threadIdx.x;
-        if (J >= cny || K >= cnz) continue;
-        const i64 ci = gidx(I, J, K, cny, cnz);
-        cp[ci] = 0.0f;
-        float rhs = 0.0f;
-        if (interior(I, J, K, cnx, cny, cnz)) {
-#pragma unroll
-            for (int ch = 0; ch < 8; ++ch) {
-                const int di = ch >> 2, dj = (ch >> 1) & 1, dk = ch & 1;
-                const int i = 2 * I - 1 + di, j = 2 * J - 1 + dj, k = 2 * K - 1 + dk;
-                if (!interior(i, j, k, fnx, fny, fnz)) continue;
-                const int q = ((i - gi) * RS_PJ + (j - gj)) * RS_PK + (k - gk);
-                const uint32_t o = s_o[q];
-                if (!(o & 64u)) continue;
-                const float ws = bitf(o, 3) * s_p[q + RS_PJ * RS_PK] + bitf(s_o[q - RS_PJ * RS_PK], 3) * s_p[q - RS_PJ * RS_PK] +
-                                 bitf(o, 4) * s_p[q + RS_PK] + bitf(s_o[q - RS_PK], 4) * s_p[q - RS_PK] +
-                                 bitf(o, 5) * s_p[q + 1] + bitf(s_o[q - 1], 5) * s_p[q - 1];
-                const float ap = (ws - (float)(o & 7u) * s_p[q]) * inv_delta2;
-                const int qb = ((i - gi - 1) * RS_BJ + (j - gj - 1)) * RS_BK + (k - gk - 1);
-                rhs += s_b[qb] - ap;
-            }
-        }
-        cb[ci] = rhs;
-    }
-}
-
 // Prolongation (prolong_at) into the fine cells of the listed fine tiles (TK = 32 VEC cells along k).
 // V4 (finest level, VEC = 4; the caller checked that x is 16-byte and the operator 4-byte aligned):
 // each thread's four cells as vectors.
