@@ -99,6 +99,7 @@ SIGNATURES: dict[str, list[Any]] = {
     "clb_mg_residual_partials": [L],
     "clb_mg_tile_capacity": [I, I, I, I],
     "clb_mg_fused_tile_capacity": [I, I, I],
+    "clb_mg_cluster_list_capacity": [P],
     "clb_mg_residual_norms": [P, I, P, P, F, I, I, I, P, P, P, P],
     "clb_mg_ir_init": [P, P, P, I, I, I, P],
     "clb_mg_ir_step": [P, P, P, P, P, F, I, I, I, P, P, P, P],
@@ -132,6 +133,7 @@ _RESTYPES = {
     "clb_launch_count": ctypes.c_int64,
     "clb_mg_tile_capacity": ctypes.c_int64,
     "clb_mg_fused_tile_capacity": ctypes.c_int64,
+    "clb_mg_cluster_list_capacity": ctypes.c_int64,
 }
 
 
@@ -158,6 +160,7 @@ class MGHierarchy(ctypes.Structure):
         ("zero_outside", ctypes.c_int32),
         ("fused_tiles", ctypes.c_void_p),
         ("fused_tile_count", ctypes.c_void_p),
+        ("cluster_lists", ctypes.c_void_p),
     ]
 
 

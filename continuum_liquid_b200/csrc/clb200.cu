@@ -709,6 +709,55 @@ static int check_hierarchy(const clb_mg_hierarchy* h) {
 
 static inline bool is_half(const clb_mg_hierarchy* h, int l) { return h->fp16_level > 0 && l >= h->fp16_level; }
 
+// The cluster launch that runs the visits of the third-coarsest level `level` with both bottom levels
+// (mg_cluster.cuh), whatever the launch options: false when these levels cannot run as one (their
+// storage types differ, or they do not fit).
+struct ClusterShape {
+    int cs;        // slab CTAs (the cluster has cs + 1)
+    int ka, ns;    // A slots and C slots of each colour per thread
+    size_t bytes;  // dynamic shared memory per CTA
+    bool half;
+};
+
+static bool cluster_shape(const clb_mg_hierarchy* h, int level, ClusterShape& out) {
+    if (level < 1 || level != h->levels - 3) return false;
+    const bool half = is_half(h, level);
+    if (is_half(h, level + 1) != half || is_half(h, level + 2) != half) return false;
+    const int* c = h->shape[level];
+    const int* a = h->shape[level + 1];
+    const int* b = h->shape[level + 2];
+    const int sa = colour_slots(a[0], a[1], a[2]), sb = colour_slots(b[0], b[1], b[2]);
+    const int ka = (sa + BOTTOM_THREADS - 1) / BOTTOM_THREADS, kb = (sb + BOTTOM_BTHREADS - 1) / BOTTOM_BTHREADS;
+    if (kb > 1 || ka > 4) return false;
+    const int pairs = (c[0] - 1) / 2;
+    const int cs = pairs < CLUSTER_MAX - 1 ? pairs : CLUSTER_MAX - 1;
+    if (cs < 1) return false;
+    const ClusterLayout L = cluster_layout(cs, c[0], c[1], c[2], half);
+    const size_t bottom = bottom_smem_bytes(a[0] * a[1] * a[2], b[0] * b[1] * b[2]);
+    const size_t bytes = L.slab_bytes > bottom ? L.slab_bytes : bottom;
+    if (bytes > kBottomSmemLimit) return false;
+    const long long slots = (long long)L.own_max * (c[1] - 2) * ((c[2] - 1) / 2);
+    const int ns = (int)((slots + BOTTOM_THREADS - 1) / BOTTOM_THREADS);
+    if (ns > 8) return false;
+    out = ClusterShape{cs, ka, ns, bytes, half};
+    return true;
+}
+
+static int64_t cluster_list_ints(const clb_mg_hierarchy* h, const ClusterShape& cl) {
+    const int level = h->levels - 3;
+    const int* c = h->shape[level];
+    const int* a = h->shape[level + 1];
+    const int* b = h->shape[level + 2];
+    return cluster_lists_bottom_ints(a[0] * a[1] * a[2], b[0] * b[1] * b[2]) +
+           (int64_t)cl.cs * cluster_lists_slab_ints(cluster_layout(cl.cs, c[0], c[1], c[2], cl.half));
+}
+
+int64_t clb_mg_cluster_list_capacity(const clb_mg_hierarchy* h) {
+    ClusterShape cl;
+    if (!h || h->levels < 4 || h->levels > CLB_MG_MAX_LEVELS || !cluster_shape(h, h->levels - 3, cl)) return 0;
+    return cluster_list_ints(h, cl);
+}
+
 int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream) {
     if (check_hierarchy(h)) return 1;
     cudaStream_t s = CLB_STREAM(stream);
@@ -767,6 +816,23 @@ int clb_mg_build_coarse(const clb_mg_hierarchy* h, void* stream) {
                                                       h->fused_tiles, h->fused_tile_count);
             CLB_LAUNCH_CHECK("k_l0_fused_tiles");
         }
+    }
+    ClusterShape cl;
+    if (h->cluster_lists && cluster_shape(h, h->levels - 3, cl)) {
+        const int level = h->levels - 3;
+        const int* c = h->shape[level];
+        const int* a = h->shape[level + 1];
+        const int* b = h->shape[level + 2];
+#define CLB_CLUSTER_LISTS(H)                                                                                    \
+    launch(cl.cs + 1, BOTTOM_THREADS, 0, s)(k_cluster_lists<H>, h->cluster_lists, (const void*)h->op[level],     \
+                                            (const uint8_t*)h->mask[level], c[0], c[1], c[2],                    \
+                                            (const void*)h->op[level + 1], (const uint8_t*)h->mask[level + 1],   \
+                                            a[0], a[1], a[2], (const void*)h->op[level + 2],                     \
+                                            (const uint8_t*)h->mask[level + 2], b[0], b[1], b[2], cl.cs)
+        if (cl.half) CLB_CLUSTER_LISTS(true);
+        else CLB_CLUSTER_LISTS(false);
+#undef CLB_CLUSTER_LISTS
+        CLB_LAUNCH_CHECK("k_cluster_lists");
     }
     return 0;
 }
@@ -1027,7 +1093,7 @@ static int launch_cluster_visit(const clb_mg_hierarchy* h, int level, int csize,
                              (const float4*)h->op[level + 1], (const uint8_t*)h->mask[level + 1], a[0], a[1], a[2],
                              (const float4*)h->op[level + 2], (const uint8_t*)h->mask[level + 2], b[0], b[1], b[2],
                              h->delta, pre, post, coarse_iters, (const float*)h->fp16_scale, visits,
-                             visits_of(level + 1), visits_of(level + 2));
+                             visits_of(level + 1), visits_of(level + 2), (const int*)h->cluster_lists);
     return check_launch("k_cluster_visit") ? -1 : 1;
 }
 }  // extern "C++"
@@ -1037,24 +1103,11 @@ static int launch_cluster_visit(const clb_mg_hierarchy* h, int level, int csize,
 // if it launched, 0 if the caller must go on level by level, -1 on error.
 int cluster_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int coarse_iters, cudaStream_t s,
                   int visits = 1) {
-    if (!g_use_cluster || !g_use_bottom || level < 1 || level != h->levels - 3) return 0;
-    const bool half = is_half(h, level);
-    if (is_half(h, level + 1) != half || is_half(h, level + 2) != half) return 0;
-    const int* c = h->shape[level];
-    const int* a = h->shape[level + 1];
-    const int* b = h->shape[level + 2];
-    const int sa = colour_slots(a[0], a[1], a[2]), sb = colour_slots(b[0], b[1], b[2]);
-    const int ka = (sa + BOTTOM_THREADS - 1) / BOTTOM_THREADS, kb = (sb + BOTTOM_BTHREADS - 1) / BOTTOM_BTHREADS;
-    if (kb > 1 || ka > 4) return 0;
-    const int pairs = (c[0] - 1) / 2;
-    const int cs = pairs < CLUSTER_MAX - 1 ? pairs : CLUSTER_MAX - 1;
-    if (cs < 1) return 0;
-    const ClusterLayout L = cluster_layout(cs, c[0], c[1], c[2], half);
-    const size_t bottom = bottom_smem_bytes(a[0] * a[1] * a[2], b[0] * b[1] * b[2]);
-    const size_t bytes = L.slab_bytes > bottom ? L.slab_bytes : bottom;
-    if (bytes > kBottomSmemLimit) return 0;
-    const long long slots = (long long)L.own_max * (c[1] - 2) * ((c[2] - 1) / 2);
-    const int ns = (int)((slots + BOTTOM_THREADS - 1) / BOTTOM_THREADS);
+    ClusterShape cl;
+    if (!g_use_cluster || !g_use_bottom || !cluster_shape(h, level, cl)) return 0;
+    const int cs = cl.cs, ka = cl.ka, ns = cl.ns;
+    const size_t bytes = cl.bytes;
+    const bool half = cl.half;
 #define CLB_CLUSTER(NS, KA, H) \
     launch_cluster_visit<NS, KA, 1, H>(h, level, cs + 1, bytes, pre, post, coarse_iters, visits, s)
 #define CLB_CLUSTER_KINDS(H)                                  \

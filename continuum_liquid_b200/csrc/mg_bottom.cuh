@@ -203,65 +203,93 @@ __device__ __forceinline__ void bottom_stage(const BottomSmem& S, const float* _
     }
 }
 
-// One visit of A from staged shared memory: pre-smoothing of
-// A, restriction into B (B's p zeroed, multigrid.cl:114), the two coarse solves of B, prolongation,
-// post-smoothing of A. bb (nullable): B's right-hand side is stored there (FP16 when H). KA: A slots of
-// each colour per thread (of BOTTOM_THREADS); KB: B slots of each colour per B thread.
-template <int KA, int KB, bool H>
-__device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int any, int anz, int bnx, int bny, int bnz,
-                                            float d2, float inv_delta2, int pre, int post, int coarse_iters,
-                                            float* __restrict__ bb, int b_solves = 2) {
-    float* spa = S.spa;
-    const float* sba = S.sba;
-    const float4* soa = S.soa;
-    float* spb = S.spb;
-    const float4* sob = S.sob;
-    const int CB = bnx * bny * bnz;
-    auto st = [&](float* a, int c, float v) {
-        if (H) reinterpret_cast<__half*>(a)[c] = __float2half_rn(v);
-        else a[c] = v;
-    };
-    __syncthreads();  // staging and the caller's writes to shared memory are complete
+// The cells a thread owns in a bottom visit: A cells of each colour (index, diagonal, delta^2 * b) and
+// B cells of each colour with their neighbour weights. Index, diagonal and weights depend on the
+// operators only, so a launch that visits A several times sets them once (bottom_cells); A's delta^2 * b
+// is set again whenever A's right-hand side changes (bottom_rhs).
+template <int KA, int KB>
+struct BottomCells {
+    OwnedCell A[2][KA];   // [colour][m]: the thread's fluid cells (bottom_lists)
+    OwnedCellW B[2][KB];  // [colour][m]
+};
 
-    const int asx = any * anz, asy = anz, bsx = bny * bnz, bsy = bnz;
-    const int la = (anx * any * anz) / 2 + 1, lb = CB / 2 + 1;
-    OwnedCell A[2][KA];  // [colour][m]: the thread's fluid cells (bottom_lists)
+// After the lists are built and the block has synchronised.
+template <int KA, int KB>
+__device__ __forceinline__ void bottom_cells(const BottomSmem& S, BottomCells<KA, KB>& R, int anx, int any, int anz,
+                                             int bnx, int bny, int bnz) {
+    const int la = (anx * any * anz) / 2 + 1, lb = (bnx * bny * bnz) / 2 + 1;
+    const int bsx = bny * bnz, bsy = bnz;
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KA; ++m) {
             const int r = threadIdx.x + m * BOTTOM_THREADS;
             const int c = r < S.count[colour] ? S.list_a[colour * la + r] : -1;
-            OwnedCell& o = A[colour][m];
+            OwnedCell& o = R.A[colour][m];
             o.c = c < 0 ? 0 : c;
-            o.d = c < 0 ? -1.0f : soa[c].x;  // fluid: >= 0
-            o.d2b = c < 0 ? 0.0f : d2 * sba[c];
+            o.d = c < 0 ? -1.0f : S.soa[c].x;  // fluid: >= 0
+            o.d2b = 0.0f;
         }
     const bool btile = threadIdx.x < BOTTOM_BTHREADS;
-    OwnedCellW B[2][KB];  // [colour][m]
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < KB; ++m) {
             const int r = threadIdx.x + m * BOTTOM_BTHREADS;
             const int c = btile && r < S.count[2 + colour] ? S.list_b[colour * lb + r] : -1;
-            OwnedCellW& o = B[colour][m];
+            OwnedCellW& o = R.B[colour][m];
             o.d2b = 0.0f;
             o.c = 0;
             o.d = -1.0f;
             o.wxp = o.wxm = o.wyp = o.wym = o.wzp = o.wzm = 0.0f;
             if (c >= 0) {
-                const float4 self = sob[c];
+                const float4 self = S.sob[c];
                 o.c = c;
                 o.d = self.x;
                 o.wxp = self.y;
                 o.wyp = self.z;
                 o.wzp = self.w;
-                o.wxm = sob[c - bsx].y;
-                o.wym = sob[c - bsy].z;
-                o.wzm = sob[c - 1].w;
+                o.wxm = S.sob[c - bsx].y;
+                o.wym = S.sob[c - bsy].z;
+                o.wzm = S.sob[c - 1].w;
             }
         }
+}
+
+// A's delta^2 * b of the owned cells, after A's right-hand side is in shared memory and visible.
+template <int KA, int KB>
+__device__ __forceinline__ void bottom_rhs(const BottomSmem& S, BottomCells<KA, KB>& R, float d2) {
+#pragma unroll
+    for (int colour = 0; colour < 2; ++colour)
+#pragma unroll
+        for (int m = 0; m < KA; ++m) {
+            OwnedCell& o = R.A[colour][m];
+            o.d2b = o.d < 0.0f ? 0.0f : d2 * S.sba[o.c];
+        }
+}
+
+// One visit of A from staged shared memory with the owned cells set (bottom_cells, bottom_rhs):
+// pre-smoothing of A, restriction into B (B's p zeroed, multigrid.cl:114), the two coarse solves of B,
+// prolongation, post-smoothing of A. bb (nullable): B's right-hand side is stored there (FP16 when H).
+// KA: A slots of each colour per thread (of BOTTOM_THREADS); KB: B slots of each colour per B thread.
+template <int KA, int KB, bool H>
+__device__ __forceinline__ void bottom_core(const BottomSmem& S, BottomCells<KA, KB>& R, int anx, int any, int anz,
+                                            int bnx, int bny, int bnz, float d2, float inv_delta2, int pre, int post,
+                                            int coarse_iters, float* __restrict__ bb, int b_solves = 2) {
+    float* spa = S.spa;
+    const float* sba = S.sba;
+    const float4* soa = S.soa;
+    float* spb = S.spb;
+    const int CB = bnx * bny * bnz;
+    auto st = [&](float* a, int c, float v) {
+        if (H) reinterpret_cast<__half*>(a)[c] = __float2half_rn(v);
+        else a[c] = v;
+    };
+    const int asx = any * anz, asy = anz, bsx = bny * bnz, bsy = bnz;
+    const int lb = CB / 2 + 1;
+    OwnedCell (&A)[2][KA] = R.A;
+    OwnedCellW (&B)[2][KB] = R.B;
+    const bool btile = threadIdx.x < BOTTOM_BTHREADS;
 
     auto smooth_a = [&](int iterations) {
         for (int it = 0; it < iterations; ++it)
@@ -274,47 +302,41 @@ __device__ __forceinline__ void bottom_core(const BottomSmem& S, int anx, int an
             }
     };
 
-    __syncthreads();
+    __syncthreads();  // staging and the caller's writes to shared memory are complete
     smooth_a(pre);
     // restriction of the residual (multigrid.cl:90-180, right-hand-side part) of B's fluid cells (both
-    // lists): eight threads per coarse cell, thread l forms the residual of child l = 4 di + 2 dj + dk
-    // (interior fluid children only), and the group's first thread adds them in that order, as one
-    // thread running over di, dj, dk does. The sums go to B's p (free until the coarse solves), from
-    // which B's owners take them.
+    // lists), one thread per coarse cell: the residuals of the eight children l = 4 di + 2 dj + dk are
+    // formed independently (interior fluid children only) and added in that order, as the reference's
+    // loop over di, dj, dk adds them. The sums go to B's p (free until the coarse solves), from which B's
+    // owners take them.
     {
-        const int lane = threadIdx.x & 31, l = threadIdx.x & 7;
         const int n0 = S.count[2], nb = n0 + S.count[3];
-        for (int g0 = 0; g0 < nb; g0 += BOTTOM_THREADS / 8) {  // the same trip count in every thread
-            const int g = g0 + (int)(threadIdx.x >> 3);
-            int cb = -1;
-            float r = 0.0f;
-            bool present = false;
-            if (g < nb) {
-                cb = g < n0 ? S.list_b[g] : S.list_b[lb + g - n0];
-                const int I = cb / bsx, J = (cb / bsy) % bny, K = cb % bnz;
+        for (int g = threadIdx.x; g < nb; g += BOTTOM_THREADS) {
+            const int cb = g < n0 ? S.list_b[g] : S.list_b[lb + g - n0];
+            const int I = cb / bsx, J = (cb / bsy) % bny, K = cb % bnz;
+            float r[8];
+            bool present[8];
+#pragma unroll
+            for (int l = 0; l < 8; ++l) {
                 const int i = 2 * I - 1 + (l >> 2), j = 2 * J - 1 + ((l >> 1) & 1), k = 2 * K - 1 + (l & 1);
+                r[l] = 0.0f;
+                present[l] = false;
                 if (interior(i, j, k, anx, any, anz)) {
                     const int f = (i * any + j) * anz + k;
                     const float4 o = soa[f];
                     if (o.x >= 0.0f) {
                         const float ws = o.y * spa[f + asx] + soa[f - asx].y * spa[f - asx] + o.z * spa[f + asy] +
                                          soa[f - asy].z * spa[f - asy] + o.w * spa[f + 1] + soa[f - 1].w * spa[f - 1];
-                        r = sba[f] - (ws - o.x * spa[f]) * inv_delta2;
-                        present = true;
+                        r[l] = sba[f] - (ws - o.x * spa[f]) * inv_delta2;
+                        present[l] = true;
                     }
                 }
             }
-            const unsigned have = __ballot_sync(0xffffffffu, present) >> (lane & ~7);
-            float v[8];
+            float rhs = 0.0f;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) v[q] = __shfl_sync(0xffffffffu, r, (lane & ~7) + q);
-            if (l == 0 && cb >= 0) {
-                float rhs = 0.0f;
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if ((have >> q) & 1u) rhs += v[q];
-                spb[cb] = rhs;
-            }
+            for (int l = 0; l < 8; ++l)
+                if (present[l]) rhs += r[l];
+            spb[cb] = rhs;
         }
     }
     __syncthreads();
@@ -389,7 +411,10 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
     };
     bottom_stage<H>(S, pa, ba, opa, ma, CA, opb, mb, CB);
     bottom_lists(S, anx, any, anz, bnx, bny, bnz);
-    bottom_core<KA, KB, H>(S, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, bb, b_solves);
+    BottomCells<KA, KB> R;
+    bottom_cells(S, R, anx, any, anz, bnx, bny, bnz);
+    bottom_rhs(S, R, d2);
+    bottom_core<KA, KB, H>(S, R, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, bb, b_solves);
     const int bsx = bny * bnz, bsy = bnz;
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) st(pa, c, S.spa[c]);
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {

@@ -84,6 +84,18 @@ __host__ __device__ __forceinline__ ClusterLayout cluster_layout(int cs, int nx,
     return L;
 }
 
+// Fluid-cell lists of a cluster launch in global memory (clb_mg_hierarchy.cluster_lists), built once
+// per solve by k_cluster_lists: first the first CTA's count and list arrays as they lie in its shared
+// memory (BottomSmem from `count` on: four counts, A's two lists of CA / 2 + 1 entries, B's two of
+// CB / 2 + 1), then per slab its two lists of list_len entries and its two counts (the slab's list
+// region); each part padded to a multiple of four entries.
+__host__ __device__ __forceinline__ long long cluster_lists_bottom_ints(int CA, int CB) {
+    return (4LL + 2 * (CA / 2 + 1) + 2 * (CB / 2 + 1) + 3) & ~3LL;
+}
+__host__ __device__ __forceinline__ long long cluster_lists_slab_ints(const ClusterLayout& L) {
+    return (2LL * L.list_len + 2 + 3) & ~3LL;
+}
+
 // Owned C cell: local shared-memory index, diagonal (-1: not updated) and delta^2 * b.
 struct SlabCell {
     int c;
@@ -91,11 +103,13 @@ struct SlabCell {
     float d2b;
 };
 
+// glist (nullable): the slab's part of the lists built by k_cluster_lists.
 template <int NS, bool H>
 __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, float* __restrict__ pc_out,
                                   const float* __restrict__ bc, const void* __restrict__ opc_,
                                   const uint8_t* __restrict__ mc, int nx, int ny, int nz, int anx, int any, int anz,
-                                  float d2, float inv_delta2, int pre, int post, int visits) {
+                                  float d2, float inv_delta2, int pre, int post, int visits,
+                                  const int* __restrict__ glist) {
     namespace cgx = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem[];
     using OpT = typename std::conditional<H, uint2, float4>::type;
@@ -134,27 +148,34 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
     __syncthreads();
 
     // owned cells: the slab's fluid cells of each colour (the slab seen as a level of np planes; the
-    // local plane il is global plane il + i_lo - 1), listed in arbitrary order and taken in turn by the
-    // threads, so only a warp's last owned slots can be empty (bottom_lists)
-    const int flip = (sl.i_lo - 1) & 1;
+    // local plane il is global plane il + i_lo - 1), taken in turn by the threads, so only a warp's last
+    // owned slots can be empty (bottom_lists). From glist when given (k_cluster_lists, in slot order),
+    // otherwise listed here in arbitrary order; cells of one colour are independent, so the order does
+    // not change any value.
     int* list = reinterpret_cast<int*>(smem + L.list_off);
-    int* count = list + 2 * L.list_len;
-    if (threadIdx.x < 2) count[threadIdx.x] = 0;
+    const int* src = glist;
+    if (!glist) {
+        const int flip = (sl.i_lo - 1) & 1;
+        int* count = list + 2 * L.list_len;
+        if (threadIdx.x < 2) count[threadIdx.x] = 0;
+        __syncthreads();
+        const int slots = colour_slots(np, ny, nz);
+        for (int colour = 0; colour < 2; ++colour)
+            for (int r = threadIdx.x; r < slots; r += BOTTOM_THREADS) {
+                const int c = colour_cell(r, colour ^ flip, np, ny, nz);
+                if (c >= 0 && op4(c).x >= 0.0f) list[colour * L.list_len + atomicAdd(count + colour, 1)] = c;
+            }
+        src = list;
+    }
     __syncthreads();
-    const int slots = colour_slots(np, ny, nz);
-    for (int colour = 0; colour < 2; ++colour)
-        for (int r = threadIdx.x; r < slots; r += BOTTOM_THREADS) {
-            const int c = colour_cell(r, colour ^ flip, np, ny, nz);
-            if (c >= 0 && op4(c).x >= 0.0f) list[colour * L.list_len + atomicAdd(count + colour, 1)] = c;
-        }
-    __syncthreads();
+    const int counts[2] = {src[2 * L.list_len], src[2 * L.list_len + 1]};
     SlabCell C[2][NS];
 #pragma unroll
     for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
         for (int m = 0; m < NS; ++m) {
             const int r = threadIdx.x + m * BOTTOM_THREADS;
-            const int c = r < count[colour] ? list[colour * L.list_len + r] : -1;
+            const int c = r < counts[colour] ? src[colour * L.list_len + r] : -1;
             SlabCell& o = C[colour][m];
             o.c = c < 0 ? 0 : c;
             o.d = c < 0 ? -1.0f : op4(c).x;
@@ -204,7 +225,9 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
     }
 
     // restriction of the residual into A's b in the first CTA (multigrid.cl:90-180; FP16:
-    // k_restrict_h<2>, rounded to FP16 as stored there)
+    // k_restrict_h<2>, rounded to FP16 as stored there). The residuals of the eight children
+    // l = 4 di + 2 dj + dk are formed independently (interior fluid children only) and added in that
+    // order, as the reference's loop over di, dj, dk adds them.
     {
         const int CA = anx * any * anz;
         const BottomSmem S = bottom_smem(cluster.map_shared_rank(smem, 0u), CA, 1);
@@ -212,20 +235,29 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
         const int my = any - 2, mz = anz - 2;
         for (int t = threadIdx.x; t < (I1 - I0) * my * mz; t += BOTTOM_THREADS) {
             const int I = I0 + t / (my * mz), r = t % (my * mz), J = 1 + r / mz, K = 1 + r % mz;
-            float rhs = 0.0f;
             if (I <= anx - 2) {
-                for (int di = 0; di < 2; ++di)
-                    for (int dj = 0; dj < 2; ++dj)
-                        for (int dk = 0; dk < 2; ++dk) {
-                            const int i = 2 * I - 1 + di, j = 2 * J - 1 + dj, k = 2 * K - 1 + dk;
-                            if (!interior(i, j, k, nx, ny, nz)) continue;
-                            const int f = ((i - sl.i_lo + 1) * ny + j) * nz + k;
-                            const float4 o = op4(f);
-                            if (o.x < 0.0f) continue;  // not fluid
+                float res[8];
+                bool present[8];
+#pragma unroll
+                for (int l = 0; l < 8; ++l) {
+                    const int i = 2 * I - 1 + (l >> 2), j = 2 * J - 1 + ((l >> 1) & 1), k = 2 * K - 1 + (l & 1);
+                    res[l] = 0.0f;
+                    present[l] = false;
+                    if (interior(i, j, k, nx, ny, nz)) {
+                        const int f = ((i - sl.i_lo + 1) * ny + j) * nz + k;
+                        const float4 o = op4(f);
+                        if (o.x >= 0.0f) {  // fluid
                             const float ws = o.y * sp[f + PL] + op4(f - PL).y * sp[f - PL] + o.z * sp[f + nz] +
                                              op4(f - nz).z * sp[f - nz] + o.w * sp[f + 1] + op4(f - 1).w * sp[f - 1];
-                            rhs += sb[f - PL] - (ws - o.x * sp[f]) * inv_delta2;
+                            res[l] = sb[f - PL] - (ws - o.x * sp[f]) * inv_delta2;
+                            present[l] = true;
                         }
+                    }
+                }
+                float rhs = 0.0f;
+#pragma unroll
+                for (int l = 0; l < 8; ++l)
+                    if (present[l]) rhs += res[l];
                 S.sba[(I * any + J) * anz + K] = stored(rhs);
             }
         }
@@ -233,10 +265,39 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
     cluster_barrier();  // A's right-hand side is complete
     cluster_barrier();  // the first CTA finished both visits of A
 
-    // prolongation (multigrid.cl:182-201) from A's p in the first CTA
+    // prolongation (multigrid.cl:182-201) from A's p in the first CTA. The owned planes' parents lie in
+    // A's planes [I_lo, I_hi]; they are first copied into the list region (free once the owned cells
+    // are in registers) with every remote load of a thread issued before its stores, so each owned cell
+    // then reads its parent from this CTA's shared memory instead of waiting on a remote load.
     {
-        const int CA = anx * any * anz;
+        const int CA = anx * any * anz, APL = any * anz;
         const float* spa = bottom_smem(cluster.map_shared_rank(smem, 0u), CA, 1).spa;
+        const int I_lo = min(sl.p0 + 1, anx - 2), I_hi = min(sl.p1, anx - 2);
+        const int n_a = (I_hi - I_lo + 1) * APL;
+        const bool local = n_a > 0 && n_a <= 2 * L.list_len;  // uniform over the CTA
+        const float* parent = spa;
+        int base = 0;
+        if (local) {
+            float* sa = reinterpret_cast<float*>(list);
+            const float* src = spa + (size_t)I_lo * APL;
+            constexpr int U = 4;
+            for (int q0 = threadIdx.x; q0 < n_a; q0 += U * BOTTOM_THREADS) {
+                float v[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int q = q0 + u * BOTTOM_THREADS;
+                    v[u] = q < n_a ? src[q] : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int q = q0 + u * BOTTOM_THREADS;
+                    if (q < n_a) sa[q] = v[u];
+                }
+            }
+            __syncthreads();
+            parent = sa;
+            base = I_lo * APL;
+        }
 #pragma unroll
         for (int colour = 0; colour < 2; ++colour)
 #pragma unroll
@@ -248,7 +309,7 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
                 const int i = il + sl.i_lo - 1;
                 const int I = min((i - 1) / 2 + 1, anx - 2), J = min((j - 1) / 2 + 1, any - 2),
                           K = min((k - 1) / 2 + 1, anz - 2);
-                sp[c] = stored(sp[c] + spa[(I * any + J) * anz + K]);
+                sp[c] = stored(sp[c] + parent[(I * any + J) * anz + K - base]);
             }
     }
     push();
@@ -271,23 +332,39 @@ __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __rest
                                     const uint8_t* __restrict__ ma, int anx, int any, int anz,
                                     const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny,
                                     int bnz, float d2, float inv_delta2, int pre, int post, int coarse_iters,
-                                    int visits, int a_visits, int b_solves) {
+                                    int visits, int a_visits, int b_solves, const int* __restrict__ glist) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     const BottomSmem S = bottom_smem(smem, CA, CB);
     bottom_stage<H>(S, nullptr, nullptr, opa, ma, CA, opb, mb, CB);
-    bottom_lists(S, anx, any, anz, bnx, bny, bnz);
-    for (int visit_c = 0; visit_c < visits; ++visit_c) {
-    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
-        S.spa[c] = 0.0f;  // restriction zeroes the coarse pressure (multigrid.cl:114)
-        S.sba[c] = 0.0f;  // cells the restriction does not write (non-interior) hold 0
+    if (glist) {
+        // the counts and lists as k_cluster_lists built them (16-byte aligned at both ends; the padded
+        // length fits the shared list region, bottom_smem_bytes)
+        const int n4 = (int)(cluster_lists_bottom_ints(CA, CB) / 4);
+        const int4* from = reinterpret_cast<const int4*>(glist);
+        int4* to = reinterpret_cast<int4*>(S.count);
+        for (int q = threadIdx.x; q < n4; q += BOTTOM_THREADS) to[q] = from[q];
+        __syncthreads();
+    } else {
+        bottom_lists(S, anx, any, anz, bnx, bny, bnz);
     }
-    cluster_barrier();  // staged (for a later visit of C: the slabs finished reading A's p)
+    BottomCells<KA, KB> R;  // the owned cells and B's weights, set once for every visit of A
+    bottom_cells(S, R, anx, any, anz, bnx, bny, bnz);
+    // the restriction zeroes the coarse pressure (multigrid.cl:114) before every visit of A's parent;
+    // cells of b that the restriction does not write (not interior) hold 0, and the slabs write every
+    // interior cell of b in each visit of C, so b is zeroed once
+    for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
+        S.spa[c] = 0.0f;
+        S.sba[c] = 0.0f;
+    }
+    for (int visit_c = 0; visit_c < visits; ++visit_c) {
+    cluster_barrier();  // staged (for a later visit of C: A's p zeroed after the slabs read it)
     for (int it = 0; it < 2 * pre; ++it) cluster_barrier();  // the C-level pre-smoothing phases
     cluster_barrier();  // A's right-hand side is complete
+    bottom_rhs(S, R, d2);
     for (int visit = 0; visit < a_visits; ++visit) {  // two, or one when A is visited once
-        bottom_core<KA, KB, H>(S, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, nullptr,
-                               b_solves);
+        bottom_core<KA, KB, H>(S, R, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters,
+                               nullptr, b_solves);
         __syncthreads();
         if (H)  // A's p as the bottom visit stores it (FP16) before it is read again
             for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) S.spa[c] = __half2float(__float2half_rn(S.spa[c]));
@@ -295,6 +372,8 @@ __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __rest
     }
     cluster_barrier();  // both visits done; the slabs read A's p next
     cluster_barrier();  // prolongation done
+    if (visit_c + 1 < visits)  // the next visit's zero p, while the slabs post-smooth
+        for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) S.spa[c] = 0.0f;
     for (int it = 0; it < 2 * post; ++it) cluster_barrier();  // the C-level post-smoothing phases
     }  // visits of C
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) {
@@ -311,7 +390,7 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
                     const float4* __restrict__ opa, const uint8_t* __restrict__ ma, int anx, int any, int anz,
                     const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
                     float delta, int pre, int post, int coarse_iters, const float* __restrict__ scale,
-                    int visits, int a_visits, int b_solves) {
+                    int visits, int a_visits, int b_solves, const int* __restrict__ lists) {
     pdl_begin();
     const float d2 = H ? scale[2] : delta * delta;
     const float inv_delta2 = H ? scale[3] : 1.0f / (delta * delta);
@@ -319,10 +398,98 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
     const int cs = (int)cooperative_groups::this_cluster().num_blocks() - 1;
     if (rank == 0)
         cluster_bottom_path<KA, KB, H>(pa, opa, ma, anx, any, anz, opb, mb, bnx, bny, bnz, d2, inv_delta2, pre, post,
-                                       coarse_iters, visits, a_visits, b_solves);
+                                       coarse_iters, visits, a_visits, b_solves, lists);
     else
         cluster_slab_path<NS, H>((int)rank - 1, cs, pc, pc, bc, opc, mc, nx, ny, nz, anx, any, anz, d2, inv_delta2,
-                                 pre, post, visits);
+                                 pre, post, visits,
+                                 lists ? lists + cluster_lists_bottom_ints(anx * any * anz, bnx * bny * bnz) +
+                                             (rank - 1) * cluster_lists_slab_ints(cluster_layout(cs, nx, ny, nz, H))
+                                       : nullptr);
+}
+
+// Lists the fluid cells that the CTAs of a cluster launch own, as the launch would list them but in
+// slot order: block 0 those of A and B (bottom_lists), block s + 1 those of slab s (the launch's
+// per-slab lists). Once per solve, after the coarse operators are built; a cell is listed when the
+// diagonal the launch stages for it (-1 where not fluid) is not negative, the launch's own test.
+template <bool H>
+__global__ void __launch_bounds__(BOTTOM_THREADS)
+    k_cluster_lists(int* __restrict__ lists, const void* __restrict__ opc, const uint8_t* __restrict__ mc, int nx,
+                    int ny, int nz, const void* __restrict__ opa, const uint8_t* __restrict__ ma, int anx, int any,
+                    int anz, const void* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
+                    int cs) {
+    pdl_begin();
+    __shared__ int warp_n[BOTTOM_THREADS / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // appends the cells cell(r) >= 0 of slots r < slots to out in slot order; returns how many
+    auto compact = [&](int slots, auto cell, int* out) -> int {
+        int base = 0;
+        for (int r0 = 0; r0 < slots; r0 += BOTTOM_THREADS) {  // the same trip count in every thread
+            const int r = r0 + (int)threadIdx.x;
+            const int c = r < slots ? cell(r) : -1;
+            const unsigned ballot = __ballot_sync(0xffffffffu, c >= 0);
+            if (lane == 0) warp_n[w] = __popc(ballot);
+            __syncthreads();
+            int before = 0, all = 0;
+            for (int q = 0; q < BOTTOM_THREADS / 32; ++q) {
+                const int v = warp_n[q];
+                before += q < w ? v : 0;
+                all += v;
+            }
+            if (c >= 0) out[base + before + __popc(ballot & ((1u << lane) - 1u))] = c;
+            __syncthreads();
+            base += all;
+        }
+        return base;
+    };
+    auto diag = [](const void* op, const uint8_t* m, long long g) -> float {
+        if (!m[g]) return -1.0f;
+        if constexpr (H) return h4_to_f4(reinterpret_cast<const uint2*>(op)[g]).x;
+        else return reinterpret_cast<const float4*>(op)[g].x;
+    };
+    if (blockIdx.x == 0) {
+        const int CA = anx * any * anz, CB = bnx * bny * bnz, la = CA / 2 + 1, lb = CB / 2 + 1;
+        int* list_a = lists + 4;
+        int* list_b = list_a + 2 * la;
+        const int sa = colour_slots(anx, any, anz), sb = colour_slots(bnx, bny, bnz);
+        int n[4];
+#pragma unroll
+        for (int colour = 0; colour < 2; ++colour) {
+            n[colour] = compact(sa, [&](int r) {
+                const int c = colour_cell(r, colour, anx, any, anz);
+                return c >= 0 && diag(opa, ma, c) >= 0.0f ? c : -1;
+            }, list_a + colour * la);
+            n[2 + colour] = compact(sb, [&](int r) {
+                const int c = colour_cell(r, colour, bnx, bny, bnz);
+                return c >= 0 && diag(opb, mb, c) >= 0.0f ? c : -1;
+            }, list_b + colour * lb);
+        }
+        if (threadIdx.x == 0) {
+            lists[0] = n[0];
+            lists[1] = n[1];
+            lists[2] = n[2];
+            lists[3] = n[3];
+        }
+    } else {
+        const int s = (int)blockIdx.x - 1;
+        const ClusterLayout L = cluster_layout(cs, nx, ny, nz, H);
+        const Slab sl = cluster_slab(s, cs, nx);
+        const int np = sl.i_hi - sl.i_lo + 2, flip = (sl.i_lo - 1) & 1;
+        const long long g0 = (long long)(sl.i_lo - 1) * ny * nz;
+        int* list = lists + cluster_lists_bottom_ints(anx * any * anz, bnx * bny * bnz) +
+                    (long long)s * cluster_lists_slab_ints(L);
+        const int slots = colour_slots(np, ny, nz);
+        int n[2];
+#pragma unroll
+        for (int colour = 0; colour < 2; ++colour)
+            n[colour] = compact(slots, [&](int r) {
+                const int c = colour_cell(r, colour ^ flip, np, ny, nz);
+                return c >= 0 && diag(opc, mc, g0 + c) >= 0.0f ? c : -1;
+            }, list + colour * L.list_len);
+        if (threadIdx.x == 0) {
+            list[2 * L.list_len] = n[0];
+            list[2 * L.list_len + 1] = n[1];
+        }
+    }
 }
 
 }  // namespace clb

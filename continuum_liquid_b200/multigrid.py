@@ -16,6 +16,7 @@ Both give the reference's values bit for bit (tests compare them with the CPU re
 
 from __future__ import annotations
 
+import ctypes
 from typing import Any
 
 import numpy as np
@@ -236,6 +237,12 @@ class MultigridHierarchy:
             self.fused_tile_count = torch.zeros(1, dtype=torch.int32, device=device)
             self.struct.fused_tiles = self.fused_tiles.data_ptr()
             self.struct.fused_tile_count = self.fused_tile_count.data_ptr()
+        # the fluid cells of the three coarsest levels for the one-launch visits of the third-coarsest
+        # level (csrc/mg_cluster.cuh), listed once per solve by build_coarse
+        cap = int(kernels.lib.clb_mg_cluster_list_capacity(ctypes.byref(self.struct)))
+        self.cluster_lists = torch.zeros(max(cap, 1), dtype=torch.int32, device=device) if cap > 0 else None
+        if self.cluster_lists is not None:
+            self.struct.cluster_lists = self.cluster_lists.data_ptr()
         for l in range(1, levels):
             if self.is_fp16(l):
                 self.struct.sweep[l] = 4

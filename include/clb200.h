@@ -309,6 +309,11 @@ typedef struct clb_mg_hierarchy {
      * cell (1, 1, 1)) that sweep kind 7 walks; clb_mg_build_coarse lists them. NULL: kind 7 runs as 1. */
     int32_t* fused_tiles;                /* clb_mg_fused_tile_capacity(level-0 shape) entries */
     int32_t* fused_tile_count;           /* device int32: listed tiles */
+    /* No counterpart in the reference: the fluid cells of each colour of the three coarsest levels, as
+     * the one-launch visits of the third-coarsest level (a thread-block cluster) own them;
+     * clb_mg_build_coarse lists them once per solve, so a launch does not. NULL: every launch lists
+     * them itself (the same cells). */
+    int32_t* cluster_lists;              /* clb_mg_cluster_list_capacity(h) entries */
 } clb_mg_hierarchy;
 
 /* Number of tiles of a level of nx x ny x nz cells (finest != 0: the finest level's tile shape). */
@@ -316,6 +321,10 @@ int64_t clb_mg_tile_capacity(int nx, int ny, int nz, int finest);
 
 /* Number of 3-D fluid tiles of level 0 (clb_mg_hierarchy.fused_tiles) for nx x ny x nz cells. */
 int64_t clb_mg_fused_tile_capacity(int nx, int ny, int nz);
+
+/* Entries of clb_mg_hierarchy.cluster_lists for the hierarchy's levels and shapes (0 when the visits of
+ * its third-coarsest level do not run as one cluster launch). */
+int64_t clb_mg_cluster_list_capacity(const clb_mg_hierarchy* h);
 
 /* pressure_solve.cl:3-24 pressure_rhs fused with multigrid.cl:63-88 build_finest_operator, writing
  * the packed level-0 operator. */
