@@ -41,6 +41,8 @@ UNIT = "steps/s"
 TOL = 1e-6
 COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarsest-level iterations
 SMOOTHING_CHOICES = ((2, 4), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
+# factor of every prolonged correction in the W-cycle preconditioner; 1.0: the reference's prolongation
+PROLONG_SCALE_CHOICES = (1.0, 1.7)
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
                      "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
@@ -79,6 +81,10 @@ def parse_args():
                     help="red-black iterations before,after the coarse-grid correction in the W-cycle preconditioner "
                          "of the timed steps, e.g. 2,4 (auto: the fastest of 2,4 (the reference's), 1,2 and 1,1 to the "
                          "tolerance in the Poisson comparison, with 4 coarsest-level iterations)")
+    ap.add_argument("--prolong-scale", default="auto",
+                    help="factor of every correction the W-cycle preconditioner of the timed steps prolongs (1: the "
+                         "reference's piecewise-constant prolongation; auto: 1.7 when it is the fastest to the tolerance "
+                         "with 4 coarsest-level iterations in the Poisson comparison, together with its smoothing)")
     ap.add_argument("--single-visit", type=int, default=0,
                     help="first multigrid level visited once (not twice) per visit of the level above in the W-cycle "
                          "preconditioner (0 = the reference's W-cycle; at 256^3 levels 3 and 2 need 20 and 27 FCG "
@@ -427,8 +433,10 @@ def workload_config(size, n_particles, args):
     }
 
 
-def solver_description(method, pre, post, k, fp16_levels=None, single_from=0):
+def solver_description(method, pre, post, k, fp16_levels=None, single_from=0, prolong_scale=1.0):
     storage = f", levels {fp16_levels[0][0]}^3 and coarser stored in FP16" if fp16_levels else ""
+    if prolong_scale != 1.0:
+        storage += f", prolonged corrections x{prolong_scale:g}"
     cycle = "W-cycle" if not single_from else f"W-cycle (levels {single_from}+ visited once per parent visit)"
     if method == "fcg":
         return (f"flexible CG preconditioned by one {cycle} computed in FP32 (pre {pre}, post {post}, coarse "
@@ -504,17 +512,19 @@ CPU_FCG = {"coarse_iterations": 4, "pre_smooth": 1, "post_smooth": 1}
 REFERENCE_FIXED_CYCLES = 6
 
 
-def cpu_sim(scene, positions, velocities, tol=TOL, cycles=None):
+def cpu_sim(scene, positions, velocities, tol=TOL, cycles=None, prolong_scale=1.0):
     """The reference algorithm on the host cores: the oracle (every reference kernel restated in C++
     with OpenMP, the step order of solver.py:243-529). With ``tol`` each pressure is solved to that
     FP64 relative residual by the flexible CG with the reference's W-cycle as preconditioner (the same
     work as the GPU's timed step); with ``cycles`` by the reference's own method, that fixed number of
-    FP32 W-cycles."""
+    FP32 W-cycles. ``prolong_scale``: the factor of the W-cycle's prolonged corrections (1: the
+    reference's)."""
     from oracle import oracle
 
     return oracle.OracleSim(scene.grid_shape, scene.dx, positions, velocities, dt=scene.dt, flip_ratio=0.95,
                             gravity=scene.gravity, rho=scene.rho, nu=scene.nu, min_size=scene.min_size,
-                            num_vcycles=cycles or 1, tol=None if cycles else tol, **CPU_FCG)
+                            num_vcycles=cycles or 1, tol=None if cycles else tol, prolong_scale=prolong_scale,
+                            **CPU_FCG)
 
 
 def cpu_steps(sim, steps):
@@ -770,6 +780,13 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             solvers[f"fcg{'_fp16' if fp16 else ''}_c4_s{pre}{post}"] = PressureSolver(
                 kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16, coarse_iterations=4,
                 pre_smooth=pre, post_smooth=post)
+    # the same with every prolonged correction scaled by each larger factor (names end in _w17 for 1.7)
+    for name in [n for n in solvers if n.endswith("_c4") or "_c4_s" in n]:
+        ps = solvers[name]
+        for w in PROLONG_SCALE_CHOICES[1:]:
+            solvers[f"{name}_w{round(w * 10)}"] = PressureSolver(
+                kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=ps.coarse_fp16,
+                coarse_iterations=4, pre_smooth=ps.pre_smooth, post_smooth=ps.post_smooth, prolong_scale=w)
     single = {}  # variant name -> first level visited once (clb_mg_set_option 4); none by default
     p_tmp = torch.empty_like(sim.pressure)
     rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": [], "fcg_tuned_learned": []}
@@ -872,6 +889,22 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             if r and r["ms_mean"] < best_ms:
                 best_s, best_ms = (pre, post), r["ms_mean"]
     out["smoothing_chosen"] = list(best_s)
+    # the rule for the prolongation factor (with 4 coarsest-level iterations chosen): the fastest to the
+    # tolerance of the chosen smoothing with factor 1 and every smoothing with a larger factor, which
+    # may change the smoothing too
+    best_w = PROLONG_SCALE_CHOICES[0]
+    if best_k == 4:
+        def c4_name(s):
+            return f"{base}_c4" if tuple(s) == SMOOTHING_CHOICES[0] else f"{base}_c4_s{s[0]}{s[1]}"
+
+        best_ms = out[c4_name(best_s)]["ms_mean"]
+        for w in PROLONG_SCALE_CHOICES[1:]:
+            for s in SMOOTHING_CHOICES:
+                r = out.get(f"{c4_name(s)}_w{round(w * 10)}")
+                if r and r["ms_mean"] < best_ms:
+                    best_w, best_s, best_ms = w, s, r["ms_mean"]
+    out["smoothing_chosen"] = list(best_s)
+    out["prolong_scale_chosen"] = best_w
     if rows["fcg_learned"]:
         out["speedup_learned_vs_plain_fcg"] = out["fcg"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
         out["speedup_learned_vs_refine"] = out["refine"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
@@ -922,6 +955,7 @@ def our_arm(args):
     use_learned = args.learned == "on"
     coarse_k = COARSE_ITERATION_CHOICES[0] if args.coarse_iterations == "auto" else int(args.coarse_iterations)
     smoothing = SMOOTHING_CHOICES[0] if args.smoothing == "auto" else tuple(int(x) for x in args.smoothing.split(","))
+    prolong = PROLONG_SCALE_CHOICES[0] if args.prolong_scale == "auto" else float(args.prolong_scale)
     single_from = int(args.single_visit)
     if args.poisson_steps > 0:
         poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
@@ -931,6 +965,8 @@ def our_arm(args):
             coarse_k = poisson.get("coarse_iterations_chosen", coarse_k)
         if args.smoothing == "auto":
             smoothing = tuple(poisson.get("smoothing_chosen", smoothing))
+        if args.prolong_scale == "auto":
+            prolong = float(poisson.get("prolong_scale_chosen", prolong))
         if args.learned == "auto" and "fcg_tuned_learned" in poisson:
             # the rule: the learned guess in the timed steps only when it makes the solve faster,
             # network evaluation included
@@ -942,15 +978,16 @@ def our_arm(args):
         warm_note += " (not used in the timed steps: no faster than without it in the comparison)"
     kernels.call("clb_mg_set_option", 4, single_from)  # read when the timed solver captures its graphs
     if use_fp16 or coarse_k != sim.options.coarse_iterations or single_from or \
-            smoothing != (sim.options.pre_smooth, sim.options.post_smooth):
+            smoothing != (sim.options.pre_smooth, sim.options.post_smooth) or prolong != sim.options.prolong_scale:
         from continuum_liquid_b200.pressure_solve import PressureSolver
 
         sim.options.coarse_fp16 = use_fp16
         sim.options.coarse_iterations = coarse_k
         sim.options.pre_smooth, sim.options.post_smooth = smoothing
+        sim.options.prolong_scale = prolong
         sim.pressure_solver = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=scene.min_size,
                                              method=args.method, coarse_fp16=use_fp16, coarse_iterations=coarse_k,
-                                             pre_smooth=smoothing[0], post_smooth=smoothing[1])
+                                             pre_smooth=smoothing[0], post_smooth=smoothing[1], prolong_scale=prolong)
         for _ in range(2):  # tuning and graph capture of the new solver
             sim.step()
         torch.cuda.synchronize()
@@ -988,7 +1025,7 @@ def our_arm(args):
 
     # --- Poisson time to 1e-6 in the timed steps ------------------------------------------------
     poisson = {"timed_steps": {"method": args.method, "learned": warm_note, "coarse_fp16": use_fp16,
-                               "coarse_iterations": coarse_k, "smoothing": list(smoothing),
+                               "coarse_iterations": coarse_k, "smoothing": list(smoothing), "prolong_scale": prolong,
                                "ms_mean": float(np.mean(solve_ms)),
                                "cycles_mean": float(np.mean(cycles)),
                                "final_rel_residual_max": float(max(s.rel_residual or 0.0 for s in stats)),
@@ -1065,7 +1102,8 @@ def our_arm(args):
     # --- CPU baseline (rank 0, N = 1): the reference algorithm on the host cores ---------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu_times, cpu_cycles = cpu_steps(cpu_sim(scene, positions, velocities), 1)
+        cpu_times, cpu_cycles = cpu_steps(cpu_sim(scene, positions, velocities,
+                                                  prolong_scale=sim.options.prolong_scale), 1)
         cpu = {"value": 1.0 / cpu_times[0], "unit": UNIT, "cores": cpu_threads(), "kind": "port",
                "sample": f"the first step of the same scene ({n} particles) by the CPU restatement of the reference "
                          f"kernels, its pressure solved to {TOL:g} ({cpu_cycles[0]} cycles of the same iteration)"}
@@ -1074,7 +1112,8 @@ def our_arm(args):
         config = workload_config(args.size, n, args)
         fp16_levels = [list(s) for s in h.shapes[h.fp16_level:]] if h.fp16_level else None
         solver_info = {"pressure": solver_description(args.method, sim.options.pre_smooth, sim.options.post_smooth,
-                                                      sim.options.coarse_iterations, fp16_levels, single_from),
+                                                      sim.options.coarse_iterations, fp16_levels, single_from,
+                                                      sim.options.prolong_scale),
                        "p2g": "tiled scatter (k_p2g_tiled)" if sim.options.tiled_p2g() else
                               "reference-order gather (k_p2g_gather)",
                        "multigrid_levels": [list(s) for s in h.shapes], "sweep_kinds": h.sweeps(),

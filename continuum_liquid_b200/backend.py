@@ -161,6 +161,7 @@ class MGHierarchy(ctypes.Structure):
         ("fused_tiles", ctypes.c_void_p),
         ("fused_tile_count", ctypes.c_void_p),
         ("cluster_lists", ctypes.c_void_p),
+        ("prolong_scale", ctypes.c_float),
     ]
 
 

@@ -708,6 +708,8 @@ static int check_hierarchy(const clb_mg_hierarchy* h) {
 }
 
 static inline bool is_half(const clb_mg_hierarchy* h, int l) { return h->fp16_level > 0 && l >= h->fp16_level; }
+// The factor of every prolonged correction (clb_mg_hierarchy.prolong_scale; 0 reads as 1).
+static inline float pscale(const clb_mg_hierarchy* h) { return h->prolong_scale > 0.0f ? h->prolong_scale : 1.0f; }
 
 // The cluster launch that runs the visits of the third-coarsest level `level` with both bottom levels
 // (mg_cluster.cuh), whatever the launch options: false when these levels cannot run as one (their
@@ -1093,7 +1095,7 @@ static int launch_cluster_visit(const clb_mg_hierarchy* h, int level, int csize,
                              (const float4*)h->op[level + 1], (const uint8_t*)h->mask[level + 1], a[0], a[1], a[2],
                              (const float4*)h->op[level + 2], (const uint8_t*)h->mask[level + 2], b[0], b[1], b[2],
                              h->delta, pre, post, coarse_iters, (const float*)h->fp16_scale, visits,
-                             visits_of(level + 1), visits_of(level + 2), (const int*)h->cluster_lists);
+                             visits_of(level + 1), visits_of(level + 2), (const int*)h->cluster_lists, pscale(h));
     return check_launch("k_cluster_visit") ? -1 : 1;
 }
 }  // extern "C++"
@@ -1142,7 +1144,7 @@ int bottom_visit(const clb_mg_hierarchy* h, int level, int pre, int post, int co
     launch(1, BOTTOM_THREADS, bytes, s)(k_bottom_visit<KA, KB, H>,                                                    \
         h->p[level], h->b[level], (const float4*)h->op[level], h->mask[level], a[0], a[1], a[2], h->p[level + 1],      \
         h->b[level + 1], (const float4*)h->op[level + 1], h->mask[level + 1], b[0], b[1], b[2], h->delta, pre,         \
-                                        post, coarse_iters, h->fp16_scale, visits_of(level + 1))
+                                        post, coarse_iters, h->fp16_scale, visits_of(level + 1), pscale(h))
 #define CLB_BOTTOM_KINDS(H)                                 \
     if (ka <= 1 && kb <= 1) CLB_BOTTOM(1, 1, H);            \
     else if (ka <= 2 && kb <= 1) CLB_BOTTOM(2, 1, H);       \
@@ -1204,7 +1206,7 @@ void launch_l0_iter(const clb_mg_hierarchy* h, const float* in, float* out, cons
     const unsigned grid = (unsigned)(cap < most ? (cap > 0 ? cap : 1) : most);
     launch(grid, L0T_THREADS, L0Region<(MODE & L0F_RESTRICT) ? 3 : 2>::smem(), s)(
         k_l0_iter_tiles<MODE>, h->fused_tiles, h->fused_tile_count, in, out, rhs, h->op0, h->delta, n[0], n[1], n[2],
-        h->p[1], h->b[1], h->p[1], c[0], c[1], c[2]);
+        h->p[1], h->b[1], h->p[1], c[0], c[1], c[2], pscale(h));
 }
 }  // extern "C++"
 
@@ -1299,37 +1301,38 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
             if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     const i64 Cf = (i64)v.nx * v.ny * v.nz;
     const int fvec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
+    const float w = pscale(h);
     if (!c.half && !v.half && v.tiles) {  // prolongation into the fine fluid tiles
         if (v.l0 && fvec == 4 && ((((uintptr_t)v.p) & 15) | (((uintptr_t)v.op0) & 3)) == 0)
             launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<true, 4, true>, v.tiles, v.tile_count, c.p, v.p,
-                                                    v.op0, nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
+                                                    v.op0, nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz, w);
         else if (v.l0 && fvec == 4)
             launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<true, 4>, v.tiles, v.tile_count, c.p, v.p, v.op0,
-                                                    nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
+                                                    nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz, w);
         else if (v.l0)
             launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<true, 1>, v.tiles, v.tile_count, c.p, v.p, v.op0,
-                                                    nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
+                                                    nullptr, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz, w);
         else
             launch(tile_grid(v), dim3(32, 4), 0, s)(k_prolong_tiles<false, 1>, v.tiles, v.tile_count, c.p, v.p,
-                                                    nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz);
+                                                    nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny, v.nz, w);
     } else if (c.half) {
         const dim3 grid = blocks_for(Cf, MGT);
         const __half* ce = reinterpret_cast<const __half*>(c.p);
         if (v.half)
             launch(grid, MGT, 0, s)(k_prolong_h<2>, ce, v.p, nullptr, v.mask, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                    v.nz);
+                                    v.nz, w);
         else if (v.l0)
             launch(grid, MGT, 0, s)(k_prolong_h<0>, ce, v.p, v.op0, nullptr, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                    v.nz);
+                                    v.nz, w);
         else
             launch(grid, MGT, 0, s)(k_prolong_h<1>, ce, v.p, nullptr, v.mask, h->fp16_scale, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                    v.nz);
+                                    v.nz, w);
     } else if (v.l0)
         launch(blocks_for(Cf, MGT), MGT, 0, s)(k_prolong<true>, c.p, v.p, v.op0, nullptr, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                               v.nz);
+                                               v.nz, w);
     else
         launch(blocks_for(Cf, MGT), MGT, 0, s)(k_prolong<false>, c.p, v.p, nullptr, v.mask, c.nx, c.ny, c.nz, v.nx, v.ny,
-                                               v.nz);
+                                               v.nz, w);
     CLB_LAUNCH_CHECK("k_prolong");
     return smooth(v, h->delta, post, s, sparse);
 }

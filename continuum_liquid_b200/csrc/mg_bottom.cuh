@@ -275,7 +275,8 @@ __device__ __forceinline__ void bottom_rhs(const BottomSmem& S, BottomCells<KA, 
 template <int KA, int KB, bool H>
 __device__ __forceinline__ void bottom_core(const BottomSmem& S, BottomCells<KA, KB>& R, int anx, int any, int anz,
                                             int bnx, int bny, int bnz, float d2, float inv_delta2, int pre, int post,
-                                            int coarse_iters, float* __restrict__ bb, int b_solves = 2) {
+                                            int coarse_iters, float* __restrict__ bb, int b_solves = 2,
+                                            float w = 1.0f) {
     float* spa = S.spa;
     const float* sba = S.sba;
     const float4* soa = S.soa;
@@ -377,7 +378,7 @@ __device__ __forceinline__ void bottom_core(const BottomSmem& S, BottomCells<KA,
             const int i = c / asx, j = (c / asy) % any, k = c % anz;
             const int I = min((i - 1) / 2 + 1, bnx - 2), J = min((j - 1) / 2 + 1, bny - 2),
                       K = min((k - 1) / 2 + 1, bnz - 2);
-            spa[c] += spb[(I * bny + J) * bnz + K];
+            spa[c] += w * spb[(I * bny + J) * bnz + K];
         }
     __syncthreads();
     smooth_a(post);
@@ -399,7 +400,8 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
                                                    float* __restrict__ bb, const float4* __restrict__ opb,
                                                    const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
                                                    float delta, int pre, int post, int coarse_iters,
-                                                   const float* __restrict__ scale, int b_solves = 2) {
+                                                   const float* __restrict__ scale, int b_solves = 2,
+                                                   float w = 1.0f) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     const BottomSmem S = bottom_smem(smem, CA, CB);
@@ -414,7 +416,8 @@ __device__ __forceinline__ void bottom_visit_block(float* __restrict__ pa, const
     BottomCells<KA, KB> R;
     bottom_cells(S, R, anx, any, anz, bnx, bny, bnz);
     bottom_rhs(S, R, d2);
-    bottom_core<KA, KB, H>(S, R, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, bb, b_solves);
+    bottom_core<KA, KB, H>(S, R, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters, bb, b_solves,
+                           w);
     const int bsx = bny * bnz, bsy = bnz;
     for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) st(pa, c, S.spa[c]);
     for (int c = threadIdx.x; c < CB; c += BOTTOM_THREADS) {
@@ -431,10 +434,10 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
                    const uint8_t* __restrict__ ma, int anx, int any, int anz, float* __restrict__ pb,
                    float* __restrict__ bb, const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx,
                    int bny, int bnz, float delta, int pre, int post, int coarse_iters,
-                   const float* __restrict__ scale = nullptr, int b_solves = 2) {
+                   const float* __restrict__ scale, int b_solves, float w) {
     pdl_begin();
     bottom_visit_block<KA, KB, H>(pa, ba, opa, ma, anx, any, anz, pb, bb, opb, mb, bnx, bny, bnz, delta, pre, post,
-                                  coarse_iters, scale, b_solves);
+                                  coarse_iters, scale, b_solves, w);
 }
 
 }  // namespace clb

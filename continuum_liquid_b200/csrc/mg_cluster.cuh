@@ -109,7 +109,7 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
                                   const float* __restrict__ bc, const void* __restrict__ opc_,
                                   const uint8_t* __restrict__ mc, int nx, int ny, int nz, int anx, int any, int anz,
                                   float d2, float inv_delta2, int pre, int post, int visits,
-                                  const int* __restrict__ glist) {
+                                  const int* __restrict__ glist, float w) {
     namespace cgx = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem[];
     using OpT = typename std::conditional<H, uint2, float4>::type;
@@ -309,7 +309,7 @@ __device__ void cluster_slab_path(int s, int cs, const float* __restrict__ pc, f
                 const int i = il + sl.i_lo - 1;
                 const int I = min((i - 1) / 2 + 1, anx - 2), J = min((j - 1) / 2 + 1, any - 2),
                           K = min((k - 1) / 2 + 1, anz - 2);
-                sp[c] = stored(sp[c] + parent[(I * any + J) * anz + K - base]);
+                sp[c] = stored(sp[c] + w * parent[(I * any + J) * anz + K - base]);
             }
     }
     push();
@@ -332,7 +332,7 @@ __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __rest
                                     const uint8_t* __restrict__ ma, int anx, int any, int anz,
                                     const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny,
                                     int bnz, float d2, float inv_delta2, int pre, int post, int coarse_iters,
-                                    int visits, int a_visits, int b_solves, const int* __restrict__ glist) {
+                                    int visits, int a_visits, int b_solves, const int* __restrict__ glist, float w) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int CA = anx * any * anz, CB = bnx * bny * bnz;
     const BottomSmem S = bottom_smem(smem, CA, CB);
@@ -364,7 +364,7 @@ __device__ void cluster_bottom_path(float* __restrict__ pa, const float4* __rest
     bottom_rhs(S, R, d2);
     for (int visit = 0; visit < a_visits; ++visit) {  // two, or one when A is visited once
         bottom_core<KA, KB, H>(S, R, anx, any, anz, bnx, bny, bnz, d2, inv_delta2, pre, post, coarse_iters,
-                               nullptr, b_solves);
+                               nullptr, b_solves, w);
         __syncthreads();
         if (H)  // A's p as the bottom visit stores it (FP16) before it is read again
             for (int c = threadIdx.x; c < CA; c += BOTTOM_THREADS) S.spa[c] = __half2float(__float2half_rn(S.spa[c]));
@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
                     const float4* __restrict__ opa, const uint8_t* __restrict__ ma, int anx, int any, int anz,
                     const float4* __restrict__ opb, const uint8_t* __restrict__ mb, int bnx, int bny, int bnz,
                     float delta, int pre, int post, int coarse_iters, const float* __restrict__ scale,
-                    int visits, int a_visits, int b_solves, const int* __restrict__ lists) {
+                    int visits, int a_visits, int b_solves, const int* __restrict__ lists, float w) {
     pdl_begin();
     const float d2 = H ? scale[2] : delta * delta;
     const float inv_delta2 = H ? scale[3] : 1.0f / (delta * delta);
@@ -398,13 +398,14 @@ __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
     const int cs = (int)cooperative_groups::this_cluster().num_blocks() - 1;
     if (rank == 0)
         cluster_bottom_path<KA, KB, H>(pa, opa, ma, anx, any, anz, opb, mb, bnx, bny, bnz, d2, inv_delta2, pre, post,
-                                       coarse_iters, visits, a_visits, b_solves, lists);
+                                       coarse_iters, visits, a_visits, b_solves, lists, w);
     else
         cluster_slab_path<NS, H>((int)rank - 1, cs, pc, pc, bc, opc, mc, nx, ny, nz, anx, any, anz, d2, inv_delta2,
                                  pre, post, visits,
                                  lists ? lists + cluster_lists_bottom_ints(anx * any * anz, bnx * bny * bnz) +
                                              (rank - 1) * cluster_lists_slab_ints(cluster_layout(cs, nx, ny, nz, H))
-                                       : nullptr);
+                                       : nullptr,
+                                 w);
 }
 
 // Lists the fluid cells that the CTAs of a cluster launch own, as the launch would list them but in

@@ -126,12 +126,12 @@ __global__ void __launch_bounds__(MGT) k_restrict_h(const void* __restrict__ fp,
 }
 
 // Prolongation (multigrid.cl:182-201) from an FP16 coarse level into a fine level of layout FS; into
-// an FP32 level the coarse value is unscaled by 1 / sigma_p.
+// an FP32 level the coarse value is unscaled by 1 / sigma_p. w multiplies the prolonged correction.
 template <int FS>
 __device__ __forceinline__ void prolong_h_at(i64 f, const __half* __restrict__ ce, void* __restrict__ fp,
                                              const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
                                              const float* __restrict__ scale, int cnx, int cny, int cnz, int fnx,
-                                             int fny, int fnz) {
+                                             int fny, int fnz, float w) {
     int i, j, k;
     gcoord(f, fny, fnz, i, j, k);
     const bool fl = FS == 0 ? ((__ldg(fop0 + f) & 64u) != 0u) : (__ldg(fmask + f) != 0);
@@ -140,9 +140,9 @@ __device__ __forceinline__ void prolong_h_at(i64 f, const __half* __restrict__ c
     const float e = ldh(ce, gidx(I, J, K, cny, cnz));
     if (FS == 2) {
         __half* p = reinterpret_cast<__half*>(fp);
-        p[f] = __float2half_rn(__half2float(p[f]) + e);
+        p[f] = __float2half_rn(__half2float(p[f]) + w * e);
     } else {
-        reinterpret_cast<float*>(fp)[f] += e * scale[1];
+        reinterpret_cast<float*>(fp)[f] += w * (e * scale[1]);
     }
 }
 
@@ -150,12 +150,12 @@ template <int FS>
 __global__ void __launch_bounds__(MGT) k_prolong_h(const __half* __restrict__ ce, void* __restrict__ fp,
                                                     const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
                                                     const float* __restrict__ scale, int cnx, int cny, int cnz,
-                                                    int fnx, int fny, int fnz) {
+                                                    int fnx, int fny, int fnz, float w) {
     pdl_begin();
     const i64 C = (i64)fnx * fny * fnz;
     const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
     if (f >= C) return;
-    prolong_h_at<FS>(f, ce, fp, fop0, fmask, scale, cnx, cny, cnz, fnx, fny, fnz);
+    prolong_h_at<FS>(f, ce, fp, fop0, fmask, scale, cnx, cny, cnz, fnx, fny, fnz, w);
 }
 
 }  // namespace clb

@@ -79,7 +79,7 @@ enum { L0F_ZERO = 1, L0F_RESTRICT = 2, L0F_PROLONG = 4 };
 //   L0F_ZERO:     x counts as 0 on entry (pin is not read);
 //   L0F_RESTRICT: also the residual of the smoothed x and its restriction into level 1 (cp = 0,
 //                 cb = the children's residual sum), as restrict_at writes them;
-//   L0F_PROLONG:  x + e(parent) on entry at fluid interior cells, e = level 1's p (prolong_at).
+//   L0F_PROLONG:  x + w e(parent) on entry at fluid interior cells, e = level 1's p (prolong_at).
 // Blocks walk the list (tile t, t + gridDim.x, ...).
 template <int MODE>
 __global__ void __launch_bounds__(L0T_THREADS) k_l0_iter_tiles(const int* __restrict__ list,
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(L0T_THREADS) k_l0_iter_tiles(const int* __rest
                                                                 const uint8_t* __restrict__ op0, float delta, int nx,
                                                                 int ny, int nz, float* __restrict__ cp,
                                                                 float* __restrict__ cb, const float* __restrict__ ce,
-                                                                int cnx, int cny, int cnz) {
+                                                                int cnx, int cny, int cnz, float w) {
     pdl_begin();
     constexpr bool ZERO = (MODE & L0F_ZERO) != 0, RESTR = (MODE & L0F_RESTRICT) != 0, PROL = (MODE & L0F_PROLONG) != 0;
     static_assert(!(ZERO && PROL), "a prolongation adds to an x that is read");
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(L0T_THREADS) k_l0_iter_tiles(const int* __rest
                         k <= nz - 2) {
                         const int I = min((i - 1) / 2 + 1, cnx - 2), J = min((j - 1) / 2 + 1, cny - 2),
                                   K = min((k - 1) / 2 + 1, cnz - 2);
-                        pv[u] += __ldg(ce + gidx(I, J, K, cny, cnz));
+                        pv[u] += w * __ldg(ce + gidx(I, J, K, cny, cnz));
                     }
                 }
             }

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(128) k_prolong_tiles(const int* __restrict__ l
                                                         const float* __restrict__ ce, float* __restrict__ fp,
                                                         const uint8_t* __restrict__ fop0,
                                                         const uint8_t* __restrict__ fmask, int cnx, int cny, int cnz,
-                                                        int fnx, int fny, int fnz) {
+                                                        int fnx, int fny, int fnz, float w) {
     pdl_begin();
     const int tk = 32 * VEC, jg = (fny + 3) / 4, kg = (fnz + tk - 1) / tk;
     const int n = *count;
@@ -129,16 +129,17 @@ __global__ void __launch_bounds__(128) k_prolong_tiles(const int* __restrict__ l
             auto parent = [&](int k) { return __ldg(ce + cb + min((k - 1) / 2 + 1, cnz - 2)); };
             const float e0 = parent(k0), e1 = parent(k0 + 1), e2 = parent(k0 + 2), e3 = parent(k0 + 3);
             auto live = [&](unsigned ob, int k) { return (ob & 64u) && k >= 1 && k <= fnz - 2; };
-            if (live(o.x, k0)) x.x += e0;
-            if (live(o.y, k0 + 1)) x.y += e1;
-            if (live(o.z, k0 + 2)) x.z += e2;
-            if (live(o.w, k0 + 3)) x.w += e3;
+            if (live(o.x, k0)) x.x += w * e0;
+            if (live(o.y, k0 + 1)) x.y += w * e1;
+            if (live(o.z, k0 + 2)) x.z += w * e2;
+            if (live(o.w, k0 + 3)) x.w += w * e3;
             *reinterpret_cast<float4*>(fp + c0) = x;
         } else {
 #pragma unroll
             for (int q = 0; q < VEC; ++q) {
                 const int k = (kb * 32 + threadIdx.x) * VEC + q;
-                if (k < fnz) prolong_at<L0>(gidx(i, j, k, fny, fnz), ce, fp, fop0, fmask, cnx, cny, cnz, fnx, fny, fnz);
+                if (k < fnz)
+                    prolong_at<L0>(gidx(i, j, k, fny, fnz), ce, fp, fop0, fmask, cnx, cny, cnz, fnx, fny, fnz, w);
             }
         }
     }

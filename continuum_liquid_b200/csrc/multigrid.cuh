@@ -366,28 +366,30 @@ __global__ void __launch_bounds__(MGT) k_restrict(const float* __restrict__ fp, 
     restrict_at<L0>(ci, fp, fb, fop0, fopc, fmask, cp, cb, delta, fnx, fny, fnz, cnx, cny, cnz);
 }
 
-// prolongate (multigrid.cl:182-201) for either layout
+// prolongate (multigrid.cl:182-201) for either layout. w multiplies the prolonged correction (1: the
+// reference's prolongation, bit for bit since 1 * e = e; see clb_mg_hierarchy.prolong_scale).
 template <bool L0>
 __device__ __forceinline__ void prolong_at(i64 f, const float* __restrict__ ce, float* __restrict__ fp,
                                                   const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
-                                                  int cnx, int cny, int cnz, int fnx, int fny, int fnz) {
+                                                  int cnx, int cny, int cnz, int fnx, int fny, int fnz,
+                                                  float w = 1.0f) {
     int i, j, k;
     gcoord(f, fny, fnz, i, j, k);
     const bool fl = L0 ? ((__ldg(fop0 + f) & 64u) != 0u) : (__ldg(fmask + f) != 0);
     if (!interior(i, j, k, fnx, fny, fnz) || !fl) return;
     const int I = min((i - 1) / 2 + 1, cnx - 2), J = min((j - 1) / 2 + 1, cny - 2), K = min((k - 1) / 2 + 1, cnz - 2);
-    fp[f] += __ldg(ce + gidx(I, J, K, cny, cnz));
+    fp[f] += w * __ldg(ce + gidx(I, J, K, cny, cnz));
 }
 
 template <bool L0>
 __global__ void __launch_bounds__(MGT) k_prolong(const float* __restrict__ ce, float* __restrict__ fp,
                                                   const uint8_t* __restrict__ fop0, const uint8_t* __restrict__ fmask,
-                                                  int cnx, int cny, int cnz, int fnx, int fny, int fnz) {
+                                                  int cnx, int cny, int cnz, int fnx, int fny, int fnz, float w) {
     pdl_begin();
     const i64 C = (i64)fnx * fny * fnz;
     const i64 f = (i64)blockIdx.x * MGT + threadIdx.x;
     if (f >= C) return;
-    prolong_at<L0>(f, ce, fp, fop0, fmask, cnx, cny, cnz, fnx, fny, fnz);
+    prolong_at<L0>(f, ce, fp, fop0, fmask, cnx, cny, cnz, fnx, fny, fnz, w);
 }
 
 // coarse_smooth (multigrid.cl:232-264): one block runs all colour sweeps of the coarsest level,

@@ -271,13 +271,16 @@ class MultigridHierarchy:
 
     def w_cycle(self, x, rhs, pre_smooth=PRE_SMOOTH, post_smooth=POST_SMOOTH,
                 coarse_iterations=COARSE_SMOOTH_ITERATIONS, queue=None, x_zero_outside: bool = False,
-                x_from_zero: bool = False) -> None:
+                x_from_zero: bool = False, prolong_scale: float = 1.0) -> None:
         """One W-cycle on level-0 unknown ``x`` and right-hand side ``rhs``. ``x_zero_outside``: the
         caller guarantees that ``x`` is 0 at every cell that is not fluid (a zeroed correction), so the
         level-0 sweeps may skip the tiles without fluid. ``x_from_zero``: the W-cycle starts from a zero
         ``x`` although ``x`` still holds a previous correction at fluid cells (it must be 0 at every
-        other cell): the first sweep ignores ``x`` instead of the caller zeroing it."""
+        other cell): the first sweep ignores ``x`` instead of the caller zeroing it.
+        ``prolong_scale``: every prolonged correction is multiplied by it (1: the reference's W-cycle;
+        no counterpart in the reference, see clb_mg_hierarchy.prolong_scale)."""
         self.struct.zero_outside = 2 if x_from_zero else (1 if x_zero_outside else 0)
+        self.struct.prolong_scale = float(prolong_scale)
         self.kernels.call_hierarchy("clb_mg_w_cycle", self.struct, x, rhs, int(pre_smooth), int(post_smooth),
                                     int(coarse_iterations), stream=queue)
 

@@ -115,7 +115,7 @@ class PressureSolver:
                  autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64,
                  coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS,
                  pre_smooth: int = multigrid.PRE_SMOOTH, post_smooth: int = multigrid.POST_SMOOTH,
-                 fused_level0: bool = False, device_loop: bool = False):
+                 fused_level0: bool = False, device_loop: bool = False, prolong_scale: float = 1.0):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.coarse_fp16 = bool(coarse_fp16)
@@ -133,6 +133,13 @@ class PressureSolver:
         # tolerance mode's W-cycle preconditioner; the reference's 2 and 4 by default (fixed-cycle mode
         # always uses those)
         self.pre_smooth, self.post_smooth = int(pre_smooth), int(post_smooth)
+        # factor of every correction the tolerance mode's W-cycle prolongs (no counterpart in the
+        # reference, whose piecewise-constant prolongation is 1; fixed-cycle mode always uses 1). About
+        # 1.7 over-corrects what the constant prolongation under-corrects: at 256^3 the flexible CG then
+        # needs 8 instead of 13 cycles per solve
+        self.prolong_scale = float(prolong_scale)
+        if not self.prolong_scale > 0.0:
+            raise ValueError("prolong_scale must be > 0")
         # fused_level0: the tolerance mode's W-cycles run level 0 as fused tile launches (sweep kind 7,
         # csrc/mg_level0.cuh), with the values of the launch-per-step path. Off by default: at 256^3 the
         # recomputed halo costs more instructions than the four launches it saves
@@ -209,7 +216,8 @@ class PressureSolver:
             h.struct.sweep[0] = 7
         try:
             h.w_cycle(self.correction, self.residual, pre_smooth=self.pre_smooth, post_smooth=self.post_smooth,
-                      coarse_iterations=self.coarse_iterations, queue=queue, x_from_zero=True)
+                      coarse_iterations=self.coarse_iterations, queue=queue, x_from_zero=True,
+                      prolong_scale=self.prolong_scale)
         finally:
             h.struct.sweep[0] = kind0
         delta = float(FIELD_DTYPE(self.dx))
@@ -355,6 +363,7 @@ class PressureSolver:
         kind0 = int(h.struct.sweep[0])
         if self.fused_level0:
             h.struct.sweep[0] = 7
+        h.struct.prolong_scale = self.prolong_scale  # read when the loop's refinement is captured
         out = ctypes.c_void_p()
         from .backend import ptr
 

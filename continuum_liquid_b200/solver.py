@@ -60,6 +60,9 @@ class StepOptions:
     # preconditioner (the reference's 2 and 4)
     pre_smooth: int = 2
     post_smooth: int = 4
+    # tolerance mode: the factor of every correction the W-cycle preconditioner prolongs (1: the
+    # reference's piecewise-constant prolongation; about 1.7 needs far fewer cycles, see PressureSolver)
+    prolong_scale: float = 1.0
     revoxelise: bool = False  # voxelise the colliders again at every step (moving or deforming meshes)
     # P2G gather: "exact" (the reference's summation order, bit for bit), "tiled" (each particle visited
     # once; equal to float rounding) or "auto" (exact in the reference's fixed-cycle mode, tiled when
@@ -124,7 +127,8 @@ class FlipSolver:
                                               method=self.options.method, coarse_fp16=self.options.coarse_fp16,
                                               coarse_iterations=self.options.coarse_iterations,
                                               pre_smooth=self.options.pre_smooth,
-                                              post_smooth=self.options.post_smooth)
+                                              post_smooth=self.options.post_smooth,
+                                              prolong_scale=self.options.prolong_scale)
         self.last_solve: SolveStats | None = None
         self.steps_done = 0
 

@@ -314,6 +314,11 @@ typedef struct clb_mg_hierarchy {
      * clb_mg_build_coarse lists them once per solve, so a launch does not. NULL: every launch lists
      * them itself (the same cells). */
     int32_t* cluster_lists;              /* clb_mg_cluster_list_capacity(h) entries */
+    /* No counterpart in the reference: every correction a W-cycle prolongs (multigrid.cl:182-201, all
+     * levels) is multiplied by it. 0 and 1 give the reference's W-cycle bit for bit. The reference's
+     * piecewise-constant prolongation under-corrects; about 1.7 makes the W-cycle a much stronger
+     * preconditioner of the tolerance mode's iteration. */
+    float prolong_scale;
 } clb_mg_hierarchy;
 
 /* Number of tiles of a level of nx x ny x nz cells (finest != 0: the finest level's tile shape). */

@@ -889,8 +889,10 @@ void restrict_residual(const T* fp, const T* fb, const T* fm, const T* fd, const
     }
 }
 
-template <typename T>  // multigrid.cl:182-201 prolongate
-void prolongate(const T* ce, T* fp, const T* fm, int cnx, int cny, int cnz, int fnx, int fny, int fnz) {
+// multigrid.cl:182-201 prolongate. w multiplies the prolonged correction (no counterpart in the
+// reference, whose prolongation is w = 1: 1 * e = e, so w = 1 is the reference bit for bit).
+template <typename T>
+void prolongate(const T* ce, T* fp, const T* fm, int cnx, int cny, int cnz, int fnx, int fny, int fnz, T w = 1) {
     const i64 C = (i64)fnx * fny * fnz;
 #pragma omp parallel for schedule(static)
     for (i64 f = 0; f < C; ++f) {
@@ -900,7 +902,7 @@ void prolongate(const T* ce, T* fp, const T* fm, int cnx, int cny, int cnz, int 
         const int I = std::min((i - 1) / 2 + 1, cnx - 2);
         const int J = std::min((j - 1) / 2 + 1, cny - 2);
         const int K = std::min((k - 1) / 2 + 1, cnz - 2);
-        fp[f] += ce[gidx(I, J, K, cny, cnz)];
+        fp[f] += w * ce[gidx(I, J, K, cny, cnz)];
     }
 }
 
@@ -959,7 +961,8 @@ struct Levels {
 // single_from > 0 (no counterpart in the reference): levels from single_from on are visited once per
 // visit of the level above instead of twice (the solver's clb_mg_set_option 4).
 template <typename T>
-void w_cycle(const Levels<T>& L, int level, T delta, int pre, int post, int coarse_iters, int single_from = 0) {
+void w_cycle(const Levels<T>& L, int level, T delta, int pre, int post, int coarse_iters, int single_from = 0,
+             T prolong_scale = 1) {
     const int* s = L.shape + 3 * level;
     if (level == L.count - 1) {
         coarse_smooth<T>(L.p[level], L.b[level], L.m[level], L.d[level], L.wx[level], L.wy[level], L.wz[level], delta,
@@ -976,8 +979,8 @@ void w_cycle(const Levels<T>& L, int level, T delta, int pre, int post, int coar
                          L.b[c], L.m[c], L.d[c], L.wx[c], L.wy[c], L.wz[c], delta, s[0], s[1], s[2], cs[0], cs[1],
                          cs[2]);
     const int visits = single_from > 0 && c >= single_from ? 1 : 2;
-    for (int v = 0; v < visits; ++v) w_cycle<T>(L, c, delta, pre, post, coarse_iters, single_from);
-    prolongate<T>(L.p[c], L.p[level], L.m[level], cs[0], cs[1], cs[2], s[0], s[1], s[2]);
+    for (int v = 0; v < visits; ++v) w_cycle<T>(L, c, delta, pre, post, coarse_iters, single_from, prolong_scale);
+    prolongate<T>(L.p[c], L.p[level], L.m[level], cs[0], cs[1], cs[2], s[0], s[1], s[2], prolong_scale);
     for (int it = 0; it < post; ++it)
         for (int parity = 0; parity < 2; ++parity)
             rbgs_step<T>(L.p[level], L.b[level], L.m[level], L.d[level], L.wx[level], L.wy[level], L.wz[level], delta,
@@ -1037,14 +1040,16 @@ void orc_coarse_smooth_f32(float* p, const float* b, const float* m, const float
 
 // W-cycle over a level list whose arrays are given as pointer tables (level 0 = finest).
 void orc_w_cycle_f32(float** p, float** b, float** m, float** d, float** wx, float** wy, float** wz, const int* shapes,
-                     int levels, float delta, int pre, int post, int coarse_iters, int single_from) {
+                     int levels, float delta, int pre, int post, int coarse_iters, int single_from,
+                     float prolong_scale) {
     Levels<float> L{p, b, m, d, wx, wy, wz, shapes, levels};
-    w_cycle<float>(L, 0, delta, pre, post, coarse_iters, single_from);
+    w_cycle<float>(L, 0, delta, pre, post, coarse_iters, single_from, prolong_scale);
 }
 void orc_w_cycle_f64(double** p, double** b, double** m, double** d, double** wx, double** wy, double** wz,
-                     const int* shapes, int levels, double delta, int pre, int post, int coarse_iters, int single_from) {
+                     const int* shapes, int levels, double delta, int pre, int post, int coarse_iters, int single_from,
+                     double prolong_scale) {
     Levels<double> L{p, b, m, d, wx, wy, wz, shapes, levels};
-    w_cycle<double>(L, 0, delta, pre, post, coarse_iters, single_from);
+    w_cycle<double>(L, 0, delta, pre, post, coarse_iters, single_from, prolong_scale);
 }
 void orc_residual_norms_f32(const float* p, const float* b, const float* m, const float* d, const float* wx,
                             const float* wy, const float* wz, float delta, int nx, int ny, int nz, double* rr,

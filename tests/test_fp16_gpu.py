@@ -134,8 +134,9 @@ def test_fp16_fused_sweeps_equal_per_cell_sweeps(backend, kind):
     assert backend.device_error() == 0
 
 
+@pytest.mark.parametrize("scale", [1.0, 1.7])
 @pytest.mark.parametrize("shape", [(130, 130, 130), (134, 120, 125)])
-def test_fp16_cluster_visit_equals_level_by_level(backend, shape):
+def test_fp16_cluster_visit_equals_level_by_level(backend, shape, scale):
     """With FP16 storage the cluster visit of the third-coarsest level (and its bottom visits) rounds
     exactly where the level-by-level kernels store FP16: W-cycles agree bit for bit."""
     dx = 1.0 / shape[0]
@@ -152,7 +153,7 @@ def test_fp16_cluster_visit_equals_level_by_level(backend, shape):
             backend.lib.clb_mg_set_option(2, cluster)
             e = torch.zeros_like(rhs)
             for _ in range(2):
-                h.w_cycle(e, rhs)
+                h.w_cycle(e, rhs, prolong_scale=scale)
             out[cluster] = e
     finally:
         backend.lib.clb_mg_set_option(2, 1)

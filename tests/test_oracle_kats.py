@@ -413,6 +413,28 @@ def test_fcg_restatement(oracle):
     assert np.array_equal(x1, np.where(mask > 0, p, 0).astype(np.float64))
 
 
+def test_scaled_prolongation(oracle):
+    """prolong_scale = 1 is the reference's W-cycle bit for bit; 1.7 over-corrects the piecewise-constant
+    prolongation and the FCG restatement needs fewer W-cycles to the same tolerance."""
+    n, dx = 34, np.float32(1.0 / 34.0)
+    shape = (n, n, n)
+    mask = np.zeros(shape, np.float32)
+    mask[1:-1, 1 : n // 2 + 1, 1:-1] = 1.0  # a liquid slab under air, no air cells inside it
+    rng = np.random.default_rng(15)
+    b = (rng.standard_normal(shape) * (mask > 0)).astype(np.float32)
+    ops = oracle.build_finest_operator(mask, shape)
+    p1, p2 = np.zeros(shape, np.float32), np.zeros(shape, np.float32)
+    oracle.Levels(shape).w_cycle(p1, b, mask, ops, dx)
+    oracle.Levels(shape).w_cycle(p2, b, mask, ops, dx, prolong_scale=1.0)
+    assert np.array_equal(p1, p2)
+    _, hist1 = oracle.fcg_solve(b, mask, shape, dx, tol=1e-8, max_cycles=60, coarse_iterations=4, pre_smooth=1,
+                                post_smooth=1)
+    _, hist17 = oracle.fcg_solve(b, mask, shape, dx, tol=1e-8, max_cycles=60, coarse_iterations=4, pre_smooth=1,
+                                 post_smooth=1, prolong_scale=1.7)
+    assert hist1[-1] <= 1e-8 and hist17[-1] <= 1e-8
+    assert len(hist17) + 4 <= len(hist1)  # 13 against 19 W-cycles
+
+
 def test_fcg_with_fewer_coarse_iterations(oracle):
     """The FCG restatement still converges with a weak coarsest-level solve in its W-cycle."""
     n, dx = 18, np.float32(1.0 / 18.0)

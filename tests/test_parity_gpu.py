@@ -406,21 +406,24 @@ def test_iterative_refinement_reaches_tolerance(backend, oracle, method):
     assert np.array_equal(got, oracle.neumann_domain_bc(got, shape))
 
 
-@pytest.mark.parametrize("method,coarse,smooth", [("fcg", 64, (2, 4)), ("refine", 64, (2, 4)), ("fcg", 4, (2, 4)),
-                                                  ("fcg", 0, (2, 4)), ("fcg", 4, (1, 1)), ("fcg", 4, (1, 2))])
-def test_refinement_history_matches_oracle(backend, oracle, method, coarse, smooth):
+@pytest.mark.parametrize("method,coarse,smooth,w", [("fcg", 64, (2, 4), 1.0), ("refine", 64, (2, 4), 1.0),
+                                                    ("fcg", 4, (2, 4), 1.0), ("fcg", 0, (2, 4), 1.0),
+                                                    ("fcg", 4, (1, 1), 1.0), ("fcg", 4, (1, 2), 1.0),
+                                                    ("fcg", 4, (1, 1), 1.7), ("refine", 4, (1, 1), 1.7)])
+def test_refinement_history_matches_oracle(backend, oracle, method, coarse, smooth, w):
     """Every W-cycle of the GPU iteration against the oracle's restatement (same FP32 W-cycle, with
     the reference's or fewer coarsest-level iterations, FP64 accumulation and scalars; only summation
     orders differ)."""
     shape, dx = (34, 30, 38), F32(1.0 / 34)
     rng = np.random.default_rng(5)
-    u, v, w = (rng.standard_normal(shape).astype(F32) for _ in range(3))
+    u, v, w_vel = (rng.standard_normal(shape).astype(F32) for _ in range(3))
     ff, _, _ = random_system(shape, 6)
     dt, rho = 1.0 / 240.0, 1000.0
     ps = pressure_solve.PressureSolver(backend, shape, float(dx), method=method, autotune=False,
-                                       coarse_iterations=coarse, pre_smooth=smooth[0], post_smooth=smooth[1])
+                                       coarse_iterations=coarse, pre_smooth=smooth[0], post_smooth=smooth[1],
+                                       prolong_scale=w)
     P = torch.zeros(shape, dtype=torch.float32, device="cuda")
-    ps.solve((dev(u), dev(v), dev(w)), dev(ff), P, dt, rho, tol=1e-3, use_graph=False)  # builds the system
+    ps.solve((dev(u), dev(v), dev(w_vel)), dev(ff), P, dt, rho, tol=1e-3, use_graph=False)  # builds the system
     h = ps.hierarchy
     p0 = rng.standard_normal(shape).astype(F32) * 10.0
     ps.cur = 0
@@ -431,9 +434,10 @@ def test_refinement_history_matches_oracle(backend, oracle, method, coarse, smoo
     for _ in range(8):
         ps._refine(use_graph=False)
         got.append(ps._relative(h.norms))
-    orhs = oracle.pressure_rhs(u, v, w, ff, dx, dt, rho, shape)
+    orhs = oracle.pressure_rhs(u, v, w_vel, ff, dx, dt, rho, shape)
     x, want = oracle.fcg_solve(orhs, ff, shape, dx, p0=p0, tol=0.0, max_cycles=8, flexible=(method == "fcg"),
-                               coarse_iterations=coarse, pre_smooth=smooth[0], post_smooth=smooth[1])
+                               coarse_iterations=coarse, pre_smooth=smooth[0], post_smooth=smooth[1],
+                               prolong_scale=w)
     np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-14)  # FP64 summation orders differ
     assert want[-1] < 1e-3 * want[0]
     scale = np.abs(x).max()
@@ -559,6 +563,33 @@ def test_w_cycle_paths_agree(backend, oracle, shape, bottom, pdl, cluster):
         backend.lib.clb_mg_set_option(0, 1)
         backend.lib.clb_mg_set_option(1, 1)
         backend.lib.clb_mg_set_option(2, 1)
+
+
+@pytest.mark.parametrize("cluster", [1, 0])
+@pytest.mark.parametrize("shape", [(66, 66, 66), (70, 66, 61), (130, 96, 100)])
+def test_scaled_prolongation_matches_oracle(backend, oracle, shape, cluster):
+    """W-cycles whose prolonged corrections are scaled (clb_mg_hierarchy.prolong_scale = 1.7) equal the
+    oracle's bit for bit, through the cluster visit and level by level; scale 1 is the reference."""
+    dx = F32(1.0 / shape[0])
+    ff, b, p0 = random_system(shape, 25)
+    backend.lib.clb_mg_set_option(2, cluster)
+    try:
+        h = multigrid.MultigridHierarchy(backend, shape, float(dx))
+        u, v, w = (np.random.default_rng(26 + a).standard_normal(shape).astype(F32) for a in range(3))
+        rhs = torch.zeros(shape, dtype=torch.float32, device="cuda")
+        h.rhs_operator((dev(u), dev(v), dev(w)), dev(ff), rhs, 1.0 / 240.0, 1000.0)
+        h.build_coarse()
+        orhs = oracle.pressure_rhs(u, v, w, ff, dx, 1.0 / 240.0, 1000.0, shape)
+        op = oracle.build_finest_operator(ff, shape)
+        for scale in (1.7, 1.0):
+            P = dev(p0)
+            h.w_cycle(P, rhs, pre_smooth=1, post_smooth=1, coarse_iterations=4, prolong_scale=scale)
+            q = p0.copy()
+            oracle.Levels(shape).w_cycle(q, orhs, ff, op, dx, pre=1, post=1, coarse=4, prolong_scale=scale)
+            assert np.array_equal(host(P), q), scale
+    finally:
+        backend.lib.clb_mg_set_option(2, 1)
+    assert backend.device_error() == 0
 
 
 def test_programmatic_launch_changes_nothing(backend):
