@@ -40,7 +40,7 @@ METRIC = "steps/s at 256^3; Poisson ms to 1e-6 rel. residual, learned vs plain W
 UNIT = "steps/s"
 TOL = 1e-6
 COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarsest-level iterations
-SMOOTHING_CHOICES = ((2, 4), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
+SMOOTHING_CHOICES = ((2, 4), (2, 2), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
 # factor of every prolonged correction in the W-cycle preconditioner; 1.0: the reference's prolongation
 PROLONG_SCALE_CHOICES = (1.0, 1.7)
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
@@ -79,8 +79,8 @@ def parse_args():
                          "than 64 in the Poisson comparison)")
     ap.add_argument("--smoothing", default="auto",
                     help="red-black iterations before,after the coarse-grid correction in the W-cycle preconditioner "
-                         "of the timed steps, e.g. 2,4 (auto: the fastest of 2,4 (the reference's), 1,2 and 1,1 to the "
-                         "tolerance in the Poisson comparison, with 4 coarsest-level iterations)")
+                         "of the timed steps, e.g. 2,4 (auto: the fastest of 2,4 (the reference's), 2,2, 1,2 and 1,1 to "
+                         "the tolerance in the Poisson comparison, with 4 coarsest-level iterations)")
     ap.add_argument("--prolong-scale", default="auto",
                     help="factor of every correction the W-cycle preconditioner of the timed steps prolongs (1: the "
                          "reference's piecewise-constant prolongation; auto: 1.7 when it is the fastest to the tolerance "
