@@ -43,6 +43,7 @@ COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarses
 SMOOTHING_CHOICES = ((2, 4), (2, 2), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
 # factor of every prolonged correction in the W-cycle preconditioner; 1.0: the reference's prolongation
 PROLONG_SCALE_CHOICES = (1.0, 1.7)
+SCALED_COARSE_ITERATIONS = (4, 0)  # coarsest-level iterations tried with the larger factors
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
                      "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
@@ -780,13 +781,15 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
             solvers[f"fcg{'_fp16' if fp16 else ''}_c4_s{pre}{post}"] = PressureSolver(
                 kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16, coarse_iterations=4,
                 pre_smooth=pre, post_smooth=post)
-    # the same with every prolonged correction scaled by each larger factor (names end in _w17 for 1.7)
+    # the same with every prolonged correction scaled by each larger factor (names end in _w17 for 1.7),
+    # with 4 and with 0 coarsest-level iterations (the scaled W-cycle needs no more cycles without them)
     for name in [n for n in solvers if n.endswith("_c4") or "_c4_s" in n]:
         ps = solvers[name]
         for w in PROLONG_SCALE_CHOICES[1:]:
-            solvers[f"{name}_w{round(w * 10)}"] = PressureSolver(
-                kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=ps.coarse_fp16,
-                coarse_iterations=4, pre_smooth=ps.pre_smooth, post_smooth=ps.post_smooth, prolong_scale=w)
+            for k in SCALED_COARSE_ITERATIONS:
+                solvers[f"{name.replace('_c4', f'_c{k}')}_w{round(w * 10)}"] = PressureSolver(
+                    kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=ps.coarse_fp16,
+                    coarse_iterations=k, pre_smooth=ps.pre_smooth, post_smooth=ps.post_smooth, prolong_scale=w)
     single = {}  # variant name -> first level visited once (clb_mg_set_option 4); none by default
     p_tmp = torch.empty_like(sim.pressure)
     rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": [], "fcg_tuned_learned": []}
@@ -890,19 +893,21 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                 best_s, best_ms = (pre, post), r["ms_mean"]
     out["smoothing_chosen"] = list(best_s)
     # the rule for the prolongation factor (with 4 coarsest-level iterations chosen): the fastest to the
-    # tolerance of the chosen smoothing with factor 1 and every smoothing with a larger factor, which
-    # may change the smoothing too
+    # tolerance of the chosen smoothing with factor 1 and every smoothing and scaled coarsest-level
+    # count with a larger factor, which may change the smoothing and the count too
     best_w = PROLONG_SCALE_CHOICES[0]
     if best_k == 4:
-        def c4_name(s):
-            return f"{base}_c4" if tuple(s) == SMOOTHING_CHOICES[0] else f"{base}_c4_s{s[0]}{s[1]}"
+        def c_name(k, s):
+            return f"{base}_c{k}" if tuple(s) == SMOOTHING_CHOICES[0] else f"{base}_c{k}_s{s[0]}{s[1]}"
 
-        best_ms = out[c4_name(best_s)]["ms_mean"]
+        best_ms = out[c_name(4, best_s)]["ms_mean"]
         for w in PROLONG_SCALE_CHOICES[1:]:
-            for s in SMOOTHING_CHOICES:
-                r = out.get(f"{c4_name(s)}_w{round(w * 10)}")
-                if r and r["ms_mean"] < best_ms:
-                    best_w, best_s, best_ms = w, s, r["ms_mean"]
+            for k in SCALED_COARSE_ITERATIONS:
+                for s in SMOOTHING_CHOICES:
+                    r = out.get(f"{c_name(k, s)}_w{round(w * 10)}")
+                    if r and r["ms_mean"] < best_ms:
+                        best_w, best_k, best_s, best_ms = w, k, s, r["ms_mean"]
+    out["coarse_iterations_chosen"] = best_k
     out["smoothing_chosen"] = list(best_s)
     out["prolong_scale_chosen"] = best_w
     if rows["fcg_learned"]:
