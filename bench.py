@@ -43,6 +43,8 @@ COARSE_ITERATION_CHOICES = (64, 16, 8, 4)  # 64: the reference W-cycle's coarses
 SMOOTHING_CHOICES = ((2, 4), (2, 2), (1, 2), (1, 1))  # (pre, post); (2, 4): the reference W-cycle's
 # factor of every prolonged correction in the W-cycle preconditioner; 1.0: the reference's prolongation
 PROLONG_SCALE_CHOICES = (1.0, 1.7)
+# the W-cycle preconditioner settings the Poisson comparison picks at 256^3, used by the other cases
+TUNED_WCYCLE = {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 1, "prolong_scale": 1.7}
 SCALED_COARSE_ITERATIONS = (4, 0)  # coarsest-level iterations tried with the larger factors
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
@@ -117,9 +119,9 @@ def batch_case(args):
     kernels = Backend(0)
     scs = scenes.uneven_batch(args.scenes, seed=0)
     t0 = time.perf_counter()
-    # the W-cycle settings the single-scene comparison picks at 256^3 (4 coarsest-level iterations, one
-    # smoothing sweep each way), in the batch and in the one-scene-at-a-time arm alike
-    wset = {"coarse_iterations": 4, "pre_smooth": 1, "post_smooth": 1}
+    # the W-cycle settings the single-scene comparison picks at 256^3, in the batch and in the
+    # one-scene-at-a-time arm alike
+    wset = dict(TUNED_WCYCLE)
     b = batch.BatchedFlip(kernels, scs, tol=TOL, **wset)
     setup_s = time.perf_counter() - t0
     for _ in range(args.warmup):
@@ -141,8 +143,10 @@ def batch_case(args):
         "value": len(scs) * 1e3 / ms, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
         "config": {"workload": f"uneven_batch_{len(scs)}", "sizes": [s.grid_shape[0] for s in scs],
                    "particles": b.n, "cells": b.C0, "pressure_tolerance": TOL,
-                   "pressure_solver": "per-scene flexible CG preconditioned by one W-cycle (pre 1, post 1, coarse "
-                                      "1+4), FP64 accumulation"},
+                   "pressure_solver": f"per-scene flexible CG preconditioned by one W-cycle (pre {wset['pre_smooth']}, "
+                                      f"post {wset['post_smooth']}, coarse {wset['pre_smooth']}+"
+                                      f"{wset['coarse_iterations']}, prolonged corrections x{wset['prolong_scale']:g}), "
+                                      "FP64 accumulation"},
         "particles_per_s": b.n * 1e3 / ms,
         "cycles_per_step": [st.cycles for st in stats],
         "rel_residual_max": max(max(st.rel_residual) for st in stats),
@@ -183,7 +187,7 @@ def collider_case(args):
     kernels = Backend(0)
     sc = scenes.collider_pool(128, seed=0, subdivisions=4)
     opts = solver.StepOptions(flip_ratio=sc.flip_ratio, tol=TOL, gravity=sc.gravity, rho=sc.rho, nu=sc.nu,
-                              revoxelise=True)
+                              revoxelise=True, **TUNED_WCYCLE)
     sim = solver.scene_solver(kernels, sc, opts)
     triangles = sum(int(t.shape[0]) for t in sim.colliders)
     for _ in range(args.warmup):
@@ -210,7 +214,7 @@ def collider_case(args):
         "case": "collider", "metric": "steps/s of the 128^3 collider pool, collider voxelised every step",
         "unit": "steps/s", "value": 1e3 / ms, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
         "config": {"workload": "collider_pool_128^3", "grid": list(sc.grid_shape), "particles": sim.n,
-                   "triangles": triangles, "pressure_tolerance": TOL},
+                   "triangles": triangles, "pressure_tolerance": TOL, "w_cycle_preconditioner": TUNED_WCYCLE},
         "particles_per_s": sim.n * 1e3 / ms, "cycles_per_step": [s.cycles for s in stats],
         "rel_residual_max": max(s.rel_residual for s in stats),
         "voxelise_ms": vox_ms,

@@ -228,6 +228,7 @@ class Batch(ctypes.Structure):
         ("b", ctypes.c_void_p * MG_MAX_LEVELS),
         ("mask", ctypes.c_void_p * MG_MAX_LEVELS),
         ("op", ctypes.c_void_p * MG_MAX_LEVELS),
+        ("prolong_scale", ctypes.c_float),
     ]
 
 

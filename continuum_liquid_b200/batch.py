@@ -71,7 +71,8 @@ class BatchedFlip:
     def __init__(self, kernels: Backend, scenes: list[Scene], flip_ratio: float | None = None, tol: float | None = 1e-6,
                  num_vcycles: int = 1, reduce_blocks: int = 32, sweep0: int = 1, use_graph: bool = True,
                  max_cycles: int = 100, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS,
-                 pre_smooth: int = PRE_SMOOTH, post_smooth: int = POST_SMOOTH, tiled_p2g: bool | None = None):
+                 pre_smooth: int = PRE_SMOOTH, post_smooth: int = POST_SMOOTH, tiled_p2g: bool | None = None,
+                 prolong_scale: float = 1.0):
         if not 1 <= len(scenes) <= BATCH_MAX_SCENES:
             raise ValueError(f"a batch holds 1..{BATCH_MAX_SCENES} scenes, got {len(scenes)}")
         first = scenes[0]
@@ -91,6 +92,11 @@ class BatchedFlip:
         self.pre_smooth, self.post_smooth = int(pre_smooth), int(post_smooth)
         if self.pre_smooth < 0 or self.post_smooth < 0 or self.pre_smooth + self.post_smooth == 0:
             raise ValueError("pre_smooth and post_smooth must be >= 0 and not both 0")
+        # factor of every correction the tolerance mode's W-cycle prolongs (PressureSolver.prolong_scale;
+        # fixed-cycle mode: 1, the reference's prolongation)
+        self.prolong_scale = float(prolong_scale)
+        if not self.prolong_scale > 0.0:
+            raise ValueError("prolong_scale must be > 0")
         self.ppc = first.particles_per_cell
         self.use_graph = use_graph
         dev = kernels.device
@@ -290,7 +296,8 @@ class BatchedFlip:
         self._swap()
 
     def _w_cycle(self, x, rhs, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS, pre: int = PRE_SMOOTH,
-                 post: int = POST_SMOOTH) -> None:
+                 post: int = POST_SMOOTH, prolong_scale: float = 1.0) -> None:
+        self.batch.prolong_scale = float(prolong_scale)  # read when the W-cycle is launched or captured
         self._call("clb_batch_w_cycle", x, rhs, int(pre), int(post), int(coarse_iterations))
 
     def _init_solve(self) -> None:
@@ -302,7 +309,8 @@ class BatchedFlip:
 
     def _iteration(self, src: int) -> None:
         self.correction.zero_()
-        self._w_cycle(self.correction, self.residual, self.coarse_iterations, self.pre_smooth, self.post_smooth)
+        self._w_cycle(self.correction, self.residual, self.coarse_iterations, self.pre_smooth, self.post_smooth,
+                      self.prolong_scale)
         self._call("clb_batch_fcg_dots", self.correction, self.direction[src], self.residual, self.partials4,
                    self.fcg_state)
         self._call("clb_batch_fcg_step", self.p64[src], self.correction, self.direction[src], self.p64[1 - src],

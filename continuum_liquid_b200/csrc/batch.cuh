@@ -350,12 +350,12 @@ __global__ void __launch_bounds__(BT) kb_restrict(BList L, i64 total, const clb_
 template <bool L0>
 __global__ void __launch_bounds__(BT) kb_prolong(BList L, i64 total, const clb_batch_scene* __restrict__ G, int level,
                                                  const float* ce, float* fp, const uint8_t* fop0,
-                                                 const uint8_t* fmask) {
+                                                 const uint8_t* fmask, float w) {
     batch_items(L, total, [&](int s, i64 f) {
         const clb_batch_scene& g = G[s];
         const i64 of = g.base[level], oc = g.base[level + 1];
         prolong_at<L0>(f, ce + oc, fp + of, L0 ? fop0 + of : nullptr, L0 ? nullptr : fmask + of,
-                       CLB_DIMS(g, level + 1), CLB_DIMS(g, level));
+                       CLB_DIMS(g, level + 1), CLB_DIMS(g, level), w);
     });
 }
 
@@ -364,12 +364,12 @@ template <int KA, int KB>
 __global__ void __launch_bounds__(BOTTOM_THREADS, 1)
     kb_bottom_visit(BList L, const clb_batch_scene* __restrict__ G, int level, float* pa, const float* ba,
                     const float4* opa, const uint8_t* ma, float* pb, float* bb, const float4* opb, const uint8_t* mb,
-                    int pre, int post, int coarse_iters) {
+                    int pre, int post, int coarse_iters, float w) {
     const clb_batch_scene& g = G[L.scene[blockIdx.x]];
     const i64 oa = g.base[level], ob = g.base[level + 1];
     bottom_visit_block<KA, KB, false>(pa + oa, ba + oa, opa + oa, ma + oa, CLB_DIMS(g, level), pb + ob, bb + ob,
                                       opb + ob, mb + ob, CLB_DIMS(g, level + 1), g.delta, pre, post, coarse_iters,
-                                      nullptr);
+                                      nullptr, 2, w);
 }
 
 // Coarse solve of level `level` from shared memory, one block per listed scene.

@@ -57,6 +57,9 @@ int batch_smooth(const clb_batch* B, int level, const clb_batch_list& L, float* 
     return 0;
 }
 
+// The factor of every prolonged correction (clb_batch.prolong_scale; 0 reads as 1).
+static inline float batch_pscale(const clb_batch* B) { return B->prolong_scale > 0.0f ? B->prolong_scale : 1.0f; }
+
 int batch_bottom(const clb_batch* B, int level, int pre, int post, int coarse_iters, cudaStream_t s) {
     const clb_batch_list& L = B->bottom[level];
     if (L.count <= 0) return 0;
@@ -66,7 +69,7 @@ int batch_bottom(const clb_batch* B, int level, int pre, int post, int coarse_it
     kb_bottom_visit<KA, KB><<<L.count, BOTTOM_THREADS, bytes, s>>>(                                               \
         blist(L), B->geom, level, B->p[level], B->b[level], (const float4*)B->op[level], B->mask[level],          \
         B->p[level + 1], B->b[level + 1], (const float4*)B->op[level + 1], B->mask[level + 1], pre, post,         \
-        coarse_iters)
+        coarse_iters, batch_pscale(B))
     const int ka = B->bottom_ka, kb = B->bottom_kb;
     if (ka <= 1 && kb <= 1) CLB_BB(1, 1);
     else if (ka <= 2 && kb <= 1) CLB_BB(2, 1);
@@ -122,10 +125,10 @@ int batch_w_cycle(const clb_batch* B, int level, float* x, const float* rhs, int
     if (batch_w_cycle(B, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
     if (level == 0)
         kb_prolong<true><<<batch_grid(R.total, BT), BT, 0, s>>>(blist(R), R.total, B->geom, 0, B->p[1], fp, B->op0,
-                                                                 nullptr);
+                                                                 nullptr, batch_pscale(B));
     else
         kb_prolong<false><<<batch_grid(R.total, BT), BT, 0, s>>>(blist(R), R.total, B->geom, level, B->p[level + 1],
-                                                                  fp, nullptr, B->mask[level]);
+                                                                  fp, nullptr, B->mask[level], batch_pscale(B));
     CLB_LAUNCH_CHECK("kb_prolong");
     return batch_smooth(B, level, R, fp, fb, post, s);
 }

@@ -608,6 +608,8 @@ typedef struct clb_batch {
     float* b[CLB_MG_MAX_LEVELS];
     uint8_t* mask[CLB_MG_MAX_LEVELS];
     void* op[CLB_MG_MAX_LEVELS];            /* float4 per cell */
+    float prolong_scale;                    /* factor of every prolonged correction (0 or 1: the reference's
+                                               W-cycle), as clb_mg_hierarchy.prolong_scale */
 } clb_batch;
 
 /* Stage API over a batch (pointers are the batch-wide arrays; per-scene constants come from geom).

@@ -80,7 +80,8 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
                              "tile_counts", "zero_outside", "fused_tiles", "cluster_lists", "prolong_scale"],
         "clb_batch_scene": ["base", "particle_base", "delta", "upper", "pad"],
         "clb_batch_list": ["start", "count", "total"],
-        "clb_batch": ["geom_host", "particles", "cells", "colour0", "sweep0", "bottom_smem", "op0", "op"],
+        "clb_batch": ["geom_host", "particles", "cells", "colour0", "sweep0", "bottom_smem", "op0", "op",
+                      "prolong_scale"],
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "clb200.h"', "int main(void) {"]
     for struct, names in fields.items():

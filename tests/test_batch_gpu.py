@@ -55,8 +55,9 @@ def test_reference_mode_matches_single_scenes(backend, use_graph):
     assert backend.device_error() == 0
 
 
-@pytest.mark.parametrize("wset", [{}, {"coarse_iterations": 4, "pre_smooth": 1, "post_smooth": 1}],
-                         ids=["reference-cycle", "c4-s11"])
+@pytest.mark.parametrize("wset", [{}, {"coarse_iterations": 4, "pre_smooth": 1, "post_smooth": 1},
+                                  {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 1, "prolong_scale": 1.7}],
+                         ids=["reference-cycle", "c4-s11", "c0-s11-w17"])
 def test_tolerance_mode_solves_every_scene(backend, wset):
     sc = mixed_scenes()
     b = batch.BatchedFlip(backend, sc, flip_ratio=0.95, tol=1e-6, **wset)
