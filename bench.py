@@ -44,8 +44,12 @@ SMOOTHING_CHOICES = ((2, 4), (2, 2), (1, 2), (1, 1))  # (pre, post); (2, 4): the
 # factor of every prolonged correction in the W-cycle preconditioner; 1.0: the reference's prolongation
 PROLONG_SCALE_CHOICES = (1.0, 1.7)
 # the W-cycle preconditioner settings the Poisson comparison picks at 256^3, used by the other cases
-TUNED_WCYCLE = {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 1, "prolong_scale": 1.7}
+TUNED_WCYCLE = {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 1, "prolong_scale": 1.8,
+                "coarse_smooth": (1, 0)}
 SCALED_COARSE_ITERATIONS = (4, 0)  # coarsest-level iterations tried with the larger factors
+# (coarse-level (pre, post) sweeps, factor) tried with 0 coarsest-level iterations and smoothing (1, 1) and
+# (1, 2) on level 0: with the scaled prolongation the coarse levels' post-smoothing can go
+COARSE_SMOOTH_VARIANTS = (((1, 0), 1.7), ((1, 0), 1.8))
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
                      "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
@@ -88,6 +92,10 @@ def parse_args():
                     help="factor of every correction the W-cycle preconditioner of the timed steps prolongs (1: the "
                          "reference's piecewise-constant prolongation; auto: 1.7 when it is the fastest to the tolerance "
                          "with 4 coarsest-level iterations in the Poisson comparison, together with its smoothing)")
+    ap.add_argument("--coarse-smooth", default="auto",
+                    help="smoothing sweeps before,after the coarse-grid correction on the levels below the finest in "
+                         "the timed steps, e.g. 1,0 (none: the --smoothing counts on every level, the reference; auto: "
+                         "the Poisson comparison's choice)")
     ap.add_argument("--single-visit", type=int, default=0,
                     help="first multigrid level visited once (not twice) per visit of the level above in the W-cycle "
                          "preconditioner (0 = the reference's W-cycle; at 256^3 levels 3 and 2 need 20 and 27 FCG "
@@ -145,8 +153,8 @@ def batch_case(args):
                    "particles": b.n, "cells": b.C0, "pressure_tolerance": TOL,
                    "pressure_solver": f"per-scene flexible CG preconditioned by one W-cycle (pre {wset['pre_smooth']}, "
                                       f"post {wset['post_smooth']}, coarse {wset['pre_smooth']}+"
-                                      f"{wset['coarse_iterations']}, prolonged corrections x{wset['prolong_scale']:g}), "
-                                      "FP64 accumulation"},
+                                      f"{wset['coarse_iterations']}, prolonged corrections x{wset['prolong_scale']:g}, "
+                                      f"coarser levels {wset.get('coarse_smooth')}), FP64 accumulation"},
         "particles_per_s": b.n * 1e3 / ms,
         "cycles_per_step": [st.cycles for st in stats],
         "rel_residual_max": max(max(st.rel_residual) for st in stats),
@@ -438,10 +446,12 @@ def workload_config(size, n_particles, args):
     }
 
 
-def solver_description(method, pre, post, k, fp16_levels=None, single_from=0, prolong_scale=1.0):
+def solver_description(method, pre, post, k, fp16_levels=None, single_from=0, prolong_scale=1.0, coarse_smooth=None):
     storage = f", levels {fp16_levels[0][0]}^3 and coarser stored in FP16" if fp16_levels else ""
     if prolong_scale != 1.0:
         storage += f", prolonged corrections x{prolong_scale:g}"
+    if coarse_smooth:
+        storage += f", coarser levels pre {coarse_smooth[0]}, post {coarse_smooth[1]}"
     cycle = "W-cycle" if not single_from else f"W-cycle (levels {single_from}+ visited once per parent visit)"
     if method == "fcg":
         return (f"flexible CG preconditioned by one {cycle} computed in FP32 (pre {pre}, post {post}, coarse "
@@ -517,19 +527,18 @@ CPU_FCG = {"coarse_iterations": 4, "pre_smooth": 1, "post_smooth": 1}
 REFERENCE_FIXED_CYCLES = 6
 
 
-def cpu_sim(scene, positions, velocities, tol=TOL, cycles=None, prolong_scale=1.0):
+def cpu_sim(scene, positions, velocities, tol=TOL, cycles=None, **fcg):
     """The reference algorithm on the host cores: the oracle (every reference kernel restated in C++
     with OpenMP, the step order of solver.py:243-529). With ``tol`` each pressure is solved to that
     FP64 relative residual by the flexible CG with the reference's W-cycle as preconditioner (the same
     work as the GPU's timed step); with ``cycles`` by the reference's own method, that fixed number of
-    FP32 W-cycles. ``prolong_scale``: the factor of the W-cycle's prolonged corrections (1: the
-    reference's)."""
+    FP32 W-cycles. ``fcg``: preconditioner settings replacing CPU_FCG's (coarse_iterations, pre_smooth,
+    post_smooth) or adding prolong_scale and coarse_smooth (the timed steps' choices)."""
     from oracle import oracle
 
     return oracle.OracleSim(scene.grid_shape, scene.dx, positions, velocities, dt=scene.dt, flip_ratio=0.95,
                             gravity=scene.gravity, rho=scene.rho, nu=scene.nu, min_size=scene.min_size,
-                            num_vcycles=cycles or 1, tol=None if cycles else tol, prolong_scale=prolong_scale,
-                            **CPU_FCG)
+                            num_vcycles=cycles or 1, tol=None if cycles else tol, **{**CPU_FCG, **fcg})
 
 
 def cpu_steps(sim, steps):
@@ -794,6 +803,13 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                 solvers[f"{name.replace('_c4', f'_c{k}')}_w{round(w * 10)}"] = PressureSolver(
                     kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=ps.coarse_fp16,
                     coarse_iterations=k, pre_smooth=ps.pre_smooth, post_smooth=ps.post_smooth, prolong_scale=w)
+    for fp16 in (False, True):
+        for pre, post in ((1, 1), (1, 2)):
+            for cs, w in COARSE_SMOOTH_VARIANTS:
+                solvers[f"fcg{'_fp16' if fp16 else ''}_c0_s{pre}{post}_w{round(w * 10)}_cs{cs[0]}{cs[1]}"] = \
+                    PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16,
+                                   coarse_iterations=0, pre_smooth=pre, post_smooth=post, prolong_scale=w,
+                                   coarse_smooth=cs)
     single = {}  # variant name -> first level visited once (clb_mg_set_option 4); none by default
     p_tmp = torch.empty_like(sim.pressure)
     rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": [], "fcg_tuned_learned": []}
@@ -899,7 +915,7 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
     # the rule for the prolongation factor (with 4 coarsest-level iterations chosen): the fastest to the
     # tolerance of the chosen smoothing with factor 1 and every smoothing and scaled coarsest-level
     # count with a larger factor, which may change the smoothing and the count too
-    best_w = PROLONG_SCALE_CHOICES[0]
+    best_w, best_cs = PROLONG_SCALE_CHOICES[0], None
     if best_k == 4:
         def c_name(k, s):
             return f"{base}_c{k}" if tuple(s) == SMOOTHING_CHOICES[0] else f"{base}_c{k}_s{s[0]}{s[1]}"
@@ -911,6 +927,12 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                     r = out.get(f"{c_name(k, s)}_w{round(w * 10)}")
                     if r and r["ms_mean"] < best_ms:
                         best_w, best_k, best_s, best_ms = w, k, s, r["ms_mean"]
+        for s in ((1, 1), (1, 2)):
+            for cs, w in COARSE_SMOOTH_VARIANTS:
+                r = out.get(f"{base}_c0_s{s[0]}{s[1]}_w{round(w * 10)}_cs{cs[0]}{cs[1]}")
+                if r and r["ms_mean"] < best_ms:
+                    best_w, best_k, best_s, best_cs, best_ms = w, 0, s, cs, r["ms_mean"]
+    out["coarse_smooth_chosen"] = list(best_cs) if best_cs else None
     out["coarse_iterations_chosen"] = best_k
     out["smoothing_chosen"] = list(best_s)
     out["prolong_scale_chosen"] = best_w
@@ -965,6 +987,8 @@ def our_arm(args):
     coarse_k = COARSE_ITERATION_CHOICES[0] if args.coarse_iterations == "auto" else int(args.coarse_iterations)
     smoothing = SMOOTHING_CHOICES[0] if args.smoothing == "auto" else tuple(int(x) for x in args.smoothing.split(","))
     prolong = PROLONG_SCALE_CHOICES[0] if args.prolong_scale == "auto" else float(args.prolong_scale)
+    coarse_smooth = None if args.coarse_smooth in ("auto", "none") else \
+        tuple(int(x) for x in args.coarse_smooth.split(","))
     single_from = int(args.single_visit)
     if args.poisson_steps > 0:
         poisson.update(poisson_comparison(kernels, sim, args.poisson_steps, warm, scene.min_size))
@@ -976,6 +1000,8 @@ def our_arm(args):
             smoothing = tuple(poisson.get("smoothing_chosen", smoothing))
         if args.prolong_scale == "auto":
             prolong = float(poisson.get("prolong_scale_chosen", prolong))
+        if args.coarse_smooth == "auto" and poisson.get("coarse_smooth_chosen"):
+            coarse_smooth = tuple(poisson["coarse_smooth_chosen"])
         if args.learned == "auto" and "fcg_tuned_learned" in poisson:
             # the rule: the learned guess in the timed steps only when it makes the solve faster,
             # network evaluation included
@@ -987,16 +1013,19 @@ def our_arm(args):
         warm_note += " (not used in the timed steps: no faster than without it in the comparison)"
     kernels.call("clb_mg_set_option", 4, single_from)  # read when the timed solver captures its graphs
     if use_fp16 or coarse_k != sim.options.coarse_iterations or single_from or \
-            smoothing != (sim.options.pre_smooth, sim.options.post_smooth) or prolong != sim.options.prolong_scale:
+            smoothing != (sim.options.pre_smooth, sim.options.post_smooth) or prolong != sim.options.prolong_scale or \
+            coarse_smooth != sim.options.coarse_smooth:
         from continuum_liquid_b200.pressure_solve import PressureSolver
 
         sim.options.coarse_fp16 = use_fp16
         sim.options.coarse_iterations = coarse_k
         sim.options.pre_smooth, sim.options.post_smooth = smoothing
         sim.options.prolong_scale = prolong
+        sim.options.coarse_smooth = coarse_smooth
         sim.pressure_solver = PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=scene.min_size,
                                              method=args.method, coarse_fp16=use_fp16, coarse_iterations=coarse_k,
-                                             pre_smooth=smoothing[0], post_smooth=smoothing[1], prolong_scale=prolong)
+                                             pre_smooth=smoothing[0], post_smooth=smoothing[1], prolong_scale=prolong,
+                                             coarse_smooth=coarse_smooth)
         for _ in range(2):  # tuning and graph capture of the new solver
             sim.step()
         torch.cuda.synchronize()
@@ -1035,6 +1064,7 @@ def our_arm(args):
     # --- Poisson time to 1e-6 in the timed steps ------------------------------------------------
     poisson = {"timed_steps": {"method": args.method, "learned": warm_note, "coarse_fp16": use_fp16,
                                "coarse_iterations": coarse_k, "smoothing": list(smoothing), "prolong_scale": prolong,
+                               "coarse_smooth": list(coarse_smooth) if coarse_smooth else None,
                                "ms_mean": float(np.mean(solve_ms)),
                                "cycles_mean": float(np.mean(cycles)),
                                "final_rel_residual_max": float(max(s.rel_residual or 0.0 for s in stats)),
@@ -1111,8 +1141,10 @@ def our_arm(args):
     # --- CPU baseline (rank 0, N = 1): the reference algorithm on the host cores ---------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu_times, cpu_cycles = cpu_steps(cpu_sim(scene, positions, velocities,
-                                                  prolong_scale=sim.options.prolong_scale), 1)
+        o = sim.options
+        cpu_times, cpu_cycles = cpu_steps(cpu_sim(scene, positions, velocities, coarse_iterations=o.coarse_iterations,
+                                                  pre_smooth=o.pre_smooth, post_smooth=o.post_smooth,
+                                                  prolong_scale=o.prolong_scale, coarse_smooth=o.coarse_smooth), 1)
         cpu = {"value": 1.0 / cpu_times[0], "unit": UNIT, "cores": cpu_threads(), "kind": "port",
                "sample": f"the first step of the same scene ({n} particles) by the CPU restatement of the reference "
                          f"kernels, its pressure solved to {TOL:g} ({cpu_cycles[0]} cycles of the same iteration)"}
@@ -1122,7 +1154,7 @@ def our_arm(args):
         fp16_levels = [list(s) for s in h.shapes[h.fp16_level:]] if h.fp16_level else None
         solver_info = {"pressure": solver_description(args.method, sim.options.pre_smooth, sim.options.post_smooth,
                                                       sim.options.coarse_iterations, fp16_levels, single_from,
-                                                      sim.options.prolong_scale),
+                                                      sim.options.prolong_scale, sim.options.coarse_smooth),
                        "p2g": "tiled scatter (k_p2g_tiled)" if sim.options.tiled_p2g() else
                               "reference-order gather (k_p2g_gather)",
                        "multigrid_levels": [list(s) for s in h.shapes], "sweep_kinds": h.sweeps(),

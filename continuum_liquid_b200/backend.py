@@ -162,6 +162,9 @@ class MGHierarchy(ctypes.Structure):
         ("fused_tile_count", ctypes.c_void_p),
         ("cluster_lists", ctypes.c_void_p),
         ("prolong_scale", ctypes.c_float),
+        ("coarse_smoothing", ctypes.c_int32),
+        ("coarse_pre_smooth", ctypes.c_int32),
+        ("coarse_post_smooth", ctypes.c_int32),
     ]
 
 
@@ -229,6 +232,9 @@ class Batch(ctypes.Structure):
         ("mask", ctypes.c_void_p * MG_MAX_LEVELS),
         ("op", ctypes.c_void_p * MG_MAX_LEVELS),
         ("prolong_scale", ctypes.c_float),
+        ("coarse_smoothing", ctypes.c_int32),
+        ("coarse_pre_smooth", ctypes.c_int32),
+        ("coarse_post_smooth", ctypes.c_int32),
     ]
 
 

@@ -72,7 +72,7 @@ class BatchedFlip:
                  num_vcycles: int = 1, reduce_blocks: int = 32, sweep0: int = 1, use_graph: bool = True,
                  max_cycles: int = 100, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS,
                  pre_smooth: int = PRE_SMOOTH, post_smooth: int = POST_SMOOTH, tiled_p2g: bool | None = None,
-                 prolong_scale: float = 1.0):
+                 prolong_scale: float = 1.0, coarse_smooth=None):
         if not 1 <= len(scenes) <= BATCH_MAX_SCENES:
             raise ValueError(f"a batch holds 1..{BATCH_MAX_SCENES} scenes, got {len(scenes)}")
         first = scenes[0]
@@ -97,6 +97,8 @@ class BatchedFlip:
         self.prolong_scale = float(prolong_scale)
         if not self.prolong_scale > 0.0:
             raise ValueError("prolong_scale must be > 0")
+        # smoothing counts (pre, post) of levels >= 1 (PressureSolver.coarse_smooth; None: every level as 0)
+        self.coarse_smooth = None if coarse_smooth is None else tuple(int(x) for x in coarse_smooth)
         self.ppc = first.particles_per_cell
         self.use_graph = use_graph
         dev = kernels.device
@@ -296,8 +298,12 @@ class BatchedFlip:
         self._swap()
 
     def _w_cycle(self, x, rhs, coarse_iterations: int = COARSE_SMOOTH_ITERATIONS, pre: int = PRE_SMOOTH,
-                 post: int = POST_SMOOTH, prolong_scale: float = 1.0) -> None:
-        self.batch.prolong_scale = float(prolong_scale)  # read when the W-cycle is launched or captured
+                 post: int = POST_SMOOTH, prolong_scale: float = 1.0, coarse_smooth=None) -> None:
+        # read when the W-cycle is launched or captured
+        self.batch.prolong_scale = float(prolong_scale)
+        self.batch.coarse_smoothing = 0 if coarse_smooth is None else 1
+        if coarse_smooth is not None:
+            self.batch.coarse_pre_smooth, self.batch.coarse_post_smooth = (int(x) for x in coarse_smooth)
         self._call("clb_batch_w_cycle", x, rhs, int(pre), int(post), int(coarse_iterations))
 
     def _init_solve(self) -> None:
@@ -310,7 +316,7 @@ class BatchedFlip:
     def _iteration(self, src: int) -> None:
         self.correction.zero_()
         self._w_cycle(self.correction, self.residual, self.coarse_iterations, self.pre_smooth, self.post_smooth,
-                      self.prolong_scale)
+                      self.prolong_scale, self.coarse_smooth)
         self._call("clb_batch_fcg_dots", self.correction, self.direction[src], self.residual, self.partials4,
                    self.fcg_state)
         self._call("clb_batch_fcg_step", self.p64[src], self.correction, self.direction[src], self.p64[1 - src],

@@ -102,8 +102,12 @@ int batch_coarse(const clb_batch* B, int level, int iterations, cudaStream_t s) 
 
 // multigrid.py:53-187 w_cycle for every scene at once: at each level the scenes split into those whose
 // coarsest level this is, those whose bottom visit runs here and those that smooth and recurse.
-int batch_w_cycle(const clb_batch* B, int level, float* x, const float* rhs, int pre, int post, int coarse_iters,
+// pre0 / post0: the W-cycle's smoothing counts; levels >= 1 use the batch's coarse counts when it sets
+// them (clb_batch.coarse_smoothing)
+int batch_w_cycle(const clb_batch* B, int level, float* x, const float* rhs, int pre0, int post0, int coarse_iters,
                   cudaStream_t s) {
+    const bool coarse = level > 0 && B->coarse_smoothing;
+    const int pre = coarse ? B->coarse_pre_smooth : pre0, post = coarse ? B->coarse_post_smooth : post0;
     if (batch_coarse(B, level, pre + coarse_iters, s)) return 1;
     if (batch_bottom(B, level, pre, post, coarse_iters, s)) return 1;
     const clb_batch_list& R = B->recurse[level];
@@ -121,8 +125,8 @@ int batch_w_cycle(const clb_batch* B, int level, float* x, const float* rhs, int
             blist(RC), RC.total, B->geom, level, fp, fb, nullptr, (const float4*)B->op[level], B->mask[level],
             B->p[level + 1], B->b[level + 1]);
     CLB_LAUNCH_CHECK("kb_restrict");
-    if (batch_w_cycle(B, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
-    if (batch_w_cycle(B, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+    if (batch_w_cycle(B, level + 1, x, rhs, pre0, post0, coarse_iters, s)) return 1;
+    if (batch_w_cycle(B, level + 1, x, rhs, pre0, post0, coarse_iters, s)) return 1;
     if (level == 0)
         kb_prolong<true><<<batch_grid(R.total, BT), BT, 0, s>>>(blist(R), R.total, B->geom, 0, B->p[1], fp, B->op0,
                                                                  nullptr, batch_pscale(B));
@@ -247,6 +251,8 @@ int clb_batch_w_cycle(const clb_batch* b, float* x, const float* rhs, int pre_sm
     if (check_batch(b)) return 1;
     CLB_REQUIRE(x && rhs && b->op0, "batch_w_cycle: null level-0 array");
     CLB_REQUIRE(pre_smooth >= 0 && post_smooth >= 0 && coarse_iterations >= 0, "batch_w_cycle: negative count");
+    CLB_REQUIRE(!b->coarse_smoothing || (b->coarse_pre_smooth >= 0 && b->coarse_post_smooth >= 0),
+                "batch_w_cycle: negative coarse-level count");
     CLB_REQUIRE(b->sweep0 == 4 || (b->sweep0 == 1 && list_ok(b->colour0)), "batch_w_cycle: bad level-0 sweep");
     return batch_w_cycle(b, 0, x, rhs, pre_smooth, post_smooth, coarse_iterations, CLB_STREAM(stream));
 }

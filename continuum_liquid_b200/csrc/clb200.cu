@@ -1178,6 +1178,14 @@ int level0_zero(const clb_mg_hierarchy* h, const LevelView& v, int first_sweeps,
 int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int pre, int post, int coarse_iters,
             cudaStream_t s);
 
+// pre / post: the W-cycle's smoothing counts (level 0's). Levels >= 1 use the hierarchy's coarse counts
+// when it sets them (clb_mg_hierarchy.coarse_smoothing), so each frame maps the counts of its own level
+// and of the level below, and passes the W-cycle's on.
+static inline int coarse_pre(const clb_mg_hierarchy* h, int pre) { return h->coarse_smoothing ? h->coarse_pre_smooth : pre; }
+static inline int coarse_post(const clb_mg_hierarchy* h, int post) {
+    return h->coarse_smoothing ? h->coarse_post_smooth : post;
+}
+
 // Whether level 0 of this W-cycle runs as the fused tile launches of mg_level0.cuh: sweep kind 7 on
 // level 0, its 3-D fluid tiles and second buffer, a correction from zero (zero_outside = 2), at least
 // one pre- and one post-smoothing iteration, and an FP32 level 1 below.
@@ -1230,7 +1238,7 @@ int w_cycle_level0_fused(const clb_mg_hierarchy* h, float* x, const float* rhs, 
         dst ^= 1;
     }
     const int visits = visits_of(1);
-    const int both = cluster_visit(h, 1, pre, post, coarse_iters, s, visits);
+    const int both = cluster_visit(h, 1, coarse_pre(h, pre), coarse_post(h, post), coarse_iters, s, visits);
     if (both < 0) return 1;
     if (both == 0)
         for (int v2 = 0; v2 < visits; ++v2)
@@ -1246,9 +1254,12 @@ int w_cycle_level0_fused(const clb_mg_hierarchy* h, float* x, const float* rhs, 
     return 0;
 }
 
-int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int pre, int post, int coarse_iters,
+int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, int pre0, int post0, int coarse_iters,
             cudaStream_t s) {
-    if (level == 0 && level0_fused(h, pre, post)) return w_cycle_level0_fused(h, x, rhs, pre, post, coarse_iters, s);
+    if (level == 0 && level0_fused(h, pre0, post0))
+        return w_cycle_level0_fused(h, x, rhs, pre0, post0, coarse_iters, s);
+    const int pre = level > 0 ? coarse_pre(h, pre0) : pre0, post = level > 0 ? coarse_post(h, post0) : post0;
+    const int cpre = coarse_pre(h, pre0), cpost = coarse_post(h, post0);  // the level below's
     const LevelView v = level_view(h, level, x, rhs);
     // coarse levels hold 0 outside the fluid (zeroed by clb_mg_build_coarse and the restriction);
     // level 0 does when the caller says so
@@ -1294,11 +1305,11 @@ int w_cycle(const clb_mg_hierarchy* h, int level, float* x, const float* rhs, in
     // the visits of the level below (two, or one from the single-visit level on): one cluster launch
     // for them when it takes the cluster path
     const int visits = visits_of(level + 1);
-    const int both = cluster_visit(h, level + 1, pre, post, coarse_iters, s, visits);
+    const int both = cluster_visit(h, level + 1, cpre, cpost, coarse_iters, s, visits);
     if (both < 0) return 1;
     if (both == 0)
         for (int v2 = 0; v2 < visits; ++v2)
-            if (w_cycle(h, level + 1, x, rhs, pre, post, coarse_iters, s)) return 1;
+            if (w_cycle(h, level + 1, x, rhs, pre0, post0, coarse_iters, s)) return 1;
     const i64 Cf = (i64)v.nx * v.ny * v.nz;
     const int fvec = v.l0 && tile_k(v.nz, true) == 128 ? 4 : 1;
     const float w = pscale(h);
@@ -1344,6 +1355,8 @@ int clb_mg_w_cycle(const clb_mg_hierarchy* h, float* x, const float* rhs, int pr
     if (check_hierarchy(h)) return 1;
     CLB_REQUIRE(x && rhs, "mg_w_cycle: null level-0 array");
     CLB_REQUIRE(pre_smooth >= 0 && post_smooth >= 0 && coarse_iterations >= 0, "mg_w_cycle: negative sweep count");
+    CLB_REQUIRE(!h->coarse_smoothing || (h->coarse_pre_smooth >= 0 && h->coarse_post_smooth >= 0),
+                "mg_w_cycle: negative coarse-level sweep count");
     cudaStream_t s = CLB_STREAM(stream);
     if (h->fp16_level > 0) {
         CLB_REQUIRE(h->rhs_norms != nullptr, "mg_w_cycle: FP16 levels need rhs_norms");

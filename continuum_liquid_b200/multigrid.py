@@ -271,18 +271,32 @@ class MultigridHierarchy:
 
     def w_cycle(self, x, rhs, pre_smooth=PRE_SMOOTH, post_smooth=POST_SMOOTH,
                 coarse_iterations=COARSE_SMOOTH_ITERATIONS, queue=None, x_zero_outside: bool = False,
-                x_from_zero: bool = False, prolong_scale: float = 1.0) -> None:
+                x_from_zero: bool = False, prolong_scale: float = 1.0, coarse_smooth=None) -> None:
         """One W-cycle on level-0 unknown ``x`` and right-hand side ``rhs``. ``x_zero_outside``: the
         caller guarantees that ``x`` is 0 at every cell that is not fluid (a zeroed correction), so the
         level-0 sweeps may skip the tiles without fluid. ``x_from_zero``: the W-cycle starts from a zero
         ``x`` although ``x`` still holds a previous correction at fluid cells (it must be 0 at every
         other cell): the first sweep ignores ``x`` instead of the caller zeroing it.
         ``prolong_scale``: every prolonged correction is multiplied by it (1: the reference's W-cycle;
-        no counterpart in the reference, see clb_mg_hierarchy.prolong_scale)."""
+        no counterpart in the reference, see clb_mg_hierarchy.prolong_scale). ``coarse_smooth``: (pre, post)
+        smoothing counts of levels >= 1 (None: ``pre_smooth`` / ``post_smooth`` on every level, the
+        reference)."""
         self.struct.zero_outside = 2 if x_from_zero else (1 if x_zero_outside else 0)
         self.struct.prolong_scale = float(prolong_scale)
+        self.set_coarse_smooth(coarse_smooth)
         self.kernels.call_hierarchy("clb_mg_w_cycle", self.struct, x, rhs, int(pre_smooth), int(post_smooth),
                                     int(coarse_iterations), stream=queue)
+
+    def set_coarse_smooth(self, coarse_smooth) -> None:
+        """Smoothing counts (pre, post) of levels >= 1 for the W-cycles that follow (None: the W-cycle's)."""
+        if coarse_smooth is None:
+            self.struct.coarse_smoothing = 0
+            return
+        pre, post = (int(x) for x in coarse_smooth)
+        if pre < 0 or post < 0:
+            raise ValueError("coarse_smooth counts must be >= 0")
+        self.struct.coarse_smoothing = 1
+        self.struct.coarse_pre_smooth, self.struct.coarse_post_smooth = pre, post
 
     def set_sweep(self, level: int, kind: int) -> None:
         """Red-black sweep implementation of one level (see clb_mg_hierarchy.sweep); FP16 levels take

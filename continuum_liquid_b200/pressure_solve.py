@@ -115,7 +115,8 @@ class PressureSolver:
                  autotune: bool = True, method: str = "fcg", coarse_fp16: bool = False, fp16_max_size: int = 64,
                  coarse_iterations: int = multigrid.COARSE_SMOOTH_ITERATIONS,
                  pre_smooth: int = multigrid.PRE_SMOOTH, post_smooth: int = multigrid.POST_SMOOTH,
-                 fused_level0: bool = False, device_loop: bool = False, prolong_scale: float = 1.0):
+                 fused_level0: bool = False, device_loop: bool = False, prolong_scale: float = 1.0,
+                 coarse_smooth=None):
         if method not in METHODS:
             raise ValueError(f"unknown pressure solve method {method!r} (expected one of {METHODS})")
         self.coarse_fp16 = bool(coarse_fp16)
@@ -140,6 +141,12 @@ class PressureSolver:
         self.prolong_scale = float(prolong_scale)
         if not self.prolong_scale > 0.0:
             raise ValueError("prolong_scale must be > 0")
+        # smoothing counts (pre, post) of levels >= 1 in the tolerance mode's W-cycle (None: pre_smooth and
+        # post_smooth on every level, as the reference). With the scaled prolongation the coarse levels'
+        # post-smoothing can go: (1, 0) needs 0-1 more cycles and each cycle is ~20 % cheaper at 256^3
+        self.coarse_smooth = None if coarse_smooth is None else tuple(int(x) for x in coarse_smooth)
+        if self.coarse_smooth is not None and (len(self.coarse_smooth) != 2 or min(self.coarse_smooth) < 0):
+            raise ValueError("coarse_smooth must be a pair of counts >= 0")
         # fused_level0: the tolerance mode's W-cycles run level 0 as fused tile launches (sweep kind 7,
         # csrc/mg_level0.cuh), with the values of the launch-per-step path. Off by default: at 256^3 the
         # recomputed halo costs more instructions than the four launches it saves
@@ -217,7 +224,7 @@ class PressureSolver:
         try:
             h.w_cycle(self.correction, self.residual, pre_smooth=self.pre_smooth, post_smooth=self.post_smooth,
                       coarse_iterations=self.coarse_iterations, queue=queue, x_from_zero=True,
-                      prolong_scale=self.prolong_scale)
+                      prolong_scale=self.prolong_scale, coarse_smooth=self.coarse_smooth)
         finally:
             h.struct.sweep[0] = kind0
         delta = float(FIELD_DTYPE(self.dx))
@@ -364,6 +371,7 @@ class PressureSolver:
         if self.fused_level0:
             h.struct.sweep[0] = 7
         h.struct.prolong_scale = self.prolong_scale  # read when the loop's refinement is captured
+        h.set_coarse_smooth(self.coarse_smooth)
         out = ctypes.c_void_p()
         from .backend import ptr
 

@@ -63,6 +63,9 @@ class StepOptions:
     # tolerance mode: the factor of every correction the W-cycle preconditioner prolongs (1: the
     # reference's piecewise-constant prolongation; about 1.7 needs far fewer cycles, see PressureSolver)
     prolong_scale: float = 1.0
+    # tolerance mode: (pre, post) smoothing counts of levels >= 1 in the W-cycle preconditioner (None: the
+    # pre_smooth / post_smooth above on every level, the reference)
+    coarse_smooth: tuple | None = None
     revoxelise: bool = False  # voxelise the colliders again at every step (moving or deforming meshes)
     # P2G gather: "exact" (the reference's summation order, bit for bit), "tiled" (each particle visited
     # once; equal to float rounding) or "auto" (exact in the reference's fixed-cycle mode, tiled when
@@ -128,7 +131,8 @@ class FlipSolver:
                                               coarse_iterations=self.options.coarse_iterations,
                                               pre_smooth=self.options.pre_smooth,
                                               post_smooth=self.options.post_smooth,
-                                              prolong_scale=self.options.prolong_scale)
+                                              prolong_scale=self.options.prolong_scale,
+                                              coarse_smooth=self.options.coarse_smooth)
         self.last_solve: SolveStats | None = None
         self.steps_done = 0
 

@@ -319,6 +319,12 @@ typedef struct clb_mg_hierarchy {
      * piecewise-constant prolongation under-corrects; about 1.7 makes the W-cycle a much stronger
      * preconditioner of the tolerance mode's iteration. */
     float prolong_scale;
+    /* No counterpart in the reference: 1 gives levels >= 1 their own smoothing counts (coarse_pre_smooth
+     * sweeps before and coarse_post_smooth after the coarse-grid correction, the coarsest level's solve
+     * coarse_pre_smooth + coarse_iterations); 0: every level uses clb_mg_w_cycle's counts (the reference). */
+    int32_t coarse_smoothing;
+    int32_t coarse_pre_smooth;
+    int32_t coarse_post_smooth;
 } clb_mg_hierarchy;
 
 /* Number of tiles of a level of nx x ny x nz cells (finest != 0: the finest level's tile shape). */
@@ -610,6 +616,9 @@ typedef struct clb_batch {
     void* op[CLB_MG_MAX_LEVELS];            /* float4 per cell */
     float prolong_scale;                    /* factor of every prolonged correction (0 or 1: the reference's
                                                W-cycle), as clb_mg_hierarchy.prolong_scale */
+    int32_t coarse_smoothing;               /* as clb_mg_hierarchy.coarse_smoothing */
+    int32_t coarse_pre_smooth;
+    int32_t coarse_post_smooth;
 } clb_batch;
 
 /* Stage API over a batch (pointers are the batch-wide arrays; per-scene constants come from geom).

@@ -962,8 +962,12 @@ struct Levels {
 // visit of the level above instead of twice (the solver's clb_mg_set_option 4).
 template <typename T>
 void w_cycle(const Levels<T>& L, int level, T delta, int pre, int post, int coarse_iters, int single_from = 0,
-             T prolong_scale = 1) {
+             T prolong_scale = 1, int pre_coarse = -1, int post_coarse = -1) {
     const int* s = L.shape + 3 * level;
+    // pre_coarse / post_coarse >= 0 (no counterpart in the reference): the smoothing counts of levels >= 1,
+    // the coarsest level's solve included (pre + coarse_iters iterations)
+    if (level > 0 && pre_coarse >= 0) pre = pre_coarse;
+    if (level > 0 && post_coarse >= 0) post = post_coarse;
     if (level == L.count - 1) {
         coarse_smooth<T>(L.p[level], L.b[level], L.m[level], L.d[level], L.wx[level], L.wy[level], L.wz[level], delta,
                          pre + coarse_iters, s[0], s[1], s[2]);
@@ -979,7 +983,8 @@ void w_cycle(const Levels<T>& L, int level, T delta, int pre, int post, int coar
                          L.b[c], L.m[c], L.d[c], L.wx[c], L.wy[c], L.wz[c], delta, s[0], s[1], s[2], cs[0], cs[1],
                          cs[2]);
     const int visits = single_from > 0 && c >= single_from ? 1 : 2;
-    for (int v = 0; v < visits; ++v) w_cycle<T>(L, c, delta, pre, post, coarse_iters, single_from, prolong_scale);
+    for (int v = 0; v < visits; ++v)
+        w_cycle<T>(L, c, delta, pre, post, coarse_iters, single_from, prolong_scale, pre_coarse, post_coarse);
     prolongate<T>(L.p[c], L.p[level], L.m[level], cs[0], cs[1], cs[2], s[0], s[1], s[2], prolong_scale);
     for (int it = 0; it < post; ++it)
         for (int parity = 0; parity < 2; ++parity)
@@ -1041,15 +1046,15 @@ void orc_coarse_smooth_f32(float* p, const float* b, const float* m, const float
 // W-cycle over a level list whose arrays are given as pointer tables (level 0 = finest).
 void orc_w_cycle_f32(float** p, float** b, float** m, float** d, float** wx, float** wy, float** wz, const int* shapes,
                      int levels, float delta, int pre, int post, int coarse_iters, int single_from,
-                     float prolong_scale) {
+                     float prolong_scale, int pre_coarse, int post_coarse) {
     Levels<float> L{p, b, m, d, wx, wy, wz, shapes, levels};
-    w_cycle<float>(L, 0, delta, pre, post, coarse_iters, single_from, prolong_scale);
+    w_cycle<float>(L, 0, delta, pre, post, coarse_iters, single_from, prolong_scale, pre_coarse, post_coarse);
 }
 void orc_w_cycle_f64(double** p, double** b, double** m, double** d, double** wx, double** wy, double** wz,
                      const int* shapes, int levels, double delta, int pre, int post, int coarse_iters, int single_from,
-                     double prolong_scale) {
+                     double prolong_scale, int pre_coarse, int post_coarse) {
     Levels<double> L{p, b, m, d, wx, wy, wz, shapes, levels};
-    w_cycle<double>(L, 0, delta, pre, post, coarse_iters, single_from, prolong_scale);
+    w_cycle<double>(L, 0, delta, pre, post, coarse_iters, single_from, prolong_scale, pre_coarse, post_coarse);
 }
 void orc_residual_norms_f32(const float* p, const float* b, const float* m, const float* d, const float* wx,
                             const float* wy, const float* wz, float delta, int nx, int ny, int nz, double* rr,

@@ -57,8 +57,8 @@ _SIGS = {
     "orc_prolongate_f32": [_f32p, _f32p, _f32p, _I, _I, _I, _I, _I, _I],
     "orc_rbgs_step_f32": [_f32p] * 7 + [_F, _I, _I, _I, _I],
     "orc_coarse_smooth_f32": [_f32p] * 7 + [_F, _I, _I, _I, _I],
-    "orc_w_cycle_f32": [_P] * 7 + [_P, _I, _F, _I, _I, _I, _I, _F],
-    "orc_w_cycle_f64": [_P] * 7 + [_P, _I, _D, _I, _I, _I, _I, _D],
+    "orc_w_cycle_f32": [_P] * 7 + [_P, _I, _F, _I, _I, _I, _I, _F, _I, _I],
+    "orc_w_cycle_f64": [_P] * 7 + [_P, _I, _D, _I, _I, _I, _I, _D, _I, _I],
     "orc_residual_norms_f32": [_f32p] * 7 + [_F, _I, _I, _I, _P, _P],
     "orc_residual_norms_f64": [_f64p] * 7 + [_D, _I, _I, _I, _P, _P],
     "orc_fcg_update": [_f32p, _f32p, _f64p, _f64p, _f32p, _f64p, _f32p, _f64p, _f64p, _f64p, _f64p, _D, _I, _I, _I,
@@ -273,10 +273,12 @@ class Levels:
         self.m = [None] + [np.zeros(s, dtype) for s in self.shapes[1:]]
         self.ops = [None] + [[np.zeros(s, dtype) for _ in range(4)] for s in self.shapes[1:]]
 
-    def w_cycle(self, p, b, mask, op0, delta, pre=2, post=4, coarse=64, single_from=0, prolong_scale=1.0):
+    def w_cycle(self, p, b, mask, op0, delta, pre=2, post=4, coarse=64, single_from=0, prolong_scale=1.0,
+                pre_coarse=-1, post_coarse=-1):
         """multigrid.py:53-187 (C++ recursion over the whole pyramid). single_from > 0: levels from it on
         are visited once per visit of the level above; prolong_scale: every prolonged correction is
-        multiplied by it (1: the reference). Both are preconditioner variants of the solver's."""
+        multiplied by it (1: the reference); pre_coarse / post_coarse >= 0: the smoothing counts of levels >= 1
+        (-1: pre / post, the reference). All are preconditioner variants of the solver's."""
         dt = self.dtype
         arrs = [c(p, dt), c(b, dt), c(mask, dt), [c(a, dt) for a in op0]]
         assert arrs[0] is p, "p must be a contiguous array of the level dtype (updated in place)"
@@ -296,10 +298,10 @@ class Levels:
         keep = (arrs, P, B, M, Dg, Wx, Wy, Wz, shapes)  # noqa: F841 - keep buffers alive during the call
         if dt == np.float32:
             lib().orc_w_cycle_f32(P, B, M, Dg, Wx, Wy, Wz, shapes, n, F32(delta), pre, post, coarse, single_from,
-                                  F32(prolong_scale))
+                                  F32(prolong_scale), int(pre_coarse), int(post_coarse))
         else:
             lib().orc_w_cycle_f64(P, B, M, Dg, Wx, Wy, Wz, shapes, n, float(delta), pre, post, coarse, single_from,
-                                  float(prolong_scale))
+                                  float(prolong_scale), int(pre_coarse), int(post_coarse))
 
 
 def residual_norms(p, b, mask, op0, delta):
@@ -365,14 +367,15 @@ def apply_operator64(p, mask, op0, delta):
 
 
 def fcg_solve(rhs, ff, shape, dx, p0=None, tol=1e-6, max_cycles=100, flexible=True, coarse_iterations=64,
-              pre_smooth=2, post_smooth=4, single_from=0, prolong_scale=1.0):
+              pre_smooth=2, post_smooth=4, single_from=0, prolong_scale=1.0, coarse_smooth=None):
     """Flexible CG (Notay, truncation 1) preconditioned by one FP32 W-cycle from zero, with the
     pressure, residual and scalars in FP64 (the product's tolerance-mode iteration; the reference
     has no counterpart). ``flexible=False`` is plain refinement p += W(r). ``coarse_iterations``:
     red-black iterations of each coarsest-level solve in the W-cycle (the reference's 64 by default);
     ``pre_smooth``/``post_smooth``: its smoothing sweeps per level (the reference's 2 and 4);
     ``single_from``: levels from it on visited once per parent visit (0: the reference's two);
-    ``prolong_scale``: the factor of every prolonged correction (1: the reference's W-cycle).
+    ``prolong_scale``: the factor of every prolonged correction (1: the reference's W-cycle);
+    ``coarse_smooth``: (pre, post) smoothing counts of levels >= 1 (None: pre_smooth / post_smooth).
     Returns the FP64 pressure and the relative-residual history (one entry per W-cycle, the first
     for p0)."""
     levels = Levels(shape)
@@ -395,12 +398,13 @@ def fcg_solve(rhs, ff, shape, dx, p0=None, tol=1e-6, max_cycles=100, flexible=Tr
                              ctypes.addressof(rr))
         return float(np.sqrt(rr.value)) / nb if nb else 0.0
 
+    cpre, cpost = (-1, -1) if coarse_smooth is None else (int(coarse_smooth[0]), int(coarse_smooth[1]))
     hist = [update(False)]  # e = 0: only the initial residual
     while hist[-1] > tol and len(hist) <= max_cycles:
         e[...] = 0.0
         levels.w_cycle(e, r32.copy(), ff32, op32, F32(float(dx)), pre=int(pre_smooth), post=int(post_smooth),
                        coarse=int(coarse_iterations), single_from=int(single_from),
-                       prolong_scale=float(prolong_scale))
+                       prolong_scale=float(prolong_scale), pre_coarse=cpre, post_coarse=cpost)
         hist.append(update(flexible))
     return x, hist
 
@@ -413,7 +417,7 @@ class OracleSim:
     def __init__(self, shape, dx, positions, velocities, obstacle=None, dt=1.0 / 240.0, flip_ratio=1.0,
                  gravity=(0.0, 0.0, -9.81), rho=1000.0, nu=1.0e-6, ppc=8, min_size=8, num_vcycles=1, tol=None,
                  coarse_iterations=64, pre_smooth=2, post_smooth=4, collider_pose=None, origin=(0.0, 0.0, 0.0),
-                 prolong_scale=1.0):
+                 prolong_scale=1.0, coarse_smooth=None):
         self.shape = tuple(int(s) for s in shape)
         self.dx, self.dt, self.flip_ratio = float(dx), float(dt), float(flip_ratio)
         self.gravity, self.rho, self.nu, self.ppc = tuple(gravity), float(rho), float(nu), ppc
@@ -423,7 +427,7 @@ class OracleSim:
         # the reference's fixed num_vcycles W-cycles
         self.tol = tol
         self.fcg_options = dict(coarse_iterations=coarse_iterations, pre_smooth=pre_smooth, post_smooth=post_smooth,
-                                prolong_scale=prolong_scale)
+                                prolong_scale=prolong_scale, coarse_smooth=coarse_smooth)
         self.last_cycles = 0
         # moving colliders: collider_pose(t) -> (world triangle arrays at time t, the 9 motion parameters
         # in grid-local coordinates); each step voxelises them at the step's start time

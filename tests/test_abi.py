@@ -43,7 +43,8 @@ def test_hierarchy_struct_layout():
     # int32 levels (0), int32[16][3] (4..196), float delta (196), int32 fp16_level (200), then
     # 8-byte-aligned pointers: op0 at 208, the five pointer tables, int32 sweep[16], the three FP16
     # pointers, the tile table, the tile counts, the int32 zero_outside flag (padded to 8 bytes), the
-    # two fused-tile pointers, the cluster lists and the float prolong_scale
+    # two fused-tile pointers, the cluster lists, the float prolong_scale and the three int32 coarse
+    # smoothing fields
     assert backend.MGHierarchy.delta.offset == 196
     assert backend.MGHierarchy.fp16_level.offset == 200
     assert backend.MGHierarchy.op0.offset == 208
@@ -55,7 +56,8 @@ def test_hierarchy_struct_layout():
     assert backend.MGHierarchy.fused_tiles.offset == tiles + 16 * 8 + 8 + 8
     assert backend.MGHierarchy.cluster_lists.offset == tiles + 16 * 8 + 8 + 8 + 2 * 8
     assert backend.MGHierarchy.prolong_scale.offset == tiles + 16 * 8 + 8 + 8 + 3 * 8
-    assert ctypes.sizeof(backend.MGHierarchy) == tiles + 16 * 8 + 8 + 8 + 4 * 8  # the float padded to 8
+    assert backend.MGHierarchy.coarse_post_smooth.offset == tiles + 16 * 8 + 8 + 8 + 3 * 8 + 12
+    assert ctypes.sizeof(backend.MGHierarchy) == tiles + 16 * 8 + 8 + 8 + 5 * 8
 
 
 def test_backend_without_gpu_fails_loudly(monkeypatch):
@@ -77,11 +79,12 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
     src = tmp_path / "layout.c"
     fields = {
         "clb_mg_hierarchy": ["fp16_level", "op0", "sweep", "fp16_scale", "rhs_norms", "fp16_inexact", "tiles",
-                             "tile_counts", "zero_outside", "fused_tiles", "cluster_lists", "prolong_scale"],
+                             "tile_counts", "zero_outside", "fused_tiles", "cluster_lists", "prolong_scale",
+                             "coarse_smoothing", "coarse_post_smooth"],
         "clb_batch_scene": ["base", "particle_base", "delta", "upper", "pad"],
         "clb_batch_list": ["start", "count", "total"],
         "clb_batch": ["geom_host", "particles", "cells", "colour0", "sweep0", "bottom_smem", "op0", "op",
-                      "prolong_scale"],
+                      "prolong_scale", "coarse_smoothing", "coarse_post_smooth"],
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "clb200.h"', "int main(void) {"]
     for struct, names in fields.items():

@@ -56,8 +56,10 @@ def test_reference_mode_matches_single_scenes(backend, use_graph):
 
 
 @pytest.mark.parametrize("wset", [{}, {"coarse_iterations": 4, "pre_smooth": 1, "post_smooth": 1},
-                                  {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 1, "prolong_scale": 1.7}],
-                         ids=["reference-cycle", "c4-s11", "c0-s11-w17"])
+                                  {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 1, "prolong_scale": 1.7},
+                                  {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 1, "prolong_scale": 1.8,
+                                   "coarse_smooth": (1, 0)}],
+                         ids=["reference-cycle", "c4-s11", "c0-s11-w17", "c0-s11-w18-cs10"])
 def test_tolerance_mode_solves_every_scene(backend, wset):
     sc = mixed_scenes()
     b = batch.BatchedFlip(backend, sc, flip_ratio=0.95, tol=1e-6, **wset)

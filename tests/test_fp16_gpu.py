@@ -134,9 +134,9 @@ def test_fp16_fused_sweeps_equal_per_cell_sweeps(backend, kind):
     assert backend.device_error() == 0
 
 
-@pytest.mark.parametrize("scale", [1.0, 1.7])
+@pytest.mark.parametrize("scale,cs", [(1.0, None), (1.7, None), (1.8, (1, 0))])
 @pytest.mark.parametrize("shape", [(130, 130, 130), (134, 120, 125)])
-def test_fp16_cluster_visit_equals_level_by_level(backend, shape, scale):
+def test_fp16_cluster_visit_equals_level_by_level(backend, shape, scale, cs):
     """With FP16 storage the cluster visit of the third-coarsest level (and its bottom visits) rounds
     exactly where the level-by-level kernels store FP16: W-cycles agree bit for bit."""
     dx = 1.0 / shape[0]
@@ -153,7 +153,7 @@ def test_fp16_cluster_visit_equals_level_by_level(backend, shape, scale):
             backend.lib.clb_mg_set_option(2, cluster)
             e = torch.zeros_like(rhs)
             for _ in range(2):
-                h.w_cycle(e, rhs, prolong_scale=scale)
+                h.w_cycle(e, rhs, prolong_scale=scale, coarse_smooth=cs)
             out[cluster] = e
     finally:
         backend.lib.clb_mg_set_option(2, 1)

@@ -435,6 +435,27 @@ def test_scaled_prolongation(oracle):
     assert len(hist17) + 4 <= len(hist1)  # 13 against 19 W-cycles
 
 
+def test_coarse_level_smoothing_counts(oracle):
+    """Coarse-level counts equal to the W-cycle's give the reference's W-cycle bit for bit; without the
+    coarse levels' post-smoothing and with the scaled prolongation the FCG restatement still converges."""
+    n, dx = 34, np.float32(1.0 / 34.0)
+    shape = (n, n, n)
+    mask = np.zeros(shape, np.float32)
+    mask[1:-1, 1 : n // 2 + 1, 1:-1] = 1.0
+    b = (np.random.default_rng(16).standard_normal(shape) * (mask > 0)).astype(np.float32)
+    ops = oracle.build_finest_operator(mask, shape)
+    p1, p2 = np.zeros(shape, np.float32), np.zeros(shape, np.float32)
+    oracle.Levels(shape).w_cycle(p1, b, mask, ops, dx, pre=2, post=4, coarse=8)
+    oracle.Levels(shape).w_cycle(p2, b, mask, ops, dx, pre=2, post=4, coarse=8, pre_coarse=2, post_coarse=4)
+    assert np.array_equal(p1, p2)
+    p3 = np.zeros(shape, np.float32)
+    oracle.Levels(shape).w_cycle(p3, b, mask, ops, dx, pre=2, post=4, coarse=8, pre_coarse=1, post_coarse=0)
+    assert not np.array_equal(p1, p3)
+    _, hist = oracle.fcg_solve(b, mask, shape, dx, tol=1e-8, max_cycles=60, coarse_iterations=0, pre_smooth=1,
+                               post_smooth=1, prolong_scale=1.8, coarse_smooth=(1, 0))
+    assert hist[-1] <= 1e-8 and len(hist) <= 30
+
+
 def test_fcg_with_fewer_coarse_iterations(oracle):
     """The FCG restatement still converges with a weak coarsest-level solve in its W-cycle."""
     n, dx = 18, np.float32(1.0 / 18.0)

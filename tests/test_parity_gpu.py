@@ -406,11 +406,12 @@ def test_iterative_refinement_reaches_tolerance(backend, oracle, method):
     assert np.array_equal(got, oracle.neumann_domain_bc(got, shape))
 
 
-@pytest.mark.parametrize("method,coarse,smooth,w", [("fcg", 64, (2, 4), 1.0), ("refine", 64, (2, 4), 1.0),
-                                                    ("fcg", 4, (2, 4), 1.0), ("fcg", 0, (2, 4), 1.0),
-                                                    ("fcg", 4, (1, 1), 1.0), ("fcg", 4, (1, 2), 1.0),
-                                                    ("fcg", 4, (1, 1), 1.7), ("refine", 4, (1, 1), 1.7)])
-def test_refinement_history_matches_oracle(backend, oracle, method, coarse, smooth, w):
+@pytest.mark.parametrize("method,coarse,smooth,w,cs", [("fcg", 64, (2, 4), 1.0, None), ("refine", 64, (2, 4), 1.0, None),
+                                                       ("fcg", 4, (2, 4), 1.0, None), ("fcg", 0, (2, 4), 1.0, None),
+                                                       ("fcg", 4, (1, 1), 1.0, None), ("fcg", 4, (1, 2), 1.0, None),
+                                                       ("fcg", 4, (1, 1), 1.7, None), ("refine", 4, (1, 1), 1.7, None),
+                                                       ("fcg", 0, (1, 1), 1.8, (1, 0)), ("fcg", 0, (1, 2), 1.8, (1, 0))])
+def test_refinement_history_matches_oracle(backend, oracle, method, coarse, smooth, w, cs):
     """Every W-cycle of the GPU iteration against the oracle's restatement (same FP32 W-cycle, with
     the reference's or fewer coarsest-level iterations, FP64 accumulation and scalars; only summation
     orders differ)."""
@@ -421,7 +422,7 @@ def test_refinement_history_matches_oracle(backend, oracle, method, coarse, smoo
     dt, rho = 1.0 / 240.0, 1000.0
     ps = pressure_solve.PressureSolver(backend, shape, float(dx), method=method, autotune=False,
                                        coarse_iterations=coarse, pre_smooth=smooth[0], post_smooth=smooth[1],
-                                       prolong_scale=w)
+                                       prolong_scale=w, coarse_smooth=cs)
     P = torch.zeros(shape, dtype=torch.float32, device="cuda")
     ps.solve((dev(u), dev(v), dev(w_vel)), dev(ff), P, dt, rho, tol=1e-3, use_graph=False)  # builds the system
     h = ps.hierarchy
@@ -437,7 +438,7 @@ def test_refinement_history_matches_oracle(backend, oracle, method, coarse, smoo
     orhs = oracle.pressure_rhs(u, v, w_vel, ff, dx, dt, rho, shape)
     x, want = oracle.fcg_solve(orhs, ff, shape, dx, p0=p0, tol=0.0, max_cycles=8, flexible=(method == "fcg"),
                                coarse_iterations=coarse, pre_smooth=smooth[0], post_smooth=smooth[1],
-                               prolong_scale=w)
+                               prolong_scale=w, coarse_smooth=cs)
     np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-14)  # FP64 summation orders differ
     assert want[-1] < 1e-3 * want[0]
     scale = np.abs(x).max()
@@ -581,12 +582,13 @@ def test_scaled_prolongation_matches_oracle(backend, oracle, shape, cluster):
         h.build_coarse()
         orhs = oracle.pressure_rhs(u, v, w, ff, dx, 1.0 / 240.0, 1000.0, shape)
         op = oracle.build_finest_operator(ff, shape)
-        for scale in (1.7, 1.0):
+        for scale, cs, k in ((1.7, None, 4), (1.0, None, 4), (1.8, (1, 0), 0), (1.0, (2, 1), 3)):
             P = dev(p0)
-            h.w_cycle(P, rhs, pre_smooth=1, post_smooth=1, coarse_iterations=4, prolong_scale=scale)
+            h.w_cycle(P, rhs, pre_smooth=1, post_smooth=1, coarse_iterations=k, prolong_scale=scale, coarse_smooth=cs)
             q = p0.copy()
-            oracle.Levels(shape).w_cycle(q, orhs, ff, op, dx, pre=1, post=1, coarse=4, prolong_scale=scale)
-            assert np.array_equal(host(P), q), scale
+            oracle.Levels(shape).w_cycle(q, orhs, ff, op, dx, pre=1, post=1, coarse=k, prolong_scale=scale,
+                                         pre_coarse=-1 if cs is None else cs[0], post_coarse=-1 if cs is None else cs[1])
+            assert np.array_equal(host(P), q), (scale, cs)
     finally:
         backend.lib.clb_mg_set_option(2, 1)
     assert backend.device_error() == 0
