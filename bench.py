@@ -44,7 +44,7 @@ SMOOTHING_CHOICES = ((2, 4), (2, 2), (1, 2), (1, 1))  # (pre, post); (2, 4): the
 # factor of every prolonged correction in the W-cycle preconditioner; 1.0: the reference's prolongation
 PROLONG_SCALE_CHOICES = (1.0, 1.7)
 # the W-cycle preconditioner settings the Poisson comparison picks at 256^3, used by the other cases
-TUNED_WCYCLE = {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 1, "prolong_scale": 1.8,
+TUNED_WCYCLE = {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 2, "prolong_scale": 1.8,
                 "coarse_smooth": (1, 0)}
 SCALED_COARSE_ITERATIONS = (4, 0)  # coarsest-level iterations tried with the larger factors
 # (coarse-level (pre, post) sweeps, factor) tried with 0 coarsest-level iterations and smoothing (1, 1) and
