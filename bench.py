@@ -47,9 +47,11 @@ PROLONG_SCALE_CHOICES = (1.0, 1.7)
 TUNED_WCYCLE = {"coarse_iterations": 0, "pre_smooth": 1, "post_smooth": 2, "prolong_scale": 1.8,
                 "coarse_smooth": (1, 0)}
 SCALED_COARSE_ITERATIONS = (4, 0)  # coarsest-level iterations tried with the larger factors
-# (coarse-level (pre, post) sweeps, factor) tried with 0 coarsest-level iterations and smoothing (1, 1) and
-# (1, 2) on level 0: with the scaled prolongation the coarse levels' post-smoothing can go
-COARSE_SMOOTH_VARIANTS = (((1, 0), 1.7), ((1, 0), 1.8))
+# (level-0 (pre, post) sweeps, coarse-level (pre, post) sweeps, factor) tried with 0 coarsest-level
+# iterations: with the scaled prolongation the coarse levels' post-smoothing can go, and a sweep more on
+# level 0 can save a cycle
+COARSE_SMOOTH_VARIANTS = (((1, 1), (1, 0), 1.7), ((1, 1), (1, 0), 1.8), ((1, 2), (1, 0), 1.7), ((1, 2), (1, 0), 1.8),
+                          ((1, 3), (1, 0), 1.8), ((1, 4), (1, 0), 1.8), ((2, 3), (1, 0), 1.8))
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel named (profiles/)
 NCU_TRAFFIC_BYTES = {"k_rbgs_colour<true,4>": 95_471_872 + 12_911_360,
                      "k_rbgs_colour_tiles<true,4>": 27_892_224 + 256}
@@ -804,12 +806,11 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                     kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=ps.coarse_fp16,
                     coarse_iterations=k, pre_smooth=ps.pre_smooth, post_smooth=ps.post_smooth, prolong_scale=w)
     for fp16 in (False, True):
-        for pre, post in ((1, 1), (1, 2)):
-            for cs, w in COARSE_SMOOTH_VARIANTS:
-                solvers[f"fcg{'_fp16' if fp16 else ''}_c0_s{pre}{post}_w{round(w * 10)}_cs{cs[0]}{cs[1]}"] = \
-                    PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16,
-                                   coarse_iterations=0, pre_smooth=pre, post_smooth=post, prolong_scale=w,
-                                   coarse_smooth=cs)
+        for (pre, post), cs, w in COARSE_SMOOTH_VARIANTS:
+            solvers[f"fcg{'_fp16' if fp16 else ''}_c0_s{pre}{post}_w{round(w * 10)}_cs{cs[0]}{cs[1]}"] = \
+                PressureSolver(kernels, sim.grid_shape, sim.dx, min_size=min_size, method="fcg", coarse_fp16=fp16,
+                               coarse_iterations=0, pre_smooth=pre, post_smooth=post, prolong_scale=w,
+                               coarse_smooth=cs)
     single = {}  # variant name -> first level visited once (clb_mg_set_option 4); none by default
     p_tmp = torch.empty_like(sim.pressure)
     rows = {"refine": [], "fcg": [], "fcg_fp16": [], "fcg_learned": [], "fcg_tuned_learned": []}
@@ -927,11 +928,10 @@ def poisson_comparison(kernels, sim, steps, warm, min_size):
                     r = out.get(f"{c_name(k, s)}_w{round(w * 10)}")
                     if r and r["ms_mean"] < best_ms:
                         best_w, best_k, best_s, best_ms = w, k, s, r["ms_mean"]
-        for s in ((1, 1), (1, 2)):
-            for cs, w in COARSE_SMOOTH_VARIANTS:
-                r = out.get(f"{base}_c0_s{s[0]}{s[1]}_w{round(w * 10)}_cs{cs[0]}{cs[1]}")
-                if r and r["ms_mean"] < best_ms:
-                    best_w, best_k, best_s, best_cs, best_ms = w, 0, s, cs, r["ms_mean"]
+        for s, cs, w in COARSE_SMOOTH_VARIANTS:
+            r = out.get(f"{base}_c0_s{s[0]}{s[1]}_w{round(w * 10)}_cs{cs[0]}{cs[1]}")
+            if r and r["ms_mean"] < best_ms:
+                best_w, best_k, best_s, best_cs, best_ms = w, 0, s, cs, r["ms_mean"]
     out["coarse_smooth_chosen"] = list(best_cs) if best_cs else None
     out["coarse_iterations_chosen"] = best_k
     out["smoothing_chosen"] = list(best_s)
