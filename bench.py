@@ -354,11 +354,14 @@ def sweep_case(args):
     ff = torch.from_numpy(liquid.astype(np.float32)).cuda()
     del X, Y, Z
     zero = torch.zeros(scene.grid_shape, dtype=torch.float32, device="cuda")
-    ps = PressureSolver(kernels, scene.grid_shape, scene.dx, min_size=scene.min_size, autotune=False)
+    ps = PressureSolver(kernels, scene.grid_shape, scene.dx, min_size=scene.min_size, autotune=False,
+                        coarse_fp16=args.coarse_fp16 == "on")
     ps.prepare((zero, zero, zero), ff, scene.dt, scene.rho)
     gen = torch.Generator(device="cuda").manual_seed(0)
     ps.rhs.copy_(torch.randn(scene.grid_shape, device="cuda", generator=gen) * ff)
     h = ps.hierarchy
+    if ps.coarse_fp16:
+        h.residual_norms(zero, ps.rhs)  # the FP16 levels' scale comes from the right-hand side's norm
     tune_hierarchy(h, ps.correction, ps.residual)
     kernels.call("clb_mg_set_option", 4, args.single_visit)
     if args.fused_level0:
@@ -372,10 +375,13 @@ def sweep_case(args):
         # first sweep ignoring the previous correction), fluid tiles on every level
         k = 4 if args.coarse_iterations == "auto" else int(args.coarse_iterations)
         pre, post = (2, 4) if args.smoothing == "auto" else (int(x) for x in args.smoothing.split(","))
+        w = 1.0 if args.prolong_scale == "auto" else float(args.prolong_scale)
+        cs = None if args.coarse_smooth in ("auto", "none") else tuple(int(x) for x in args.coarse_smooth.split(","))
         p.zero_()
 
         def cycle():
-            h.w_cycle(p, ps.rhs, pre_smooth=pre, post_smooth=post, coarse_iterations=k, x_from_zero=True)
+            h.w_cycle(p, ps.rhs, pre_smooth=pre, post_smooth=post, coarse_iterations=k, x_from_zero=True,
+                      prolong_scale=w, coarse_smooth=cs)
 
         cycle()
         torch.cuda.synchronize()
@@ -388,6 +394,7 @@ def sweep_case(args):
         torch.cuda.synchronize()
         print(json.dumps({"case": "wcycle", "grid": list(scene.grid_shape), "levels": [list(x) for x in h.shapes],
                           "sweep_kinds": h.sweeps(), "coarse_iterations": k, "smoothing": [pre, post],
+                          "prolong_scale": w, "coarse_smooth": list(cs) if cs else None,
                           "ms_per_w_cycle": e0.elapsed_time(e1) / args.sweeps}), flush=True)
         return
     if not args.fused_level0:
