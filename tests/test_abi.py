@@ -60,6 +60,19 @@ def test_hierarchy_struct_layout():
     assert ctypes.sizeof(backend.MGHierarchy) == tiles + 16 * 8 + 8 + 8 + 5 * 8
 
 
+def test_tuned_preconditioner_settings_agree():
+    """The benchmark's other cases run the library's tuned preconditioner settings."""
+    import importlib.util
+
+    from continuum_liquid_b200 import pressure_solve, solver
+
+    spec = importlib.util.spec_from_file_location("bench_module", Path(__file__).resolve().parents[1] / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    assert bench.TUNED_WCYCLE == pressure_solve.TUNED_PRECONDITIONER
+    solver.StepOptions(tol=1e-6, **pressure_solve.TUNED_PRECONDITIONER)  # every key is an option
+
+
 def test_backend_without_gpu_fails_loudly(monkeypatch):
     import pytest
     import torch
